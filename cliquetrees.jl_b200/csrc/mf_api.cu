@@ -1,0 +1,445 @@
+// C ABI of the B200 multifrontal numeric phase (include/mfgpu.h).
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <new>
+
+#include "../../include/mfgpu.h"
+#include "mf_internal.cuh"
+
+using namespace mf;
+
+namespace {
+
+template <typename T>
+int dalloc(mf_handle* h, T** p, int64_t count, int64_t* total) {
+    *p = nullptr;
+    if (count <= 0) return 0;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (size_t)count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string("cudaMalloc of ") + std::to_string(sizeof(T) * (size_t)count) +
+                  " bytes failed: " + cudaGetErrorString(e));
+        *p = nullptr;
+        return -4;
+    }
+    *total += sizeof(T) * count;
+    (void)h;
+    return 0;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void free_all(mf_handle* h) {
+    void* ptrs[] = {h->d_fronts, h->d_septgt, h->d_reltgt, h->d_chdtgt, h->d_colfront, h->d_Dptr, h->d_Lptr,
+                    h->d_items,  h->d_P,      h->d_M,      h->d_d,      h->d_signs,    h->d_info, h->d_R,
+                    h->d_W,      h->d_C,      h->d_B,      h->d_perm,   h->d_DL,       h->d_slot, h->d_pslot,
+                    h->d_nz};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+int init_info(mf_handle* h) {
+    static const long long big = LLONG_MAX;
+    MF_CUDA(cudaMemcpyAsync(h->d_info, &big, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+    return 0;
+}
+
+int read_info(mf_handle* h, int64_t* info) {
+    long long v = 0;
+    MF_CUDA(cudaMemcpyAsync(&v, h->d_info, sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    if (info) *info = (v == LLONG_MAX) ? 0 : (int64_t)v;
+    return 0;
+}
+
+int upload_signs(mf_handle* h, const double* signs, const double** dsigns) {
+    *dsigns = nullptr;
+    if (!signs) return 0;
+    if (!h->d_signs) {
+        int64_t tot = 0;
+        int rc = dalloc(h, &h->d_signs, h->n, &tot);
+        if (rc) return rc;
+    }
+    MF_CUDA(cudaMemcpyAsync(h->d_signs, signs, sizeof(double) * h->n, cudaMemcpyHostToDevice, h->stream));
+    *dsigns = h->d_signs;
+    return 0;
+}
+
+int64_t g_total_bytes_last = 0;
+
+}  // namespace
+
+extern "C" {
+
+const char* mf_last_error(void) { return mf::last_error(); }
+
+int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+              const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+              const int64_t* Lptr, int diag, int nrhs_cap, int device, mf_handle** out) {
+    if (!out) { set_error("mf_create: out is NULL"); return -1; }
+    *out = nullptr;
+    if (n < 0 || nfr < 0 || (n > 0 && nfr == 0) || !resptr || !sepptr || !chdptr || !Dptr || !Lptr ||
+        (nfr > 0 && !chdtgt) || (diag != 0 && diag != 1) || nrhs_cap < 1 || nrhs_cap > 16 || device < 0) {
+        set_error("mf_create: bad arguments");
+        return -1;
+    }
+    if (n > INT32_MAX / 2) { set_error("mf_create: n too large for 32-bit row indices"); return -1; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
+        cudaGetLastError();
+        set_error("mf_create: no CUDA device");
+        return -3;
+    }
+    DeviceGuard g(device);
+    mf_handle* h = new (std::nothrow) mf_handle();
+    if (!h) { set_error("out of host memory"); return -4; }
+    h->device = device;
+    h->diag = diag;
+    h->n = n;
+    h->nfr = nfr;
+    h->nrhs_cap = nrhs_cap;
+    int rc;
+    try {
+        rc = build_plan(h, resptr, sepptr, septgt, reltgt, chdptr, chdtgt, Dptr, Lptr);
+    } catch (const std::bad_alloc&) {
+        set_error("out of host memory building the plan");
+        rc = -4;
+    }
+    if (rc) { delete h; return rc; }
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaStreamCreate failed");
+        delete h;
+        return -3;
+    }
+    h->own_stream = true;
+
+    int64_t tot = 0;
+    int64_t nsep = h->nsep;
+    std::vector<int32_t> sep32(nsep), rel32(nsep), chd32(nfr), colfront(n);
+    for (int64_t i = 0; i < nsep; ++i) { sep32[i] = (int32_t)septgt[i]; rel32[i] = (int32_t)reltgt[i]; }
+    for (int64_t i = 0; i < nfr; ++i) chd32[i] = (int32_t)chdtgt[i];
+    for (int64_t j = 0; j < nfr; ++j)
+        for (int64_t c = resptr[j]; c < resptr[j + 1]; ++c) colfront[c] = (int32_t)j;
+    rc = 0;
+    rc = rc ? rc : dalloc(h, &h->d_fronts, nfr, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_septgt, nsep, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_reltgt, nsep, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_chdtgt, nfr, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_colfront, n, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_Dptr, nfr + 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_Lptr, nfr + 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_items, (int64_t)h->h_items.size(), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_P, h->npanel, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_M, h->nmval, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_d, std::max<int64_t>(n, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_info, 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_R, std::max<int64_t>(h->nrval_per_rhs * nrhs_cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_W, std::max<int64_t>(n * nrhs_cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_C, std::max<int64_t>(n * nrhs_cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_B, std::max<int64_t>(n * nrhs_cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_perm, std::max<int64_t>(n, 1), &tot);
+    if (rc) { free_all(h); delete h; return rc; }
+    auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+        if (!bytes) return cudaSuccess;
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = up(h->d_fronts, h->h_fronts.data(), sizeof(Front) * nfr);
+    if (e == cudaSuccess) e = up(h->d_septgt, sep32.data(), sizeof(int32_t) * nsep);
+    if (e == cudaSuccess) e = up(h->d_reltgt, rel32.data(), sizeof(int32_t) * nsep);
+    if (e == cudaSuccess) e = up(h->d_chdtgt, chd32.data(), sizeof(int32_t) * nfr);
+    if (e == cudaSuccess) e = up(h->d_colfront, colfront.data(), sizeof(int32_t) * n);
+    if (e == cudaSuccess) e = up(h->d_Dptr, Dptr, sizeof(int64_t) * (nfr + 1));
+    if (e == cudaSuccess) e = up(h->d_Lptr, Lptr, sizeof(int64_t) * (nfr + 1));
+    if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
+    if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
+    if (e != cudaSuccess) {
+        cuda_fail(e, "mf_create upload");
+        free_all(h);
+        delete h;
+        return -3;
+    }
+    g_total_bytes_last = tot;
+    h->times = KernelTimes();
+    // remember the allocation size in the level-independent slot of times
+    h->times.ms[15] = (double)tot;
+    *out = h;
+    return 0;
+}
+
+void mf_destroy(mf_handle* h) {
+    if (!h) return;
+    DeviceGuard g(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+}
+
+int mf_set_stream(mf_handle* h, void* stream) {
+    if (!h) { set_error("null handle"); return -1; }
+    DeviceGuard g(h->device);
+    if (h->own_stream && h->stream) {
+        cudaStreamSynchronize(h->stream);
+        cudaStreamDestroy(h->stream);
+        h->own_stream = false;
+        h->stream = nullptr;
+    }
+    if (stream) {
+        h->stream = (cudaStream_t)stream;
+        h->own_stream = false;
+    } else {
+        MF_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        h->own_stream = true;
+    }
+    return 0;
+}
+
+int mf_chol_impl(mf_handle* h, double* Dval, double* Lval, double* d, const double* signs, int64_t* info) {
+    if (!h || (!Dval && h->ndz) || (!Lval && h->nlz) || (h->diag && !d && h->n)) {
+        set_error("mf_chol_impl: bad arguments");
+        return -1;
+    }
+    DeviceGuard g(h->device);
+    int rc;
+    if (!h->d_DL) {
+        int64_t tot = 0;
+        if ((rc = dalloc(h, &h->d_DL, std::max<int64_t>(h->ndz + h->nlz, 1), &tot))) return rc;
+    }
+    if (h->ndz)
+        MF_CUDA(cudaMemcpyAsync(h->d_DL, Dval, sizeof(double) * h->ndz, cudaMemcpyHostToDevice, h->stream));
+    if (h->nlz)
+        MF_CUDA(cudaMemcpyAsync(h->d_DL + h->ndz, Lval, sizeof(double) * h->nlz, cudaMemcpyHostToDevice,
+                                h->stream));
+    if ((rc = launch_dl_to_panel(h, h->d_DL, h->d_DL + h->ndz))) return rc;
+    const double* ds = nullptr;
+    if ((rc = upload_signs(h, signs, &ds))) return rc;
+    double* keep = h->d_signs;
+    h->d_signs = const_cast<double*>(ds);
+    if ((rc = init_info(h))) { h->d_signs = keep; return rc; }
+    rc = launch_factor(h);
+    h->d_signs = keep;
+    if (rc) return rc;
+    if ((rc = launch_panel_to_dl(h, h->d_DL, h->d_DL + h->ndz))) return rc;
+    if (h->ndz)
+        MF_CUDA(cudaMemcpyAsync(Dval, h->d_DL, sizeof(double) * h->ndz, cudaMemcpyDeviceToHost, h->stream));
+    if (h->nlz)
+        MF_CUDA(cudaMemcpyAsync(Lval, h->d_DL + h->ndz, sizeof(double) * h->nlz, cudaMemcpyDeviceToHost,
+                                h->stream));
+    if (h->diag && h->n)
+        MF_CUDA(cudaMemcpyAsync(d, h->d_d, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    return read_info(h, info);
+}
+
+static int solve_chunks(mf_handle* h, const int64_t* dperm, double* hostB, double* devB, int64_t nrhs, int64_t ldb) {
+    int rc;
+    for (int64_t c0 = 0; c0 < nrhs; c0 += h->nrhs_cap) {
+        int64_t nc = std::min<int64_t>(h->nrhs_cap, nrhs - c0);
+        if (hostB) {
+            if (dperm) {
+                MF_CUDA(cudaMemcpy2DAsync(h->d_B, sizeof(double) * h->n, hostB + c0 * ldb, sizeof(double) * ldb,
+                                          sizeof(double) * h->n, nc, cudaMemcpyHostToDevice, h->stream));
+                if ((rc = launch_permute_in(h, h->d_B, h->n, dperm, nc))) return rc;
+            } else {
+                MF_CUDA(cudaMemcpy2DAsync(h->d_C, sizeof(double) * h->n, hostB + c0 * ldb, sizeof(double) * ldb,
+                                          sizeof(double) * h->n, nc, cudaMemcpyHostToDevice, h->stream));
+            }
+        } else {
+            if ((rc = launch_permute_in(h, devB + c0 * ldb, ldb, dperm, nc))) return rc;
+        }
+        if ((rc = launch_solve(h, nc))) return rc;
+        if (hostB) {
+            if (dperm) {
+                if ((rc = launch_permute_out(h, h->d_B, h->n, dperm, nc))) return rc;
+                MF_CUDA(cudaMemcpy2DAsync(hostB + c0 * ldb, sizeof(double) * ldb, h->d_B, sizeof(double) * h->n,
+                                          sizeof(double) * h->n, nc, cudaMemcpyDeviceToHost, h->stream));
+            } else {
+                MF_CUDA(cudaMemcpy2DAsync(hostB + c0 * ldb, sizeof(double) * ldb, h->d_C, sizeof(double) * h->n,
+                                          sizeof(double) * h->n, nc, cudaMemcpyDeviceToHost, h->stream));
+            }
+        } else {
+            if ((rc = launch_permute_out(h, devB + c0 * ldb, ldb, dperm, nc))) return rc;
+        }
+    }
+    return 0;
+}
+
+int mf_div_impl(mf_handle* h, double* B, int64_t nrhs, int64_t ldb) {
+    if (!h || nrhs < 0 || (nrhs > 0 && (!B || ldb < h->n))) { set_error("mf_div_impl: bad arguments"); return -1; }
+    DeviceGuard g(h->device);
+    int rc = solve_chunks(h, nullptr, B, nullptr, nrhs, ldb);
+    if (rc) return rc;
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot) {
+    if (!h || nnz < 0 || (nnz > 0 && !slot)) { set_error("mf_set_assembly: bad arguments"); return -1; }
+    DeviceGuard g(h->device);
+    std::vector<int64_t> pslot(nnz);
+    const int64_t ndz = h->ndz, nlz = h->nlz;
+    std::vector<char> seen;
+    for (int64_t k = 0; k < nnz; ++k) {
+        int64_t s = slot[k];
+        if (s < 0 || s >= ndz + nlz) { set_error("mf_set_assembly: slot out of range"); return -2; }
+        int64_t p;
+        if (s < ndz) {
+            int64_t j = std::upper_bound(h->h_Dptr.begin(), h->h_Dptr.end(), s) - h->h_Dptr.begin() - 1;
+            const Front& f = h->h_fronts[j];
+            int64_t loc = s - h->h_Dptr[j];
+            int64_t r = loc % f.nn, c = loc / f.nn;
+            if (r < c) { set_error("mf_set_assembly: slot in the upper triangle of a diagonal block"); return -2; }
+            p = f.poff + r + c * (int64_t)(f.nn + f.na);
+        } else {
+            int64_t s2 = s - ndz;
+            int64_t j = std::upper_bound(h->h_Lptr.begin(), h->h_Lptr.end(), s2) - h->h_Lptr.begin() - 1;
+            const Front& f = h->h_fronts[j];
+            int64_t loc = s2 - h->h_Lptr[j];
+            int64_t a = loc % f.na, c = loc / f.na;
+            p = f.poff + f.nn + a + c * (int64_t)(f.nn + f.na);
+        }
+        pslot[k] = p;
+    }
+    {
+        // slots must be distinct: the scatter writes each entry once
+        std::vector<int64_t> tmp(pslot);
+        std::sort(tmp.begin(), tmp.end());
+        if (std::adjacent_find(tmp.begin(), tmp.end()) != tmp.end()) {
+            set_error("mf_set_assembly: duplicate slots");
+            return -2;
+        }
+    }
+    if (h->d_pslot) { cudaFree(h->d_pslot); h->d_pslot = nullptr; }
+    if (h->d_nz) { cudaFree(h->d_nz); h->d_nz = nullptr; }
+    int64_t tot = 0;
+    int rc;
+    if ((rc = dalloc(h, &h->d_pslot, std::max<int64_t>(nnz, 1), &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_nz, std::max<int64_t>(nnz, 1), &tot))) return rc;
+    if (nnz) MF_CUDA(cudaMemcpy(h->d_pslot, pslot.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));
+    h->nnz = nnz;
+    return 0;
+}
+
+int mf_assemble(mf_handle* h, const double* nzval) {
+    if (!h || (h->nnz && !nzval)) { set_error("mf_assemble: bad arguments"); return -1; }
+    if (!h->d_pslot) { set_error("mf_assemble: call mf_set_assembly first"); return -1; }
+    DeviceGuard g(h->device);
+    if (h->nnz)
+        MF_CUDA(cudaMemcpyAsync(h->d_nz, nzval, sizeof(double) * h->nnz, cudaMemcpyHostToDevice, h->stream));
+    return launch_assemble(h, h->d_nz);
+}
+
+int mf_assemble_device(mf_handle* h, const double* nzval_dev) {
+    if (!h || (h->nnz && !nzval_dev)) { set_error("mf_assemble_device: bad arguments"); return -1; }
+    if (!h->d_pslot) { set_error("mf_assemble_device: call mf_set_assembly first"); return -1; }
+    DeviceGuard g(h->device);
+    return launch_assemble(h, nzval_dev);
+}
+
+int mf_factorize(mf_handle* h, const double* signs, int64_t* info) {
+    if (!h) { set_error("null handle"); return -1; }
+    DeviceGuard g(h->device);
+    const double* ds = nullptr;
+    int rc;
+    if ((rc = upload_signs(h, signs, &ds))) return rc;
+    double* keep = h->d_signs;
+    h->d_signs = const_cast<double*>(ds);
+    if ((rc = init_info(h))) { h->d_signs = keep; return rc; }
+    rc = launch_factor(h);
+    h->d_signs = keep;
+    if (rc) return rc;
+    if (info) return read_info(h, info);
+    return 0;
+}
+
+int mf_solve(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm) {
+    if (!h || nrhs < 0 || (nrhs > 0 && (!B || ldb < h->n))) { set_error("mf_solve: bad arguments"); return -1; }
+    DeviceGuard g(h->device);
+    if (perm && h->n) {
+        for (int64_t i = 0; i < h->n; ++i)
+            if (perm[i] < 0 || perm[i] >= h->n) { set_error("mf_solve: perm out of range"); return -2; }
+        MF_CUDA(cudaMemcpyAsync(h->d_perm, perm, sizeof(int64_t) * h->n, cudaMemcpyHostToDevice, h->stream));
+    }
+    int rc = solve_chunks(h, h->d_perm, B, nullptr, nrhs, ldb);
+    if (rc) return rc;
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev) {
+    if (!h || nrhs < 0 || (nrhs > 0 && (!B_dev || ldb < h->n))) {
+        set_error("mf_solve_device: bad arguments");
+        return -1;
+    }
+    DeviceGuard g(h->device);
+    return solve_chunks(h, perm_dev ? perm_dev : h->d_perm, nullptr, B_dev, nrhs, ldb);
+}
+
+int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d) {
+    if (!h) { set_error("null handle"); return -1; }
+    DeviceGuard g(h->device);
+    int rc;
+    if (Dval || Lval) {
+        if (!h->d_DL) {
+            int64_t tot = 0;
+            if ((rc = dalloc(h, &h->d_DL, std::max<int64_t>(h->ndz + h->nlz, 1), &tot))) return rc;
+        }
+        if ((rc = launch_panel_to_dl(h, h->d_DL, h->d_DL + h->ndz))) return rc;
+        if (Dval && h->ndz)
+            MF_CUDA(cudaMemcpyAsync(Dval, h->d_DL, sizeof(double) * h->ndz, cudaMemcpyDeviceToHost, h->stream));
+        if (Lval && h->nlz)
+            MF_CUDA(cudaMemcpyAsync(Lval, h->d_DL + h->ndz, sizeof(double) * h->nlz, cudaMemcpyDeviceToHost,
+                                    h->stream));
+    }
+    if (d && h->n) MF_CUDA(cudaMemcpyAsync(d, h->d_d, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_synchronize(mf_handle* h) {
+    if (!h) { set_error("null handle"); return -1; }
+    DeviceGuard g(h->device);
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_info(const mf_handle* h, int64_t* out) {
+    if (!h || !out) { set_error("mf_info: bad arguments"); return -1; }
+    out[0] = h->n; out[1] = h->nfr; out[2] = h->ndz; out[3] = h->nlz;
+    out[4] = h->npanel; out[5] = h->nmval; out[6] = (int64_t)h->times.ms[15];
+    out[7] = (int64_t)h->levels.size();
+    return 0;
+}
+
+int mf_profile(mf_handle* h, int enable) {
+    if (!h) { set_error("null handle"); return -1; }
+    double keep = h->times.ms[15];
+    h->profile = enable != 0;
+    h->times = KernelTimes();
+    h->times.ms[15] = keep;
+    return 0;
+}
+
+int mf_kernel_times(const mf_handle* h, double* ms, int64_t* launches) {
+    if (!h) { set_error("null handle"); return -1; }
+    for (int k = 0; k < K_COUNT; ++k) {
+        if (ms) ms[k] = h->times.ms[k];
+        if (launches) launches[k] = h->times.launches[k];
+    }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// Internal declarations of the B200 multifrontal numeric phase.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace mf {
+
+// ---------------------------------------------------------------------------
+// Device layout.  Every front j (postorder, 0-based) owns
+//   * a panel   P_j : nj x nn column major, leading dimension nj, at Pval+poff.
+//                     Rows 0..nn-1 are the diagonal block D (lower triangle
+//                     used), rows nn..nj-1 are the off-diagonal block L.
+//                     This is the reference's Dval/Lval pair stacked into one
+//                     matrix so that every kernel sees one leading dimension.
+//   * an update matrix M_j : na x na column major (lower triangle used) at
+//                     Mval+moff, alive from the factorization of j until its
+//                     parent has been assembled.
+// ---------------------------------------------------------------------------
+struct Front {
+    int64_t poff;   // panel offset in Pval
+    int64_t moff;   // update-matrix offset in Mval (na > 0)
+    int64_t roff;   // offset of this front's solve update (na x nrhs_cap) in Rval
+    int32_t nn;     // |res(j)|
+    int32_t na;     // |sep(j)|
+    int32_t col0;   // first (permuted) column of res(j)
+    int32_t sep0;   // offset of sep(j)/rel(j) in septgt/reltgt
+    int32_t chd0;   // children of j are chdtgt[chd0:chd1]
+    int32_t chd1;
+    int32_t parent; // -1 for roots
+    int32_t level;  // height above the leaves
+};
+
+// One unit of grouped work: front plus up to two tile coordinates.
+struct Item {
+    int32_t front;
+    int32_t a;
+    int32_t b;
+    int32_t pad;
+};
+
+// A contiguous list of items inside the uploaded item buffer.
+struct ItemList {
+    int64_t off = 0;
+    int64_t cnt = 0;
+};
+
+constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
+constexpr int kNB = 64;         // panel width of the blocked path
+constexpr int kTile = 64;       // tile edge of the grouped update kernels
+constexpr int kEAcols = 16;     // parent columns per extend-add work item
+constexpr int kSolveRows = 128; // rows per solve work item
+
+struct PanelStep {
+    ItemList panel;   // (front, row tile)  : diag factor + panel TRSM
+    ItemList update;  // (front, ti, tj)    : trailing update inside the panel
+};
+
+struct SolveStep {
+    ItemList fwd;     // (front, row tile)
+    ItemList bwd;     // (front, col tile)
+};
+
+struct Level {
+    ItemList small;          // (front)           fused small-front kernel
+    ItemList ea;             // (front, col tile) extend-add for blocked fronts
+    std::vector<PanelStep> steps;
+    ItemList syrk;           // (front, ti, tj)   M -= L L^T
+    // solves
+    ItemList s_small;        // (front)
+    ItemList s_gather;       // (front, row tile) forward gather of child updates
+    std::vector<SolveStep> s_steps;
+    ItemList s_bwd_l;        // (front, col tile) C1 -= L^T x[sep]
+    int max_nn_blocked = 0;
+};
+
+struct KernelTimes {
+    double ms[16] = {0};
+    int64_t launches[16] = {0};
+};
+
+enum KernelId {
+    K_ASSEMBLE = 0, K_SMALL, K_EA, K_PANEL, K_UPDATE, K_SYRK,
+    K_S_SMALL, K_S_GATHER, K_S_FWD, K_S_BWD_L, K_S_BWD, K_PERM, K_OTHER, K_COUNT
+};
+
+}  // namespace mf
+
+struct mf_handle {
+    int device = 0;
+    int diag = 0;                 // 0 Cholesky, 1 LDLt
+    int64_t n = 0, nfr = 0, nsep = 0;
+    int64_t ndz = 0, nlz = 0, npanel = 0, nmval = 0, nrval_per_rhs = 0;
+    int nrhs_cap = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // host copies
+    std::vector<mf::Front> h_fronts;
+    std::vector<int64_t> h_resptr, h_sepptr, h_Dptr, h_Lptr;
+    std::vector<mf::Level> levels;
+    std::vector<mf::Item> h_items;
+
+    // device symbolic
+    mf::Front* d_fronts = nullptr;
+    int32_t* d_septgt = nullptr;
+    int32_t* d_reltgt = nullptr;
+    int32_t* d_chdtgt = nullptr;
+    int32_t* d_colfront = nullptr;  // column -> front (n)
+    int64_t* d_Dptr = nullptr;      // reference Dval offsets (nfr+1)
+    int64_t* d_Lptr = nullptr;      // reference Lval offsets (nfr+1)
+    mf::Item* d_items = nullptr;
+
+    // device numeric
+    double* d_P = nullptr;         // panels
+    double* d_M = nullptr;         // update matrices
+    double* d_d = nullptr;         // LDLt pivots (n)
+    double* d_signs = nullptr;     // pivot signs (n) or null
+    long long* d_info = nullptr;   // first failing column (1-based), LLONG_MAX if none
+    double* d_R = nullptr;         // solve updates (sum na * nrhs_cap)
+    double* d_W = nullptr;         // solve work (n * nrhs_cap)
+    double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
+    double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
+    int64_t* d_perm = nullptr;     // permutation (n)
+    double* d_DL = nullptr;        // staging for reference-layout Dval|Lval (ndz+nlz)
+    int64_t* d_slot = nullptr;     // assembly map into Dval|Lval (nnz)
+    int64_t* d_pslot = nullptr;    // assembly map into panels (nnz)
+    double* d_nz = nullptr;        // nonzero values staging (nnz)
+    int64_t nnz = 0;
+
+    // optional per-kernel timing
+    bool profile = false;
+    mf::KernelTimes times;
+    std::vector<cudaEvent_t> ev_pool;
+};
+
+namespace mf {
+
+void set_error(const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define MF_CUDA(call)                                                  \
+    do {                                                               \
+        cudaError_t _e = (call);                                       \
+        if (_e != cudaSuccess) return mf::cuda_fail(_e, #call);        \
+    } while (0)
+
+// plan construction (mf_plan.cu)
+int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+               const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+               const int64_t* Lptr);
+
+// kernel launchers (mf_factor.cu / mf_solve.cu); all stream ordered
+int launch_factor(mf_handle* h);
+int launch_dl_to_panel(mf_handle* h, const double* dDval, const double* dLval);
+int launch_panel_to_dl(mf_handle* h, double* dDval, double* dLval);
+int launch_assemble(mf_handle* h, const double* dnz);
+int launch_solve(mf_handle* h, int64_t nrhs);
+int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
+int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
+const char* last_error();
+
+// timing helpers
+struct Timer {
+    mf_handle* h;
+    int k;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer(mf_handle* h_, int k_);
+    ~Timer();
+};
+
+}  // namespace mf

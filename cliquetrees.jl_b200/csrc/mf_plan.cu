@@ -1,0 +1,327 @@
+// Host-side plan: per-front device metadata, level schedule and the grouped
+// work lists each kernel launch consumes.  Built once per sparsity pattern.
+//
+// The reference walks the fronts in postorder with one LIFO stack of update
+// matrices (chol_impl!, src/Multifrontal.jl/src/cholesky.jl:361-392).  Here
+// fronts are grouped by height in the tree: all fronts of one level depend
+// only on lower levels, so each level is a handful of grouped launches.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <set>
+
+#include "mf_internal.cuh"
+
+namespace mf {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+const char* last_error() { return g_last_error.c_str(); }
+
+int cuda_fail(cudaError_t e, const char* where) {
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return -3;
+}
+
+static inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Best-fit allocator over one device pool (offsets in elements).  Blocks
+// are 32-element aligned; freed neighbours are coalesced.  Used to give the
+// update matrices (and the forward-solve updates) of each front a slot that
+// lives from the level that produces it to the level of its parent, so the
+// pool holds only the live frontier instead of every front at once.
+class PoolAllocator {
+  public:
+    int64_t alloc(int64_t size) {
+        size = (size + 31) & ~int64_t(31);
+        if (size == 0) return 0;
+        auto it = by_size_.lower_bound({size, -1});
+        if (it != by_size_.end()) {
+            int64_t off = it->second, bsz = it->first;
+            by_size_.erase(it);
+            by_off_.erase(off);
+            if (bsz > size) insert_free(off + size, bsz - size);
+            return off;
+        }
+        // grow: extend a free block that touches the end, else append
+        if (!by_off_.empty()) {
+            auto last = std::prev(by_off_.end());
+            if (last->first + last->second == top_) {
+                int64_t off = last->first;
+                by_size_.erase({last->second, off});
+                by_off_.erase(last);
+                top_ = off + size;
+                return off;
+            }
+        }
+        int64_t off = top_;
+        top_ += size;
+        return off;
+    }
+    void release(int64_t off, int64_t size) {
+        size = (size + 31) & ~int64_t(31);
+        if (size == 0) return;
+        auto nx = by_off_.lower_bound(off);
+        if (nx != by_off_.end() && nx->first == off + size) {
+            size += nx->second;
+            by_size_.erase({nx->second, nx->first});
+            nx = by_off_.erase(nx);
+        }
+        if (nx != by_off_.begin()) {
+            auto pv = std::prev(nx);
+            if (pv->first + pv->second == off) {
+                off = pv->first;
+                size += pv->second;
+                by_size_.erase({pv->second, pv->first});
+                by_off_.erase(pv);
+            }
+        }
+        insert_free(off, size);
+    }
+    int64_t high_water() const { return top_; }
+
+  private:
+    void insert_free(int64_t off, int64_t size) {
+        by_off_[off] = size;
+        by_size_.insert({size, off});
+    }
+    std::map<int64_t, int64_t> by_off_;
+    std::set<std::pair<int64_t, int64_t>> by_size_;
+    int64_t top_ = 0;
+};
+
+int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+               const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+               const int64_t* Lptr) {
+    const int64_t nfr = h->nfr, n = h->n;
+    // ---- validate the symbolic input (a corrupted pattern must not reach a kernel)
+    if (resptr[0] != 0 || resptr[nfr] != n) { set_error("resptr does not cover 0..n"); return -2; }
+    if (sepptr[0] != 0) { set_error("sepptr must start at 0"); return -2; }
+    if (chdptr[0] != 0 || chdptr[nfr + 1] != nfr) { set_error("chdptr must cover nfr children"); return -2; }
+    h->nsep = sepptr[nfr];
+    std::vector<int32_t> parent(nfr, -1);
+    for (int64_t j = 0; j < nfr; ++j) {
+        if (resptr[j + 1] <= resptr[j]) { set_error("empty residual"); return -2; }
+        if (sepptr[j + 1] < sepptr[j]) { set_error("sepptr not monotone"); return -2; }
+        if (resptr[j + 1] - resptr[j] + sepptr[j + 1] - sepptr[j] > (int64_t)1 << 30) {
+            set_error("front too large"); return -2;
+        }
+    }
+    for (int64_t j = 0; j <= nfr; ++j) {
+        if (chdptr[j + 1] < chdptr[j]) { set_error("chdptr not monotone"); return -2; }
+        for (int64_t p = chdptr[j]; p < chdptr[j + 1]; ++p) {
+            int64_t c = chdtgt[p];
+            if (c < 0 || c >= nfr) { set_error("child index out of range"); return -2; }
+            if (j < nfr && c >= j) { set_error("tree is not postordered (child >= parent)"); return -2; }
+            if (parent[c] != -1) { set_error("front has two parents"); return -2; }
+            parent[c] = (int32_t)(j < nfr ? j : -1);
+        }
+    }
+    for (int64_t j = 0; j < nfr; ++j) {
+        int64_t nn = resptr[j + 1] - resptr[j], na = sepptr[j + 1] - sepptr[j];
+        int64_t prev = resptr[j + 1] - 1;
+        for (int64_t p = sepptr[j]; p < sepptr[j + 1]; ++p) {
+            if (septgt[p] <= prev || septgt[p] >= n) { set_error("separator rows not increasing past res"); return -2; }
+            prev = septgt[p];
+        }
+        int64_t pj = parent[j];
+        if (na > 0 && pj < 0) { set_error("root front with a separator"); return -2; }
+        if (pj >= 0) {
+            int64_t pn = resptr[pj + 1] - resptr[pj] + sepptr[pj + 1] - sepptr[pj];
+            int64_t prevr = -1;
+            for (int64_t p = sepptr[j]; p < sepptr[j + 1]; ++p) {
+                int64_t r = reltgt[p];
+                if (r <= prevr || r >= pn) { set_error("rel index outside the parent bag"); return -2; }
+                // rel must point at the same global row in the parent's bag
+                int64_t pnn = resptr[pj + 1] - resptr[pj];
+                int64_t row = r < pnn ? resptr[pj] + r : septgt[sepptr[pj] + r - pnn];
+                if (row != septgt[p]) { set_error("rel index does not match the parent's bag"); return -2; }
+                prevr = r;
+            }
+        }
+        if (Dptr[j + 1] - Dptr[j] != nn * nn || Lptr[j + 1] - Lptr[j] != nn * na) {
+            set_error("Dptr/Lptr disagree with the front sizes"); return -2;
+        }
+        (void)nn;
+    }
+    h->ndz = Dptr[nfr];
+    h->nlz = Lptr[nfr];
+    h->h_resptr.assign(resptr, resptr + nfr + 1);
+    h->h_sepptr.assign(sepptr, sepptr + nfr + 1);
+    h->h_Dptr.assign(Dptr, Dptr + nfr + 1);
+    h->h_Lptr.assign(Lptr, Lptr + nfr + 1);
+
+    // ---- fronts, levels, offsets
+    h->h_fronts.resize(nfr);
+    int64_t poff = 0;
+    int max_level = 0;
+    std::vector<int32_t> level(nfr, 0);
+    for (int64_t j = 0; j < nfr; ++j) {
+        int64_t pj = parent[j];
+        if (pj >= 0) level[pj] = std::max(level[pj], level[j] + 1);
+    }
+    for (int64_t j = 0; j < nfr; ++j) {
+        Front& f = h->h_fronts[j];
+        int64_t nn = resptr[j + 1] - resptr[j], na = sepptr[j + 1] - sepptr[j];
+        f.nn = (int32_t)nn; f.na = (int32_t)na;
+        f.col0 = (int32_t)resptr[j];
+        f.sep0 = (int32_t)sepptr[j];
+        f.chd0 = (int32_t)chdptr[j]; f.chd1 = (int32_t)chdptr[j + 1];
+        f.parent = parent[j];
+        f.level = level[j];
+        f.poff = poff; poff += (nn + na) * nn;
+        f.moff = 0;
+        f.roff = 0;
+        max_level = std::max(max_level, level[j]);
+    }
+    h->npanel = poff;
+    {
+        // slot lifetimes: produced at level(j), read while level(parent(j))
+        // is processed, reusable from the next level on
+        std::vector<std::vector<int32_t>> born(max_level + 1), dies(max_level + 1);
+        for (int64_t j = 0; j < nfr; ++j) {
+            if (h->h_fronts[j].na == 0) continue;
+            born[level[j]].push_back((int32_t)j);
+            dies[level[parent[j]]].push_back((int32_t)j);
+        }
+        PoolAllocator pm, pr;
+        for (int L = 0; L <= max_level; ++L) {
+            for (int32_t j : born[L]) {
+                Front& f = h->h_fronts[j];
+                f.moff = pm.alloc((int64_t)f.na * f.na);
+                f.roff = pr.alloc((int64_t)f.na);  // rows; block is R + roff*nrhs
+            }
+            for (int32_t j : dies[L]) {
+                Front& f = h->h_fronts[j];
+                pm.release(f.moff, (int64_t)f.na * f.na);
+                pr.release(f.roff, (int64_t)f.na);
+            }
+        }
+        h->nmval = pm.high_water();
+        h->nrval_per_rhs = pr.high_water();
+    }
+
+    // ---- work lists
+    h->levels.assign(max_level + 1, Level());
+    std::vector<std::vector<int32_t>> by_level(max_level + 1);
+    for (int64_t j = 0; j < nfr; ++j) by_level[level[j]].push_back((int32_t)j);
+    std::vector<Item>& items = h->h_items;
+    items.clear();
+    auto begin = [&](ItemList& l) { l.off = (int64_t)items.size(); };
+    auto end = [&](ItemList& l) { l.cnt = (int64_t)items.size() - l.off; };
+    auto push = [&](int32_t f, int32_t a, int32_t b) { items.push_back(Item{f, a, b, 0}); };
+
+    for (int L = 0; L <= max_level; ++L) {
+        Level& lv = h->levels[L];
+        const std::vector<int32_t>& fr = by_level[L];
+        // factorization
+        begin(lv.small);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn + f.na <= kSmallMax) push(j, 0, 0);
+        }
+        end(lv.small);
+        begin(lv.ea);
+        int max_steps = 0;
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            int nj = f.nn + f.na;
+            if (nj <= kSmallMax) continue;
+            for (int t = 0; t < cdiv(nj, kEAcols); ++t) push(j, t, 0);
+            max_steps = std::max<int>(max_steps, (int)cdiv(f.nn, kNB));
+            lv.max_nn_blocked = std::max(lv.max_nn_blocked, f.nn);
+        }
+        end(lv.ea);
+        lv.steps.resize(max_steps);
+        for (int k = 0; k < max_steps; ++k) {
+            PanelStep& st = lv.steps[k];
+            begin(st.panel);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                int nj = f.nn + f.na;
+                if (nj <= kSmallMax || f.nn <= k * kNB) continue;
+                int w = std::min(kNB, f.nn - k * kNB);
+                int below = nj - (k * kNB + w);
+                int tiles = 1 + (int)cdiv(below, kTile);
+                for (int t = 0; t < tiles; ++t) push(j, t, 0);
+            }
+            end(st.panel);
+            begin(st.update);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                int nj = f.nn + f.na;
+                if (nj <= kSmallMax || f.nn <= k * kNB) continue;
+                int c0 = k * kNB + std::min(kNB, f.nn - k * kNB);
+                if (c0 >= f.nn) continue;
+                int ctiles = (int)cdiv(f.nn - c0, kTile);
+                for (int tj = 0; tj < ctiles; ++tj) {
+                    int cs = c0 + tj * kTile;
+                    int rtiles = (int)cdiv(nj - cs, kTile);
+                    for (int ti = 0; ti < rtiles; ++ti) push(j, ti, tj);
+                }
+            }
+            end(st.update);
+        }
+        begin(lv.syrk);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn + f.na <= kSmallMax || f.na == 0) continue;
+            int t = (int)cdiv(f.na, kTile);
+            for (int tj = 0; tj < t; ++tj)
+                for (int ti = tj; ti < t; ++ti) push(j, ti, tj);
+        }
+        end(lv.syrk);
+
+        // solves
+        begin(lv.s_small);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn <= kNB && f.na <= 1024) push(j, 0, 0);
+        }
+        end(lv.s_small);
+        begin(lv.s_gather);
+        int max_sblocks = 0;
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn <= kNB && f.na <= 1024) continue;
+            int nj = f.nn + f.na;
+            for (int t = 0; t < cdiv(nj, kSolveRows); ++t) push(j, t, 0);
+            max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kNB));
+        }
+        end(lv.s_gather);
+        lv.s_steps.resize(max_sblocks);
+        for (int k = 0; k < max_sblocks; ++k) {
+            SolveStep& st = lv.s_steps[k];
+            begin(st.fwd);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                if ((f.nn <= kNB && f.na <= 1024) || f.nn <= k * kNB) continue;
+                int nj = f.nn + f.na;
+                int w = std::min(kNB, f.nn - k * kNB);
+                int below = nj - (k * kNB + w);
+                int tiles = 1 + (int)cdiv(below, kSolveRows);
+                for (int t = 0; t < tiles; ++t) push(j, t, 0);
+            }
+            end(st.fwd);
+            begin(st.bwd);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                if ((f.nn <= kNB && f.na <= 1024) || f.nn <= k * kNB) continue;
+                int tiles = 1 + (int)cdiv(k * kNB, kNB);
+                for (int t = 0; t < tiles; ++t) push(j, t, 0);
+            }
+            end(st.bwd);
+        }
+        begin(lv.s_bwd_l);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn <= kNB && f.na <= 1024) continue;
+            for (int t = 0; t < cdiv(f.nn, kNB); ++t) push(j, t, 0);
+        }
+        end(lv.s_bwd_l);
+    }
+    return 0;
+}
+
+}  // namespace mf

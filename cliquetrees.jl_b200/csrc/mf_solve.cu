@@ -1,0 +1,456 @@
+// Supernodal forward and backward solves (FP64) for the B200 multifrontal
+// solver, with many right-hand sides.
+//
+// Reference: div_impl! (src/Multifrontal.jl/src/divide.jl:417-450), the
+// forward loop div_fwd_loop_snd!/_nod! (:493-821) with div_fwd_update!
+// (:1206-1248), the backward loop div_bwd_loop_snd!/_nod! (:864-1204) with
+// div_bwd_update! (:1250-1293), and ldiv!(W, NaturalFactorization, B)
+// (:191-199) for the L, D, L^T sequence.
+//
+// Layout: C (n x nrhs, ld n) holds the right-hand sides in elimination
+// order and receives the solution.  Forward updates of front j (the
+// reference's M2 = F2 - L21 C1 pushed on the stack) live at R + roff_j*nrhs
+// (na x nrhs, ld na) and are pulled by the parent.  In the backward pass the
+// reference pushes F restricted to sep(i) to each child; that vector is the
+// already-final solution at rows sep(i), so children read it from C directly.
+#include "mf_internal.cuh"
+
+namespace mf {
+
+constexpr int kMaxRhs = 16;   // right-hand sides per pass (larger counts are chunked)
+constexpr int SLD = kNB + 1;  // smem leading dimension of the diagonal block
+
+// ---------------------------------------------------------------------------
+// permutation (mul!(C, P, B), multiply.jl:277-280): C[i] = B[perm[i]]
+// ---------------------------------------------------------------------------
+template <bool IN>
+__global__ void k_perm(double* __restrict__ C, double* B, const int64_t* __restrict__ perm, int64_t n,
+                       int64_t ldb, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) {
+        int64_t r = i / n, row = i % n;
+        if (IN) C[row + r * n] = B[perm[row] + r * ldb];
+        else B[perm[row] + r * ldb] = C[row + r * n];
+    }
+}
+
+__global__ void k_diag_div(double* __restrict__ C, const double* __restrict__ d, int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) C[i] /= d[i % n];
+}
+
+// ---------------------------------------------------------------------------
+// small fronts (nn <= 64, na <= 1024): one CTA per front
+// ---------------------------------------------------------------------------
+template <int UNIT>
+__global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                     const int32_t* __restrict__ reltgt,
+                                                     const int32_t* __restrict__ chdtgt, const double* __restrict__ P,
+                                                     double* __restrict__ C, double* __restrict__ R, int64_t n,
+                                                     int nrhs) {
+    __shared__ double C1[kNB * kMaxRhs];
+    const Front f = fronts[items[blockIdx.x].front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const double* Pj = P + f.poff;
+    double* Rj = R + f.roff * nrhs;
+    for (int i = tid; i < nn * nrhs; i += nt) {
+        int a = i % nn, r = i / nn;
+        C1[a + r * kNB] = C[f.col0 + a + (int64_t)r * n];
+    }
+    for (int i = tid; i < na * nrhs; i += nt) Rj[i] = 0.0;
+    __syncthreads();
+    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
+        const Front fc = fronts[chdtgt[p]];
+        const int ma = fc.na;
+        const int32_t* rel = reltgt + fc.sep0;
+        const double* Mc = R + fc.roff * nrhs;
+        for (int i = tid; i < ma * nrhs; i += nt) {
+            int a = i % ma, r = i / ma;
+            int q = rel[a];
+            if (q < nn) C1[q + r * kNB] += Mc[i];
+            else Rj[(q - nn) + r * na] += Mc[i];
+        }
+        __syncthreads();
+    }
+    // C1 <- D^{-1} C1
+    for (int k = 0; k < nn; ++k) {
+        if (!UNIT) {
+            double inv = 1.0 / Pj[k + (int64_t)k * nj];
+            for (int r = tid; r < nrhs; r += nt) C1[k + r * kNB] *= inv;
+            __syncthreads();
+        }
+        const int m = nn - k - 1;
+        for (int i = tid; i < m * nrhs; i += nt) {
+            int a = k + 1 + i % m, r = i / m;
+            C1[a + r * kNB] -= Pj[a + (int64_t)k * nj] * C1[k + r * kNB];
+        }
+        __syncthreads();
+    }
+    // R_j -= L21 C1
+    for (int i = tid; i < na * nrhs; i += nt) {
+        int a = i % na, r = i / na;
+        double s = 0.0;
+        for (int k = 0; k < nn; ++k) s += Pj[(nn + a) + (int64_t)k * nj] * C1[k + r * kNB];
+        Rj[a + r * na] -= s;
+    }
+    for (int i = tid; i < nn * nrhs; i += nt) {
+        int a = i % nn, r = i / nn;
+        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kNB];
+    }
+}
+
+template <int UNIT>
+__global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                     const int32_t* __restrict__ septgt, const double* __restrict__ P,
+                                                     double* __restrict__ C, int64_t n, int nrhs) {
+    __shared__ double C1[kNB * kMaxRhs];
+    const Front f = fronts[items[blockIdx.x].front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+    const double* Pj = P + f.poff;
+    const int32_t* sep = septgt + f.sep0;
+    // C1 = C[res] - L21^T x[sep]   (one warp per column of L21)
+    for (int k = warp; k < nn; k += nw) {
+        double acc[kMaxRhs];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
+        const double* lc = Pj + nn + (int64_t)k * nj;
+        for (int a = lane; a < na; a += 32) {
+            double l = lc[a];
+            int64_t row = sep[a];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; ++r)
+                if (r < nrhs) acc[r] += l * C[row + (int64_t)r * n];
+        }
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) {
+            double v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc[r] = v;
+        }
+        if (lane == 0)
+            for (int r = 0; r < nrhs; ++r) C1[k + r * kNB] = C[f.col0 + k + (int64_t)r * n] - acc[r];
+    }
+    __syncthreads();
+    // C1 <- D^{-T} C1 (backward substitution, column oriented)
+    for (int k = nn - 1; k >= 0; --k) {
+        // C1[k] -= sum_{a>k} D[a,k] C1[a]
+        if (warp == 0) {
+            for (int r = 0; r < nrhs; ++r) {
+                double s = 0.0;
+                for (int a = k + 1 + lane; a < nn; a += 32) s += Pj[a + (int64_t)k * nj] * C1[a + r * kNB];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+                if (lane == 0) {
+                    double v = C1[k + r * kNB] - s;
+                    if (!UNIT) v /= Pj[k + (int64_t)k * nj];
+                    C1[k + r * kNB] = v;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < nn * nrhs; i += nt) {
+        int a = i % nn, r = i / nn;
+        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kNB];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// blocked fronts
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int lb32(const int32_t* a, int n, int v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// forward gather: W[res] = C[res] + child updates, R_j = child updates
+__global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                  const int32_t* __restrict__ reltgt,
+                                                  const int32_t* __restrict__ chdtgt, const double* __restrict__ C,
+                                                  double* __restrict__ W, double* __restrict__ R, int64_t n,
+                                                  int nrhs) {
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double* Rj = R + f.roff * nrhs;
+    const int w = p1 - p0;
+    for (int i = tid; i < w * nrhs; i += nt) {
+        int q = p0 + i % w, r = i / w;
+        if (q < nn) W[f.col0 + q + (int64_t)r * n] = C[f.col0 + q + (int64_t)r * n];
+        else Rj[(q - nn) + r * na] = 0.0;
+    }
+    __syncthreads();
+    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
+        const Front fc = fronts[chdtgt[p]];
+        const int ma = fc.na;
+        const int32_t* rel = reltgt + fc.sep0;
+        const double* Mc = R + fc.roff * nrhs;
+        const int a0 = lb32(rel, ma, p0), a1 = lb32(rel, ma, p1);
+        const int cnt = a1 - a0;
+        for (int i = tid; i < cnt * nrhs; i += nt) {
+            int a = a0 + i % cnt, r = i / cnt;
+            int q = rel[a];
+            double v = Mc[a + r * ma];
+            if (q < nn) W[f.col0 + q + (int64_t)r * n] += v;
+            else Rj[(q - nn) + r * na] += v;
+        }
+        __syncthreads();
+    }
+}
+
+// solve the w x w diagonal block of step k in shared memory.  Loads
+// Dk (w x w) and the right-hand side block (w x nrhs) from `src`.
+template <int UNIT, int TRANS>
+__device__ void diag_block_solve(const double* Pj, int nj, int k0, int w, const double* src, int64_t n, int nrhs,
+                                 double* Dk, double* X) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < w * w; i += nt) {
+        int r = i % w, c = i / w;
+        Dk[r + c * SLD] = (r >= c) ? Pj[(k0 + r) + (int64_t)(k0 + c) * nj] : 0.0;
+    }
+    for (int i = tid; i < w * nrhs; i += nt) {
+        int a = i % w, r = i / w;
+        X[a + r * SLD] = src[a + (int64_t)r * n];
+    }
+    __syncthreads();
+    // one thread per right-hand side column: w <= 64 sequential steps
+    for (int r = tid; r < nrhs; r += nt) {
+        double* x = X + r * SLD;
+        if (!TRANS) {
+            for (int a = 0; a < w; ++a) {
+                double v = x[a];
+                for (int c = 0; c < a; ++c) v -= Dk[a + c * SLD] * x[c];
+                x[a] = UNIT ? v : v / Dk[a + a * SLD];
+            }
+        } else {
+            for (int a = w - 1; a >= 0; --a) {
+                double v = x[a];
+                for (int c = a + 1; c < w; ++c) v -= Dk[c + a * SLD] * x[c];
+                x[a] = UNIT ? v : v / Dk[a + a * SLD];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int UNIT>
+__global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                               int step, const double* __restrict__ P, double* __restrict__ C,
+                                               double* __restrict__ W, double* __restrict__ R, int64_t n, int nrhs) {
+    __shared__ double Dk[kNB * SLD];
+    __shared__ double X[kMaxRhs * SLD];
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int k0 = step * kNB, w = min(kNB, nn - k0);
+    const double* Pj = P + f.poff;
+    diag_block_solve<UNIT, 0>(Pj, nj, k0, w, W + f.col0 + k0, n, nrhs, Dk, X);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (it.a == 0) {
+        for (int i = tid; i < w * nrhs; i += nt) {
+            int a = i % w, r = i / w;
+            C[f.col0 + k0 + a + (int64_t)r * n] = X[a + r * SLD];
+        }
+        return;
+    }
+    const int r0 = k0 + w + (it.a - 1) * kSolveRows;
+    const int r1 = min(r0 + kSolveRows, nj);
+    double* Rj = R + f.roff * nrhs;
+    for (int q = r0 + tid; q < r1; q += nt) {
+        double acc[kMaxRhs];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
+        for (int c = 0; c < w; ++c) {
+            double l = Pj[q + (int64_t)(k0 + c) * nj];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; ++r) acc[r] += l * X[c + r * SLD];
+        }
+        for (int r = 0; r < nrhs; ++r) {
+            if (q < nn) W[f.col0 + q + (int64_t)r * n] -= acc[r];
+            else Rj[(q - nn) + r * na] -= acc[r];
+        }
+    }
+}
+
+// backward: W[res] = C[res] - L21^T x[sep], one warp per column
+__global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 const int32_t* __restrict__ septgt, const double* __restrict__ P,
+                                                 const double* __restrict__ C, double* __restrict__ W, int64_t n,
+                                                 int nrhs) {
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const double* Pj = P + f.poff;
+    const int32_t* sep = septgt + f.sep0;
+    const int c0 = it.a * kNB, c1 = min(c0 + kNB, nn);
+    for (int k = c0 + warp; k < c1; k += nw) {
+        double acc[kMaxRhs];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
+        const double* lc = Pj + nn + (int64_t)k * nj;
+        for (int a = lane; a < na; a += 32) {
+            double l = lc[a];
+            int64_t row = sep[a];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; ++r)
+                if (r < nrhs) acc[r] += l * C[row + (int64_t)r * n];
+        }
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) {
+            double v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc[r] = v;
+        }
+        if (lane == 0)
+            for (int r = 0; r < nrhs; ++r)
+                W[f.col0 + k + (int64_t)r * n] = C[f.col0 + k + (int64_t)r * n] - acc[r];
+    }
+}
+
+template <int UNIT>
+__global__ void __launch_bounds__(256) k_s_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                               int step, const double* __restrict__ P, double* __restrict__ C,
+                                               double* __restrict__ W, int64_t n, int nrhs) {
+    __shared__ double Dk[kNB * SLD];
+    __shared__ double X[kMaxRhs * SLD];
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, nj = nn + f.na;
+    const int k0 = step * kNB, w = min(kNB, nn - k0);
+    const double* Pj = P + f.poff;
+    diag_block_solve<UNIT, 1>(Pj, nj, k0, w, W + f.col0 + k0, n, nrhs, Dk, X);
+    const int tid = threadIdx.x;
+    if (it.a == 0) {
+        for (int i = tid; i < w * nrhs; i += blockDim.x) {
+            int a = i % w, r = i / w;
+            C[f.col0 + k0 + a + (int64_t)r * n] = X[a + r * SLD];
+        }
+        return;
+    }
+    // W[c] -= sum_i D[k0+i, c] x[i] for columns c of tile (it.a-1) below k0
+    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int c0 = (it.a - 1) * kNB, c1 = min(c0 + kNB, k0);
+    for (int c = c0 + warp; c < c1; c += nw) {
+        double acc[kMaxRhs];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
+        for (int i = lane; i < w; i += 32) {
+            double dv = Pj[(k0 + i) + (int64_t)c * nj];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; ++r) acc[r] += dv * X[i + r * SLD];
+        }
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) {
+            double v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            acc[r] = v;
+        }
+        if (lane == 0)
+            for (int r = 0; r < nrhs; ++r) W[f.col0 + c + (int64_t)r * n] -= acc[r];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static unsigned grid_stride_blocks(int64_t work) {
+    int64_t b = (work + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs) {
+    Timer t(h, K_PERM);
+    k_perm<true><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->d_C, const_cast<double*>(B), perm, h->n,
+                                                                         ldb, (int)nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs) {
+    Timer t(h, K_PERM);
+    k_perm<false><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->d_C, B, perm, h->n, ldb, (int)nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <int UNIT>
+static int solve_impl(mf_handle* h, int nrhs) {
+    const Item* items = h->d_items;
+    const int64_t n = h->n;
+    // forward: levels ascending
+    for (const Level& lv : h->levels) {
+        if (lv.s_small.cnt) {
+            Timer t(h, K_S_SMALL);
+            k_s_small_fwd<UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
+                h->d_fronts, items + lv.s_small.off, h->d_reltgt, h->d_chdtgt, h->d_P, h->d_C, h->d_R, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        if (lv.s_gather.cnt) {
+            Timer t(h, K_S_GATHER);
+            k_s_gather<<<(unsigned)lv.s_gather.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_gather.off,
+                                                                         h->d_reltgt, h->d_chdtgt, h->d_C, h->d_W,
+                                                                         h->d_R, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        for (size_t k = 0; k < lv.s_steps.size(); ++k) {
+            const SolveStep& st = lv.s_steps[k];
+            if (!st.fwd.cnt) continue;
+            Timer t(h, K_S_FWD);
+            k_s_fwd<UNIT><<<(unsigned)st.fwd.cnt, 256, 0, h->stream>>>(h->d_fronts, items + st.fwd.off, (int)k,
+                                                                       h->d_P, h->d_C, h->d_W, h->d_R, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+    }
+    if (UNIT) {
+        Timer t(h, K_OTHER);
+        k_diag_div<<<grid_stride_blocks(n * nrhs), 256, 0, h->stream>>>(h->d_C, h->d_d, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+    }
+    // backward: levels descending
+    for (size_t L = h->levels.size(); L-- > 0;) {
+        const Level& lv = h->levels[L];
+        if (lv.s_bwd_l.cnt) {
+            Timer t(h, K_S_BWD_L);
+            k_s_bwd_l<<<(unsigned)lv.s_bwd_l.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_bwd_l.off,
+                                                                       h->d_septgt, h->d_P, h->d_C, h->d_W, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        for (size_t k = lv.s_steps.size(); k-- > 0;) {
+            const SolveStep& st = lv.s_steps[k];
+            if (!st.bwd.cnt) continue;
+            Timer t(h, K_S_BWD);
+            k_s_bwd<UNIT><<<(unsigned)st.bwd.cnt, 256, 0, h->stream>>>(h->d_fronts, items + st.bwd.off, (int)k,
+                                                                       h->d_P, h->d_C, h->d_W, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        if (lv.s_small.cnt) {
+            Timer t(h, K_S_SMALL);
+            k_s_small_bwd<UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
+                h->d_fronts, items + lv.s_small.off, h->d_septgt, h->d_P, h->d_C, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+    }
+    return 0;
+}
+
+// Solve in place on d_C (n x nrhs, ld n, elimination order); nrhs <= nrhs_cap.
+int launch_solve(mf_handle* h, int64_t nrhs) {
+    if (nrhs <= 0) return 0;
+    if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
+    return h->diag ? solve_impl<1>(h, (int)nrhs) : solve_impl<0>(h, (int)nrhs);
+}
+
+}  // namespace mf

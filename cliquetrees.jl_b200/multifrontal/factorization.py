@@ -1,0 +1,279 @@
+"""Factorization objects and the numeric entry points, mirroring the
+reference's Julia API for the multifrontal hot path.
+
+  ChordalCholesky(A; alg) / ChordalLDLt(A; alg)
+        src/Multifrontal.jl/src/chordal_factorization.jl:1-20, :45, :95, :146-239
+  cholesky_(F; check)   = cholesky!(F)     src/Multifrontal.jl/src/cholesky.jl:80-101
+  ldlt_(F; signs, check) = ldlt!(F)        src/Multifrontal.jl/src/cholesky.jl:181-203
+  factorize! info mapping (info -> perm[info])  cholesky.jl:233-257
+  checkinfo (PosDefException / SingularException)  utils.jl:775-785
+  ldiv(F, B)  = F \\ B = ldiv!!            src/Multifrontal.jl/src/divide.jl:201-206, :1762-1764
+  rdiv(B, F)  = B / F = rdiv!!             src/Multifrontal.jl/src/divide.jl:287-292, :1769-1771
+  issuccess, logdet, det                   abstract_factorization.jl:100-102, :156-179
+  flatindices / value refresh              chordal_symbolic.jl:731-752, chordal_factorization.jl:322-338
+
+Every numeric operation runs in ``libmfgpu.so`` on the GPU; there is no CPU
+code path for the numbers.  Python ``!`` cannot appear in names, so
+``cholesky!`` is ``cholesky_`` and ``ldlt!`` is ``ldlt_``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import check, ptr64, ptrd
+from .sparse import assembly_map
+from .symbolic import ChordalSymbolic, Permutation, symbolic
+
+
+class PosDefException(Exception):
+    """LinearAlgebra.PosDefException(info): pivot `info` (1-based, original order) was not positive."""
+
+    def __init__(self, info):
+        super().__init__(f"matrix is not positive definite; pivot {info} failed")
+        self.info = info
+
+
+class SingularException(Exception):
+    """LinearAlgebra.SingularException(info): pivot `info` (1-based, original order) is zero."""
+
+    def __init__(self, info):
+        super().__init__(f"matrix is singular; pivot {info} is zero")
+        self.info = info
+
+
+class _Handle:
+    """Owns one device handle (pattern + factor)."""
+
+    def __init__(self, S: ChordalSymbolic, diag: int, nrhs_cap: int, device: int):
+        lib = _native.gpulib()
+        h = ctypes.c_void_p()
+        rc = lib.mf_create(S.n, S.nfr, ptr64(S.resptr), ptr64(S.sepptr), ptr64(S.septgt), ptr64(S.reltgt),
+                           ptr64(S.chdptr), ptr64(S.chdtgt), ptr64(S.Dptr), ptr64(S.Lptr), diag, nrhs_cap,
+                           device, ctypes.byref(h))
+        check(rc, "mf_create")
+        self.h = h
+        self.lib = lib
+
+    def close(self):
+        if self.h is not None and self.h.value:
+            self.lib.mf_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ChordalFactorization:
+    """``ChordalFactorization{DIAG, :L, Float64, Int}`` with its numeric
+    storage on the GPU.  ``diag = 0`` is ChordalCholesky (DIAG = :N),
+    ``diag = 1`` is ChordalLDLt (DIAG = :U)."""
+
+    DIAG = 0
+
+    def __init__(self, A, P: Permutation | None = None, S: ChordalSymbolic | None = None, *, alg="amf",
+                 device: int = 0, nrhs_cap: int = 16):
+        if (P is None) != (S is None):
+            raise ValueError("pass both P and S or neither")
+        if P is None:
+            P, S = symbolic(A, alg=alg)
+        self.P = P
+        self.S = S
+        self.info = 0
+        self._factored = False
+        self._handle = _Handle(S, self.DIAG, nrhs_cap, device)
+        self._slot_for = None
+        self.copyto(A)
+
+    # -- reference fields ------------------------------------------------
+    @property
+    def perm(self):
+        return self.P.perm
+
+    @property
+    def invp(self):
+        return self.P.invp
+
+    @property
+    def n(self):
+        return self.S.n
+
+    def copyto(self, A):
+        """copyto!(F, A) (abstract_factorization.jl:68-71): assemble A's
+        values into the factor storage.  The slot map (flatindices) is
+        computed once per pattern and cached on the device."""
+        Lo, slot = assembly_map(self.S, self.P.invp, A)
+        key = (Lo.indptr.tobytes(), Lo.indices.tobytes())
+        lib = self._handle.lib
+        if self._slot_for != key:
+            slot = np.ascontiguousarray(slot, dtype=np.int64)
+            check(lib.mf_set_assembly(self._handle.h, slot.size, ptr64(slot)), "mf_set_assembly")
+            self._slot_for = key
+        vals = np.ascontiguousarray(Lo.data, dtype=np.float64)
+        check(lib.mf_assemble(self._handle.h, ptrd(vals)), "mf_assemble")
+        self._factored = False
+        return self
+
+    def refresh(self, values):
+        """Value refresh on the cached pattern: ``values`` are A's stored
+        lower-triangle entries in the order of the matrix passed at
+        construction (setflatindex! loop, test/multifrontal.jl:76-113)."""
+        vals = np.ascontiguousarray(values, dtype=np.float64)
+        check(self._handle.lib.mf_assemble(self._handle.h, ptrd(vals)), "mf_assemble")
+        self._factored = False
+        return self
+
+    def factor_arrays(self):
+        """(Dval, Lval, d) in the reference layout, downloaded from the GPU."""
+        Dval = np.empty(self.S.ndz, np.float64)
+        Lval = np.empty(self.S.nlz, np.float64)
+        d = np.ones(self.S.n, np.float64)
+        check(self._handle.lib.mf_get_factor(self._handle.h, ptrd(Dval), ptrd(Lval),
+                                             ptrd(d) if self.DIAG else None), "mf_get_factor")
+        return Dval, Lval, d
+
+    @property
+    def Dval(self):
+        return self.factor_arrays()[0]
+
+    @property
+    def Lval(self):
+        return self.factor_arrays()[1]
+
+    @property
+    def d(self):
+        return self.factor_arrays()[2]
+
+    # -- numeric phase -----------------------------------------------------
+    def _factorize(self, signs, check_info: bool):
+        sg = None
+        if signs is not None:
+            # permuteto(T, signs, F.perm) (cholesky.jl:242)
+            sg = np.ascontiguousarray(np.asarray(signs, dtype=np.float64)[self.P.perm])
+        info = ctypes.c_int64(0)
+        check(self._handle.lib.mf_factorize(self._handle.h, ptrd(sg), ctypes.byref(info)), "mf_factorize")
+        k = int(info.value)
+        # factorize! level 1: local info -> perm[info] (cholesky.jl:250-254)
+        self.info = 0 if k == 0 else int(self.P.perm[k - 1]) + 1
+        self._factored = True
+        if check_info and self.info != 0:
+            if self.DIAG == 0:
+                raise PosDefException(self.info)
+            raise SingularException(self.info)
+        return self
+
+    def issuccess(self) -> bool:
+        return self._factored and self.info == 0
+
+    def solve(self, B):
+        return ldiv(self, B)
+
+    def logdet(self) -> float:
+        Dval, _, d = self.factor_arrays()
+        diag = _diag_entries(self.S, Dval)
+        if self.DIAG == 0:
+            return float(2.0 * np.sum(np.log(diag)))
+        return float(np.sum(np.log(np.abs(d)).astype(np.float64)))
+
+    def det(self) -> float:
+        Dval, _, d = self.factor_arrays()
+        if self.DIAG == 0:
+            diag = _diag_entries(self.S, Dval)
+            return float(np.prod(diag) ** 2)
+        return float(np.prod(d))
+
+    def close(self):
+        self._handle.close()
+
+
+def _diag_entries(S: ChordalSymbolic, Dval):
+    out = np.empty(S.n, np.float64)
+    for j in range(S.nfr):
+        nn = S.nn(j)
+        blk = Dval[S.Dptr[j]:S.Dptr[j] + nn * nn].reshape(nn, nn, order="F")
+        out[S.resptr[j]:S.resptr[j + 1]] = np.diag(blk)
+    return out
+
+
+class ChordalCholesky(ChordalFactorization):
+    """P A P^T = L L^T (chordal_factorization.jl:22-45)."""
+    DIAG = 0
+
+
+class ChordalLDLt(ChordalFactorization):
+    """P A P^T = L D L^T with static 1x1 pivots (chordal_factorization.jl:70-95)."""
+    DIAG = 1
+
+
+def cholesky_(F: ChordalFactorization, *, check: bool = True):
+    """cholesky!(F; check) (cholesky.jl:80-101): signs = ones."""
+    if F.DIAG != 0:
+        raise TypeError("cholesky_ needs a ChordalCholesky")
+    return F._factorize(None, check)
+
+
+def ldlt_(F: ChordalFactorization, *, signs=None, check: bool = True):
+    """ldlt!(F; signs=zeros, check) (cholesky.jl:181-203)."""
+    if F.DIAG != 1:
+        raise TypeError("ldlt_ needs a ChordalLDLt")
+    return F._factorize(signs, check)
+
+
+def ldiv(F: ChordalFactorization, B):
+    """F \\ B (divide.jl:201-206): x = P^T L^-T D^-1 L^-1 P b, on the GPU."""
+    if not F._factored:
+        raise RuntimeError("factorize first (cholesky_ / ldlt_)")
+    if F.info != 0:
+        raise RuntimeError("factorization failed; no solve possible")
+    B = np.asarray(B, dtype=np.float64)
+    vec = B.ndim == 1
+    X = np.asfortranarray(B.reshape(-1, 1) if vec else B).copy(order="F")
+    if X.shape[0] != F.n:
+        raise ValueError("dimension mismatch")
+    check(F._handle.lib.mf_solve(F._handle.h, ptrd(X), X.shape[1], F.n, ptr64(F.P.perm)), "mf_solve")
+    return X[:, 0].copy() if vec else X
+
+
+def rdiv(B, F: ChordalFactorization):
+    """B / F for a symmetric factorization: (F \\ B^T)^T (divide.jl:287-292)."""
+    B = np.asarray(B, dtype=np.float64)
+    return ldiv(F, B.T).T
+
+
+def issuccess(F: ChordalFactorization) -> bool:
+    return F.issuccess()
+
+
+def logdet(F: ChordalFactorization) -> float:
+    return F.logdet()
+
+
+def det(F: ChordalFactorization) -> float:
+    return F.det()
+
+
+# -- the drop-in boundary in the reference's own terms -----------------------
+
+def chol_impl(S: ChordalSymbolic, Dval, Lval, *, diag: int, signs=None, d=None, device: int = 0):
+    """chol_impl! (cholesky.jl:361-392) on the GPU through the C ABI:
+    Dval/Lval hold the assembled (permuted) matrix and are overwritten with
+    the factor; returns (info, d) with info the 1-based permuted column of
+    the first rejected pivot (0 on success)."""
+    h = _Handle(S, diag, 1, device)
+    try:
+        Dval = np.ascontiguousarray(Dval, dtype=np.float64)
+        Lval = np.ascontiguousarray(Lval, dtype=np.float64)
+        if d is None:
+            d = np.zeros(S.n, np.float64)
+        sg = None if signs is None else np.ascontiguousarray(signs, dtype=np.float64)
+        info = ctypes.c_int64(0)
+        check(h.lib.mf_chol_impl(h.h, ptrd(Dval), ptrd(Lval), ptrd(d) if diag else None, ptrd(sg),
+                                 ctypes.byref(info)), "mf_chol_impl")
+        return int(info.value), Dval, Lval, d
+    finally:
+        h.close()

@@ -1,0 +1,126 @@
+/*
+ * mfgpu.h -- B200 (sm_100a) numeric phase of CliqueTrees.jl's Multifrontal
+ * submodule behind a plain C ABI (no torch or CUDA types in the signatures).
+ *
+ * The reference numeric phase is two Julia functions over flat arrays:
+ *   chol_impl!(Mptr, Mval, Dptr, Dval, Lptr, Lval, d, Fval, res, rel, chd,
+ *              uplo, S, R, diag)        src/Multifrontal.jl/src/cholesky.jl:361-392
+ *   div_impl!(B, Mptr, Mval, Dptr, Dval, Lptr, Lval, Fval, res, rel, chd,
+ *             tA, tB, uplo, side, diag) src/Multifrontal.jl/src/divide.jl:417-450
+ * reached from factorize! (cholesky.jl:304-315) and ldiv! (divide.jl:167-199,
+ * :1762-1764).  This library replaces both.  A Julia caller passes the
+ * ChordalSymbolic arrays once (mf_create), then calls mf_chol_impl /
+ * mf_div_impl with the same Dval/Lval/d/B arrays the reference uses.
+ *
+ * Conventions
+ *   - every index array is 0-based int64 (a Julia shim subtracts 1);
+ *   - matrices are column major, values float64;
+ *   - Dval: per front nn x nn (lower triangle used) at Dptr[j];
+ *     Lval: per front na x nn at Lptr[j]  (UPLO = :L layout,
+ *     chordal_factorization.jl:146-167);
+ *   - info follows the reference: 0 = success, k > 0 = 1-based column (in
+ *     the elimination order) of the first rejected pivot (cholesky.jl:384-388);
+ *     the caller maps it through perm as factorize! does (cholesky.jl:250-254);
+ *   - return codes: 0 ok, -1 bad argument, -2 invalid symbolic input,
+ *     -3 CUDA error, -4 out of device memory; mf_last_error() explains.
+ *   - one handle = one pattern + its device factor; a handle is used by one
+ *     host thread at a time; all work runs on the handle's stream.
+ */
+#ifndef MFGPU_H
+#define MFGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mf_handle mf_handle;
+
+/* Upload a ChordalSymbolic (chordal_symbolic.jl:15-28) and allocate the
+ * device factor.  diag: 0 = Cholesky (ChordalCholesky, DIAG=:N),
+ * 1 = LDLt (ChordalLDLt, DIAG=:U).  nrhs_cap: largest number of right-hand
+ * sides solved per pass (<= 16; larger blocks are processed in chunks).
+ * Arrays: resptr, sepptr, Dptr, Lptr: nfr+1; septgt, reltgt: sepptr[nfr];
+ * chdptr: nfr+2; chdtgt: nfr (children ascending, roots in list nfr).
+ * Replaces: ChordalFactorization(P, S) allocation, chordal_factorization.jl:146-167,
+ * and the workspaces FactorizationWorkspace (cholesky.jl:15-24) and
+ * DivisionWorkspace (divide.jl:13-18). */
+int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+              const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+              const int64_t* Lptr, int diag, int nrhs_cap, int device, mf_handle** out);
+
+void mf_destroy(mf_handle* h);
+
+/* Run the work of a handle on a caller-owned CUDA stream (a cudaStream_t
+ * passed as void*); NULL restores the handle's own stream. */
+int mf_set_stream(mf_handle* h, void* stream);
+
+/* Full reference-equivalent factorization with host arrays:
+ * Dval/Lval hold the assembled matrix on entry and the factor on exit (in
+ * place, as chol_impl! does); d receives the LDLt pivots (length n, may be
+ * NULL for Cholesky); signs (length n, may be NULL) are the pivot signs S
+ * of NoRegularization (no_regularization.jl:27-42): NULL means all ones for
+ * Cholesky and all zeros for LDLt.
+ * Replaces chol_impl!, cholesky.jl:361-392. */
+int mf_chol_impl(mf_handle* h, double* Dval, double* Lval, double* d, const double* signs, int64_t* info);
+
+/* Natural-factorization solve with host arrays: B (n x nrhs, leading
+ * dimension ldb, elimination order) <- (L D L^T)^{-1} B, or (L L^T)^{-1} B.
+ * Uses the factor left on the device by the last factorization.
+ * Replaces ldiv!(W, NaturalFactorization(F), B) = div_impl! forward, D,
+ * div_impl! backward, divide.jl:191-199, :417-450. */
+int mf_div_impl(mf_handle* h, double* B, int64_t nrhs, int64_t ldb);
+
+/* ---- device-resident path (pattern cached on the device) ---------------- */
+
+/* Assembly map: slot[k] = flat 0-based index into [Dval; Lval] of the k-th
+ * stored value the caller will pass to mf_assemble (flatindices,
+ * chordal_symbolic.jl:731-752).  Uploaded once per pattern. */
+int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot);
+
+/* Refill the device factor from nonzero values (host pointer), i.e.
+ * fill!(F, 0); setflatindex!(F, v, slot) (chordal_factorization.jl:322-338). */
+int mf_assemble(mf_handle* h, const double* nzval);
+
+/* Same with a device pointer (values already in HBM). */
+int mf_assemble_device(mf_handle* h, const double* nzval_dev);
+
+/* Factor the device-resident values (chol_impl! without host copies).
+ * info as above (host int64); signs may be NULL (see mf_chol_impl). */
+int mf_factorize(mf_handle* h, const double* signs, int64_t* info);
+
+/* x = A^{-1} b with the permutation applied on the device, host buffers:
+ * B (n x nrhs, leading dimension ldb, ORIGINAL order) is overwritten with
+ * the solution; perm (length n) is the elimination order (perm[i] = original
+ * vertex at position i).  Replaces ldiv!!(C, F, B), divide.jl:1762-1764. */
+int mf_solve(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm);
+
+/* Same with device pointers (B_dev n x nrhs, leading dimension ldb). */
+int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev);
+
+/* Copy the device factor out in the reference layout (any pointer may be NULL). */
+int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d);
+
+/* Wait for the handle's stream. */
+int mf_synchronize(mf_handle* h);
+
+/* Sizes: out[0..7] = n, nfr, ndz, nlz, panel values, update values,
+ * device bytes allocated, number of tree levels. */
+int mf_info(const mf_handle* h, int64_t* out);
+
+/* Optional per-kernel timing (CUDA events around every launch, stream
+ * synchronised after each: for profiling passes only).  mf_kernel_times
+ * fills ms[13] and launches[13] in the order: assemble, small, extend-add,
+ * panel, update, syrk, solve-small, solve-gather, solve-fwd, solve-bwd-l,
+ * solve-bwd, permute, other. */
+int mf_profile(mf_handle* h, int enable);
+int mf_kernel_times(const mf_handle* h, double* ms, int64_t* launches);
+
+const char* mf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,197 @@
+"""GPU numeric phase (libmfgpu.so, through the C ABI) against the CPU oracle
+on the same seeded inputs.
+
+Bars (stated per test): the factor entries agree with the oracle to
+rtol 1e-10 relative to each front's largest entry; solutions have normwise
+backward error <= 1e-13 and agree with the oracle's to 1e-9 relative.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import multifrontal as mf
+from multifrontal import testmatrices as tm
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+KA = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+CHOL_ORDER = np.array([3, 1, 4, 2, 5]) - 1
+
+
+def lower_mask(S):
+    """Boolean mask over Dval selecting the lower triangle of each block."""
+    m = np.zeros(S.ndz, bool)
+    for j in range(S.nfr):
+        nn = S.nn(j)
+        r, c = np.indices((nn, nn))
+        m[S.Dptr[j]:S.Dptr[j] + nn * nn] = (r >= c).ravel(order="F")
+    return m
+
+
+def diag_mask(S):
+    m = np.zeros(S.ndz, bool)
+    for j in range(S.nfr):
+        nn = S.nn(j)
+        m[S.Dptr[j] + np.arange(nn) * (nn + 1)] = True
+    return m
+
+
+def assert_factor_close(S, got, want, diag, rtol=1e-10):
+    Dg, Lg, dg = got
+    Dw, Lw, dw = want
+    m = lower_mask(S)
+    if diag:
+        m &= ~diag_mask(S)  # LDLt: unit diagonal implied, stored value unspecified
+    scale = max(np.abs(Dw[m]).max(initial=0), np.abs(Lw).max(initial=0), 1e-300)
+    np.testing.assert_allclose(Dg[m], Dw[m], rtol=0, atol=rtol * scale)
+    np.testing.assert_allclose(Lg, Lw, rtol=0, atol=rtol * scale)
+    if diag:
+        np.testing.assert_allclose(dg, dw[:S.n], rtol=1e-10, atol=0)
+
+
+def oracle_factor(A, P, S, diag, signs=None):
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    sg = None if signs is None else np.asarray(signs, float)[P.perm]
+    info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, diag, signs=sg)
+    return info, (Dval, Lval, d)
+
+
+def check_solution(A, P, S, F, B, diag):
+    X = mf.ldiv(F, B)
+    eta = tm.backward_error(A, X, B)
+    assert eta.max() <= 1e-13, eta.max()
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, diag)
+    assert info == 0
+    rel = np.abs(X - Xo).max() / np.abs(Xo).max()
+    assert rel <= 1e-9, rel
+    return X
+
+
+def test_known_answer_cholesky():
+    ka = KA["cholesky"]
+    A = np.array(ka["A"])
+    P, S = mf.symbolic(A, alg=CHOL_ORDER)
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S))
+    assert mf.issuccess(F)
+    Dval, Lval, _ = F.factor_arrays()
+    from test_known_answers import dense_factor
+    np.testing.assert_allclose(dense_factor(S, Dval, Lval), np.nan_to_num(np.array(ka["L"])), atol=1e-15)
+    np.testing.assert_allclose(mf.ldiv(F, np.array(ka["b"])), np.array(ka["x"]), atol=1e-15)
+    assert abs(F.logdet() - np.log(np.linalg.det(A))) < 1e-12
+
+
+@pytest.mark.parametrize("use_signs", [False, True])
+def test_known_answer_ldlt(use_signs):
+    ka = KA["ldlt"]
+    A = np.array(ka["A"])
+    P, S = mf.symbolic(A, alg=CHOL_ORDER)
+    F = mf.ldlt_(mf.ChordalLDLt(A, P, S), signs=np.array(ka["signs"]) if use_signs else None)
+    Dval, Lval, d = F.factor_arrays()
+    np.testing.assert_allclose(d, np.array(ka["d_signs" if use_signs else "d"]), atol=1e-15)
+    np.testing.assert_allclose(mf.ldiv(F, np.array(ka["b"])), np.array(ka["x"]), atol=1e-15)
+
+
+@pytest.mark.parametrize("case", ["grid2d", "grid3d", "grid2d9"])
+def test_cholesky_parity(case):
+    if case == "grid2d":
+        A = tm.grid_laplacian(60, 50, seed=11)
+        order = mf.grid_nd_order(60, 50, 1)
+    elif case == "grid3d":
+        A = tm.grid_laplacian(18, 17, 16, seed=12, lo=1e-3, hi=1e3, shift=1e-6)
+        order = mf.grid_nd_order(18, 17, 16)
+    else:
+        A = tm.grid_laplacian(40, 40, stencil=9, seed=13, lo=0.5, hi=2.0, dist="uniform", shift=1e-3)
+        order = mf.grid_nd_order(40, 40, 1)
+    P, S = mf.symbolic(A, alg=order)
+    info, want = oracle_factor(A, P, S, 0)
+    assert info == 0
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S))
+    assert F.info == 0
+    assert_factor_close(S, F.factor_arrays(), want, 0)
+    for k in (1, 4, 16, 19):
+        check_solution(A, P, S, F, tm.rhs(S.n, k, seed=k), 0)
+    # a vector right-hand side takes the same path
+    b = tm.rhs(S.n, 1, seed=99)[:, 0]
+    x = mf.ldiv(F, b)
+    assert x.shape == b.shape
+
+
+def test_ldlt_quasidefinite_parity():
+    K = tm.config4(side=7, m=120, per_row=6, seed=5)
+    P, S = mf.symbolic(K, alg="natural")
+    info, want = oracle_factor(K, P, S, 1)
+    assert info == 0
+    F = mf.ldlt_(mf.ChordalLDLt(K, P, S))
+    assert_factor_close(S, F.factor_arrays(), want, 1)
+    B = tm.rhs(S.n, 8, seed=4)
+    X = mf.ldiv(F, B)
+    info, Xo, _ = oracle.factor_and_solve(K, P, S, B, 1)
+    assert np.abs(X - Xo).max() / np.abs(Xo).max() <= 1e-9
+    assert tm.backward_error(K, X, B).max() <= 1e-12
+
+
+def test_ldlt_blocked_fronts_parity():
+    # 3D grid shifted to be indefinite: LDLt with static pivots, big fronts
+    A = tm.grid_laplacian(14, 13, 12, seed=21)
+    A = (A - 0.3 * sp.eye(A.shape[0])).tocsc()
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(14, 13, 12))
+    info, want = oracle_factor(A, P, S, 1)
+    assert info == 0
+    F = mf.ldlt_(mf.ChordalLDLt(A, P, S))
+    assert_factor_close(S, F.factor_arrays(), want, 1, rtol=1e-8)
+    B = tm.rhs(S.n, 3, seed=5)
+    X = mf.ldiv(F, B)
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, 1)
+    assert np.abs(X - Xo).max() / np.abs(Xo).max() <= 1e-8
+
+
+def test_not_positive_definite_reports_reference_info():
+    A = tm.grid_laplacian(30, 30, seed=3)
+    A = A.tolil()
+    A[417, 417] = -5.0
+    A = A.tocsc()
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(30, 30, 1))
+    info_o, _ = oracle_factor(A, P, S, 0)
+    assert info_o > 0
+    F = mf.ChordalCholesky(A, P, S)
+    with pytest.raises(mf.PosDefException) as ei:
+        mf.cholesky_(F)
+    assert ei.value.info == P.perm[info_o - 1] + 1
+    F2 = mf.cholesky_(mf.ChordalCholesky(A, P, S), check=False)
+    assert not mf.issuccess(F2)
+
+
+def test_value_refresh_on_cached_pattern():
+    A = tm.grid_laplacian(25, 24, 3, seed=31)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(25, 24, 3))
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S))
+    A2 = tm.grid_laplacian(25, 24, 3, seed=32)
+    F.copyto(A2)
+    mf.cholesky_(F)
+    info, want = oracle_factor(A2, P, S, 0)
+    assert_factor_close(S, F.factor_arrays(), want, 0)
+    check_solution(A2, P, S, F, tm.rhs(S.n, 2, seed=1), 0)
+
+
+def test_reference_layout_boundary():
+    """mf_chol_impl takes and returns the reference's Dval/Lval arrays."""
+    A = tm.grid_laplacian(20, 20, 4, seed=41)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(20, 20, 4))
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    info, Dg, Lg, d = mf.chol_impl(S, Dval.copy(), Lval.copy(), diag=0)
+    assert info == 0
+    info_o, want = oracle_factor(A, P, S, 0)
+    assert_factor_close(S, (Dg, Lg, d), want, 0)
+
+
+def test_rdiv_row_rhs():
+    A = tm.grid_laplacian(16, 16, seed=5)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(16, 16, 1))
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S))
+    B = tm.rhs(3, S.n, seed=2)
+    X = mf.rdiv(B, F)
+    np.testing.assert_allclose(X @ A, B, atol=1e-10)
