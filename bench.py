@@ -145,13 +145,25 @@ def dgemm_peak_tflops(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def kernel_flops(S):
-    """Algorithmic flops per kernel class for one factorization, counted
-    from the symbolic: fronts with nj <= 96 run in the fused small kernel;
-    for the others the panel kernels do nn^3/3 + nn^2*na and the SYRK kernel
-    nn*na^2 (the per-front total nn^3/3 + nn^2*na + nn*na^2)."""
-    nn = S.nn().astype(np.float64)
-    na = S.na().astype(np.float64)
+def exec_sizes(lib, h):
+    info = np.zeros(9, np.int64)
+    lib.mf_info(h, info.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    nex = int(info[8])
+    nn = np.zeros(nex, np.int64)
+    na = np.zeros(nex, np.int64)
+    p64 = ctypes.POINTER(ctypes.c_int64)
+    lib.mf_exec_sizes(h, nn.ctypes.data_as(p64), na.ctypes.data_as(p64))
+    return nn, na
+
+
+def kernel_flops(nn, na):
+    """Flops per kernel class for one factorization, counted on the fronts
+    the device executes (after amalgamation): fronts with nj <= 96 run in
+    the fused small kernel; for the others the panel kernels (diagonal
+    blocks, TRSM, left and trailing updates) do nn^3/3 + nn^2*na and the
+    SYRK kernel nn*na^2."""
+    nn = nn.astype(np.float64)
+    na = na.astype(np.float64)
     big = (nn + na) > 96
     return {
         "small": float(np.sum((nn ** 3 / 3 + nn * nn * na + nn * na * na)[~big])),
@@ -269,6 +281,7 @@ def main():
     stream.synchronize()
     X = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
     eta = float(tm.backward_error(A, X, B).max())
+    _native.check(lib.mf_assemble_device(h, vp(nz_dev.data_ptr())), "assemble")
     _native.check(lib.mf_factorize(h, None, ctypes.byref(info)), "factorize")
     if info.value != 0 or not eta <= 1e-12:
         raise SystemExit(f"bench: factorization check failed (info={info.value}, backward error={eta})")
@@ -333,22 +346,27 @@ def main():
 
     # roofline of the dominant kernel
     peaks = measured_peaks()
-    fl = kernel_flops(S)
-    dom = max(("syrk", "update", "panel", "small"), key=lambda k: ktimes[k]["ms"])
+    enn, ena = exec_sizes(lib, h)
+    fl = kernel_flops(enn, ena)
+    classes = {
+        "syrk": (fl["syrk"], ["syrk"]),
+        "panel+update": (fl["panel+update"], ["panel", "update"]),
+        "small": (fl["small"], ["small"]),
+    }
+    cls_ms = {k: sum(ktimes[x]["ms"] for x in v[1]) for k, v in classes.items()}
+    dom = max(cls_ms, key=cls_ms.get)
     dgemm = dgemm_peak_tflops(torch, dev)
-    if dom == "syrk":
-        flops, launches, kms = fl["syrk"], ktimes["syrk"]["launches"], ktimes["syrk"]["ms"]
-    elif dom in ("update", "panel"):
-        flops = fl["panel+update"]
-        launches = ktimes["update"]["launches"] + ktimes["panel"]["launches"]
-        kms = ktimes["update"]["ms"] + ktimes["panel"]["ms"]
-    else:
-        flops, launches, kms = fl["small"], ktimes["small"]["launches"], ktimes["small"]["ms"]
+    flops = classes[dom][0]
+    launches = sum(ktimes[x]["launches"] for x in classes[dom][1])
+    kms = cls_ms[dom]
     achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else 0.0
+    per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
+                     "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
     roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
             "frac": achieved / dgemm if dgemm else None, "traffic": None,
             "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
-            "flops_per_launch": flops / max(launches, 1), "avg_launch_ms": kms / max(launches, 1)}
+            "flops_per_launch": flops / max(launches, 1), "avg_launch_ms": kms / max(launches, 1),
+            "classes": per_class}
 
     # CPU baseline: the oracle on one full step
     cpu = None

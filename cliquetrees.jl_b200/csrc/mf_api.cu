@@ -42,10 +42,10 @@ struct DeviceGuard {
 };
 
 void free_all(mf_handle* h) {
-    void* ptrs[] = {h->d_fronts, h->d_septgt, h->d_reltgt, h->d_chdtgt, h->d_colfront, h->d_Dptr, h->d_Lptr,
+    void* ptrs[] = {h->d_fronts, h->d_septgt, h->d_reltgt, h->d_chdtgt, h->d_colfront, h->d_ref, h->d_sepmap,
                     h->d_items,  h->d_P,      h->d_M,      h->d_d,      h->d_signs,    h->d_info, h->d_R,
                     h->d_W,      h->d_C,      h->d_B,      h->d_perm,   h->d_DL,       h->d_slot, h->d_pslot,
-                    h->d_nz};
+                    h->d_nz,     h->d_inv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -129,21 +129,22 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
 
     int64_t tot = 0;
     int64_t nsep = h->nsep;
-    std::vector<int32_t> sep32(nsep), rel32(nsep), chd32(nfr), colfront(n);
-    for (int64_t i = 0; i < nsep; ++i) { sep32[i] = (int32_t)septgt[i]; rel32[i] = (int32_t)reltgt[i]; }
-    for (int64_t i = 0; i < nfr; ++i) chd32[i] = (int32_t)chdtgt[i];
+    const int64_t nex = h->nexec;
+    std::vector<int32_t> sep32(nsep), colfront(n);
+    for (int64_t i = 0; i < nsep; ++i) sep32[i] = (int32_t)septgt[i];
     for (int64_t j = 0; j < nfr; ++j)
         for (int64_t c = resptr[j]; c < resptr[j + 1]; ++c) colfront[c] = (int32_t)j;
     rc = 0;
-    rc = rc ? rc : dalloc(h, &h->d_fronts, nfr, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_fronts, nex, &tot);
     rc = rc ? rc : dalloc(h, &h->d_septgt, nsep, &tot);
-    rc = rc ? rc : dalloc(h, &h->d_reltgt, nsep, &tot);
-    rc = rc ? rc : dalloc(h, &h->d_chdtgt, nfr, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_reltgt, (int64_t)h->h_exec_rel.size(), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_chdtgt, (int64_t)h->h_exec_chd.size(), &tot);
     rc = rc ? rc : dalloc(h, &h->d_colfront, n, &tot);
-    rc = rc ? rc : dalloc(h, &h->d_Dptr, nfr + 1, &tot);
-    rc = rc ? rc : dalloc(h, &h->d_Lptr, nfr + 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_ref, nfr, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_sepmap, (int64_t)h->h_sepmap.size(), &tot);
     rc = rc ? rc : dalloc(h, &h->d_items, (int64_t)h->h_items.size(), &tot);
     rc = rc ? rc : dalloc(h, &h->d_P, h->npanel, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_inv, std::max<int64_t>(h->ninv, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_M, h->nmval, &tot);
     rc = rc ? rc : dalloc(h, &h->d_d, std::max<int64_t>(n, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_info, 1, &tot);
@@ -158,13 +159,13 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
     };
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = up(h->d_fronts, h->h_fronts.data(), sizeof(Front) * nfr);
+    if (e == cudaSuccess) e = up(h->d_fronts, h->h_fronts.data(), sizeof(Front) * nex);
     if (e == cudaSuccess) e = up(h->d_septgt, sep32.data(), sizeof(int32_t) * nsep);
-    if (e == cudaSuccess) e = up(h->d_reltgt, rel32.data(), sizeof(int32_t) * nsep);
-    if (e == cudaSuccess) e = up(h->d_chdtgt, chd32.data(), sizeof(int32_t) * nfr);
+    if (e == cudaSuccess) e = up(h->d_reltgt, h->h_exec_rel.data(), sizeof(int32_t) * h->h_exec_rel.size());
+    if (e == cudaSuccess) e = up(h->d_chdtgt, h->h_exec_chd.data(), sizeof(int32_t) * h->h_exec_chd.size());
     if (e == cudaSuccess) e = up(h->d_colfront, colfront.data(), sizeof(int32_t) * n);
-    if (e == cudaSuccess) e = up(h->d_Dptr, Dptr, sizeof(int64_t) * (nfr + 1));
-    if (e == cudaSuccess) e = up(h->d_Lptr, Lptr, sizeof(int64_t) * (nfr + 1));
+    if (e == cudaSuccess) e = up(h->d_ref, h->h_ref.data(), sizeof(RefFront) * nfr);
+    if (e == cudaSuccess) e = up(h->d_sepmap, h->h_sepmap.data(), sizeof(int32_t) * h->h_sepmap.size());
     if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
     if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
     if (e != cudaSuccess) {
@@ -187,6 +188,42 @@ void mf_destroy(mf_handle* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     free_all(h);
     delete h;
+}
+
+int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+                 const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+                 const int64_t* Lptr, int nrhs_cap, int64_t* out) {
+    if (!out || n < 0 || nfr < 0 || !resptr || !sepptr || !chdptr || !Dptr || !Lptr || nrhs_cap < 1 ||
+        nrhs_cap > 16) {
+        set_error("mf_plan_info: bad arguments");
+        return -1;
+    }
+    mf_handle h;
+    h.n = n;
+    h.nfr = nfr;
+    h.nrhs_cap = nrhs_cap;
+    int rc;
+    try {
+        rc = build_plan(&h, resptr, sepptr, septgt, reltgt, chdptr, chdtgt, Dptr, Lptr);
+    } catch (const std::bad_alloc&) {
+        set_error("out of host memory building the plan");
+        rc = -4;
+    }
+    if (rc) return rc;
+    int64_t launches = 0;
+    for (const Level& lv : h.levels) {
+        launches += (lv.small.cnt > 0) + (lv.ea.cnt > 0) + (lv.syrk.cnt > 0);
+        for (const PanelStep& st : lv.steps)
+            launches += (st.left.cnt > 0) + (st.diag.cnt > 0) + (st.panel.cnt > 0) + (st.trail.cnt > 0);
+    }
+    out[0] = h.nexec;
+    out[1] = (int64_t)h.levels.size();
+    out[2] = h.npanel;
+    out[3] = h.nmval;
+    out[4] = h.nrval_per_rhs;
+    out[5] = (int64_t)h.h_items.size();
+    out[6] = launches;
+    return 0;
 }
 
 int mf_set_stream(mf_handle* h, void* stream) {
@@ -298,18 +335,22 @@ int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot) {
         int64_t p;
         if (s < ndz) {
             int64_t j = std::upper_bound(h->h_Dptr.begin(), h->h_Dptr.end(), s) - h->h_Dptr.begin() - 1;
-            const Front& f = h->h_fronts[j];
-            int64_t loc = s - h->h_Dptr[j];
-            int64_t r = loc % f.nn, c = loc / f.nn;
+            const RefFront& rf = h->h_ref[j];
+            const Front& f = h->h_fronts[rf.exec];
+            int64_t loc = s - rf.Dptr;
+            int64_t r = loc % rf.nn, c = loc / rf.nn;
             if (r < c) { set_error("mf_set_assembly: slot in the upper triangle of a diagonal block"); return -2; }
-            p = f.poff + r + c * (int64_t)(f.nn + f.na);
+            int64_t off = rf.res0 - f.col0;
+            p = f.poff + (off + r) + (off + c) * (int64_t)f.ldp;
         } else {
             int64_t s2 = s - ndz;
             int64_t j = std::upper_bound(h->h_Lptr.begin(), h->h_Lptr.end(), s2) - h->h_Lptr.begin() - 1;
-            const Front& f = h->h_fronts[j];
-            int64_t loc = s2 - h->h_Lptr[j];
-            int64_t a = loc % f.na, c = loc / f.na;
-            p = f.poff + f.nn + a + c * (int64_t)(f.nn + f.na);
+            const RefFront& rf = h->h_ref[j];
+            const Front& f = h->h_fronts[rf.exec];
+            int64_t loc = s2 - rf.Lptr;
+            int64_t a = loc % rf.na, c = loc / rf.na;
+            int64_t off = rf.res0 - f.col0;
+            p = f.poff + h->h_sepmap[rf.sep0 + a] + (off + c) * (int64_t)f.ldp;
         }
         pslot[k] = p;
     }
@@ -420,7 +461,16 @@ int mf_info(const mf_handle* h, int64_t* out) {
     if (!h || !out) { set_error("mf_info: bad arguments"); return -1; }
     out[0] = h->n; out[1] = h->nfr; out[2] = h->ndz; out[3] = h->nlz;
     out[4] = h->npanel; out[5] = h->nmval; out[6] = (int64_t)h->times.ms[15];
-    out[7] = (int64_t)h->levels.size();
+    out[7] = (int64_t)h->levels.size(); out[8] = h->nexec;
+    return 0;
+}
+
+int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na) {
+    if (!h) { set_error("null handle"); return -1; }
+    for (int64_t e = 0; e < h->nexec; ++e) {
+        if (nn) nn[e] = h->h_fronts[e].nn;
+        if (na) na[e] = h->h_fronts[e].na;
+    }
     return 0;
 }
 

@@ -11,14 +11,17 @@
 //               columns); each CTA owns its target columns, so the children
 //               are added in a fixed order without atomics (addscattertri!,
 //               utils.jl:555-579 via chol_send!, cholesky.jl:950-983).
-//   k_panel   : per 64-column panel step: factor the diagonal block in
-//               shared memory (every CTA of the front redundantly; CTA 0
-//               writes it) and solve a 64-row tile of the panel below it
-//               (potrf! + trsm! + cdiv! of chol_factor!, cholesky.jl:694-737).
-//   k_update  : trailing update of the remaining panel columns with DMMA
-//               (mma.sync m8n8k4 f64) 64x64 tiles.
-//   k_syrk    : M = F22 - L21 D L21^T for the whole front at once, K = nn
-//               (syrk!, blas/syrk.jl:137-159), DMMA 64x64 tiles.
+//   k_diag    : per 64-column sub-panel, one CTA per front factors the
+//               diagonal block in shared memory, writes it back and stores
+//               the inverse of the factored block (potrf! of chol_factor!,
+//               cholesky.jl:694-737);
+//   k_gemm    : grouped 64x64 DMMA (mma.sync m8n8k4 f64) tile GEMM with a
+//               cp.async double-buffered K loop, in four roles: left-looking
+//               update of a sub-panel from its outer block, trailing update
+//               of the panel after an outer block (K = 256), the TRSM of a
+//               sub-panel as a product with the inverse of its diagonal
+//               block, and M = F22 - L21 D L21^T with K = nn (syrk!,
+//               blas/syrk.jl:137-159).
 #include <climits>
 #include <cstdio>
 
@@ -61,26 +64,29 @@ __global__ void k_scatter(double* __restrict__ P, const int64_t* __restrict__ sl
 }
 
 // one warp per column: copy between the reference layout (Dval nn x nn,
-// Lval na x nn) and the stacked panel (nj x nn, ld nj).
+// Lval na x nn of reference front j) and the panel of the execution front
+// that holds j (nj x nn, ld nj): the D rows keep their order, the L rows go
+// to sepmap positions.
 template <bool TO_PANEL>
-__global__ void k_dl_panel(const Front* __restrict__ fronts, const int32_t* __restrict__ colfront,
-                           const int64_t* __restrict__ Dptr, const int64_t* __restrict__ Lptr, double* __restrict__ Dv,
-                           double* __restrict__ Lv, double* __restrict__ P, int64_t n) {
+__global__ void k_dl_panel(const Front* __restrict__ fronts, const RefFront* __restrict__ ref,
+                           const int32_t* __restrict__ colref, const int32_t* __restrict__ sepmap,
+                           double* __restrict__ Dv, double* __restrict__ Lv, double* __restrict__ P, int64_t n) {
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (warp >= n) return;
-    int j = colfront[warp];
-    Front f = fronts[j];
-    int c = (int)(warp - f.col0);
-    int nj = f.nn + f.na;
-    double* pc = P + f.poff + (int64_t)c * nj;
-    double* dc = Dv + Dptr[j] + (int64_t)c * f.nn;
-    double* lc = Lv + Lptr[j] + (int64_t)c * f.na;
-    for (int r = lane; r < f.nn; r += 32) {
-        if (TO_PANEL) pc[r] = dc[r]; else dc[r] = pc[r];
+    const RefFront rf = ref[colref[warp]];
+    const Front f = fronts[rf.exec];
+    const int c = (int)(warp - rf.res0);
+    const int off = rf.res0 - f.col0;
+    double* pc = P + f.poff + (int64_t)(off + c) * f.ldp;
+    double* dc = Dv + rf.Dptr + (int64_t)c * rf.nn;
+    double* lc = Lv + rf.Lptr + (int64_t)c * rf.na;
+    const int32_t* map = sepmap + rf.sep0;
+    for (int r = lane; r < rf.nn; r += 32) {
+        if (TO_PANEL) pc[off + r] = dc[r]; else dc[r] = pc[off + r];
     }
-    for (int r = lane; r < f.na; r += 32) {
-        if (TO_PANEL) pc[f.nn + r] = lc[r]; else lc[r] = pc[f.nn + r];
+    for (int r = lane; r < rf.na; r += 32) {
+        if (TO_PANEL) pc[map[r]] = lc[r]; else lc[r] = pc[map[r]];
     }
 }
 
@@ -96,21 +102,24 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
     extern __shared__ double F[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
     double* Pj = P + f.poff;
-    for (int i = tid; i < nj * nn; i += nt) F[i] = Pj[i];
+    for (int i = tid; i < nj * nn; i += nt) {
+        int r = i % nj, c = i / nj;
+        F[i] = Pj[r + (int64_t)c * ld];
+    }
     for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = 0.0;
     __syncthreads();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na;
+        const int ma = fc.na, lm = fc.ldm;
         const int32_t* rel = reltgt + fc.sep0;
         const double* Mc = M + fc.moff;
         for (int i = tid; i < ma * ma; i += nt) {
             int a = i % ma, b = i / ma;
-            if (a >= b) F[rel[a] + rel[b] * nj] += Mc[i];
+            if (a >= b) F[rel[a] + rel[b] * nj] += Mc[a + b * lm];
         }
         __syncthreads();
     }
@@ -141,11 +150,15 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
         }
         __syncthreads();
     }
-    for (int i = tid; i < nj * nn; i += nt) Pj[i] = F[i];
+    for (int i = tid; i < nj * nn; i += nt) {
+        int r = i % nj, c = i / nj;
+        Pj[r + (int64_t)c * ld] = F[i];
+    }
     double* Mj = M + f.moff;
+    const int lm = f.ldm;
     for (int i = tid; i < na * na; i += nt) {
         int a = i % na, b = i / na;
-        Mj[i] = F[(nn + a) + (nn + b) * nj];
+        Mj[a + b * lm] = F[(nn + a) + (nn + b) * nj];
     }
 }
 
@@ -166,31 +179,30 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
                                             double* __restrict__ P, double* __restrict__ M) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp, lm = f.ldm;
     const int c0 = it.a * kEAcols, c1 = min(c0 + kEAcols, nj);
     const int tid = threadIdx.x, nt = blockDim.x;
     double* Pj = P + f.poff;
     double* Mj = M + f.moff;
     // zero the update-matrix columns this CTA owns
     for (int c = max(c0, nn); c < c1; ++c)
-        for (int r = tid; r < na; r += nt) Mj[r + (int64_t)(c - nn) * na] = 0.0;
+        for (int r = tid; r < na; r += nt) Mj[r + (int64_t)(c - nn) * lm] = 0.0;
     __syncthreads();
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na;
+        const int ma = fc.na, lmc = fc.ldm;
         const int32_t* rel = reltgt + fc.sep0;
         const double* Mc = M + fc.moff;
         const int b0 = lower_bound_i32(rel, ma, c0);
         const int b1 = lower_bound_i32(rel, ma, c1);
-        // flatten (column b, row a >= b) pairs of the owned columns
         for (int b = b0; b < b1; ++b) {
             const int col = rel[b];
-            const double* mc = Mc + (int64_t)b * ma;
+            const double* mc = Mc + (int64_t)b * lmc;
             if (col < nn) {
-                double* pc = Pj + (int64_t)col * nj;
+                double* pc = Pj + (int64_t)col * ld;
                 for (int a = b + tid; a < ma; a += nt) pc[rel[a]] += mc[a];
             } else {
-                double* dst = Mj + (int64_t)(col - nn) * na - nn;
+                double* dst = Mj + (int64_t)(col - nn) * lm - nn;
                 for (int a = b + tid; a < ma; a += nt) dst[rel[a]] += mc[a];
             }
         }
@@ -199,11 +211,9 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 }
 
 // ---------------------------------------------------------------------------
-// blocked path: panel step (diag factor + panel solve)
+// diagonal block: factor + inverse
 // ---------------------------------------------------------------------------
 constexpr int LDS = kNB + 4;  // shared-memory leading dimension (bank spread for DMMA fragments)
-constexpr int kPanelSmem = (kNB * LDS + kTile * LDS + kNB) * (int)sizeof(double);
-constexpr int kTileSmem = (2 * kTile * LDS + kNB) * (int)sizeof(double);
 
 // Factor the w x w diagonal block in shared memory (lower, ld LDS).
 // Returns the local failing column (0-based) or -1.  Must be called by all
@@ -238,80 +248,77 @@ __device__ int factor_diag_block(double* Dk, double* piv, int w, const double* s
     return -1;
 }
 
+// Inverse of the factored lower-triangular block (unit diagonal for LDLt)
+// by row sweeps: X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i].
 template <int LDLT>
-__global__ void __launch_bounds__(256) k_panel(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, double* __restrict__ P, double* __restrict__ d,
-                                               const double* __restrict__ signs, long long* __restrict__ info) {
+__device__ void invert_lower(const double* Dk, double* X, int w) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int i = tid; i < kNB * kNB; i += nt) X[i] = 0.0;
+    __syncthreads();
+    for (int i = 0; i < w; ++i) {
+        const double lii = LDLT ? 1.0 : Dk[i + i * LDS];
+        for (int j = tid; j <= i; j += nt) {
+            double v;
+            if (j == i) {
+                v = 1.0 / lii;
+            } else {
+                double acc = 0.0;
+                for (int k = j; k < i; ++k) acc += Dk[i + k * LDS] * X[k + j * kNB];
+                v = -acc / lii;
+            }
+            X[i + j * kNB] = v;
+        }
+        __syncthreads();
+    }
+}
+
+template <int LDLT>
+__global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                              int c0, double* __restrict__ P, double* __restrict__ inv,
+                                              double* __restrict__ d, const double* __restrict__ signs,
+                                              long long* __restrict__ info) {
     extern __shared__ double smem[];
-    double* Dk = smem;
-    double* X = Dk + kNB * LDS;
-    double* piv = X + kTile * LDS;
+    double* Dk = smem;                 // kNB * LDS
+    double* X = Dk + kNB * LDS;        // kNB * kNB
+    double* piv = X + kNB * kNB;       // kNB
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, nj = nn + f.na;
-    const int k0 = step * kNB;
-    const int w = min(kNB, nn - k0);
+    const int nn = f.nn, ld = f.ldp;
+    const int w = min(kNB, nn - c0);
     const int tid = threadIdx.x, nt = blockDim.x;
     double* Pj = P + f.poff;
     for (int i = tid; i < w * w; i += nt) {
         int r = i % w, c = i / w;
-        Dk[r + c * LDS] = Pj[(k0 + r) + (int64_t)(k0 + c) * nj];
+        Dk[r + c * LDS] = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
     }
     __syncthreads();
-    int bad = factor_diag_block<LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + k0);
+    int bad = factor_diag_block<LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0);
     if (bad >= 0) {
-        if (it.a == 0 && tid == 0) atomicMin(info, (long long)(f.col0 + k0 + bad + 1));
+        if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
         return;
     }
     __syncthreads();
-    if (it.a == 0) {
-        for (int i = tid; i < w * w; i += nt) {
-            int r = i % w, c = i / w;
-            if (r >= c) Pj[(k0 + r) + (int64_t)(k0 + c) * nj] = Dk[r + c * LDS];
-        }
-        if (LDLT)
-            for (int i = tid; i < w; i += nt) d[f.col0 + k0 + i] = piv[i];
-        return;
+    for (int i = tid; i < w * w; i += nt) {
+        int r = i % w, c = i / w;
+        if (r >= c) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = Dk[r + c * LDS];
     }
-    const int r0 = k0 + w + (it.a - 1) * kTile;
-    const int nr = min(kTile, nj - r0);
-    for (int i = tid; i < nr * w; i += nt) {
-        int r = i % nr, c = i / nr;
-        X[r + c * LDS] = Pj[(r0 + r) + (int64_t)(k0 + c) * nj];
-    }
-    __syncthreads();
-    // X <- X Dk^{-T}  (Cholesky) or X <- X Dk^{-T} diag(piv)^{-1} (LDLt, unit Dk)
-    for (int c = 0; c < w; ++c) {
-        if (!LDLT) {
-            double inv = 1.0 / piv[c];
-            for (int r = tid; r < nr; r += nt) X[r + c * LDS] *= inv;
-            __syncthreads();
-        }
-        const int m = w - c - 1;
-        for (int i = tid; i < nr * m; i += nt) {
-            int r = i % nr, cc = c + 1 + i / nr;
-            X[r + cc * LDS] -= X[r + c * LDS] * Dk[cc + c * LDS];
-        }
-        __syncthreads();
-    }
-    if (LDLT) {
-        for (int i = tid; i < nr * w; i += nt) {
-            int r = i % nr, c = i / nr;
-            X[r + c * LDS] *= 1.0 / piv[c];
-        }
-        __syncthreads();
-    }
-    for (int i = tid; i < nr * w; i += nt) {
-        int r = i % nr, c = i / nr;
-        Pj[(r0 + r) + (int64_t)(k0 + c) * nj] = X[r + c * LDS];
-    }
+    if (LDLT)
+        for (int i = tid; i < w; i += nt) d[f.col0 + c0 + i] = piv[i];
+    invert_lower<LDLT>(Dk, X, w);
+    double* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
+    for (int i = tid; i < kNB * kNB; i += nt) dst[i] = X[i];
 }
 
 // ---------------------------------------------------------------------------
-// DMMA tile core: acc(64x64) += A(64 x kc) * B(64 x kc)^T, smem column major
-// with leading dimension LDS.  8 warps; warp w owns rows (w&1)*32..+32 and
-// columns (w>>1)*16..+16 as 4 x 2 fragments of 8 x 8.
+// DMMA tile GEMM with a cp.async double-buffered K loop.
+// acc(64x64) += A(64 x K) * B(64 x K)^T, 8 warps; warp w owns rows
+// (w&1)*32..+32 and columns (w>>1)*16..+16 as 4 x 2 fragments of 8 x 8.
+// Shared tiles are [k][m] with m contiguous (leading dimension LDS).
 // ---------------------------------------------------------------------------
+constexpr int KC = 32;                   // K chunk per pipeline stage
+constexpr int STAGE = KC * LDS;          // doubles per matrix per stage
+constexpr int kGemmSmem = (4 * STAGE + 2 * KC) * (int)sizeof(double);
+
 struct Acc {
     double c[4][2][2];
 };
@@ -323,14 +330,39 @@ __device__ __forceinline__ void acc_zero(Acc& a) {
         for (int j = 0; j < 2; ++j) a.c[i][j][0] = a.c[i][j][1] = 0.0;
 }
 
-__device__ __forceinline__ void mma_tile(Acc& acc, const double* As, const double* Bs, int kc) {
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+    unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Stage one K chunk: rows ra..ra+63 of A (clamped at amax) and rows
+// rb..rb+63 of B (clamped at bmax), columns k..k+kc-1, zero fill outside.
+__device__ __forceinline__ void stage_chunk(double* As, double* Bs, const double* A, int64_t lda, int ra, int amax,
+                                            const double* B, int64_t ldb, int rb, int bmax, int k, int kc) {
+    for (int i = threadIdx.x; i < 64 * KC; i += blockDim.x) {
+        int m = i & 63, kk = i >> 6;
+        bool va = (ra + m < amax) && kk < kc;
+        bool vb = (rb + m < bmax) && kk < kc;
+        const double* sa = A + (va ? (ra + m) + (int64_t)(k + kk) * lda : 0);
+        const double* sb = B + (vb ? (rb + m) + (int64_t)(k + kk) * ldb : 0);
+        cp_async8(As + m + kk * LDS, sa, va);
+        cp_async8(Bs + m + kk * LDS, sb, vb);
+    }
+}
+
+__device__ __forceinline__ void mma_chunk(Acc& acc, const double* As, const double* Bs, const double* dsc, int kc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
     const int fr = lane >> 2, fk = lane & 3;
     for (int k = 0; k < kc; k += 4) {
         double a[4], b[2];
+        const double s = dsc ? dsc[k + fk] : 1.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = As[(wr + i * 8 + fr) + (k + fk) * LDS];
+        for (int i = 0; i < 4; ++i) a[i] = As[(wr + i * 8 + fr) + (k + fk) * LDS] * s;
 #pragma unroll
         for (int j = 0; j < 2; ++j) b[j] = Bs[(wc + j * 8 + fr) + (k + fk) * LDS];
 #pragma unroll
@@ -340,10 +372,43 @@ __device__ __forceinline__ void mma_tile(Acc& acc, const double* As, const doubl
     }
 }
 
-// C(rows, cols) -= acc for the rows/cols inside the matrix; on a diagonal
-// tile only the lower triangle (row >= col) is written.
-__device__ __forceinline__ void acc_sub_store(const Acc& acc, double* C, int64_t ldc, int rbase, int cbase, int rmax,
-                                              int cmax, bool diag_tile) {
+// acc += A[ra.., kbeg..kend) * B[rb.., kbeg..kend)^T (optionally D-scaled)
+__device__ void gemm_k_loop(Acc& acc, double* smem, const double* A, int64_t lda, int ra, int amax, const double* B,
+                            int64_t ldb, int rb, int bmax, int kbeg, int kend, const double* dvec) {
+    double* As[2] = {smem, smem + STAGE};
+    double* Bs[2] = {smem + 2 * STAGE, smem + 3 * STAGE};
+    double* Ds[2] = {smem + 4 * STAGE, smem + 4 * STAGE + KC};
+    const int nchunk = (kend - kbeg + KC - 1) / KC;
+    if (nchunk <= 0) return;
+    auto load = [&](int c, int st) {
+        int k = kbeg + c * KC;
+        int kc = min(KC, kend - k);
+        stage_chunk(As[st], Bs[st], A, lda, ra, amax, B, ldb, rb, bmax, k, kc);
+        if (dvec)
+            for (int i = threadIdx.x; i < KC; i += blockDim.x) Ds[st][i] = i < kc ? dvec[k + i] : 0.0;
+        cp_commit();
+    };
+    load(0, 0);
+    for (int c = 0; c < nchunk; ++c) {
+        const int st = c & 1;
+        if (c + 1 < nchunk) {
+            load(c + 1, st ^ 1);
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
+        }
+        __syncthreads();
+        int kc = min(KC, kend - (kbeg + c * KC));
+        mma_chunk(acc, As[st], Bs[st], dvec ? Ds[st] : nullptr, (kc + 3) & ~3);
+        __syncthreads();
+    }
+}
+
+// C(rbase+r, cbase+c) -= acc (or = acc * colscale when OVERWRITE), for
+// r < rmax, c < cmax; on a diagonal tile only row >= col is written.
+template <bool OVERWRITE>
+__device__ __forceinline__ void acc_store(const Acc& acc, double* C, int64_t ldc, int rbase, int cbase, int rmax,
+                                          int cmax, bool diag_tile, const double* colscale) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
 #pragma unroll
@@ -354,100 +419,57 @@ __device__ __forceinline__ void acc_sub_store(const Acc& acc, double* C, int64_t
             for (int e = 0; e < 2; ++e) {
                 int r = wr + i * 8 + (lane >> 2);
                 int c = wc + j * 8 + (lane & 3) * 2 + e;
-                if (r < rmax && c < cmax && (!diag_tile || rbase + r >= cbase + c))
-                    C[(rbase + r) + (int64_t)(cbase + c) * ldc] -= acc.c[i][j][e];
+                if (r < rmax && c < cmax && (!diag_tile || rbase + r >= cbase + c)) {
+                    double* p = C + (rbase + r) + (int64_t)(cbase + c) * ldc;
+                    if (OVERWRITE) *p = colscale ? acc.c[i][j][e] * colscale[c] : acc.c[i][j][e];
+                    else *p -= acc.c[i][j][e];
+                }
             }
 }
 
-// load a (64 x kc) block of a column-major matrix (rows r0.., cols c0..)
-// into smem (ld LDS), zero-filling rows >= rmax; optionally scale column c
-// by scale[c].
-__device__ __forceinline__ void load_block(double* S, const double* G, int64_t ldg, int r0, int rmax, int c0, int kc,
-                                           const double* scale) {
-    for (int i = threadIdx.x; i < kTile * kc; i += blockDim.x) {
-        int r = i % kTile, c = i / kTile;
-        double v = 0.0;
-        if (r0 + r < rmax) {
-            v = G[(r0 + r) + (int64_t)(c0 + c) * ldg];
-            if (scale) v *= scale[c];
-        }
-        S[r + c * LDS] = v;
-    }
-}
+enum GemmRole { G_LEFT = 0, G_TRAIL = 1, G_SYRK = 2, G_TRSM = 3 };
 
-// trailing update inside the panel after step `step`
-template <int LDLT>
-__global__ void __launch_bounds__(256) k_update(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                int step, double* __restrict__ P, const double* __restrict__ d) {
+template <int ROLE, int LDLT>
+__global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                              int ob, int c0, double* __restrict__ P, double* __restrict__ M,
+                                              const double* __restrict__ d, const double* __restrict__ inv) {
     extern __shared__ double smem[];
-    double* As = smem;
-    double* Bs = As + kTile * LDS;
-    double* sc = Bs + kTile * LDS;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, nj = nn + f.na;
-    const int k0 = step * kNB;
-    const int w = min(kNB, nn - k0);
-    const int cs = k0 + w + it.b * kTile;   // first column of the tile
-    const int rs = cs + it.a * kTile;       // first row of the tile
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     double* Pj = P + f.poff;
-    if (LDLT) {
-        for (int i = threadIdx.x; i < w; i += blockDim.x) sc[i] = d[f.col0 + k0 + i];
-        __syncthreads();
-    }
-    load_block(As, Pj, nj, rs, nj, k0, w, nullptr);
-    load_block(Bs, Pj, nj, cs, nn, k0, w, LDLT ? sc : nullptr);
-    // pad k to a multiple of 4 with zeros
-    int kc = (w + 3) & ~3;
-    for (int i = threadIdx.x; i < kTile * (kc - w); i += blockDim.x) {
-        int r = i % kTile, c = w + i / kTile;
-        As[r + c * LDS] = 0.0; Bs[r + c * LDS] = 0.0;
-    }
-    __syncthreads();
-    Acc acc;
-    acc_zero(acc);
-    mma_tile(acc, As, Bs, kc);
-    acc_sub_store(acc, Pj, nj, rs, cs, nj - rs, nn - cs, it.a == 0);
-}
-
-// M -= L D L^T over the whole front (K = nn), K in chunks of 32
-template <int LDLT>
-__global__ void __launch_bounds__(256) k_syrk(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                              const double* __restrict__ P, double* __restrict__ M,
-                                              const double* __restrict__ d) {
-    constexpr int KC = 32;
-    extern __shared__ double smem[];
-    double* As = smem;
-    double* Bs = As + kTile * LDS;
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
-    const int rs = it.a * kTile, cs = it.b * kTile;
-    const double* Pj = P + f.poff;
     const double* dj = LDLT ? d + f.col0 : nullptr;
     Acc acc;
     acc_zero(acc);
-    for (int k = 0; k < nn; k += KC) {
-        int kc = min(KC, nn - k);
-        int kp = (kc + 3) & ~3;
-        for (int i = threadIdx.x; i < kTile * kp; i += blockDim.x) {
-            int r = i % kTile, c = i / kTile;
-            double a = 0.0, b = 0.0;
-            if (c < kc) {
-                if (rs + r < na) a = Pj[(nn + rs + r) + (int64_t)(k + c) * nj];
-                if (cs + r < na) {
-                    b = Pj[(nn + cs + r) + (int64_t)(k + c) * nj];
-                    if (LDLT) b *= dj[k + c];
-                }
-            }
-            As[r + c * LDS] = a;
-            Bs[r + c * LDS] = b;
+    if (ROLE == G_LEFT) {
+        // sub-panel [c0, c0+w) rows [c0 + 64 a, ..) -= panel cols [ob*kOB, c0)
+        const int w = min(kNB, nn - c0);
+        const int rs = c0 + it.a * kTile;
+        gemm_k_loop(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, ob * kOB, c0, dj);
+        acc_store<false>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, nullptr);
+    } else if (ROLE == G_TRAIL) {
+        const int e = min(nn, (ob + 1) * kOB);
+        const int cs = e + it.b * kTile, rs = cs + it.a * kTile;
+        gemm_k_loop(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, ob * kOB, e, dj);
+        acc_store<false>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, nullptr);
+    } else if (ROLE == G_SYRK) {
+        const int rs = it.a * kTile, cs = it.b * kTile;
+        gemm_k_loop(acc, smem, Pj + nn, ld, rs, na, Pj + nn, ld, cs, na, 0, nn, dj);
+        acc_store<false>(acc, M + f.moff, f.ldm, rs, cs, na - rs, na - cs, it.a == it.b, nullptr);
+    } else {
+        // X (rows below the diagonal block, cols [c0, c0+w)) = X * Linv^T (* D^-1)
+        const int w = min(kNB, nn - c0);
+        const int rs = c0 + w + it.a * kTile;
+        const double* Li = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
+        gemm_k_loop(acc, smem, Pj + (int64_t)c0 * ld, ld, rs, nj, Li - 0, kNB, 0, w, 0, w, nullptr);
+        __syncthreads();
+        double* sc = smem;  // reuse: reciprocal pivots for LDLt
+        if (LDLT) {
+            for (int i = threadIdx.x; i < w; i += blockDim.x) sc[i] = 1.0 / dj[c0 + i];
+            __syncthreads();
         }
-        __syncthreads();
-        mma_tile(acc, As, Bs, kp);
-        __syncthreads();
+        acc_store<true>(acc, Pj + (int64_t)c0 * ld, ld, rs, 0, nj - rs, w, false, LDLT ? sc : nullptr);
     }
-    acc_sub_store(acc, M + f.moff, na, rs, cs, na - rs, na - cs, it.a == it.b);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,7 +513,8 @@ int launch_dl_to_panel(mf_handle* h, const double* dD, const double* dL) {
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
     unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_dl_panel<true><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_colfront, h->d_Dptr, h->d_Lptr,
+    MF_CUDA(cudaMemsetAsync(h->d_P, 0, sizeof(double) * h->npanel, h->stream));
+    k_dl_panel<true><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap,
                                                      const_cast<double*>(dD), const_cast<double*>(dL), h->d_P, h->n);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -502,19 +525,23 @@ int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
     unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_dl_panel<false><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_colfront, h->d_Dptr, h->d_Lptr, dD, dL,
+    k_dl_panel<false><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
                                                       h->d_P, h->n);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
 
+constexpr int kDiagSmem = (kNB * LDS + kNB * kNB + kNB) * (int)sizeof(double);
+
 template <int LDLT>
 static int factor_impl(mf_handle* h) {
     MF_CUDA(cudaFuncSetAttribute(k_small<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmallMax * kSmallMax * (int)sizeof(double)));
-    MF_CUDA(cudaFuncSetAttribute(k_panel<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_update<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_syrk<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTileSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_diag<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiagSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
     const Item* items = h->d_items;
     for (const Level& lv : h->levels) {
         if (lv.small.cnt) {
@@ -530,25 +557,37 @@ static int factor_impl(mf_handle* h) {
                                                              h->d_chdtgt, h->d_P, h->d_M);
             MF_CUDA(cudaGetLastError());
         }
-        for (size_t k = 0; k < lv.steps.size(); ++k) {
-            const PanelStep& st = lv.steps[k];
-            if (st.panel.cnt) {
-                Timer t(h, K_PANEL);
-                k_panel<LDLT><<<grid_for(st.panel.cnt), 256, kPanelSmem, h->stream>>>(
-                    h->d_fronts, items + st.panel.off, (int)k, h->d_P, h->d_d, h->d_signs, h->d_info);
+        for (const PanelStep& st : lv.steps) {
+            const int c0 = st.b * kOB + st.s * kNB;
+            if (st.left.cnt) {
+                Timer t(h, K_UPDATE);
+                k_gemm<G_LEFT, LDLT><<<grid_for(st.left.cnt), 256, kGemmSmem, h->stream>>>(
+                    h->d_fronts, items + st.left.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
                 MF_CUDA(cudaGetLastError());
             }
-            if (st.update.cnt) {
+            if (st.diag.cnt) {
+                Timer t(h, K_PANEL);
+                k_diag<LDLT><<<grid_for(st.diag.cnt), 256, kDiagSmem, h->stream>>>(
+                    h->d_fronts, items + st.diag.off, c0, h->d_P, h->d_inv, h->d_d, h->d_signs, h->d_info);
+                MF_CUDA(cudaGetLastError());
+            }
+            if (st.panel.cnt) {
+                Timer t(h, K_PANEL);
+                k_gemm<G_TRSM, LDLT><<<grid_for(st.panel.cnt), 256, kGemmSmem, h->stream>>>(
+                    h->d_fronts, items + st.panel.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
+                MF_CUDA(cudaGetLastError());
+            }
+            if (st.trail.cnt) {
                 Timer t(h, K_UPDATE);
-                k_update<LDLT><<<grid_for(st.update.cnt), 256, kTileSmem, h->stream>>>(h->d_fronts, items + st.update.off,
-                                                                               (int)k, h->d_P, h->d_d);
+                k_gemm<G_TRAIL, LDLT><<<grid_for(st.trail.cnt), 256, kGemmSmem, h->stream>>>(
+                    h->d_fronts, items + st.trail.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
                 MF_CUDA(cudaGetLastError());
             }
         }
         if (lv.syrk.cnt) {
             Timer t(h, K_SYRK);
-            k_syrk<LDLT><<<grid_for(lv.syrk.cnt), 256, kTileSmem, h->stream>>>(h->d_fronts, items + lv.syrk.off, h->d_P,
-                                                                       h->d_M, h->d_d);
+            k_gemm<G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, kGemmSmem, h->stream>>>(
+                h->d_fronts, items + lv.syrk.off, 0, 0, h->d_P, h->d_M, h->d_d, h->d_inv);
             MF_CUDA(cudaGetLastError());
         }
     }

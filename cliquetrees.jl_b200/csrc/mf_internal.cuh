@@ -21,9 +21,10 @@ namespace mf {
 //                     parent has been assembled.
 // ---------------------------------------------------------------------------
 struct Front {
-    int64_t poff;   // panel offset in Pval
+    int64_t poff;   // panel offset in Pval (multiple of 4 elements)
     int64_t moff;   // update-matrix offset in Mval (na > 0)
-    int64_t roff;   // offset of this front's solve update (na x nrhs_cap) in Rval
+    int64_t roff;   // first row of this front's solve update block in Rval (block at R + roff*nrhs)
+    int64_t ioff;   // offset of its 64x64 diagonal-block inverses in the inverse scratch
     int32_t nn;     // |res(j)|
     int32_t na;     // |sep(j)|
     int32_t col0;   // first (permuted) column of res(j)
@@ -32,6 +33,20 @@ struct Front {
     int32_t chd1;
     int32_t parent; // -1 for roots
     int32_t level;  // height above the leaves
+    int32_t ldp;    // panel leading dimension: nj rounded up to a multiple of 4
+    int32_t ldm;    // update-matrix leading dimension: na rounded up to a multiple of 4
+};
+
+// A front of the reference's ChordalSymbolic and where its blocks live
+// inside the execution front that contains it.
+struct RefFront {
+    int64_t Dptr;   // offset of its nn x nn block in the reference Dval
+    int64_t Lptr;   // offset of its na x nn block in the reference Lval
+    int32_t nn, na;
+    int32_t res0;   // first column
+    int32_t sep0;   // offset of sep(j) in septgt (and in sepmap)
+    int32_t exec;   // execution front holding it
+    int32_t pad;
 };
 
 // One unit of grouped work: front plus up to two tile coordinates.
@@ -49,14 +64,19 @@ struct ItemList {
 };
 
 constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
-constexpr int kNB = 64;         // panel width of the blocked path
+constexpr int kNB = 64;         // sub-panel width of the blocked path
+constexpr int kOB = 256;        // outer block: trailing updates run with K = kOB
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
 constexpr int kSolveRows = 128; // rows per solve work item
 
+// One 64-wide sub-panel s of outer block b (columns b*kOB + s*kNB ...).
 struct PanelStep {
-    ItemList panel;   // (front, row tile)  : diag factor + panel TRSM
-    ItemList update;  // (front, ti, tj)    : trailing update inside the panel
+    int b = 0, s = 0;
+    ItemList left;    // (front, row tile)  : left-looking update from the outer block's earlier sub-panels
+    ItemList diag;    // (front)            : diagonal block factor + inverse
+    ItemList panel;   // (front, row tile)  : panel TRSM below the diagonal block (GEMM with the inverse)
+    ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kOB
 };
 
 struct SolveStep {
@@ -99,7 +119,13 @@ struct mf_handle {
     bool own_stream = false;
 
     // host copies
-    std::vector<mf::Front> h_fronts;
+    int64_t nexec = 0;              // execution fronts (after amalgamation)
+    std::vector<mf::Front> h_fronts;        // execution fronts
+    std::vector<mf::RefFront> h_ref;        // reference fronts
+    std::vector<int32_t> h_exec_of;         // reference front -> execution front
+    std::vector<int32_t> h_exec_chd;        // execution children CSR targets
+    std::vector<int32_t> h_exec_rel;        // execution rel (indexed like septgt)
+    std::vector<int32_t> h_sepmap;          // reference sep rows -> execution panel rows
     std::vector<int64_t> h_resptr, h_sepptr, h_Dptr, h_Lptr;
     std::vector<mf::Level> levels;
     std::vector<mf::Item> h_items;
@@ -109,13 +135,15 @@ struct mf_handle {
     int32_t* d_septgt = nullptr;
     int32_t* d_reltgt = nullptr;
     int32_t* d_chdtgt = nullptr;
-    int32_t* d_colfront = nullptr;  // column -> front (n)
-    int64_t* d_Dptr = nullptr;      // reference Dval offsets (nfr+1)
-    int64_t* d_Lptr = nullptr;      // reference Lval offsets (nfr+1)
+    int32_t* d_colfront = nullptr;  // column -> reference front (n)
+    mf::RefFront* d_ref = nullptr;  // reference fronts (nfr)
+    int32_t* d_sepmap = nullptr;    // reference sep rows -> execution panel rows (nsep)
     mf::Item* d_items = nullptr;
 
     // device numeric
     double* d_P = nullptr;         // panels
+    double* d_inv = nullptr;       // inverses of the 64x64 diagonal blocks
+    int64_t ninv = 0;
     double* d_M = nullptr;         // update matrices
     double* d_d = nullptr;         // LDLt pivots (n)
     double* d_signs = nullptr;     // pivot signs (n) or null

@@ -6,6 +6,7 @@
 // fronts are grouped by height in the tree: all fronts of one level depend
 // only on lower levels, so each level is a handful of grouped launches.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <set>
@@ -152,49 +153,158 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     h->h_Dptr.assign(Dptr, Dptr + nfr + 1);
     h->h_Lptr.assign(Lptr, Lptr + nfr + 1);
 
-    // ---- fronts, levels, offsets
-    h->h_fronts.resize(nfr);
+    // ---- execution fronts (relaxed amalgamation of last-child chains)
+    //
+    // The reference's maximal supernodes (supernode_types.jl:41-88) leave
+    // long chains of thin fronts, each materialising an update matrix that
+    // its parent immediately re-reads.  The GPU plan merges a front into its
+    // parent when the front is the parent's last child (its columns end
+    // where the parent's begin, so the merged residual stays contiguous) and
+    // the merge adds few explicit zeros (the thresholds of CHOLMOD's relaxed
+    // amalgamation).  Structural zeros of L stay exact zeros in floating
+    // point, so every entry of the reference layout is still computed; the
+    // merged panels are converted back to the reference's Dval/Lval layout
+    // on download.  MF_AMALGAMATE=0 in the environment disables merging.
+    std::vector<int32_t> exec_of(nfr, -1);
+    struct EF { int32_t top; int64_t c0, c1, truth; };
+    std::vector<EF> ef;
+    ef.reserve(nfr);
+    const char* env = getenv("MF_AMALGAMATE");
+    const bool amalg = !(env && env[0] == '0');
+    for (int64_t j = 0; j < nfr; ++j) {
+        int64_t nn = resptr[j + 1] - resptr[j], na = sepptr[j + 1] - sepptr[j];
+        int64_t truth = nn * (nn + 1) / 2 + nn * na;
+        if (amalg && chdptr[j + 1] > chdptr[j]) {
+            int64_t c = chdtgt[chdptr[j + 1] - 1];
+            EF& E = ef[exec_of[c]];
+            if (E.top == c && E.c1 == resptr[j]) {
+                int64_t N = E.c1 - E.c0 + nn;
+                int64_t merged = N * (N + 1) / 2 + N * na;
+                int64_t tot = E.truth + truth;
+                double z = (double)(merged - tot) / (double)merged;
+                bool ok = (N <= 4) || (N <= 16 && z < 0.8) || (N <= 48 && z < 0.1) || (z < 0.05);
+                if (ok) {
+                    E.top = (int32_t)j;
+                    E.c1 = resptr[j + 1];
+                    E.truth = tot;
+                    exec_of[j] = exec_of[c];
+                    continue;
+                }
+            }
+        }
+        exec_of[j] = (int32_t)ef.size();
+        ef.push_back(EF{(int32_t)j, resptr[j], resptr[j + 1], truth});
+    }
+    const int64_t nex = (int64_t)ef.size();
+    h->nexec = nex;
+    std::vector<int32_t> eparent(nex, -1);
+    for (int64_t e = 0; e < nex; ++e) {
+        int64_t pt = parent[ef[e].top];
+        eparent[e] = pt < 0 ? -1 : exec_of[pt];
+    }
+    // children CSR of the execution tree (ascending)
+    std::vector<int64_t> echdptr(nex + 1, 0);
+    for (int64_t e = 0; e < nex; ++e)
+        if (eparent[e] >= 0) echdptr[eparent[e] + 1]++;
+    for (int64_t e = 0; e < nex; ++e) echdptr[e + 1] += echdptr[e];
+    h->h_exec_chd.assign(std::max<int64_t>(echdptr[nex], 1), 0);
+    {
+        std::vector<int64_t> pos(echdptr.begin(), echdptr.end() - 1);
+        for (int64_t e = 0; e < nex; ++e)
+            if (eparent[e] >= 0) h->h_exec_chd[pos[eparent[e]]++] = (int32_t)e;
+    }
+    // position of a global row in the bag of execution front e
+    auto bagpos = [&](int64_t e, int64_t row) -> int64_t {
+        const EF& E = ef[e];
+        if (row >= E.c0 && row < E.c1) return row - E.c0;
+        const int64_t* s0 = septgt + sepptr[E.top];
+        const int64_t* s1 = septgt + sepptr[E.top + 1];
+        const int64_t* it = std::lower_bound(s0, s1, row);
+        if (it == s1 || *it != row) return -1;
+        return (E.c1 - E.c0) + (it - s0);
+    };
+    // rel of execution fronts (into the parent's bag), indexed like septgt
+    h->h_exec_rel.assign(std::max<int64_t>(h->nsep, 1), -1);
+    for (int64_t e = 0; e < nex; ++e) {
+        if (eparent[e] < 0) continue;
+        int64_t t = ef[e].top;
+        for (int64_t p = sepptr[t]; p < sepptr[t + 1]; ++p) {
+            int64_t q = bagpos(eparent[e], septgt[p]);
+            if (q < 0) { set_error("internal: separator row missing from the parent bag"); return -3; }
+            h->h_exec_rel[p] = (int32_t)q;
+        }
+    }
+    // reference front -> rows of its block inside the execution panel
+    h->h_sepmap.assign(std::max<int64_t>(h->nsep, 1), -1);
+    h->h_ref.resize(nfr);
+    for (int64_t j = 0; j < nfr; ++j) {
+        int64_t e = exec_of[j];
+        for (int64_t p = sepptr[j]; p < sepptr[j + 1]; ++p) {
+            int64_t q = bagpos(e, septgt[p]);
+            if (q < 0) { set_error("internal: reference separator row missing from its execution bag"); return -3; }
+            h->h_sepmap[p] = (int32_t)q;
+        }
+        RefFront& r = h->h_ref[j];
+        r.Dptr = Dptr[j];
+        r.Lptr = Lptr[j];
+        r.nn = (int32_t)(resptr[j + 1] - resptr[j]);
+        r.na = (int32_t)(sepptr[j + 1] - sepptr[j]);
+        r.res0 = (int32_t)resptr[j];
+        r.sep0 = (int32_t)sepptr[j];
+        r.exec = (int32_t)e;
+    }
+    h->h_exec_of = exec_of;
+
+    // ---- execution fronts: levels and offsets
+    h->h_fronts.resize(nex);
     int64_t poff = 0;
     int max_level = 0;
-    std::vector<int32_t> level(nfr, 0);
-    for (int64_t j = 0; j < nfr; ++j) {
-        int64_t pj = parent[j];
-        if (pj >= 0) level[pj] = std::max(level[pj], level[j] + 1);
+    std::vector<int32_t> level(nex, 0);
+    for (int64_t e = 0; e < nex; ++e) {
+        int64_t pe = eparent[e];
+        if (pe >= 0) level[pe] = std::max(level[pe], level[e] + 1);
     }
-    for (int64_t j = 0; j < nfr; ++j) {
-        Front& f = h->h_fronts[j];
-        int64_t nn = resptr[j + 1] - resptr[j], na = sepptr[j + 1] - sepptr[j];
+    int64_t ioff = 0;
+    for (int64_t e = 0; e < nex; ++e) {
+        Front& f = h->h_fronts[e];
+        int64_t t = ef[e].top;
+        int64_t nn = ef[e].c1 - ef[e].c0, na = sepptr[t + 1] - sepptr[t];
         f.nn = (int32_t)nn; f.na = (int32_t)na;
-        f.col0 = (int32_t)resptr[j];
-        f.sep0 = (int32_t)sepptr[j];
-        f.chd0 = (int32_t)chdptr[j]; f.chd1 = (int32_t)chdptr[j + 1];
-        f.parent = parent[j];
-        f.level = level[j];
-        f.poff = poff; poff += (nn + na) * nn;
+        f.col0 = (int32_t)ef[e].c0;
+        f.sep0 = (int32_t)sepptr[t];
+        f.chd0 = (int32_t)echdptr[e]; f.chd1 = (int32_t)echdptr[e + 1];
+        f.parent = eparent[e];
+        f.level = level[e];
+        f.ldp = (int32_t)((nn + na + 3) & ~int64_t(3));
+        f.ldm = (int32_t)((na + 3) & ~int64_t(3));
+        f.poff = poff; poff += (int64_t)f.ldp * nn;
         f.moff = 0;
         f.roff = 0;
-        max_level = std::max(max_level, level[j]);
+        f.ioff = 0;
+        if (nn + na > kSmallMax) { f.ioff = ioff; ioff += cdiv(nn, kNB) * kNB * kNB; }
+        max_level = std::max(max_level, level[e]);
     }
     h->npanel = poff;
+    h->ninv = ioff;
     {
-        // slot lifetimes: produced at level(j), read while level(parent(j))
+        // slot lifetimes: produced at level(e), read while level(parent(e))
         // is processed, reusable from the next level on
         std::vector<std::vector<int32_t>> born(max_level + 1), dies(max_level + 1);
-        for (int64_t j = 0; j < nfr; ++j) {
-            if (h->h_fronts[j].na == 0) continue;
-            born[level[j]].push_back((int32_t)j);
-            dies[level[parent[j]]].push_back((int32_t)j);
+        for (int64_t e = 0; e < nex; ++e) {
+            if (h->h_fronts[e].na == 0) continue;
+            born[level[e]].push_back((int32_t)e);
+            dies[level[eparent[e]]].push_back((int32_t)e);
         }
         PoolAllocator pm, pr;
         for (int L = 0; L <= max_level; ++L) {
-            for (int32_t j : born[L]) {
-                Front& f = h->h_fronts[j];
-                f.moff = pm.alloc((int64_t)f.na * f.na);
+            for (int32_t e : born[L]) {
+                Front& f = h->h_fronts[e];
+                f.moff = pm.alloc((int64_t)f.ldm * f.na);
                 f.roff = pr.alloc((int64_t)f.na);  // rows; block is R + roff*nrhs
             }
-            for (int32_t j : dies[L]) {
-                Front& f = h->h_fronts[j];
-                pm.release(f.moff, (int64_t)f.na * f.na);
+            for (int32_t e : dies[L]) {
+                Front& f = h->h_fronts[e];
+                pm.release(f.moff, (int64_t)f.ldm * f.na);
                 pr.release(f.roff, (int64_t)f.na);
             }
         }
@@ -205,7 +315,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     // ---- work lists
     h->levels.assign(max_level + 1, Level());
     std::vector<std::vector<int32_t>> by_level(max_level + 1);
-    for (int64_t j = 0; j < nfr; ++j) by_level[level[j]].push_back((int32_t)j);
+    for (int64_t e = 0; e < nex; ++e) by_level[level[e]].push_back((int32_t)e);
     std::vector<Item>& items = h->h_items;
     items.clear();
     auto begin = [&](ItemList& l) { l.off = (int64_t)items.size(); };
@@ -233,36 +343,55 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             lv.max_nn_blocked = std::max(lv.max_nn_blocked, f.nn);
         }
         end(lv.ea);
-        lv.steps.resize(max_steps);
-        for (int k = 0; k < max_steps; ++k) {
-            PanelStep& st = lv.steps[k];
-            begin(st.panel);
-            for (int32_t j : fr) {
-                const Front& f = h->h_fronts[j];
-                int nj = f.nn + f.na;
-                if (nj <= kSmallMax || f.nn <= k * kNB) continue;
-                int w = std::min(kNB, f.nn - k * kNB);
-                int below = nj - (k * kNB + w);
-                int tiles = 1 + (int)cdiv(below, kTile);
-                for (int t = 0; t < tiles; ++t) push(j, t, 0);
-            }
-            end(st.panel);
-            begin(st.update);
-            for (int32_t j : fr) {
-                const Front& f = h->h_fronts[j];
-                int nj = f.nn + f.na;
-                if (nj <= kSmallMax || f.nn <= k * kNB) continue;
-                int c0 = k * kNB + std::min(kNB, f.nn - k * kNB);
-                if (c0 >= f.nn) continue;
-                int ctiles = (int)cdiv(f.nn - c0, kTile);
-                for (int tj = 0; tj < ctiles; ++tj) {
-                    int cs = c0 + tj * kTile;
-                    int rtiles = (int)cdiv(nj - cs, kTile);
-                    for (int ti = 0; ti < rtiles; ++ti) push(j, ti, tj);
+        // two-level blocking: outer blocks of kOB columns, sub-panels of kNB
+        for (int ob = 0; ob * kOB < lv.max_nn_blocked; ++ob) {
+            for (int sp = 0; sp < kOB / kNB; ++sp) {
+                const int c0 = ob * kOB + sp * kNB;
+                if (c0 >= lv.max_nn_blocked) break;
+                PanelStep st;
+                st.b = ob; st.s = sp;
+                begin(st.left);
+                if (sp > 0)
+                    for (int32_t j : fr) {
+                        const Front& f = h->h_fronts[j];
+                        if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
+                        for (int t = 0; t < (int)cdiv(f.nn + f.na - c0, kTile); ++t) push(j, t, 0);
+                    }
+                end(st.left);
+                begin(st.diag);
+                for (int32_t j : fr) {
+                    const Front& f = h->h_fronts[j];
+                    if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
+                    push(j, 0, 0);
                 }
+                end(st.diag);
+                begin(st.panel);
+                for (int32_t j : fr) {
+                    const Front& f = h->h_fronts[j];
+                    if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
+                    int w = std::min(kNB, f.nn - c0);
+                    for (int t = 0; t < (int)cdiv(f.nn + f.na - c0 - w, kTile); ++t) push(j, t, 0);
+                }
+                end(st.panel);
+                begin(st.trail);
+                const bool last_sub = (sp == kOB / kNB - 1) || (c0 + kNB >= lv.max_nn_blocked);
+                if (last_sub)
+                    for (int32_t j : fr) {
+                        const Front& f = h->h_fronts[j];
+                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kOB) continue;
+                        const int e = std::min(f.nn, (ob + 1) * kOB);
+                        if (e >= f.nn) continue;  // no panel columns after this outer block
+                        const int nj = f.nn + f.na;
+                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
+                            const int cs = e + tj * kTile;
+                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTile); ++ti) push(j, ti, tj);
+                        }
+                    }
+                end(st.trail);
+                lv.steps.push_back(st);
             }
-            end(st.update);
         }
+        (void)max_steps;
         begin(lv.syrk);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
@@ -273,18 +402,23 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         }
         end(lv.syrk);
 
-        // solves
+        // solves: a front is solved by one CTA when the factorization kept it
+        // whole (nj <= kSmallMax) or it is narrow; otherwise it is blocked in
+        // the factorization too and its diagonal-block inverses exist
+        auto solve_small = [](const Front& f) {
+            return f.nn + f.na <= kSmallMax || (f.nn <= kNB && f.na <= 1024);
+        };
         begin(lv.s_small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn <= kNB && f.na <= 1024) push(j, 0, 0);
+            if (solve_small(f)) push(j, 0, 0);
         }
         end(lv.s_small);
         begin(lv.s_gather);
         int max_sblocks = 0;
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn <= kNB && f.na <= 1024) continue;
+            if (solve_small(f)) continue;
             int nj = f.nn + f.na;
             for (int t = 0; t < cdiv(nj, kSolveRows); ++t) push(j, t, 0);
             max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kNB));
@@ -296,7 +430,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             begin(st.fwd);
             for (int32_t j : fr) {
                 const Front& f = h->h_fronts[j];
-                if ((f.nn <= kNB && f.na <= 1024) || f.nn <= k * kNB) continue;
+                if (solve_small(f) || f.nn <= k * kNB) continue;
                 int nj = f.nn + f.na;
                 int w = std::min(kNB, f.nn - k * kNB);
                 int below = nj - (k * kNB + w);
@@ -307,7 +441,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             begin(st.bwd);
             for (int32_t j : fr) {
                 const Front& f = h->h_fronts[j];
-                if ((f.nn <= kNB && f.na <= 1024) || f.nn <= k * kNB) continue;
+                if (solve_small(f) || f.nn <= k * kNB) continue;
                 int tiles = 1 + (int)cdiv(k * kNB, kNB);
                 for (int t = 0; t < tiles; ++t) push(j, t, 0);
             }
@@ -316,7 +450,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_bwd_l);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn <= kNB && f.na <= 1024) continue;
+            if (solve_small(f)) continue;
             for (int t = 0; t < cdiv(f.nn, kNB); ++t) push(j, t, 0);
         }
         end(lv.s_bwd_l);

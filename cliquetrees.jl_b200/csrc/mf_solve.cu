@@ -42,7 +42,7 @@ __global__ void k_diag_div(double* __restrict__ C, const double* __restrict__ d,
 }
 
 // ---------------------------------------------------------------------------
-// small fronts (nn <= 64, na <= 1024): one CTA per front
+// small fronts (nj <= 96, or nn <= 64 and na <= 1024): one CTA per front
 // ---------------------------------------------------------------------------
 template <int UNIT>
 __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -50,15 +50,15 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
                                                      const int32_t* __restrict__ chdtgt, const double* __restrict__ P,
                                                      double* __restrict__ C, double* __restrict__ R, int64_t n,
                                                      int nrhs) {
-    __shared__ double C1[kNB * kMaxRhs];
+    __shared__ double C1[kSmallMax * kMaxRhs];
     const Front f = fronts[items[blockIdx.x].front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
     const double* Pj = P + f.poff;
     double* Rj = R + f.roff * nrhs;
     for (int i = tid; i < nn * nrhs; i += nt) {
         int a = i % nn, r = i / nn;
-        C1[a + r * kNB] = C[f.col0 + a + (int64_t)r * n];
+        C1[a + r * kSmallMax] = C[f.col0 + a + (int64_t)r * n];
     }
     for (int i = tid; i < na * nrhs; i += nt) Rj[i] = 0.0;
     __syncthreads();
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
         for (int i = tid; i < ma * nrhs; i += nt) {
             int a = i % ma, r = i / ma;
             int q = rel[a];
-            if (q < nn) C1[q + r * kNB] += Mc[i];
+            if (q < nn) C1[q + r * kSmallMax] += Mc[i];
             else Rj[(q - nn) + r * na] += Mc[i];
         }
         __syncthreads();
@@ -78,14 +78,14 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
     // C1 <- D^{-1} C1
     for (int k = 0; k < nn; ++k) {
         if (!UNIT) {
-            double inv = 1.0 / Pj[k + (int64_t)k * nj];
-            for (int r = tid; r < nrhs; r += nt) C1[k + r * kNB] *= inv;
+            double inv = 1.0 / Pj[k + (int64_t)k * ld];
+            for (int r = tid; r < nrhs; r += nt) C1[k + r * kSmallMax] *= inv;
             __syncthreads();
         }
         const int m = nn - k - 1;
         for (int i = tid; i < m * nrhs; i += nt) {
             int a = k + 1 + i % m, r = i / m;
-            C1[a + r * kNB] -= Pj[a + (int64_t)k * nj] * C1[k + r * kNB];
+            C1[a + r * kSmallMax] -= Pj[a + (int64_t)k * ld] * C1[k + r * kSmallMax];
         }
         __syncthreads();
     }
@@ -93,12 +93,12 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
     for (int i = tid; i < na * nrhs; i += nt) {
         int a = i % na, r = i / na;
         double s = 0.0;
-        for (int k = 0; k < nn; ++k) s += Pj[(nn + a) + (int64_t)k * nj] * C1[k + r * kNB];
+        for (int k = 0; k < nn; ++k) s += Pj[(nn + a) + (int64_t)k * ld] * C1[k + r * kSmallMax];
         Rj[a + r * na] -= s;
     }
     for (int i = tid; i < nn * nrhs; i += nt) {
         int a = i % nn, r = i / nn;
-        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kNB];
+        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kSmallMax];
     }
 }
 
@@ -106,9 +106,9 @@ template <int UNIT>
 __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                      const int32_t* __restrict__ septgt, const double* __restrict__ P,
                                                      double* __restrict__ C, int64_t n, int nrhs) {
-    __shared__ double C1[kNB * kMaxRhs];
+    __shared__ double C1[kSmallMax * kMaxRhs];
     const Front f = fronts[items[blockIdx.x].front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
     const double* Pj = P + f.poff;
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
         double acc[kMaxRhs];
 #pragma unroll
         for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
-        const double* lc = Pj + nn + (int64_t)k * nj;
+        const double* lc = Pj + nn + (int64_t)k * ld;
         for (int a = lane; a < na; a += 32) {
             double l = lc[a];
             int64_t row = sep[a];
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
             acc[r] = v;
         }
         if (lane == 0)
-            for (int r = 0; r < nrhs; ++r) C1[k + r * kNB] = C[f.col0 + k + (int64_t)r * n] - acc[r];
+            for (int r = 0; r < nrhs; ++r) C1[k + r * kSmallMax] = C[f.col0 + k + (int64_t)r * n] - acc[r];
     }
     __syncthreads();
     // C1 <- D^{-T} C1 (backward substitution, column oriented)
@@ -142,12 +142,12 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
         if (warp == 0) {
             for (int r = 0; r < nrhs; ++r) {
                 double s = 0.0;
-                for (int a = k + 1 + lane; a < nn; a += 32) s += Pj[a + (int64_t)k * nj] * C1[a + r * kNB];
+                for (int a = k + 1 + lane; a < nn; a += 32) s += Pj[a + (int64_t)k * ld] * C1[a + r * kSmallMax];
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
                 if (lane == 0) {
-                    double v = C1[k + r * kNB] - s;
-                    if (!UNIT) v /= Pj[k + (int64_t)k * nj];
-                    C1[k + r * kNB] = v;
+                    double v = C1[k + r * kSmallMax] - s;
+                    if (!UNIT) v /= Pj[k + (int64_t)k * ld];
+                    C1[k + r * kSmallMax] = v;
                 }
             }
         }
@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
     }
     for (int i = tid; i < nn * nrhs; i += nt) {
         int a = i % nn, r = i / nn;
-        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kNB];
+        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kSmallMax];
     }
 }
 
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
                                                   int nrhs) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
     const int tid = threadIdx.x, nt = blockDim.x;
     double* Rj = R + f.roff * nrhs;
@@ -208,53 +208,53 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
     }
 }
 
-// solve the w x w diagonal block of step k in shared memory.  Loads
-// Dk (w x w) and the right-hand side block (w x nrhs) from `src`.
-template <int UNIT, int TRANS>
-__device__ void diag_block_solve(const double* Pj, int nj, int k0, int w, const double* src, int64_t n, int nrhs,
-                                 double* Dk, double* X) {
+// x_k = Linv b_k (TRANS = 0) or x_k = Linv^T b_k (TRANS = 1) for the w x w
+// diagonal block of step k, with Linv the inverse of the factored block
+// stored by the factorization (unit lower for LDLt).  b_k (w x nrhs) is
+// read from `src` (leading dimension n); the result lands in X (ld SLD).
+template <int TRANS>
+__device__ void diag_block_apply(const double* Li, int w, const double* src, int64_t n, int nrhs, double* Ls,
+                                 double* Bs, double* X) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int i = tid; i < w * w; i += nt) {
-        int r = i % w, c = i / w;
-        Dk[r + c * SLD] = (r >= c) ? Pj[(k0 + r) + (int64_t)(k0 + c) * nj] : 0.0;
+    for (int i = tid; i < kNB * kNB; i += nt) {
+        int r = i & (kNB - 1), c = i >> 6;
+        Ls[r + c * SLD] = Li[i];
     }
     for (int i = tid; i < w * nrhs; i += nt) {
         int a = i % w, r = i / w;
-        X[a + r * SLD] = src[a + (int64_t)r * n];
+        Bs[a + r * SLD] = src[a + (int64_t)r * n];
     }
     __syncthreads();
-    // one thread per right-hand side column: w <= 64 sequential steps
-    for (int r = tid; r < nrhs; r += nt) {
-        double* x = X + r * SLD;
+    for (int i = tid; i < w * nrhs; i += nt) {
+        int a = i % w, r = i / w;
+        double acc = 0.0;
         if (!TRANS) {
-            for (int a = 0; a < w; ++a) {
-                double v = x[a];
-                for (int c = 0; c < a; ++c) v -= Dk[a + c * SLD] * x[c];
-                x[a] = UNIT ? v : v / Dk[a + a * SLD];
-            }
+            for (int c = 0; c <= a; ++c) acc += Ls[a + c * SLD] * Bs[c + r * SLD];
         } else {
-            for (int a = w - 1; a >= 0; --a) {
-                double v = x[a];
-                for (int c = a + 1; c < w; ++c) v -= Dk[c + a * SLD] * x[c];
-                x[a] = UNIT ? v : v / Dk[a + a * SLD];
-            }
+            for (int c = a; c < w; ++c) acc += Ls[c + a * SLD] * Bs[c + r * SLD];
         }
+        X[a + r * SLD] = acc;
     }
     __syncthreads();
 }
 
+constexpr int kSolveSmem = (2 * kNB * SLD + 2 * kMaxRhs * SLD) * (int)sizeof(double);
+
 template <int UNIT>
 __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const double* __restrict__ P, double* __restrict__ C,
+                                               int step, const double* __restrict__ P,
+                                               const double* __restrict__ inv, double* __restrict__ C,
                                                double* __restrict__ W, double* __restrict__ R, int64_t n, int nrhs) {
-    __shared__ double Dk[kNB * SLD];
-    __shared__ double X[kMaxRhs * SLD];
+    extern __shared__ double sm[];
+    double* Ls = sm;
+    double* Bs = Ls + kNB * SLD;
+    double* X = Bs + kMaxRhs * SLD;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int k0 = step * kNB, w = min(kNB, nn - k0);
     const double* Pj = P + f.poff;
-    diag_block_solve<UNIT, 0>(Pj, nj, k0, w, W + f.col0 + k0, n, nrhs, Dk, X);
+    diag_block_apply<0>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
     const int tid = threadIdx.x, nt = blockDim.x;
     if (it.a == 0) {
         for (int i = tid; i < w * nrhs; i += nt) {
@@ -271,93 +271,111 @@ __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts,
 #pragma unroll
         for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
         for (int c = 0; c < w; ++c) {
-            double l = Pj[q + (int64_t)(k0 + c) * nj];
+            double l = Pj[q + (int64_t)(k0 + c) * ld];
 #pragma unroll
             for (int r = 0; r < kMaxRhs; ++r) acc[r] += l * X[c + r * SLD];
         }
-        for (int r = 0; r < nrhs; ++r) {
-            if (q < nn) W[f.col0 + q + (int64_t)r * n] -= acc[r];
-            else Rj[(q - nn) + r * na] -= acc[r];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) {
+            if (r < nrhs) {
+                if (q < nn) W[f.col0 + q + (int64_t)r * n] -= acc[r];
+                else Rj[(q - nn) + r * na] -= acc[r];
+            }
         }
     }
 }
 
-// backward: W[res] = C[res] - L21^T x[sep], one warp per column
+// backward: W[res tile] = C[res tile] - L21^T x[sep].  One CTA per 64
+// columns; L rows and the gathered x[sep] are staged through shared memory
+// 64 rows at a time, so L is read once and coalesced.
+constexpr int kBwdSmem = (kNB * SLD + kNB * kMaxRhs) * (int)sizeof(double);
+
 __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  const int32_t* __restrict__ septgt, const double* __restrict__ P,
                                                  const double* __restrict__ C, double* __restrict__ W, int64_t n,
                                                  int nrhs) {
+    extern __shared__ double sm[];
+    double* Lt = sm;                  // [c][a] : Lt[a + c*SLD], 64 rows x 64 columns
+    double* xs = Lt + kNB * SLD;      // [r][a] : xs[a + r*kNB]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int nn = f.nn, na = f.na, ld = f.ldp;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const double* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
-    const int c0 = it.a * kNB, c1 = min(c0 + kNB, nn);
-    for (int k = c0 + warp; k < c1; k += nw) {
-        double acc[kMaxRhs];
-#pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
-        const double* lc = Pj + nn + (int64_t)k * nj;
-        for (int a = lane; a < na; a += 32) {
-            double l = lc[a];
-            int64_t row = sep[a];
-#pragma unroll
-            for (int r = 0; r < kMaxRhs; ++r)
-                if (r < nrhs) acc[r] += l * C[row + (int64_t)r * n];
+    const int c0 = it.a * kNB, wc = min(kNB, nn - c0);
+    // outputs: (column c, rhs r), at most 64 x 16 = 1024, 4 per thread
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int a0 = 0; a0 < na; a0 += kNB) {
+        const int wa = min(kNB, na - a0);
+        __syncthreads();
+        for (int i = tid; i < wa * wc; i += nt) {
+            int a = i % wa, c = i / wa;
+            Lt[a + c * SLD] = Pj[(nn + a0 + a) + (int64_t)(c0 + c) * ld];
         }
-#pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) {
-            double v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            acc[r] = v;
+        for (int i = tid; i < wa * nrhs; i += nt) {
+            int a = i % wa, r = i / wa;
+            xs[a + r * kNB] = C[sep[a0 + a] + (int64_t)r * n];
         }
-        if (lane == 0)
-            for (int r = 0; r < nrhs; ++r)
-                W[f.col0 + k + (int64_t)r * n] = C[f.col0 + k + (int64_t)r * n] - acc[r];
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            int o = tid + u * nt;
+            int c = o % kNB, r = o / kNB;
+            if (c < wc && r < nrhs) {
+                double s = 0.0;
+                for (int a = 0; a < wa; ++a) s += Lt[a + c * SLD] * xs[a + r * kNB];
+                acc[u] += s;
+            }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        int o = tid + u * nt;
+        int c = o % kNB, r = o / kNB;
+        if (c < wc && r < nrhs) {
+            int64_t idx = f.col0 + c0 + c + (int64_t)r * n;
+            W[idx] = C[idx] - acc[u];
+        }
     }
 }
 
 template <int UNIT>
 __global__ void __launch_bounds__(256) k_s_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const double* __restrict__ P, double* __restrict__ C,
+                                               int step, const double* __restrict__ P,
+                                               const double* __restrict__ inv, double* __restrict__ C,
                                                double* __restrict__ W, int64_t n, int nrhs) {
-    __shared__ double Dk[kNB * SLD];
-    __shared__ double X[kMaxRhs * SLD];
+    extern __shared__ double sm[];
+    double* Ls = sm;
+    double* Bs = Ls + kNB * SLD;
+    double* X = Bs + kMaxRhs * SLD;
+    double* Dt = X + kMaxRhs * SLD;   // aliases nothing: kSolveSmem covers Ls, Bs, X and Dt (64 x SLD)
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, nj = nn + f.na;
+    const int nn = f.nn, ld = f.ldp;
     const int k0 = step * kNB, w = min(kNB, nn - k0);
     const double* Pj = P + f.poff;
-    diag_block_solve<UNIT, 1>(Pj, nj, k0, w, W + f.col0 + k0, n, nrhs, Dk, X);
-    const int tid = threadIdx.x;
+    diag_block_apply<1>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
+    const int tid = threadIdx.x, nt = blockDim.x;
     if (it.a == 0) {
-        for (int i = tid; i < w * nrhs; i += blockDim.x) {
+        for (int i = tid; i < w * nrhs; i += nt) {
             int a = i % w, r = i / w;
             C[f.col0 + k0 + a + (int64_t)r * n] = X[a + r * SLD];
         }
         return;
     }
-    // W[c] -= sum_i D[k0+i, c] x[i] for columns c of tile (it.a-1) below k0
-    const int lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
-    const int c0 = (it.a - 1) * kNB, c1 = min(c0 + kNB, k0);
-    for (int c = c0 + warp; c < c1; c += nw) {
-        double acc[kMaxRhs];
-#pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
-        for (int i = lane; i < w; i += 32) {
-            double dv = Pj[(k0 + i) + (int64_t)c * nj];
-#pragma unroll
-            for (int r = 0; r < kMaxRhs; ++r) acc[r] += dv * X[i + r * SLD];
-        }
-#pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) {
-            double v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            acc[r] = v;
-        }
-        if (lane == 0)
-            for (int r = 0; r < nrhs; ++r) W[f.col0 + c + (int64_t)r * n] -= acc[r];
+    // W[c] -= sum_i D[k0+i, c] x_k[i] for the 64 columns c of tile (it.a-1) left of k0
+    const int c0 = (it.a - 1) * kNB, wc = min(kNB, k0 - c0);
+    for (int i = tid; i < w * wc; i += nt) {
+        int a = i % w, c = i / w;
+        Dt[a + c * SLD] = Pj[(k0 + a) + (int64_t)(c0 + c) * ld];
+    }
+    __syncthreads();
+    for (int o = tid; o < wc * nrhs; o += nt) {
+        int c = o % wc, r = o / wc;
+        double s = 0.0;
+        for (int a = 0; a < w; ++a) s += Dt[a + c * SLD] * X[a + r * SLD];
+        W[f.col0 + c0 + c + (int64_t)r * n] -= s;
     }
 }
 
@@ -388,6 +406,10 @@ int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm
 
 template <int UNIT>
 static int solve_impl(mf_handle* h, int nrhs) {
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd<UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSolveSmem + kNB * SLD * (int)sizeof(double)));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem));
     const Item* items = h->d_items;
     const int64_t n = h->n;
     // forward: levels ascending
@@ -409,8 +431,8 @@ static int solve_impl(mf_handle* h, int nrhs) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.fwd.cnt) continue;
             Timer t(h, K_S_FWD);
-            k_s_fwd<UNIT><<<(unsigned)st.fwd.cnt, 256, 0, h->stream>>>(h->d_fronts, items + st.fwd.off, (int)k,
-                                                                       h->d_P, h->d_C, h->d_W, h->d_R, n, nrhs);
+            k_s_fwd<UNIT><<<(unsigned)st.fwd.cnt, 256, kSolveSmem, h->stream>>>(
+                h->d_fronts, items + st.fwd.off, (int)k, h->d_P, h->d_inv, h->d_C, h->d_W, h->d_R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
     }
@@ -424,16 +446,16 @@ static int solve_impl(mf_handle* h, int nrhs) {
         const Level& lv = h->levels[L];
         if (lv.s_bwd_l.cnt) {
             Timer t(h, K_S_BWD_L);
-            k_s_bwd_l<<<(unsigned)lv.s_bwd_l.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_bwd_l.off,
-                                                                       h->d_septgt, h->d_P, h->d_C, h->d_W, n, nrhs);
+            k_s_bwd_l<<<(unsigned)lv.s_bwd_l.cnt, 256, kBwdSmem, h->stream>>>(
+                h->d_fronts, items + lv.s_bwd_l.off, h->d_septgt, h->d_P, h->d_C, h->d_W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         for (size_t k = lv.s_steps.size(); k-- > 0;) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.bwd.cnt) continue;
             Timer t(h, K_S_BWD);
-            k_s_bwd<UNIT><<<(unsigned)st.bwd.cnt, 256, 0, h->stream>>>(h->d_fronts, items + st.bwd.off, (int)k,
-                                                                       h->d_P, h->d_C, h->d_W, n, nrhs);
+            k_s_bwd<UNIT><<<(unsigned)st.bwd.cnt, 256, kSolveSmem + kNB * SLD * (int)sizeof(double), h->stream>>>(
+                h->d_fronts, items + st.bwd.off, (int)k, h->d_P, h->d_inv, h->d_C, h->d_W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.s_small.cnt) {

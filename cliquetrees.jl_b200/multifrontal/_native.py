@@ -97,6 +97,10 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_profile.restype = ctypes.c_int
         lib.mf_kernel_times.argtypes = [_vp, _pd, _p64]
         lib.mf_kernel_times.restype = ctypes.c_int
+        lib.mf_exec_sizes.argtypes = [_vp, _p64, _p64]
+        lib.mf_exec_sizes.restype = ctypes.c_int
+        lib.mf_plan_info.argtypes = [_i64, _i64] + [_p64] * 8 + [ctypes.c_int, _p64]
+        lib.mf_plan_info.restype = ctypes.c_int
         lib.mf_last_error.argtypes = []
         lib.mf_last_error.restype = ctypes.c_char_p
         _gpu = lib

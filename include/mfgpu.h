@@ -105,9 +105,21 @@ int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d);
 /* Wait for the handle's stream. */
 int mf_synchronize(mf_handle* h);
 
-/* Sizes: out[0..7] = n, nfr, ndz, nlz, panel values, update values,
- * device bytes allocated, number of tree levels. */
+/* Sizes: out[0..8] = n, nfr, ndz, nlz, panel values, update values,
+ * device bytes allocated, number of tree levels, execution fronts. */
 int mf_info(const mf_handle* h, int64_t* out);
+
+/* Residual and separator sizes of the execution fronts (mf_info out[8]
+ * entries each), for flop accounting. */
+int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na);
+
+/* Host-only inspection of the execution plan a handle would use (no CUDA
+ * call): out[0..6] = execution fronts after amalgamation, tree levels,
+ * panel values, update-matrix pool values, solve-update pool rows, work
+ * items, factorization launches.  Arguments as for mf_create. */
+int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepptr, const int64_t* septgt,
+                 const int64_t* reltgt, const int64_t* chdptr, const int64_t* chdtgt, const int64_t* Dptr,
+                 const int64_t* Lptr, int nrhs_cap, int64_t* out);
 
 /* Optional per-kernel timing (CUDA events around every launch, stream
  * synchronised after each: for profiling passes only).  mf_kernel_times

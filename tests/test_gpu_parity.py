@@ -40,7 +40,10 @@ def diag_mask(S):
     return m
 
 
-def assert_factor_close(S, got, want, diag, rtol=1e-10):
+def assert_factor_close(S, got, want, diag, rtol=1e-10, adiag=None):
+    """Factor entries within rtol of each factor's largest entry; LDLt pivots
+    within rtol of |d| + |a_kk| (a pivot is a_kk minus a sum of terms of
+    that size, so cancellation leaves an absolute error on that scale)."""
     Dg, Lg, dg = got
     Dw, Lw, dw = want
     m = lower_mask(S)
@@ -50,7 +53,8 @@ def assert_factor_close(S, got, want, diag, rtol=1e-10):
     np.testing.assert_allclose(Dg[m], Dw[m], rtol=0, atol=rtol * scale)
     np.testing.assert_allclose(Lg, Lw, rtol=0, atol=rtol * scale)
     if diag:
-        np.testing.assert_allclose(dg, dw[:S.n], rtol=1e-10, atol=0)
+        scale = np.abs(dw[:S.n]) + (0 if adiag is None else np.abs(adiag))
+        assert np.all(np.abs(dg - dw[:S.n]) <= rtol * scale), np.max(np.abs(dg - dw[:S.n]) / scale)
 
 
 def oracle_factor(A, P, S, diag, signs=None):
@@ -60,14 +64,33 @@ def oracle_factor(A, P, S, diag, signs=None):
     return info, (Dval, Lval, d)
 
 
+def cond1(A, P, S, diag):
+    """1-norm condition estimate kappa_1(A) = ||A||_1 ||A^-1||_1 with the
+    Hager/Higham estimator (the reference's condest1, operator.jl:348),
+    A^-1 applied through the oracle factorization."""
+    import scipy.sparse.linalg as sla
+    n = S.n
+    def solve(b):
+        info, x, _ = oracle.factor_and_solve(A, P, S, np.asarray(b, float).reshape(n, -1), diag)
+        return x
+    op = sla.LinearOperator((n, n), matvec=lambda v: solve(v)[:, 0], rmatvec=lambda v: solve(v)[:, 0],
+                            matmat=solve, rmatmat=solve, dtype=float)
+    return float(abs(A).sum(axis=0).max()) * float(sla.onenormest(op))
+
+
 def check_solution(A, P, S, F, B, diag):
+    """Backward error <= 1e-13; the solution agrees with the oracle's to
+    1e-9 relative, or to 4 kappa_1 eps where the problem's conditioning
+    makes 1e-9 unattainable for two backward-stable solvers."""
     X = mf.ldiv(F, B)
     eta = tm.backward_error(A, X, B)
     assert eta.max() <= 1e-13, eta.max()
     info, Xo, _ = oracle.factor_and_solve(A, P, S, B, diag)
     assert info == 0
     rel = np.abs(X - Xo).max() / np.abs(Xo).max()
-    assert rel <= 1e-9, rel
+    if rel > 1e-9:
+        kappa = cond1(A, P, S, diag)
+        assert rel <= 4 * kappa * np.finfo(float).eps, (rel, kappa)
     return X
 
 
@@ -95,7 +118,7 @@ def test_known_answer_ldlt(use_signs):
     np.testing.assert_allclose(mf.ldiv(F, np.array(ka["b"])), np.array(ka["x"]), atol=1e-15)
 
 
-@pytest.mark.parametrize("case", ["grid2d", "grid3d", "grid2d9"])
+@pytest.mark.parametrize("case", ["grid2d", "grid3d", "grid2d9", "grid3d_large"])
 def test_cholesky_parity(case):
     if case == "grid2d":
         A = tm.grid_laplacian(60, 50, seed=11)
@@ -103,9 +126,13 @@ def test_cholesky_parity(case):
     elif case == "grid3d":
         A = tm.grid_laplacian(18, 17, 16, seed=12, lo=1e-3, hi=1e3, shift=1e-6)
         order = mf.grid_nd_order(18, 17, 16)
-    else:
+    elif case == "grid2d9":
         A = tm.grid_laplacian(40, 40, stencil=9, seed=13, lo=0.5, hi=2.0, dist="uniform", shift=1e-3)
         order = mf.grid_nd_order(40, 40, 1)
+    else:
+        # fronts up to nj ~ 1300: every blocked kernel runs in several waves
+        A = tm.grid_laplacian(30, 30, 30, seed=14, lo=1e-3, hi=1e3, shift=1e-6)
+        order = mf.grid_nd_order(30, 30, 30)
     P, S = mf.symbolic(A, alg=order)
     info, want = oracle_factor(A, P, S, 0)
     assert info == 0
@@ -126,7 +153,7 @@ def test_ldlt_quasidefinite_parity():
     info, want = oracle_factor(K, P, S, 1)
     assert info == 0
     F = mf.ldlt_(mf.ChordalLDLt(K, P, S))
-    assert_factor_close(S, F.factor_arrays(), want, 1)
+    assert_factor_close(S, F.factor_arrays(), want, 1, adiag=K.diagonal()[P.perm])
     B = tm.rhs(S.n, 8, seed=4)
     X = mf.ldiv(F, B)
     info, Xo, _ = oracle.factor_and_solve(K, P, S, B, 1)
@@ -142,7 +169,7 @@ def test_ldlt_blocked_fronts_parity():
     info, want = oracle_factor(A, P, S, 1)
     assert info == 0
     F = mf.ldlt_(mf.ChordalLDLt(A, P, S))
-    assert_factor_close(S, F.factor_arrays(), want, 1, rtol=1e-8)
+    assert_factor_close(S, F.factor_arrays(), want, 1, rtol=1e-8, adiag=A.diagonal()[P.perm])
     B = tm.rhs(S.n, 3, seed=5)
     X = mf.ldiv(F, B)
     info, Xo, _ = oracle.factor_and_solve(A, P, S, B, 1)
@@ -163,6 +190,22 @@ def test_not_positive_definite_reports_reference_info():
     assert ei.value.info == P.perm[info_o - 1] + 1
     F2 = mf.cholesky_(mf.ChordalCholesky(A, P, S), check=False)
     assert not mf.issuccess(F2)
+
+
+@pytest.mark.parametrize("amalgamate", ["0", "1"])
+def test_exact_and_amalgamated_partitions_agree(amalgamate, monkeypatch):
+    """The device plan may merge reference fronts; the reference-layout
+    factor must not depend on it."""
+    monkeypatch.setenv("MF_AMALGAMATE", amalgamate)
+    A = tm.grid_laplacian(22, 21, 20, seed=51, lo=1e-3, hi=1e3, shift=1e-6)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(22, 21, 20))
+    info, want = oracle_factor(A, P, S, 0)
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S))
+    assert_factor_close(S, F.factor_arrays(), want, 0)
+    check_solution(A, P, S, F, tm.rhs(S.n, 4, seed=8), 0)
+    Fl = mf.ldlt_(mf.ChordalLDLt(A, P, S))
+    info, wantl = oracle_factor(A, P, S, 1)
+    assert_factor_close(S, Fl.factor_arrays(), wantl, 1, adiag=A.diagonal()[P.perm])
 
 
 def test_value_refresh_on_cached_pattern():
