@@ -270,6 +270,18 @@ def main():
         _native.check(lib.mf_solve(h, ctypes.cast(X_host.data_ptr(), ctypes.POINTER(ctypes.c_double)), args.nrhs,
                                    n, None), "solve")
 
+    if args.profile_only:
+        # one assemble + factor + solve on the device and nothing else: the
+        # command the committed ncu summaries were taken with
+        with torch.cuda.stream(stream):
+            step_device()
+        stream.synchronize()
+        X = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
+        eta = float(tm.backward_error(A, X, B).max())
+        print(json.dumps({"profile_only": True, "n": int(n), "backward_error": eta}))
+        F.close()
+        return
+
     # perm for the host path is uploaded once (pattern constant)
     perm_np = np.ascontiguousarray(P.perm, dtype=np.int64)
     Xtmp = np.asfortranarray(B.copy())

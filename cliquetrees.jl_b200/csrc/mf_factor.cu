@@ -272,6 +272,126 @@ __device__ void invert_lower(const double* Dk, double* X, int w) {
     }
 }
 
+// Blocked factorization of a 64 x 64 diagonal block held in shared memory
+// (lower, ld LDS; columns >= w are padded with the identity).  Four 16-wide
+// steps: warp 0 factors the 16 x 16 diagonal sub-block with warp
+// synchronisation only, then all threads solve the rows below it and apply
+// the rank-16 update to the trailing block.  piv[k] receives sqrt(pivot)
+// (Cholesky) or the pivot (LDLt).  Returns the first rejected local column
+// (< w) or -1; called by all threads.
+template <int LDLT>
+__device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs, int64_t col0, int* flag) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    for (int p = 0; p < 4; ++p) {
+        const int pb = p * 16;
+        if (warp == 0) {
+            int bad = -1;
+            for (int k = 0; k < 16; ++k) {
+                const int c = pb + k;
+                const double pv = Dk[c + c * LDS];
+                if (c < w) {
+                    const double sg = pivot_sign(signs, LDLT, col0 + c);
+                    if (!pivot_ok(sg, pv) || (!LDLT && !(pv > 0.0))) { bad = c; break; }
+                }
+                const double dk = LDLT ? pv : sqrt(pv);
+                const double inv = 1.0 / dk;
+                __syncwarp();
+                if (lane > k && lane < 16) Dk[(pb + lane) + c * LDS] *= inv;
+                if (lane == 0) {
+                    piv[c] = dk;
+                    if (!LDLT) Dk[c + c * LDS] = dk;
+                }
+                __syncwarp();
+                // rank-1 update of the rest of the 16 x 16 sub-block
+                for (int e = lane; e < 256; e += 32) {
+                    const int i = e & 15, j = e >> 4;
+                    if (j > k && i >= j) {
+                        double lj = Dk[(pb + j) + c * LDS];
+                        if (LDLT) lj *= pv;
+                        Dk[(pb + i) + (pb + j) * LDS] -= Dk[(pb + i) + c * LDS] * lj;
+                    }
+                }
+                __syncwarp();
+            }
+            if (lane == 0) *flag = bad;
+        }
+        __syncthreads();
+        if (*flag >= 0) return *flag;
+        // rows below the sub-block: X <- X Lpp^{-T} (Cholesky) or X Lpp^{-T} D^{-1} (LDLt)
+        for (int r = pb + 16 + tid; r < 64; r += nt) {
+            for (int c = 0; c < 16; ++c) {
+                double v = Dk[r + (pb + c) * LDS];
+                for (int q = 0; q < c; ++q) v -= Dk[r + (pb + q) * LDS] * Dk[(pb + c) + (pb + q) * LDS];
+                if (!LDLT) v /= piv[pb + c];
+                Dk[r + (pb + c) * LDS] = v;
+            }
+            if (LDLT)
+                for (int c = 0; c < 16; ++c) Dk[r + (pb + c) * LDS] /= piv[pb + c];
+        }
+        __syncthreads();
+        // trailing update: rank 16
+        const int m = 64 - pb - 16;
+        for (int e = tid; e < m * m; e += nt) {
+            const int i = pb + 16 + e % m, j = pb + 16 + e / m;
+            if (i >= j) {
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    double lj = Dk[j + (pb + q) * LDS];
+                    if (LDLT) lj *= piv[pb + q];
+                    acc += Dk[i + (pb + q) * LDS] * lj;
+                }
+                Dk[i + j * LDS] -= acc;
+            }
+        }
+        __syncthreads();
+    }
+    return -1;
+}
+
+// Inverse X (ld 64) of the factored 64 x 64 lower block (unit diagonal for
+// LDLt) in 16 x 16 blocks: the four diagonal blocks by one warp each, then
+// X_ij = -X_ii (sum_{k=j}^{i-1} L_ik X_kj) along the block sub-diagonals.
+template <int LDLT>
+__device__ void invert_lower64(const double* Dk, double* X, double* T) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < kNB * kNB; i += nt) X[i] = 0.0;
+    __syncthreads();
+    if (warp < 4 && lane < 16) {
+        const int b = warp * 16, j = lane;
+        const double* L = Dk + b + b * LDS;
+        double* Xb = X + b + b * kNB;
+        Xb[j + j * kNB] = LDLT ? 1.0 : 1.0 / L[j + j * LDS];
+        for (int i = j + 1; i < 16; ++i) {
+            double acc = 0.0;
+            for (int k = j; k < i; ++k) acc += L[i + k * LDS] * Xb[k + j * kNB];
+            Xb[i + j * kNB] = LDLT ? -acc : -acc / L[i + i * LDS];
+        }
+    }
+    __syncthreads();
+    for (int dist = 1; dist < 4; ++dist) {
+        const int nb = 4 - dist;  // blocks (jb + dist, jb) for jb = 0 .. nb-1
+        // T_ij = sum_{k=j}^{i-1} L_ik X_kj   (16 x 16 per block)
+        for (int e = tid; e < nb * 256; e += nt) {
+            const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
+            const int ib = (blk + dist) * 16, jb = blk * 16;
+            double acc = 0.0;
+            for (int k = jb; k < ib; ++k) acc += Dk[(ib + r) + k * LDS] * X[k + (jb + c) * kNB];
+            T[e] = acc;
+        }
+        __syncthreads();
+        // X_ij = -X_ii T_ij
+        for (int e = tid; e < nb * 256; e += nt) {
+            const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
+            const int ib = (blk + dist) * 16, jb = blk * 16;
+            double acc = 0.0;
+            for (int k = 0; k <= r; ++k) acc += X[(ib + r) + (ib + k) * kNB] * T[(blk << 8) + (k << 4) + c];
+            X[(ib + r) + (jb + c) * kNB] = -acc;
+        }
+        __syncthreads();
+    }
+}
+
 template <int LDLT>
 __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                               int c0, double* __restrict__ P, double* __restrict__ inv,
@@ -280,33 +400,40 @@ __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, 
     extern __shared__ double smem[];
     double* Dk = smem;                 // kNB * LDS
     double* X = Dk + kNB * LDS;        // kNB * kNB
-    double* piv = X + kNB * kNB;       // kNB
+    double* T = X + kNB * kNB;         // 3 * 256
+    double* piv = T + 3 * 256;         // kNB
+    __shared__ int flag;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int w = min(kNB, nn - c0);
     const int tid = threadIdx.x, nt = blockDim.x;
     double* Pj = P + f.poff;
-    for (int i = tid; i < w * w; i += nt) {
-        int r = i % w, c = i / w;
-        Dk[r + c * LDS] = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
+    for (int i = tid; i < kNB * kNB; i += nt) {
+        int r = i & (kNB - 1), c = i >> 6;
+        double v;
+        if (r < w && c < w) v = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
+        else v = (r == c) ? 1.0 : 0.0;
+        Dk[r + c * LDS] = v;
     }
     __syncthreads();
-    int bad = factor_diag_block<LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0);
+    int bad = factor_diag64<LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0, &flag);
     if (bad >= 0) {
         if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
         return;
     }
-    __syncthreads();
     for (int i = tid; i < w * w; i += nt) {
         int r = i % w, c = i / w;
         if (r >= c) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = Dk[r + c * LDS];
     }
     if (LDLT)
         for (int i = tid; i < w; i += nt) d[f.col0 + c0 + i] = piv[i];
-    invert_lower<LDLT>(Dk, X, w);
+    invert_lower64<LDLT>(Dk, X, T);
     double* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
-    for (int i = tid; i < kNB * kNB; i += nt) dst[i] = X[i];
+    for (int i = tid; i < kNB * kNB; i += nt) {
+        int r = i & (kNB - 1), c = i >> 6;
+        dst[i] = (r < w && c < w) ? X[i] : 0.0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -531,7 +658,7 @@ int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
     return 0;
 }
 
-constexpr int kDiagSmem = (kNB * LDS + kNB * kNB + kNB) * (int)sizeof(double);
+constexpr int kDiagSmem = (kNB * LDS + kNB * kNB + 3 * 256 + kNB) * (int)sizeof(double);
 
 template <int LDLT>
 static int factor_impl(mf_handle* h) {

@@ -68,7 +68,7 @@ constexpr int kNB = 64;         // sub-panel width of the blocked path
 constexpr int kOB = 256;        // outer block: trailing updates run with K = kOB
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
-constexpr int kSolveRows = 128; // rows per solve work item
+constexpr int kSolveRows = 256; // rows per solve work item
 
 // One 64-wide sub-panel s of outer block b (columns b*kOB + s*kNB ...).
 struct PanelStep {

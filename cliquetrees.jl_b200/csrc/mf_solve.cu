@@ -240,7 +240,7 @@ __device__ void diag_block_apply(const double* Li, int w, const double* src, int
 
 constexpr int kSolveSmem = (2 * kNB * SLD + 2 * kMaxRhs * SLD) * (int)sizeof(double);
 
-template <int UNIT>
+template <int UNIT, int NR>
 __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                int step, const double* __restrict__ P,
                                                const double* __restrict__ inv, double* __restrict__ C,
@@ -267,16 +267,18 @@ __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts,
     const int r1 = min(r0 + kSolveRows, nj);
     double* Rj = R + f.roff * nrhs;
     for (int q = r0 + tid; q < r1; q += nt) {
-        double acc[kMaxRhs];
+        double acc[NR];
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
+        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+        const double* pq = Pj + q + (int64_t)k0 * ld;
+#pragma unroll 4
         for (int c = 0; c < w; ++c) {
-            double l = Pj[q + (int64_t)(k0 + c) * ld];
+            double l = pq[(int64_t)c * ld];
 #pragma unroll
-            for (int r = 0; r < kMaxRhs; ++r) acc[r] += l * X[c + r * SLD];
+            for (int r = 0; r < NR; ++r) acc[r] += l * X[c + r * SLD];
         }
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) {
+        for (int r = 0; r < NR; ++r) {
             if (r < nrhs) {
                 if (q < nn) W[f.col0 + q + (int64_t)r * n] -= acc[r];
                 else Rj[(q - nn) + r * na] -= acc[r];
@@ -406,7 +408,11 @@ int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm
 
 template <int UNIT>
 static int solve_impl(mf_handle* h, int nrhs) {
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd<UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSolveSmem + kNB * SLD * (int)sizeof(double)));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem));
@@ -431,7 +437,9 @@ static int solve_impl(mf_handle* h, int nrhs) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.fwd.cnt) continue;
             Timer t(h, K_S_FWD);
-            k_s_fwd<UNIT><<<(unsigned)st.fwd.cnt, 256, kSolveSmem, h->stream>>>(
+            auto* kern = nrhs <= 1 ? k_s_fwd<UNIT, 1> : nrhs <= 2 ? k_s_fwd<UNIT, 2> : nrhs <= 4 ? k_s_fwd<UNIT, 4>
+                       : nrhs <= 8 ? k_s_fwd<UNIT, 8> : k_s_fwd<UNIT, 16>;
+            kern<<<(unsigned)st.fwd.cnt, 256, kSolveSmem, h->stream>>>(
                 h->d_fronts, items + st.fwd.off, (int)k, h->d_P, h->d_inv, h->d_C, h->d_W, h->d_R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
