@@ -40,7 +40,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "cliquetrees.jl_b200"))
 
 KERNEL_NAMES = ["assemble", "small", "extend_add", "panel", "update", "syrk", "solve_small", "solve_gather",
-                "solve_fwd", "solve_bwd_l", "solve_bwd", "permute", "other"]
+                "solve_fwd", "solve_bwd_l", "solve_bwd", "permute", "other", "diag", "left", "residual"]
+NK = len(KERNEL_NAMES)
 
 
 def parse():
@@ -53,6 +54,7 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
+    ap.add_argument("--mixed-profile", action="store_true", help="with --profile-only: the mixed form")
     return ap.parse_args()
 
 
@@ -231,19 +233,124 @@ def main():
     import torch
     import multifrontal as mf
     from multifrontal import _native
-    from multifrontal import testmatrices as tm
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     A, P, S, B = workload(args.side, args.nrhs)
+
+    if args.profile_only:
+        r = run_form(args, A, P, S, B, mixed=args.mixed_profile, local=local, world=world, profile_only=True)
+        print(json.dumps(r))
+        return
+
+    mixed = run_form(args, A, P, S, B, mixed=True, local=local, world=world)
+    plain = run_form(args, A, P, S, B, mixed=False, local=local, world=world)
+
+    # roofline: the dominant kernel class of the headline (mixed) form
+    peaks = measured_peaks()
+    dgemm = dgemm_peak_tflops(torch, dev)
+    sgemm = sgemm_peak_tflops(torch, dev)
+
+    def roofline(form, peak, peak_src, fl):
+        kt = form["kernels"]
+        classes = {
+            "syrk": (fl["syrk"], ["syrk"]),
+            "panel+update": (fl["panel+update"], ["panel", "update", "diag", "left"]),
+            "small": (fl["small"], ["small"]),
+        }
+        cls_ms = {k: sum(kt[x]["ms"] for x in v[1]) for k, v in classes.items()}
+        dom = max(cls_ms, key=cls_ms.get)
+        launches = sum(kt[x]["launches"] for x in classes[dom][1])
+        kms = cls_ms[dom]
+        achieved = classes[dom][0] / (kms / 1e3) / 1e12 if kms > 0 else 0.0
+        per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
+                         "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
+        return {"kernel": dom, "bound": "tensor" if dom != "small" else "latency", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": peak_src, "flops_per_launch": classes[dom][0] / max(launches, 1),
+                "avg_launch_ms": kms / max(launches, 1), "classes": per_class}
+
+    roof_mixed = roofline(mixed, sgemm, "cuBLAS SGEMM 8192^3 (FP32, TF32 off) measured in this run", mixed["flops"])
+    roof_plain = roofline(plain, dgemm, "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
+                                        "MEASURED_PEAKS.json)", plain["flops"])
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        oracle.set_threads(threads)
+        dt, cinfo, _ = cpu_reference_step(A, P, S, B)
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"one full FP64 factor+{args.nrhs}-RHS solve of the {args.side}^3 system ({dt:.2f} s)"}
+
+    if rank == 0:
+        line = {
+            "metric": "solves_per_s", "value": mixed["value"], "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"3d7pt_{args.side}^3_chol_factor+solve_{args.nrhs}rhs", "n": int(S.n),
+                       "fronts": int(S.nfr), "factor_gflop": S.factor_flops() / 1e9, "nnz_L": int(S.nnz()),
+                       "mode": "mixed: FP32 fronts + FP64 PCG to backward error 1e-12",
+                       "l2": "inputs larger than L2 (factor 2-4 GB)", "parallelism": f"replicas x{world}"},
+            "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"], "backward_error": mixed["backward_error"],
+            "refine_iterations": mixed["iterations"],
+            "e2e": mixed["e2e"],
+            "gpu_launches": mixed["gpu_launches"],
+            "roofline": roof_mixed,
+            "kernels": mixed["kernels"],
+            "clocks": mixed["clocks"],
+            "plain_fp64": {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                           "p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"],
+                           "backward_error": plain["backward_error"], "e2e": plain["e2e"],
+                           "roofline": roof_plain, "kernels": plain["kernels"], "clocks": plain["clocks"]},
+            "mixed_over_plain": mixed["value"] / plain["value"],
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def sgemm_peak_tflops(torch, dev):
+    """cuBLAS SGEMM 8192^3 with TF32 disabled, best of 5 (the FP32 denominator)."""
+    keep = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float32, device=dev)
+    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    torch.backends.cuda.matmul.allow_tf32 = keep
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
+    """Time one form (mixed or plain FP64) of the step; returns a dict."""
+    import torch
+    import multifrontal as mf
+    from multifrontal import _native
+    from multifrontal import testmatrices as tm
+    from multifrontal.sparse import assembly_map
+
+    dev = torch.device("cuda", local)
     n = S.n
-    F = mf.ChordalCholesky(A, P, S, device=local, nrhs_cap=16)
+    F = mf.ChordalCholesky(A, P, S, device=local, nrhs_cap=16, mixed=mixed)
     lib = _native.gpulib()
     h = F._handle.h
     stream = torch.cuda.Stream(device=dev)
     _native.check(lib.mf_set_stream(h, ctypes.c_void_p(stream.cuda_stream)), "mf_set_stream")
-
-    from multifrontal.sparse import assembly_map
     Lo, _ = assembly_map(S, P.invp, A)
     nz_host = torch.from_numpy(np.ascontiguousarray(Lo.data)).pin_memory()
     nz_dev = nz_host.to(dev)
@@ -253,61 +360,71 @@ def main():
     perm_dev = torch.from_numpy(P.perm.astype(np.int64)).to(dev)
     X_host = torch.empty_like(B_host).pin_memory()
     info = ctypes.c_int64(0)
+    fp64 = ctypes.c_int(0)
+    iters = ctypes.c_int(0)
+    eta_dev = ctypes.c_double(0.0)
     vp = ctypes.c_void_p
+    pd = ctypes.POINTER(ctypes.c_double)
+    tol, maxit = 1e-12, 100
 
     def step_device():
+        # the RHS copy must run on the library's stream (same stream order)
+        with torch.cuda.stream(stream):
+            X_dev.copy_(B_dev0)
         _native.check(lib.mf_assemble_device(h, vp(nz_dev.data_ptr())), "assemble")
-        _native.check(lib.mf_factorize(h, None, None), "factorize")
-        X_dev.copy_(B_dev0)
-        _native.check(lib.mf_solve_device(h, vp(X_dev.data_ptr()), args.nrhs, n, vp(perm_dev.data_ptr())),
-                      "solve")
+        if mixed:
+            _native.check(lib.mf_factorize_mixed(h, None, ctypes.byref(info), ctypes.byref(fp64)), "factorize")
+            _native.check(lib.mf_solve_refined_device(h, vp(X_dev.data_ptr()), args.nrhs, n, vp(perm_dev.data_ptr()),
+                                                      tol, maxit, ctypes.byref(iters), ctypes.byref(eta_dev)),
+                          "solve")
+        else:
+            _native.check(lib.mf_factorize(h, None, None), "factorize")
+            _native.check(lib.mf_solve_device(h, vp(X_dev.data_ptr()), args.nrhs, n, vp(perm_dev.data_ptr())),
+                          "solve")
 
     def step_e2e():
-        _native.check(lib.mf_assemble(h, ctypes.cast(nz_host.data_ptr(), ctypes.POINTER(ctypes.c_double))),
-                      "assemble")
-        _native.check(lib.mf_factorize(h, None, ctypes.byref(info)), "factorize")
+        _native.check(lib.mf_assemble(h, ctypes.cast(nz_host.data_ptr(), pd)), "assemble")
         X_host.copy_(B_host)
-        _native.check(lib.mf_solve(h, ctypes.cast(X_host.data_ptr(), ctypes.POINTER(ctypes.c_double)), args.nrhs,
-                                   n, None), "solve")
+        if mixed:
+            _native.check(lib.mf_factorize_mixed(h, None, ctypes.byref(info), ctypes.byref(fp64)), "factorize")
+            _native.check(lib.mf_solve_refined(h, ctypes.cast(X_host.data_ptr(), pd), args.nrhs, n, None, tol, maxit,
+                                               ctypes.byref(iters), ctypes.byref(eta_dev)), "solve")
+        else:
+            _native.check(lib.mf_factorize(h, None, ctypes.byref(info)), "factorize")
+            _native.check(lib.mf_solve(h, ctypes.cast(X_host.data_ptr(), pd), args.nrhs, n, None), "solve")
 
-    if args.profile_only:
-        # one assemble + factor + solve on the device and nothing else: the
-        # command the committed ncu summaries were taken with
-        with torch.cuda.stream(stream):
-            step_device()
-        stream.synchronize()
-        X = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
-        eta = float(tm.backward_error(A, X, B).max())
-        print(json.dumps({"profile_only": True, "n": int(n), "backward_error": eta}))
-        F.close()
-        return
-
-    # perm for the host path is uploaded once (pattern constant)
-    perm_np = np.ascontiguousarray(P.perm, dtype=np.int64)
-    Xtmp = np.asfortranarray(B.copy())
-    _native.check(lib.mf_solve(h, _native.ptrd(Xtmp), 0, n, _native.ptr64(perm_np)), "perm upload")
-
-    # correctness of what is timed
     with torch.cuda.stream(stream):
         step_device()
     stream.synchronize()
     X = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
     eta = float(tm.backward_error(A, X, B).max())
-    _native.check(lib.mf_assemble_device(h, vp(nz_dev.data_ptr())), "assemble")
-    _native.check(lib.mf_factorize(h, None, ctypes.byref(info)), "factorize")
+    if profile_only:
+        F.close()
+        return {"profile_only": True, "mixed": mixed, "n": int(n), "backward_error": eta,
+                "iterations": int(iters.value) if mixed else None}
+
+    # perm for the host path is uploaded once (pattern constant)
+    perm_np = np.ascontiguousarray(P.perm, dtype=np.int64)
+    Xtmp = np.asfortranarray(B.copy())
+    _native.check(lib.mf_solve(h, _native.ptrd(Xtmp), 0, n, _native.ptr64(perm_np)), "perm upload")
+    if mixed:
+        _native.check(lib.mf_solve_refined(h, _native.ptrd(Xtmp), 0, n, _native.ptr64(perm_np), tol, maxit,
+                                           ctypes.byref(iters), ctypes.byref(eta_dev)), "perm upload")
     if info.value != 0 or not eta <= 1e-12:
-        raise SystemExit(f"bench: factorization check failed (info={info.value}, backward error={eta})")
+        raise SystemExit(f"bench: check failed (mixed={mixed}, info={info.value}, backward error={eta})")
 
     # profiling pass (per-kernel events; not the timed pass)
     lib.mf_profile(h, 1)
     step_device()
     stream.synchronize()
-    ms = (ctypes.c_double * 13)()
-    ln = (ctypes.c_int64 * 13)()
+    ms = (ctypes.c_double * NK)()
+    ln = (ctypes.c_int64 * NK)()
     lib.mf_kernel_times(h, ms, ln)
     lib.mf_profile(h, 0)
-    ktimes = {KERNEL_NAMES[i]: {"ms": ms[i], "launches": int(ln[i])} for i in range(13)}
-    launches_per_step = int(sum(ln[i] for i in range(13)))
+    ktimes = {KERNEL_NAMES[i]: {"ms": ms[i], "launches": int(ln[i])} for i in range(NK)}
+    launches_per_step = int(sum(ln[i] for i in range(NK)))
+    enn, ena = exec_sizes(lib, h)
+    fl = kernel_flops(enn, ena)
 
     # timed device-resident pass
     for _ in range(args.warmup):
@@ -321,9 +438,11 @@ def main():
     torch.cuda.synchronize()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     evs[0].record(stream)
+    its = []
     for i in range(args.steps):
         step_device()
         evs[i + 1].record(stream)
+        its.append(int(iters.value))
     stream.synchronize()
     torch.cuda.synchronize()
     ck = clocks.stop()
@@ -335,6 +454,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_s = float(t.item())
     value = world * args.steps / total_s
+    Xt = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
+    eta_t = float(tm.backward_error(A, Xt, B).max())
 
     # e2e pass through the host-buffer C ABI
     for _ in range(args.warmup):
@@ -355,68 +476,18 @@ def main():
     e2e_value = world * args.steps / e2e_total
     Xe = X_host.numpy().reshape(n, args.nrhs, order="F")
     eta_e2e = float(tm.backward_error(A, Xe, B).max())
-
-    # roofline of the dominant kernel
-    peaks = measured_peaks()
-    enn, ena = exec_sizes(lib, h)
-    fl = kernel_flops(enn, ena)
-    classes = {
-        "syrk": (fl["syrk"], ["syrk"]),
-        "panel+update": (fl["panel+update"], ["panel", "update"]),
-        "small": (fl["small"], ["small"]),
-    }
-    cls_ms = {k: sum(ktimes[x]["ms"] for x in v[1]) for k, v in classes.items()}
-    dom = max(cls_ms, key=cls_ms.get)
-    dgemm = dgemm_peak_tflops(torch, dev)
-    flops = classes[dom][0]
-    launches = sum(ktimes[x]["launches"] for x in classes[dom][1])
-    kms = cls_ms[dom]
-    achieved = flops / (kms / 1e3) / 1e12 if kms > 0 else 0.0
-    per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
-                     "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
-    roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
-            "frac": achieved / dgemm if dgemm else None, "traffic": None,
-            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in MEASURED_PEAKS.json)",
-            "flops_per_launch": flops / max(launches, 1), "avg_launch_ms": kms / max(launches, 1),
-            "classes": per_class}
-
-    # CPU baseline: the oracle on one full step
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle
-        threads = os.cpu_count() or 1
-        oracle.set_threads(threads)
-        dt, cinfo, _ = cpu_reference_step(A, P, S, B)
-        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": f"one full factor+{args.nrhs}-RHS solve of the {args.side}^3 system ({dt:.2f} s)"}
-
-    if rank == 0:
-        line = {
-            "metric": "solves_per_s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"3d7pt_{args.side}^3_chol_factor+solve_{args.nrhs}rhs", "n": int(n),
-                       "fronts": int(S.nfr), "factor_gflop": S.factor_flops() / 1e9,
-                       "nnz_L": int(S.nnz()), "mode": "plain FP64", "l2": "inputs larger than L2 (factor 3.4 GB)",
-                       "parallelism": f"replicas x{world}"},
-            "factor_gflops_per_s": S.factor_flops() / (total_s / args.steps) / 1e9,
-            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "backward_error": eta,
-            "e2e": {"value": e2e_value, "unit": "solves/s",
-                    "h2d_bytes_per_step": int(nz_host.numel() * 8 + n * args.nrhs * 8),
-                    "d2h_bytes_per_step": int(n * args.nrhs * 8 + 8), "backward_error": eta_e2e,
-                    "p50_ms": float(np.percentile(e2e_ms, 50)), "p99_ms": float(np.percentile(e2e_ms, 99))},
-            "gpu_launches": launches_per_step * args.steps,
-            "roofline": roof,
-            "kernels": ktimes,
-            "clocks": ck,
-            "cpu_baseline": cpu,
-        }
-        print(json.dumps(line), flush=True)
     F.close()
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    del F
+    torch.cuda.empty_cache()
+    return {
+        "value": value, "ms_per_step": 1e3 * total_s / args.steps,
+        "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+        "backward_error": max(eta, eta_t), "iterations": its if mixed else None,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nz_host.numel() * 8 + n * args.nrhs * 8),
+                "d2h_bytes_per_step": int(n * args.nrhs * 8 + 8), "backward_error": eta_e2e,
+                "p50_ms": float(np.percentile(e2e_ms, 50)), "p99_ms": float(np.percentile(e2e_ms, 99))},
+        "gpu_launches": launches_per_step * args.steps, "kernels": ktimes, "clocks": ck, "flops": fl,
+    }
 
 
 if __name__ == "__main__":

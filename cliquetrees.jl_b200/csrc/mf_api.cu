@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <cstdlib>
 #include <new>
 
 #include "../../include/mfgpu.h"
@@ -45,7 +46,10 @@ void free_all(mf_handle* h) {
     void* ptrs[] = {h->d_fronts, h->d_septgt, h->d_reltgt, h->d_chdtgt, h->d_colfront, h->d_ref, h->d_sepmap,
                     h->d_items,  h->d_P,      h->d_M,      h->d_d,      h->d_signs,    h->d_info, h->d_R,
                     h->d_W,      h->d_C,      h->d_B,      h->d_perm,   h->d_DL,       h->d_slot, h->d_pslot,
-                    h->d_nz,     h->d_inv};
+                    h->d_nz,     h->d_inv,    h->d_nzrow,  h->d_nzcol,  h->d_dslot,    h->d_scale,
+                    h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
+                    h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
+                    h->d_part,   h->f32.part};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -148,8 +152,10 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     rc = rc ? rc : dalloc(h, &h->d_M, h->nmval, &tot);
     rc = rc ? rc : dalloc(h, &h->d_d, std::max<int64_t>(n, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_info, 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_err, 1, &tot);
     rc = rc ? rc : dalloc(h, &h->d_R, std::max<int64_t>(h->nrval_per_rhs * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_W, std::max<int64_t>(n * nrhs_cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_part, std::max<int64_t>(h->nbwd_part * kNB * 16, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_C, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_B, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_perm, std::max<int64_t>(n, 1), &tot);
@@ -168,6 +174,11 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     if (e == cudaSuccess) e = up(h->d_sepmap, h->h_sepmap.data(), sizeof(int32_t) * h->h_sepmap.size());
     if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
     if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
+    if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    {
+        const char* tcenv = getenv("MF_TENSOR_CORES");
+        h->use_tc = !(tcenv && tcenv[0] == '0');
+    }
     if (e != cudaSuccess) {
         cuda_fail(e, "mf_create upload");
         free_all(h);
@@ -176,8 +187,7 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     }
     g_total_bytes_last = tot;
     h->times = KernelTimes();
-    // remember the allocation size in the level-independent slot of times
-    h->times.ms[15] = (double)tot;
+    h->bytes = tot;
     *out = h;
     return 0;
 }
@@ -363,13 +373,78 @@ int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot) {
             return -2;
         }
     }
-    if (h->d_pslot) { cudaFree(h->d_pslot); h->d_pslot = nullptr; }
-    if (h->d_nz) { cudaFree(h->d_nz); h->d_nz = nullptr; }
+    // permuted (row, col) of every stored value, diagonal positions and the
+    // CSR of the whole symmetric matrix (residuals of the mixed path)
+    const int64_t n = h->n;
+    std::vector<int32_t> rowi(nnz), coli(nnz);
+    std::vector<int64_t> dslot(n, -1);
+    for (int64_t k = 0; k < nnz; ++k) {
+        int64_t s = slot[k];
+        int64_t r, c;
+        if (s < ndz) {
+            int64_t j = std::upper_bound(h->h_Dptr.begin(), h->h_Dptr.end(), s) - h->h_Dptr.begin() - 1;
+            const RefFront& rf = h->h_ref[j];
+            int64_t loc = s - rf.Dptr;
+            r = rf.res0 + loc % rf.nn;
+            c = rf.res0 + loc / rf.nn;
+        } else {
+            int64_t s2 = s - ndz;
+            int64_t j = std::upper_bound(h->h_Lptr.begin(), h->h_Lptr.end(), s2) - h->h_Lptr.begin() - 1;
+            const RefFront& rf = h->h_ref[j];
+            int64_t loc = s2 - rf.Lptr;
+            r = h->h_septgt[rf.sep0 + loc % rf.na];
+            c = rf.res0 + loc / rf.na;
+        }
+        rowi[k] = (int32_t)r;
+        coli[k] = (int32_t)c;
+        if (r == c) dslot[r] = k;
+    }
+    std::vector<int64_t> cptr(n + 1, 0);
+    for (int64_t k = 0; k < nnz; ++k) {
+        cptr[rowi[k] + 1]++;
+        if (rowi[k] != coli[k]) cptr[coli[k] + 1]++;
+    }
+    for (int64_t i = 0; i < n; ++i) cptr[i + 1] += cptr[i];
+    const int64_t nfull = cptr[n];
+    std::vector<int32_t> ccol(nfull);
+    std::vector<int64_t> csrc(nfull);
+    {
+        std::vector<int64_t> pos(cptr.begin(), cptr.end() - 1);
+        for (int64_t k = 0; k < nnz; ++k) {
+            int64_t r = rowi[k], c = coli[k];
+            ccol[pos[r]] = (int32_t)c; csrc[pos[r]++] = k;
+            if (r != c) { ccol[pos[c]] = (int32_t)r; csrc[pos[c]++] = k; }
+        }
+    }
+    void* olds[] = {h->d_pslot, h->d_nz, h->d_nzrow, h->d_nzcol, h->d_dslot, h->d_csrptr, h->d_csrcol, h->d_csrsrc};
+    for (void* o : olds)
+        if (o) cudaFree(o);
+    h->d_pslot = nullptr; h->d_nz = nullptr; h->d_nzrow = nullptr; h->d_nzcol = nullptr; h->d_dslot = nullptr;
+    h->d_csrptr = nullptr; h->d_csrcol = nullptr; h->d_csrsrc = nullptr;
     int64_t tot = 0;
     int rc;
     if ((rc = dalloc(h, &h->d_pslot, std::max<int64_t>(nnz, 1), &tot))) return rc;
     if ((rc = dalloc(h, &h->d_nz, std::max<int64_t>(nnz, 1), &tot))) return rc;
-    if (nnz) MF_CUDA(cudaMemcpy(h->d_pslot, pslot.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));
+    if ((rc = dalloc(h, &h->d_nzrow, std::max<int64_t>(nnz, 1), &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_nzcol, std::max<int64_t>(nnz, 1), &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_dslot, std::max<int64_t>(n, 1), &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_csrptr, n + 1, &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_csrcol, std::max<int64_t>(nfull, 1), &tot))) return rc;
+    if ((rc = dalloc(h, &h->d_csrsrc, std::max<int64_t>(nfull, 1), &tot))) return rc;
+    if (nnz) {
+        MF_CUDA(cudaMemcpy(h->d_pslot, pslot.data(), sizeof(int64_t) * nnz, cudaMemcpyHostToDevice));
+        MF_CUDA(cudaMemcpy(h->d_nzrow, rowi.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
+        MF_CUDA(cudaMemcpy(h->d_nzcol, coli.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice));
+    }
+    if (n) MF_CUDA(cudaMemcpy(h->d_dslot, dslot.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice));
+    MF_CUDA(cudaMemcpy(h->d_csrptr, cptr.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
+    if (nfull) {
+        MF_CUDA(cudaMemcpy(h->d_csrcol, ccol.data(), sizeof(int32_t) * nfull, cudaMemcpyHostToDevice));
+        MF_CUDA(cudaMemcpy(h->d_csrsrc, csrc.data(), sizeof(int64_t) * nfull, cudaMemcpyHostToDevice));
+    }
+    h->bytes += tot;
+    h->nnz_full = nfull;
+    h->cur_nz = nullptr;
     h->nnz = nnz;
     return 0;
 }
@@ -380,6 +455,8 @@ int mf_assemble(mf_handle* h, const double* nzval) {
     DeviceGuard g(h->device);
     if (h->nnz)
         MF_CUDA(cudaMemcpyAsync(h->d_nz, nzval, sizeof(double) * h->nnz, cudaMemcpyHostToDevice, h->stream));
+    h->cur_nz = h->d_nz;
+    if (h->mixed) return 0;  // the mixed factorization assembles its own scaled FP32 panels
     return launch_assemble(h, h->d_nz);
 }
 
@@ -387,6 +464,8 @@ int mf_assemble_device(mf_handle* h, const double* nzval_dev) {
     if (!h || (h->nnz && !nzval_dev)) { set_error("mf_assemble_device: bad arguments"); return -1; }
     if (!h->d_pslot) { set_error("mf_assemble_device: call mf_set_assembly first"); return -1; }
     DeviceGuard g(h->device);
+    h->cur_nz = nzval_dev;
+    if (h->mixed) return 0;
     return launch_assemble(h, nzval_dev);
 }
 
@@ -429,6 +508,161 @@ int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, cons
     return solve_chunks(h, perm_dev ? perm_dev : h->d_perm, nullptr, B_dev, nrhs, ldb);
 }
 
+int mf_enable_mixed(mf_handle* h) {
+    if (!h) { set_error("null handle"); return -1; }
+    if (!h->d_csrptr) { set_error("mf_enable_mixed: call mf_set_assembly first"); return -1; }
+    if (h->mixed) return 0;
+    DeviceGuard g(h->device);
+    int64_t tot = 0;
+    int rc = 0;
+    const int64_t n = h->n, cap = h->nrhs_cap;
+    rc = rc ? rc : dalloc(h, &h->f32.P, std::max<int64_t>(h->npanel, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.M, std::max<int64_t>(h->nmval, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.inv, std::max<int64_t>(h->ninv, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.d, std::max<int64_t>(n, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.R, std::max<int64_t>(h->nrval_per_rhs * cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.W, std::max<int64_t>(n * cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.part, std::max<int64_t>(h->nbwd_part * kNB * 16, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.C, std::max<int64_t>(n * cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_scale, std::max<int64_t>(n, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_iv, std::max<int64_t>(6 * n * cap, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_red, kRedDoubles, &tot);
+    if (rc) return rc;
+    h->bytes += tot;
+    h->mixed = true;
+    return 0;
+}
+
+int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* used_fp64) {
+    if (!h) { set_error("null handle"); return -1; }
+    if (!h->mixed) { set_error("mf_factorize_mixed: call mf_enable_mixed first"); return -1; }
+    if (!h->cur_nz) { set_error("mf_factorize_mixed: no values (mf_assemble)"); return -1; }
+    DeviceGuard g(h->device);
+    const double* ds = nullptr;
+    int rc;
+    if ((rc = upload_signs(h, signs, &ds))) return rc;
+    double* keep = h->d_signs;
+    h->d_signs = const_cast<double*>(ds);
+    int64_t inf = 0;
+    rc = launch_assemble_mixed(h, h->cur_nz);
+    if (!rc) rc = init_info(h);
+    if (!rc) rc = launch_factor_mixed(h);
+    if (!rc) rc = read_info(h, &inf);
+    h->mixed_fallback = false;
+    if (!rc && inf != 0) {
+        // FP32 rejected a pivot: factor in FP64 (the refinement then takes one
+        // FP64 solve), so an FP32 breakdown is never reported as a failure
+        rc = launch_assemble(h, h->cur_nz);
+        if (!rc) rc = init_info(h);
+        if (!rc) rc = launch_factor(h);
+        if (!rc) rc = read_info(h, &inf);
+        h->mixed_fallback = true;
+    }
+    if (!rc) rc = launch_anorm(h);
+    h->d_signs = keep;
+    if (rc) return rc;
+    int err = 0;
+    MF_CUDA(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    if (err) {
+        set_error("mf_factorize_mixed: a tensor-core wait timed out");
+        return -3;
+    }
+    if (info) *info = inf;
+    if (used_fp64) *used_fp64 = h->mixed_fallback ? 1 : 0;
+    return 0;
+}
+
+static int refined_chunks(mf_handle* h, double* hostB, double* devB, int64_t nrhs, int64_t ldb, const int64_t* dperm,
+                          double tol, int maxit, int* iters, double* eta) {
+    const int64_t cap = (int64_t)h->n * h->nrhs_cap;
+    double* bp = h->d_iv;
+    double* xp = h->d_iv + cap;
+    int worst_it = 0;
+    double worst_eta = 0.0;
+    int rc;
+    for (int64_t c0 = 0; c0 < nrhs; c0 += h->nrhs_cap) {
+        int64_t nc = std::min<int64_t>(h->nrhs_cap, nrhs - c0);
+        if (hostB) {
+            MF_CUDA(cudaMemcpy2DAsync(h->d_B, sizeof(double) * h->n, hostB + c0 * ldb, sizeof(double) * ldb,
+                                      sizeof(double) * h->n, nc, cudaMemcpyHostToDevice, h->stream));
+            if ((rc = launch_permute_to(h, h->d_B, h->n, dperm, nc, bp))) return rc;
+        } else {
+            if ((rc = launch_permute_to(h, devB + c0 * ldb, ldb, dperm, nc, bp))) return rc;
+        }
+        int it = 0;
+        double e = 0.0;
+        if ((rc = refine(h, bp, xp, (int)nc, tol, maxit, &it, &e))) return rc;
+        worst_it = std::max(worst_it, it);
+        worst_eta = std::max(worst_eta, e);
+        if (hostB) {
+            if ((rc = launch_permute_from(h, h->d_B, h->n, dperm, nc, xp))) return rc;
+            MF_CUDA(cudaMemcpy2DAsync(hostB + c0 * ldb, sizeof(double) * ldb, h->d_B, sizeof(double) * h->n,
+                                      sizeof(double) * h->n, nc, cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            if ((rc = launch_permute_from(h, devB + c0 * ldb, ldb, dperm, nc, xp))) return rc;
+        }
+    }
+    if (iters) *iters = worst_it;
+    if (eta) *eta = worst_eta;
+    return 0;
+}
+
+int mf_solve_refined(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm, double tol, int maxit,
+                     int* iters, double* eta) {
+    if (!h || nrhs < 0 || (nrhs > 0 && (!B || ldb < h->n)) || maxit < 1) {
+        set_error("mf_solve_refined: bad arguments");
+        return -1;
+    }
+    if (!h->mixed) { set_error("mf_solve_refined: call mf_enable_mixed and mf_factorize_mixed first"); return -1; }
+    DeviceGuard g(h->device);
+    if (perm && h->n) {
+        for (int64_t i = 0; i < h->n; ++i)
+            if (perm[i] < 0 || perm[i] >= h->n) { set_error("mf_solve_refined: perm out of range"); return -2; }
+        MF_CUDA(cudaMemcpyAsync(h->d_perm, perm, sizeof(int64_t) * h->n, cudaMemcpyHostToDevice, h->stream));
+    }
+    int rc = refined_chunks(h, B, nullptr, nrhs, ldb, h->d_perm, tol, maxit, iters, eta);
+    if (rc) return rc;
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev,
+                            double tol, int maxit, int* iters, double* eta) {
+    if (!h || nrhs < 0 || (nrhs > 0 && (!B_dev || ldb < h->n)) || maxit < 1) {
+        set_error("mf_solve_refined_device: bad arguments");
+        return -1;
+    }
+    if (!h->mixed) { set_error("mf_solve_refined_device: call mf_enable_mixed first"); return -1; }
+    DeviceGuard g(h->device);
+    return refined_chunks(h, nullptr, B_dev, nrhs, ldb, perm_dev ? perm_dev : h->d_perm, tol, maxit, iters, eta);
+}
+
+int mf_get_factor_mixed(mf_handle* h, double* Dval, double* Lval, double* d, double* scale) {
+    if (!h || !h->mixed) { set_error("mf_get_factor_mixed: no mixed factorization"); return -1; }
+    DeviceGuard g(h->device);
+    int rc;
+    if (!h->d_DL) {
+        int64_t tot = 0;
+        if ((rc = dalloc(h, &h->d_DL, std::max<int64_t>(h->ndz + h->nlz, 1), &tot))) return rc;
+    }
+    if ((rc = launch_panel32_to_dl(h, h->d_DL, h->d_DL + h->ndz))) return rc;
+    if (Dval && h->ndz)
+        MF_CUDA(cudaMemcpyAsync(Dval, h->d_DL, sizeof(double) * h->ndz, cudaMemcpyDeviceToHost, h->stream));
+    if (Lval && h->nlz)
+        MF_CUDA(cudaMemcpyAsync(Lval, h->d_DL + h->ndz, sizeof(double) * h->nlz, cudaMemcpyDeviceToHost, h->stream));
+    if (d && h->n) {
+        std::vector<float> tmp(h->n);
+        MF_CUDA(cudaMemcpyAsync(tmp.data(), h->f32.d, sizeof(float) * h->n, cudaMemcpyDeviceToHost, h->stream));
+        MF_CUDA(cudaStreamSynchronize(h->stream));
+        for (int64_t i = 0; i < h->n; ++i) d[i] = tmp[i];
+    }
+    if (scale && h->n)
+        MF_CUDA(cudaMemcpyAsync(scale, h->d_scale, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
 int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d) {
     if (!h) { set_error("null handle"); return -1; }
     DeviceGuard g(h->device);
@@ -460,7 +694,7 @@ int mf_synchronize(mf_handle* h) {
 int mf_info(const mf_handle* h, int64_t* out) {
     if (!h || !out) { set_error("mf_info: bad arguments"); return -1; }
     out[0] = h->n; out[1] = h->nfr; out[2] = h->ndz; out[3] = h->nlz;
-    out[4] = h->npanel; out[5] = h->nmval; out[6] = (int64_t)h->times.ms[15];
+    out[4] = h->npanel; out[5] = h->nmval; out[6] = h->bytes;
     out[7] = (int64_t)h->levels.size(); out[8] = h->nexec;
     return 0;
 }
@@ -476,10 +710,8 @@ int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na) {
 
 int mf_profile(mf_handle* h, int enable) {
     if (!h) { set_error("null handle"); return -1; }
-    double keep = h->times.ms[15];
     h->profile = enable != 0;
     h->times = KernelTimes();
-    h->times.ms[15] = keep;
     return 0;
 }
 

@@ -24,6 +24,7 @@
 //               blas/syrk.jl:137-159).
 #include <climits>
 #include <cstdio>
+#include <type_traits>
 
 #include "mf_internal.cuh"
 
@@ -56,11 +57,27 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 // assembly and layout conversion
 // ---------------------------------------------------------------------------
 
-__global__ void k_scatter(double* __restrict__ P, const int64_t* __restrict__ slot, const double* __restrict__ v,
-                          int64_t nnz) {
+template <typename T>
+__global__ void k_scatter(T* __restrict__ P, const int64_t* __restrict__ slot, const double* __restrict__ v,
+                          int64_t nnz, const int32_t* __restrict__ rowi, const int32_t* __restrict__ coli,
+                          const double* __restrict__ scale) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; i < nnz; i += stride) P[slot[i]] = v[i];
+    for (; i < nnz; i += stride) {
+        double x = v[i];
+        if (scale) x *= scale[rowi[i]] * scale[coli[i]];
+        P[slot[i]] = (T)x;
+    }
+}
+
+// scale[i] = 1/sqrt(|a_ii|) (1 where a_ii = 0) from the assembled values
+__global__ void k_diag_scale(double* __restrict__ scale, const int64_t* __restrict__ dslot,
+                             const double* __restrict__ v, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t k = dslot[i];
+    double a = k >= 0 ? fabs(v[k]) : 0.0;
+    scale[i] = a > 0.0 ? 1.0 / sqrt(a) : 1.0;
 }
 
 // one warp per column: copy between the reference layout (Dval nn x nn,
@@ -90,33 +107,54 @@ __global__ void k_dl_panel(const Front* __restrict__ fronts, const RefFront* __r
     }
 }
 
+// single-precision panels -> reference layout (mixed-mode factor download)
+__global__ void k_panel32_to_dl(const Front* __restrict__ fronts, const RefFront* __restrict__ ref,
+                                const int32_t* __restrict__ colref, const int32_t* __restrict__ sepmap,
+                                double* __restrict__ Dv, double* __restrict__ Lv, const float* __restrict__ P,
+                                int64_t n) {
+    int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const RefFront rf = ref[colref[warp]];
+    const Front f = fronts[rf.exec];
+    const int c = (int)(warp - rf.res0);
+    const int off = rf.res0 - f.col0;
+    const float* pc = P + f.poff + (int64_t)(off + c) * f.ldp;
+    double* dc = Dv + rf.Dptr + (int64_t)c * rf.nn;
+    double* lc = Lv + rf.Lptr + (int64_t)c * rf.na;
+    const int32_t* map = sepmap + rf.sep0;
+    for (int r = lane; r < rf.nn; r += 32) dc[r] = pc[off + r];
+    for (int r = lane; r < rf.na; r += 32) lc[r] = pc[map[r]];
+}
+
 // ---------------------------------------------------------------------------
 // small fronts: whole frontal matrix in shared memory
 // ---------------------------------------------------------------------------
-template <int LDLT>
+template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                const int32_t* __restrict__ reltgt,
-                                               const int32_t* __restrict__ chdtgt, double* __restrict__ P,
-                                               double* __restrict__ M, double* __restrict__ d,
+                                               const int32_t* __restrict__ chdtgt, T* __restrict__ P,
+                                               T* __restrict__ M, T* __restrict__ d,
                                                const double* __restrict__ signs, long long* __restrict__ info) {
-    extern __shared__ double F[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* F = reinterpret_cast<T*>(smem_raw);
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
-    double* Pj = P + f.poff;
+    T* Pj = P + f.poff;
     for (int i = tid; i < nj * nn; i += nt) {
         int r = i % nj, c = i / nj;
         F[i] = Pj[r + (int64_t)c * ld];
     }
-    for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = 0.0;
+    for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = T(0);
     __syncthreads();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na, lm = fc.ldm;
         const int32_t* rel = reltgt + fc.sep0;
-        const double* Mc = M + fc.moff;
+        const T* Mc = M + fc.moff;
         for (int i = tid; i < ma * ma; i += nt) {
             int a = i % ma, b = i / ma;
             if (a >= b) F[rel[a] + rel[b] * nj] += Mc[a + b * lm];
@@ -125,14 +163,14 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
     }
     // right-looking partial factorization of the first nn columns
     for (int k = 0; k < nn; ++k) {
-        double piv = F[k + k * nj];
+        T piv = F[k + k * nj];
         double s = pivot_sign(signs, LDLT, f.col0 + k);
-        if (!pivot_ok(s, piv) || (!LDLT && !(piv > 0.0))) {
+        if (!pivot_ok(s, (double)piv) || (!LDLT && !(piv > T(0)))) {
             if (tid == 0) atomicMin(info, (long long)(f.col0 + k + 1));
             return;  // uniform across the block
         }
-        double dk = LDLT ? piv : sqrt(piv);
-        double inv = 1.0 / dk;
+        T dk = LDLT ? piv : sqrt(piv);
+        T inv = T(1) / dk;
         __syncthreads();
         if (tid == 0) {
             if (LDLT) d[f.col0 + k] = piv; else F[k + k * nj] = dk;
@@ -143,7 +181,7 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
         for (int i = tid; i < m * m; i += nt) {
             int r = k + 1 + i % m, c = k + 1 + i / m;
             if (r >= c) {
-                double lc = F[c + k * nj];
+                T lc = F[c + k * nj];
                 if (LDLT) lc *= piv;
                 F[r + c * nj] -= F[r + k * nj] * lc;
             }
@@ -154,7 +192,7 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
         int r = i % nj, c = i / nj;
         Pj[r + (int64_t)c * ld] = F[i];
     }
-    double* Mj = M + f.moff;
+    T* Mj = M + f.moff;
     const int lm = f.ldm;
     for (int i = tid; i < na * na; i += nt) {
         int a = i % na, b = i / na;
@@ -174,35 +212,36 @@ __device__ __forceinline__ int lower_bound_i32(const int32_t* a, int n, int v) {
     return lo;
 }
 
+template <typename T>
 __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                             const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
-                                            double* __restrict__ P, double* __restrict__ M) {
+                                            T* __restrict__ P, T* __restrict__ M) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp, lm = f.ldm;
     const int c0 = it.a * kEAcols, c1 = min(c0 + kEAcols, nj);
     const int tid = threadIdx.x, nt = blockDim.x;
-    double* Pj = P + f.poff;
-    double* Mj = M + f.moff;
+    T* Pj = P + f.poff;
+    T* Mj = M + f.moff;
     // zero the update-matrix columns this CTA owns
     for (int c = max(c0, nn); c < c1; ++c)
-        for (int r = tid; r < na; r += nt) Mj[r + (int64_t)(c - nn) * lm] = 0.0;
+        for (int r = tid; r < na; r += nt) Mj[r + (int64_t)(c - nn) * lm] = T(0);
     __syncthreads();
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na, lmc = fc.ldm;
         const int32_t* rel = reltgt + fc.sep0;
-        const double* Mc = M + fc.moff;
+        const T* Mc = M + fc.moff;
         const int b0 = lower_bound_i32(rel, ma, c0);
         const int b1 = lower_bound_i32(rel, ma, c1);
         for (int b = b0; b < b1; ++b) {
             const int col = rel[b];
-            const double* mc = Mc + (int64_t)b * lmc;
+            const T* mc = Mc + (int64_t)b * lmc;
             if (col < nn) {
-                double* pc = Pj + (int64_t)col * ld;
+                T* pc = Pj + (int64_t)col * ld;
                 for (int a = b + tid; a < ma; a += nt) pc[rel[a]] += mc[a];
             } else {
-                double* dst = Mj + (int64_t)(col - nn) * lm - nn;
+                T* dst = Mj + (int64_t)(col - nn) * lm - nn;
                 for (int a = b + tid; a < ma; a += nt) dst[rel[a]] += mc[a];
             }
         }
@@ -213,64 +252,7 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 // ---------------------------------------------------------------------------
 // diagonal block: factor + inverse
 // ---------------------------------------------------------------------------
-constexpr int LDS = kNB + 4;  // shared-memory leading dimension (bank spread for DMMA fragments)
-
-// Factor the w x w diagonal block in shared memory (lower, ld LDS).
-// Returns the local failing column (0-based) or -1.  Must be called by all
-// threads of the block.
-template <int LDLT>
-__device__ int factor_diag_block(double* Dk, double* piv, int w, const double* signs, int64_t col0) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int k = 0; k < w; ++k) {
-        double p = Dk[k + k * LDS];
-        double s = pivot_sign(signs, LDLT, col0 + k);
-        if (!pivot_ok(s, p) || (!LDLT && !(p > 0.0))) return k;
-        double dk = LDLT ? p : sqrt(p);
-        double inv = 1.0 / dk;
-        __syncthreads();
-        if (tid == 0) {
-            piv[k] = LDLT ? p : dk;
-            if (!LDLT) Dk[k + k * LDS] = dk;
-        }
-        for (int i = k + 1 + tid; i < w; i += nt) Dk[i + k * LDS] *= inv;
-        __syncthreads();
-        const int m = w - k - 1;
-        for (int i = tid; i < m * m; i += nt) {
-            int r = k + 1 + i % m, c = k + 1 + i / m;
-            if (r >= c) {
-                double lc = Dk[c + k * LDS];
-                if (LDLT) lc *= p;
-                Dk[r + c * LDS] -= Dk[r + k * LDS] * lc;
-            }
-        }
-        __syncthreads();
-    }
-    return -1;
-}
-
-// Inverse of the factored lower-triangular block (unit diagonal for LDLt)
-// by row sweeps: X[i][j] = -(sum_{k=j}^{i-1} L[i][k] X[k][j]) / L[i][i].
-template <int LDLT>
-__device__ void invert_lower(const double* Dk, double* X, int w) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int i = tid; i < kNB * kNB; i += nt) X[i] = 0.0;
-    __syncthreads();
-    for (int i = 0; i < w; ++i) {
-        const double lii = LDLT ? 1.0 : Dk[i + i * LDS];
-        for (int j = tid; j <= i; j += nt) {
-            double v;
-            if (j == i) {
-                v = 1.0 / lii;
-            } else {
-                double acc = 0.0;
-                for (int k = j; k < i; ++k) acc += Dk[i + k * LDS] * X[k + j * kNB];
-                v = -acc / lii;
-            }
-            X[i + j * kNB] = v;
-        }
-        __syncthreads();
-    }
-}
+constexpr int LDS = kNB + 4;  // shared-memory leading dimension (bank spread for fragment loads)
 
 // Blocked factorization of a 64 x 64 diagonal block held in shared memory
 // (lower, ld LDS; columns >= w are padded with the identity).  Four 16-wide
@@ -279,8 +261,8 @@ __device__ void invert_lower(const double* Dk, double* X, int w) {
 // the rank-16 update to the trailing block.  piv[k] receives sqrt(pivot)
 // (Cholesky) or the pivot (LDLt).  Returns the first rejected local column
 // (< w) or -1; called by all threads.
-template <int LDLT>
-__device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs, int64_t col0, int* flag) {
+template <typename T, int LDLT>
+__device__ int factor_diag64(T* Dk, T* piv, int w, const double* signs, int64_t col0, int* flag) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     for (int p = 0; p < 4; ++p) {
         const int pb = p * 16;
@@ -288,13 +270,13 @@ __device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs
             int bad = -1;
             for (int k = 0; k < 16; ++k) {
                 const int c = pb + k;
-                const double pv = Dk[c + c * LDS];
+                const T pv = Dk[c + c * LDS];
                 if (c < w) {
                     const double sg = pivot_sign(signs, LDLT, col0 + c);
-                    if (!pivot_ok(sg, pv) || (!LDLT && !(pv > 0.0))) { bad = c; break; }
+                    if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) { bad = c; break; }
                 }
-                const double dk = LDLT ? pv : sqrt(pv);
-                const double inv = 1.0 / dk;
+                const T dk = LDLT ? pv : sqrt(pv);
+                const T inv = T(1) / dk;
                 __syncwarp();
                 if (lane > k && lane < 16) Dk[(pb + lane) + c * LDS] *= inv;
                 if (lane == 0) {
@@ -302,11 +284,10 @@ __device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs
                     if (!LDLT) Dk[c + c * LDS] = dk;
                 }
                 __syncwarp();
-                // rank-1 update of the rest of the 16 x 16 sub-block
                 for (int e = lane; e < 256; e += 32) {
                     const int i = e & 15, j = e >> 4;
                     if (j > k && i >= j) {
-                        double lj = Dk[(pb + j) + c * LDS];
+                        T lj = Dk[(pb + j) + c * LDS];
                         if (LDLT) lj *= pv;
                         Dk[(pb + i) + (pb + j) * LDS] -= Dk[(pb + i) + c * LDS] * lj;
                     }
@@ -317,10 +298,9 @@ __device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs
         }
         __syncthreads();
         if (*flag >= 0) return *flag;
-        // rows below the sub-block: X <- X Lpp^{-T} (Cholesky) or X Lpp^{-T} D^{-1} (LDLt)
         for (int r = pb + 16 + tid; r < 64; r += nt) {
             for (int c = 0; c < 16; ++c) {
-                double v = Dk[r + (pb + c) * LDS];
+                T v = Dk[r + (pb + c) * LDS];
                 for (int q = 0; q < c; ++q) v -= Dk[r + (pb + q) * LDS] * Dk[(pb + c) + (pb + q) * LDS];
                 if (!LDLT) v /= piv[pb + c];
                 Dk[r + (pb + c) * LDS] = v;
@@ -329,15 +309,14 @@ __device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs
                 for (int c = 0; c < 16; ++c) Dk[r + (pb + c) * LDS] /= piv[pb + c];
         }
         __syncthreads();
-        // trailing update: rank 16
         const int m = 64 - pb - 16;
         for (int e = tid; e < m * m; e += nt) {
             const int i = pb + 16 + e % m, j = pb + 16 + e / m;
             if (i >= j) {
-                double acc = 0.0;
+                T acc = T(0);
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    double lj = Dk[j + (pb + q) * LDS];
+                    T lj = Dk[j + (pb + q) * LDS];
                     if (LDLT) lj *= piv[pb + q];
                     acc += Dk[i + (pb + q) * LDS] * lj;
                 }
@@ -352,72 +331,70 @@ __device__ int factor_diag64(double* Dk, double* piv, int w, const double* signs
 // Inverse X (ld 64) of the factored 64 x 64 lower block (unit diagonal for
 // LDLt) in 16 x 16 blocks: the four diagonal blocks by one warp each, then
 // X_ij = -X_ii (sum_{k=j}^{i-1} L_ik X_kj) along the block sub-diagonals.
-template <int LDLT>
-__device__ void invert_lower64(const double* Dk, double* X, double* T) {
+template <typename T, int LDLT>
+__device__ void invert_lower64(const T* Dk, T* X, T* Tm) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < kNB * kNB; i += nt) X[i] = 0.0;
+    for (int i = tid; i < kNB * kNB; i += nt) X[i] = T(0);
     __syncthreads();
     if (warp < 4 && lane < 16) {
         const int b = warp * 16, j = lane;
-        const double* L = Dk + b + b * LDS;
-        double* Xb = X + b + b * kNB;
-        Xb[j + j * kNB] = LDLT ? 1.0 : 1.0 / L[j + j * LDS];
+        const T* L = Dk + b + b * LDS;
+        T* Xb = X + b + b * kNB;
+        Xb[j + j * kNB] = LDLT ? T(1) : T(1) / L[j + j * LDS];
         for (int i = j + 1; i < 16; ++i) {
-            double acc = 0.0;
+            T acc = T(0);
             for (int k = j; k < i; ++k) acc += L[i + k * LDS] * Xb[k + j * kNB];
             Xb[i + j * kNB] = LDLT ? -acc : -acc / L[i + i * LDS];
         }
     }
     __syncthreads();
     for (int dist = 1; dist < 4; ++dist) {
-        const int nb = 4 - dist;  // blocks (jb + dist, jb) for jb = 0 .. nb-1
-        // T_ij = sum_{k=j}^{i-1} L_ik X_kj   (16 x 16 per block)
+        const int nb = 4 - dist;
         for (int e = tid; e < nb * 256; e += nt) {
             const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
             const int ib = (blk + dist) * 16, jb = blk * 16;
-            double acc = 0.0;
+            T acc = T(0);
             for (int k = jb; k < ib; ++k) acc += Dk[(ib + r) + k * LDS] * X[k + (jb + c) * kNB];
-            T[e] = acc;
+            Tm[e] = acc;
         }
         __syncthreads();
-        // X_ij = -X_ii T_ij
         for (int e = tid; e < nb * 256; e += nt) {
             const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
             const int ib = (blk + dist) * 16, jb = blk * 16;
-            double acc = 0.0;
-            for (int k = 0; k <= r; ++k) acc += X[(ib + r) + (ib + k) * kNB] * T[(blk << 8) + (k << 4) + c];
+            T acc = T(0);
+            for (int k = 0; k <= r; ++k) acc += X[(ib + r) + (ib + k) * kNB] * Tm[(blk << 8) + (k << 4) + c];
             X[(ib + r) + (jb + c) * kNB] = -acc;
         }
         __syncthreads();
     }
 }
 
-template <int LDLT>
+template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                              int c0, double* __restrict__ P, double* __restrict__ inv,
-                                              double* __restrict__ d, const double* __restrict__ signs,
+                                              int c0, T* __restrict__ P, T* __restrict__ inv,
+                                              T* __restrict__ d, const double* __restrict__ signs,
                                               long long* __restrict__ info) {
-    extern __shared__ double smem[];
-    double* Dk = smem;                 // kNB * LDS
-    double* X = Dk + kNB * LDS;        // kNB * kNB
-    double* T = X + kNB * kNB;         // 3 * 256
-    double* piv = T + 3 * 256;         // kNB
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* Dk = reinterpret_cast<T*>(smem_raw);  // kNB * LDS
+    T* X = Dk + kNB * LDS;                   // kNB * kNB
+    T* Tm = X + kNB * kNB;                   // 3 * 256
+    T* piv = Tm + 3 * 256;                   // kNB
     __shared__ int flag;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int w = min(kNB, nn - c0);
     const int tid = threadIdx.x, nt = blockDim.x;
-    double* Pj = P + f.poff;
+    T* Pj = P + f.poff;
     for (int i = tid; i < kNB * kNB; i += nt) {
         int r = i & (kNB - 1), c = i >> 6;
-        double v;
+        T v;
         if (r < w && c < w) v = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
-        else v = (r == c) ? 1.0 : 0.0;
+        else v = (r == c) ? T(1) : T(0);
         Dk[r + c * LDS] = v;
     }
     __syncthreads();
-    int bad = factor_diag64<LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0, &flag);
+    int bad = factor_diag64<T, LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0, &flag);
     if (bad >= 0) {
         if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
         return;
@@ -428,60 +405,81 @@ __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, 
     }
     if (LDLT)
         for (int i = tid; i < w; i += nt) d[f.col0 + c0 + i] = piv[i];
-    invert_lower64<LDLT>(Dk, X, T);
-    double* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
+    invert_lower64<T, LDLT>(Dk, X, Tm);
+    T* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
     for (int i = tid; i < kNB * kNB; i += nt) {
         int r = i & (kNB - 1), c = i >> 6;
-        dst[i] = (r < w && c < w) ? X[i] : 0.0;
+        dst[i] = (r < w && c < w) ? X[i] : T(0);
     }
 }
 
 // ---------------------------------------------------------------------------
-// DMMA tile GEMM with a cp.async double-buffered K loop.
-// acc(64x64) += A(64 x K) * B(64 x K)^T, 8 warps; warp w owns rows
-// (w&1)*32..+32 and columns (w>>1)*16..+16 as 4 x 2 fragments of 8 x 8.
-// Shared tiles are [k][m] with m contiguous (leading dimension LDS).
+// Tile GEMM with a cp.async double-buffered K loop:
+// acc(64x64) += A(64 x K) * B(64 x K)^T.  Shared tiles are [k][m] with m
+// contiguous (leading dimension LDS).
+//   double: DMMA (mma.sync m8n8k4 f64), 8 warps; warp w owns rows
+//           (w&1)*32..+32 and columns (w>>1)*16..+16 as 4 x 2 fragments.
+//   float : FMA, thread t owns rows (t>>4)*4..+4 and columns (t&15)*4..+4.
 // ---------------------------------------------------------------------------
 constexpr int KC = 32;                   // K chunk per pipeline stage
-constexpr int STAGE = KC * LDS;          // doubles per matrix per stage
-constexpr int kGemmSmem = (4 * STAGE + 2 * KC) * (int)sizeof(double);
+constexpr int STAGE = KC * LDS;          // elements per matrix per stage
 
-struct Acc {
+template <typename T>
+constexpr int gemm_smem() { return (4 * STAGE + 2 * KC) * (int)sizeof(T); }
+
+template <typename T>
+struct Acc;
+template <>
+struct Acc<double> {
     double c[4][2][2];
 };
+template <>
+struct Acc<float> {
+    float c[4][4];
+};
 
-__device__ __forceinline__ void acc_zero(Acc& a) {
+__device__ __forceinline__ void acc_zero(Acc<double>& a) {
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j) a.c[i][j][0] = a.c[i][j][1] = 0.0;
 }
+__device__ __forceinline__ void acc_zero(Acc<float>& a) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a.c[i][j] = 0.f;
+}
 
-__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+template <typename T>
+__device__ __forceinline__ void cp_async_el(T* dst, const T* src, bool valid) {
     unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
-    int n = valid ? 8 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(n));
+    int n = valid ? (int)sizeof(T) : 0;
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(src), "r"(n));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-// Stage one K chunk: rows ra..ra+63 of A (clamped at amax) and rows
-// rb..rb+63 of B (clamped at bmax), columns k..k+kc-1, zero fill outside.
-__device__ __forceinline__ void stage_chunk(double* As, double* Bs, const double* A, int64_t lda, int ra, int amax,
-                                            const double* B, int64_t ldb, int rb, int bmax, int k, int kc) {
+template <typename T>
+__device__ __forceinline__ void stage_chunk(T* As, T* Bs, const T* A, int64_t lda, int ra, int amax, const T* B,
+                                            int64_t ldb, int rb, int bmax, int k, int kc) {
     for (int i = threadIdx.x; i < 64 * KC; i += blockDim.x) {
         int m = i & 63, kk = i >> 6;
         bool va = (ra + m < amax) && kk < kc;
         bool vb = (rb + m < bmax) && kk < kc;
-        const double* sa = A + (va ? (ra + m) + (int64_t)(k + kk) * lda : 0);
-        const double* sb = B + (vb ? (rb + m) + (int64_t)(k + kk) * ldb : 0);
-        cp_async8(As + m + kk * LDS, sa, va);
-        cp_async8(Bs + m + kk * LDS, sb, vb);
+        const T* sa = A + (va ? (ra + m) + (int64_t)(k + kk) * lda : 0);
+        const T* sb = B + (vb ? (rb + m) + (int64_t)(k + kk) * ldb : 0);
+        cp_async_el(As + m + kk * LDS, sa, va);
+        cp_async_el(Bs + m + kk * LDS, sb, vb);
     }
 }
 
-__device__ __forceinline__ void mma_chunk(Acc& acc, const double* As, const double* Bs, const double* dsc, int kc) {
+__device__ __forceinline__ void mma_chunk(Acc<double>& acc, const double* As, const double* Bs, const double* dsc,
+                                          int kc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
     const int fr = lane >> 2, fk = lane & 3;
@@ -499,20 +497,37 @@ __device__ __forceinline__ void mma_chunk(Acc& acc, const double* As, const doub
     }
 }
 
+__device__ __forceinline__ void mma_chunk(Acc<float>& acc, const float* As, const float* Bs, const float* dsc,
+                                          int kc) {
+    const int tr = (threadIdx.x >> 4) * 4, tc = (threadIdx.x & 15) * 4;
+    for (int k = 0; k < kc; ++k) {
+        const float4 a4 = *reinterpret_cast<const float4*>(As + tr + k * LDS);
+        const float4 b4 = *reinterpret_cast<const float4*>(Bs + tc + k * LDS);
+        const float s = dsc ? dsc[k] : 1.f;
+        const float a[4] = {a4.x * s, a4.y * s, a4.z * s, a4.w * s};
+        const float b[4] = {b4.x, b4.y, b4.z, b4.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc.c[i][j] = fmaf(a[i], b[j], acc.c[i][j]);
+    }
+}
+
 // acc += A[ra.., kbeg..kend) * B[rb.., kbeg..kend)^T (optionally D-scaled)
-__device__ void gemm_k_loop(Acc& acc, double* smem, const double* A, int64_t lda, int ra, int amax, const double* B,
-                            int64_t ldb, int rb, int bmax, int kbeg, int kend, const double* dvec) {
-    double* As[2] = {smem, smem + STAGE};
-    double* Bs[2] = {smem + 2 * STAGE, smem + 3 * STAGE};
-    double* Ds[2] = {smem + 4 * STAGE, smem + 4 * STAGE + KC};
+template <typename T>
+__device__ void gemm_k_loop(Acc<T>& acc, T* smem, const T* A, int64_t lda, int ra, int amax, const T* B,
+                            int64_t ldb, int rb, int bmax, int kbeg, int kend, const T* dvec) {
     const int nchunk = (kend - kbeg + KC - 1) / KC;
     if (nchunk <= 0) return;
+    auto buf_a = [&](int st) { return smem + st * STAGE; };
+    auto buf_b = [&](int st) { return smem + (2 + st) * STAGE; };
+    auto buf_d = [&](int st) { return smem + 4 * STAGE + st * KC; };
     auto load = [&](int c, int st) {
         int k = kbeg + c * KC;
         int kc = min(KC, kend - k);
-        stage_chunk(As[st], Bs[st], A, lda, ra, amax, B, ldb, rb, bmax, k, kc);
+        stage_chunk(buf_a(st), buf_b(st), A, lda, ra, amax, B, ldb, rb, bmax, k, kc);
         if (dvec)
-            for (int i = threadIdx.x; i < KC; i += blockDim.x) Ds[st][i] = i < kc ? dvec[k + i] : 0.0;
+            for (int i = threadIdx.x; i < KC; i += blockDim.x) buf_d(st)[i] = i < kc ? dvec[k + i] : T(0);
         cp_commit();
     };
     load(0, 0);
@@ -526,16 +541,14 @@ __device__ void gemm_k_loop(Acc& acc, double* smem, const double* A, int64_t lda
         }
         __syncthreads();
         int kc = min(KC, kend - (kbeg + c * KC));
-        mma_chunk(acc, As[st], Bs[st], dvec ? Ds[st] : nullptr, (kc + 3) & ~3);
+        mma_chunk(acc, buf_a(st), buf_b(st), dvec ? buf_d(st) : nullptr, (kc + 3) & ~3);
         __syncthreads();
     }
 }
 
-// C(rbase+r, cbase+c) -= acc (or = acc * colscale when OVERWRITE), for
-// r < rmax, c < cmax; on a diagonal tile only row >= col is written.
-template <bool OVERWRITE>
-__device__ __forceinline__ void acc_store(const Acc& acc, double* C, int64_t ldc, int rbase, int cbase, int rmax,
-                                          int cmax, bool diag_tile, const double* colscale) {
+// visit every accumulator element as (row, col, value)
+template <typename F>
+__device__ __forceinline__ void acc_for_each(const Acc<double>& acc, F&& fn) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;
 #pragma unroll
@@ -543,59 +556,74 @@ __device__ __forceinline__ void acc_store(const Acc& acc, double* C, int64_t ldc
 #pragma unroll
         for (int j = 0; j < 2; ++j)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                int r = wr + i * 8 + (lane >> 2);
-                int c = wc + j * 8 + (lane & 3) * 2 + e;
-                if (r < rmax && c < cmax && (!diag_tile || rbase + r >= cbase + c)) {
-                    double* p = C + (rbase + r) + (int64_t)(cbase + c) * ldc;
-                    if (OVERWRITE) *p = colscale ? acc.c[i][j][e] * colscale[c] : acc.c[i][j][e];
-                    else *p -= acc.c[i][j][e];
-                }
-            }
+            for (int e = 0; e < 2; ++e)
+                fn(wr + i * 8 + (lane >> 2), wc + j * 8 + (lane & 3) * 2 + e, acc.c[i][j][e]);
+}
+template <typename F>
+__device__ __forceinline__ void acc_for_each(const Acc<float>& acc, F&& fn) {
+    const int tr = (threadIdx.x >> 4) * 4, tc = (threadIdx.x & 15) * 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) fn(tr + i, tc + j, acc.c[i][j]);
+}
+
+// C(rbase+r, cbase+c) -= acc (or = acc * colscale when OVERWRITE), for
+// r < rmax, c < cmax; on a diagonal tile only row >= col is written.
+template <bool OVERWRITE, typename T>
+__device__ __forceinline__ void acc_store(const Acc<T>& acc, T* C, int64_t ldc, int rbase, int cbase, int rmax,
+                                          int cmax, bool diag_tile, const T* colscale) {
+    acc_for_each(acc, [&](int r, int c, T v) {
+        if (r < rmax && c < cmax && (!diag_tile || rbase + r >= cbase + c)) {
+            T* p = C + (rbase + r) + (int64_t)(cbase + c) * ldc;
+            if (OVERWRITE) *p = colscale ? v * colscale[c] : v;
+            else *p -= v;
+        }
+    });
 }
 
 enum GemmRole { G_LEFT = 0, G_TRAIL = 1, G_SYRK = 2, G_TRSM = 3 };
 
-template <int ROLE, int LDLT>
+template <typename T, int ROLE, int LDLT>
 __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                              int ob, int c0, double* __restrict__ P, double* __restrict__ M,
-                                              const double* __restrict__ d, const double* __restrict__ inv) {
-    extern __shared__ double smem[];
+                                              int ob, int c0, T* __restrict__ P, T* __restrict__ M,
+                                              const T* __restrict__ d, const T* __restrict__ inv) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* smem = reinterpret_cast<T*>(smem_raw);
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
-    double* Pj = P + f.poff;
-    const double* dj = LDLT ? d + f.col0 : nullptr;
-    Acc acc;
+    T* Pj = P + f.poff;
+    const T* dj = LDLT ? d + f.col0 : nullptr;
+    Acc<T> acc;
     acc_zero(acc);
     if (ROLE == G_LEFT) {
-        // sub-panel [c0, c0+w) rows [c0 + 64 a, ..) -= panel cols [ob*kOB, c0)
         const int w = min(kNB, nn - c0);
         const int rs = c0 + it.a * kTile;
-        gemm_k_loop(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, ob * kOB, c0, dj);
-        acc_store<false>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, nullptr);
+        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, ob * kOB, c0, dj);
+        acc_store<false>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_TRAIL) {
         const int e = min(nn, (ob + 1) * kOB);
         const int cs = e + it.b * kTile, rs = cs + it.a * kTile;
-        gemm_k_loop(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, ob * kOB, e, dj);
-        acc_store<false>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, nullptr);
+        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, ob * kOB, e, dj);
+        acc_store<false>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_SYRK) {
         const int rs = it.a * kTile, cs = it.b * kTile;
-        gemm_k_loop(acc, smem, Pj + nn, ld, rs, na, Pj + nn, ld, cs, na, 0, nn, dj);
-        acc_store<false>(acc, M + f.moff, f.ldm, rs, cs, na - rs, na - cs, it.a == it.b, nullptr);
+        gemm_k_loop<T>(acc, smem, Pj + nn, ld, rs, na, Pj + nn, ld, cs, na, 0, nn, dj);
+        acc_store<false>(acc, M + f.moff, f.ldm, rs, cs, na - rs, na - cs, it.a == it.b, (const T*)nullptr);
     } else {
         // X (rows below the diagonal block, cols [c0, c0+w)) = X * Linv^T (* D^-1)
         const int w = min(kNB, nn - c0);
         const int rs = c0 + w + it.a * kTile;
-        const double* Li = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
-        gemm_k_loop(acc, smem, Pj + (int64_t)c0 * ld, ld, rs, nj, Li - 0, kNB, 0, w, 0, w, nullptr);
+        const T* Li = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
+        gemm_k_loop<T>(acc, smem, Pj + (int64_t)c0 * ld, ld, rs, nj, Li, kNB, 0, w, 0, w, (const T*)nullptr);
         __syncthreads();
-        double* sc = smem;  // reuse: reciprocal pivots for LDLt
+        T* sc = smem;  // reuse: reciprocal pivots for LDLt
         if (LDLT) {
-            for (int i = threadIdx.x; i < w; i += blockDim.x) sc[i] = 1.0 / dj[c0 + i];
+            for (int i = threadIdx.x; i < w; i += blockDim.x) sc[i] = T(1) / dj[c0 + i];
             __syncthreads();
         }
-        acc_store<true>(acc, Pj + (int64_t)c0 * ld, ld, rs, 0, nj - rs, w, false, LDLT ? sc : nullptr);
+        acc_store<true>(acc, Pj + (int64_t)c0 * ld, ld, rs, 0, nj - rs, w, false, LDLT ? (const T*)sc : nullptr);
     }
 }
 
@@ -623,16 +651,28 @@ Timer::~Timer() {
 
 static inline unsigned grid_for(int64_t cnt) { return (unsigned)cnt; }
 
-int launch_assemble(mf_handle* h, const double* dnz) {
+template <typename T>
+static int assemble_impl(mf_handle* h, const double* dnz, T* P, const double* scale) {
     Timer t(h, K_ASSEMBLE);
-    MF_CUDA(cudaMemsetAsync(h->d_P, 0, sizeof(double) * h->npanel, h->stream));
+    MF_CUDA(cudaMemsetAsync(P, 0, sizeof(T) * h->npanel, h->stream));
     if (h->nnz > 0) {
         int64_t blocks = (h->nnz + 255) / 256;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        k_scatter<<<(unsigned)blocks, 256, 0, h->stream>>>(h->d_P, h->d_pslot, dnz, h->nnz);
+        k_scatter<T><<<(unsigned)blocks, 256, 0, h->stream>>>(P, h->d_pslot, dnz, h->nnz, h->d_nzrow, h->d_nzcol,
+                                                               scale);
         MF_CUDA(cudaGetLastError());
     }
     return 0;
+}
+
+int launch_assemble(mf_handle* h, const double* dnz) { return assemble_impl<double>(h, dnz, h->d_P, nullptr); }
+
+int launch_assemble_mixed(mf_handle* h, const double* dnz) {
+    if (h->n > 0) {
+        k_diag_scale<<<(unsigned)((h->n + 255) / 256), 256, 0, h->stream>>>(h->d_scale, h->d_dslot, dnz, h->n);
+        MF_CUDA(cudaGetLastError());
+    }
+    return assemble_impl<float>(h, dnz, h->f32.P, h->d_scale);
 }
 
 int launch_dl_to_panel(mf_handle* h, const double* dD, const double* dL) {
@@ -658,63 +698,103 @@ int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
     return 0;
 }
 
-constexpr int kDiagSmem = (kNB * LDS + kNB * kNB + 3 * 256 + kNB) * (int)sizeof(double);
+int launch_panel32_to_dl(mf_handle* h, double* dD, double* dL) {
+    if (h->n == 0) return 0;
+    int64_t threads = h->n * 32;
+    unsigned blocks = (unsigned)((threads + 255) / 256);
+    k_panel32_to_dl<<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
+                                                   h->f32.P, h->n);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
 
-template <int LDLT>
-static int factor_impl(mf_handle* h) {
-    MF_CUDA(cudaFuncSetAttribute(k_small<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kSmallMax * kSmallMax * (int)sizeof(double)));
-    MF_CUDA(cudaFuncSetAttribute(k_diag<LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDiagSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm<G_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGemmSmem));
+template <typename T>
+constexpr int diag_smem() { return (kNB * LDS + kNB * kNB + 3 * 256 + kNB) * (int)sizeof(T); }
+
+template <typename T, int LDLT>
+static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
+    constexpr int gs = gemm_smem<T>();
+    MF_CUDA(cudaFuncSetAttribute(k_small<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSmallMax * kSmallMax * (int)sizeof(T)));
+    MF_CUDA(cudaFuncSetAttribute(k_diag<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
     const Item* items = h->d_items;
     for (const Level& lv : h->levels) {
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
-            k_small<LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(double), h->stream>>>(
-                h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, h->d_P, h->d_M, h->d_d, h->d_signs,
+            k_small<T, LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream>>>(
+                h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
                 h->d_info);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.ea.cnt) {
             Timer t(h, K_EA);
-            k_ea<<<grid_for(lv.ea.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea.off, h->d_reltgt,
-                                                             h->d_chdtgt, h->d_P, h->d_M);
+            k_ea<T><<<grid_for(lv.ea.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea.off, h->d_reltgt,
+                                                                h->d_chdtgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
         for (const PanelStep& st : lv.steps) {
             const int c0 = st.b * kOB + st.s * kNB;
+            if (std::is_same<T, float>::value && h->use_tc) {
+                // single precision: the GEMM roles run on the tcgen05 tensor cores
+                const FactorBufs<float>& f32b = reinterpret_cast<const FactorBufs<float>&>(fb);
+                int rc;
+                {
+                    Timer t(h, K_LEFT);
+                    if ((rc = tc_launch(h, 0, st.left_tc, st.b, c0, f32b))) return rc;
+                }
+                if (st.diag.cnt) {
+                    Timer t(h, K_DIAG);
+                    k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
+                        h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info);
+                    MF_CUDA(cudaGetLastError());
+                }
+                {
+                    Timer t(h, K_PANEL);
+                    if ((rc = tc_launch(h, 3, st.panel_tc, st.b, c0, f32b))) return rc;
+                }
+                {
+                    Timer t(h, K_UPDATE);
+                    if ((rc = tc_launch(h, 1, st.trail_tc, st.b, c0, f32b))) return rc;
+                }
+                continue;
+            }
             if (st.left.cnt) {
-                Timer t(h, K_UPDATE);
-                k_gemm<G_LEFT, LDLT><<<grid_for(st.left.cnt), 256, kGemmSmem, h->stream>>>(
-                    h->d_fronts, items + st.left.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
+                Timer t(h, K_LEFT);
+                k_gemm<T, G_LEFT, LDLT><<<grid_for(st.left.cnt), 256, gs, h->stream>>>(
+                    h->d_fronts, items + st.left.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.diag.cnt) {
-                Timer t(h, K_PANEL);
-                k_diag<LDLT><<<grid_for(st.diag.cnt), 256, kDiagSmem, h->stream>>>(
-                    h->d_fronts, items + st.diag.off, c0, h->d_P, h->d_inv, h->d_d, h->d_signs, h->d_info);
+                Timer t(h, K_DIAG);
+                k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
+                    h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.panel.cnt) {
                 Timer t(h, K_PANEL);
-                k_gemm<G_TRSM, LDLT><<<grid_for(st.panel.cnt), 256, kGemmSmem, h->stream>>>(
-                    h->d_fronts, items + st.panel.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
+                k_gemm<T, G_TRSM, LDLT><<<grid_for(st.panel.cnt), 256, gs, h->stream>>>(
+                    h->d_fronts, items + st.panel.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.trail.cnt) {
                 Timer t(h, K_UPDATE);
-                k_gemm<G_TRAIL, LDLT><<<grid_for(st.trail.cnt), 256, kGemmSmem, h->stream>>>(
-                    h->d_fronts, items + st.trail.off, st.b, c0, h->d_P, h->d_M, h->d_d, h->d_inv);
+                k_gemm<T, G_TRAIL, LDLT><<<grid_for(st.trail.cnt), 256, gs, h->stream>>>(
+                    h->d_fronts, items + st.trail.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
         }
-        if (lv.syrk.cnt) {
+        if (std::is_same<T, float>::value && h->use_tc) {
             Timer t(h, K_SYRK);
-            k_gemm<G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, kGemmSmem, h->stream>>>(
-                h->d_fronts, items + lv.syrk.off, 0, 0, h->d_P, h->d_M, h->d_d, h->d_inv);
+            int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
+            if (rc) return rc;
+        } else if (lv.syrk.cnt) {
+            Timer t(h, K_SYRK);
+            k_gemm<T, G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, gs, h->stream>>>(
+                h->d_fronts, items + lv.syrk.off, 0, 0, fb.P, fb.M, fb.d, fb.inv);
             MF_CUDA(cudaGetLastError());
         }
     }
@@ -722,7 +802,17 @@ static int factor_impl(mf_handle* h) {
 }
 
 int launch_factor(mf_handle* h) {
-    return h->diag ? factor_impl<1>(h) : factor_impl<0>(h);
+    FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d};
+    return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
+}
+
+int launch_factor_mixed(mf_handle* h) {
+    FactorBufs<float> fb{h->f32.P, h->f32.M, h->f32.inv, h->f32.d};
+    if (h->use_tc) {
+        int rc = tc_prepare(h);
+        if (rc) return rc;
+    }
+    return h->diag ? factor_impl<float, 1>(h, fb) : factor_impl<float, 0>(h, fb);
 }
 
 }  // namespace mf

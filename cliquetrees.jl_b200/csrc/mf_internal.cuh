@@ -67,8 +67,11 @@ constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
 constexpr int kNB = 64;         // sub-panel width of the blocked path
 constexpr int kOB = 256;        // outer block: trailing updates run with K = kOB
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
+constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns stay kTile
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
-constexpr int kSolveRows = 256; // rows per solve work item
+constexpr int kSolveRows = 256; // rows per gather work item
+constexpr int kFwdRows = 64;    // rows per forward-update work item
+constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
 
 // One 64-wide sub-panel s of outer block b (columns b*kOB + s*kNB ...).
 struct PanelStep {
@@ -77,6 +80,8 @@ struct PanelStep {
     ItemList diag;    // (front)            : diagonal block factor + inverse
     ItemList panel;   // (front, row tile)  : panel TRSM below the diagonal block (GEMM with the inverse)
     ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kOB
+    // the same work in 128-row tiles for the tensor-core (tcgen05) kernels
+    ItemList left_tc, panel_tc, trail_tc;
 };
 
 struct SolveStep {
@@ -89,22 +94,57 @@ struct Level {
     ItemList ea;             // (front, col tile) extend-add for blocked fronts
     std::vector<PanelStep> steps;
     ItemList syrk;           // (front, ti, tj)   M -= L L^T
+    ItemList syrk_tc;        // 128 x 64 tiles for the tcgen05 kernel
     // solves
     ItemList s_small;        // (front)
     ItemList s_gather;       // (front, row tile) forward gather of child updates
     std::vector<SolveStep> s_steps;
-    ItemList s_bwd_l;        // (front, col tile) C1 -= L^T x[sep]
+    ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
+    ItemList s_bwd_red;      // (front, col tile, first partial slot)
     int max_nn_blocked = 0;
 };
 
 struct KernelTimes {
-    double ms[16] = {0};
-    int64_t launches[16] = {0};
+    double ms[24] = {0};
+    int64_t launches[24] = {0};
 };
 
 enum KernelId {
     K_ASSEMBLE = 0, K_SMALL, K_EA, K_PANEL, K_UPDATE, K_SYRK,
-    K_S_SMALL, K_S_GATHER, K_S_FWD, K_S_BWD_L, K_S_BWD, K_PERM, K_OTHER, K_COUNT
+    K_S_SMALL, K_S_GATHER, K_S_FWD, K_S_BWD_L, K_S_BWD, K_PERM, K_OTHER,
+    K_DIAG, K_LEFT, K_SPMV, K_COUNT
+};
+
+// numeric buffers of one precision
+template <typename T>
+struct FactorBufs {
+    T* P = nullptr;    // panels
+    T* M = nullptr;    // update matrices
+    T* inv = nullptr;  // diagonal-block inverses
+    T* d = nullptr;    // LDLt pivots (n)
+};
+
+template <typename T>
+struct SolveBufs {
+    const T* P = nullptr;
+    const T* inv = nullptr;
+    const T* d = nullptr;
+    T* R = nullptr;
+    T* W = nullptr;
+    T* C = nullptr;
+    T* part = nullptr;  // backward partial sums (nbwd_part * 64 * 16)
+};
+
+// single-precision copy of the factor and solve workspaces (mixed mode)
+struct Mixed {
+    float* P = nullptr;
+    float* M = nullptr;
+    float* inv = nullptr;
+    float* d = nullptr;
+    float* R = nullptr;
+    float* W = nullptr;
+    float* C = nullptr;
+    float* part = nullptr;
 };
 
 }  // namespace mf
@@ -126,7 +166,7 @@ struct mf_handle {
     std::vector<int32_t> h_exec_chd;        // execution children CSR targets
     std::vector<int32_t> h_exec_rel;        // execution rel (indexed like septgt)
     std::vector<int32_t> h_sepmap;          // reference sep rows -> execution panel rows
-    std::vector<int64_t> h_resptr, h_sepptr, h_Dptr, h_Lptr;
+    std::vector<int64_t> h_resptr, h_sepptr, h_septgt, h_Dptr, h_Lptr;
     std::vector<mf::Level> levels;
     std::vector<mf::Item> h_items;
 
@@ -148,8 +188,12 @@ struct mf_handle {
     double* d_d = nullptr;         // LDLt pivots (n)
     double* d_signs = nullptr;     // pivot signs (n) or null
     long long* d_info = nullptr;   // first failing column (1-based), LLONG_MAX if none
+    int* d_err = nullptr;          // set by a kernel whose bounded wait timed out
+    bool use_tc = true;            // tcgen05 tensor cores for the FP32 GEMMs
     double* d_R = nullptr;         // solve updates (sum na * nrhs_cap)
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
+    double* d_part = nullptr;      // backward partial sums
+    int64_t nbwd_part = 0;         // partial slots (max over levels)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
     double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
     int64_t* d_perm = nullptr;     // permutation (n)
@@ -157,8 +201,26 @@ struct mf_handle {
     int64_t* d_slot = nullptr;     // assembly map into Dval|Lval (nnz)
     int64_t* d_pslot = nullptr;    // assembly map into panels (nnz)
     double* d_nz = nullptr;        // nonzero values staging (nnz)
+    int32_t* d_nzrow = nullptr;    // permuted row of each stored value (nnz)
+    int32_t* d_nzcol = nullptr;    // permuted column of each stored value (nnz)
+    int64_t* d_dslot = nullptr;    // index of a_ii among the stored values (n), -1 if absent
     int64_t nnz = 0;
 
+    // mixed precision (FP32 fronts + FP64 refinement)
+    bool mixed = false;
+    mf::Mixed f32;
+    double* d_scale = nullptr;     // symmetric diagonal scaling, elimination order (n)
+    // FP64 residual: CSR of the whole symmetric matrix in elimination order
+    int64_t* d_csrptr = nullptr;   // n+1
+    int32_t* d_csrcol = nullptr;   // nnz_full
+    int64_t* d_csrsrc = nullptr;   // index of each entry among the stored values
+    int64_t nnz_full = 0;
+    double* d_iv = nullptr;        // refinement vectors: b, x, r, z, p, q (6 * n * nrhs_cap)
+    double* d_red = nullptr;       // reductions and scalars (see mf_refine.cu)
+    const double* cur_nz = nullptr; // values of the current matrix (device)
+    bool mixed_fallback = false;   // FP32 factorization failed; the FP64 factor is used
+
+    int64_t bytes = 0;             // device bytes allocated
     // optional per-kernel timing
     bool profile = false;
     mf::KernelTimes times;
@@ -183,10 +245,21 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
 
 // kernel launchers (mf_factor.cu / mf_solve.cu); all stream ordered
 int launch_factor(mf_handle* h);
+int launch_factor_mixed(mf_handle* h);
+int tc_prepare(mf_handle* h);
+int tc_launch(mf_handle* h, int role, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb);
+int launch_assemble_mixed(mf_handle* h, const double* dnz);
 int launch_dl_to_panel(mf_handle* h, const double* dDval, const double* dLval);
 int launch_panel_to_dl(mf_handle* h, double* dDval, double* dLval);
+int launch_panel32_to_dl(mf_handle* h, double* dDval, double* dLval);
 int launch_assemble(mf_handle* h, const double* dnz);
 int launch_solve(mf_handle* h, int64_t nrhs);
+int launch_solve_mixed(mf_handle* h, int64_t nrhs);
+int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst);
+int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);
+int launch_anorm(mf_handle* h);
+int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters, double* eta);
+constexpr int kRedDoubles = 256 + 16 * 148 * 4;
 int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
 int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
 const char* last_error();

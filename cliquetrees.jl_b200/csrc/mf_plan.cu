@@ -150,6 +150,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     h->nlz = Lptr[nfr];
     h->h_resptr.assign(resptr, resptr + nfr + 1);
     h->h_sepptr.assign(sepptr, sepptr + nfr + 1);
+    h->h_septgt.assign(septgt, septgt + sepptr[nfr]);
     h->h_Dptr.assign(Dptr, Dptr + nfr + 1);
     h->h_Lptr.assign(Lptr, Lptr + nfr + 1);
 
@@ -388,6 +389,38 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                         }
                     }
                 end(st.trail);
+                // 128-row tiles for the tcgen05 kernels
+                begin(st.left_tc);
+                if (sp > 0)
+                    for (int32_t j : fr) {
+                        const Front& f = h->h_fronts[j];
+                        if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
+                        for (int t = 0; t < (int)cdiv(f.nn + f.na - c0, kTM); ++t) push(j, t, 0);
+                    }
+                end(st.left_tc);
+                begin(st.panel_tc);
+                for (int32_t j : fr) {
+                    const Front& f = h->h_fronts[j];
+                    if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
+                    int w = std::min(kNB, f.nn - c0);
+                    for (int t = 0; t < (int)cdiv(f.nn + f.na - c0 - w, kTM); ++t) push(j, t, 0);
+                }
+                end(st.panel_tc);
+                begin(st.trail_tc);
+                if (last_sub)
+                    for (int32_t j : fr) {
+                        const Front& f = h->h_fronts[j];
+                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kOB) continue;
+                        const int e = std::min(f.nn, (ob + 1) * kOB);
+                        if (e >= f.nn) continue;
+                        const int nj = f.nn + f.na;
+                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
+                            const int cs = e + tj * kTile;
+                            // rows from the first 128-aligned tile that reaches the diagonal
+                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti) push(j, ti, tj);
+                        }
+                    }
+                end(st.trail_tc);
                 lv.steps.push_back(st);
             }
         }
@@ -401,6 +434,16 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 for (int ti = tj; ti < t; ++ti) push(j, ti, tj);
         }
         end(lv.syrk);
+        begin(lv.syrk_tc);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn + f.na <= kSmallMax || f.na == 0) continue;
+            int tc = (int)cdiv(f.na, kTile);
+            for (int tj = 0; tj < tc; ++tj)
+                // 128-row tiles starting at the diagonal column block: rows cs + 128 ti
+                for (int ti = 0; ti < (int)cdiv(f.na - tj * kTile, kTM); ++ti) push(j, ti, tj);
+        }
+        end(lv.syrk_tc);
 
         // solves: a front is solved by one CTA when the factorization kept it
         // whole (nj <= kSmallMax) or it is narrow; otherwise it is blocked in
@@ -434,7 +477,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 int nj = f.nn + f.na;
                 int w = std::min(kNB, f.nn - k * kNB);
                 int below = nj - (k * kNB + w);
-                int tiles = 1 + (int)cdiv(below, kSolveRows);
+                int tiles = 1 + (int)cdiv(below, kFwdRows);
                 for (int t = 0; t < tiles; ++t) push(j, t, 0);
             }
             end(st.fwd);
@@ -448,12 +491,22 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             end(st.bwd);
         }
         begin(lv.s_bwd_l);
+        int32_t slot = 0;
+        std::vector<Item> red;
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (solve_small(f)) continue;
-            for (int t = 0; t < cdiv(f.nn, kNB); ++t) push(j, t, 0);
+            const int nchunk = std::max<int>(1, (int)cdiv(f.na, kBwdRows));
+            for (int t = 0; t < cdiv(f.nn, kNB); ++t) {
+                red.push_back(Item{j, t, slot, 0});
+                for (int q = 0; q < nchunk; ++q) items.push_back(Item{j, t, q, slot++});
+            }
         }
         end(lv.s_bwd_l);
+        h->nbwd_part = std::max<int64_t>(h->nbwd_part, slot);
+        begin(lv.s_bwd_red);
+        for (const Item& r : red) items.push_back(r);
+        end(lv.s_bwd_red);
     }
     return 0;
 }

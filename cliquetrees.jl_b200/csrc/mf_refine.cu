@@ -1,0 +1,317 @@
+// Mixed precision: FP64 refinement around the single-precision factor.
+//
+// The matrix is scaled symmetrically, A_hat = S A S with S = diag(|a_ii|^-1/2),
+// and A_hat is factored in FP32 (the same plan and kernels as the FP64 path,
+// instantiated for float).  M^-1 r = S A_hat^-1 S r is applied by an FP32
+// supernodal solve.  FP64 stays in the residual b - A x (CSR of the original
+// values, elimination order), the solution update and the scalars:
+//   Cholesky : preconditioned conjugate gradients, one CG per right-hand side;
+//   LDLt     : classical iterative refinement x += M^-1 (b - A x).
+// Every iteration measures the normwise backward error
+//   eta = ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+// per column and stops when all columns reach the tolerance.  Reductions are
+// two-pass in a fixed order (dots) or order-independent (max), so a run is
+// bitwise repeatable.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "mf_internal.cuh"
+
+namespace mf {
+
+constexpr int kRedBlocks = 148 * 4;  // partial sums per reduction
+// d_red layout: [0,48) residual maxima, [48] ||A||_inf, [64,144) CG scalars,
+// [256, 256 + 16*kRedBlocks) dot partials
+constexpr int kRedPart = 256;
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+    // non-negative doubles order like their bit patterns
+    atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+// y = A x for nrhs columns (ld n); values read through the stored-value map
+__global__ void k_spmv(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                       const int64_t* __restrict__ src, const double* __restrict__ nz, const double* __restrict__ x,
+                       double* __restrict__ y, int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double acc[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) acc[r] = 0.0;
+    for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+        const double a = nz[src[p]];
+        const int64_t c = col[p];
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+            if (r < nrhs) acc[r] += a * x[c + r * n];
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+        if (r < nrhs) y[i + r * n] = acc[r];
+}
+
+// t = b - A x and the maxima needed by the backward error:
+// red[0..nrhs) = max|t|, red[16..) = max|x|, red[32..) = max|b|
+__global__ void k_resid(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                        const int64_t* __restrict__ src, const double* __restrict__ nz, const double* __restrict__ x,
+                        const double* __restrict__ b, double* __restrict__ t, double* __restrict__ red, int64_t n,
+                        int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    if (!live) i = n - 1;  // keep the whole block in the reductions; results of this lane are ignored below
+    double acc[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) acc[r] = 0.0;
+    for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+        const double a = nz[src[p]];
+        const int64_t c = col[p];
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+            if (r < nrhs) acc[r] += a * x[c + r * n];
+    }
+    // block-level maxima first, then one atomic per block and quantity
+    __shared__ double mx[48];
+    if (threadIdx.x < 48) mx[threadIdx.x] = 0.0;
+    __syncthreads();
+    for (int r = 0; r < nrhs; ++r) {
+        const double bi = b[i + r * n];
+        const double ti = bi - acc[r];
+        if (t && live) t[i + r * n] = ti;
+        double v0 = fabs(ti), v1 = fabs(x[i + r * n]), v2 = fabs(bi);
+        for (int o = 16; o > 0; o >>= 1) {
+            v0 = fmax(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+            v1 = fmax(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+            v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomic_max_nonneg(mx + r, v0);
+            atomic_max_nonneg(mx + 16 + r, v1);
+            atomic_max_nonneg(mx + 32 + r, v2);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 48 && (threadIdx.x & 15) < nrhs) atomic_max_nonneg(red + threadIdx.x, mx[threadIdx.x]);
+}
+
+// ||A||_inf (max absolute row sum) into *out
+__global__ void k_anorm(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
+                        const double* __restrict__ nz, double* __restrict__ out, int64_t n) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) s += fabs(nz[src[p]]);
+    atomic_max_nonneg(out, s);
+}
+
+// per-column partial dot products: part[blk * 16 + r]
+__global__ void k_dot_part(const double* __restrict__ u, const double* __restrict__ v, double* __restrict__ part,
+                           int64_t n, int nrhs) {
+    __shared__ double sh[256];
+    for (int r = 0; r < nrhs; ++r) {
+        double s = 0.0;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            s += u[i + r * n] * v[i + r * n];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) part[blockIdx.x * 16 + r] = sh[0];
+        __syncthreads();
+    }
+}
+
+// out[r] = sum over blocks (fixed order)
+__global__ void k_dot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int nrhs) {
+    int r = threadIdx.x;
+    if (r >= nrhs) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += part[b * 16 + r];
+    out[r] = s;
+}
+
+// CG scalars: mode 0: alpha = rz / pq; mode 1: beta = rz_new / rz, rz = rz_new
+__global__ void k_cg_scalars(double* __restrict__ sc, int nrhs, int mode) {
+    int r = threadIdx.x;
+    if (r >= nrhs) return;
+    double* rz = sc;           // [0..16)
+    double* pq = sc + 16;      // [16..32)
+    double* alpha = sc + 32;   // [32..48)
+    double* rzn = sc + 48;     // [48..64)
+    double* beta = sc + 64;    // [64..80)
+    if (mode == 0) {
+        alpha[r] = (pq[r] != 0.0 && rz[r] != 0.0) ? rz[r] / pq[r] : 0.0;
+    } else {
+        beta[r] = rz[r] != 0.0 ? rzn[r] / rz[r] : 0.0;
+        rz[r] = rzn[r];
+    }
+}
+
+// x += alpha p ; r -= alpha q
+__global__ void k_cg_xr(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                        const double* __restrict__ q, const double* __restrict__ alpha, int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) {
+        const double a = alpha[i / n];
+        x[i] += a * p[i];
+        r[i] -= a * q[i];
+    }
+}
+
+// p = z + beta p
+__global__ void k_cg_p(double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ beta,
+                       int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) p[i] = z[i] + beta[i / n] * p[i];
+}
+
+// c = (float)(s .* r)   and   z = s .* (double)c  (+= when ACC)
+__global__ void k_to32(float* __restrict__ c, const double* __restrict__ r, const double* __restrict__ s, int64_t n,
+                       int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) c[i] = (float)(s[i % n] * r[i]);
+}
+template <bool ACC>
+__global__ void k_from32(double* __restrict__ z, const float* __restrict__ c, const double* __restrict__ s, int64_t n,
+                         int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) {
+        double v = s[i % n] * (double)c[i];
+        if (ACC) z[i] += v; else z[i] = v;
+    }
+}
+
+static unsigned gs_blocks(int64_t work) {
+    int64_t b = (work + 255) / 256;
+    if (b > 148 * 8) b = 148 * 8;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+static inline unsigned row_blocks(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + 255) / 256); }
+
+// z = M^-1 r (ACC: z += M^-1 r) through the FP32 factor
+template <bool ACC>
+static int apply_prec(mf_handle* h, const double* r, double* z, int nrhs) {
+    k_to32<<<gs_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->f32.C, r, h->d_scale, h->n, nrhs);
+    MF_CUDA(cudaGetLastError());
+    int rc = launch_solve_mixed(h, nrhs);
+    if (rc) return rc;
+    k_from32<ACC><<<gs_blocks(h->n * nrhs), 256, 0, h->stream>>>(z, h->f32.C, h->d_scale, h->n, nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+static int dot(mf_handle* h, const double* u, const double* v, double* out, int nrhs) {
+    double* part = h->d_red + kRedPart;
+    k_dot_part<<<kRedBlocks, 256, 0, h->stream>>>(u, v, part, h->n, nrhs);
+    MF_CUDA(cudaGetLastError());
+    k_dot_final<<<1, 32, 0, h->stream>>>(part, out, kRedBlocks, nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// backward error per column into eta[] (host); t receives b - A x when non-null
+static int backward_error(mf_handle* h, const double* x, const double* b, double* t, int nrhs, double* eta) {
+    Timer tm(h, K_SPMV);
+    double* red = h->d_red;  // [0..48) maxima, [48] ||A||_inf
+    MF_CUDA(cudaMemsetAsync(red, 0, 48 * sizeof(double), h->stream));
+    k_resid<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b, t, red,
+                                                      h->n, nrhs);
+    MF_CUDA(cudaGetLastError());
+    double hred[49];
+    MF_CUDA(cudaMemcpyAsync(hred, red, 49 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    for (int r = 0; r < nrhs; ++r) {
+        double den = hred[48] * hred[16 + r] + hred[32 + r];
+        eta[r] = den > 0.0 ? hred[r] / den : (hred[r] > 0.0 ? INFINITY : 0.0);
+    }
+    return 0;
+}
+
+int launch_anorm(mf_handle* h) {
+    double* out = h->d_red + 48;
+    MF_CUDA(cudaMemsetAsync(out, 0, sizeof(double), h->stream));
+    k_anorm<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, out, h->n);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// Solve A x = b (b, x: n x nrhs, ld n, elimination order, device) to
+// backward error <= tol with at most maxit refinement steps.
+int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters, double* eta_out) {
+    const int64_t n = h->n;
+    const int64_t cap = (int64_t)n * h->nrhs_cap;
+    double* R = h->d_iv + 2 * cap;  // [0, 2cap) hold b and x of the caller
+    double* Z = R + cap;
+    double* Pv = Z + cap;
+    double* Q = Pv + cap;
+    double* sc = h->d_red + 64;  // CG scalars (80 doubles)
+    double eta[16];
+    int rc, it = 0;
+    double worst = INFINITY;
+    if (h->mixed_fallback) {
+        // the FP32 factorization failed: the FP64 factor is on the device
+        MF_CUDA(cudaMemcpyAsync(h->d_C, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = launch_solve(h, nrhs))) return rc;
+        MF_CUDA(cudaMemcpyAsync(x, h->d_C, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = backward_error(h, x, b, nullptr, nrhs, eta))) return rc;
+        worst = 0.0;
+        for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
+        if (iters) *iters = 1;
+        if (eta_out) *eta_out = worst;
+        return 0;
+    }
+    if (!h->diag) {
+        // preconditioned conjugate gradients
+        MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
+        MF_CUDA(cudaMemcpyAsync(R, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = apply_prec<false>(h, R, Z, nrhs))) return rc;
+        MF_CUDA(cudaMemcpyAsync(Pv, Z, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        if ((rc = dot(h, R, Z, sc, nrhs))) return rc;  // rz
+        for (it = 1; it <= maxit; ++it) {
+            {
+                Timer tm(h, K_SPMV);
+                k_spmv<<<row_blocks(n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Pv, Q,
+                                                              n, nrhs);
+                MF_CUDA(cudaGetLastError());
+            }
+            if ((rc = dot(h, Pv, Q, sc + 16, nrhs))) return rc;  // pq
+            k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, 0);
+            k_cg_xr<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, sc + 32, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+            if ((rc = backward_error(h, x, b, nullptr, nrhs, eta))) return rc;
+            worst = 0.0;
+            for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
+            if (worst <= tol || it == maxit) break;
+            if ((rc = apply_prec<false>(h, R, Z, nrhs))) return rc;
+            if ((rc = dot(h, R, Z, sc + 48, nrhs))) return rc;  // rz_new
+            k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, 1);
+            k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+    } else {
+        // classical iterative refinement
+        MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
+        MF_CUDA(cudaMemcpyAsync(R, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
+        for (it = 1; it <= maxit; ++it) {
+            if ((rc = apply_prec<true>(h, R, x, nrhs))) return rc;
+            if ((rc = backward_error(h, x, b, R, nrhs, eta))) return rc;
+            worst = 0.0;
+            for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
+            if (worst <= tol) break;
+        }
+        if (it > maxit) it = maxit;
+    }
+    if (iters) *iters = it;
+    if (eta_out) *eta_out = worst;
+    return 0;
+}
+
+}  // namespace mf

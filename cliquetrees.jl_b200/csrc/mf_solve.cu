@@ -35,7 +35,8 @@ __global__ void k_perm(double* __restrict__ C, double* B, const int64_t* __restr
     }
 }
 
-__global__ void k_diag_div(double* __restrict__ C, const double* __restrict__ d, int64_t n, int nrhs) {
+template <typename T>
+__global__ void k_diag_div(T* __restrict__ C, const T* __restrict__ d, int64_t n, int nrhs) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) C[i] /= d[i % n];
@@ -44,29 +45,28 @@ __global__ void k_diag_div(double* __restrict__ C, const double* __restrict__ d,
 // ---------------------------------------------------------------------------
 // small fronts (nj <= 96, or nn <= 64 and na <= 1024): one CTA per front
 // ---------------------------------------------------------------------------
-template <int UNIT>
+template <typename T, int UNIT>
 __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                      const int32_t* __restrict__ reltgt,
-                                                     const int32_t* __restrict__ chdtgt, const double* __restrict__ P,
-                                                     double* __restrict__ C, double* __restrict__ R, int64_t n,
-                                                     int nrhs) {
-    __shared__ double C1[kSmallMax * kMaxRhs];
+                                                     const int32_t* __restrict__ chdtgt, const T* __restrict__ P,
+                                                     T* __restrict__ C, T* __restrict__ R, int64_t n, int nrhs) {
+    __shared__ T C1[kSmallMax * kMaxRhs];
     const Front f = fronts[items[blockIdx.x].front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const double* Pj = P + f.poff;
-    double* Rj = R + f.roff * nrhs;
+    const T* Pj = P + f.poff;
+    T* Rj = R + f.roff * nrhs;
     for (int i = tid; i < nn * nrhs; i += nt) {
         int a = i % nn, r = i / nn;
         C1[a + r * kSmallMax] = C[f.col0 + a + (int64_t)r * n];
     }
-    for (int i = tid; i < na * nrhs; i += nt) Rj[i] = 0.0;
+    for (int i = tid; i < na * nrhs; i += nt) Rj[i] = T(0);
     __syncthreads();
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na;
         const int32_t* rel = reltgt + fc.sep0;
-        const double* Mc = R + fc.roff * nrhs;
+        const T* Mc = R + fc.roff * nrhs;
         for (int i = tid; i < ma * nrhs; i += nt) {
             int a = i % ma, r = i / ma;
             int q = rel[a];
@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
     // C1 <- D^{-1} C1
     for (int k = 0; k < nn; ++k) {
         if (!UNIT) {
-            double inv = 1.0 / Pj[k + (int64_t)k * ld];
+            T inv = T(1) / Pj[k + (int64_t)k * ld];
             for (int r = tid; r < nrhs; r += nt) C1[k + r * kSmallMax] *= inv;
             __syncthreads();
         }
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
     // R_j -= L21 C1
     for (int i = tid; i < na * nrhs; i += nt) {
         int a = i % na, r = i / na;
-        double s = 0.0;
+        T s = T(0);
         for (int k = 0; k < nn; ++k) s += Pj[(nn + a) + (int64_t)k * ld] * C1[k + r * kSmallMax];
         Rj[a + r * na] -= s;
     }
@@ -102,25 +102,25 @@ __global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ f
     }
 }
 
-template <int UNIT>
+template <typename T, int UNIT>
 __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                     const int32_t* __restrict__ septgt, const double* __restrict__ P,
-                                                     double* __restrict__ C, int64_t n, int nrhs) {
-    __shared__ double C1[kSmallMax * kMaxRhs];
+                                                     const int32_t* __restrict__ septgt, const T* __restrict__ P,
+                                                     T* __restrict__ C, int64_t n, int nrhs) {
+    __shared__ T C1[kSmallMax * kMaxRhs];
     const Front f = fronts[items[blockIdx.x].front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-    const double* Pj = P + f.poff;
+    const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
     // C1 = C[res] - L21^T x[sep]   (one warp per column of L21)
     for (int k = warp; k < nn; k += nw) {
-        double acc[kMaxRhs];
+        T acc[kMaxRhs];
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = 0.0;
-        const double* lc = Pj + nn + (int64_t)k * ld;
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = T(0);
+        const T* lc = Pj + nn + (int64_t)k * ld;
         for (int a = lane; a < na; a += 32) {
-            double l = lc[a];
+            T l = lc[a];
             int64_t row = sep[a];
 #pragma unroll
             for (int r = 0; r < kMaxRhs; ++r)
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
         }
 #pragma unroll
         for (int r = 0; r < kMaxRhs; ++r) {
-            double v = acc[r];
+            T v = acc[r];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
             acc[r] = v;
         }
@@ -141,11 +141,11 @@ __global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ f
         // C1[k] -= sum_{a>k} D[a,k] C1[a]
         if (warp == 0) {
             for (int r = 0; r < nrhs; ++r) {
-                double s = 0.0;
+                T s = T(0);
                 for (int a = k + 1 + lane; a < nn; a += 32) s += Pj[a + (int64_t)k * ld] * C1[a + r * kSmallMax];
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
                 if (lane == 0) {
-                    double v = C1[k + r * kSmallMax] - s;
+                    T v = C1[k + r * kSmallMax] - s;
                     if (!UNIT) v /= Pj[k + (int64_t)k * ld];
                     C1[k + r * kSmallMax] = v;
                 }
@@ -172,35 +172,35 @@ __device__ __forceinline__ int lb32(const int32_t* a, int n, int v) {
 }
 
 // forward gather: W[res] = C[res] + child updates, R_j = child updates
+template <typename T>
 __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                   const int32_t* __restrict__ reltgt,
-                                                  const int32_t* __restrict__ chdtgt, const double* __restrict__ C,
-                                                  double* __restrict__ W, double* __restrict__ R, int64_t n,
-                                                  int nrhs) {
+                                                  const int32_t* __restrict__ chdtgt, const T* __restrict__ C,
+                                                  T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
     const int tid = threadIdx.x, nt = blockDim.x;
-    double* Rj = R + f.roff * nrhs;
+    T* Rj = R + f.roff * nrhs;
     const int w = p1 - p0;
     for (int i = tid; i < w * nrhs; i += nt) {
         int q = p0 + i % w, r = i / w;
         if (q < nn) W[f.col0 + q + (int64_t)r * n] = C[f.col0 + q + (int64_t)r * n];
-        else Rj[(q - nn) + r * na] = 0.0;
+        else Rj[(q - nn) + r * na] = T(0);
     }
     __syncthreads();
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na;
         const int32_t* rel = reltgt + fc.sep0;
-        const double* Mc = R + fc.roff * nrhs;
+        const T* Mc = R + fc.roff * nrhs;
         const int a0 = lb32(rel, ma, p0), a1 = lb32(rel, ma, p1);
         const int cnt = a1 - a0;
         for (int i = tid; i < cnt * nrhs; i += nt) {
             int a = a0 + i % cnt, r = i / cnt;
             int q = rel[a];
-            double v = Mc[a + r * ma];
+            T v = Mc[a + r * ma];
             if (q < nn) W[f.col0 + q + (int64_t)r * n] += v;
             else Rj[(q - nn) + r * na] += v;
         }
@@ -212,9 +212,8 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
 // diagonal block of step k, with Linv the inverse of the factored block
 // stored by the factorization (unit lower for LDLt).  b_k (w x nrhs) is
 // read from `src` (leading dimension n); the result lands in X (ld SLD).
-template <int TRANS>
-__device__ void diag_block_apply(const double* Li, int w, const double* src, int64_t n, int nrhs, double* Ls,
-                                 double* Bs, double* X) {
+template <typename T, int TRANS>
+__device__ void diag_block_apply(const T* Li, int w, const T* src, int64_t n, int nrhs, T* Ls, T* Bs, T* X) {
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int i = tid; i < kNB * kNB; i += nt) {
         int r = i & (kNB - 1), c = i >> 6;
@@ -225,9 +224,10 @@ __device__ void diag_block_apply(const double* Li, int w, const double* src, int
         Bs[a + r * SLD] = src[a + (int64_t)r * n];
     }
     __syncthreads();
-    for (int i = tid; i < w * nrhs; i += nt) {
-        int a = i % w, r = i / w;
-        double acc = 0.0;
+    for (int i = tid; i < kNB * nrhs; i += nt) {
+        int a = i % kNB, r = i / kNB;
+        if (a >= w) { X[a + r * SLD] = T(0); continue; }
+        T acc = T(0);
         if (!TRANS) {
             for (int c = 0; c <= a; ++c) acc += Ls[a + c * SLD] * Bs[c + r * SLD];
         } else {
@@ -238,23 +238,24 @@ __device__ void diag_block_apply(const double* Li, int w, const double* src, int
     __syncthreads();
 }
 
-constexpr int kSolveSmem = (2 * kNB * SLD + 2 * kMaxRhs * SLD) * (int)sizeof(double);
+template <typename T>
+constexpr int solve_smem() { return (2 * kNB * SLD + 2 * kMaxRhs * SLD) * (int)sizeof(T); }
 
-template <int UNIT, int NR>
+template <typename T, int UNIT, int NR>
 __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const double* __restrict__ P,
-                                               const double* __restrict__ inv, double* __restrict__ C,
-                                               double* __restrict__ W, double* __restrict__ R, int64_t n, int nrhs) {
-    extern __shared__ double sm[];
-    double* Ls = sm;
-    double* Bs = Ls + kNB * SLD;
-    double* X = Bs + kMaxRhs * SLD;
+                                               int step, const T* __restrict__ P, const T* __restrict__ inv,
+                                               T* __restrict__ C, T* __restrict__ W, T* __restrict__ R, int64_t n,
+                                               int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* Ls = reinterpret_cast<T*>(sm_raw);
+    T* Bs = Ls + kNB * SLD;
+    T* X = Bs + kMaxRhs * SLD;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int k0 = step * kNB, w = min(kNB, nn - k0);
-    const double* Pj = P + f.poff;
-    diag_block_apply<0>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
+    const T* Pj = P + f.poff;
+    diag_block_apply<T, 0>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
     const int tid = threadIdx.x, nt = blockDim.x;
     if (it.a == 0) {
         for (int i = tid; i < w * nrhs; i += nt) {
@@ -263,53 +264,69 @@ __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts,
         }
         return;
     }
-    const int r0 = k0 + w + (it.a - 1) * kSolveRows;
-    const int r1 = min(r0 + kSolveRows, nj);
-    double* Rj = R + f.roff * nrhs;
-    for (int q = r0 + tid; q < r1; q += nt) {
-        double acc[NR];
+    const int r0 = k0 + w + (it.a - 1) * kFwdRows;
+    const int nr = min(kFwdRows, nj - r0);
+    const int rl = tid & (kFwdRows - 1), g = tid / kFwdRows;  // row, 16-column group
+    T acc[NR];
 #pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-        const double* pq = Pj + q + (int64_t)k0 * ld;
-#pragma unroll 4
-        for (int c = 0; c < w; ++c) {
-            double l = pq[(int64_t)c * ld];
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    if (rl < nr) {
+        const T* pq = Pj + (r0 + rl) + (int64_t)(k0 + g * 16) * ld;
+        T l[16];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) acc[r] += l * X[c + r * SLD];
-        }
+        for (int c = 0; c < 16; ++c) l[c] = (g * 16 + c < w) ? pq[(int64_t)c * ld] : T(0);
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] += l[c] * X[(g * 16 + c) + r * SLD];
+    }
+    T* red = Ls;  // the inverse tile is no longer needed: [g][r][row]
+#pragma unroll
+    for (int r = 0; r < NR; ++r) red[(g * NR + r) * kFwdRows + rl] = acc[r];
+    __syncthreads();
+    if (g == 0 && rl < nr) {
+        T* Rj = R + f.roff * nrhs;
+        const int q = r0 + rl;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
             if (r < nrhs) {
-                if (q < nn) W[f.col0 + q + (int64_t)r * n] -= acc[r];
-                else Rj[(q - nn) + r * na] -= acc[r];
+                T v = red[(0 * NR + r) * kFwdRows + rl] + red[(1 * NR + r) * kFwdRows + rl] +
+                      red[(2 * NR + r) * kFwdRows + rl] + red[(3 * NR + r) * kFwdRows + rl];
+                if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
+                else Rj[(q - nn) + r * na] -= v;
             }
         }
     }
 }
 
-// backward: W[res tile] = C[res tile] - L21^T x[sep].  One CTA per 64
-// columns; L rows and the gathered x[sep] are staged through shared memory
-// 64 rows at a time, so L is read once and coalesced.
-constexpr int kBwdSmem = (kNB * SLD + kNB * kMaxRhs) * (int)sizeof(double);
+// backward: W[res tile] = C[res tile] - L21^T x[sep].  Items are (front,
+// 64-column tile, chunk of kBwdRows rows of L21); each writes its partial
+// sums to part[item.pad], staging L rows and the gathered x[sep] through
+// shared memory 64 rows at a time (L read once, coalesced).  k_s_bwd_red
+// then adds the chunks of a tile in a fixed order.
+template <typename T>
+constexpr int bwd_smem() { return (kNB * SLD + kNB * kMaxRhs) * (int)sizeof(T); }
 
+template <typename T>
 __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                 const int32_t* __restrict__ septgt, const double* __restrict__ P,
-                                                 const double* __restrict__ C, double* __restrict__ W, int64_t n,
+                                                 const int32_t* __restrict__ septgt, const T* __restrict__ P,
+                                                 const T* __restrict__ C, T* __restrict__ part, int64_t n,
                                                  int nrhs) {
-    extern __shared__ double sm[];
-    double* Lt = sm;                  // [c][a] : Lt[a + c*SLD], 64 rows x 64 columns
-    double* xs = Lt + kNB * SLD;      // [r][a] : xs[a + r*kNB]
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* Lt = reinterpret_cast<T*>(sm_raw);  // [c][a] : Lt[a + c*SLD], 64 rows x 64 columns
+    T* xs = Lt + kNB * SLD;                // [r][a] : xs[a + r*kNB]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const double* Pj = P + f.poff;
+    const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
     const int c0 = it.a * kNB, wc = min(kNB, nn - c0);
+    const int a_beg = it.b * kBwdRows, a_end = min(na, a_beg + kBwdRows);
     // outputs: (column c, rhs r), at most 64 x 16 = 1024, 4 per thread
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int a0 = 0; a0 < na; a0 += kNB) {
-        const int wa = min(kNB, na - a0);
+    T acc[4] = {T(0), T(0), T(0), T(0)};
+    for (int a0 = a_beg; a0 < a_end; a0 += kNB) {
+        const int wa = min(kNB, a_end - a0);
         __syncthreads();
         for (int i = tid; i < wa * wc; i += nt) {
             int a = i % wa, c = i / wa;
@@ -325,39 +342,51 @@ __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ front
             int o = tid + u * nt;
             int c = o % kNB, r = o / kNB;
             if (c < wc && r < nrhs) {
-                double s = 0.0;
+                T s = T(0);
                 for (int a = 0; a < wa; ++a) s += Lt[a + c * SLD] * xs[a + r * kNB];
                 acc[u] += s;
             }
         }
     }
+    T* dst = part + (int64_t)it.pad * (kNB * kMaxRhs);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        int o = tid + u * nt;
-        int c = o % kNB, r = o / kNB;
-        if (c < wc && r < nrhs) {
-            int64_t idx = f.col0 + c0 + c + (int64_t)r * n;
-            W[idx] = C[idx] - acc[u];
-        }
+    for (int u = 0; u < 4; ++u) dst[tid + u * nt] = acc[u];
+}
+
+// W[res tile] = C[res tile] - sum over the tile's chunks (in order)
+template <typename T>
+__global__ void __launch_bounds__(256) k_s_bwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                   const T* __restrict__ part, const T* __restrict__ C,
+                                                   T* __restrict__ W, int64_t n, int nrhs) {
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int c0 = it.a * kNB, wc = min(kNB, f.nn - c0);
+    const int nchunk = (f.na + kBwdRows - 1) / kBwdRows;
+    for (int o = threadIdx.x; o < kNB * kMaxRhs; o += blockDim.x) {
+        const int c = o % kNB, r = o / kNB;
+        if (c >= wc || r >= nrhs) continue;
+        T s = T(0);
+        for (int q = 0; q < nchunk; ++q) s += part[(int64_t)(it.b + q) * (kNB * kMaxRhs) + o];
+        const int64_t idx = f.col0 + c0 + c + (int64_t)r * n;
+        W[idx] = C[idx] - s;
     }
 }
 
-template <int UNIT>
+template <typename T, int UNIT>
 __global__ void __launch_bounds__(256) k_s_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const double* __restrict__ P,
-                                               const double* __restrict__ inv, double* __restrict__ C,
-                                               double* __restrict__ W, int64_t n, int nrhs) {
-    extern __shared__ double sm[];
-    double* Ls = sm;
-    double* Bs = Ls + kNB * SLD;
-    double* X = Bs + kMaxRhs * SLD;
-    double* Dt = X + kMaxRhs * SLD;   // aliases nothing: kSolveSmem covers Ls, Bs, X and Dt (64 x SLD)
+                                               int step, const T* __restrict__ P, const T* __restrict__ inv,
+                                               T* __restrict__ C, T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* Ls = reinterpret_cast<T*>(sm_raw);
+    T* Bs = Ls + kNB * SLD;
+    T* X = Bs + kMaxRhs * SLD;
+    T* Dt = X + kMaxRhs * SLD;  // solve_smem<T>() covers Ls, Bs, X and Dt (64 x SLD)
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int k0 = step * kNB, w = min(kNB, nn - k0);
-    const double* Pj = P + f.poff;
-    diag_block_apply<1>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
+    const T* Pj = P + f.poff;
+    diag_block_apply<T, 1>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
     const int tid = threadIdx.x, nt = blockDim.x;
     if (it.a == 0) {
         for (int i = tid; i < w * nrhs; i += nt) {
@@ -375,7 +404,7 @@ __global__ void __launch_bounds__(256) k_s_bwd(const Front* __restrict__ fronts,
     __syncthreads();
     for (int o = tid; o < wc * nrhs; o += nt) {
         int c = o % wc, r = o / wc;
-        double s = 0.0;
+        T s = T(0);
         for (int a = 0; a < w; ++a) s += Dt[a + c * SLD] * X[a + r * SLD];
         W[f.col0 + c0 + c + (int64_t)r * n] -= s;
     }
@@ -406,47 +435,62 @@ int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm
     return 0;
 }
 
-template <int UNIT>
-static int solve_impl(mf_handle* h, int nrhs) {
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSolveSmem));
-    MF_CUDA(cudaFuncSetAttribute(k_s_bwd<UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kSolveSmem + kNB * SLD * (int)sizeof(double)));
-    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l, cudaFuncAttributeMaxDynamicSharedMemorySize, kBwdSmem));
+int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst) {
+    Timer t(h, K_PERM);
+    k_perm<true><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(dst, const_cast<double*>(B), perm, h->n, ldb,
+                                                                         (int)nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src) {
+    Timer t(h, K_PERM);
+    k_perm<false><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(const_cast<double*>(src), B, perm, h->n,
+                                                                          ldb, (int)nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename T, int UNIT>
+static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
+    constexpr int ss = solve_smem<T>();
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd<T, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T>()));
     const Item* items = h->d_items;
     const int64_t n = h->n;
     // forward: levels ascending
     for (const Level& lv : h->levels) {
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
-            k_s_small_fwd<UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
-                h->d_fronts, items + lv.s_small.off, h->d_reltgt, h->d_chdtgt, h->d_P, h->d_C, h->d_R, n, nrhs);
+            k_s_small_fwd<T, UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
+                h->d_fronts, items + lv.s_small.off, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.s_gather.cnt) {
             Timer t(h, K_S_GATHER);
-            k_s_gather<<<(unsigned)lv.s_gather.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_gather.off,
-                                                                         h->d_reltgt, h->d_chdtgt, h->d_C, h->d_W,
-                                                                         h->d_R, n, nrhs);
+            k_s_gather<T><<<(unsigned)lv.s_gather.cnt, 256, 0, h->stream>>>(
+                h->d_fronts, items + lv.s_gather.off, h->d_reltgt, h->d_chdtgt, sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         for (size_t k = 0; k < lv.s_steps.size(); ++k) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.fwd.cnt) continue;
             Timer t(h, K_S_FWD);
-            auto* kern = nrhs <= 1 ? k_s_fwd<UNIT, 1> : nrhs <= 2 ? k_s_fwd<UNIT, 2> : nrhs <= 4 ? k_s_fwd<UNIT, 4>
-                       : nrhs <= 8 ? k_s_fwd<UNIT, 8> : k_s_fwd<UNIT, 16>;
-            kern<<<(unsigned)st.fwd.cnt, 256, kSolveSmem, h->stream>>>(
-                h->d_fronts, items + st.fwd.off, (int)k, h->d_P, h->d_inv, h->d_C, h->d_W, h->d_R, n, nrhs);
+            auto* kern = nrhs <= 1 ? k_s_fwd<T, UNIT, 1> : nrhs <= 2 ? k_s_fwd<T, UNIT, 2>
+                       : nrhs <= 4 ? k_s_fwd<T, UNIT, 4> : nrhs <= 8 ? k_s_fwd<T, UNIT, 8> : k_s_fwd<T, UNIT, 16>;
+            kern<<<(unsigned)st.fwd.cnt, 256, ss, h->stream>>>(h->d_fronts, items + st.fwd.off, (int)k, sb.P, sb.inv,
+                                                               sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
     }
     if (UNIT) {
         Timer t(h, K_OTHER);
-        k_diag_div<<<grid_stride_blocks(n * nrhs), 256, 0, h->stream>>>(h->d_C, h->d_d, n, nrhs);
+        k_diag_div<T><<<grid_stride_blocks(n * nrhs), 256, 0, h->stream>>>(sb.C, sb.d, n, nrhs);
         MF_CUDA(cudaGetLastError());
     }
     // backward: levels descending
@@ -454,22 +498,25 @@ static int solve_impl(mf_handle* h, int nrhs) {
         const Level& lv = h->levels[L];
         if (lv.s_bwd_l.cnt) {
             Timer t(h, K_S_BWD_L);
-            k_s_bwd_l<<<(unsigned)lv.s_bwd_l.cnt, 256, kBwdSmem, h->stream>>>(
-                h->d_fronts, items + lv.s_bwd_l.off, h->d_septgt, h->d_P, h->d_C, h->d_W, n, nrhs);
+            k_s_bwd_l<T><<<(unsigned)lv.s_bwd_l.cnt, 256, bwd_smem<T>(), h->stream>>>(
+                h->d_fronts, items + lv.s_bwd_l.off, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+            k_s_bwd_red<T><<<(unsigned)lv.s_bwd_red.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_bwd_red.off,
+                                                                              sb.part, sb.C, sb.W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         for (size_t k = lv.s_steps.size(); k-- > 0;) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.bwd.cnt) continue;
             Timer t(h, K_S_BWD);
-            k_s_bwd<UNIT><<<(unsigned)st.bwd.cnt, 256, kSolveSmem + kNB * SLD * (int)sizeof(double), h->stream>>>(
-                h->d_fronts, items + st.bwd.off, (int)k, h->d_P, h->d_inv, h->d_C, h->d_W, n, nrhs);
+            k_s_bwd<T, UNIT><<<(unsigned)st.bwd.cnt, 256, ss, h->stream>>>(h->d_fronts, items + st.bwd.off, (int)k,
+                                                                          sb.P, sb.inv, sb.C, sb.W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
-            k_s_small_bwd<UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
-                h->d_fronts, items + lv.s_small.off, h->d_septgt, h->d_P, h->d_C, n, nrhs);
+            k_s_small_bwd<T, UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
+                h->d_fronts, items + lv.s_small.off, h->d_septgt, sb.P, sb.C, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
     }
@@ -480,7 +527,16 @@ static int solve_impl(mf_handle* h, int nrhs) {
 int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
-    return h->diag ? solve_impl<1>(h, (int)nrhs) : solve_impl<0>(h, (int)nrhs);
+    SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, h->d_R, h->d_W, h->d_C, h->d_part};
+    return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
+}
+
+// Same on the single-precision factor: f32.C (n x nrhs, elimination order) in place.
+int launch_solve_mixed(mf_handle* h, int64_t nrhs) {
+    if (nrhs <= 0) return 0;
+    if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
+    SolveBufs<float> sb{h->f32.P, h->f32.inv, h->f32.d, h->f32.R, h->f32.W, h->f32.C, h->f32.part};
+    return h->diag ? solve_impl<float, 1>(h, sb, (int)nrhs) : solve_impl<float, 0>(h, sb, (int)nrhs);
 }
 
 }  // namespace mf

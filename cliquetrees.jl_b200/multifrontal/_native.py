@@ -97,6 +97,18 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_profile.restype = ctypes.c_int
         lib.mf_kernel_times.argtypes = [_vp, _pd, _p64]
         lib.mf_kernel_times.restype = ctypes.c_int
+        pint = ctypes.POINTER(ctypes.c_int)
+        lib.mf_enable_mixed.argtypes = [_vp]
+        lib.mf_enable_mixed.restype = ctypes.c_int
+        lib.mf_factorize_mixed.argtypes = [_vp, _pd, _p64, pint]
+        lib.mf_factorize_mixed.restype = ctypes.c_int
+        lib.mf_solve_refined.argtypes = [_vp, _pd, _i64, _i64, _p64, ctypes.c_double, ctypes.c_int, pint, _pd]
+        lib.mf_solve_refined.restype = ctypes.c_int
+        lib.mf_solve_refined_device.argtypes = [_vp, _vp, _i64, _i64, _vp, ctypes.c_double, ctypes.c_int, pint,
+                                                _pd]
+        lib.mf_solve_refined_device.restype = ctypes.c_int
+        lib.mf_get_factor_mixed.argtypes = [_vp, _pd, _pd, _pd, _pd]
+        lib.mf_get_factor_mixed.restype = ctypes.c_int
         lib.mf_exec_sizes.argtypes = [_vp, _p64, _p64]
         lib.mf_exec_sizes.restype = ctypes.c_int
         lib.mf_plan_info.argtypes = [_i64, _i64] + [_p64] * 8 + [ctypes.c_int, _p64]

@@ -77,7 +77,10 @@ class ChordalFactorization:
     DIAG = 0
 
     def __init__(self, A, P: Permutation | None = None, S: ChordalSymbolic | None = None, *, alg="amf",
-                 device: int = 0, nrhs_cap: int = 16):
+                 device: int = 0, nrhs_cap: int = 16, mixed: bool = False, tol: float = 1e-12, maxit: int = 100):
+        """``mixed=True`` selects the mixed-precision form: FP32 fronts on the
+        GPU, FP64 refinement in ``ldiv`` to backward error ``tol`` (the
+        reference has no such mode; see the module docstring)."""
         if (P is None) != (S is None):
             raise ValueError("pass both P and S or neither")
         if P is None:
@@ -85,6 +88,11 @@ class ChordalFactorization:
         self.P = P
         self.S = S
         self.info = 0
+        self.mixed = mixed
+        self.tol = tol
+        self.maxit = maxit
+        self.used_fp64 = False
+        self.last_refinement = None
         self._factored = False
         self._handle = _Handle(S, self.DIAG, nrhs_cap, device)
         self._slot_for = None
@@ -114,6 +122,8 @@ class ChordalFactorization:
             slot = np.ascontiguousarray(slot, dtype=np.int64)
             check(lib.mf_set_assembly(self._handle.h, slot.size, ptr64(slot)), "mf_set_assembly")
             self._slot_for = key
+            if self.mixed:
+                check(lib.mf_enable_mixed(self._handle.h), "mf_enable_mixed")
         vals = np.ascontiguousarray(Lo.data, dtype=np.float64)
         check(lib.mf_assemble(self._handle.h, ptrd(vals)), "mf_assemble")
         self._factored = False
@@ -137,6 +147,17 @@ class ChordalFactorization:
                                              ptrd(d) if self.DIAG else None), "mf_get_factor")
         return Dval, Lval, d
 
+    def factor_arrays_mixed(self):
+        """(Dval, Lval, d, scale) of the single-precision factor of S A S
+        (mixed form only)."""
+        Dval = np.empty(self.S.ndz, np.float64)
+        Lval = np.empty(self.S.nlz, np.float64)
+        d = np.ones(self.S.n, np.float64)
+        sc = np.empty(self.S.n, np.float64)
+        check(self._handle.lib.mf_get_factor_mixed(self._handle.h, ptrd(Dval), ptrd(Lval),
+                                                   ptrd(d) if self.DIAG else None, ptrd(sc)), "mf_get_factor_mixed")
+        return Dval, Lval, d, sc
+
     @property
     def Dval(self):
         return self.factor_arrays()[0]
@@ -156,7 +177,13 @@ class ChordalFactorization:
             # permuteto(T, signs, F.perm) (cholesky.jl:242)
             sg = np.ascontiguousarray(np.asarray(signs, dtype=np.float64)[self.P.perm])
         info = ctypes.c_int64(0)
-        check(self._handle.lib.mf_factorize(self._handle.h, ptrd(sg), ctypes.byref(info)), "mf_factorize")
+        if self.mixed:
+            fp64 = ctypes.c_int(0)
+            check(self._handle.lib.mf_factorize_mixed(self._handle.h, ptrd(sg), ctypes.byref(info), ctypes.byref(fp64)),
+                  "mf_factorize_mixed")
+            self.used_fp64 = bool(fp64.value)
+        else:
+            check(self._handle.lib.mf_factorize(self._handle.h, ptrd(sg), ctypes.byref(info)), "mf_factorize")
         k = int(info.value)
         # factorize! level 1: local info -> perm[info] (cholesky.jl:250-254)
         self.info = 0 if k == 0 else int(self.P.perm[k - 1]) + 1
@@ -235,7 +262,14 @@ def ldiv(F: ChordalFactorization, B):
     X = np.asfortranarray(B.reshape(-1, 1) if vec else B).copy(order="F")
     if X.shape[0] != F.n:
         raise ValueError("dimension mismatch")
-    check(F._handle.lib.mf_solve(F._handle.h, ptrd(X), X.shape[1], F.n, ptr64(F.P.perm)), "mf_solve")
+    if F.mixed:
+        it = ctypes.c_int(0)
+        eta = ctypes.c_double(0.0)
+        check(F._handle.lib.mf_solve_refined(F._handle.h, ptrd(X), X.shape[1], F.n, ptr64(F.P.perm), F.tol, F.maxit,
+                                             ctypes.byref(it), ctypes.byref(eta)), "mf_solve_refined")
+        F.last_refinement = (int(it.value), float(eta.value))
+    else:
+        check(F._handle.lib.mf_solve(F._handle.h, ptrd(X), X.shape[1], F.n, ptr64(F.P.perm)), "mf_solve")
     return X[:, 0].copy() if vec else X
 
 

@@ -99,6 +99,31 @@ int mf_solve(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* 
 /* Same with device pointers (B_dev n x nrhs, leading dimension ldb). */
 int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev);
 
+/* ---- mixed precision (FP32 fronts, FP64 refinement) -------------------- */
+
+/* Allocate the single-precision factor and the refinement workspace (after
+ * mf_set_assembly).  From then on mf_assemble only stages the values. */
+int mf_enable_mixed(mf_handle* h);
+
+/* Scale A symmetrically by diag(|a_ii|)^-1/2, factor it in FP32 (same plan,
+ * single-precision kernels) and compute ||A||_inf.  If FP32 rejects a pivot
+ * the matrix is refactored in FP64 and *used_fp64 = 1; info then follows
+ * the FP64 factorization (the reference's convention). */
+int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* used_fp64);
+
+/* x = A^-1 b to normwise backward error <= tol: preconditioned conjugate
+ * gradients (Cholesky) or iterative refinement (LDLt) in FP64 with the FP32
+ * factor as preconditioner; B (n x nrhs, ORIGINAL order) is overwritten
+ * with x.  *iters and *eta report the worst right-hand side. */
+int mf_solve_refined(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm, double tol, int maxit,
+                     int* iters, double* eta);
+int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev,
+                            double tol, int maxit, int* iters, double* eta);
+
+/* The single-precision factor of the scaled matrix S A S (reference layout,
+ * widened to double) and the scaling S (elimination order). */
+int mf_get_factor_mixed(mf_handle* h, double* Dval, double* Lval, double* d, double* scale);
+
 /* Copy the device factor out in the reference layout (any pointer may be NULL). */
 int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d);
 
@@ -123,9 +148,10 @@ int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* s
 
 /* Optional per-kernel timing (CUDA events around every launch, stream
  * synchronised after each: for profiling passes only).  mf_kernel_times
- * fills ms[13] and launches[13] in the order: assemble, small, extend-add,
- * panel, update, syrk, solve-small, solve-gather, solve-fwd, solve-bwd-l,
- * solve-bwd, permute, other. */
+ * fills ms[16] and launches[16] in the order: assemble, small, extend-add,
+ * panel TRSM, trailing update, syrk, solve-small, solve-gather, solve-fwd,
+ * solve-bwd-l, solve-bwd, permute, other, diagonal blocks, left update,
+ * residual. */
 int mf_profile(mf_handle* h, int enable);
 int mf_kernel_times(const mf_handle* h, double* ms, int64_t* launches);
 

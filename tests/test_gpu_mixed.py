@@ -1,0 +1,110 @@
+"""Mixed-precision form on the GPU: FP32 fronts (same plan, single-precision
+kernels) with FP64 refinement, checked against the FP64 oracle.
+
+Bar: normwise backward error <= 1e-12 (the north star's mixed target) and
+the solution within 1e-9 relative of the oracle's or 4 kappa_1 eps."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import multifrontal as mf
+from multifrontal import testmatrices as tm
+from oracle import oracle
+
+from test_gpu_parity import cond1
+
+pytestmark = pytest.mark.gpu
+
+
+def check(A, P, S, F, B, diag):
+    X = mf.ldiv(F, B)
+    it, eta_dev = F.last_refinement
+    eta = tm.backward_error(A, X, B).max()
+    assert eta <= 1e-12, (eta, it)
+    assert abs(eta - eta_dev) <= 1e-3 * max(eta, 1e-300) + 1e-16  # device estimate matches
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, diag)
+    rel = np.abs(X - Xo).max() / np.abs(Xo).max()
+    if rel > 1e-9:
+        assert rel <= 4 * cond1(A, P, S, diag) * np.finfo(float).eps, rel
+    return it
+
+
+@pytest.mark.parametrize("case", ["grid2d", "grid3d_contrast", "grid3d_large"])
+def test_mixed_cholesky(case):
+    if case == "grid2d":
+        A = tm.grid_laplacian(60, 50, seed=11)
+        order = mf.grid_nd_order(60, 50, 1)
+    elif case == "grid3d_contrast":
+        A = tm.grid_laplacian(18, 17, 16, seed=12, lo=1e-3, hi=1e3, shift=1e-6)
+        order = mf.grid_nd_order(18, 17, 16)
+    else:
+        A = tm.grid_laplacian(30, 30, 30, seed=14, lo=1e-3, hi=1e3, shift=1e-6)
+        order = mf.grid_nd_order(30, 30, 30)
+    P, S = mf.symbolic(A, alg=order)
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
+    assert F.info == 0
+    for k in (1, 4, 16, 19):
+        it = check(A, P, S, F, tm.rhs(S.n, k, seed=k), 0)
+        assert it <= 100
+
+
+def test_mixed_ldlt_quasidefinite():
+    K = tm.config4(side=7, m=120, per_row=6, seed=5)
+    P, S = mf.symbolic(K, alg="natural")
+    F = mf.ldlt_(mf.ChordalLDLt(K, P, S, mixed=True))
+    assert F.info == 0
+    check(K, P, S, F, tm.rhs(S.n, 8, seed=4), 1)
+
+
+def test_mixed_value_refresh():
+    A = tm.grid_laplacian(25, 24, 3, seed=31)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(25, 24, 3))
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
+    A2 = tm.grid_laplacian(25, 24, 3, seed=32)
+    F.copyto(A2)
+    mf.cholesky_(F)
+    check(A2, P, S, F, tm.rhs(S.n, 3, seed=2), 0)
+
+
+def test_mixed_not_positive_definite_reports_info():
+    A = tm.grid_laplacian(30, 30, seed=3).tolil()
+    A[417, 417] = -5.0
+    A = A.tocsc()
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(30, 30, 1))
+    F = mf.ChordalCholesky(A, P, S, mixed=True)
+    with pytest.raises(mf.PosDefException):
+        mf.cholesky_(F)
+    assert F.used_fp64  # FP32 rejected a pivot; the FP64 factorization decided
+
+
+@pytest.mark.parametrize("tensor_cores", ["1", "0"])
+def test_single_precision_factor_matches_scaled_oracle(tensor_cores, monkeypatch):
+    """The FP32 factor (tcgen05 3xTF32 GEMMs, or FFMA with MF_TENSOR_CORES=0)
+    of S A S agrees with the FP64 oracle factor of S A S to FP32 accuracy."""
+    monkeypatch.setenv("MF_TENSOR_CORES", tensor_cores)
+    import scipy.sparse as sp
+    from test_gpu_parity import lower_mask
+    A = tm.grid_laplacian(26, 25, 24, seed=61)  # fronts up to nj ~ 1100: all tensor-core roles run
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(26, 25, 24))
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
+    assert not F.used_fp64
+    Dg, Lg, _, sc = F.factor_arrays_mixed()
+    s_orig = np.empty(S.n)
+    s_orig[P.perm] = sc                      # scaling in original order
+    As = sp.tril(sp.diags(s_orig) @ A @ sp.diags(s_orig)).tocsc()  # lower triangle: exact symmetry
+    info, (Dw, Lw, _) = oracle_factor_scaled(As, P, S)
+    m = lower_mask(S)
+    scale = max(np.abs(Dw[m]).max(), np.abs(Lw).max())
+    assert np.abs(Dg[m] - Dw[m]).max() <= 2e-4 * scale
+    assert np.abs(Lg - Lw).max() <= 2e-4 * scale
+    B = tm.rhs(S.n, 4, seed=9)
+    mf.ldiv(F, B)
+    it, eta = F.last_refinement
+    assert eta <= 1e-12 and it <= 8, (it, eta)
+
+
+def oracle_factor_scaled(As, P, S):
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, As)
+    info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0)
+    assert info == 0
+    return info, (Dval, Lval, d)
