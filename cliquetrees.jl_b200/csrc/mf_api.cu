@@ -175,6 +175,11 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
     if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    if (e == cudaSuccess && n) {  // the permutation a NULL perm argument stands for, until one is passed
+        std::vector<int64_t> iota((size_t)n);
+        for (int64_t i = 0; i < n; ++i) iota[(size_t)i] = i;
+        e = up(h->d_perm, iota.data(), sizeof(int64_t) * (size_t)n);
+    }
     {
         const char* tcenv = getenv("MF_TENSOR_CORES");
         h->use_tc = !(tcenv && tcenv[0] == '0');

@@ -93,7 +93,9 @@ int mf_factorize(mf_handle* h, const double* signs, int64_t* info);
 /* x = A^{-1} b with the permutation applied on the device, host buffers:
  * B (n x nrhs, leading dimension ldb, ORIGINAL order) is overwritten with
  * the solution; perm (length n) is the elimination order (perm[i] = original
- * vertex at position i).  Replaces ldiv!!(C, F, B), divide.jl:1762-1764. */
+ * vertex at position i).  Replaces ldiv!!(C, F, B), divide.jl:1762-1764.
+ * perm NULL reuses the permutation last passed to this handle (the identity
+ * before any). */
 int mf_solve(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm);
 
 /* Same with device pointers (B_dev n x nrhs, leading dimension ldb). */
