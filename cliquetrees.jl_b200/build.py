@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "multifrontal")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-GPU_SOURCES = ["mf_plan.cu", "mf_factor.cu", "mf_tc.cu", "mf_solve.cu", "mf_refine.cu", "mf_api.cu"]
+GPU_SOURCES = ["mf_plan.cu", "mf_factor.cu", "mf_tc.cu", "mf_solve.cu", "mf_refine.cu", "mf_api.cu", "mf_static.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -254,6 +254,9 @@ int launch_panel_to_dl(mf_handle* h, double* dDval, double* dLval);
 int launch_panel32_to_dl(mf_handle* h, double* dDval, double* dLval);
 int launch_assemble(mf_handle* h, const double* dnz);
 int launch_solve(mf_handle* h, int64_t nrhs);
+// the FP64 solve with caller-provided work buffers in place of the handle's
+// (R: nrval_per_rhs*nrhs, W and C: n*nrhs, part: nbwd_part*64*16 doubles)
+int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* C, double* part);
 int launch_solve_mixed(mf_handle* h, int64_t nrhs);
 int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst);
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);

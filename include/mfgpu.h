@@ -159,6 +159,27 @@ int mf_kernel_times(const mf_handle* h, double* ms, int64_t* launches);
 
 const char* mf_last_error(void);
 
+/* ---- solve without device allocation ----------------------------------- */
+
+/* mf_solve_device with its work buffers taken from one fixed 32 MiB device
+ * region (a file-scope __device__ array) instead of the handle's: the call
+ * allocates no device memory.  For callers that must not reach the device
+ * allocator while solving, e.g. a serving loop whose device memory is already
+ * fully committed under an admission cap, or one that keeps the handle's own
+ * solve buffers busy on another stream.  No reference counterpart.
+ *
+ * A chunk of c = min(nrhs, 16) right-hand sides needs 2*n*c + R*c + 1024*P
+ * doubles (R, P fixed by the plan; each part rounded up to 256 bytes); a solve
+ * that needs more than 4,194,304 doubles returns -1 with the sizes in
+ * mf_last_error() and does nothing.  Nothing in the region has to start at
+ * zero.  The first call on a device looks up the region's address
+ * (cudaGetSymbolAddress, which loads the module holding it); make that first
+ * call before any stream capture.  There is one region per device shared by
+ * every handle: two calls whose work overlaps on the device race and corrupt
+ * each other's results, so serialise them (same stream, or an event between).
+ * Work runs on the handle's stream and is not synchronised. */
+int mf_solve_device_static(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev);
+
 #ifdef __cplusplus
 }
 #endif
