@@ -49,7 +49,7 @@ void free_all(mf_handle* h) {
                     h->d_nz,     h->d_inv,    h->d_nzrow,  h->d_nzcol,  h->d_dslot,    h->d_scale,
                     h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
-                    h->d_part,   h->f32.part};
+                    h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);

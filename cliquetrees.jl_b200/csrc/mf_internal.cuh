@@ -70,6 +70,7 @@ constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns stay kTile
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
 constexpr int kSolveRows = 256; // rows per gather work item
+constexpr int kTcSyrkN = 128;   // tile columns of the tensor-core SYRK
 constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
 
@@ -190,6 +191,8 @@ struct mf_handle {
     long long* d_info = nullptr;   // first failing column (1-based), LLONG_MAX if none
     int* d_err = nullptr;          // set by a kernel whose bounded wait timed out
     bool use_tc = true;            // tcgen05 tensor cores for the FP32 GEMMs
+    void* d_tmaps = nullptr;       // CUtensorMap per execution front (FP32 panels)
+    void* d_tmap_inv = nullptr;    // CUtensorMap over the FP32 diagonal-block inverses
     double* d_R = nullptr;         // solve updates (sum na * nrhs_cap)
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
     double* d_part = nullptr;      // backward partial sums

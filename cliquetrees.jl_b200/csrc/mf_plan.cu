@@ -402,8 +402,9 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 for (int32_t j : fr) {
                     const Front& f = h->h_fronts[j];
                     if (f.nn + f.na <= kSmallMax || f.nn <= c0) continue;
-                    int w = std::min(kNB, f.nn - c0);
-                    for (int t = 0; t < (int)cdiv(f.nn + f.na - c0 - w, kTM); ++t) push(j, t, 0);
+                    // rows from the 4-aligned row at or before the first one below the block
+                    const int r0 = (c0 + std::min(kNB, f.nn - c0)) & ~3;
+                    for (int t = 0; t < (int)cdiv(f.nn + f.na - r0, kTM); ++t) push(j, t, 0);
                 }
                 end(st.panel_tc);
                 begin(st.trail_tc);
@@ -438,10 +439,12 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (f.nn + f.na <= kSmallMax || f.na == 0) continue;
-            int tc = (int)cdiv(f.na, kTile);
-            for (int tj = 0; tj < tc; ++tj)
-                // 128-row tiles starting at the diagonal column block: rows cs + 128 ti
-                for (int ti = 0; ti < (int)cdiv(f.na - tj * kTile, kTM); ++ti) push(j, ti, tj);
+            // tiles start at the 4-aligned panel row nn & ~3, delta rows before L21
+            const int delta = f.nn & 3;
+            const int tcn = (int)cdiv(f.na + delta, kTcSyrkN);
+            for (int tj = 0; tj < tcn; ++tj)
+                // 128-row tiles from the diagonal: L21 rows tj * N - delta + 128 ti
+                for (int ti = 0; ti < (int)cdiv(f.na + delta - tj * kTcSyrkN, kTM); ++ti) push(j, ti, tj);
         }
         end(lv.syrk_tc);
 
