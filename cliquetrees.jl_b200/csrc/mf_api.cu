@@ -49,7 +49,9 @@ void free_all(mf_handle* h) {
                     h->d_nz,     h->d_inv,    h->d_nzrow,  h->d_nzcol,  h->d_dslot,    h->d_scale,
                     h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
-                    h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv};
+                    h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
+                    h->d_segeta};
+    release_graphs(h);
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -111,6 +113,10 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     mf_handle* h = new (std::nothrow) mf_handle();
     if (!h) { set_error("out of host memory"); return -4; }
     h->device = device;
+    if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        h->num_sms = 148;
+    }
     h->diag = diag;
     h->n = n;
     h->nfr = nfr;
@@ -183,6 +189,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     {
         const char* tcenv = getenv("MF_TENSOR_CORES");
         h->use_tc = !(tcenv && tcenv[0] == '0');
+        const char* genv = getenv("MF_GRAPHS");
+        h->use_graphs = !(genv && genv[0] == '0');
     }
     if (e != cudaSuccess) {
         cuda_fail(e, "mf_create upload");
@@ -641,6 +649,43 @@ int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t l
     if (!h->mixed) { set_error("mf_solve_refined_device: call mf_enable_mixed first"); return -1; }
     DeviceGuard g(h->device);
     return refined_chunks(h, nullptr, B_dev, nrhs, ldb, perm_dev ? perm_dev : h->d_perm, tol, maxit, iters, eta);
+}
+
+int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
+    if (!h || nseg < 0 || (nseg > 0 && !segptr)) { set_error("mf_set_segments: bad arguments"); return -1; }
+    if (nseg > 0) {
+        if (segptr[0] != 0 || segptr[nseg] != h->n) {
+            set_error("mf_set_segments: segments must start at row 0 and end at row n");
+            return -1;
+        }
+        for (int64_t s = 0; s < nseg; ++s)
+            if (segptr[s + 1] < segptr[s]) { set_error("mf_set_segments: boundaries must not decrease"); return -1; }
+    }
+    DeviceGuard g(h->device);
+    for (void* p : {(void*)h->d_segptr, (void*)h->d_segred, (void*)h->d_segeta})
+        if (p) cudaFree(p);
+    h->d_segptr = nullptr; h->d_segred = nullptr; h->d_segeta = nullptr;
+    h->nseg = 0;
+    if (nseg == 0) return 0;
+    int64_t tot = 0;
+    int rc = dalloc(h, &h->d_segptr, nseg + 1, &tot);
+    if (!rc) rc = dalloc(h, &h->d_segred, nseg * kSegRed, &tot);
+    if (!rc) rc = dalloc(h, &h->d_segeta, nseg, &tot);
+    if (rc) return rc;
+    MF_CUDA(cudaMemcpy(h->d_segptr, segptr, sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice));
+    MF_CUDA(cudaMemset(h->d_segeta, 0, sizeof(double) * nseg));
+    h->bytes += tot;
+    h->nseg = nseg;
+    return 0;
+}
+
+int mf_segment_errors(mf_handle* h, double* eta) {
+    if (!h || (h->nseg > 0 && !eta)) { set_error("mf_segment_errors: bad arguments"); return -1; }
+    if (h->nseg == 0) return 0;
+    DeviceGuard g(h->device);
+    MF_CUDA(cudaMemcpyAsync(eta, h->d_segeta, sizeof(double) * h->nseg, cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
 }
 
 int mf_get_factor_mixed(mf_handle* h, double* Dval, double* Lval, double* d, double* scale) {

@@ -252,122 +252,20 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 // ---------------------------------------------------------------------------
 // diagonal block: factor + inverse
 // ---------------------------------------------------------------------------
-constexpr int LDS = kNB + 4;  // shared-memory leading dimension (bank spread for fragment loads)
 
-// Blocked factorization of a 64 x 64 diagonal block held in shared memory
-// (lower, ld LDS; columns >= w are padded with the identity).  Four 16-wide
-// steps: warp 0 factors the 16 x 16 diagonal sub-block with warp
-// synchronisation only, then all threads solve the rows below it and apply
-// the rank-16 update to the trailing block.  piv[k] receives sqrt(pivot)
-// (Cholesky) or the pivot (LDLt).  Returns the first rejected local column
-// (< w) or -1; called by all threads.
-template <typename T, int LDLT>
-__device__ int factor_diag64(T* Dk, T* piv, int w, const double* signs, int64_t col0, int* flag) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int p = 0; p < 4; ++p) {
-        const int pb = p * 16;
-        if (warp == 0) {
-            int bad = -1;
-            for (int k = 0; k < 16; ++k) {
-                const int c = pb + k;
-                const T pv = Dk[c + c * LDS];
-                if (c < w) {
-                    const double sg = pivot_sign(signs, LDLT, col0 + c);
-                    if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) { bad = c; break; }
-                }
-                const T dk = LDLT ? pv : sqrt(pv);
-                const T inv = T(1) / dk;
-                __syncwarp();
-                if (lane > k && lane < 16) Dk[(pb + lane) + c * LDS] *= inv;
-                if (lane == 0) {
-                    piv[c] = dk;
-                    if (!LDLT) Dk[c + c * LDS] = dk;
-                }
-                __syncwarp();
-                for (int e = lane; e < 256; e += 32) {
-                    const int i = e & 15, j = e >> 4;
-                    if (j > k && i >= j) {
-                        T lj = Dk[(pb + j) + c * LDS];
-                        if (LDLT) lj *= pv;
-                        Dk[(pb + i) + (pb + j) * LDS] -= Dk[(pb + i) + c * LDS] * lj;
-                    }
-                }
-                __syncwarp();
-            }
-            if (lane == 0) *flag = bad;
-        }
-        __syncthreads();
-        if (*flag >= 0) return *flag;
-        for (int r = pb + 16 + tid; r < 64; r += nt) {
-            for (int c = 0; c < 16; ++c) {
-                T v = Dk[r + (pb + c) * LDS];
-                for (int q = 0; q < c; ++q) v -= Dk[r + (pb + q) * LDS] * Dk[(pb + c) + (pb + q) * LDS];
-                if (!LDLT) v /= piv[pb + c];
-                Dk[r + (pb + c) * LDS] = v;
-            }
-            if (LDLT)
-                for (int c = 0; c < 16; ++c) Dk[r + (pb + c) * LDS] /= piv[pb + c];
-        }
-        __syncthreads();
-        const int m = 64 - pb - 16;
-        for (int e = tid; e < m * m; e += nt) {
-            const int i = pb + 16 + e % m, j = pb + 16 + e / m;
-            if (i >= j) {
-                T acc = T(0);
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    T lj = Dk[j + (pb + q) * LDS];
-                    if (LDLT) lj *= piv[pb + q];
-                    acc += Dk[i + (pb + q) * LDS] * lj;
-                }
-                Dk[i + j * LDS] -= acc;
-            }
-        }
-        __syncthreads();
-    }
-    return -1;
-}
-
-// Inverse X (ld 64) of the factored 64 x 64 lower block (unit diagonal for
-// LDLt) in 16 x 16 blocks: the four diagonal blocks by one warp each, then
-// X_ij = -X_ii (sum_{k=j}^{i-1} L_ik X_kj) along the block sub-diagonals.
-template <typename T, int LDLT>
-__device__ void invert_lower64(const T* Dk, T* X, T* Tm) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < kNB * kNB; i += nt) X[i] = T(0);
-    __syncthreads();
-    if (warp < 4 && lane < 16) {
-        const int b = warp * 16, j = lane;
-        const T* L = Dk + b + b * LDS;
-        T* Xb = X + b + b * kNB;
-        Xb[j + j * kNB] = LDLT ? T(1) : T(1) / L[j + j * LDS];
-        for (int i = j + 1; i < 16; ++i) {
-            T acc = T(0);
-            for (int k = j; k < i; ++k) acc += L[i + k * LDS] * Xb[k + j * kNB];
-            Xb[i + j * kNB] = LDLT ? -acc : -acc / L[i + i * LDS];
-        }
-    }
-    __syncthreads();
-    for (int dist = 1; dist < 4; ++dist) {
-        const int nb = 4 - dist;
-        for (int e = tid; e < nb * 256; e += nt) {
-            const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
-            const int ib = (blk + dist) * 16, jb = blk * 16;
-            T acc = T(0);
-            for (int k = jb; k < ib; ++k) acc += Dk[(ib + r) + k * LDS] * X[k + (jb + c) * kNB];
-            Tm[e] = acc;
-        }
-        __syncthreads();
-        for (int e = tid; e < nb * 256; e += nt) {
-            const int blk = e >> 8, r = (e >> 4) & 15, c = e & 15;
-            const int ib = (blk + dist) * 16, jb = blk * 16;
-            T acc = T(0);
-            for (int k = 0; k <= r; ++k) acc += X[(ib + r) + (ib + k) * kNB] * Tm[(blk << 8) + (k << 4) + c];
-            X[(ib + r) + (jb + c) * kNB] = -acc;
-        }
-        __syncthreads();
-    }
-}
+// Diagonal block: factor + inverse, one CTA of 256 threads per front.
+//
+// The 16 x 16 threads each own a 4 x 4 tile of the 64 x 64 block in
+// registers (columns >= w are padded with the identity).  Right-looking
+// elimination with one barrier per pivot: step k reads column k from a
+// double-buffered shared vector, applies A_ij -= A_ik A_jk / p (p = A_kk;
+// the Cholesky and the LDLt update alike) to the tile, scales column k to
+// L_ik = A_ik / sqrt(p) (Cholesky) or A_ik / p (LDLt), and the owners of
+// column k + 1 publish it for the next step.  The inverse X = L^-1 (unit
+// diagonal for LDLt) follows by the row sweep: step k scales row k of X by
+// 1 / L_kk and eliminates it from the rows below, again on register tiles.
+constexpr int LDS = kNB + 4;  // shared-memory leading dimension of the GEMM stages
+constexpr int LDA = kNB + 1;  // leading dimension of the factored block in the diagonal kernel
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -375,43 +273,145 @@ __global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, 
                                               T* __restrict__ d, const double* __restrict__ signs,
                                               long long* __restrict__ info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Dk = reinterpret_cast<T*>(smem_raw);  // kNB * LDS
-    T* X = Dk + kNB * LDS;                   // kNB * kNB
-    T* Tm = X + kNB * kNB;                   // 3 * 256
-    T* piv = Tm + 3 * 256;                   // kNB
-    __shared__ int flag;
+    T* Ls = reinterpret_cast<T*>(smem_raw);  // factored block, column major, ld LDA
+    T* vec = Ls + kNB * LDA;                 // 2 x 64 broadcast vectors
+    T* rinv = vec + 2 * kNB;                 // 1 / L_kk (Cholesky) or 1 / d_k
+    T* pivs = rinv + kNB;                    // L_kk (Cholesky) or d_k (LDLt)
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int w = min(kNB, nn - c0);
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x;
+    const int ti = tid & 15, tj = tid >> 4;  // rows 4ti.., columns 4tj..
+    const int r0 = 4 * ti, q0 = 4 * tj;
     T* Pj = P + f.poff;
-    for (int i = tid; i < kNB * kNB; i += nt) {
-        int r = i & (kNB - 1), c = i >> 6;
-        T v;
-        if (r < w && c < w) v = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
-        else v = (r == c) ? T(1) : T(0);
-        Dk[r + c * LDS] = v;
-    }
+    T a[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = r0 + r, j = q0 + c;
+            T v = (i == j) ? T(1) : T(0);
+            if (i >= j && i < w && j < w) v = Pj[(c0 + i) + (int64_t)(c0 + j) * ld];
+            a[r][c] = v;
+        }
+    // column 0 into the first broadcast vector
+    if (tj == 0)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) vec[r0 + r] = a[r][0];
     __syncthreads();
-    int bad = factor_diag64<T, LDLT>(Dk, piv, w, signs, (int64_t)f.col0 + c0, &flag);
+    int bad = -1;
+    for (int k = 0; k < kNB; ++k) {
+        const T* col = vec + (k & 1) * kNB;
+        T* nxt = vec + ((k + 1) & 1) * kNB;
+        const T pv = col[k];
+        if (k < w) {
+            const double sg = pivot_sign(signs, LDLT, (int64_t)f.col0 + c0 + k);
+            if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) { bad = k; break; }  // uniform
+        }
+        const T rp = T(1) / pv;
+        T ci[4], cj[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) { ci[r] = col[r0 + r]; cj[r] = col[q0 + r] * rp; }
+        // trailing update A_ij -= A_ik A_jk / p  (k < j <= i)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (q0 + c > k && r0 + r >= q0 + c) a[r][c] -= ci[r] * cj[c];
+        // column k: L_ik = A_ik / sqrt(p) (Cholesky) or A_ik / p (LDLt)
+        const T sc = LDLT ? rp : T(1) / sqrt(pv);
+        if (tj == (k >> 2)) {
+            const int cc = k & 3;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (c == cc)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int i = r0 + r;
+                        if (i > k) a[r][c] *= sc;
+                        else if (i == k && !LDLT) a[r][c] = pv * sc;
+                    }
+        }
+        if (tid == 0) { rinv[k] = sc; pivs[k] = LDLT ? pv : pv * sc; }
+        // publish column k + 1 (already updated by this step)
+        if (k + 1 < kNB && tj == ((k + 1) >> 2)) {
+            const int cc = (k + 1) & 3;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (c == cc)
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) nxt[r0 + r] = a[r][c];
+        }
+        __syncthreads();
+    }
     if (bad >= 0) {
         if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
         return;
     }
-    for (int i = tid; i < w * w; i += nt) {
-        int r = i % w, c = i / w;
-        if (r >= c) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = Dk[r + c * LDS];
+    // factored block: to shared memory (the inverse reads its columns) and to the panel
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = r0 + r, j = q0 + c;
+            Ls[i + j * LDA] = i >= j ? a[r][c] : T(0);
+            if (i >= j && i < w && j < w) Pj[(c0 + i) + (int64_t)(c0 + j) * ld] = a[r][c];
+        }
+    if (LDLT && tid < w) d[f.col0 + c0 + tid] = pivs[tid];
+    // inverse X = L^-1 by the row sweep: step k scales row k by 1 / L_kk and
+    // eliminates it from the rows below; X tiles stay in registers
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a[r][c] = (r0 + r == q0 + c) ? T(1) : T(0);
+    if (ti == 0)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) vec[q0 + c] = a[0][c];
+    __syncthreads();
+    for (int k = 0; k < kNB; ++k) {
+        const T* row = vec + (k & 1) * kNB;  // row k of X before its scaling
+        T* nxt = vec + ((k + 1) & 1) * kNB;
+        const T rk = LDLT ? T(1) : rinv[k];
+        T xr[4], li[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) xr[c] = row[q0 + c] * rk;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) li[r] = Ls[(r0 + r) + k * LDA];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (r0 + r > k && q0 + c <= k) a[r][c] -= li[r] * xr[c];
+        if (ti == (k >> 2)) {
+            const int rr = k & 3;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (r == rr)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) a[r][c] *= rk;
+        }
+        if (k + 1 < kNB && ti == ((k + 1) >> 2)) {
+            const int rr = (k + 1) & 3;
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+                if (r == rr)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) nxt[q0 + c] = a[r][c];
+        }
+        __syncthreads();
     }
-    if (LDLT)
-        for (int i = tid; i < w; i += nt) d[f.col0 + c0 + i] = piv[i];
-    invert_lower64<T, LDLT>(Dk, X, Tm);
     T* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
-    for (int i = tid; i < kNB * kNB; i += nt) {
-        int r = i & (kNB - 1), c = i >> 6;
-        dst[i] = (r < w && c < w) ? X[i] : T(0);
-    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int i = r0 + r, j = q0 + c;
+            dst[i + j * kNB] = (i < w && j < w) ? a[r][c] : T(0);
+        }
 }
+template <typename T>
+constexpr int diag_smem() { return (kNB * LDA + 4 * kNB) * (int)sizeof(T); }
 
 // ---------------------------------------------------------------------------
 // Tile GEMM with a cp.async double-buffered K loop:
@@ -708,8 +708,6 @@ int launch_panel32_to_dl(mf_handle* h, double* dD, double* dL) {
     return 0;
 }
 
-template <typename T>
-constexpr int diag_smem() { return (kNB * LDS + kNB * kNB + 3 * 256 + kNB) * (int)sizeof(T); }
 
 template <typename T, int LDLT>
 static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
@@ -801,9 +799,47 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     return 0;
 }
 
+int run_captured(mf_handle* h, int64_t k0, int64_t k1, int64_t k2, int64_t k3, const std::function<int()>& body) {
+    if (!h->use_graphs || h->profile || !h->stream) return body();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    MF_CUDA(cudaStreamIsCapturing(h->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return body();
+    for (const GraphEntry& g : h->graphs)
+        if (g.key[0] == k0 && g.key[1] == k1 && g.key[2] == k2 && g.key[3] == k3) {
+            MF_CUDA(cudaGraphLaunch(g.exec, h->stream));
+            return 0;
+        }
+    MF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return rc ? rc : cuda_fail(e, "cudaStreamEndCapture");
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+    h->graphs.push_back(GraphEntry{{k0, k1, k2, k3}, exec});
+    MF_CUDA(cudaGraphLaunch(exec, h->stream));
+    return 0;
+}
+
+void release_graphs(mf_handle* h) {
+    for (GraphEntry& g : h->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+}
+
+// graph keys: kind (1 FP64 factor, 2 FP32 factor), then what the launch
+// sequence reads through pointers that can change between calls
 int launch_factor(mf_handle* h) {
     FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d};
-    return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
+    return run_captured(h, 1, (int64_t)(uintptr_t)h->d_signs, 0, 0, [&]() {
+        return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
+    });
 }
 
 int launch_factor_mixed(mf_handle* h) {
@@ -812,7 +848,9 @@ int launch_factor_mixed(mf_handle* h) {
         int rc = tc_prepare(h);
         if (rc) return rc;
     }
-    return h->diag ? factor_impl<float, 1>(h, fb) : factor_impl<float, 0>(h, fb);
+    return run_captured(h, 2, (int64_t)(uintptr_t)h->d_signs, h->use_tc ? 1 : 0, 0, [&]() {
+        return h->diag ? factor_impl<float, 1>(h, fb) : factor_impl<float, 0>(h, fb);
+    });
 }
 
 }  // namespace mf

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -136,6 +137,13 @@ struct SolveBufs {
     T* part = nullptr;  // backward partial sums (nbwd_part * 64 * 16)
 };
 
+// An instantiated CUDA graph of one fixed launch sequence of a handle (a
+// factorization or a solve), keyed by what the sequence depends on.
+struct GraphEntry {
+    int64_t key[4];
+    cudaGraphExec_t exec;
+};
+
 // single-precision copy of the factor and solve workspaces (mixed mode)
 struct Mixed {
     float* P = nullptr;
@@ -152,6 +160,7 @@ struct Mixed {
 
 struct mf_handle {
     int device = 0;
+    int num_sms = 0;              // streaming multiprocessors of the device (persistent grids)
     int diag = 0;                 // 0 Cholesky, 1 LDLt
     int64_t n = 0, nfr = 0, nsep = 0;
     int64_t ndz = 0, nlz = 0, npanel = 0, nmval = 0, nrval_per_rhs = 0;
@@ -222,11 +231,20 @@ struct mf_handle {
     double* d_red = nullptr;       // reductions and scalars (see mf_refine.cu)
     const double* cur_nz = nullptr; // values of the current matrix (device)
     bool mixed_fallback = false;   // FP32 factorization failed; the FP64 factor is used
+    // independent row segments (a batch of matrices factored as one forest):
+    // the refinement measures the backward error of every segment separately
+    int64_t nseg = 0;
+    int64_t* d_segptr = nullptr;   // nseg + 1 row boundaries, elimination order
+    double* d_segred = nullptr;    // per segment: max|t|, max|x|, max|b| (3 x 16), ||A||_inf
+    double* d_segeta = nullptr;    // per segment: worst backward error of the last refinement step
 
     int64_t bytes = 0;             // device bytes allocated
     // optional per-kernel timing
     bool profile = false;
     mf::KernelTimes times;
+    // CUDA graphs of the factorization and solve launch sequences
+    bool use_graphs = true;
+    std::vector<mf::GraphEntry> graphs;
     std::vector<cudaEvent_t> ev_pool;
 };
 
@@ -264,11 +282,20 @@ int launch_solve_mixed(mf_handle* h, int64_t nrhs);
 int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst);
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);
 int launch_anorm(mf_handle* h);
+constexpr int kSegRed = 49;  // doubles per segment in d_segred
 int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters, double* eta);
 constexpr int kRedDoubles = 256 + 16 * 148 * 4;
 int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
 int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);
 const char* last_error();
+
+// Run `body` (stream-ordered launches on h->stream) as a CUDA graph: the
+// first call with a key captures and instantiates it, later calls replay it.
+// Runs `body` directly when graphs are off, per-kernel profiling is on, the
+// handle's stream is the legacy default stream, or the caller is already
+// capturing that stream.
+int run_captured(mf_handle* h, int64_t k0, int64_t k1, int64_t k2, int64_t k3, const std::function<int()>& body);
+void release_graphs(mf_handle* h);
 
 // timing helpers
 struct Timer {

@@ -6,7 +6,10 @@
 // supernodal solve.  FP64 stays in the residual b - A x (CSR of the original
 // values, elimination order), the solution update and the scalars:
 //   Cholesky : preconditioned conjugate gradients, one CG per right-hand side;
-//   LDLt     : classical iterative refinement x += M^-1 (b - A x).
+//   LDLt, and any handle split into row segments (a batch of independent
+//   matrices): classical iterative refinement x += M^-1 (b - A x), which
+//   keeps the segments independent; the backward error is then measured per
+//   segment and the loop runs until the worst segment meets the tolerance.
 // Every iteration measures the normwise backward error
 //   eta = ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
 // per column and stops when all columns reach the tolerance.  Reductions are
@@ -92,6 +95,105 @@ __global__ void k_resid(const int64_t* __restrict__ ptr, const int32_t* __restri
     }
     __syncthreads();
     if (threadIdx.x < 48 && (threadIdx.x & 15) < nrhs) atomic_max_nonneg(red + threadIdx.x, mx[threadIdx.x]);
+}
+
+// Per-segment version of k_resid: one CTA per segment of rows
+// [segptr[s], segptr[s+1]); maxima into segred[s * kSegRed + (0|16|32) + r].
+__global__ void k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                            const int64_t* __restrict__ src, const double* __restrict__ nz,
+                            const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ t,
+                            const int64_t* __restrict__ segptr, double* __restrict__ segred, int64_t n, int nrhs) {
+    const int64_t s = blockIdx.x;
+    const int64_t r0 = segptr[s], r1 = segptr[s + 1];
+    double m[48];
+#pragma unroll
+    for (int q = 0; q < 48; ++q) m[q] = 0.0;
+    for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        double acc[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) acc[r] = 0.0;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+            const double a = nz[src[p]];
+            const int64_t c = col[p];
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+                if (r < nrhs) acc[r] += a * x[c + r * n];
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+            if (r < nrhs) {
+                const double bi = b[i + r * n];
+                const double ti = bi - acc[r];
+                if (t) t[i + r * n] = ti;
+                m[r] = fmax(m[r], fabs(ti));
+                m[16 + r] = fmax(m[16 + r], fabs(x[i + r * n]));
+                m[32 + r] = fmax(m[32 + r], fabs(bi));
+            }
+    }
+    __shared__ double mx[48];
+    if (threadIdx.x < 48) mx[threadIdx.x] = 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 48; ++q) {
+        double v = m[q];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && (q & 15) < nrhs) atomic_max_nonneg(mx + q, v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 48) segred[s * kSegRed + threadIdx.x] = mx[threadIdx.x];
+}
+
+// ||A||_inf of every segment into segred[s * kSegRed + 48]
+__global__ void k_anorm_seg(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
+                            const double* __restrict__ nz, const int64_t* __restrict__ segptr,
+                            double* __restrict__ segred) {
+    const int64_t s = blockIdx.x;
+    double v = 0.0;
+    for (int64_t i = segptr[s] + threadIdx.x; i < segptr[s + 1]; i += blockDim.x) {
+        double rs = 0.0;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) rs += fabs(nz[src[p]]);
+        v = fmax(v, rs);
+    }
+    __shared__ double mx;
+    if (threadIdx.x == 0) mx = 0.0;
+    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&mx, v);
+    __syncthreads();
+    if (threadIdx.x == 0) segred[s * kSegRed + 48] = mx;
+}
+
+// eta of every (segment, column); segeta[s] = worst column of segment s,
+// out[r] = worst segment of column r
+__global__ void k_seg_eta(const double* __restrict__ segred, int64_t nseg, int nrhs, double* __restrict__ out,
+                          double* __restrict__ segeta) {
+    __shared__ double mx[16];
+    if (threadIdx.x < 16) mx[threadIdx.x] = 0.0;
+    __syncthreads();
+    double worst[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) worst[r] = 0.0;
+    for (int64_t s = threadIdx.x; s < nseg; s += blockDim.x) {
+        const double* q = segred + s * kSegRed;
+        double w = 0.0;
+#pragma unroll
+        for (int r = 0; r < 16; ++r)
+            if (r < nrhs) {
+                const double den = q[48] * q[16 + r] + q[32 + r];
+                const double e = den > 0.0 ? q[r] / den : (q[r] > 0.0 ? INFINITY : 0.0);
+                w = fmax(w, e);
+                worst[r] = fmax(worst[r], e);
+            }
+        segeta[s] = w;
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        double v = worst[r];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0 && r < nrhs) atomic_max_nonneg(mx + r, v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 16) out[threadIdx.x] = mx[threadIdx.x];
 }
 
 // ||A||_inf (max absolute row sum) into *out
@@ -221,6 +323,16 @@ static int dot(mf_handle* h, const double* u, const double* v, double* out, int 
 static int backward_error(mf_handle* h, const double* x, const double* b, double* t, int nrhs, double* eta) {
     Timer tm(h, K_SPMV);
     double* red = h->d_red;  // [0..48) maxima, [48] ||A||_inf
+    if (h->nseg > 0) {
+        k_resid_seg<<<(unsigned)h->nseg, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b,
+                                                               t, h->d_segptr, h->d_segred, h->n, nrhs);
+        MF_CUDA(cudaGetLastError());
+        k_seg_eta<<<1, 256, 0, h->stream>>>(h->d_segred, h->nseg, nrhs, red, h->d_segeta);
+        MF_CUDA(cudaGetLastError());
+        MF_CUDA(cudaMemcpyAsync(eta, red, 16 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        MF_CUDA(cudaStreamSynchronize(h->stream));
+        return 0;
+    }
     MF_CUDA(cudaMemsetAsync(red, 0, 48 * sizeof(double), h->stream));
     k_resid<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b, t, red,
                                                       h->n, nrhs);
@@ -240,6 +352,11 @@ int launch_anorm(mf_handle* h) {
     MF_CUDA(cudaMemsetAsync(out, 0, sizeof(double), h->stream));
     k_anorm<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, out, h->n);
     MF_CUDA(cudaGetLastError());
+    if (h->nseg > 0) {
+        k_anorm_seg<<<(unsigned)h->nseg, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, h->d_segptr,
+                                                               h->d_segred);
+        MF_CUDA(cudaGetLastError());
+    }
     return 0;
 }
 
@@ -268,8 +385,9 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
         if (eta_out) *eta_out = worst;
         return 0;
     }
-    if (!h->diag) {
-        // preconditioned conjugate gradients
+    if (!h->diag && h->nseg == 0) {
+        // preconditioned conjugate gradients (segmented batches use the
+        // refinement below, which keeps every segment independent)
         MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
         MF_CUDA(cudaMemcpyAsync(R, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
         if ((rc = apply_prec<false>(h, R, Z, nrhs))) return rc;

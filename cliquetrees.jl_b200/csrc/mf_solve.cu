@@ -534,7 +534,9 @@ int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
     SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, h->d_R, h->d_W, h->d_C, h->d_part};
-    return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
+    return run_captured(h, 3, nrhs, 0, 0, [&]() {
+        return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
+    });
 }
 
 // Same on the single-precision factor: f32.C (n x nrhs, elimination order) in place.
@@ -542,7 +544,9 @@ int launch_solve_mixed(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
     SolveBufs<float> sb{h->f32.P, h->f32.inv, h->f32.d, h->f32.R, h->f32.W, h->f32.C, h->f32.part};
-    return h->diag ? solve_impl<float, 1>(h, sb, (int)nrhs) : solve_impl<float, 0>(h, sb, (int)nrhs);
+    return run_captured(h, 4, nrhs, 0, 0, [&]() {
+        return h->diag ? solve_impl<float, 1>(h, sb, (int)nrhs) : solve_impl<float, 0>(h, sb, (int)nrhs);
+    });
 }
 
 }  // namespace mf

@@ -8,31 +8,36 @@
 // keeps the factor close to FP32 accuracy so the FP64 refinement converges
 // in a few steps.
 //
-// Data path per CTA (256 threads, one output tile):
-//   * thread 0 issues cp.async.bulk.tensor 2D loads (no swizzle) of
-//     32-row x KC-column boxes of the column-major panel into a ring of
+// Persistent and warp-specialised: a CTA (one per SM) walks the launch's
+// tiles t = blockIdx.x, blockIdx.x + gridDim.x, ...; its warps form a
+// pipeline connected by mbarriers:
+//   * warp 16 (one lane) issues cp.async.bulk.tensor 2D loads (no swizzle)
+//     of 32-row x KC-column boxes of the column-major panel into a ring of
 //     NRAW raw stages; a box lands as [k][32 rows] (rows contiguous);
-//   * all threads wait on the stage's mbarrier and convert it into one of
-//     NOP operand stages: 4 consecutive k of one row are read (conflict-free
-//     across a warp: consecutive rows), scaled by the LDLt pivots where the
-//     role needs A*D, split into hi/lo and stored as one 16-byte row of an
-//     8-row core matrix of the canonical K-major no-swizzle UMMA layout
-//     (core matrices 128 B apart along M/N, (rows/8)*128 B apart along K);
-//     `kind::tf32` takes K-major operands only, so this conversion is also
-//     the transpose;
-//   * thread 0 issues 3 tcgen05.mma per K slice of 8, commits them to the
-//     operand stage's mbarrier and refills the raw stage it just released,
-//     so TMA, the conversion of chunk c+1 and the MMAs of chunk c overlap.
+//   * warps 8..15 convert a raw stage into one of NOP operand stages: 4
+//     consecutive k of one row are read (conflict-free across a warp:
+//     consecutive rows), scaled by the LDLt pivots where the role needs A*D,
+//     split into hi/lo and stored as one 16-byte row of an 8-row core matrix
+//     of the canonical K-major no-swizzle UMMA layout (core matrices 128 B
+//     apart along M/N, (rows/8)*128 B apart along K); `kind::tf32` takes
+//     K-major operands only, so this conversion is also the transpose;
+//   * warp 17 (one lane) issues 3 tcgen05.mma per K slice of 8 into one of
+//     two TMEM accumulators and commits each operand stage back to the
+//     converters and each finished tile to the epilogue;
+//   * warps 0..7 (warp w reads TMEM lanes 32(w%4).. = tile rows, column
+//     half w/4) load the C tile into registers while its MMAs run, then read
+//     the finished accumulator with tcgen05.ld and store C - acc (or
+//     acc / d for the TRSM role) while the next tile is multiplied.
 // Tiles start on a 4-row boundary (a TMA box must start on 16 bytes): a
 // tile whose first wanted row is not aligned starts at the aligned row below
-// it and the epilogue drops the extra rows.  The epilogue reads TMEM with
-// tcgen05.ld (warp w owns TMEM lanes 32(w%4).. and column half w/4) and
-// applies C -= acc (or C = acc / d for the TRSM role).  Every mbarrier wait
-// is bounded by %globaltimer; a timeout sets an error flag, waits (bounded)
-// for the loads and MMAs in flight, frees the TMEM and returns.
+// it and the epilogue drops the extra rows.  Every mbarrier wait is bounded
+// by %globaltimer and by a shared abort flag; a timeout sets the error flag
+// and every role drains what it has in flight (each wait bounded) before the
+// TMEM is freed.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <string>
@@ -44,9 +49,18 @@ namespace mf {
 
 namespace tc {
 
+#ifndef MF_TC_TERMS
+#define MF_TC_TERMS 3  // products per K slice: hi*hi + hi*lo + lo*hi
+#endif
+
 constexpr int TM = kTM;        // 128 tile rows (UMMA M)
 constexpr int KC = 32;         // K per pipeline stage (4 UMMA K-slices of 8)
-constexpr int NT = 256;        // threads per CTA
+constexpr int NEPI = 8;        // epilogue warps 0..7 (warp w: TMEM lane quarter w % 4, column half w / 4)
+constexpr int NCONV = 8;       // converter warps 8..15
+constexpr int WTMA = 16;       // TMA producer warp
+constexpr int WMMA = 17;       // MMA issuer warp (also allocates the TMEM)
+constexpr int NT = 18 * 32;    // threads per CTA
+constexpr int CT = NCONV * 32; // converter threads
 constexpr int BOX_BYTES = 32 * KC * 4;  // one 32-row raw box: 4 KB
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any wait
 
@@ -59,9 +73,9 @@ struct Cfg {
     static constexpr int NRAW = TN == 64 ? 4 : 3;
     static constexpr int NOP = 2;
     static constexpr int RING_BYTES = NRAW * RAW_BYTES + NOP * OP_BYTES;
-    static constexpr int SMEM_BYTES = RING_BYTES + 512 /* barriers, pivots, TMEM slot */ + 128 /* alignment */;
+    static constexpr int SMEM_BYTES = RING_BYTES + 256 /* barriers, TMEM slot, abort flag */ + 128 /* alignment */;
     static constexpr uint32_t TX_BYTES = (uint32_t)RAW_BYTES;  // bytes the TMA writes per stage
-    static constexpr uint32_t TMEM_COLS = TN;
+    static constexpr uint32_t TMEM_COLS = 2 * TN;              // two accumulators
     static constexpr uint32_t LBO_A = (TM / 8) * 128;  // K-adjacent core matrices
     static constexpr uint32_t LBO_B = (TN / 8) * 128;
     // instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = TN
@@ -98,14 +112,42 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// bounded wait on one mbarrier phase; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// try_wait that lets the hardware suspend the thread (up to `hint_ns`)
+// until the phase completes, so waiting warps do not take issue slots from
+// the working ones
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait on one mbarrier phase; false on timeout or once *abort is set
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const volatile int* abort) {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
+        if (*abort || globaltimer() - t0 > kWaitNs) return false;
+    }
+    return true;
+}
+
+// bounded wait that ignores the abort flag: used to drain copies and MMAs
+// still in flight before the CTA exits
+__device__ __forceinline__ bool mbar_drain(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    while (!mbar_try_wait_sleep(bar, parity, 20000u)) {
         if (globaltimer() - t0 > kWaitNs) return false;
     }
     return true;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // 2D tiled TMA load of one 32 x KC box (x = row, y = column) into shared memory
@@ -154,20 +196,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ uint32_t f2tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
+// x rounded to TF32 (10 explicit mantissa bits, ties away from zero) with
+// integer operations: adding half a TF32 unit to the magnitude bits and
+// clearing the 13 dropped bits.  Finite inputs only.  Integer ALU work keeps
+// the split off the conversion pipe, which would otherwise limit the MMAs.
+__device__ __forceinline__ uint32_t f2tf32(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 
 // Convert ROWS rows x KC columns of a raw stage ([row/32][k][row%32]) into
 // the hi/lo K-major operand tiles.  Columns k >= kc are zero; when dsc is
 // given, column k is scaled by dsc[k] first.
 template <int ROWS>
-__device__ __forceinline__ void convert(const float* __restrict__ raw, uint32_t* __restrict__ hi,
+__device__ __forceinline__ void convert(int ct, const float* __restrict__ raw, uint32_t* __restrict__ hi,
                                         uint32_t* __restrict__ lo, int kc, const float* __restrict__ dsc) {
 #pragma unroll 2
-    for (int i = threadIdx.x; i < ROWS * (KC / 4); i += NT) {
+    for (int i = ct; i < ROWS * (KC / 4); i += CT) {
         const int m = i % ROWS, kq = i / ROWS;
         const float* src = raw + (m >> 5) * (32 * KC) + (kq * 4) * 32 + (m & 31);
         float x[4];
@@ -202,12 +244,67 @@ struct TcTileN {
     static constexpr int value = ROLE == TC_SYRK ? kTcSyrkN : kTile;
 };
 
+// Geometry of one tile: TMA rows xa (A) and xb (B); K range [kbeg, kend)
+// of map columns (A at ka0 + k, B at kb0 + k); C coordinates of tile row 0
+// / column 0 are (orow, ocol); valid C range rows [rlo, rhi) x columns
+// [clo, chi); lower triangle only if tri.
+struct TileGeom {
+    int xa, xb, kbeg, kend, ka0, kb0, orow, ocol, rlo, rhi, clo, chi, nchunk, front;
+    bool tri;
+    float* C;
+    int64_t ldc;
+};
+
+template <int ROLE>
+__device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, const Item& it, int ob, int c0,
+                                              float* P, float* M) {
+    constexpr int TN = TcTileN<ROLE>::value;
+    const Front f = fronts[it.front];
+    const int nn = f.nn, na = f.na, nj = nn + na;
+    TileGeom g;
+    g.front = it.front;
+    if (ROLE == TC_LEFT) {
+        const int w = min(kNB, nn - c0);
+        g.xa = c0 + it.a * tc::TM; g.xb = c0;
+        g.kbeg = ob * kOB; g.kend = c0; g.ka0 = g.kb0 = 0;
+        g.orow = g.xa; g.ocol = c0; g.rlo = c0; g.rhi = nj; g.clo = c0; g.chi = c0 + w; g.tri = true;
+        g.C = P + f.poff; g.ldc = f.ldp;
+    } else if (ROLE == TC_TRAIL) {
+        const int e = min(nn, (ob + 1) * kOB);
+        const int cs = e + it.b * TN;
+        g.xa = cs + it.a * tc::TM; g.xb = cs;
+        g.kbeg = ob * kOB; g.kend = e; g.ka0 = g.kb0 = 0;
+        g.orow = g.xa; g.ocol = cs; g.rlo = cs; g.rhi = nj; g.clo = cs; g.chi = nn; g.tri = true;
+        g.C = P + f.poff; g.ldc = f.ldp;
+    } else if (ROLE == TC_SYRK) {
+        const int x0 = nn & ~3;            // aligned start at or before the first L21 row
+        const int cs = x0 + it.b * TN;     // panel row of tile column 0
+        g.xa = cs + it.a * tc::TM; g.xb = cs;
+        g.kbeg = 0; g.kend = nn; g.ka0 = g.kb0 = 0;
+        g.orow = g.xa - nn; g.ocol = cs - nn; g.rlo = 0; g.rhi = na; g.clo = 0; g.chi = na; g.tri = true;
+        g.C = M + f.moff; g.ldc = f.ldm;
+    } else {
+        const int w = min(kNB, nn - c0);
+        const int r0 = c0 + w;
+        g.xa = (r0 & ~3) + it.a * tc::TM; g.xb = 0;
+        g.kbeg = 0; g.kend = w; g.ka0 = c0;
+        g.kb0 = (int)((f.ioff + (int64_t)(c0 / kNB) * kNB * kNB) / kNB);
+        g.orow = g.xa; g.ocol = c0; g.rlo = r0; g.rhi = nj; g.clo = c0; g.chi = c0 + w; g.tri = false;
+        g.C = P + f.poff; g.ldc = f.ldp;
+    }
+    // a TMA box must start on a 16-byte boundary: rows on multiples of 4
+    const bool aligned = ((g.xa | g.xb) & 3) == 0;
+    g.nchunk = aligned ? (g.kend - g.kbeg + tc::KC - 1) / tc::KC : 0;
+    return g;
+}
+
 template <int ROLE, int LDLT>
-__global__ void __launch_bounds__(tc::NT) k_gemm_tc(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                    int ob, int c0, float* __restrict__ P, float* __restrict__ M,
-                                                    const float* __restrict__ d,
-                                                    const CUtensorMap* __restrict__ maps,
-                                                    const CUtensorMap* __restrict__ inv_map, int* __restrict__ err) {
+__global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__ fronts,
+                                                       const Item* __restrict__ items, int64_t ntiles, int ob, int c0,
+                                                       float* __restrict__ P, float* __restrict__ M,
+                                                       const float* __restrict__ d,
+                                                       const CUtensorMap* __restrict__ maps,
+                                                       const CUtensorMap* __restrict__ inv_map, int* __restrict__ err) {
     using namespace tc;
     constexpr int TN = TcTileN<ROLE>::value;
     using C_ = Cfg<TN>;
@@ -216,182 +313,199 @@ __global__ void __launch_bounds__(tc::NT) k_gemm_tc(const Front* __restrict__ fr
     unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
     unsigned char* raw_base = base;
     unsigned char* op_base = base + NRAW * C_::RAW_BYTES;
-    uint64_t* full = reinterpret_cast<uint64_t*>(base + C_::RING_BYTES);  // raw stage landed
-    uint64_t* opfree = full + NRAW;                                        // MMAs done with an operand stage
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(opfree + NOP);
-    float* scl = reinterpret_cast<float*>(base + C_::RING_BYTES + 256);    // 64 reciprocal pivots (TRSM, LDLt)
+    uint64_t* raw_full = reinterpret_cast<uint64_t*>(base + C_::RING_BYTES);  // TMA landed
+    uint64_t* raw_empty = raw_full + NRAW;    // converters done with a raw stage
+    uint64_t* op_full = raw_empty + NRAW;     // converters filled an operand stage
+    uint64_t* op_empty = op_full + NOP;       // MMAs done with an operand stage
+    uint64_t* acc_full = op_empty + NOP;      // accumulator ready for the epilogue
+    uint64_t* acc_empty = acc_full + 2;       // epilogue done with an accumulator
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + 2);
+    volatile int* abort = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
-    float* Pj = P + f.poff;
-    const float* dj = LDLT ? d + f.col0 : nullptr;
-    const int tid = threadIdx.x, warp = tid >> 5;
-    const CUtensorMap* amap = maps + it.front;
-    const CUtensorMap* bmap = amap;
-
-    // tile geometry: TMA rows xa (A) and xb (B); K range [kbeg, kend) of
-    // map columns (A at ka0 + k, B at kb0 + k); C coordinates of tile row 0
-    // / column 0 are (orow, ocol); valid C range rows [rlo, rhi) x columns
-    // [clo, chi); lower triangle only if tri.
-    int xa, xb, kbeg, kend, ka0, kb0, orow, ocol, rlo, rhi, clo, chi;
-    bool tri;
-    float* C;
-    int64_t ldc;
-    if (ROLE == TC_LEFT) {
-        const int w = min(kNB, nn - c0);
-        xa = c0 + it.a * TM; xb = c0;
-        kbeg = ob * kOB; kend = c0; ka0 = kb0 = 0;
-        orow = xa; ocol = c0; rlo = c0; rhi = nj; clo = c0; chi = c0 + w; tri = true;
-        C = Pj; ldc = ld;
-    } else if (ROLE == TC_TRAIL) {
-        const int e = min(nn, (ob + 1) * kOB);
-        const int cs = e + it.b * TN;
-        xa = cs + it.a * TM; xb = cs;
-        kbeg = ob * kOB; kend = e; ka0 = kb0 = 0;
-        orow = xa; ocol = cs; rlo = cs; rhi = nj; clo = cs; chi = nn; tri = true;
-        C = Pj; ldc = ld;
-    } else if (ROLE == TC_SYRK) {
-        const int x0 = nn & ~3;            // aligned start at or before the first L21 row
-        const int cs = x0 + it.b * TN;     // panel row of tile column 0
-        xa = cs + it.a * TM; xb = cs;
-        kbeg = 0; kend = nn; ka0 = kb0 = 0;
-        orow = xa - nn; ocol = cs - nn; rlo = 0; rhi = na; clo = 0; chi = na; tri = true;
-        C = M + f.moff; ldc = f.ldm;
-    } else {
-        const int w = min(kNB, nn - c0);
-        const int r0 = c0 + w;
-        xa = (r0 & ~3) + it.a * TM; xb = 0;
-        kbeg = 0; kend = w; ka0 = c0;
-        kb0 = (int)((f.ioff + (int64_t)(c0 / kNB) * kNB * kNB) / kNB);
-        orow = xa; ocol = c0; rlo = r0; rhi = nj; clo = c0; chi = c0 + w; tri = false;
-        C = Pj; ldc = ld;
-        bmap = inv_map;
-    }
-    const float* dvec = (LDLT && ROLE != TC_TRSM) ? dj : nullptr;
-
-    if (warp == 0) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == WMMA) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(C_::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < NRAW; ++s) mbar_init(&full[s], 1);
-        for (int s = 0; s < NOP; ++s) mbar_init(&opfree[s], 1);
+        for (int s = 0; s < NRAW; ++s) { mbar_init(&raw_full[s], 1); mbar_init(&raw_empty[s], NCONV); }
+        for (int s = 0; s < NOP; ++s) { mbar_init(&op_full[s], NCONV); mbar_init(&op_empty[s], 1); }
+        for (int s = 0; s < 2; ++s) { mbar_init(&acc_full[s], 1); mbar_init(&acc_empty[s], NEPI); }
+        *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (ROLE == TC_TRSM && LDLT) {
-        for (int i = tid; i < kNB; i += NT) scl[i] = ocol + i < chi ? 1.f / dj[ocol + i] : 0.f;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-
-    // a TMA box must start on a 16-byte boundary: rows on multiples of 4
-    const bool aligned = ((xa | xb) & 3) == 0;
-    const int nchunk = aligned ? (kend - kbeg + KC - 1) / KC : 0;
-    if (!aligned && tid == 0) atomicExch(err, 2);
-
-    auto raw_ptr = [&](int s) { return raw_base + s * C_::RAW_BYTES; };
-    auto op_ptr = [&](int s) { return op_base + s * C_::OP_BYTES; };
-    auto issue = [&](int c) {  // thread 0: loads of chunk c into raw stage c % NRAW
-        const int s = c % NRAW;
-        unsigned char* st = raw_ptr(s);
-        const int k = kbeg + c * KC;
-        mbar_expect_tx(&full[s], C_::TX_BYTES);
-#pragma unroll
-        for (int i = 0; i < TM / 32; ++i) tma_load_2d(st + i * BOX_BYTES, amap, xa + 32 * i, ka0 + k, &full[s]);
-#pragma unroll
-        for (int i = 0; i < TN / 32; ++i)
-            tma_load_2d(st + C_::A_BYTES + i * BOX_BYTES, bmap, xb + 32 * i, kb0 + k, &full[s]);
+    auto fail = [&](int code) {
+        *abort = 1;
+        atomicExch(err, code);
     };
 
-    int issued = 0;  // chunks whose loads thread 0 has issued
-    if (tid == 0)
-        for (; issued < NRAW && issued < nchunk; ++issued) issue(issued);
-
-    bool bad = false;
-    int consumed = 0;   // chunks whose loads every thread has seen land
-    int committed = 0;  // chunks whose MMAs thread 0 has committed
-    for (int c = 0; c < nchunk; ++c) {
-        const int rs = c % NRAW, os = c % NOP;
-        bool ok = mbar_wait(&full[rs], (uint32_t)((c / NRAW) & 1));
-        if (ok && c >= NOP) ok = mbar_wait(&opfree[os], (uint32_t)(((c - NOP) / NOP) & 1));
-        if (__syncthreads_or(!ok)) { bad = true; break; }
-        consumed = c + 1;
-        const float* raw = reinterpret_cast<const float*>(raw_ptr(rs));
-        uint32_t* op = reinterpret_cast<uint32_t*>(op_ptr(os));
-        const int kc = min(KC, kend - (kbeg + c * KC));
-        convert<TM>(raw, op, op + C_::A_BYTES / 4, kc, dvec ? dvec + kbeg + c * KC : nullptr);
-        convert<TN>(raw + C_::A_BYTES / 4, op + 2 * C_::A_BYTES / 4, op + (2 * C_::A_BYTES + C_::B_BYTES) / 4, kc,
-                    nullptr);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ahi = smem_u32(op), alo = ahi + C_::A_BYTES;
-            const uint32_t bhi = alo + C_::A_BYTES, blo = bhi + C_::B_BYTES;
-            const int nslices = (kc + 7) / 8;
-            for (int q = 0; q < nslices; ++q) {
-                const uint32_t oa = (uint32_t)(2 * q) * C_::LBO_A, ob_ = (uint32_t)(2 * q) * C_::LBO_B;
-                const uint64_t dah = make_desc(ahi + oa, C_::LBO_A, 128);
-                const uint64_t dal = make_desc(alo + oa, C_::LBO_A, 128);
-                const uint64_t dbh = make_desc(bhi + ob_, C_::LBO_B, 128);
-                const uint64_t dbl = make_desc(blo + ob_, C_::LBO_B, 128);
-                mma_tf32<TN>(tmem, dah, dbh, (c > 0 || q > 0) ? 1u : 0u);
-                mma_tf32<TN>(tmem, dah, dbl, 1u);
-                mma_tf32<TN>(tmem, dal, dbh, 1u);
-            }
-            mma_commit(&opfree[os]);
-            committed = c + 1;
-            // the raw stage of chunk c has been converted by every thread
-            if (issued < nchunk) issue(issued++);
-        }
-    }
-    if (!bad && nchunk > 0) {
-        const int last = nchunk - 1;
-        bad = !mbar_wait(&opfree[last % NOP], (uint32_t)((last / NOP) & 1));
-        bad = __syncthreads_or(bad);
-    }
-    if (bad) {
-        if (tid == 0) {
-            atomicExch(err, 1);
-            // let the loads and MMAs already in flight finish before the
-            // shared buffers and the TMEM go away (each wait bounded)
-            for (int c = consumed; c < issued; ++c) (void)mbar_wait(&full[c % NRAW], (uint32_t)((c / NRAW) & 1));
-            if (committed > 0)
-                (void)mbar_wait(&opfree[(committed - 1) % NOP], (uint32_t)(((committed - 1) / NOP) & 1));
-        }
-        __syncthreads();
-    } else if (nchunk > 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const int lw = warp & 3;                 // TMEM lane quarter this warp may read
-        const int r = lw * 32 + (tid & 31);
-        const int row = orow + r;
-        const uint32_t lane_base = tmem + ((uint32_t)(lw * 32) << 16);
-        const int cb0 = (warp >> 2) * (TN / 2);  // column half
+    if (warp == WTMA) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            int64_t g = 0;  // chunks issued by this CTA
+            bool ok = true;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const Item it = items[t];
+                const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+                if (tg.nchunk == 0) { fail(2); ok = false; break; }
+                const CUtensorMap* amap = maps + it.front;
+                const CUtensorMap* bmap = ROLE == TC_TRSM ? inv_map : amap;
+                for (int c = 0; c < tg.nchunk; ++c, ++g) {
+                    const int s = (int)(g % NRAW);
+                    if (g >= NRAW && !mbar_wait(&raw_empty[s], (uint32_t)(((g / NRAW) - 1) & 1), abort)) {
+                        fail(1);
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* st = raw_base + s * C_::RAW_BYTES;
+                    const int k = tg.kbeg + c * KC;
+                    mbar_expect_tx(&raw_full[s], C_::TX_BYTES);
 #pragma unroll
-        for (int cb = cb0; cb < cb0 + TN / 2; cb += 16) {
-            float v[16];
-            tc::tmem_ld16(lane_base + (uint32_t)cb, v);
-            if (row >= rlo && row < rhi) {
+                    for (int i = 0; i < TM / 32; ++i)
+                        tma_load_2d(st + i * BOX_BYTES, amap, tg.xa + 32 * i, tg.ka0 + k, &raw_full[s]);
+#pragma unroll
+                    for (int i = 0; i < TN / 32; ++i)
+                        tma_load_2d(st + C_::A_BYTES + i * BOX_BYTES, bmap, tg.xb + 32 * i, tg.kb0 + k, &raw_full[s]);
+                }
+            }
+            // drain: the last NRAW stages' loads must land before the CTA exits
+            for (int64_t q = (g > NRAW ? g - NRAW : 0); q < g; ++q)
+                (void)mbar_drain(&raw_full[q % NRAW], (uint32_t)((q / NRAW) & 1));
+        }
+    } else if (warp >= NEPI && warp < NEPI + NCONV) {
+        // ---------------- converters ----------------
+        const int ct = tid - NEPI * 32;
+        int64_t g = 0;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const Item it = items[t];
+            const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+            const float* dvec = (LDLT && ROLE != TC_TRSM) ? d + fronts[it.front].col0 : nullptr;
+            bool ok = true;
+            for (int c = 0; c < tg.nchunk; ++c, ++g) {
+                const int rs = (int)(g % NRAW), os = (int)(g % NOP);
+                ok = mbar_wait(&raw_full[rs], (uint32_t)((g / NRAW) & 1), abort);
+                if (ok && g >= NOP) ok = mbar_wait(&op_empty[os], (uint32_t)(((g / NOP) - 1) & 1), abort);
+                if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
+                const float* raw = reinterpret_cast<const float*>(raw_base + rs * C_::RAW_BYTES);
+                uint32_t* op = reinterpret_cast<uint32_t*>(op_base + os * C_::OP_BYTES);
+                const int kc = min(KC, tg.kend - (tg.kbeg + c * KC));
+                convert<TM>(ct, raw, op, op + C_::A_BYTES / 4, kc, dvec ? dvec + tg.kbeg + c * KC : nullptr);
+                convert<TN>(ct, raw + C_::A_BYTES / 4, op + 2 * C_::A_BYTES / 4,
+                            op + (2 * C_::A_BYTES + C_::B_BYTES) / 4, kc, nullptr);
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&raw_empty[rs]);
+                    mbar_arrive(&op_full[os]);
+                }
+            }
+            if (!ok) { if (lane == 0) fail(1); break; }
+        }
+    } else if (warp == WMMA) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            int64_t g = 0, i = 0;
+            bool ok = true;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+                const Item it = items[t];
+                const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+                const int a = (int)(i & 1);
+                if (i >= 2 && !mbar_wait(&acc_empty[a], (uint32_t)(((i / 2) - 1) & 1), abort)) {
+                    fail(1);
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t dt = tmem + (uint32_t)(a * TN);
+                for (int c = 0; c < tg.nchunk; ++c, ++g) {
+                    const int os = (int)(g % NOP);
+                    if (!mbar_wait(&op_full[os], (uint32_t)((g / NOP) & 1), abort)) { fail(1); ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t ahi = smem_u32(op_base + os * C_::OP_BYTES), alo = ahi + C_::A_BYTES;
+                    const uint32_t bhi = alo + C_::A_BYTES, blo = bhi + C_::B_BYTES;
+                    const int kc = min(KC, tg.kend - (tg.kbeg + c * KC));
+                    const int nslices = (kc + 7) / 8;
+                    for (int q = 0; q < nslices; ++q) {
+                        const uint32_t oa = (uint32_t)(2 * q) * C_::LBO_A, ob_ = (uint32_t)(2 * q) * C_::LBO_B;
+                        const uint64_t dah = make_desc(ahi + oa, C_::LBO_A, 128);
+                        const uint64_t dal = make_desc(alo + oa, C_::LBO_A, 128);
+                        const uint64_t dbh = make_desc(bhi + ob_, C_::LBO_B, 128);
+                        const uint64_t dbl = make_desc(blo + ob_, C_::LBO_B, 128);
+                        mma_tf32<TN>(dt, dah, dbh, (c > 0 || q > 0) ? 1u : 0u);
+#if MF_TC_TERMS > 1
+                        mma_tf32<TN>(dt, dah, dbl, 1u);
+                        mma_tf32<TN>(dt, dal, dbh, 1u);
+#endif
+                    }
+                    mma_commit(&op_empty[os]);
+                }
+                if (ok) mma_commit(&acc_full[a]);
+            }
+            // drain: every MMA issued must finish before the TMEM is freed
+            if (g > 0) (void)mbar_drain(&op_empty[(g - 1) % NOP], (uint32_t)(((g - 1) / NOP) & 1));
+        }
+    } else {
+        // ---------------- epilogue (warps 0..7) ----------------
+        // C -= acc: the C values of the next tile are loaded into registers
+        // while its MMAs run, so the read latency is hidden behind them
+        constexpr int HC = TN / 2;  // columns per epilogue thread
+        const int quarter = warp & 3, half = warp >> 2;
+        int64_t i = 0;
+        for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+            const Item it = items[t];
+            const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+            const int a = (int)(i & 1);
+            const int row = tg.orow + quarter * 32 + lane;
+            const int cbase = tg.ocol + half * HC;
+            const bool row_ok = row >= tg.rlo && row < tg.rhi;
+            // 32-bit offsets: a front's panel and update matrix stay below 2^31 elements
+            const int ldc = (int)tg.ldc;
+            float* cblk = tg.C + row + (int64_t)cbase * ldc;
+            float cv[HC];
+            if (ROLE != TC_TRSM) {
+#pragma unroll
+                for (int q = 0; q < HC; ++q) {
+                    const int col = cbase + q;
+                    const bool valid = row_ok && col >= tg.clo && col < tg.chi && (!tg.tri || row >= col);
+                    cv[q] = valid ? __ldcg(cblk + q * ldc) : 0.f;
+                }
+            }
+            const bool ok = mbar_wait(&acc_full[a], (uint32_t)((i / 2) & 1), abort);
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) fail(1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * TN + half * HC);
+            const float* dj = (ROLE == TC_TRSM && LDLT) ? d + fronts[it.front].col0 : nullptr;
+#pragma unroll
+            for (int cb = 0; cb < HC; cb += 16) {
+                float v[16];
+                tc::tmem_ld16(lane_base + (uint32_t)cb, v);
 #pragma unroll
                 for (int q = 0; q < 16; ++q) {
-                    const int col = ocol + cb + q;
-                    if (col >= clo && col < chi && (!tri || row >= col)) {
-                        float* p = C + row + (int64_t)col * ldc;
-                        if (ROLE == TC_TRSM) *p = LDLT ? v[q] * scl[cb + q] : v[q];
-                        else *p -= v[q];
+                    const int col = cbase + cb + q;
+                    if (row_ok && col >= tg.clo && col < tg.chi && (!tg.tri || row >= col)) {
+                        float* p = cblk + (cb + q) * ldc;
+                        if (ROLE == TC_TRSM) *p = LDLT ? v[q] / dj[col] : v[q];
+                        else *p = cv[cb + q] - v[q];
                     }
                 }
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[a]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if (warp == WMMA) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C_::TMEM_COLS)
                      : "memory");
@@ -402,8 +516,9 @@ template <int ROLE, int LDLT>
 static int launch_one(mf_handle* h, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb) {
     if (!l.cnt) return 0;
     constexpr int smem = tc::Cfg<TcTileN<ROLE>::value>::SMEM_BYTES;
-    k_gemm_tc<ROLE, LDLT><<<(unsigned)l.cnt, tc::NT, smem, h->stream>>>(
-        h->d_fronts, h->d_items + l.off, ob, c0, fb.P, fb.M, fb.d,
+    const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
+    k_gemm_tc<ROLE, LDLT><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
+        h->d_fronts, h->d_items + l.off, l.cnt, ob, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
         h->d_err);
     MF_CUDA(cudaGetLastError());

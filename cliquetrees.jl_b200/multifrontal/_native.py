@@ -113,6 +113,10 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_exec_sizes.restype = ctypes.c_int
         lib.mf_plan_info.argtypes = [_i64, _i64] + [_p64] * 8 + [ctypes.c_int, _p64]
         lib.mf_plan_info.restype = ctypes.c_int
+        lib.mf_set_segments.argtypes = [_vp, _i64, _p64]
+        lib.mf_set_segments.restype = ctypes.c_int
+        lib.mf_segment_errors.argtypes = [_vp, _pd]
+        lib.mf_segment_errors.restype = ctypes.c_int
         lib.mf_last_error.argtypes = []
         lib.mf_last_error.restype = ctypes.c_char_p
         _gpu = lib

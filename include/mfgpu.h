@@ -180,6 +180,22 @@ const char* mf_last_error(void);
  * Work runs on the handle's stream and is not synchronised. */
 int mf_solve_device_static(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev);
 
+/* ---- batches of independent matrices ------------------------------------ */
+
+/* Split the rows (elimination order) into nseg independent segments,
+ * segptr[0] = 0 <= segptr[1] <= ... <= segptr[nseg] = n.  Used when the
+ * handle holds a batch of matrices as one block-diagonal forest (their
+ * ChordalSymbolic arrays concatenated): the mixed refinement then measures
+ * the normwise backward error of every segment separately, refines with
+ * x += M^-1 (b - A x) so segments stay independent, and stops when the
+ * worst segment meets the tolerance.  nseg = 0 removes the split.
+ * No reference counterpart (the reference factors one matrix per object). */
+int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr);
+
+/* Per-segment backward error (worst right-hand side) of the last refined
+ * solve; eta has nseg entries. */
+int mf_segment_errors(mf_handle* h, double* eta);
+
 #ifdef __cplusplus
 }
 #endif
