@@ -35,8 +35,7 @@ def _stale(target, sources):
 
 
 def build_sym(verbose=False, force=False):
-    src = [os.path.join(CSRC, "symbolic.cpp"), os.path.join(CSRC, "amf.cpp")]
-    src = [s for s in src if os.path.exists(s)]
+    src = [os.path.join(CSRC, "symbolic.cpp"), os.path.join(CSRC, "mindeg.cpp")]
     hdr = [os.path.join(HERE, "..", "include", "cliquetrees_symbolic.h")]
     target = os.path.join(OUT, "libctsym.so")
     if force or _stale(target, src + hdr):

@@ -50,6 +50,7 @@ struct ct_symbolic {
 static thread_local std::string g_err;
 
 extern "C" const char* ct_last_error(void) { return g_err.c_str(); }
+void ct_set_error(const std::string& msg) { g_err = msg; }
 
 // ---------------------------------------------------------------------------
 // graph helpers

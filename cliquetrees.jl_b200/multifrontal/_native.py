@@ -50,9 +50,8 @@ def symlib() -> ctypes.CDLL:
         lib.ct_symbolic_arrays.restype = ctypes.c_int
         lib.ct_grid_nd_order.argtypes = [_i64, _i64, _i64, _i64, _p64]
         lib.ct_grid_nd_order.restype = ctypes.c_int
-        if hasattr(lib, "ct_amf_order"):
-            lib.ct_amf_order.argtypes = [_i64, _p64, _p64, _p64]
-            lib.ct_amf_order.restype = ctypes.c_int
+        lib.ct_mindeg_order.argtypes = [_i64, _p64, _p64, _p64]
+        lib.ct_mindeg_order.restype = ctypes.c_int
         lib.ct_last_error.argtypes = []
         lib.ct_last_error.restype = ctypes.c_char_p
         _sym = lib

@@ -146,30 +146,40 @@ def grid_nd_order(nx: int, ny: int, nz: int = 1, leaf: int = 8) -> np.ndarray:
     return order
 
 
-def amf_order(pattern: SymmetricPattern) -> np.ndarray:
-    """Approximate minimum fill order (AMFLib.amf, src/AMFLib.jl/src/AMFLib.jl:56-91)."""
+def mindeg_order(pattern) -> np.ndarray:
+    """Minimum-degree order (quotient graph, approximate external degrees;
+    Amestoy, Davis & Duff 1996), computed by ``libctsym``."""
+    pattern = as_pattern(pattern)
     lib = _native.symlib()
-    if not hasattr(lib, "ct_amf_order"):
-        raise NotImplementedError("AMF ordering is not available in this build")
     order = np.empty(pattern.n, np.int64)
-    rc = lib.ct_amf_order(pattern.n, _native.ptr64(pattern.colptr), _native.ptr64(pattern.rowval),
-                          _native.ptr64(order))
+    rc = lib.ct_mindeg_order(pattern.n, _native.ptr64(pattern.colptr), _native.ptr64(pattern.rowval),
+                             _native.ptr64(order))
     if rc != 0:
         raise RuntimeError(lib.ct_last_error().decode())
     return order
 
 
-def symbolic(A, alg="amf"):
+def amf_order(pattern) -> np.ndarray:
+    """The reference's default ordering is AMF (AMFLib.amf,
+    src/AMFLib.jl:56-91, approximate minimum fill); it is not restated in
+    this package, so this raises.  ``mindeg_order`` is the general-purpose
+    substitute."""
+    raise NotImplementedError("AMF is not restated in this package; use alg='mindeg' (minimum degree)")
+
+
+def symbolic(A, alg="mindeg"):
     """``symbolic(A; alg)`` (chordal_symbolic.jl:68-91) -> (Permutation, ChordalSymbolic).
 
-    ``alg`` is "amf" (the reference default, elimination_algorithms.jl:2380),
-    "natural", or an explicit order vector (0-based; order[i] = vertex
-    eliminated i-th), as `permutation(weights, graph, order)` accepts
-    (elimination_algorithms.jl:776-779)."""
+    ``alg`` is "mindeg" (minimum degree; stands in for the reference default
+    AMF, elimination_algorithms.jl:2380), "natural", or an explicit order
+    vector (0-based; order[i] = vertex eliminated i-th), as
+    `permutation(weights, graph, order)` accepts (elimination_algorithms.jl:776-779)."""
     pat = as_pattern(A)
     n = pat.n
     if isinstance(alg, str):
-        if alg == "amf":
+        if alg == "mindeg":
+            order = mindeg_order(pat)
+        elif alg == "amf":
             order = amf_order(pat)
         elif alg == "natural":
             order = np.arange(n, dtype=np.int64)
