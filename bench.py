@@ -1,23 +1,38 @@
-"""Benchmark: factor + solve of the 80^3 3D 7-point problem on the GPU.
+"""Benchmark: multifrontal factor + solve on the GPU (CliqueTrees.jl's
+Multifrontal numeric phase: chol_impl!, cholesky.jl:361-392; ldiv!!,
+divide.jl:1762-1764), on the synthetic configurations of the headline metric
+"solves/s and p99 latency at 1e-12 backward error, mixed/served vs plain
+FP64 GPU".
 
-One step = assemble the matrix values on the device, multifrontal Cholesky
-factorization, and a 4-right-hand-side solve (permutation included), the
-hot path of CliqueTrees.jl's Multifrontal numeric phase
-(chol_impl!, cholesky.jl:361-392; ldiv!!, divide.jl:1762-1764).
+--config 2 (default; the workload the metric is quoted on): 3D 7-point
+  Laplacian on an 80^3 grid (n = 512,000), seeded log-uniform [1e-3, 1e3]
+  coefficients, diagonal = row sum + 1e-6, geometric nested-dissection order,
+  4 N(0,1) right-hand sides.  One step = assemble the values on the device,
+  factor, 4-RHS solve (permutation included).  The factor (2-4 GB) is far
+  larger than L2, so no flush is needed between steps.
+--config 1: 2D 5-point 100x100, log-uniform [0.1, 10], diag + 1e-2, 1 RHS.
+--config 3: 4,096 2D 9-point matrices, side U{8..48}, weights U[0.5, 2],
+  diag + 1e-3, 4 RHS each, all factored as one forest (one step = the whole
+  batch; value counts matrices solved).
+--config 4: KKT [H A^T; A -1e-6 I], H = 40^3 7-point + 1e-4 I, A 16,000 x
+  64,000 with 6 N(0,1) entries per row; LDLt, static pivots, 8 RHS.
+--config 5: serving -- a Poisson stream of requests over 6 patterns (2D
+  5-point 64..512, 3D 7-point 16^3 and 48^3), 1-16 RHS, fresh coefficients;
+  value = requests/s of the served mixed batched form, with p50/p99.
+Orderings: geometric nested dissection for the grids of configs 2 and 5's
+3D patterns, minimum degree (the stand-in for the reference's AMF) for the
+others.
 
-Workload: 3D 7-point Laplacian on an 80^3 grid (n = 512,000), seeded
-log-uniform [1e-3, 1e3] edge coefficients, diagonal = row sum + 1e-6,
-geometric nested-dissection order, 4 N(0,1) right-hand sides; synthetic,
-the inputs (factor 3.4 GB) are far larger than L2.
-
-value      : solves/s (one solve = factor + 4-RHS solve of one system) with
-             the matrix values and right-hand sides already in HBM;
+value      : solves/s of the mixed form (FP32 fronts on tcgen05 tensor cores,
+             FP64 refinement to backward error <= 1e-12) with values and
+             right-hand sides already in HBM; the plain FP64 form is reported
+             beside it ("plain_fp64") with the same fields;
 e2e        : the same through the public C ABI with pinned host buffers
              (values + RHS copied in, solution copied out every step);
-roofline   : the dominant kernel (per-kernel CUDA events in a separate
-             profiling pass) against a DGEMM peak measured in this run;
+roofline   : the dominant kernel class (per-kernel CUDA events in a separate
+             profiling pass) against cuBLAS peaks measured in this run;
 cpu_baseline: the CPU oracle (C restatement of the reference path, scipy's
-             OpenBLAS, all host threads) on one full step.
+             OpenBLAS, all host threads) on a bounded sample of the workload.
 
 --impl reference times that CPU path alone (rank 0 only).
 Multi-GPU: every rank factors its own replica (no collective); value is
@@ -50,22 +65,87 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--side", type=int, default=80)
-    ap.add_argument("--nrhs", type=int, default=4)
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--side", type=int, default=None, help="grid side of configs 2 and 4 (default 80 / 40)")
+    ap.add_argument("--nrhs", type=int, default=None)
+    ap.add_argument("--batch", type=int, default=4096, help="config 3: matrices per batch")
+    ap.add_argument("--requests", type=int, default=600, help="config 5: requests per arrival rate")
+    ap.add_argument("--rates", default="50,200,1000", help="config 5: Poisson arrival rates (requests/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
     ap.add_argument("--mixed-profile", action="store_true", help="with --profile-only: the mixed form")
     return ap.parse_args()
 
 
-def workload(side, nrhs, seed=2):
+class Work:
+    """One configuration's synthetic input: the matrix (block-diagonal for a
+    batch), its symbolic analysis, the right-hand sides, and how to name it."""
+
+    def __init__(self, A, P, S, B, *, name, diag=0, segments=None, units=1, ordering="", sample=None):
+        self.A, self.P, self.S, self.B = A, P, S, B
+        self.name, self.diag, self.segments, self.units = name, diag, segments, units
+        self.ordering = ordering
+        self.sample = sample  # (A, P, S, B, scale) for the bounded CPU sample
+
+
+def workload(args, seed=2):
     import multifrontal as mf
     from multifrontal import testmatrices as tm
-    A = tm.config2(side, seed=seed)
-    order = mf.grid_nd_order(side, side, side, 8)
-    P, S = mf.symbolic(A, alg=order)
-    B = tm.rhs(A.shape[0], nrhs, seed=seed + 1)
-    return A, P, S, B
+    c = args.config
+    if c == 2:
+        side = args.side or 80
+        nrhs = args.nrhs or 4
+        A = tm.config2(side, seed=seed)
+        P, S = mf.symbolic(A, alg=mf.grid_nd_order(side, side, side, 8))
+        B = tm.rhs(A.shape[0], nrhs, seed=seed + 1)
+        # CPU sample: the same problem on a 48^3 grid, scaled by factor flops
+        ss = min(side, 48)
+        As = tm.config2(ss, seed=seed)
+        Ps, Ss = mf.symbolic(As, alg=mf.grid_nd_order(ss, ss, ss, 8))
+        return Work(A, P, S, B, name=f"3d7pt_{side}^3_chol_factor+solve_{nrhs}rhs", ordering="geometric ND",
+                    sample=(As, Ps, Ss, tm.rhs(As.shape[0], nrhs, seed=seed + 1),
+                            S.factor_flops() / Ss.factor_flops(), f"the same problem on a {ss}^3 grid"))
+    if c == 1:
+        nrhs = args.nrhs or 1
+        A = tm.config1(seed=1)
+        P, S = mf.symbolic(A, alg="mindeg")
+        B = tm.rhs(A.shape[0], nrhs, seed=5)
+        return Work(A, P, S, B, name=f"2d5pt_100^2_chol_factor+solve_{nrhs}rhs", ordering="minimum degree",
+                    sample=(A, P, S, B, 1.0, "the full problem"))
+    if c == 3:
+        import scipy.sparse as sp
+        from multifrontal import batch
+        nrhs = args.nrhs or 4
+        rng = np.random.default_rng(seed)
+        sides = rng.integers(8, 49, size=args.batch)
+        mats = [tm.config3_matrix(int(s), seed=1000 + i) for i, s in enumerate(sides)]
+        parts = [mf.symbolic(Ai, alg="mindeg") for Ai in mats]
+        P, S, off = batch.block_symbolic(parts)
+        A = sp.block_diag(mats, format="csc")
+        B = tm.rhs(S.n, nrhs, seed=7)
+        m = min(64, args.batch)
+        Ps, Ss, offs = batch.block_symbolic(parts[:m])
+        As = sp.block_diag(mats[:m], format="csc")
+        return Work(A, P, S, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
+                    segments=off, units=args.batch, ordering="minimum degree",
+                    sample=(As, Ps, Ss, tm.rhs(Ss.n, nrhs, seed=7), args.batch / m,
+                            f"the first {m} matrices of the batch, scaled by count"))
+    if c == 4:
+        side = args.side or 40
+        nrhs = args.nrhs or 8
+        m = 16000 * side ** 3 // 64000
+        A = tm.config4(side=side, m=m, seed=4)
+        P, S = mf.symbolic(A, alg="mindeg")
+        B = tm.rhs(A.shape[0], nrhs, seed=9)
+        ss = min(side, 20)
+        ms = 16000 * ss ** 3 // 64000
+        As = tm.config4(side=ss, m=ms, seed=4)
+        Ps, Ss = mf.symbolic(As, alg="mindeg")
+        return Work(A, P, S, B, name=f"kkt_{side}^3+{m}_ldlt_factor+solve_{nrhs}rhs", diag=1,
+                    ordering="minimum degree",
+                    sample=(As, Ps, Ss, tm.rhs(As.shape[0], nrhs, seed=9), S.factor_flops() / Ss.factor_flops(),
+                            f"the same construction with a {ss}^3 grid, scaled by factor flops"))
+    raise ValueError("config 5 has its own driver")
 
 
 class Clocks:
@@ -174,12 +254,18 @@ def kernel_flops(nn, na):
     }
 
 
-def cpu_reference_step(A, P, S, B):
+def cpu_sample(work):
+    """Time the CPU oracle on the bounded sample of the workload; returns
+    (seconds per full workload estimated from the sample, sample seconds,
+    description)."""
     from oracle import oracle
+    A, P, S, B, scale, what = work.sample
     t0 = time.perf_counter()
-    info, X, _ = oracle.factor_and_solve(A, P, S, B, 0)
+    info, X, _ = oracle.factor_and_solve(A, P, S, B, work.diag)
     dt = time.perf_counter() - t0
-    return dt, info, X
+    if info != 0:
+        raise SystemExit(f"bench: CPU oracle failed (info={info})")
+    return dt * scale, dt, what
 
 
 def run_reference(args, rank):
@@ -188,30 +274,59 @@ def run_reference(args, rank):
     from oracle import oracle
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    A, P, S, B = workload(args.side, args.nrhs)
+    if args.config == 5:
+        print(json.dumps({"impl": "reference", "metric": "requests_per_s",
+                          "unavailable": "the serving configuration has no CPU counterpart in the reference; "
+                                         "its CPU leg is reported inside the GPU arm's line"}), flush=True)
+        return
+    work = workload(args)
     for _ in range(args.warmup):
-        cpu_reference_step(A, P, S, B)
+        cpu_sample(work)
     times = []
+    sample_s = 0.0
+    what = ""
     for _ in range(args.steps):
-        dt, info, X = cpu_reference_step(A, P, S, B)
-        times.append(dt)
+        est, dt, what = cpu_sample(work)
+        times.append(est)
+        sample_s += dt
     tot = sum(times)
-    value = args.steps / tot
-    from multifrontal import testmatrices as tm
-    eta = float(tm.backward_error(A, X, B).max())
+    value = work.units * args.steps / tot
     line = {
         "impl": "reference", "metric": "solves_per_s", "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3d7pt_{args.side}^3_chol_factor+solve_{args.nrhs}rhs", "n": int(S.n),
-                   "factor_gflop": S.factor_flops() / 1e9, "ordering": "geometric nested dissection"},
-        "backward_error": eta,
+        "config": {"workload": work.name, "n": int(work.S.n), "factor_gflop": work.S.factor_flops() / 1e9,
+                   "ordering": work.ordering},
         "p50_ms": float(np.percentile(times, 50) * 1e3), "p99_ms": float(np.percentile(times, 99) * 1e3),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"full factor+solve of the {args.side}^3 system per step"},
+                         "sample": f"each step times {what} ({sample_s / args.steps:.2f} s) and scales it to "
+                                   f"the workload"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def roofline(form, peak, peak_src, fl, passes=1):
+    kt = form["kernels"]
+    classes = {
+        "syrk": (fl["syrk"], ["syrk"]),
+        "panel+update": (fl["panel+update"], ["panel", "update", "diag", "left"]),
+        "small": (fl["small"], ["small"]),
+    }
+    cls_ms = {k: sum(kt[x]["ms"] for x in v[1]) for k, v in classes.items()}
+    dom = max(cls_ms, key=cls_ms.get)
+    launches = sum(kt[x]["launches"] for x in classes[dom][1])
+    kms = cls_ms[dom]
+    achieved = classes[dom][0] / (kms / 1e3) / 1e12 if kms > 0 else 0.0
+    per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
+                     "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
+    out = {"kernel": dom, "bound": "tensor" if dom != "small" else "latency", "achieved": achieved,
+           "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+           "peak_source": peak_src, "flops_per_launch": classes[dom][0] / max(launches, 1),
+           "avg_launch_ms": kms / max(launches, 1), "classes": per_class}
+    if passes > 1:
+        out["mma_passes_per_product"] = passes
+    return out
 
 
 def main():
@@ -231,46 +346,33 @@ def main():
         return
 
     import torch
-    import multifrontal as mf
-    from multifrontal import _native
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    A, P, S, B = workload(args.side, args.nrhs)
+    if args.config == 5:
+        line = run_serving(args, local, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    work = workload(args)
 
     if args.profile_only:
-        r = run_form(args, A, P, S, B, mixed=args.mixed_profile, local=local, world=world, profile_only=True)
+        r = run_form(args, work, mixed=args.mixed_profile, local=local, world=world, profile_only=True)
         print(json.dumps(r))
         return
 
-    mixed = run_form(args, A, P, S, B, mixed=True, local=local, world=world)
-    plain = run_form(args, A, P, S, B, mixed=False, local=local, world=world)
+    mixed = run_form(args, work, mixed=True, local=local, world=world)
+    plain = run_form(args, work, mixed=False, local=local, world=world)
 
-    # roofline: the dominant kernel class of the headline (mixed) form
-    peaks = measured_peaks()
+    # roofline: the dominant kernel class of each form against cuBLAS peaks
+    # of the same arithmetic measured in this run
     dgemm = dgemm_peak_tflops(torch, dev)
-    sgemm = sgemm_peak_tflops(torch, dev)
-
-    def roofline(form, peak, peak_src, fl):
-        kt = form["kernels"]
-        classes = {
-            "syrk": (fl["syrk"], ["syrk"]),
-            "panel+update": (fl["panel+update"], ["panel", "update", "diag", "left"]),
-            "small": (fl["small"], ["small"]),
-        }
-        cls_ms = {k: sum(kt[x]["ms"] for x in v[1]) for k, v in classes.items()}
-        dom = max(cls_ms, key=cls_ms.get)
-        launches = sum(kt[x]["launches"] for x in classes[dom][1])
-        kms = cls_ms[dom]
-        achieved = classes[dom][0] / (kms / 1e3) / 1e12 if kms > 0 else 0.0
-        per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
-                         "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
-        return {"kernel": dom, "bound": "tensor" if dom != "small" else "latency", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
-                "peak_source": peak_src, "flops_per_launch": classes[dom][0] / max(launches, 1),
-                "avg_launch_ms": kms / max(launches, 1), "classes": per_class}
-
-    roof_mixed = roofline(mixed, sgemm, "cuBLAS SGEMM 8192^3 (FP32, TF32 off) measured in this run", mixed["flops"])
+    tf32 = gemm_peak_tflops(torch, dev, torch.float32, allow_tf32=True)
+    roof_mixed = roofline(mixed, tf32, "cuBLAS TF32 GEMM 8192^3 measured in this run (the kernels run 3 TF32 "
+                                       "MMA passes per product: hi*hi + hi*lo + lo*hi)", mixed["flops"], passes=3)
     roof_plain = roofline(plain, dgemm, "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
                                         "MEASURED_PEAKS.json)", plain["flops"])
 
@@ -279,19 +381,22 @@ def main():
         from oracle import oracle
         threads = os.cpu_count() or 1
         oracle.set_threads(threads)
-        dt, cinfo, _ = cpu_reference_step(A, P, S, B)
-        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": f"one full FP64 factor+{args.nrhs}-RHS solve of the {args.side}^3 system ({dt:.2f} s)"}
+        est, dt, what = cpu_sample(work)
+        cpu = {"value": work.units / est, "unit": "solves/s", "cores": threads, "kind": "port",
+               "sample": f"{what}: {dt:.2f} s for FP64 factor+solve, scaled to {est:.1f} s for the workload"}
 
     if rank == 0:
         line = {
             "metric": "solves_per_s", "value": mixed["value"], "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"3d7pt_{args.side}^3_chol_factor+solve_{args.nrhs}rhs", "n": int(S.n),
-                       "fronts": int(S.nfr), "factor_gflop": S.factor_flops() / 1e9, "nnz_L": int(S.nnz()),
-                       "mode": "mixed: FP32 fronts + FP64 PCG to backward error 1e-12",
-                       "l2": "inputs larger than L2 (factor 2-4 GB)", "parallelism": f"replicas x{world}"},
+            "config": {"workload": work.name, "n": int(work.S.n), "fronts": int(work.S.nfr),
+                       "factor_gflop": work.S.factor_flops() / 1e9, "nnz_L": int(work.S.nnz()),
+                       "ordering": work.ordering, "matrices_per_step": work.units,
+                       "mode": "mixed: FP32 fronts (3xTF32 tcgen05) + FP64 refinement to backward error 1e-12",
+                       "l2": "inputs larger than L2" if work.S.nnz() * 4 > 126e6 else
+                             "working set fits L2 (no flush: a step rewrites every factor entry)",
+                       "parallelism": f"replicas x{world}"},
             "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"], "backward_error": mixed["backward_error"],
             "refine_iterations": mixed["iterations"],
             "e2e": mixed["e2e"],
@@ -312,13 +417,13 @@ def main():
         dist.destroy_process_group()
 
 
-def sgemm_peak_tflops(torch, dev):
-    """cuBLAS SGEMM 8192^3 with TF32 disabled, best of 5 (the FP32 denominator)."""
+def gemm_peak_tflops(torch, dev, dtype, allow_tf32=False):
+    """cuBLAS GEMM 8192^3 in `dtype`, best of 5."""
     keep = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = allow_tf32
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float32, device=dev)
-    b = torch.randn(n, n, dtype=torch.float32, device=dev)
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e9
@@ -336,7 +441,114 @@ def sgemm_peak_tflops(torch, dev):
     return 2.0 * n ** 3 / best / 1e12
 
 
-def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
+def seg_backward_error(A, X, B, segments=None):
+    """Worst normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+    over the columns and, for a batch, over the matrices (row segments)."""
+    X = np.asarray(X).reshape(A.shape[0], -1)
+    B = np.asarray(B).reshape(A.shape[0], -1)
+    R = np.abs(B - A @ X)
+    rows = np.asarray(abs(A).sum(axis=1)).ravel()
+    off = np.asarray([0, A.shape[0]] if segments is None else segments, dtype=np.int64)[:-1]
+    an = np.maximum.reduceat(rows, off)[:, None]
+    rm = np.maximum.reduceat(R, off, axis=0)
+    xm = np.maximum.reduceat(np.abs(X), off, axis=0)
+    bm = np.maximum.reduceat(np.abs(B), off, axis=0)
+    return float((rm / (an * xm + bm)).max())
+
+
+def run_serving(args, local, world):
+    """Config 5: a Poisson stream of factor+solve requests over six patterns
+    through the serving loop (multifrontal.serve), swept over arrival rate;
+    beside it the plain FP64 form, one request at a time on one stream."""
+    import multifrontal as mf
+    from multifrontal import serve
+    from multifrontal import testmatrices as tm
+
+    specs = {  # key: (grid, batch per handle, ordering)
+        "2d5pt_64": ((64, 64, 1), 16, "mindeg"), "2d5pt_128": ((128, 128, 1), 8, "mindeg"),
+        "2d5pt_256": ((256, 256, 1), 2, "mindeg"), "2d5pt_512": ((512, 512, 1), 1, "mindeg"),
+        "3d7pt_16": ((16, 16, 16), 16, "nd"), "3d7pt_48": ((48, 48, 48), 1, "nd"),
+    }
+    pools = {}   # per pattern: 4 seeded coefficient sets (log-uniform [0.1, 10], diag + 1e-2)
+    mats = {}
+    for k, ((nx, ny, nz), _, _) in specs.items():
+        mats[k] = [tm.grid_laplacian(nx, ny, nz, seed=100 + s, lo=0.1, hi=10.0, shift=1e-2) for s in range(4)]
+    rhs_cache = {}
+
+    def rhs_for(n, kk):
+        if (n, kk) not in rhs_cache:
+            rhs_cache[(n, kk)] = tm.rhs(n, kk, seed=kk)
+        return rhs_cache[(n, kk)]
+
+    def make_server(mixed, batched, workers):
+        srv = serve.Server(mixed=mixed, device=local, workers=workers)
+        for k, ((nx, ny, nz), b, o) in specs.items():
+            order = mf.grid_nd_order(nx, ny, nz) if o == "nd" else "mindeg"
+            srv.add_pattern(k, mats[k][0], order=order, batch=b if batched else 1)
+            if k not in pools:
+                pools[k] = [srv.lower_values(k, A) for A in mats[k]]
+        return srv
+
+    def stream(count, rate, seed):
+        rng = np.random.default_rng(seed)
+        keys = list(specs)
+        t, reqs = 0.0, []
+        for i in range(count):
+            k = keys[rng.integers(len(keys))]
+            n = mats[k][0].shape[0]
+            kk = int(rng.integers(1, 17))
+            t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
+            reqs.append(serve.Request(i, k, pools[k][i % 4], rhs_for(n, kk), arrival=t))
+        return reqs
+
+    def check(done):
+        worst = 0.0
+        for r in done[:: max(1, len(done) // 40)]:
+            A = mats[r.key][r.rid % 4]
+            worst = max(worst, float(tm.backward_error(A, r.X, r.B).max()))
+        return worst
+
+    rates = [float(x) for x in args.rates.split(",") if x]
+    srv = make_server(True, True, 4)
+    srv.warm()
+    sweep = []
+    for rate in rates:
+        reqs = stream(args.requests, rate, seed=int(rate))
+        done = srv.serve(reqs, realtime=True)
+        st = serve.latency_stats(done)
+        sweep.append({"rate": rate, "requests": len(done), "requests_per_s": len(done) / srv.wall,
+                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "backward_error": check(done),
+                      "mean_batch": float(np.mean([r.batch_size for r in done]))})
+    sat_reqs = stream(args.requests, 0.0, seed=1)
+    done = srv.serve(sat_reqs, realtime=False)
+    sat = {"requests_per_s": len(done) / srv.wall, "backward_error": check(done),
+           **serve.latency_stats(done), "mean_batch": float(np.mean([r.batch_size for r in done]))}
+    srv.close()
+    plain = make_server(False, False, 1)
+    plain.warm()
+    m = max(60, args.requests // 5)
+    done_p = plain.serve(stream(m, 0.0, seed=1), realtime=False)
+    plain_line = {"requests_per_s": len(done_p) / plain.wall, "requests": len(done_p),
+                  "backward_error": check(done_p), **serve.latency_stats(done_p)}
+    plain.close()
+    return {
+        "metric": "requests_per_s", "value": sat["requests_per_s"], "unit": "requests/s", "n_gpus": world,
+        "steps": args.requests, "warmup": 1, "ms_per_step": 1e3 / sat["requests_per_s"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "serving_6patterns_poisson", "patterns": {k: {"grid": v[0], "batch": v[1],
+                                                                              "ordering": v[2]}
+                                                                          for k, v in specs.items()},
+                   "rhs_per_request": "U{1..16}", "coefficients": "4 seeded log-uniform [0.1,10] sets per pattern",
+                   "mem_cap_gb": 120, "workers": 4},
+        "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"], "backward_error": sat["backward_error"],
+        "saturation": sat, "sweep": sweep, "plain_fp64_one_at_a_time": plain_line,
+        "served_over_plain": sat["requests_per_s"] / plain_line["requests_per_s"],
+        "e2e": {"value": sat["requests_per_s"], "unit": "requests/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None, "note": "every request moves its values and RHS from host buffers"},
+    }
+
+
+def run_form(args, work, *, mixed, local, world, profile_only=False):
     """Time one form (mixed or plain FP64) of the step; returns a dict."""
     import torch
     import multifrontal as mf
@@ -344,11 +556,18 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
     from multifrontal import testmatrices as tm
     from multifrontal.sparse import assembly_map
 
+    A, P, S, B = work.A, work.P, work.S, work.B
+    nrhs = B.shape[1]
     dev = torch.device("cuda", local)
     n = S.n
-    F = mf.ChordalCholesky(A, P, S, device=local, nrhs_cap=16, mixed=mixed)
+    cls = mf.ChordalLDLt if work.diag else mf.ChordalCholesky
+    F = cls(A, P, S, device=local, nrhs_cap=16, mixed=mixed)
     lib = _native.gpulib()
     h = F._handle.h
+    if work.segments is not None:
+        _native.check(lib.mf_set_segments(h, len(work.segments) - 1,
+                                          _native.ptr64(np.ascontiguousarray(work.segments, dtype=np.int64))),
+                      "mf_set_segments")
     stream = torch.cuda.Stream(device=dev)
     _native.check(lib.mf_set_stream(h, ctypes.c_void_p(stream.cuda_stream)), "mf_set_stream")
     Lo, _ = assembly_map(S, P.invp, A)
@@ -374,12 +593,12 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
         _native.check(lib.mf_assemble_device(h, vp(nz_dev.data_ptr())), "assemble")
         if mixed:
             _native.check(lib.mf_factorize_mixed(h, None, ctypes.byref(info), ctypes.byref(fp64)), "factorize")
-            _native.check(lib.mf_solve_refined_device(h, vp(X_dev.data_ptr()), args.nrhs, n, vp(perm_dev.data_ptr()),
+            _native.check(lib.mf_solve_refined_device(h, vp(X_dev.data_ptr()), nrhs, n, vp(perm_dev.data_ptr()),
                                                       tol, maxit, ctypes.byref(iters), ctypes.byref(eta_dev)),
                           "solve")
         else:
             _native.check(lib.mf_factorize(h, None, None), "factorize")
-            _native.check(lib.mf_solve_device(h, vp(X_dev.data_ptr()), args.nrhs, n, vp(perm_dev.data_ptr())),
+            _native.check(lib.mf_solve_device(h, vp(X_dev.data_ptr()), nrhs, n, vp(perm_dev.data_ptr())),
                           "solve")
 
     def step_e2e():
@@ -387,17 +606,17 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
         X_host.copy_(B_host)
         if mixed:
             _native.check(lib.mf_factorize_mixed(h, None, ctypes.byref(info), ctypes.byref(fp64)), "factorize")
-            _native.check(lib.mf_solve_refined(h, ctypes.cast(X_host.data_ptr(), pd), args.nrhs, n, None, tol, maxit,
+            _native.check(lib.mf_solve_refined(h, ctypes.cast(X_host.data_ptr(), pd), nrhs, n, None, tol, maxit,
                                                ctypes.byref(iters), ctypes.byref(eta_dev)), "solve")
         else:
             _native.check(lib.mf_factorize(h, None, ctypes.byref(info)), "factorize")
-            _native.check(lib.mf_solve(h, ctypes.cast(X_host.data_ptr(), pd), args.nrhs, n, None), "solve")
+            _native.check(lib.mf_solve(h, ctypes.cast(X_host.data_ptr(), pd), nrhs, n, None), "solve")
 
     with torch.cuda.stream(stream):
         step_device()
     stream.synchronize()
-    X = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
-    eta = float(tm.backward_error(A, X, B).max())
+    X = X_dev.cpu().numpy().reshape(n, nrhs, order="F")
+    eta = seg_backward_error(A, X, B, work.segments)
     if profile_only:
         F.close()
         return {"profile_only": True, "mixed": mixed, "n": int(n), "backward_error": eta,
@@ -453,9 +672,9 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
         t = torch.tensor([total_s], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_s = float(t.item())
-    value = world * args.steps / total_s
-    Xt = X_dev.cpu().numpy().reshape(n, args.nrhs, order="F")
-    eta_t = float(tm.backward_error(A, Xt, B).max())
+    value = world * work.units * args.steps / total_s
+    Xt = X_dev.cpu().numpy().reshape(n, nrhs, order="F")
+    eta_t = seg_backward_error(A, Xt, B, work.segments)
 
     # e2e pass through the host-buffer C ABI
     for _ in range(args.warmup):
@@ -473,9 +692,9 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
         t = torch.tensor([e2e_total], dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
-    e2e_value = world * args.steps / e2e_total
-    Xe = X_host.numpy().reshape(n, args.nrhs, order="F")
-    eta_e2e = float(tm.backward_error(A, Xe, B).max())
+    e2e_value = world * work.units * args.steps / e2e_total
+    Xe = X_host.numpy().reshape(n, nrhs, order="F")
+    eta_e2e = seg_backward_error(A, Xe, B, work.segments)
     F.close()
     del F
     torch.cuda.empty_cache()
@@ -483,8 +702,8 @@ def run_form(args, A, P, S, B, *, mixed, local, world, profile_only=False):
         "value": value, "ms_per_step": 1e3 * total_s / args.steps,
         "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
         "backward_error": max(eta, eta_t), "iterations": its if mixed else None,
-        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nz_host.numel() * 8 + n * args.nrhs * 8),
-                "d2h_bytes_per_step": int(n * args.nrhs * 8 + 8), "backward_error": eta_e2e,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nz_host.numel() * 8 + n * nrhs * 8),
+                "d2h_bytes_per_step": int(n * nrhs * 8 + 8), "backward_error": eta_e2e,
                 "p50_ms": float(np.percentile(e2e_ms, 50)), "p99_ms": float(np.percentile(e2e_ms, 99))},
         "gpu_launches": launches_per_step * args.steps, "kernels": ktimes, "clocks": ck, "flops": fl,
     }

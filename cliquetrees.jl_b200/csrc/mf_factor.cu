@@ -740,7 +740,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 // single precision: the GEMM roles run on the tcgen05 tensor cores
                 const FactorBufs<float>& f32b = reinterpret_cast<const FactorBufs<float>&>(fb);
                 int rc;
-                {
+                if (st.left_tc.cnt) {
                     Timer t(h, K_LEFT);
                     if ((rc = tc_launch(h, 0, st.left_tc, st.b, c0, f32b))) return rc;
                 }
@@ -750,11 +750,11 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                         h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info);
                     MF_CUDA(cudaGetLastError());
                 }
-                {
+                if (st.panel_tc.cnt) {
                     Timer t(h, K_PANEL);
                     if ((rc = tc_launch(h, 3, st.panel_tc, st.b, c0, f32b))) return rc;
                 }
-                {
+                if (st.trail_tc.cnt) {
                     Timer t(h, K_UPDATE);
                     if ((rc = tc_launch(h, 1, st.trail_tc, st.b, c0, f32b))) return rc;
                 }
@@ -786,6 +786,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             }
         }
         if (std::is_same<T, float>::value && h->use_tc) {
+            if (!lv.syrk_tc.cnt) continue;
             Timer t(h, K_SYRK);
             int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
             if (rc) return rc;

@@ -1,0 +1,81 @@
+"""Host logic of the serving loop, with the device batch replaced by a fake
+(no GPU): every request completes once, requests of one pattern share
+batches, the memory cap evicts idle handles, and a handle larger than the
+cap runs alone instead of waiting forever."""
+import time
+
+import numpy as np
+
+import multifrontal as mf
+from multifrontal import serve
+from multifrontal import testmatrices as tm
+
+
+class FakeBatch:
+    def __init__(self, pat, mixed, device, tol, maxit):
+        self.pat = pat
+        self.bytes = pat.S.n * 1000 * pat.batch
+        self.busy = False
+        self.last_used = 0.0
+
+    def run(self, reqs):
+        time.sleep(0.001)
+        for r in reqs:
+            r.X = np.zeros_like(r.B)
+            r.eta = 0.0
+            r.batch_size = len(reqs)
+
+    def close(self):
+        pass
+
+
+PATS = {
+    "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "mindeg", 4),
+    "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "mindeg", 4),
+    "g3d6": (lambda s: tm.grid_laplacian(6, 6, 6, seed=s), "natural", 2),
+}
+
+
+def _server(monkeypatch, workers):
+    monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
+    srv = serve.Server(mixed=False, workers=workers)
+    for k, (gen, order, batch) in PATS.items():
+        srv.add_pattern(k, gen(0), order=order, batch=batch)
+    return srv
+
+
+def _requests(srv, count, seed, spacing=0.0):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        k = list(PATS)[rng.integers(len(PATS))]
+        A = PATS[k][0](1000 + i)
+        reqs.append(serve.Request(i, k, srv.lower_values(k, A), np.ones((A.shape[0], 2)), arrival=spacing * i))
+    return reqs
+
+
+def test_all_requests_complete_and_batch(monkeypatch):
+    srv = _server(monkeypatch, workers=3)
+    done = srv.serve(_requests(srv, 40, seed=1), realtime=False, timeout=30)
+    assert sorted(r.rid for r in done) == list(range(40))
+    assert max(r.batch_size for r in done) > 1
+    for r in done:
+        assert r.batch_size <= srv.patterns[r.key].batch
+    st = serve.latency_stats(done)
+    assert st["p99_ms"] >= st["p50_ms"] >= 0
+
+
+def test_memory_cap_evicts_and_oversize_runs_alone(monkeypatch):
+    srv = _server(monkeypatch, workers=1)
+    srv.warm(["g2d12"])
+    srv.mem_cap = srv.bytes * 1.5  # g2d20's handle alone exceeds the cap
+    done = srv.serve(_requests(srv, 15, seed=3), realtime=False, timeout=30)
+    assert len(done) == 15
+    resident = [h for p in srv.patterns.values() for h in p.handles]
+    assert len(resident) == 1 or srv.bytes <= srv.mem_cap
+
+
+def test_realtime_arrivals_are_respected(monkeypatch):
+    srv = _server(monkeypatch, workers=2)
+    done = srv.serve(_requests(srv, 10, seed=5, spacing=0.01), realtime=True, timeout=30)
+    assert all(r.done >= r.arrival for r in done)
