@@ -82,6 +82,7 @@ class Work:
     batch), its symbolic analysis, the right-hand sides, and how to name it."""
 
     def __init__(self, A, P, S, B, *, name, diag=0, segments=None, units=1, ordering="", sample=None):
+        self.members = None  # batch: (matrices, symbolics) of the members
         self.A, self.P, self.S, self.B = A, P, S, B
         self.name, self.diag, self.segments, self.units = name, diag, segments, units
         self.ordering = ordering
@@ -126,10 +127,12 @@ def workload(args, seed=2):
         m = min(64, args.batch)
         Ps, Ss, offs = batch.block_symbolic(parts[:m])
         As = sp.block_diag(mats[:m], format="csc")
-        return Work(A, P, S, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
-                    segments=off, units=args.batch, ordering="minimum degree",
-                    sample=(As, Ps, Ss, tm.rhs(Ss.n, nrhs, seed=7), args.batch / m,
-                            f"the first {m} matrices of the batch, scaled by count"))
+        w = Work(A, P, S, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
+                 segments=off, units=args.batch, ordering="minimum degree",
+                 sample=(As, Ps, Ss, tm.rhs(Ss.n, nrhs, seed=7), args.batch / m,
+                         f"the first {m} matrices of the batch, scaled by count"))
+        w.members = (mats, parts)
+        return w
     if c == 4:
         side = args.side or 40
         nrhs = args.nrhs or 8
@@ -366,6 +369,7 @@ def main():
 
     mixed = run_form(args, work, mixed=True, local=local, world=world)
     plain = run_form(args, work, mixed=False, local=local, world=world)
+    unbatched = time_unbatched(work, local) if work.members is not None else None
 
     # roofline: the dominant kernel class of each form against cuBLAS peaks
     # of the same arithmetic measured in this run
@@ -411,6 +415,9 @@ def main():
             "mixed_over_plain": mixed["value"] / plain["value"],
             "cpu_baseline": cpu,
         }
+        if unbatched is not None:
+            line["plain_fp64_one_matrix_at_a_time"] = unbatched
+            line["mixed_batched_over_unbatched_plain"] = mixed["value"] / unbatched["value"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -548,6 +555,46 @@ def run_serving(args, local, world):
     }
 
 
+def time_unbatched(work, local, count=64):
+    """The plain FP64 form without batching: the first `count` members of a
+    batch, each its own handle (pattern cached), factored and solved one
+    after the other (device-resident values and right-hand sides)."""
+    import torch
+    import multifrontal as mf
+    from multifrontal import _native
+    from multifrontal.sparse import assembly_map
+    mats, parts = work.members
+    nrhs = work.B.shape[1]
+    lib = _native.gpulib()
+    jobs = []
+    for A, (P, S) in list(zip(mats, parts))[:count]:
+        F = mf.ChordalCholesky(A, P, S, device=local, nrhs_cap=16)
+        Lo, _ = assembly_map(S, P.invp, A)
+        nz = torch.from_numpy(np.ascontiguousarray(Lo.data)).to(f"cuda:{local}")
+        X = torch.ones(S.n * nrhs, dtype=torch.float64, device=f"cuda:{local}")
+        perm = torch.from_numpy(P.perm.astype(np.int64)).to(f"cuda:{local}")
+        jobs.append((F, nz, X, perm, S.n))
+    vp = ctypes.c_void_p
+
+    def one(F, nz, X, perm, n):
+        h = F._handle.h
+        _native.check(lib.mf_assemble_device(h, vp(nz.data_ptr())), "assemble")
+        _native.check(lib.mf_factorize(h, None, None), "factorize")
+        _native.check(lib.mf_solve_device(h, vp(X.data_ptr()), nrhs, n, vp(perm.data_ptr())), "solve")
+        _native.check(lib.mf_synchronize(h), "sync")
+
+    for j in jobs:  # warm-up: plans, graphs
+        one(*j)
+    t0 = time.perf_counter()
+    for j in jobs:
+        one(*j)
+    dt = time.perf_counter() - t0
+    for j in jobs:
+        j[0].close()
+    return {"value": len(jobs) / dt, "unit": "solves/s", "matrices_timed": len(jobs),
+            "note": "one handle per matrix, factor+solve one matrix after the other"}
+
+
 def run_form(args, work, *, mixed, local, world, profile_only=False):
     """Time one form (mixed or plain FP64) of the step; returns a dict."""
     import torch
@@ -629,7 +676,9 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
     if mixed:
         _native.check(lib.mf_solve_refined(h, _native.ptrd(Xtmp), 0, n, _native.ptr64(perm_np), tol, maxit,
                                            ctypes.byref(iters), ctypes.byref(eta_dev)), "perm upload")
-    if info.value != 0 or not eta <= 1e-12:
+    # the mixed form must reach 1e-12; the plain FP64 form is the reference's
+    # arithmetic (static pivots for LDLt), so it only has to be a solution
+    if info.value != 0 or not eta <= (1e-12 if mixed else 1e-8):
         raise SystemExit(f"bench: check failed (mixed={mixed}, info={info.value}, backward error={eta})")
 
     # profiling pass (per-kernel events; not the timed pass)

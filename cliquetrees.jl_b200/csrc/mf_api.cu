@@ -50,7 +50,7 @@ void free_all(mf_handle* h) {
                     h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
-                    h->d_segeta};
+                    h->d_segeta, h->d_kry};
     release_graphs(h);
     for (void* p : ptrs)
         if (p) cudaFree(p);

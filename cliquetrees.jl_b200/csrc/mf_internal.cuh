@@ -228,6 +228,8 @@ struct mf_handle {
     int64_t* d_csrsrc = nullptr;   // index of each entry among the stored values
     int64_t nnz_full = 0;
     double* d_iv = nullptr;        // refinement vectors: b, x, r, z, p, q (6 * n * nrhs_cap)
+    double* d_kry = nullptr;       // GMRES bases V, Z and partial sums (allocated on first use)
+    int64_t kry_doubles = 0;
     double* d_red = nullptr;       // reductions and scalars (see mf_refine.cu)
     const double* cur_nz = nullptr; // values of the current matrix (device)
     bool mixed_fallback = false;   // FP32 factorization failed; the FP64 factor is used

@@ -6,10 +6,16 @@
 // supernodal solve.  FP64 stays in the residual b - A x (CSR of the original
 // values, elimination order), the solution update and the scalars:
 //   Cholesky : preconditioned conjugate gradients, one CG per right-hand side;
-//   LDLt, and any handle split into row segments (a batch of independent
-//   matrices): classical iterative refinement x += M^-1 (b - A x), which
-//   keeps the segments independent; the backward error is then measured per
-//   segment and the loop runs until the worst segment meets the tolerance.
+//   LDLt      : right-preconditioned restarted GMRES (GMRES-IR; the FP32
+//               LDLt factor of an indefinite matrix is no SPD preconditioner,
+//               and classical refinement stalls when kappa * eps32 is near 1),
+//               classical Gram-Schmidt applied twice, one Krylov space per
+//               right-hand side;
+//   any handle split into row segments (a batch of independent matrices):
+//               classical iterative refinement x += M^-1 (b - A x), which
+//               keeps the segments independent; the backward error is then
+//               measured per segment and the loop runs until the worst
+//               segment meets the tolerance.
 // Every iteration measures the normwise backward error
 //   eta = ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
 // per column and stops when all columns reach the tolerance.  Reductions are
@@ -135,9 +141,10 @@ __global__ void k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __re
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 48; ++q) {
+        if ((q & 15) >= nrhs) continue;  // uniform across the block
         double v = m[q];
         for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((threadIdx.x & 31) == 0 && (q & 15) < nrhs) atomic_max_nonneg(mx + q, v);
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(mx + q, v);
     }
     __syncthreads();
     if (threadIdx.x < 48) segred[s * kSegRed + threadIdx.x] = mx[threadIdx.x];
@@ -289,6 +296,66 @@ __global__ void k_from32(double* __restrict__ z, const float* __restrict__ c, co
     }
 }
 
+// ---------------------------------------------------------------------------
+// GMRES kernels.  Krylov vectors V_i / Z_i are n x nrhs blocks (ld n) spaced
+// `vs` doubles apart; coefficient arrays are indexed [i * 16 + r].
+// ---------------------------------------------------------------------------
+constexpr int kGmresM = 24;  // restart length
+
+// part[(blk * J + i) * 16 + r] = this block's share of <V_i(:, r), w(:, r)>
+__global__ void k_mdot_part(const double* __restrict__ V, int64_t vs, int J, const double* __restrict__ w,
+                            double* __restrict__ part, int64_t n, int nrhs) {
+    __shared__ double sh[256];
+    for (int i = 0; i < J; ++i)
+        for (int r = 0; r < nrhs; ++r) {
+            const double* v = V + i * vs + (int64_t)r * n;
+            const double* ww = w + (int64_t)r * n;
+            double s = 0.0;
+            for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+                s += v[k] * ww[k];
+            sh[threadIdx.x] = s;
+            __syncthreads();
+            for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+                if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) part[((int64_t)blockIdx.x * J + i) * 16 + r] = sh[0];
+            __syncthreads();
+        }
+}
+
+// out[i * 16 + r] = sum over blocks (fixed order)
+__global__ void k_mdot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int J,
+                             int nrhs) {
+    for (int o = threadIdx.x; o < J * 16; o += blockDim.x) {
+        const int i = o / 16, r = o % 16;
+        if (r >= nrhs) continue;
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += part[((int64_t)b * J + i) * 16 + r];
+        out[o] = s;
+    }
+}
+
+// w(:, r) -= sum_{i < J} c[i * 16 + r] V_i(:, r)
+__global__ void k_mupd(double* __restrict__ w, const double* __restrict__ V, int64_t vs, int J,
+                       const double* __restrict__ c, int64_t n, int nrhs) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(k / n);
+        double s = 0.0;
+        for (int i = 0; i < J; ++i) s += c[i * 16 + r] * V[i * vs + k];
+        w[k] -= s;
+    }
+}
+
+// dst(:, r) = src(:, r) * c[r]
+__global__ void k_colscale(double* __restrict__ dst, const double* __restrict__ src, const double* __restrict__ c,
+                           int64_t n, int nrhs) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
+         k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[k] * c[k / n];
+}
+
 static unsigned gs_blocks(int64_t work) {
     int64_t b = (work + 255) / 256;
     if (b > 148 * 8) b = 148 * 8;
@@ -320,7 +387,8 @@ static int dot(mf_handle* h, const double* u, const double* v, double* out, int 
 }
 
 // backward error per column into eta[] (host); t receives b - A x when non-null
-static int backward_error(mf_handle* h, const double* x, const double* b, double* t, int nrhs, double* eta) {
+static int backward_error(mf_handle* h, const double* x, const double* b, double* t, int nrhs, double* eta,
+                          double* maxima = nullptr) {
     Timer tm(h, K_SPMV);
     double* red = h->d_red;  // [0..48) maxima, [48] ||A||_inf
     if (h->nseg > 0) {
@@ -344,6 +412,138 @@ static int backward_error(mf_handle* h, const double* x, const double* b, double
         double den = hred[48] * hred[16 + r] + hred[32 + r];
         eta[r] = den > 0.0 ? hred[r] / den : (hred[r] > 0.0 ? INFINITY : 0.0);
     }
+    if (maxima)
+        for (int q = 0; q < 49; ++q) maxima[q] = hred[q];
+    return 0;
+}
+
+// Right-preconditioned restarted GMRES, M^-1 = the FP32 factor solve; one
+// Krylov space per right-hand side, all columns advanced together.  Returns
+// the total number of preconditioner applications in *iters.
+static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters,
+                 double* eta_out) {
+    const int64_t n = h->n;
+    const int M = kGmresM;
+    const int64_t vs = n * nrhs;
+    const int nblk = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 255) / 256));
+    const int64_t need = (int64_t)(2 * M + 1) * n * h->nrhs_cap + (int64_t)148 * 4 * (M + 1) * 16 + 64 * 16;
+    if (h->kry_doubles < need) {
+        if (h->d_kry) cudaFree(h->d_kry);
+        h->d_kry = nullptr;
+        h->kry_doubles = 0;
+        MF_CUDA(cudaMalloc(&h->d_kry, sizeof(double) * need));
+        h->kry_doubles = need;
+        h->bytes += (int64_t)sizeof(double) * need;
+    }
+    double* V = h->d_kry;                                    // M + 1 blocks
+    double* Z = V + (int64_t)(M + 1) * n * h->nrhs_cap;      // M blocks
+    double* part = Z + (int64_t)M * n * h->nrhs_cap;         // nblk * (M + 1) * 16
+    double* coef = part + (int64_t)148 * 4 * (M + 1) * 16;   // (M + 1) * 16 coefficients
+    double* R = h->d_iv + 2 * (int64_t)n * h->nrhs_cap;      // residual
+    double eta[16], mx[49];
+    std::vector<double> H((size_t)(M + 1) * M * 16), g((size_t)(M + 1) * 16), cs((size_t)M * 16), sn((size_t)M * 16);
+    std::vector<double> hc((size_t)(M + 1) * 16), beta(16), tgt(16);
+    int rc, used = 0;
+    double worst = INFINITY;
+    MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
+    auto mdot = [&](const double* Vb, int J, const double* w, double* out_host) -> int {
+        k_mdot_part<<<nblk, 256, 0, h->stream>>>(Vb, vs, J, w, part, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+        k_mdot_final<<<1, 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
+        MF_CUDA(cudaGetLastError());
+        MF_CUDA(cudaMemcpyAsync(out_host, coef, sizeof(double) * J * 16, cudaMemcpyDeviceToHost, h->stream));
+        MF_CUDA(cudaStreamSynchronize(h->stream));
+        return 0;
+    };
+    while (true) {
+        // true residual and backward error of the current x
+        if ((rc = backward_error(h, x, b, R, nrhs, eta, mx))) return rc;
+        worst = 0.0;
+        for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
+        if (worst <= tol || used >= maxit) break;
+        // target on ||r||_2 (>= ||r||_inf): half the tolerance at the current scale
+        for (int r = 0; r < nrhs; ++r) tgt[r] = 0.5 * tol * (mx[48] * mx[16 + r] + mx[32 + r]);
+        if ((rc = mdot(R, 1, R, hc.data()))) return rc;
+        for (int r = 0; r < nrhs; ++r) beta[r] = std::sqrt(std::max(hc[r], 0.0));
+        for (int r = 0; r < 16; ++r) hc[r] = (r < nrhs && beta[r] > 0.0) ? 1.0 / beta[r] : 0.0;
+        MF_CUDA(cudaMemcpyAsync(coef, hc.data(), sizeof(double) * 16, cudaMemcpyHostToDevice, h->stream));
+        k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(V, R, coef, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+        std::fill(H.begin(), H.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        for (int r = 0; r < nrhs; ++r) g[r] = beta[r];
+        int j = 0;
+        bool stop = false;
+        for (; j < M && !stop && used < maxit; ++j) {
+            double* Vj = V + j * vs;
+            double* Zj = Z + j * vs;
+            double* w = V + (j + 1) * vs;
+            if ((rc = apply_prec<false>(h, Vj, Zj, nrhs))) return rc;
+            ++used;
+            {
+                Timer tm(h, K_SPMV);
+                k_spmv<<<row_blocks(n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Zj, w,
+                                                              n, nrhs);
+                MF_CUDA(cudaGetLastError());
+            }
+            // classical Gram-Schmidt, twice
+            for (int pass = 0; pass < 2; ++pass) {
+                if ((rc = mdot(V, j + 1, w, hc.data()))) return rc;
+                MF_CUDA(cudaMemcpyAsync(coef, hc.data(), sizeof(double) * (j + 1) * 16, cudaMemcpyHostToDevice,
+                                        h->stream));
+                k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(w, V, vs, j + 1, coef, n, nrhs);
+                MF_CUDA(cudaGetLastError());
+                for (int i = 0; i <= j; ++i)
+                    for (int r = 0; r < nrhs; ++r) H[((size_t)i * M + j) * 16 + r] += hc[i * 16 + r];
+            }
+            if ((rc = mdot(w, 1, w, hc.data()))) return rc;
+            std::vector<double> inv(16, 0.0);
+            stop = true;
+            for (int r = 0; r < nrhs; ++r) {
+                const double hn = std::sqrt(std::max(hc[r], 0.0));
+                H[((size_t)(j + 1) * M + j) * 16 + r] = hn;
+                inv[r] = hn > 0.0 ? 1.0 / hn : 0.0;
+                // apply the earlier rotations to column j, then a new one
+                for (int i = 0; i < j; ++i) {
+                    double& a = H[((size_t)i * M + j) * 16 + r];
+                    double& c2 = H[((size_t)(i + 1) * M + j) * 16 + r];
+                    const double t0 = cs[i * 16 + r] * a + sn[i * 16 + r] * c2;
+                    c2 = -sn[i * 16 + r] * a + cs[i * 16 + r] * c2;
+                    a = t0;
+                }
+                double& a = H[((size_t)j * M + j) * 16 + r];
+                double& c2 = H[((size_t)(j + 1) * M + j) * 16 + r];
+                const double den = std::hypot(a, c2);
+                const double c = den > 0.0 ? a / den : 1.0, s = den > 0.0 ? c2 / den : 0.0;
+                cs[j * 16 + r] = c;
+                sn[j * 16 + r] = s;
+                a = den;
+                c2 = 0.0;
+                g[(j + 1) * 16 + r] = -s * g[j * 16 + r];
+                g[j * 16 + r] = c * g[j * 16 + r];
+                if (std::fabs(g[(j + 1) * 16 + r]) > tgt[r] && hn > 0.0) stop = false;
+            }
+            MF_CUDA(cudaMemcpyAsync(coef, inv.data(), sizeof(double) * 16, cudaMemcpyHostToDevice, h->stream));
+            k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(w, w, coef, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        // y = H^-1 g (upper triangular, j x j), x += Z y
+        std::vector<double> y((size_t)j * 16, 0.0);
+        for (int r = 0; r < nrhs; ++r)
+            for (int i = j - 1; i >= 0; --i) {
+                double v = g[i * 16 + r];
+                for (int k = i + 1; k < j; ++k) v -= H[((size_t)i * M + k) * 16 + r] * y[k * 16 + r];
+                const double d = H[((size_t)i * M + i) * 16 + r];
+                y[i * 16 + r] = d != 0.0 ? v / d : 0.0;
+            }
+        for (int i = 0; i < j; ++i)
+            for (int r = 0; r < 16; ++r) y[i * 16 + r] = -y[i * 16 + r];  // k_mupd subtracts
+        MF_CUDA(cudaMemcpyAsync(coef, y.data(), sizeof(double) * j * 16, cudaMemcpyHostToDevice, h->stream));
+        k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(x, Z, vs, j, coef, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+    }
+    if (iters) *iters = used;
+    if (eta_out) *eta_out = worst;
     return 0;
 }
 
@@ -414,6 +614,8 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
             k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
+    } else if (h->diag && h->nseg == 0) {
+        return gmres(h, b, x, nrhs, tol, maxit, iters, eta_out);
     } else {
         // classical iterative refinement
         MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));

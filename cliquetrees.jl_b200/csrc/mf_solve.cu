@@ -43,118 +43,185 @@ __global__ void k_diag_div(T* __restrict__ C, const T* __restrict__ d, int64_t n
 }
 
 // ---------------------------------------------------------------------------
-// small fronts (nj <= 96, or nn <= 64 and na <= 1024): one CTA per front
+// small fronts (nj <= 96, or nn <= 64 and na <= 1024): one warp per front,
+// kSmallWarps fronts per CTA, warp-synchronous (no block barriers).  The
+// front's right-hand-side block C1 (nn x nrhs) lives in the warp's slice of
+// shared memory; lane i holds rows i, i + 32, i + 64 in registers during the
+// triangular solves.
 // ---------------------------------------------------------------------------
-template <typename T, int UNIT>
-__global__ void __launch_bounds__(256) k_s_small_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                     const int32_t* __restrict__ reltgt,
-                                                     const int32_t* __restrict__ chdtgt, const T* __restrict__ P,
-                                                     T* __restrict__ C, T* __restrict__ R, int64_t n, int nrhs) {
-    __shared__ T C1[kSmallMax * kMaxRhs];
-    const Front f = fronts[items[blockIdx.x].front];
-    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
-    const int tid = threadIdx.x, nt = blockDim.x;
+constexpr int kSmallWarps = 4;
+constexpr int kSmallRows = (kSmallMax + 31) / 32;  // rows per lane (3)
+
+template <typename T, int NR>
+constexpr int small_solve_smem() { return kSmallWarps * kSmallMax * NR * (int)sizeof(T); }
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* __restrict__ fronts,
+                                                                  const Item* __restrict__ items, int64_t cnt,
+                                                                  const int32_t* __restrict__ reltgt,
+                                                                  const int32_t* __restrict__ chdtgt,
+                                                                  const T* __restrict__ P, T* __restrict__ C,
+                                                                  T* __restrict__ R, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
+    if (w >= cnt) return;  // whole warps only
+    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;  // [r][a] : C1[a + r * kSmallMax]
+    const Front f = fronts[items[w].front];
+    const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     T* Rj = R + f.roff * nrhs;
-    for (int i = tid; i < nn * nrhs; i += nt) {
-        int a = i % nn, r = i / nn;
+    for (int i = lane; i < nn * nrhs; i += 32) {
+        const int a = i % nn, r = i / nn;
         C1[a + r * kSmallMax] = C[f.col0 + a + (int64_t)r * n];
     }
-    for (int i = tid; i < na * nrhs; i += nt) Rj[i] = T(0);
-    __syncthreads();
+    for (int i = lane; i < na * nrhs; i += 32) Rj[i] = T(0);
+    __syncwarp();
+    // child updates, children in reverse order (the reference pops its stack)
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na;
         const int32_t* rel = reltgt + fc.sep0;
         const T* Mc = R + fc.roff * nrhs;
-        for (int i = tid; i < ma * nrhs; i += nt) {
-            int a = i % ma, r = i / ma;
-            int q = rel[a];
+        for (int i = lane; i < ma * nrhs; i += 32) {
+            const int a = i % ma, r = i / ma;
+            const int q = rel[a];
             if (q < nn) C1[q + r * kSmallMax] += Mc[i];
             else Rj[(q - nn) + r * na] += Mc[i];
         }
-        __syncthreads();
+        __syncwarp();
     }
-    // C1 <- D^{-1} C1
+    // forward substitution, column oriented: x_k = C1[k] / L_kk, then
+    // rows a > k lose L_ak x_k
+    T x[kSmallRows][NR];
+#pragma unroll
+    for (int s = 0; s < kSmallRows; ++s)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const int a = lane + 32 * s;
+            x[s][r] = (a < nn && r < nrhs) ? C1[a + r * kSmallMax] : T(0);
+        }
     for (int k = 0; k < nn; ++k) {
-        if (!UNIT) {
-            T inv = T(1) / Pj[k + (int64_t)k * ld];
-            for (int r = tid; r < nrhs; r += nt) C1[k + r * kSmallMax] *= inv;
-            __syncthreads();
+        const int ko = k & 31, ks = k >> 5;
+        T lk[kSmallRows];
+#pragma unroll
+        for (int s = 0; s < kSmallRows; ++s) {
+            const int a = lane + 32 * s;
+            lk[s] = (a > k && a < nn) ? Pj[a + (int64_t)k * ld] : T(0);
         }
-        const int m = nn - k - 1;
-        for (int i = tid; i < m * nrhs; i += nt) {
-            int a = k + 1 + i % m, r = i / m;
-            C1[a + r * kSmallMax] -= Pj[a + (int64_t)k * ld] * C1[k + r * kSmallMax];
+        const T dinv = UNIT ? T(1) : T(1) / Pj[k + (int64_t)k * ld];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            T own = ks == 0 ? x[0][r] : (ks == 1 ? x[1][r] : x[2][r]);
+            const T xk = __shfl_sync(0xffffffffu, own, ko) * dinv;
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) x[s][r] -= lk[s] * xk;
+            if (lane == ko) {
+                if (ks == 0) x[0][r] = xk; else if (ks == 1) x[1][r] = xk; else x[2][r] = xk;
+            }
         }
-        __syncthreads();
     }
-    // R_j -= L21 C1
-    for (int i = tid; i < na * nrhs; i += nt) {
-        int a = i % na, r = i / na;
-        T s = T(0);
-        for (int k = 0; k < nn; ++k) s += Pj[(nn + a) + (int64_t)k * ld] * C1[k + r * kSmallMax];
-        Rj[a + r * na] -= s;
+#pragma unroll
+    for (int s = 0; s < kSmallRows; ++s) {
+        const int a = lane + 32 * s;
+        if (a < nn)
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) {
+                    C1[a + r * kSmallMax] = x[s][r];
+                    C[f.col0 + a + (int64_t)r * n] = x[s][r];
+                }
     }
-    for (int i = tid; i < nn * nrhs; i += nt) {
-        int a = i % nn, r = i / nn;
-        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kSmallMax];
+    __syncwarp();
+    // R_j -= L21 x: lanes own rows of L21 (coalesced along the panel columns)
+    for (int a = lane; a < na; a += 32) {
+        T acc[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r] = T(0);
+        const T* lr = Pj + nn + a;
+        for (int k = 0; k < nn; ++k) {
+            const T l = lr[(int64_t)k * ld];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] += l * C1[k + r * kSmallMax];
+        }
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) Rj[a + r * na] -= acc[r];
     }
 }
 
-template <typename T, int UNIT>
-__global__ void __launch_bounds__(256) k_s_small_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                     const int32_t* __restrict__ septgt, const T* __restrict__ P,
-                                                     T* __restrict__ C, int64_t n, int nrhs) {
-    __shared__ T C1[kSmallMax * kMaxRhs];
-    const Front f = fronts[items[blockIdx.x].front];
-    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* __restrict__ fronts,
+                                                                  const Item* __restrict__ items, int64_t cnt,
+                                                                  const int32_t* __restrict__ septgt,
+                                                                  const T* __restrict__ P, T* __restrict__ C,
+                                                                  int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
+    if (w >= cnt) return;
+    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;
+    const Front f = fronts[items[w].front];
+    const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
-    // C1 = C[res] - L21^T x[sep]   (one warp per column of L21)
-    for (int k = warp; k < nn; k += nw) {
-        T acc[kMaxRhs];
+    // C1 = C[res] - L21^T x[sep]: lanes own columns k, rows a walked in order
+    // (x[sep[a]] is one broadcast load per row)
+    T acc[kSmallRows][NR];
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = T(0);
-        const T* lc = Pj + nn + (int64_t)k * ld;
-        for (int a = lane; a < na; a += 32) {
-            T l = lc[a];
-            int64_t row = sep[a];
+    for (int s = 0; s < kSmallRows; ++s)
 #pragma unroll
-            for (int r = 0; r < kMaxRhs; ++r)
-                if (r < nrhs) acc[r] += l * C[row + (int64_t)r * n];
-        }
+        for (int r = 0; r < NR; ++r) acc[s][r] = T(0);
+    for (int a = 0; a < na; ++a) {
+        const int64_t row = sep[a];
+        T xv[NR];
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) {
-            T v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            acc[r] = v;
-        }
-        if (lane == 0)
-            for (int r = 0; r < nrhs; ++r) C1[k + r * kSmallMax] = C[f.col0 + k + (int64_t)r * n] - acc[r];
-    }
-    __syncthreads();
-    // C1 <- D^{-T} C1 (backward substitution, column oriented)
-    for (int k = nn - 1; k >= 0; --k) {
-        // C1[k] -= sum_{a>k} D[a,k] C1[a]
-        if (warp == 0) {
-            for (int r = 0; r < nrhs; ++r) {
-                T s = T(0);
-                for (int a = k + 1 + lane; a < nn; a += 32) s += Pj[a + (int64_t)k * ld] * C1[a + r * kSmallMax];
-                for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-                if (lane == 0) {
-                    T v = C1[k + r * kSmallMax] - s;
-                    if (!UNIT) v /= Pj[k + (int64_t)k * ld];
-                    C1[k + r * kSmallMax] = v;
-                }
+        for (int r = 0; r < NR; ++r) xv[r] = r < nrhs ? C[row + (int64_t)r * n] : T(0);
+#pragma unroll
+        for (int s = 0; s < kSmallRows; ++s) {
+            const int k = lane + 32 * s;
+            if (k < nn) {
+                const T l = Pj[(nn + a) + (int64_t)k * ld];
+#pragma unroll
+                for (int r = 0; r < NR; ++r) acc[s][r] += l * xv[r];
             }
         }
-        __syncthreads();
     }
-    for (int i = tid; i < nn * nrhs; i += nt) {
-        int a = i % nn, r = i / nn;
+#pragma unroll
+    for (int s = 0; s < kSmallRows; ++s) {
+        const int k = lane + 32 * s;
+        if (k < nn)
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) C1[k + r * kSmallMax] = C[f.col0 + k + (int64_t)r * n] - acc[s][r];
+    }
+    __syncwarp();
+    // back substitution: x_k = (C1[k] - sum_{a>k} L_ak x_a) / L_kk, k descending
+    for (int k = nn - 1; k >= 0; --k) {
+        T part[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) part[r] = T(0);
+        for (int a = k + 1 + lane; a < nn; a += 32) {
+            const T l = Pj[a + (int64_t)k * ld];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) part[r] += l * C1[a + r * kSmallMax];
+        }
+        const T dinv = UNIT ? T(1) : T(1) / Pj[k + (int64_t)k * ld];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            T v = part[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            part[r] = v;
+        }
+        __syncwarp();
+        if (lane == 0)
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if (r < nrhs) C1[k + r * kSmallMax] = (C1[k + r * kSmallMax] - part[r]) * dinv;
+        __syncwarp();
+    }
+    for (int i = lane; i < nn * nrhs; i += 32) {
+        const int a = i % nn, r = i / nn;
         C[f.col0 + a + (int64_t)r * n] = C1[a + r * kSmallMax];
     }
 }
@@ -461,14 +528,32 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd<T, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 small_solve_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_small_bwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 small_solve_smem<T, 16>()));
+    const int nrb = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
     const Item* items = h->d_items;
     const int64_t n = h->n;
     // forward: levels ascending
     for (const Level& lv : h->levels) {
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
-            k_s_small_fwd<T, UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
-                h->d_fronts, items + lv.s_small.off, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs);
+            const unsigned g = (unsigned)((lv.s_small.cnt + kSmallWarps - 1) / kSmallWarps);
+            const Item* it = items + lv.s_small.off;
+            const int64_t c = lv.s_small.cnt;
+            switch (nrb) {
+                case 1: k_s_small_fwd<T, UNIT, 1><<<g, kSmallWarps * 32, small_solve_smem<T, 1>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+                case 2: k_s_small_fwd<T, UNIT, 2><<<g, kSmallWarps * 32, small_solve_smem<T, 2>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+                case 4: k_s_small_fwd<T, UNIT, 4><<<g, kSmallWarps * 32, small_solve_smem<T, 4>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+                case 8: k_s_small_fwd<T, UNIT, 8><<<g, kSmallWarps * 32, small_solve_smem<T, 8>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+                default: k_s_small_fwd<T, UNIT, 16><<<g, kSmallWarps * 32, small_solve_smem<T, 16>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+            }
             MF_CUDA(cudaGetLastError());
         }
         if (lv.s_gather.cnt) {
@@ -515,8 +600,21 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         }
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
-            k_s_small_bwd<T, UNIT><<<(unsigned)lv.s_small.cnt, 256, 0, h->stream>>>(
-                h->d_fronts, items + lv.s_small.off, h->d_septgt, sb.P, sb.C, n, nrhs);
+            const unsigned g = (unsigned)((lv.s_small.cnt + kSmallWarps - 1) / kSmallWarps);
+            const Item* it = items + lv.s_small.off;
+            const int64_t c = lv.s_small.cnt;
+            switch (nrb) {
+                case 1: k_s_small_bwd<T, UNIT, 1><<<g, kSmallWarps * 32, small_solve_smem<T, 1>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+                case 2: k_s_small_bwd<T, UNIT, 2><<<g, kSmallWarps * 32, small_solve_smem<T, 2>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+                case 4: k_s_small_bwd<T, UNIT, 4><<<g, kSmallWarps * 32, small_solve_smem<T, 4>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+                case 8: k_s_small_bwd<T, UNIT, 8><<<g, kSmallWarps * 32, small_solve_smem<T, 8>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+                default: k_s_small_bwd<T, UNIT, 16><<<g, kSmallWarps * 32, small_solve_smem<T, 16>(), h->stream>>>(
+                            h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+            }
             MF_CUDA(cudaGetLastError());
         }
     }
