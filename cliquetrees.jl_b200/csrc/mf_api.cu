@@ -50,7 +50,7 @@ void free_all(mf_handle* h) {
                     h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
-                    h->d_segeta, h->d_kry};
+                    h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2};
     release_graphs(h);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -155,6 +155,7 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     rc = rc ? rc : dalloc(h, &h->d_items, (int64_t)h->h_items.size(), &tot);
     rc = rc ? rc : dalloc(h, &h->d_P, h->npanel, &tot);
     rc = rc ? rc : dalloc(h, &h->d_inv, std::max<int64_t>(h->ninv, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_inv2, std::max<int64_t>(h->ninv2, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_M, h->nmval, &tot);
     rc = rc ? rc : dalloc(h, &h->d_d, std::max<int64_t>(n, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_info, 1, &tot);
@@ -532,6 +533,7 @@ int mf_enable_mixed(mf_handle* h) {
     rc = rc ? rc : dalloc(h, &h->f32.P, std::max<int64_t>(h->npanel, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.M, std::max<int64_t>(h->nmval, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.inv, std::max<int64_t>(h->ninv, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->f32.inv2, std::max<int64_t>(h->ninv2, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.d, std::max<int64_t>(n, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.R, std::max<int64_t>(h->nrval_per_rhs * cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.W, std::max<int64_t>(n * cap, 1), &tot);

@@ -628,6 +628,108 @@ __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, 
 }
 
 // ---------------------------------------------------------------------------
+// 256x256 diagonal super-block inverses for the blocked solves, once after
+// the factorization.  Super-block K of a front (columns k0 = 256 K ..) is
+// made of up to four 64-column blocks with stored inverses D_s; its inverse
+// X follows by block forward substitution along the block sub-diagonals:
+//   X_ss = D_s,   X_st = -D_s sum_{u=t}^{s-1} L_su X_ut   (s > t),
+// 64 x 64 tile products in shared memory, 4 x 4 outputs per thread.
+// ---------------------------------------------------------------------------
+constexpr int ILD = kNB + 1;
+
+template <typename T>
+constexpr int inv256_smem() { return 3 * kNB * ILD * (int)sizeof(T); }
+
+template <typename T>
+__device__ __forceinline__ void tile_in(T* dst, const T* src, int64_t ld, int rows, int cols) {
+    for (int e = threadIdx.x; e < kNB * kNB; e += blockDim.x) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        dst[r + c * ILD] = (r < rows && c < cols) ? src[r + (int64_t)c * ld] : T(0);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void tile_mma(T (&acc)[4][4], const T* A, const T* B) {
+    const int tr = (threadIdx.x >> 4) * 4, tc = (threadIdx.x & 15) * 4;
+#pragma unroll 8
+    for (int k = 0; k < kNB; ++k) {
+        T a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = A[(tr + i) + k * ILD];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = B[k + (tc + j) * ILD];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_inv256(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                const T* __restrict__ P, const T* __restrict__ inv,
+                                                T* __restrict__ inv2) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* As = reinterpret_cast<T*>(smem_raw);
+    T* Bs = As + kNB * ILD;
+    T* Cs = Bs + kNB * ILD;
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int K = it.a, k0 = K * kSolveNB, wK = min(kSolveNB, f.nn - k0), ns = (wK + kNB - 1) / kNB;
+    const int ld2 = super_ld(wK), ld = f.ldp;
+    T* X = inv2 + f.i2off + (int64_t)K * kSolveNB * kSolveNB;
+    const T* Pj = P + f.poff;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < ld2 * wK; e += blockDim.x) X[e] = T(0);
+    __syncthreads();
+    for (int s = 0; s < ns; ++s) {
+        const int ws = min(kNB, wK - s * kNB);
+        const T* D = inv + f.ioff + (int64_t)(k0 / kNB + s) * kNB * kNB;
+        for (int e = tid; e < ws * ws; e += blockDim.x) {
+            const int r = e % ws, c = e / ws;
+            X[(s * kNB + r) + (int64_t)(s * kNB + c) * ld2] = D[r + c * kNB];
+        }
+    }
+    __syncthreads();
+    const int tr = (tid >> 4) * 4, tc = (tid & 15) * 4;
+    for (int d = 1; d < ns; ++d)
+        for (int s = d; s < ns; ++s) {
+            const int t = s - d;
+            const int ws = min(kNB, wK - s * kNB), wt = min(kNB, wK - t * kNB);
+            T acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+            for (int u = t; u < s; ++u) {  // T += L_su X_ut
+                tile_in(As, Pj + (k0 + s * kNB) + (int64_t)(k0 + u * kNB) * ld, ld, ws, kNB);
+                tile_in(Bs, X + u * kNB + (int64_t)(t * kNB) * ld2, ld2, kNB, wt);
+                __syncthreads();
+                tile_mma(acc, As, Bs);
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) Cs[(tr + i) + (tc + j) * ILD] = acc[i][j];
+            tile_in(As, inv + f.ioff + (int64_t)(k0 / kNB + s) * kNB * kNB, kNB, kNB, kNB);
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+            tile_mma(acc, As, Cs);
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (tr + i < ws && tc + j < wt)
+                        X[(s * kNB + tr + i) + (int64_t)(t * kNB + tc + j) * ld2] = -acc[i][j];
+            __syncthreads();  // X_st is read by the next distance
+        }
+}
+
+// ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
 Timer::Timer(mf_handle* h_, int k_) : h(h_), k(k_) {
@@ -715,6 +817,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     MF_CUDA(cudaFuncSetAttribute(k_small<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmallMax * kSmallMax * (int)sizeof(T)));
     MF_CUDA(cudaFuncSetAttribute(k_diag<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_inv256<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv256_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
@@ -797,6 +900,12 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             MF_CUDA(cudaGetLastError());
         }
     }
+    if (h->inv2_items.cnt) {
+        Timer t(h, K_OTHER);
+        k_inv256<T><<<grid_for(h->inv2_items.cnt), 256, inv256_smem<T>(), h->stream>>>(
+            h->d_fronts, items + h->inv2_items.off, fb.P, fb.inv, fb.inv2);
+        MF_CUDA(cudaGetLastError());
+    }
     return 0;
 }
 
@@ -837,14 +946,14 @@ void release_graphs(mf_handle* h) {
 // graph keys: kind (1 FP64 factor, 2 FP32 factor), then what the launch
 // sequence reads through pointers that can change between calls
 int launch_factor(mf_handle* h) {
-    FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d};
+    FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d, h->d_inv2};
     return run_captured(h, 1, (int64_t)(uintptr_t)h->d_signs, 0, 0, [&]() {
         return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
     });
 }
 
 int launch_factor_mixed(mf_handle* h) {
-    FactorBufs<float> fb{h->f32.P, h->f32.M, h->f32.inv, h->f32.d};
+    FactorBufs<float> fb{h->f32.P, h->f32.M, h->f32.inv, h->f32.d, h->f32.inv2};
     if (h->use_tc) {
         int rc = tc_prepare(h);
         if (rc) return rc;

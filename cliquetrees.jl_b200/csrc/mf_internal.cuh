@@ -26,6 +26,7 @@ struct Front {
     int64_t moff;   // update-matrix offset in Mval (na > 0)
     int64_t roff;   // first row of this front's solve update block in Rval (block at R + roff*nrhs)
     int64_t ioff;   // offset of its 64x64 diagonal-block inverses in the inverse scratch
+    int64_t i2off;  // offset of its 256x256 diagonal super-block inverses (blocked solves), -1 if none
     int32_t nn;     // |res(j)|
     int32_t na;     // |sep(j)|
     int32_t col0;   // first (permuted) column of res(j)
@@ -73,6 +74,7 @@ constexpr int kEAcols = 16;     // parent columns per extend-add work item
 constexpr int kSolveRows = 256; // rows per gather work item
 constexpr int kTcSyrkN = 128;   // tile columns of the tensor-core SYRK
 constexpr int kFwdRows = 64;    // rows per forward-update work item
+constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
 
 // One 64-wide sub-panel s of outer block b (columns b*kOB + s*kNB ...).
@@ -86,9 +88,11 @@ struct PanelStep {
     ItemList left_tc, panel_tc, trail_tc;
 };
 
+// One 256-column super-block K of the blocked fronts' diagonal blocks.
 struct SolveStep {
-    ItemList fwd;     // (front, row tile)
-    ItemList bwd;     // (front, col tile)
+    ItemList diag;    // (front)            x_K = X_K b_K (forward) or X_K^T b_K (backward)
+    ItemList fwd;     // (front, row tile)  rows below the super-block -= L x_K
+    ItemList bwd;     // (front, col tile)  columns left of the super-block -= L^T x_K
 };
 
 struct Level {
@@ -117,6 +121,18 @@ enum KernelId {
     K_DIAG, K_LEFT, K_SPMV, K_COUNT
 };
 
+// The solves handle a front with one warp when the factorization kept it
+// whole (nj <= kSmallMax) or it is narrow; otherwise it is blocked in the
+// factorization too and its diagonal-block inverses exist.
+__host__ __device__ inline bool solve_small(const Front& f) {
+    return f.nn + f.na <= kSmallMax || (f.nn <= kNB && f.na <= 1024);
+}
+
+// Super-block K of a blocked front: its inverse X_K (wK x wK, lower, unit
+// diagonal for LDLt) is stored column major with leading dimension
+// super_ld(wK) at inv2 + f.i2off + K * kSolveNB * kSolveNB.
+__host__ __device__ inline int super_ld(int wK) { return wK == kSolveNB ? kSolveNB : ((wK + 3) & ~3); }
+
 // numeric buffers of one precision
 template <typename T>
 struct FactorBufs {
@@ -124,6 +140,7 @@ struct FactorBufs {
     T* M = nullptr;    // update matrices
     T* inv = nullptr;  // diagonal-block inverses
     T* d = nullptr;    // LDLt pivots (n)
+    T* inv2 = nullptr; // 256x256 super-block inverses
 };
 
 template <typename T>
@@ -135,6 +152,7 @@ struct SolveBufs {
     T* W = nullptr;
     T* C = nullptr;
     T* part = nullptr;  // backward partial sums (nbwd_part * 64 * 16)
+    const T* inv2 = nullptr;  // super-block inverses
 };
 
 // An instantiated CUDA graph of one fixed launch sequence of a handle (a
@@ -154,6 +172,7 @@ struct Mixed {
     float* W = nullptr;
     float* C = nullptr;
     float* part = nullptr;
+    float* inv2 = nullptr;
 };
 
 }  // namespace mf
@@ -178,6 +197,7 @@ struct mf_handle {
     std::vector<int32_t> h_sepmap;          // reference sep rows -> execution panel rows
     std::vector<int64_t> h_resptr, h_sepptr, h_septgt, h_Dptr, h_Lptr;
     std::vector<mf::Level> levels;
+    mf::ItemList inv2_items;                // (front, super-block) of the super-block inverses
     std::vector<mf::Item> h_items;
 
     // device symbolic
@@ -194,6 +214,8 @@ struct mf_handle {
     double* d_P = nullptr;         // panels
     double* d_inv = nullptr;       // inverses of the 64x64 diagonal blocks
     int64_t ninv = 0;
+    double* d_inv2 = nullptr;      // inverses of the 256x256 diagonal super-blocks (blocked solves)
+    int64_t ninv2 = 0;
     double* d_M = nullptr;         // update matrices
     double* d_d = nullptr;         // LDLt pivots (n)
     double* d_signs = nullptr;     // pivot signs (n) or null

@@ -265,7 +265,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         int64_t pe = eparent[e];
         if (pe >= 0) level[pe] = std::max(level[pe], level[e] + 1);
     }
-    int64_t ioff = 0;
+    int64_t ioff = 0, ioff2 = 0;
     for (int64_t e = 0; e < nex; ++e) {
         Front& f = h->h_fronts[e];
         int64_t t = ef[e].top;
@@ -283,10 +283,17 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         f.roff = 0;
         f.ioff = 0;
         if (nn + na > kSmallMax) { f.ioff = ioff; ioff += cdiv(nn, kNB) * kNB * kNB; }
+        f.i2off = -1;
+        if (!solve_small(f)) {
+            const int64_t nK = cdiv(nn, kSolveNB), wL = nn - (nK - 1) * kSolveNB;
+            f.i2off = ioff2;
+            ioff2 += (nK - 1) * kSolveNB * kSolveNB + (int64_t)super_ld((int)wL) * wL;
+        }
         max_level = std::max(max_level, level[e]);
     }
     h->npanel = poff;
     h->ninv = ioff;
+    h->ninv2 = ioff2;
     {
         // slot lifetimes: produced at level(e), read while level(parent(e))
         // is processed, reusable from the next level on
@@ -448,12 +455,8 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         }
         end(lv.syrk_tc);
 
-        // solves: a front is solved by one CTA when the factorization kept it
-        // whole (nj <= kSmallMax) or it is narrow; otherwise it is blocked in
-        // the factorization too and its diagonal-block inverses exist
-        auto solve_small = [](const Front& f) {
-            return f.nn + f.na <= kSmallMax || (f.nn <= kNB && f.na <= 1024);
-        };
+        // solves: small fronts (solve_small) one warp each; blocked fronts in
+        // 256-column super-block steps using the super-block inverses
         begin(lv.s_small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
@@ -467,29 +470,34 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (solve_small(f)) continue;
             int nj = f.nn + f.na;
             for (int t = 0; t < cdiv(nj, kSolveRows); ++t) push(j, t, 0);
-            max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kNB));
+            max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kSolveNB));
         }
         end(lv.s_gather);
         lv.s_steps.resize(max_sblocks);
         for (int k = 0; k < max_sblocks; ++k) {
             SolveStep& st = lv.s_steps[k];
+            const int k0 = k * kSolveNB;
+            begin(st.diag);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                if (solve_small(f) || f.nn <= k0) continue;
+                push(j, 0, 0);
+            }
+            end(st.diag);
             begin(st.fwd);
             for (int32_t j : fr) {
                 const Front& f = h->h_fronts[j];
-                if (solve_small(f) || f.nn <= k * kNB) continue;
-                int nj = f.nn + f.na;
-                int w = std::min(kNB, f.nn - k * kNB);
-                int below = nj - (k * kNB + w);
-                int tiles = 1 + (int)cdiv(below, kFwdRows);
-                for (int t = 0; t < tiles; ++t) push(j, t, 0);
+                if (solve_small(f) || f.nn <= k0) continue;
+                const int w = std::min(kSolveNB, f.nn - k0);
+                const int below = f.nn + f.na - (k0 + w);
+                for (int t = 0; t < (int)cdiv(below, kFwdRows); ++t) push(j, t, 0);
             }
             end(st.fwd);
             begin(st.bwd);
             for (int32_t j : fr) {
                 const Front& f = h->h_fronts[j];
-                if (solve_small(f) || f.nn <= k * kNB) continue;
-                int tiles = 1 + (int)cdiv(k * kNB, kNB);
-                for (int t = 0; t < tiles; ++t) push(j, t, 0);
+                if (solve_small(f) || f.nn <= k0) continue;
+                for (int t = 0; t < (int)cdiv(k0, kNB); ++t) push(j, t, 0);
             }
             end(st.bwd);
         }
@@ -511,6 +519,13 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         for (const Item& r : red) items.push_back(r);
         end(lv.s_bwd_red);
     }
+    begin(h->inv2_items);
+    for (int64_t e = 0; e < (int64_t)h->h_fronts.size(); ++e) {
+        const Front& f = h->h_fronts[(size_t)e];
+        if (f.i2off < 0) continue;
+        for (int K = 0; K < (int)cdiv(f.nn, kSolveNB); ++K) push((int32_t)e, K, 0);
+    }
+    end(h->inv2_items);
     return 0;
 }
 

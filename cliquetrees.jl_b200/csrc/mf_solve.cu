@@ -275,79 +275,107 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
     }
 }
 
-// x_k = Linv b_k (TRANS = 0) or x_k = Linv^T b_k (TRANS = 1) for the w x w
-// diagonal block of step k, with Linv the inverse of the factored block
-// stored by the factorization (unit lower for LDLt).  b_k (w x nrhs) is
-// read from `src` (leading dimension n); the result lands in X (ld SLD).
-template <typename T, int TRANS>
-__device__ void diag_block_apply(const T* Li, int w, const T* src, int64_t n, int nrhs, T* Ls, T* Bs, T* X) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int i = tid; i < kNB * kNB; i += nt) {
-        int r = i & (kNB - 1), c = i >> 6;
-        Ls[r + c * SLD] = Li[i];
-    }
-    for (int i = tid; i < w * nrhs; i += nt) {
-        int a = i % w, r = i / w;
-        Bs[a + r * SLD] = src[a + (int64_t)r * n];
+// ---------------------------------------------------------------------------
+// blocked diagonal solves in steps of a 256-column super-block K (columns
+// k0 .. k0 + wK of a front), with the super-block inverse X_K stored by the
+// factorization.  Per step and level:
+//   forward : k_s_fdiag  x_K = X_K W_K            (one CTA per front), then
+//             k_s_ftile  rows below: W / R -= L[rows, K] x_K (64-row tiles);
+//   backward: k_s_bdiag  x_K = X_K^T W_K          (one CTA per front), then
+//             k_s_btile  columns left: W[c] -= sum_i L[k0 + i, c] x_K[i].
+// ---------------------------------------------------------------------------
+template <typename T, int NR>
+constexpr int sdiag_smem() { return kSolveNB * NR * (int)sizeof(T); }
+template <typename T, int NR>
+constexpr int ftile_smem() { return (kSolveNB * NR + 4 * NR * kFwdRows) * (int)sizeof(T); }
+template <typename T>
+constexpr int btile_smem() { return kSolveNB * kMaxRhs * (int)sizeof(T); }
+
+// x_K = X_K b_K (BWD = 0) or X_K^T b_K (BWD = 1), spread over kDiagSplit
+// CTAs per front so that the 256 x 256 inverse streams through many SMs:
+// CTA q owns outputs a in [16 q, 16 q + 16); thread t takes output
+// 16 q + t / 16 and every 16th input starting at t % 16, then half-warp
+// shuffles add the 16 partial sums.  Reads are along the columns of X
+// (forward: 16 consecutive rows of a column; backward: 16 consecutive
+// entries of column a), and the zero triangle is skipped.
+constexpr int kDiagSplit = kSolveNB / 16;
+
+template <typename T, int NR, int BWD>
+__global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ inv2, T* __restrict__ C,
+                                                 const T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* b = reinterpret_cast<T*>(sm_raw);  // [r][c] : b[c + r * kSolveNB]
+    const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
+    const int q = blockIdx.x % kDiagSplit;
+    const int k0 = step * kSolveNB, wK = min(kSolveNB, f.nn - k0), ld2 = super_ld(wK);
+    if (16 * q >= wK) return;  // whole CTA
+    const T* X = inv2 + f.i2off + (int64_t)step * kSolveNB * kSolveNB;
+    for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
+        const int c = i % kSolveNB, r = i / kSolveNB;
+        b[i] = (c < wK && r < nrhs) ? W[f.col0 + k0 + c + (int64_t)r * n] : T(0);
     }
     __syncthreads();
-    for (int i = tid; i < kNB * nrhs; i += nt) {
-        int a = i % kNB, r = i / kNB;
-        if (a >= w) { X[a + r * SLD] = T(0); continue; }
-        T acc = T(0);
-        if (!TRANS) {
-            for (int c = 0; c <= a; ++c) acc += Ls[a + c * SLD] * Bs[c + r * SLD];
-        } else {
-            for (int c = a; c < w; ++c) acc += Ls[c + a * SLD] * Bs[c + r * SLD];
+    const int a = 16 * q + (threadIdx.x >> 4), cl = threadIdx.x & 15;
+    T acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    if (a < wK) {
+        // forward: inputs c <= a, X[a, c]; backward: inputs c >= a, X[c, a]
+        const int cb = BWD ? a : 0, ce = BWD ? wK : a + 1;
+#pragma unroll 4
+        for (int c = cb + cl; c < ce; c += 16) {
+            const T x = BWD ? X[c + (int64_t)a * ld2] : X[a + (int64_t)c * ld2];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[r] += x * b[c + r * kSolveNB];
         }
-        X[a + r * SLD] = acc;
     }
-    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        T v = acc[r];
+        for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[r] = v;
+    }
+    if (cl == 0 && a < wK)
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) C[f.col0 + k0 + a + (int64_t)r * n] = acc[r];
 }
 
-template <typename T>
-constexpr int solve_smem() { return (2 * kNB * SLD + 2 * kMaxRhs * SLD) * (int)sizeof(T); }
-
-template <typename T, int UNIT, int NR>
-__global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const T* __restrict__ P, const T* __restrict__ inv,
-                                               T* __restrict__ C, T* __restrict__ W, T* __restrict__ R, int64_t n,
-                                               int nrhs) {
+// forward rows below super-block K: W (rows < nn) or R_j (rows >= nn) -= L[rows, K] x_K
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
+                                                 T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* Ls = reinterpret_cast<T*>(sm_raw);
-    T* Bs = Ls + kNB * SLD;
-    T* X = Bs + kMaxRhs * SLD;
+    T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * NR
+    T* red = xs + kSolveNB * NR;           // 4 * NR * kFwdRows
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
-    const int k0 = step * kNB, w = min(kNB, nn - k0);
-    const T* Pj = P + f.poff;
-    diag_block_apply<T, 0>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (it.a == 0) {
-        for (int i = tid; i < w * nrhs; i += nt) {
-            int a = i % w, r = i / w;
-            C[f.col0 + k0 + a + (int64_t)r * n] = X[a + r * SLD];
-        }
-        return;
-    }
-    const int r0 = k0 + w + (it.a - 1) * kFwdRows;
+    const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
+    const int r0 = k0 + wK + it.a * kFwdRows;
     const int nr = min(kFwdRows, nj - r0);
-    const int rl = tid & (kFwdRows - 1), g = tid / kFwdRows;  // row, 16-column group
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kSolveNB * NR; i += 256) {
+        const int a = i % kSolveNB, r = i / kSolveNB;
+        xs[i] = (a < wK && r < nrhs) ? C[f.col0 + k0 + a + (int64_t)r * n] : T(0);
+    }
+    __syncthreads();
+    const int rl = tid & (kFwdRows - 1), g = tid / kFwdRows;  // row, 64-column group
     T acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
     if (rl < nr) {
-        const T* pq = Pj + (r0 + rl) + (int64_t)(k0 + g * 16) * ld;
-        T l[16];
+        const T* pq = P + f.poff + (r0 + rl) + (int64_t)(k0 + g * kNB) * ld;
+        const int cend = min(kNB, wK - g * kNB);
+#pragma unroll 8
+        for (int c = 0; c < cend; ++c) {
+            const T l = pq[(int64_t)c * ld];
 #pragma unroll
-        for (int c = 0; c < 16; ++c) l[c] = (g * 16 + c < w) ? pq[(int64_t)c * ld] : T(0);
-#pragma unroll
-        for (int c = 0; c < 16; ++c)
-#pragma unroll
-            for (int r = 0; r < NR; ++r) acc[r] += l[c] * X[(g * 16 + c) + r * SLD];
+            for (int r = 0; r < NR; ++r) acc[r] += l * xs[g * kNB + c + r * kSolveNB];
+        }
     }
-    T* red = Ls;  // the inverse tile is no longer needed: [g][r][row]
 #pragma unroll
     for (int r = 0; r < NR; ++r) red[(g * NR + r) * kFwdRows + rl] = acc[r];
     __syncthreads();
@@ -357,11 +385,52 @@ __global__ void __launch_bounds__(256) k_s_fwd(const Front* __restrict__ fronts,
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
             if (r < nrhs) {
-                T v = red[(0 * NR + r) * kFwdRows + rl] + red[(1 * NR + r) * kFwdRows + rl] +
-                      red[(2 * NR + r) * kFwdRows + rl] + red[(3 * NR + r) * kFwdRows + rl];
+                const T v = red[(0 * NR + r) * kFwdRows + rl] + red[(1 * NR + r) * kFwdRows + rl] +
+                            red[(2 * NR + r) * kFwdRows + rl] + red[(3 * NR + r) * kFwdRows + rl];
                 if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
                 else Rj[(q - nn) + r * na] -= v;
             }
+        }
+    }
+}
+
+// backward columns left of super-block K (64-column tile it.a):
+// W[c] -= sum_i L[k0 + i, c] x_K[i]; one warp per column, lanes along the
+// column (coalesced), then a shuffle reduction per right-hand side
+template <typename T>
+__global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
+                                                 T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * kMaxRhs
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, ld = f.ldp;
+    const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
+    const int c0 = it.a * kNB, wc = min(kNB, k0 - c0);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < wK * nrhs; i += 256) {
+        const int a = i % wK, r = i / wK;
+        xs[a + r * kSolveNB] = C[f.col0 + k0 + a + (int64_t)r * n];
+    }
+    __syncthreads();
+    for (int cc = warp; cc < wc; cc += 8) {
+        const T* pc = P + f.poff + (int64_t)(c0 + cc) * ld + k0;
+        T acc[kMaxRhs];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) acc[r] = T(0);
+        for (int i = lane; i < wK; i += 32) {
+            const T l = pc[i];
+#pragma unroll
+            for (int r = 0; r < kMaxRhs; ++r)
+                if (r < nrhs) acc[r] += l * xs[i + r * kSolveNB];
+        }
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; ++r) {
+            if (r >= nrhs) break;
+            T v = acc[r];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) W[f.col0 + c0 + cc + (int64_t)r * n] -= v;
         }
     }
 }
@@ -439,44 +508,6 @@ __global__ void __launch_bounds__(256) k_s_bwd_red(const Front* __restrict__ fro
     }
 }
 
-template <typename T, int UNIT>
-__global__ void __launch_bounds__(256) k_s_bwd(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               int step, const T* __restrict__ P, const T* __restrict__ inv,
-                                               T* __restrict__ C, T* __restrict__ W, int64_t n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* Ls = reinterpret_cast<T*>(sm_raw);
-    T* Bs = Ls + kNB * SLD;
-    T* X = Bs + kMaxRhs * SLD;
-    T* Dt = X + kMaxRhs * SLD;  // solve_smem<T>() covers Ls, Bs, X and Dt (64 x SLD)
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
-    const int nn = f.nn, ld = f.ldp;
-    const int k0 = step * kNB, w = min(kNB, nn - k0);
-    const T* Pj = P + f.poff;
-    diag_block_apply<T, 1>(inv + f.ioff + (int64_t)step * kNB * kNB, w, W + f.col0 + k0, n, nrhs, Ls, Bs, X);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    if (it.a == 0) {
-        for (int i = tid; i < w * nrhs; i += nt) {
-            int a = i % w, r = i / w;
-            C[f.col0 + k0 + a + (int64_t)r * n] = X[a + r * SLD];
-        }
-        return;
-    }
-    // W[c] -= sum_i D[k0+i, c] x_k[i] for the 64 columns c of tile (it.a-1) left of k0
-    const int c0 = (it.a - 1) * kNB, wc = min(kNB, k0 - c0);
-    for (int i = tid; i < w * wc; i += nt) {
-        int a = i % w, c = i / w;
-        Dt[a + c * SLD] = Pj[(k0 + a) + (int64_t)(c0 + c) * ld];
-    }
-    __syncthreads();
-    for (int o = tid; o < wc * nrhs; o += nt) {
-        int c = o % wc, r = o / wc;
-        T s = T(0);
-        for (int a = 0; a < w; ++a) s += Dt[a + c * SLD] * X[a + r * SLD];
-        W[f.col0 + c0 + c + (int64_t)r * n] -= s;
-    }
-}
-
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -520,13 +551,9 @@ int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* per
 
 template <typename T, int UNIT>
 static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
-    constexpr int ss = solve_smem<T>();
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_s_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_s_bwd<T, UNIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 8>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_btile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, btile_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small_solve_smem<T, 16>()));
@@ -564,13 +591,30 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         }
         for (size_t k = 0; k < lv.s_steps.size(); ++k) {
             const SolveStep& st = lv.s_steps[k];
-            if (!st.fwd.cnt) continue;
+            if (!st.diag.cnt) continue;
             Timer t(h, K_S_FWD);
-            auto* kern = nrhs <= 1 ? k_s_fwd<T, UNIT, 1> : nrhs <= 2 ? k_s_fwd<T, UNIT, 2>
-                       : nrhs <= 4 ? k_s_fwd<T, UNIT, 4> : nrhs <= 8 ? k_s_fwd<T, UNIT, 8> : k_s_fwd<T, UNIT, 16>;
-            kern<<<(unsigned)st.fwd.cnt, 256, ss, h->stream>>>(h->d_fronts, items + st.fwd.off, (int)k, sb.P, sb.inv,
-                                                               sb.C, sb.W, sb.R, n, nrhs);
+            const unsigned gd = (unsigned)st.diag.cnt;
+            const Item* itd = items + st.diag.off;
+            switch (nrb) {
+                case 1: k_s_sdiag<T, 1, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: k_s_sdiag<T, 2, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: k_s_sdiag<T, 4, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: k_s_sdiag<T, 8, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: k_s_sdiag<T, 16, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+            }
             MF_CUDA(cudaGetLastError());
+            if (st.fwd.cnt) {
+                const unsigned gf = (unsigned)st.fwd.cnt;
+                const Item* itf = items + st.fwd.off;
+                switch (nrb) {
+                    case 1: k_s_ftile<T, 1><<<gf, 256, ftile_smem<T, 1>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                    case 2: k_s_ftile<T, 2><<<gf, 256, ftile_smem<T, 2>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                    case 4: k_s_ftile<T, 4><<<gf, 256, ftile_smem<T, 4>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                    case 8: k_s_ftile<T, 8><<<gf, 256, ftile_smem<T, 8>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                    default: k_s_ftile<T, 16><<<gf, 256, ftile_smem<T, 16>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                }
+                MF_CUDA(cudaGetLastError());
+            }
         }
     }
     if (UNIT) {
@@ -592,11 +636,23 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         }
         for (size_t k = lv.s_steps.size(); k-- > 0;) {
             const SolveStep& st = lv.s_steps[k];
-            if (!st.bwd.cnt) continue;
+            if (!st.diag.cnt) continue;
             Timer t(h, K_S_BWD);
-            k_s_bwd<T, UNIT><<<(unsigned)st.bwd.cnt, 256, ss, h->stream>>>(h->d_fronts, items + st.bwd.off, (int)k,
-                                                                          sb.P, sb.inv, sb.C, sb.W, n, nrhs);
+            const unsigned gd = (unsigned)st.diag.cnt;
+            const Item* itd = items + st.diag.off;
+            switch (nrb) {
+                case 1: k_s_sdiag<T, 1, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: k_s_sdiag<T, 2, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: k_s_sdiag<T, 4, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: k_s_sdiag<T, 8, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: k_s_sdiag<T, 16, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+            }
             MF_CUDA(cudaGetLastError());
+            if (st.bwd.cnt) {
+                k_s_btile<T><<<(unsigned)st.bwd.cnt, 256, btile_smem<T>(), h->stream>>>(
+                    h->d_fronts, items + st.bwd.off, (int)k, sb.P, sb.C, sb.W, n, nrhs);
+                MF_CUDA(cudaGetLastError());
+            }
         }
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
@@ -625,13 +681,13 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
 int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* C, double* part) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve_with: nrhs chunk above 16"); return -1; }
-    SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, R, W, C, part};
+    SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, R, W, C, part, h->d_inv2};
     return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
 }
 int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
-    SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, h->d_R, h->d_W, h->d_C, h->d_part};
+    SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, h->d_R, h->d_W, h->d_C, h->d_part, h->d_inv2};
     return run_captured(h, 3, nrhs, 0, 0, [&]() {
         return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
     });
@@ -641,7 +697,7 @@ int launch_solve(mf_handle* h, int64_t nrhs) {
 int launch_solve_mixed(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
-    SolveBufs<float> sb{h->f32.P, h->f32.inv, h->f32.d, h->f32.R, h->f32.W, h->f32.C, h->f32.part};
+    SolveBufs<float> sb{h->f32.P, h->f32.inv, h->f32.d, h->f32.R, h->f32.W, h->f32.C, h->f32.part, h->f32.inv2};
     return run_captured(h, 4, nrhs, 0, 0, [&]() {
         return h->diag ? solve_impl<float, 1>(h, sb, (int)nrhs) : solve_impl<float, 0>(h, sb, (int)nrhs);
     });
