@@ -255,163 +255,244 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 
 // Diagonal block: factor + inverse, one CTA of 256 threads per front.
 //
-// The 16 x 16 threads each own a 4 x 4 tile of the 64 x 64 block in
-// registers (columns >= w are padded with the identity).  Right-looking
-// elimination with one barrier per pivot: step k reads column k from a
-// double-buffered shared vector, applies A_ij -= A_ik A_jk / p (p = A_kk;
-// the Cholesky and the LDLt update alike) to the tile, scales column k to
-// L_ik = A_ik / sqrt(p) (Cholesky) or A_ik / p (LDLt), and the owners of
-// column k + 1 publish it for the next step.  The inverse X = L^-1 (unit
-// diagonal for LDLt) follows by the row sweep: step k scales row k of X by
-// 1 / L_kk and eliminates it from the rows below, again on register tiles.
+// The 64 x 64 block (columns >= w padded with the identity) sits in shared
+// memory and is factored in four 16-column panels.  Per panel, warp 0
+// factors the 16 x 16 diagonal block in registers (lane i < 16 owns row i;
+// column k reaches the other lanes by shuffles, so the 16 dependent pivot
+// steps use no barrier) and inverts it (lane j owns column j).  All threads
+// then form the rows below as A L^-T (D^-1) with that inverse and apply the
+// rank-16 update to the trailing block; both are fully unrolled 16-term dot
+// products.  Finally the off-diagonal 16 x 16 blocks of X = L^-1 (unit
+// diagonal for LDLt) follow along the block sub-diagonals,
+// X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj.  About 26 barriers in all.
 constexpr int LDS = kNB + 4;  // shared-memory leading dimension of the GEMM stages
-constexpr int LDA = kNB + 1;  // leading dimension of the factored block in the diagonal kernel
+constexpr int LDA = kNB + 1;  // leading dimension of the block and its inverse in the diagonal kernel
+
+template <typename T>
+constexpr int diag_smem() { return (2 * kNB * LDA + 2 * kNB) * (int)sizeof(T); }
+
+// The pivot's diagonal entry dk (sqrt(p) for Cholesky, p for LDLt) and its
+// reciprocal.  FP32 (the mixed form, whose factor only preconditions the
+// FP64 refinement) uses the hardware reciprocal square root / reciprocal;
+// FP64 keeps the correctly rounded operations of the plain form.
+template <typename T, int LDLT>
+__device__ __forceinline__ void diag_pivot(T p, T& dk, T& ik);
+template <>
+__device__ __forceinline__ void diag_pivot<float, 0>(float p, float& dk, float& ik) {
+    ik = rsqrtf(p);
+    dk = p * ik;
+}
+template <>
+__device__ __forceinline__ void diag_pivot<float, 1>(float p, float& dk, float& ik) {
+    dk = p;
+    ik = __frcp_rn(p);
+}
+template <>
+__device__ __forceinline__ void diag_pivot<double, 0>(double p, double& dk, double& ik) {
+    dk = sqrt(p);
+    ik = 1.0 / dk;
+}
+template <>
+__device__ __forceinline__ void diag_pivot<double, 1>(double p, double& dk, double& ik) {
+    dk = p;
+    ik = 1.0 / p;
+}
 
 template <typename T, int LDLT>
-__global__ void __launch_bounds__(256) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
+__global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                               int c0, T* __restrict__ P, T* __restrict__ inv,
                                               T* __restrict__ d, const double* __restrict__ signs,
                                               long long* __restrict__ info) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Ls = reinterpret_cast<T*>(smem_raw);  // factored block, column major, ld LDA
-    T* vec = Ls + kNB * LDA;                 // 2 x 64 broadcast vectors
-    T* rinv = vec + 2 * kNB;                 // 1 / L_kk (Cholesky) or 1 / d_k
-    T* pivs = rinv + kNB;                    // L_kk (Cholesky) or d_k (LDLt)
+    T* A = reinterpret_cast<T*>(smem_raw);  // block, A[r + c * LDA]
+    T* X = A + kNB * LDA;                   // inverse, same layout
+    T* pivs = X + kNB * LDA;                // L_kk (Cholesky) or d_k (LDLt)
+    T* rinv = pivs + kNB;                   // 1 / L_kk or 1 / d_k
+    __shared__ int bad_s;
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int w = min(kNB, nn - c0);
-    const int tid = threadIdx.x;
-    const int ti = tid & 15, tj = tid >> 4;  // rows 4ti.., columns 4tj..
-    const int r0 = 4 * ti, q0 = 4 * tj;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     T* Pj = P + f.poff;
-    T a[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int i = r0 + r, j = q0 + c;
-            T v = (i == j) ? T(1) : T(0);
-            if (i >= j && i < w && j < w) v = Pj[(c0 + i) + (int64_t)(c0 + j) * ld];
-            a[r][c] = v;
-        }
-    // column 0 into the first broadcast vector
-    if (tj == 0)
-#pragma unroll
-        for (int r = 0; r < 4; ++r) vec[r0 + r] = a[r][0];
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        T v = (r == c) ? T(1) : T(0);
+        if (r >= c && r < w && c < w) v = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
+        A[r + c * LDA] = v;
+        X[r + c * LDA] = T(0);
+    }
+    if (tid == 0) bad_s = -1;
     __syncthreads();
-    int bad = -1;
-    for (int k = 0; k < kNB; ++k) {
-        const T* col = vec + (k & 1) * kNB;
-        T* nxt = vec + ((k + 1) & 1) * kNB;
-        const T pv = col[k];
-        if (k < w) {
-            const double sg = pivot_sign(signs, LDLT, (int64_t)f.col0 + c0 + k);
-            if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) { bad = k; break; }  // uniform
-        }
-        const T rp = T(1) / pv;
-        T ci[4], cj[4];
+    for (int p = 0; p < 4; ++p) {
+        const int pb = p * 16;
+        if (warp == 0) {
+            const int i = lane & 15;  // lanes 16..31 mirror 0..15
+            T a[16];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) { ci[r] = col[r0 + r]; cj[r] = col[q0 + r] * rp; }
-        // trailing update A_ij -= A_ik A_jk / p  (k < j <= i)
+            for (int j = 0; j < 16; ++j) a[j] = j <= i ? A[(pb + i) + (pb + j) * LDA] : T(0);
+            T mypiv = T(1), myrinv = T(1);
+            int bad = -1;
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+            for (int k = 0; k < 16; ++k) {
+                const T pv = __shfl_sync(0xffffffffu, a[k], k);
+                if (bad < 0 && pb + k < w) {
+                    const double sg = pivot_sign(signs, LDLT, (int64_t)f.col0 + c0 + pb + k);
+                    if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) bad = pb + k;
+                }
+                // after a rejected pivot the remaining steps run on junk and are discarded
+                T dk, ik;
+                diag_pivot<T, LDLT>(pv, dk, ik);
+                const T aik = a[k];
+                const T lik = aik * ik;
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (q0 + c > k && r0 + r >= q0 + c) a[r][c] -= ci[r] * cj[c];
-        // column k: L_ik = A_ik / sqrt(p) (Cholesky) or A_ik / p (LDLt)
-        const T sc = LDLT ? rp : T(1) / sqrt(pv);
-        if (tj == (k >> 2)) {
-            const int cc = k & 3;
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (c == cc)
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        const int i = r0 + r;
-                        if (i > k) a[r][c] *= sc;
-                        else if (i == k && !LDLT) a[r][c] = pv * sc;
+                for (int j = 0; j < 16; ++j) {
+                    if (j > k) {  // resolved at compile time once both loops are unrolled
+                        const T u = __shfl_sync(0xffffffffu, LDLT ? aik : lik, j);
+                        if (i >= j) a[j] -= lik * u;
                     }
+                }
+                if (i > k) a[k] = lik;
+                else if (i == k) {
+                    if (!LDLT) a[k] = dk;
+                    mypiv = dk;
+                    myrinv = ik;
+                }
+            }
+            // inverse of the 16 x 16 factor: lane j owns column j
+            const int j = i;
+            T x[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                T acc = T(0);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    if (k < r) {  // resolved at compile time once both loops are unrolled
+                        const T lrk = __shfl_sync(0xffffffffu, a[k], r);
+                        if (k >= j) acc += lrk * x[k];
+                    }
+                }
+                const T rr = __shfl_sync(0xffffffffu, myrinv, r);
+                x[r] = r < j ? T(0) : (r == j ? (LDLT ? T(1) : rr) : (LDLT ? -acc : -acc * rr));
+            }
+            if (lane < 16) {
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj)
+                    if (jj <= i) A[(pb + i) + (pb + jj) * LDA] = a[jj];
+#pragma unroll
+                for (int r = 0; r < 16; ++r) X[(pb + r) + (pb + j) * LDA] = x[r];
+                pivs[pb + i] = mypiv;
+                rinv[pb + i] = myrinv;
+            }
+            if (lane == 0 && bad >= 0) bad_s = bad;
         }
-        if (tid == 0) { rinv[k] = sc; pivs[k] = LDLT ? pv : pv * sc; }
-        // publish column k + 1 (already updated by this step)
-        if (k + 1 < kNB && tj == ((k + 1) >> 2)) {
-            const int cc = (k + 1) & 3;
+        __syncthreads();
+        if (bad_s >= 0) break;  // uniform
+        const int m = 48 - pb;  // rows / columns after the panel
+        if (m == 0) break;
+        // rows below: L_rc = sum_{q <= c} A_r,pb+q Xpp_c,q (/ d_c)
+        T res[3];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (c == cc)
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            res[s] = T(0);
+            if (o < m * 16) {
+                const int r = pb + 16 + o % m, c = o / m;
+                T acc = T(0);
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) nxt[r0 + r] = a[r][c];
+                for (int q = 0; q < 16; ++q) acc += A[r + (pb + q) * LDA] * X[(pb + c) + (pb + q) * LDA];
+                res[s] = LDLT ? acc * rinv[pb + c] : acc;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            if (o < m * 16) A[(pb + 16 + o % m) + (pb + o / m) * LDA] = res[s];
+        }
+        __syncthreads();
+        // trailing update A_ij -= sum_q L_iq (d_q) L_jq, pb+16 <= j <= i
+        for (int e = tid; e < m * m; e += 256) {
+            const int i = pb + 16 + e % m, j = pb + 16 + e / m;
+            if (i >= j) {
+                T acc = T(0);
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    T lj = A[j + (pb + q) * LDA];
+                    if (LDLT) lj *= pivs[pb + q];
+                    acc += A[i + (pb + q) * LDA] * lj;
+                }
+                A[i + j * LDA] -= acc;
+            }
         }
         __syncthreads();
     }
-    if (bad >= 0) {
-        if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
+    if (bad_s >= 0) {  // uniform
+        if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad_s + 1));
         return;
     }
-    // factored block: to shared memory (the inverse reads its columns) and to the panel
+    // off-diagonal 16 x 16 blocks of the inverse, by block distance
+    for (int dist = 1; dist < 4; ++dist) {
+        const int nb = 4 - dist;
+        T tmp[3];
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+        for (int s = 0; s < 3; ++s) {  // T_ij = sum_{k=j}^{i-1} L_ik X_kj
+            const int o = tid + 256 * s;
+            tmp[s] = T(0);
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                T acc = T(0);
+                for (int bk = bj; bk < bi; ++bk)
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int i = r0 + r, j = q0 + c;
-            Ls[i + j * LDA] = i >= j ? a[r][c] : T(0);
-            if (i >= j && i < w && j < w) Pj[(c0 + i) + (int64_t)(c0 + j) * ld] = a[r][c];
+                    for (int q = 0; q < 16; ++q)
+                        acc += A[(16 * bi + r) + (16 * bk + q) * LDA] * X[(16 * bk + q) + (16 * bj + c) * LDA];
+                tmp[s] = acc;
+            }
         }
-    if (LDLT && tid < w) d[f.col0 + c0 + tid] = pivs[tid];
-    // inverse X = L^-1 by the row sweep: step k scales row k by 1 / L_kk and
-    // eliminates it from the rows below; X tiles stay in registers
+        __syncthreads();
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) a[r][c] = (r0 + r == q0 + c) ? T(1) : T(0);
-    if (ti == 0)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) vec[q0 + c] = a[0][c];
-    __syncthreads();
-    for (int k = 0; k < kNB; ++k) {
-        const T* row = vec + (k & 1) * kNB;  // row k of X before its scaling
-        T* nxt = vec + ((k + 1) & 1) * kNB;
-        const T rk = LDLT ? T(1) : rinv[k];
-        T xr[4], li[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c) xr[c] = row[q0 + c] * rk;
-#pragma unroll
-        for (int r = 0; r < 4; ++r) li[r] = Ls[(r0 + r) + k * LDA];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-                if (r0 + r > k && q0 + c <= k) a[r][c] -= li[r] * xr[c];
-        if (ti == (k >> 2)) {
-            const int rr = k & 3;
-#pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (r == rr)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) a[r][c] *= rk;
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
+            }
         }
-        if (k + 1 < kNB && ti == ((k + 1) >> 2)) {
-            const int rr = (k + 1) & 3;
+        __syncthreads();
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
-                if (r == rr)
+        for (int s = 0; s < 3; ++s) {  // X_ij = -X_ii T_ij
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                T acc = T(0);
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) nxt[q0 + c] = a[r][c];
+                for (int q = 0; q < 16; ++q)
+                    acc += X[(16 * bi + r) + (16 * bi + q) * LDA] * X[(16 * bi + q) + (16 * bj + c) * LDA];
+                tmp[s] = -acc;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
+            }
         }
         __syncthreads();
     }
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        if (r >= c && r < w && c < w) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = A[r + c * LDA];
+    }
+    if (LDLT && tid < w) d[f.col0 + c0 + tid] = pivs[tid];
     T* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const int i = r0 + r, j = q0 + c;
-            dst[i + j * kNB] = (i < w && j < w) ? a[r][c] : T(0);
-        }
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        dst[e] = (r < w && c < w) ? X[r + c * LDA] : T(0);
+    }
 }
-template <typename T>
-constexpr int diag_smem() { return (kNB * LDA + 4 * kNB) * (int)sizeof(T); }
 
 // ---------------------------------------------------------------------------
 // Tile GEMM with a cp.async double-buffered K loop:
