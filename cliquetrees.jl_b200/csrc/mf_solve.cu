@@ -285,19 +285,34 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
 //             k_s_btile  columns left: W[c] -= sum_i L[k0 + i, c] x_K[i].
 // ---------------------------------------------------------------------------
 template <typename T, int NR>
-constexpr int sdiag_smem() { return kSolveNB * NR * (int)sizeof(T); }
+constexpr int sdiag_smem() { return (kSolveNB * NR + 16 * kSolveNB) * (int)sizeof(T); }
 template <typename T, int NR>
-constexpr int ftile_smem() { return (kSolveNB * NR + 4 * NR * kFwdRows) * (int)sizeof(T); }
+constexpr int ftile_smem() { return (kSolveNB * NR + 4 * NR * kFwdRows + kSolveNB * kFwdRows) * (int)sizeof(T); }
 template <typename T>
-constexpr int btile_smem() { return kSolveNB * kMaxRhs * (int)sizeof(T); }
+constexpr int btile_smem() { return (kSolveNB * kMaxRhs + kSolveNB * kNB) * (int)sizeof(T); }
+
+// element copy global -> shared that stays in flight (cp.async); a false
+// `valid` writes zero and reads nothing
+template <typename T>
+__device__ __forceinline__ void cpa(T* dst, const T* src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    const int nb = valid ? (int)sizeof(T) : 0;
+    if (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(src), "r"(nb) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(src), "r"(nb) : "memory");
+}
+__device__ __forceinline__ void cpa_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
 
 // x_K = X_K b_K (BWD = 0) or X_K^T b_K (BWD = 1), spread over kDiagSplit
 // CTAs per front so that the 256 x 256 inverse streams through many SMs:
-// CTA q owns outputs a in [16 q, 16 q + 16); thread t takes output
-// 16 q + t / 16 and every 16th input starting at t % 16, then half-warp
-// shuffles add the 16 partial sums.  Reads are along the columns of X
-// (forward: 16 consecutive rows of a column; backward: 16 consecutive
-// entries of column a), and the zero triangle is skipped.
+// CTA q owns outputs a in [16 q, 16 q + 16); its 16 rows (forward) or 16
+// columns (backward) of X are staged in shared memory with every load in
+// flight at once, then thread t takes output 16 q + t / 16 and every 16th
+// input starting at t % 16, and half-warp shuffles add the partial sums.
 constexpr int kDiagSplit = kSolveNB / 16;
 
 template <typename T, int NR, int BWD>
@@ -306,26 +321,38 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
                                                  const T* __restrict__ W, int64_t n, int nrhs) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* b = reinterpret_cast<T*>(sm_raw);  // [r][c] : b[c + r * kSolveNB]
+    T* xt = b + kSolveNB * NR;            // forward: xt[c * 16 + a - 16q]; backward: xt[(a - 16q) * 256 + c]
     const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
     const int q = blockIdx.x % kDiagSplit;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, f.nn - k0), ld2 = super_ld(wK);
     if (16 * q >= wK) return;  // whole CTA
     const T* X = inv2 + f.i2off + (int64_t)step * kSolveNB * kSolveNB;
+    for (int e = threadIdx.x; e < 16 * kSolveNB; e += blockDim.x) {
+        if (!BWD) {
+            const int c = e >> 4, a = 16 * q + (e & 15);
+            const bool v = a < wK && c <= a;
+            cpa(xt + e, v ? X + a + (int64_t)c * ld2 : X, v);
+        } else {
+            const int a = 16 * q + (e >> 8), c = e & 255;
+            const bool v = a < wK && c >= a && c < wK;
+            cpa(xt + e, v ? X + c + (int64_t)a * ld2 : X, v);
+        }
+    }
     for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
         const int c = i % kSolveNB, r = i / kSolveNB;
         b[i] = (c < wK && r < nrhs) ? W[f.col0 + k0 + c + (int64_t)r * n] : T(0);
     }
+    cpa_wait_all();
     __syncthreads();
-    const int a = 16 * q + (threadIdx.x >> 4), cl = threadIdx.x & 15;
+    const int al = threadIdx.x >> 4, a = 16 * q + al, cl = threadIdx.x & 15;
     T acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
     if (a < wK) {
-        // forward: inputs c <= a, X[a, c]; backward: inputs c >= a, X[c, a]
         const int cb = BWD ? a : 0, ce = BWD ? wK : a + 1;
 #pragma unroll 4
         for (int c = cb + cl; c < ce; c += 16) {
-            const T x = BWD ? X[c + (int64_t)a * ld2] : X[a + (int64_t)c * ld2];
+            const T x = BWD ? xt[al * kSolveNB + c] : xt[c * 16 + al];
 #pragma unroll
             for (int r = 0; r < NR; ++r) acc[r] += x * b[c + r * kSolveNB];
         }
@@ -342,7 +369,8 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
             if (r < nrhs) C[f.col0 + k0 + a + (int64_t)r * n] = acc[r];
 }
 
-// forward rows below super-block K: W (rows < nn) or R_j (rows >= nn) -= L[rows, K] x_K
+// forward rows below super-block K: W (rows < nn) or R_j (rows >= nn) -= L[rows, K] x_K.
+// The 64-row x 256-column panel tile is staged in shared memory first.
 template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
@@ -350,6 +378,7 @@ __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ front
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * NR
     T* red = xs + kSolveNB * NR;           // 4 * NR * kFwdRows
+    T* tile = red + 4 * NR * kFwdRows;     // tile[c * 64 + r]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
@@ -357,65 +386,76 @@ __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ front
     const int r0 = k0 + wK + it.a * kFwdRows;
     const int nr = min(kFwdRows, nj - r0);
     const int tid = threadIdx.x;
+    const T* Pt = P + f.poff + r0 + (int64_t)k0 * ld;
+    for (int e = tid; e < kSolveNB * kFwdRows; e += 256) {
+        const int c = e >> 6, r = e & (kFwdRows - 1);
+        const bool v = c < wK && r < nr;
+        cpa(tile + e, v ? Pt + r + (int64_t)c * ld : Pt, v);
+    }
     for (int i = tid; i < kSolveNB * NR; i += 256) {
         const int a = i % kSolveNB, r = i / kSolveNB;
         xs[i] = (a < wK && r < nrhs) ? C[f.col0 + k0 + a + (int64_t)r * n] : T(0);
     }
+    cpa_wait_all();
     __syncthreads();
     const int rl = tid & (kFwdRows - 1), g = tid / kFwdRows;  // row, 64-column group
     T acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
-    if (rl < nr) {
-        const T* pq = P + f.poff + (r0 + rl) + (int64_t)(k0 + g * kNB) * ld;
-        const int cend = min(kNB, wK - g * kNB);
 #pragma unroll 8
-        for (int c = 0; c < cend; ++c) {
-            const T l = pq[(int64_t)c * ld];
+    for (int c = g * kNB; c < g * kNB + kNB; ++c) {
+        const T l = tile[c * kFwdRows + rl];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) acc[r] += l * xs[g * kNB + c + r * kSolveNB];
-        }
+        for (int r = 0; r < NR; ++r) acc[r] += l * xs[c + r * kSolveNB];
     }
 #pragma unroll
     for (int r = 0; r < NR; ++r) red[(g * NR + r) * kFwdRows + rl] = acc[r];
     __syncthreads();
     if (g == 0 && rl < nr) {
         T* Rj = R + f.roff * nrhs;
-        const int q = r0 + rl;
+        const int qr = r0 + rl;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
             if (r < nrhs) {
                 const T v = red[(0 * NR + r) * kFwdRows + rl] + red[(1 * NR + r) * kFwdRows + rl] +
                             red[(2 * NR + r) * kFwdRows + rl] + red[(3 * NR + r) * kFwdRows + rl];
-                if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
-                else Rj[(q - nn) + r * na] -= v;
+                if (qr < nn) W[f.col0 + qr + (int64_t)r * n] -= v;
+                else Rj[(qr - nn) + r * na] -= v;
             }
         }
     }
 }
 
 // backward columns left of super-block K (64-column tile it.a):
-// W[c] -= sum_i L[k0 + i, c] x_K[i]; one warp per column, lanes along the
-// column (coalesced), then a shuffle reduction per right-hand side
+// W[c] -= sum_i L[k0 + i, c] x_K[i].  The 256-row x 64-column panel tile is
+// staged in shared memory; one warp per column, then a shuffle reduction.
 template <typename T>
 __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * kMaxRhs
+    T* tile = xs + kSolveNB * kMaxRhs;     // tile[c * 256 + i]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
     const int c0 = it.a * kNB, wc = min(kNB, k0 - c0);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const T* Pt = P + f.poff + (int64_t)c0 * ld + k0;
+    for (int e = tid; e < kNB * kSolveNB; e += 256) {
+        const int c = e >> 8, i = e & (kSolveNB - 1);
+        const bool v = c < wc && i < wK;
+        cpa(tile + e, v ? Pt + (int64_t)c * ld + i : Pt, v);
+    }
     for (int i = tid; i < wK * nrhs; i += 256) {
         const int a = i % wK, r = i / wK;
         xs[a + r * kSolveNB] = C[f.col0 + k0 + a + (int64_t)r * n];
     }
+    cpa_wait_all();
     __syncthreads();
     for (int cc = warp; cc < wc; cc += 8) {
-        const T* pc = P + f.poff + (int64_t)(c0 + cc) * ld + k0;
+        const T* pc = tile + cc * kSolveNB;
         T acc[kMaxRhs];
 #pragma unroll
         for (int r = 0; r < kMaxRhs; ++r) acc[r] = T(0);
@@ -553,7 +593,14 @@ template <typename T, int UNIT>
 static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 8>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 4>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 2>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 1>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_btile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, btile_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 16, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small_solve_smem<T, 16>()));
