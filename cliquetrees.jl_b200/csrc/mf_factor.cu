@@ -212,6 +212,11 @@ __device__ __forceinline__ int lower_bound_i32(const int32_t* a, int n, int v) {
     return lo;
 }
 
+// One CTA per 16 parent columns; warp w owns parent columns c0 + w and
+// c0 + w + 8 and adds, child after child in a fixed order, the child
+// columns that map onto them.  A column is only ever touched by its warp, so
+// no block barrier and no atomics are needed and the sums are deterministic;
+// the eight warps stream independently.
 template <typename T>
 __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                             const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
@@ -220,13 +225,14 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp, lm = f.ldm;
     const int c0 = it.a * kEAcols, c1 = min(c0 + kEAcols, nj);
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T* Pj = P + f.poff;
     T* Mj = M + f.moff;
-    // zero the update-matrix columns this CTA owns
-    for (int c = max(c0, nn); c < c1; ++c)
-        for (int r = tid; r < na; r += nt) Mj[r + (int64_t)(c - nn) * lm] = T(0);
-    __syncthreads();
+    // zero the update-matrix columns this warp owns
+    for (int col = c0 + warp; col < c1; col += 8)
+        if (col >= nn)
+            for (int r = lane; r < na; r += 32) Mj[r + (int64_t)(col - nn) * lm] = T(0);
+    __syncwarp();
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na, lmc = fc.ldm;
@@ -236,16 +242,13 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
         const int b1 = lower_bound_i32(rel, ma, c1);
         for (int b = b0; b < b1; ++b) {
             const int col = rel[b];
+            if (((col - c0) & 7) != warp) continue;  // the owner warp of this parent column
             const T* mc = Mc + (int64_t)b * lmc;
-            if (col < nn) {
-                T* pc = Pj + (int64_t)col * ld;
-                for (int a = b + tid; a < ma; a += nt) pc[rel[a]] += mc[a];
-            } else {
-                T* dst = Mj + (int64_t)(col - nn) * lm - nn;
-                for (int a = b + tid; a < ma; a += nt) dst[rel[a]] += mc[a];
-            }
+            T* dst = col < nn ? Pj + (int64_t)col * ld : Mj + (int64_t)(col - nn) * lm - nn;
+#pragma unroll 4
+            for (int a = b + lane; a < ma; a += 32) dst[rel[a]] += mc[a];
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
