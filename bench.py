@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--rates", default="50,200,1000", help="config 5: Poisson arrival rates (requests/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="mixed form: tcgen05 tiles on every level")
     ap.add_argument("--mixed-profile", action="store_true", help="with --profile-only: the mixed form")
     return ap.parse_args()
 
@@ -407,6 +408,7 @@ def main():
             "gpu_launches": mixed["gpu_launches"],
             "roofline": roof_mixed,
             "kernels": mixed["kernels"],
+            "autotune": mixed["autotune"],
             "clocks": mixed["clocks"],
             "plain_fp64": {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
                            "p50_ms": plain["p50_ms"], "p99_ms": plain["p99_ms"],
@@ -662,6 +664,16 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
     with torch.cuda.stream(stream):
         step_device()
     stream.synchronize()
+    tune = None
+    if mixed and not args.no_autotune:
+        # per-level choice of tcgen05 vs FFMA tiles, timed on these values
+        t = F.autotune(3)
+        tune = {"tc_ms": round(t["tc_ms"], 3), "ffma_ms": round(t["ffma_ms"], 3),
+                "tuned_ms": round(t["tuned_ms"], 3), "levels": int(t["tc_steps"].size),
+                "levels_tc_steps": int(t["tc_steps"].sum()), "levels_tc_syrk": int(t["tc_syrk"].sum())}
+        with torch.cuda.stream(stream):
+            step_device()
+        stream.synchronize()
     X = X_dev.cpu().numpy().reshape(n, nrhs, order="F")
     eta = seg_backward_error(A, X, B, work.segments)
     if profile_only:
@@ -755,6 +767,7 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
                 "d2h_bytes_per_step": int(n * nrhs * 8 + 8), "backward_error": eta_e2e,
                 "p50_ms": float(np.percentile(e2e_ms, 50)), "p99_ms": float(np.percentile(e2e_ms, 99))},
         "gpu_launches": launches_per_step * args.steps, "kernels": ktimes, "clocks": ck, "flops": fl,
+        "autotune": tune,
     }
 
 

@@ -588,6 +588,86 @@ int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* us
     return 0;
 }
 
+int mf_autotune(mf_handle* h, int reps, double* ms) {
+    if (!h) { set_error("null handle"); return -1; }
+    if (!h->mixed) { set_error("mf_autotune: call mf_enable_mixed first"); return -1; }
+    if (!h->cur_nz) { set_error("mf_autotune: no values (mf_assemble)"); return -1; }
+    DeviceGuard g(h->device);
+    const size_t nl = h->levels.size();
+    reps = std::max(1, reps);
+    // best[v][L]: the fastest of `reps` timed runs (after one warm-up run) of
+    // variant v (0 = FFMA tiles, 1 = tcgen05 tiles) on level L
+    std::vector<double> steps_best[2], syrk_best[2];
+    const bool keep_profile = h->profile;
+    h->profile = false;
+    h->tuning = true;
+    int rc = 0;
+    int64_t inf = 0;
+    for (int v = 0; v < 2 && !rc; ++v) {
+        for (Level& lv : h->levels) lv.tc_steps = lv.tc_syrk = v;
+        steps_best[v].assign(nl, 1e30);
+        syrk_best[v].assign(nl, 1e30);
+        for (int r = 0; r <= reps && !rc; ++r) {
+            rc = launch_assemble_mixed(h, h->cur_nz);
+            if (!rc) rc = init_info(h);
+            if (!rc) rc = launch_factor_mixed(h);
+            if (!rc) rc = read_info(h, &inf);
+            if (rc || r == 0) continue;
+            for (size_t L = 0; L < nl; ++L) {
+                steps_best[v][L] = std::min(steps_best[v][L], h->tune_steps_ms[L]);
+                syrk_best[v][L] = std::min(syrk_best[v][L], h->tune_syrk_ms[L]);
+            }
+        }
+    }
+    h->tuning = false;
+    h->profile = keep_profile;
+    double tot[3] = {0.0, 0.0, 0.0};
+    for (size_t L = 0; L < nl && !rc; ++L) {
+        Level& lv = h->levels[L];
+        lv.tc_steps = steps_best[1][L] <= steps_best[0][L];
+        lv.tc_syrk = syrk_best[1][L] <= syrk_best[0][L];
+        tot[0] += steps_best[1][L] + syrk_best[1][L];
+        tot[1] += steps_best[0][L] + syrk_best[0][L];
+        tot[2] += std::min(steps_best[0][L], steps_best[1][L]) + std::min(syrk_best[0][L], syrk_best[1][L]);
+    }
+    if (rc) {
+        for (Level& lv : h->levels) lv.tc_steps = lv.tc_syrk = 1;
+        return rc;
+    }
+    // captured factorizations hold the previous kernel choice
+    release_graphs(h);
+    if (ms) {
+        int64_t n_steps = 0, n_syrk = 0;
+        for (const Level& lv : h->levels) { n_steps += lv.tc_steps; n_syrk += lv.tc_syrk; }
+        ms[0] = tot[0];
+        ms[1] = tot[1];
+        ms[2] = tot[2];
+        ms[3] = (double)n_steps;
+        ms[4] = (double)n_syrk;
+        ms[5] = (double)nl;
+    }
+    return 0;
+}
+
+int mf_kernel_choice(const mf_handle* h, int32_t* tc_steps, int32_t* tc_syrk) {
+    if (!h) { set_error("null handle"); return -1; }
+    for (size_t L = 0; L < h->levels.size(); ++L) {
+        if (tc_steps) tc_steps[L] = h->levels[L].tc_steps;
+        if (tc_syrk) tc_syrk[L] = h->levels[L].tc_syrk;
+    }
+    return 0;
+}
+
+int mf_set_kernel_choice(mf_handle* h, const int32_t* tc_steps, const int32_t* tc_syrk) {
+    if (!h) { set_error("null handle"); return -1; }
+    for (size_t L = 0; L < h->levels.size(); ++L) {
+        if (tc_steps) h->levels[L].tc_steps = tc_steps[L] != 0;
+        if (tc_syrk) h->levels[L].tc_syrk = tc_syrk[L] != 0;
+    }
+    release_graphs(h);
+    return 0;
+}
+
 static int refined_chunks(mf_handle* h, double* hostB, double* devB, int64_t nrhs, int64_t ldb, const int64_t* dperm,
                           double tol, int maxit, int* iters, double* eta) {
     const int64_t cap = (int64_t)h->n * h->nrhs_cap;

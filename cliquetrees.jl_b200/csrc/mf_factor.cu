@@ -907,7 +907,15 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
     const Item* items = h->d_items;
-    for (const Level& lv : h->levels) {
+    // per-level timing while autotuning (profile mode: no graph, synchronised)
+    cudaEvent_t tev[3] = {nullptr, nullptr, nullptr};
+    if (h->tuning) {
+        for (auto& e : tev) MF_CUDA(cudaEventCreate(&e));
+        h->tune_steps_ms.assign(h->levels.size(), 0.0);
+        h->tune_syrk_ms.assign(h->levels.size(), 0.0);
+    }
+    for (size_t L = 0; L < h->levels.size(); ++L) {
+        const Level& lv = h->levels[L];
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
             k_small<T, LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream>>>(
@@ -921,9 +929,10 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                                                                 h->d_chdtgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
+        if (h->tuning) MF_CUDA(cudaEventRecord(tev[0], h->stream));
         for (const PanelStep& st : lv.steps) {
             const int c0 = st.b * kOB + st.s * kNB;
-            if (std::is_same<T, float>::value && h->use_tc) {
+            if (std::is_same<T, float>::value && h->use_tc && lv.tc_steps) {
                 // single precision: the GEMM roles run on the tcgen05 tensor cores
                 const FactorBufs<float>& f32b = reinterpret_cast<const FactorBufs<float>&>(fb);
                 int rc;
@@ -972,18 +981,31 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 MF_CUDA(cudaGetLastError());
             }
         }
-        if (std::is_same<T, float>::value && h->use_tc) {
-            if (!lv.syrk_tc.cnt) continue;
-            Timer t(h, K_SYRK);
-            int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
-            if (rc) return rc;
+        if (h->tuning) MF_CUDA(cudaEventRecord(tev[1], h->stream));
+        if (std::is_same<T, float>::value && h->use_tc && lv.tc_syrk) {
+            if (lv.syrk_tc.cnt) {
+                Timer t(h, K_SYRK);
+                int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
+                if (rc) return rc;
+            }
         } else if (lv.syrk.cnt) {
             Timer t(h, K_SYRK);
             k_gemm<T, G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, gs, h->stream>>>(
                 h->d_fronts, items + lv.syrk.off, 0, 0, fb.P, fb.M, fb.d, fb.inv);
             MF_CUDA(cudaGetLastError());
         }
+        if (h->tuning) {
+            MF_CUDA(cudaEventRecord(tev[2], h->stream));
+            MF_CUDA(cudaEventSynchronize(tev[2]));
+            float a = 0.f, b = 0.f;
+            MF_CUDA(cudaEventElapsedTime(&a, tev[0], tev[1]));
+            MF_CUDA(cudaEventElapsedTime(&b, tev[1], tev[2]));
+            h->tune_steps_ms[L] += a;
+            h->tune_syrk_ms[L] += b;
+        }
     }
+    if (h->tuning)
+        for (auto& e : tev) cudaEventDestroy(e);
     if (h->inv2_items.cnt) {
         Timer t(h, K_OTHER);
         k_inv256<T><<<grid_for(h->inv2_items.cnt), 256, inv256_smem<T>(), h->stream>>>(
@@ -994,7 +1016,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
 }
 
 int run_captured(mf_handle* h, int64_t k0, int64_t k1, int64_t k2, int64_t k3, const std::function<int()>& body) {
-    if (!h->use_graphs || h->profile || !h->stream) return body();
+    if (!h->use_graphs || h->profile || h->tuning || !h->stream) return body();
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     MF_CUDA(cudaStreamIsCapturing(h->stream, &cs));
     if (cs != cudaStreamCaptureStatusNone) return body();

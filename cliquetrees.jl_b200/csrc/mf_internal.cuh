@@ -73,6 +73,7 @@ constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
 constexpr int kSolveRows = 256; // rows per gather work item
 constexpr int kTcSyrkN = 128;   // tile columns of the tensor-core SYRK
+constexpr int kTcTrailN = 128;  // tile columns of the tensor-core trailing update
 constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
@@ -108,6 +109,10 @@ struct Level {
     ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
     ItemList s_bwd_red;      // (front, col tile, first partial slot)
     int max_nn_blocked = 0;
+    // FP32 kernel choice of this level, set by mf_autotune: 1 = tcgen05
+    // tensor-core tiles (128 x 64 / 128 x 128), 0 = FFMA tiles (64 x 64)
+    int tc_steps = 1;        // left-looking, TRSM and trailing roles of the panel steps
+    int tc_syrk = 1;         // the SYRK role
 };
 
 struct KernelTimes {
@@ -266,6 +271,9 @@ struct mf_handle {
     // optional per-kernel timing
     bool profile = false;
     mf::KernelTimes times;
+    // autotuning: per-level times of the panel steps and of the SYRK
+    bool tuning = false;
+    std::vector<double> tune_steps_ms, tune_syrk_ms;
     // CUDA graphs of the factorization and solve launch sequences
     bool use_graphs = true;
     std::vector<mf::GraphEntry> graphs;

@@ -329,6 +329,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     auto begin = [&](ItemList& l) { l.off = (int64_t)items.size(); };
     auto end = [&](ItemList& l) { l.cnt = (int64_t)items.size() - l.off; };
     auto push = [&](int32_t f, int32_t a, int32_t b) { items.push_back(Item{f, a, b, 0}); };
+    std::vector<Item> gseg;  // forward-gather segments, appended after the levels
 
     for (int L = 0; L <= max_level; ++L) {
         Level& lv = h->levels[L];
@@ -422,8 +423,8 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                         const int e = std::min(f.nn, (ob + 1) * kOB);
                         if (e >= f.nn) continue;
                         const int nj = f.nn + f.na;
-                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
-                            const int cs = e + tj * kTile;
+                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTcTrailN); ++tj) {
+                            const int cs = e + tj * kTcTrailN;
                             // rows from the first 128-aligned tile that reaches the diagonal
                             for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti) push(j, ti, tj);
                         }
@@ -463,13 +464,34 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (solve_small(f)) push(j, 0, 0);
         }
         end(lv.s_small);
+        // forward gather: item (front, row tile, first segment, segments);
+        // a segment (child, a0, a1) is the run rel[a0:a1] of a child's update
+        // rows that lands in the tile, children in reverse order
         begin(lv.s_gather);
         int max_sblocks = 0;
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (solve_small(f)) continue;
-            int nj = f.nn + f.na;
-            for (int t = 0; t < cdiv(nj, kSolveRows); ++t) push(j, t, 0);
+            const int nj = f.nn + f.na;
+            const int nt = (int)cdiv(nj, kSolveRows);
+            std::vector<std::vector<Item>> per_tile((size_t)nt);
+            for (int32_t p = f.chd1 - 1; p >= f.chd0; --p) {
+                const int32_t c = h->h_exec_chd[(size_t)p];
+                const Front& fc = h->h_fronts[(size_t)c];
+                const int32_t* rel = h->h_exec_rel.data() + fc.sep0;
+                int a = 0;
+                while (a < fc.na) {
+                    const int t = rel[a] / kSolveRows;
+                    int b = a + 1;
+                    while (b < fc.na && rel[b] / kSolveRows == t) ++b;
+                    per_tile[(size_t)t].push_back(Item{c, a, b, 0});
+                    a = b;
+                }
+            }
+            for (int t = 0; t < nt; ++t) {
+                items.push_back(Item{j, t, (int32_t)gseg.size(), (int32_t)per_tile[(size_t)t].size()});
+                gseg.insert(gseg.end(), per_tile[(size_t)t].begin(), per_tile[(size_t)t].end());
+            }
             max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kSolveNB));
         }
         end(lv.s_gather);
@@ -489,8 +511,10 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 const Front& f = h->h_fronts[j];
                 if (solve_small(f) || f.nn <= k0) continue;
                 const int w = std::min(kSolveNB, f.nn - k0);
-                const int below = f.nn + f.na - (k0 + w);
-                for (int t = 0; t < (int)cdiv(below, kFwdRows); ++t) push(j, t, 0);
+                // 64-row tiles from the 4-aligned row at or before the first row below the block
+                const int below = f.nn + f.na - ((k0 + w) & ~3);
+                if (f.nn + f.na > k0 + w)
+                    for (int t = 0; t < (int)cdiv(below, kFwdRows); ++t) push(j, t, 0);
             }
             end(st.fwd);
             begin(st.bwd);
@@ -518,6 +542,17 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_bwd_red);
         for (const Item& r : red) items.push_back(r);
         end(lv.s_bwd_red);
+    }
+    {
+        const int64_t base = (int64_t)items.size();
+        if (base + (int64_t)gseg.size() > INT32_MAX) {
+            set_error("plan: too many work items");
+            return -3;
+        }
+        for (const Level& lv : h->levels)
+            for (int64_t i = lv.s_gather.off; i < lv.s_gather.off + lv.s_gather.cnt; ++i)
+                items[(size_t)i].b += (int32_t)base;
+        items.insert(items.end(), gseg.begin(), gseg.end());
     }
     begin(h->inv2_items);
     for (int64_t e = 0; e < (int64_t)h->h_fronts.size(); ++e) {

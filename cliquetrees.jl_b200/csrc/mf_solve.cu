@@ -83,11 +83,28 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* _
         const int ma = fc.na;
         const int32_t* rel = reltgt + fc.sep0;
         const T* Mc = R + fc.roff * nrhs;
-        for (int i = lane; i < ma * nrhs; i += 32) {
-            const int a = i % ma, r = i / ma;
-            const int q = rel[a];
-            if (q < nn) C1[q + r * kSmallMax] += Mc[i];
-            else Rj[(q - nn) + r * na] += Mc[i];
+        // four loads per lane in flight before the adds (the child's rows
+        // are distinct, so one child's adds never collide)
+        for (int i0 = 0; i0 < ma * nrhs; i0 += 128) {
+            int qv[4];
+            T mv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int i = i0 + 32 * u + lane;
+                qv[u] = -1;
+                mv[u] = T(0);
+                if (i < ma * nrhs) {
+                    qv[u] = rel[i % ma];
+                    mv[u] = Mc[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (qv[u] < 0) continue;
+                const int r = (i0 + 32 * u + lane) / ma;
+                if (qv[u] < nn) C1[qv[u] + r * kSmallMax] += mv[u];
+                else Rj[(qv[u] - nn) + r * na] += mv[u];
+            }
         }
         __syncwarp();
     }
@@ -165,27 +182,50 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
-    // C1 = C[res] - L21^T x[sep]: lanes own columns k, rows a walked in order
-    // (x[sep[a]] is one broadcast load per row)
+    // C1 = C[res] - L21^T x[sep]: lanes own columns k and walk the rows a in
+    // order, 32 rows at a time: lane i gathers x[sep[a0 + i]] for the chunk
+    // (the next chunk's gather is issued before this chunk's products) and
+    // the rows' x values reach the other lanes by shuffles
     T acc[kSmallRows][NR];
 #pragma unroll
     for (int s = 0; s < kSmallRows; ++s)
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[s][r] = T(0);
-    for (int a = 0; a < na; ++a) {
-        const int64_t row = sep[a];
-        T xv[NR];
+    T xv[NR];
+    {
+        const bool v = lane < na;
+        const int64_t row = v ? sep[lane] : 0;
 #pragma unroll
-        for (int r = 0; r < NR; ++r) xv[r] = r < nrhs ? C[row + (int64_t)r * n] : T(0);
+        for (int r = 0; r < NR; ++r) xv[r] = (v && r < nrhs) ? C[row + (int64_t)r * n] : T(0);
+    }
+    for (int a0 = 0; a0 < na; a0 += 32) {
+        T xn[NR];
+        {
+            const int a = a0 + 32 + lane;
+            const bool v = a < na;
+            const int64_t row = v ? sep[a] : 0;
 #pragma unroll
-        for (int s = 0; s < kSmallRows; ++s) {
-            const int k = lane + 32 * s;
-            if (k < nn) {
-                const T l = Pj[(nn + a) + (int64_t)k * ld];
+            for (int r = 0; r < NR; ++r) xn[r] = (v && r < nrhs) ? C[row + (int64_t)r * n] : T(0);
+        }
+        const int m = min(32, na - a0);
+        const T* pa = Pj + nn + a0;
+#pragma unroll 4
+        for (int j = 0; j < m; ++j) {
+            T xb[NR];
 #pragma unroll
-                for (int r = 0; r < NR; ++r) acc[s][r] += l * xv[r];
+            for (int r = 0; r < NR; ++r) xb[r] = __shfl_sync(0xffffffffu, xv[r], j);
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) {
+                const int k = lane + 32 * s;
+                if (k < nn) {
+                    const T l = pa[j + (int64_t)k * ld];
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) acc[s][r] += l * xb[r];
+                }
             }
         }
+#pragma unroll
+        for (int r = 0; r < NR; ++r) xv[r] = xn[r];
     }
 #pragma unroll
     for (int s = 0; s < kSmallRows; ++s) {
@@ -229,24 +269,15 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
 // ---------------------------------------------------------------------------
 // blocked fronts
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int lb32(const int32_t* a, int n, int v) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
 // forward gather: W[res] = C[res] + child updates, R_j = child updates
 template <typename T>
 __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                  const int32_t* __restrict__ reltgt,
-                                                  const int32_t* __restrict__ chdtgt, const T* __restrict__ C,
+                                                  const Item* __restrict__ all_items,
+                                                  const int32_t* __restrict__ reltgt, const T* __restrict__ C,
                                                   T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const int nn = f.nn, na = f.na, nj = nn + na;
     const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
     const int tid = threadIdx.x, nt = blockDim.x;
     T* Rj = R + f.roff * nrhs;
@@ -257,17 +288,19 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
         else Rj[(q - nn) + r * na] = T(0);
     }
     __syncthreads();
-    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
-        const Front fc = fronts[chdtgt[p]];
+    // the plan's segments of this tile: (child, a0, a1), children in reverse
+    // order, at all_items[it.b ...] (indices into the whole item array)
+    for (int s = 0; s < it.pad; ++s) {
+        const Item sg = all_items[it.b + s];
+        const Front fc = fronts[sg.front];
         const int ma = fc.na;
         const int32_t* rel = reltgt + fc.sep0;
         const T* Mc = R + fc.roff * nrhs;
-        const int a0 = lb32(rel, ma, p0), a1 = lb32(rel, ma, p1);
-        const int cnt = a1 - a0;
+        const int cnt = sg.b - sg.a;
         for (int i = tid; i < cnt * nrhs; i += nt) {
-            int a = a0 + i % cnt, r = i / cnt;
-            int q = rel[a];
-            T v = Mc[a + r * ma];
+            const int a = sg.a + i % cnt, r = i / cnt;
+            const int q = rel[a];
+            const T v = Mc[a + r * ma];
             if (q < nn) W[f.col0 + q + (int64_t)r * n] += v;
             else Rj[(q - nn) + r * na] += v;
         }
@@ -279,17 +312,13 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
 // blocked diagonal solves in steps of a 256-column super-block K (columns
 // k0 .. k0 + wK of a front), with the super-block inverse X_K stored by the
 // factorization.  Per step and level:
-//   forward : k_s_fdiag  x_K = X_K W_K            (one CTA per front), then
+//   forward : k_s_sdiag<.., 0>  x_K = X_K W_K    (kDiagSplit CTAs per front), then
 //             k_s_ftile  rows below: W / R -= L[rows, K] x_K (64-row tiles);
-//   backward: k_s_bdiag  x_K = X_K^T W_K          (one CTA per front), then
-//             k_s_btile  columns left: W[c] -= sum_i L[k0 + i, c] x_K[i].
+//   backward: k_s_sdiag<.., 1>  x_K = X_K^T W_K  (kDiagSplit CTAs per front), then
+//             k_s_btile  columns left: W[c] -= sum_i L[k0 + i, c] x_K[i] (64-column tiles).
 // ---------------------------------------------------------------------------
 template <typename T, int NR>
 constexpr int sdiag_smem() { return (kSolveNB * NR + 16 * kSolveNB) * (int)sizeof(T); }
-template <typename T, int NR>
-constexpr int ftile_smem() { return (kSolveNB * NR + 4 * NR * kFwdRows + kSolveNB * kFwdRows) * (int)sizeof(T); }
-template <typename T>
-constexpr int btile_smem() { return (kSolveNB * kMaxRhs + kSolveNB * kNB) * (int)sizeof(T); }
 
 // element copy global -> shared that stays in flight (cp.async); a false
 // `valid` writes zero and reads nothing
@@ -369,108 +398,176 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
             if (r < nrhs) C[f.col0 + k0 + a + (int64_t)r * n] = acc[r];
 }
 
+// 16 bytes of consecutive panel entries in one load: 4 floats or 2 doubles
+template <typename T> struct Vec16;
+template <> struct Vec16<float> {
+    using type = float4;
+    static constexpr int W = 4;
+    __device__ static float at(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+};
+template <> struct Vec16<double> {
+    using type = double2;
+    static constexpr int W = 2;
+    __device__ static double at(const double2& v, int e) { return e == 0 ? v.x : v.y; }
+};
+
 // forward rows below super-block K: W (rows < nn) or R_j (rows >= nn) -= L[rows, K] x_K.
-// The 64-row x 256-column panel tile is staged in shared memory first.
+// Work item a covers the 64 rows from (k0 + wK rounded down to 4) + 64 a;
+// rows of the block itself that fall in the first tile are computed and
+// dropped.  Warp w streams columns 32 w .. 32 w + 31 of the block straight
+// from the panel: a lane loads 16 bytes (4 float or 2 double rows) of a
+// column, 64 / VW lanes cover the tile's rows and the warp takes VW / 2
+// columns per load (coalesced runs of 256 / 512 bytes); x_K comes from
+// shared memory as a broadcast.  Partial sums are added lane half by lane
+// half, then warp by warp, in a fixed order.
+template <typename T, int NR>
+constexpr int ftile_smem() { return (kSolveNB * NR + 8 * NR * kFwdRows) * (int)sizeof(T); }
+
 template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
+    using VT = Vec16<T>;
+    using V = typename VT::type;
+    constexpr int VW = VT::W;             // rows per load
+    constexpr int LPC = kFwdRows / VW;    // lanes per column (16 float, 32 double)
+    constexpr int CPL = 32 / LPC;         // columns per warp load (2 float, 1 double)
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * NR
-    T* red = xs + kSolveNB * NR;           // 4 * NR * kFwdRows
-    T* tile = red + 4 * NR * kFwdRows;     // tile[c * 64 + r]
+    T* xs = reinterpret_cast<T*>(sm_raw);  // xs[c * NR + r]
+    T* red = xs + kSolveNB * NR;           // red[(w * NR + r) * kFwdRows + row]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
-    const int r0 = k0 + wK + it.a * kFwdRows;
-    const int nr = min(kFwdRows, nj - r0);
-    const int tid = threadIdx.x;
-    const T* Pt = P + f.poff + r0 + (int64_t)k0 * ld;
-    for (int e = tid; e < kSolveNB * kFwdRows; e += 256) {
-        const int c = e >> 6, r = e & (kFwdRows - 1);
-        const bool v = c < wK && r < nr;
-        cpa(tile + e, v ? Pt + r + (int64_t)c * ld : Pt, v);
-    }
+    const int rlo = k0 + wK;
+    const int ra = (rlo & ~3) + it.a * kFwdRows;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < kSolveNB * NR; i += 256) {
-        const int a = i % kSolveNB, r = i / kSolveNB;
-        xs[i] = (a < wK && r < nrhs) ? C[f.col0 + k0 + a + (int64_t)r * n] : T(0);
+        const int c = i & (kSolveNB - 1), r = i / kSolveNB;
+        xs[c * NR + r] = (c < wK && r < nrhs) ? C[f.col0 + k0 + c + (int64_t)r * n] : T(0);
     }
-    cpa_wait_all();
     __syncthreads();
-    const int rl = tid & (kFwdRows - 1), g = tid / kFwdRows;  // row, 64-column group
-    T acc[NR];
+    const int rr = (lane % LPC) * VW, ch = lane / LPC;
+    // row is a multiple of 4 below nj, so the 16-byte load ends inside the
+    // column's ldp (a multiple of 4) rows
+    const int row = ra + rr;
+    const int cb = warp * 32;
+    const int cn = min(32, wK - cb);
+    T acc[VW][NR];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    for (int e = 0; e < VW; ++e)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
+    if (row < nj && cn > 0) {
+        const T* pc = P + f.poff + (int64_t)(k0 + cb) * ld + row;
 #pragma unroll 8
-    for (int c = g * kNB; c < g * kNB + kNB; ++c) {
-        const T l = tile[c * kFwdRows + rl];
+        for (int c = ch; c < cn; c += CPL) {
+            const V l = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+            const T* xc = xs + (cb + c) * NR;
 #pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] += l * xs[c + r * kSolveNB];
-    }
+            for (int r = 0; r < NR; ++r) {
+                const T x = xc[r];
 #pragma unroll
-    for (int r = 0; r < NR; ++r) red[(g * NR + r) * kFwdRows + rl] = acc[r];
-    __syncthreads();
-    if (g == 0 && rl < nr) {
-        T* Rj = R + f.roff * nrhs;
-        const int qr = r0 + rl;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            if (r < nrhs) {
-                const T v = red[(0 * NR + r) * kFwdRows + rl] + red[(1 * NR + r) * kFwdRows + rl] +
-                            red[(2 * NR + r) * kFwdRows + rl] + red[(3 * NR + r) * kFwdRows + rl];
-                if (qr < nn) W[f.col0 + qr + (int64_t)r * n] -= v;
-                else Rj[(qr - nn) + r * na] -= v;
+                for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(l, e) * x;
             }
+        }
+    }
+    if (CPL == 2) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[e][r] += __shfl_xor_sync(0xffffffffu, acc[e][r], 16);
+    }
+    if (ch == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int e = 0; e < VW; ++e) red[(warp * NR + r) * kFwdRows + rr + e] = acc[e][r];
+    }
+    __syncthreads();
+    T* Rj = R + f.roff * nrhs;
+    for (int o = tid; o < kFwdRows * NR; o += 256) {
+        const int rl = o & (kFwdRows - 1), r = o / kFwdRows;
+        const int q = ra + rl;
+        if (r < nrhs && q >= rlo && q < nj) {
+            T v = T(0);
+#pragma unroll
+            for (int w = 0; w < 8; ++w) v += red[(w * NR + r) * kFwdRows + rl];
+            if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
+            else Rj[(q - nn) + r * na] -= v;
         }
     }
 }
 
 // backward columns left of super-block K (64-column tile it.a):
-// W[c] -= sum_i L[k0 + i, c] x_K[i].  The 256-row x 64-column panel tile is
-// staged in shared memory; one warp per column, then a shuffle reduction.
-template <typename T>
+// W[c] -= sum_i L[k0 + i, c] x_K[i].  Thread (q, c) owns column c over the
+// block rows 64 q .. 64 q + 63, loading 16 bytes (4 float or 2 double rows)
+// at a time, eight loads in flight; the lanes of a warp sit on the same
+// rows, so x_K is a shared-memory broadcast.  The four row quarters are
+// added in order.
+template <typename T, int NR>
+constexpr int btile_smem() { return (kSolveNB * NR + 4 * NR * kNB) * (int)sizeof(T); }
+
+template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
+    using VT = Vec16<T>;
+    using V = typename VT::type;
+    constexpr int VW = VT::W;
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* xs = reinterpret_cast<T*>(sm_raw);  // kSolveNB * kMaxRhs
-    T* tile = xs + kSolveNB * kMaxRhs;     // tile[c * 256 + i]
+    T* xs = reinterpret_cast<T*>(sm_raw);  // xs[i * NR + r]
+    T* red = xs + kSolveNB * NR;           // red[(q * NR + r) * kNB + c]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
     const int c0 = it.a * kNB, wc = min(kNB, k0 - c0);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const T* Pt = P + f.poff + (int64_t)c0 * ld + k0;
-    for (int e = tid; e < kNB * kSolveNB; e += 256) {
-        const int c = e >> 8, i = e & (kSolveNB - 1);
-        const bool v = c < wc && i < wK;
-        cpa(tile + e, v ? Pt + (int64_t)c * ld + i : Pt, v);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < kSolveNB * NR; i += 256) {
+        const int a = i & (kSolveNB - 1), r = i / kSolveNB;
+        xs[a * NR + r] = (a < wK && r < nrhs) ? C[f.col0 + k0 + a + (int64_t)r * n] : T(0);
     }
-    for (int i = tid; i < wK * nrhs; i += 256) {
-        const int a = i % wK, r = i / wK;
-        xs[a + r * kSolveNB] = C[f.col0 + k0 + a + (int64_t)r * n];
-    }
-    cpa_wait_all();
     __syncthreads();
-    for (int cc = warp; cc < wc; cc += 8) {
-        const T* pc = tile + cc * kSolveNB;
-        T acc[kMaxRhs];
+    const int c = tid & (kNB - 1), q = tid >> 6;
+    const int i0 = q * 64, ni = min(64, wK - i0);  // rows of this quarter inside the block
+    T acc[NR];
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) acc[r] = T(0);
-        for (int i = lane; i < wK; i += 32) {
-            const T l = pc[i];
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    if (c < wc && ni > 0) {
+        // k0 + i0 + i is a multiple of 4 below nn <= nj, so each 16-byte
+        // load ends inside the column's ldp rows; rows past the block are
+        // dropped by the select below
+        const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + k0 + i0;
+        for (int i = 0; i < 64; i += 8 * VW) {
+            V l[8];
 #pragma unroll
-            for (int r = 0; r < kMaxRhs; ++r)
-                if (r < nrhs) acc[r] += l * xs[i + r * kSolveNB];
+            for (int u = 0; u < 8; ++u)
+                if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int ib = i + u * VW;
+                if (ib < ni) {
+                    const T* xr = xs + (i0 + ib) * NR;
+#pragma unroll
+                    for (int e = 0; e < VW; ++e) {
+                        const T lv = ib + e < ni ? VT::at(l[u], e) : T(0);
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) acc[r] += lv * xr[e * NR + r];
+                    }
+                }
+            }
         }
+    }
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; ++r) {
-            if (r >= nrhs) break;
-            T v = acc[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) W[f.col0 + c0 + cc + (int64_t)r * n] -= v;
+    for (int r = 0; r < NR; ++r) red[(q * NR + r) * kNB + c] = acc[r];
+    __syncthreads();
+    for (int o = tid; o < kNB * NR; o += 256) {
+        const int cc = o & (kNB - 1), r = o / kNB;
+        if (cc < wc && r < nrhs) {
+            const T v = red[(0 * NR + r) * kNB + cc] + red[(1 * NR + r) * kNB + cc] +
+                        red[(2 * NR + r) * kNB + cc] + red[(3 * NR + r) * kNB + cc];
+            W[f.col0 + c0 + cc + (int64_t)r * n] -= v;
         }
     }
 }
@@ -596,7 +693,8 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 2>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 1>()));
-    MF_CUDA(cudaFuncSetAttribute(k_s_btile<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, btile_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_btile<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, btile_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_btile<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, btile_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 16, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
@@ -633,7 +731,7 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         if (lv.s_gather.cnt) {
             Timer t(h, K_S_GATHER);
             k_s_gather<T><<<(unsigned)lv.s_gather.cnt, 256, 0, h->stream>>>(
-                h->d_fronts, items + lv.s_gather.off, h->d_reltgt, h->d_chdtgt, sb.C, sb.W, sb.R, n, nrhs);
+                h->d_fronts, items + lv.s_gather.off, items, h->d_reltgt, sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         for (size_t k = 0; k < lv.s_steps.size(); ++k) {
@@ -696,8 +794,15 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             }
             MF_CUDA(cudaGetLastError());
             if (st.bwd.cnt) {
-                k_s_btile<T><<<(unsigned)st.bwd.cnt, 256, btile_smem<T>(), h->stream>>>(
-                    h->d_fronts, items + st.bwd.off, (int)k, sb.P, sb.C, sb.W, n, nrhs);
+                const unsigned gb = (unsigned)st.bwd.cnt;
+                const Item* itb = items + st.bwd.off;
+                switch (nrb) {
+                    case 1: k_s_btile<T, 1><<<gb, 256, btile_smem<T, 1>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: k_s_btile<T, 2><<<gb, 256, btile_smem<T, 2>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: k_s_btile<T, 4><<<gb, 256, btile_smem<T, 4>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: k_s_btile<T, 8><<<gb, 256, btile_smem<T, 8>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: k_s_btile<T, 16><<<gb, 256, btile_smem<T, 16>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                }
                 MF_CUDA(cudaGetLastError());
             }
         }

@@ -241,7 +241,7 @@ enum TcRole { TC_LEFT = 0, TC_TRAIL = 1, TC_SYRK = 2, TC_TRSM = 3 };
 
 template <int ROLE>
 struct TcTileN {
-    static constexpr int value = ROLE == TC_SYRK ? kTcSyrkN : kTile;
+    static constexpr int value = ROLE == TC_SYRK ? kTcSyrkN : ROLE == TC_TRAIL ? kTcTrailN : kTile;
 };
 
 // Geometry of one tile: TMA rows xa (A) and xb (B); K range [kbeg, kend)
@@ -528,8 +528,9 @@ static int launch_one(mf_handle* h, const ItemList& l, int ob, int c0, const Fac
 template <int LDLT>
 static int set_attrs() {
     constexpr int s64 = tc::Cfg<kTile>::SMEM_BYTES, ss = tc::Cfg<kTcSyrkN>::SMEM_BYTES;
+    constexpr int st = tc::Cfg<kTcTrailN>::SMEM_BYTES;
     MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, st));
     MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
     MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
     return 0;

@@ -116,6 +116,13 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_set_segments.restype = ctypes.c_int
         lib.mf_segment_errors.argtypes = [_vp, _pd]
         lib.mf_segment_errors.restype = ctypes.c_int
+        lib.mf_autotune.argtypes = [_vp, ctypes.c_int, _pd]
+        lib.mf_autotune.restype = ctypes.c_int
+        p32 = ctypes.POINTER(ctypes.c_int32)
+        lib.mf_kernel_choice.argtypes = [_vp, p32, p32]
+        lib.mf_kernel_choice.restype = ctypes.c_int
+        lib.mf_set_kernel_choice.argtypes = [_vp, p32, p32]
+        lib.mf_set_kernel_choice.restype = ctypes.c_int
         lib.mf_last_error.argtypes = []
         lib.mf_last_error.restype = ctypes.c_char_p
         _gpu = lib

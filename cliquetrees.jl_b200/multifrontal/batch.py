@@ -117,6 +117,11 @@ class BatchedFactorization:
             cholesky_(self.F, check=check)
         return self
 
+    def autotune(self, reps=3):
+        """Mixed form: per-level tcgen05/FFMA choice timed on the current values
+        (``ChordalFactorization.autotune``); factorize again afterwards."""
+        return self.F.autotune(reps)
+
     @property
     def info(self):
         return self.F.info

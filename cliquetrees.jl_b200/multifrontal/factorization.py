@@ -197,6 +197,42 @@ class ChordalFactorization:
     def issuccess(self) -> bool:
         return self._factored and self.info == 0
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Mixed form only: time every tree level's single-precision GEMM roles
+        with the tcgen05 tiles and with the FFMA tiles on the current values
+        and keep the faster per level (the factor is then refactored).
+        Returns the GEMM-role milliseconds of each choice and the per-level
+        picks."""
+        if not self.mixed:
+            raise ValueError("autotune applies to the mixed form")
+        lib, h = self._handle.lib, self._handle.h
+        ms = np.zeros(6, np.float64)
+        check(lib.mf_autotune(h, int(reps), ptrd(ms)), "mf_autotune")
+        nl = int(ms[5])
+        tc_steps = np.zeros(nl, np.int32)
+        tc_syrk = np.zeros(nl, np.int32)
+        p32 = ctypes.POINTER(ctypes.c_int32)
+        check(lib.mf_kernel_choice(h, tc_steps.ctypes.data_as(p32), tc_syrk.ctypes.data_as(p32)),
+              "mf_kernel_choice")
+        self._factored = False
+        return {"tc_ms": float(ms[0]), "ffma_ms": float(ms[1]), "tuned_ms": float(ms[2]),
+                "tc_steps": tc_steps, "tc_syrk": tc_syrk}
+
+    def set_kernel_choice(self, tc_steps=None, tc_syrk=None):
+        """Set the per-level choice (1 = tcgen05, 0 = FFMA) directly, e.g. one
+        saved from ``autotune`` on another handle of the same pattern."""
+        p32 = ctypes.POINTER(ctypes.c_int32)
+        info = np.zeros(9, np.int64)
+        check(self._handle.lib.mf_info(self._handle.h, ptr64(info)), "mf_info")
+        a = None if tc_steps is None else np.ascontiguousarray(tc_steps, dtype=np.int32)
+        b = None if tc_syrk is None else np.ascontiguousarray(tc_syrk, dtype=np.int32)
+        for v in (a, b):
+            if v is not None and v.size != info[7]:
+                raise ValueError(f"kernel choice needs one entry per tree level ({info[7]}), got {v.size}")
+        check(self._handle.lib.mf_set_kernel_choice(self._handle.h, None if a is None else a.ctypes.data_as(p32),
+                                                    None if b is None else b.ctypes.data_as(p32)),
+              "mf_set_kernel_choice")
+
     def solve(self, B):
         return ldiv(self, B)
 

@@ -56,6 +56,7 @@ class Pattern:
     lo_src: np.ndarray = None  # one entry per stored lower-triangle value
     handles: list = field(default_factory=list)
     est_bytes: int = 0         # device bytes of one handle, once known
+    choice: tuple = None       # mixed form: per-level tcgen05/FFMA choice found by autotuning
 
 
 @dataclass
@@ -95,6 +96,8 @@ class _DeviceBatch:
         self.mixed = mixed
         self.tol, self.maxit = tol, maxit
         self.perm = np.ascontiguousarray(Pb.perm, dtype=np.int64)
+        if mixed and pat.choice is not None:
+            self.F.set_kernel_choice(*pat.choice)
         self.busy = False
         self.last_used = 0.0
         self.nz = np.empty(pat.lo_src.size * B, np.float64)
@@ -140,8 +143,9 @@ class _DeviceBatch:
 
 
 class Server:
-    def __init__(self, *, mixed=True, device=0, mem_cap=120e9, workers=4, tol=1e-12, maxit=100):
+    def __init__(self, *, mixed=True, device=0, mem_cap=120e9, workers=4, tol=1e-12, maxit=100, autotune=True):
         self.mixed = mixed
+        self.autotune = autotune
         self.device = device
         self.mem_cap = mem_cap
         self.workers = workers
@@ -202,7 +206,9 @@ class Server:
 
     def warm(self, keys=None):
         """Create one handle per pattern and run a throw-away batch through it,
-        so graphs and tensor maps exist before timing."""
+        so graphs and tensor maps exist before timing; in the mixed form the
+        pattern's per-level kernel choice is autotuned on that handle and
+        every later handle of the pattern starts with it."""
         for key in keys or list(self.patterns):
             pat = self.patterns[key]
             hd = self._acquire(pat)
@@ -211,6 +217,10 @@ class Server:
             A = pat.A0
             r = Request(-1, key, self.lower_values(key, A), np.ones((pat.S.n, 1)))
             hd.run([r])
+            if self.mixed and self.autotune and pat.choice is None:
+                t = hd.F.autotune(2)
+                pat.choice = (t["tc_steps"], t["tc_syrk"])
+                hd.run([r])
             hd.busy = False
 
     # -- the loop ----------------------------------------------------------

@@ -113,10 +113,27 @@ int mf_enable_mixed(mf_handle* h);
  * the FP64 factorization (the reference's convention). */
 int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* used_fp64);
 
-/* x = A^-1 b to normwise backward error <= tol: preconditioned conjugate
- * gradients (Cholesky) or iterative refinement (LDLt) in FP64 with the FP32
- * factor as preconditioner; B (n x nrhs, ORIGINAL order) is overwritten
- * with x.  *iters and *eta report the worst right-hand side. */
+/* Autotuning of the single-precision factorization (no reference
+ * counterpart: the reference has one dense kernel per role).  For every tree
+ * level, times the level's GEMM roles (left-looking, TRSM, trailing update;
+ * and the SYRK of the update matrix) with the tcgen05 tensor-core tiles and
+ * with the FFMA tiles on the handle's current values, `reps` timed runs
+ * after one warm-up each, and keeps the faster variant per level and role.
+ * The handle's factor is overwritten: call mf_factorize_mixed afterwards.
+ * ms (may be NULL) receives 6 values: GEMM-role milliseconds with tcgen05
+ * everywhere, with FFMA everywhere, with the tuned choice; levels that kept
+ * tcgen05 for the panel steps, for the SYRK; number of levels. */
+int mf_autotune(mf_handle* h, int reps, double* ms);
+/* The per-level choice (1 = tcgen05, 0 = FFMA), one entry per tree level
+ * (mf_info out[7] levels); either array may be NULL. */
+int mf_kernel_choice(const mf_handle* h, int32_t* tc_steps, int32_t* tc_syrk);
+int mf_set_kernel_choice(mf_handle* h, const int32_t* tc_steps, const int32_t* tc_syrk);
+
+/* x = A^-1 b to normwise backward error <= tol in FP64 with the FP32 factor
+ * as preconditioner: conjugate gradients (Cholesky), GMRES (LDLt), or
+ * classical iterative refinement when segments are set (every segment is
+ * refined to its own backward error); B (n x nrhs, ORIGINAL order) is
+ * overwritten with x.  *iters and *eta report the worst right-hand side. */
 int mf_solve_refined(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm, double tol, int maxit,
                      int* iters, double* eta);
 int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev,

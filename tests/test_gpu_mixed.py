@@ -108,3 +108,32 @@ def oracle_factor_scaled(As, P, S):
     info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0)
     assert info == 0
     return info, (Dval, Lval, d)
+
+
+def test_autotune_keeps_refined_accuracy():
+    """The per-level tcgen05/FFMA choice changes only which single-precision
+    kernel runs; every choice must refine to the same 1e-12 bar."""
+    A = tm.grid_laplacian(24, 24, 24, seed=3)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(24, 24, 24))
+    F = mf.ChordalCholesky(A, P, S, mixed=True)
+    mf.cholesky_(F)
+    B = tm.rhs(A.shape[0], 3, seed=1)
+    X0 = mf.ldiv(F, B)
+    t = F.autotune(2)
+    nl = t["tc_steps"].size
+    assert nl > 0 and t["tc_syrk"].size == nl
+    assert set(np.unique(t["tc_steps"])) <= {0, 1}
+    assert t["tuned_ms"] <= min(t["tc_ms"], t["ffma_ms"]) * 1.0001
+    mf.cholesky_(F)
+    X1 = mf.ldiv(F, B)
+    assert tm.backward_error(A, X1, B).max() <= 1e-12
+    assert np.abs(X1 - X0).max() <= 1e-9 * np.abs(X0).max()
+    # FFMA tiles on every level
+    F.set_kernel_choice(np.zeros(nl, np.int32), np.zeros(nl, np.int32))
+    mf.cholesky_(F)
+    X2 = mf.ldiv(F, B)
+    assert tm.backward_error(A, X2, B).max() <= 1e-12
+    assert np.abs(X2 - X0).max() <= 1e-9 * np.abs(X0).max()
+    with pytest.raises(ValueError):
+        F.set_kernel_choice(np.zeros(nl + 1, np.int32))
+    F.close()
