@@ -74,6 +74,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="mixed form: tcgen05 tiles on every level")
+    ap.add_argument("--no-served", action="store_true", help="configs 1, 2, 4: skip the served batched form")
     ap.add_argument("--mixed-profile", action="store_true", help="with --profile-only: the mixed form")
     return ap.parse_args()
 
@@ -371,6 +372,7 @@ def main():
     mixed = run_form(args, work, mixed=True, local=local, world=world)
     plain = run_form(args, work, mixed=False, local=local, world=world)
     unbatched = time_unbatched(work, local) if work.members is not None else None
+    served = run_served(args, work, local) if args.config in SERVED and not args.no_served else None
 
     # roofline: the dominant kernel class of each form against cuBLAS peaks
     # of the same arithmetic measured in this run
@@ -420,6 +422,11 @@ def main():
         if unbatched is not None:
             line["plain_fp64_one_matrix_at_a_time"] = unbatched
             line["mixed_batched_over_unbatched_plain"] = mixed["value"] / unbatched["value"]
+        if served is not None:
+            # the served mixed-precision batched form against the plain FP64
+            # form, both through host buffers (the plain form's e2e figure)
+            line["served_mixed_batched"] = served
+            line["served_over_plain_fp64"] = served["solves_per_s"] / plain["e2e"]["value"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -555,6 +562,62 @@ def run_serving(args, local, world):
         "e2e": {"value": sat["requests_per_s"], "unit": "requests/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None, "note": "every request moves its values and RHS from host buffers"},
     }
+
+
+# served batched form per config: (matrices per device handle, workers, requests)
+SERVED = {1: (32, 4, 1024), 2: (4, 2, 16), 4: (1, 2, 6)}
+
+
+def run_served(args, work, local):
+    """The served mixed-precision batched form on this config's pattern:
+    factor+solve requests carrying the config's right-hand sides and one of
+    four coefficient sets of the same pattern (the matrix and three seeded
+    congruences D A D, D = diag(exp(0.1 z)), which keep its pattern,
+    symmetry and inertia), batched B per device handle as one forest and
+    run by W workers on their own streams.  Saturation throughput comes from
+    all requests queued at once; latency from Poisson arrivals at 70% of it."""
+    import scipy.sparse as sp
+    from multifrontal import serve
+    from multifrontal import testmatrices as tm
+
+    B, W, R = SERVED[args.config]
+    srv = serve.Server(mixed=True, device=local, workers=W)
+    srv.add_pattern("cfg", work.A, batch=B, ldlt=bool(work.diag), symbolic_result=(work.P, work.S))
+    mats = [work.A]
+    n = work.A.shape[0]
+    for s in (11, 12, 13):
+        dv = np.exp(0.1 * np.random.default_rng(s).standard_normal(n))
+        D = sp.diags(dv)
+        mats.append(sp.csc_matrix(D @ work.A @ D))
+    pool = [srv.lower_values("cfg", M) for M in mats]
+    srv.warm(per_pattern=min(2, W))
+
+    def stream(count, rate, seed):
+        rng = np.random.default_rng(seed)
+        t, reqs = 0.0, []
+        for i in range(count):
+            t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
+            reqs.append(serve.Request(i, "cfg", pool[i % 4], work.B, arrival=t))
+        return reqs
+
+    def worst(done):
+        eta = max(r.eta for r in done)
+        for r in done[:: max(1, len(done) // 8)]:
+            eta = max(eta, float(tm.backward_error(mats[r.rid % 4], r.X, r.B).max()))
+        return eta
+
+    done = srv.serve(stream(R, 0.0, 1), realtime=False)
+    sat = len(done) / srv.wall
+    sat_eta = worst(done)
+    done2 = srv.serve(stream(R, 0.7 * sat, 2), realtime=True)
+    st = serve.latency_stats(done2)
+    out = {"solves_per_s": sat, "unit": "solves/s", "batch_per_handle": B, "workers": W, "requests": R,
+           "backward_error": max(sat_eta, worst(done2)), "latency_at_70pct_load": {**st, "rate": 0.7 * sat},
+           "mean_batch": float(np.mean([r.batch_size for r in done])),
+           "device_bytes": int(srv.bytes),
+           "note": "host buffers in and out for every request (values, RHS, solution)"}
+    srv.close()
+    return out
 
 
 def time_unbatched(work, local, count=64):

@@ -276,6 +276,7 @@ int mf_chol_impl(mf_handle* h, double* Dval, double* Lval, double* d, const doub
     }
     DeviceGuard g(h->device);
     int rc;
+    if ((rc = ensure_fp64(h))) return rc;
     if (!h->d_DL) {
         int64_t tot = 0;
         if ((rc = dalloc(h, &h->d_DL, std::max<int64_t>(h->ndz + h->nlz, 1), &tot))) return rc;
@@ -488,6 +489,7 @@ int mf_factorize(mf_handle* h, const double* signs, int64_t* info) {
     DeviceGuard g(h->device);
     const double* ds = nullptr;
     int rc;
+    if ((rc = ensure_fp64(h))) return rc;
     if ((rc = upload_signs(h, signs, &ds))) return rc;
     double* keep = h->d_signs;
     h->d_signs = const_cast<double*>(ds);
@@ -522,11 +524,54 @@ int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, cons
     return solve_chunks(h, perm_dev ? perm_dev : h->d_perm, nullptr, B_dev, nrhs, ldb);
 }
 
+}  // extern "C"
+
+static int64_t fp64_bytes(const mf_handle* h) {
+    return (int64_t)sizeof(double) * (std::max<int64_t>(h->npanel, 0) + std::max<int64_t>(h->ninv, 1) +
+                                      std::max<int64_t>(h->ninv2, 1) + std::max<int64_t>(h->nmval, 0));
+}
+
+int mf::have_fp64(const mf_handle* h) { return h->d_P != nullptr || h->npanel == 0; }
+
+int mf::ensure_fp64(mf_handle* h) {
+    if (have_fp64(h) && (h->d_M || h->nmval <= 0)) return 0;
+    int64_t tot = 0;
+    int rc = 0;
+    rc = rc ? rc : dalloc(h, &h->d_P, h->npanel, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_inv, std::max<int64_t>(h->ninv, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_inv2, std::max<int64_t>(h->ninv2, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_M, h->nmval, &tot);
+    if (rc) {
+        for (double** p : {&h->d_P, &h->d_inv, &h->d_inv2, &h->d_M}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        return rc;
+    }
+    if (h->npanel) MF_CUDA(cudaMemset(h->d_P, 0, sizeof(double) * h->npanel));
+    h->bytes += tot;
+    release_graphs(h);  // captured launches hold the buffers' addresses
+    return 0;
+}
+
+extern "C" {
+
 int mf_enable_mixed(mf_handle* h) {
     if (!h) { set_error("null handle"); return -1; }
     if (!h->d_csrptr) { set_error("mf_enable_mixed: call mf_set_assembly first"); return -1; }
     if (h->mixed) return 0;
     DeviceGuard g(h->device);
+    // the FP64 factor storage is only needed if a factorization falls back
+    // to FP64: release it first (ensure_fp64 brings it back on demand)
+    MF_CUDA(cudaDeviceSynchronize());
+    release_graphs(h);
+    if (h->d_P) {
+        for (double** p : {&h->d_P, &h->d_inv, &h->d_inv2, &h->d_M}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+        h->bytes -= fp64_bytes(h);
+    }
     int64_t tot = 0;
     int rc = 0;
     const int64_t n = h->n, cap = h->nrhs_cap;
@@ -567,7 +612,8 @@ int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* us
     if (!rc && inf != 0) {
         // FP32 rejected a pivot: factor in FP64 (the refinement then takes one
         // FP64 solve), so an FP32 breakdown is never reported as a failure
-        rc = launch_assemble(h, h->cur_nz);
+        rc = ensure_fp64(h);
+        if (!rc) rc = launch_assemble(h, h->cur_nz);
         if (!rc) rc = init_info(h);
         if (!rc) rc = launch_factor(h);
         if (!rc) rc = read_info(h, &inf);

@@ -851,7 +851,13 @@ static int assemble_impl(mf_handle* h, const double* dnz, T* P, const double* sc
     return 0;
 }
 
-int launch_assemble(mf_handle* h, const double* dnz) { return assemble_impl<double>(h, dnz, h->d_P, nullptr); }
+int launch_assemble(mf_handle* h, const double* dnz) {
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
+    return assemble_impl<double>(h, dnz, h->d_P, nullptr);
+}
 
 int launch_assemble_mixed(mf_handle* h, const double* dnz) {
     if (h->n > 0) {
@@ -862,6 +868,10 @@ int launch_assemble_mixed(mf_handle* h, const double* dnz) {
 }
 
 int launch_dl_to_panel(mf_handle* h, const double* dD, const double* dL) {
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
     Timer t(h, K_OTHER);
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
@@ -874,6 +884,10 @@ int launch_dl_to_panel(mf_handle* h, const double* dD, const double* dL) {
 }
 
 int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
     Timer t(h, K_OTHER);
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
@@ -1052,6 +1066,10 @@ void release_graphs(mf_handle* h) {
 // graph keys: kind (1 FP64 factor, 2 FP32 factor), then what the launch
 // sequence reads through pointers that can change between calls
 int launch_factor(mf_handle* h) {
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
     FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d, h->d_inv2};
     return run_captured(h, 1, (int64_t)(uintptr_t)h->d_signs, 0, 0, [&]() {
         return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);

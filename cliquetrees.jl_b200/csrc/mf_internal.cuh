@@ -67,7 +67,10 @@ struct ItemList {
 
 constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
 constexpr int kNB = 64;         // sub-panel width of the blocked path
-constexpr int kOB = 256;        // outer block: trailing updates run with K = kOB
+#ifndef MF_KOB
+#define MF_KOB 256
+#endif
+constexpr int kOB = MF_KOB;     // outer block: trailing updates run with K = kOB
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns stay kTile
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
@@ -298,6 +301,11 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
 
 // kernel launchers (mf_factor.cu / mf_solve.cu); all stream ordered
 int launch_factor(mf_handle* h);
+// FP64 factor storage (panels, update matrices, block inverses): a mixed
+// handle releases it in mf_enable_mixed and allocates it again only when a
+// factorization falls back to FP64; a non-zero return means it is absent.
+int ensure_fp64(mf_handle* h);
+int have_fp64(const mf_handle* h);
 int launch_factor_mixed(mf_handle* h);
 int tc_prepare(mf_handle* h);
 int tc_launch(mf_handle* h, int role, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb);

@@ -832,12 +832,20 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
 // Solve in place on d_C (n x nrhs, ld n, elimination order); nrhs <= nrhs_cap.
 int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* C, double* part) {
     if (nrhs <= 0) return 0;
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
     if (nrhs > kMaxRhs) { set_error("launch_solve_with: nrhs chunk above 16"); return -1; }
     SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, R, W, C, part, h->d_inv2};
     return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
 }
 int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
+    if (!have_fp64(h)) {
+        set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }
     SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, h->d_R, h->d_W, h->d_C, h->d_part, h->d_inv2};
     return run_captured(h, 3, nrhs, 0, 0, [&]() {

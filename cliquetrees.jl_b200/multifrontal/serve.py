@@ -156,12 +156,13 @@ class Server:
         self.bytes = 0
 
     # -- patterns ----------------------------------------------------------
-    def add_pattern(self, key, A0, order="mindeg", batch=1, ldlt=False):
-        """Symbolic analysis of a pattern, once (cached by key)."""
+    def add_pattern(self, key, A0, order="mindeg", batch=1, ldlt=False, symbolic_result=None):
+        """Symbolic analysis of a pattern, once (cached by key); an analysis
+        already at hand is passed as ``symbolic_result=(P, S)``."""
         if key in self.patterns:
             return self.patterns[key]
         A0 = sp.csc_matrix(A0)
-        P, S = symbolic(A0, alg=order)
+        P, S = symbolic_result if symbolic_result is not None else symbolic(A0, alg=order)
         Lo, _ = assembly_map(S, P.invp, A0)
         pat = Pattern(key, A0, P, S, batch, ldlt, np.arange(Lo.nnz))
         self.patterns[key] = pat
@@ -204,24 +205,32 @@ class Server:
         self.bytes += hd.bytes
         return hd
 
-    def warm(self, keys=None):
-        """Create one handle per pattern and run a throw-away batch through it,
-        so graphs and tensor maps exist before timing; in the mixed form the
-        pattern's per-level kernel choice is autotuned on that handle and
-        every later handle of the pattern starts with it."""
+    def warm(self, keys=None, per_pattern=1):
+        """Create up to ``per_pattern`` handles per pattern (at most 2) and run
+        a throw-away batch through each, so graphs and tensor maps exist
+        before timing; in the mixed form the pattern's per-level kernel
+        choice is autotuned on its first handle and every later handle of
+        the pattern starts with it."""
         for key in keys or list(self.patterns):
             pat = self.patterns[key]
-            hd = self._acquire(pat)
-            if hd is None:
-                continue
-            A = pat.A0
-            r = Request(-1, key, self.lower_values(key, A), np.ones((pat.S.n, 1)))
-            hd.run([r])
-            if self.mixed and self.autotune and pat.choice is None:
-                t = hd.F.autotune(2)
-                pat.choice = (t["tc_steps"], t["tc_syrk"])
+            got = []
+            for _ in range(max(1, min(2, per_pattern))):
+                hd = self._acquire(pat)
+                if hd is None:
+                    break
+                got.append(hd)
+                A = pat.A0
+                r = Request(-1, key, self.lower_values(key, A), np.ones((pat.S.n, 1)))
                 hd.run([r])
-            hd.busy = False
+                if self.mixed and self.autotune and pat.choice is None:
+                    t = hd.F.autotune(2)
+                    pat.choice = (t["tc_steps"], t["tc_syrk"])
+                    for other in pat.handles:
+                        if other is not hd:
+                            other.F.set_kernel_choice(*pat.choice)
+                    hd.run([r])
+            for hd in got:
+                hd.busy = False
 
     # -- the loop ----------------------------------------------------------
     def serve(self, requests, realtime=True, timeout=600.0):

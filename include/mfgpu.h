@@ -104,7 +104,11 @@ int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, cons
 /* ---- mixed precision (FP32 fronts, FP64 refinement) -------------------- */
 
 /* Allocate the single-precision factor and the refinement workspace (after
- * mf_set_assembly).  From then on mf_assemble only stages the values. */
+ * mf_set_assembly).  From then on mf_assemble only stages the values.  The
+ * FP64 factor storage (panels, update matrices, block inverses) is released
+ * and allocated again only when a factorization needs it (mf_factorize, or a
+ * mixed factorization that falls back to FP64); the FP64 solves and
+ * mf_get_factor fail until then. */
 int mf_enable_mixed(mf_handle* h);
 
 /* Scale A symmetrically by diag(|a_ii|)^-1/2, factor it in FP32 (same plan,
