@@ -50,7 +50,8 @@ void free_all(mf_handle* h) {
                     h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->d_iv,     h->d_red,      h->f32.P,  h->f32.M,
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
-                    h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2};
+                    h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc};
     release_graphs(h);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -790,20 +791,50 @@ int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
             if (segptr[s + 1] < segptr[s]) { set_error("mf_set_segments: boundaries must not decrease"); return -1; }
     }
     DeviceGuard g(h->device);
-    for (void* p : {(void*)h->d_segptr, (void*)h->d_segred, (void*)h->d_segeta})
+    MF_CUDA(cudaDeviceSynchronize());
+    release_graphs(h);
+    for (void* p : {(void*)h->d_segptr, (void*)h->d_segred, (void*)h->d_segeta, (void*)h->d_chunkrow,
+                    (void*)h->d_chunkseg, (void*)h->d_segchunk, (void*)h->d_rowseg, (void*)h->d_chunkred,
+                    (void*)h->d_segsc})
         if (p) cudaFree(p);
     h->d_segptr = nullptr; h->d_segred = nullptr; h->d_segeta = nullptr;
+    h->d_chunkrow = nullptr; h->d_chunkseg = nullptr; h->d_segchunk = nullptr; h->d_rowseg = nullptr;
+    h->d_chunkred = nullptr; h->d_segsc = nullptr;
     h->nseg = 0;
+    h->nchunk = 0;
     if (nseg == 0) return 0;
+    // chunks of at most kChunkRows rows, never across a segment boundary
+    std::vector<int64_t> chunkrow{0}, segchunk{0};
+    std::vector<int32_t> chunkseg, rowseg((size_t)h->n);
+    for (int64_t s = 0; s < nseg; ++s) {
+        for (int64_t r = segptr[s]; r < segptr[s + 1]; r += kChunkRows) {
+            chunkrow.push_back(std::min<int64_t>(segptr[s + 1], r + kChunkRows));
+            chunkseg.push_back((int32_t)s);
+        }
+        segchunk.push_back((int64_t)chunkseg.size());
+        for (int64_t r = segptr[s]; r < segptr[s + 1]; ++r) rowseg[(size_t)r] = (int32_t)s;
+    }
+    const int64_t nch = (int64_t)chunkseg.size();
     int64_t tot = 0;
     int rc = dalloc(h, &h->d_segptr, nseg + 1, &tot);
     if (!rc) rc = dalloc(h, &h->d_segred, nseg * kSegRed, &tot);
     if (!rc) rc = dalloc(h, &h->d_segeta, nseg, &tot);
+    if (!rc) rc = dalloc(h, &h->d_chunkrow, nch + 1, &tot);
+    if (!rc) rc = dalloc(h, &h->d_chunkseg, std::max<int64_t>(nch, 1), &tot);
+    if (!rc) rc = dalloc(h, &h->d_segchunk, nseg + 1, &tot);
+    if (!rc) rc = dalloc(h, &h->d_rowseg, std::max<int64_t>(h->n, 1), &tot);
+    if (!rc) rc = dalloc(h, &h->d_chunkred, std::max<int64_t>(nch, 1) * kChunkRed, &tot);
+    if (!rc) rc = dalloc(h, &h->d_segsc, nseg * 80, &tot);
     if (rc) return rc;
     MF_CUDA(cudaMemcpy(h->d_segptr, segptr, sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice));
     MF_CUDA(cudaMemset(h->d_segeta, 0, sizeof(double) * nseg));
+    MF_CUDA(cudaMemcpy(h->d_chunkrow, chunkrow.data(), sizeof(int64_t) * (nch + 1), cudaMemcpyHostToDevice));
+    if (nch) MF_CUDA(cudaMemcpy(h->d_chunkseg, chunkseg.data(), sizeof(int32_t) * nch, cudaMemcpyHostToDevice));
+    MF_CUDA(cudaMemcpy(h->d_segchunk, segchunk.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice));
+    if (h->n) MF_CUDA(cudaMemcpy(h->d_rowseg, rowseg.data(), sizeof(int32_t) * h->n, cudaMemcpyHostToDevice));
     h->bytes += tot;
     h->nseg = nseg;
+    h->nchunk = nch;
     return 0;
 }
 

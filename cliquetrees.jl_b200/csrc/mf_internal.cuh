@@ -269,6 +269,15 @@ struct mf_handle {
     int64_t* d_segptr = nullptr;   // nseg + 1 row boundaries, elimination order
     double* d_segred = nullptr;    // per segment: max|t|, max|x|, max|b| (3 x 16), ||A||_inf
     double* d_segeta = nullptr;    // per segment: worst backward error of the last refinement step
+    // row chunks of at most kChunkRows rows inside one segment, so that the
+    // per-segment reductions spread over many CTAs even for large segments
+    int64_t nchunk = 0;
+    int64_t* d_chunkrow = nullptr; // nchunk + 1 row boundaries
+    int32_t* d_chunkseg = nullptr; // segment of every chunk
+    int64_t* d_segchunk = nullptr; // chunks of segment s: [d_segchunk[s], d_segchunk[s+1])
+    int32_t* d_rowseg = nullptr;   // segment of every row (n)
+    double* d_chunkred = nullptr;  // per chunk: residual maxima (kSegRed) and dot partials (16)
+    double* d_segsc = nullptr;     // per segment: CG scalars (80)
 
     int64_t bytes = 0;             // device bytes allocated
     // optional per-kernel timing
@@ -323,6 +332,8 @@ int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t*
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);
 int launch_anorm(mf_handle* h);
 constexpr int kSegRed = 49;  // doubles per segment in d_segred
+constexpr int kChunkRows = 16384;  // rows per reduction chunk of a segment
+constexpr int kChunkRed = kSegRed + 16;  // doubles per chunk in d_chunkred
 int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters, double* eta);
 constexpr int kRedDoubles = 256 + 16 * 148 * 4;
 int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs);

@@ -11,11 +11,14 @@
 //               and classical refinement stalls when kappa * eps32 is near 1),
 //               classical Gram-Schmidt applied twice, one Krylov space per
 //               right-hand side;
-//   any handle split into row segments (a batch of independent matrices):
-//               classical iterative refinement x += M^-1 (b - A x), which
-//               keeps the segments independent; the backward error is then
-//               measured per segment and the loop runs until the worst
-//               segment meets the tolerance.
+//   a Cholesky handle split into row segments (a batch of independent
+//               matrices): conjugate gradients with CG scalars per segment
+//               and column (segment dot products over row chunks, summed in
+//               a fixed order), so every matrix follows its own recurrence;
+//   an LDLt handle split into segments: classical iterative refinement
+//               x += M^-1 (b - A x), which keeps the segments independent.
+// With segments the backward error is measured per segment and the loop
+// runs until the worst segment meets the tolerance.
 // Every iteration measures the normwise backward error
 //   eta = ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf)
 // per column and stops when all columns reach the tolerance.  Reductions are
@@ -103,14 +106,17 @@ __global__ void k_resid(const int64_t* __restrict__ ptr, const int32_t* __restri
     if (threadIdx.x < 48 && (threadIdx.x & 15) < nrhs) atomic_max_nonneg(red + threadIdx.x, mx[threadIdx.x]);
 }
 
-// Per-segment version of k_resid: one CTA per segment of rows
-// [segptr[s], segptr[s+1]); maxima into segred[s * kSegRed + (0|16|32) + r].
-__global__ void k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
-                            const int64_t* __restrict__ src, const double* __restrict__ nz,
-                            const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ t,
-                            const int64_t* __restrict__ segptr, double* __restrict__ segred, int64_t n, int nrhs) {
-    const int64_t s = blockIdx.x;
-    const int64_t r0 = segptr[s], r1 = segptr[s + 1];
+// Per-segment version of k_resid over row chunks (one CTA per chunk, a
+// chunk never crosses a segment boundary): the chunk's maxima go to
+// chunkred[c * kChunkRed + (0|16|32) + r]; k_seg_max combines the chunks of
+// every segment.
+__global__ void k_resid_chunk(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                              const int64_t* __restrict__ src, const double* __restrict__ nz,
+                              const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ t,
+                              const int64_t* __restrict__ chunkrow, double* __restrict__ chunkred, int64_t n,
+                              int nrhs) {
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
     double m[48];
 #pragma unroll
     for (int q = 0; q < 48; ++q) m[q] = 0.0;
@@ -120,10 +126,10 @@ __global__ void k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __re
         for (int r = 0; r < 16; ++r) acc[r] = 0.0;
         for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
             const double a = nz[src[p]];
-            const int64_t c = col[p];
+            const int64_t cc = col[p];
 #pragma unroll
             for (int r = 0; r < 16; ++r)
-                if (r < nrhs) acc[r] += a * x[c + r * n];
+                if (r < nrhs) acc[r] += a * x[cc + r * n];
         }
 #pragma unroll
         for (int r = 0; r < 16; ++r)
@@ -147,7 +153,54 @@ __global__ void k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __re
         if ((threadIdx.x & 31) == 0) atomic_max_nonneg(mx + q, v);
     }
     __syncthreads();
-    if (threadIdx.x < 48) segred[s * kSegRed + threadIdx.x] = mx[threadIdx.x];
+    if (threadIdx.x < 48) chunkred[c * kChunkRed + threadIdx.x] = mx[threadIdx.x];
+}
+
+// segred[s * kSegRed + q] = max over the chunks of segment s (q < 48)
+__global__ void k_seg_max(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
+                          double* __restrict__ segred, int64_t nseg) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nseg * 48) return;
+    const int64_t sg = i / 48;
+    const int q = (int)(i % 48);
+    double v = 0.0;
+    for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v = fmax(v, chunkred[c * kChunkRed + q]);
+    segred[sg * kSegRed + q] = v;
+}
+
+// per chunk and column: sum of u .* v over the chunk's rows into
+// chunkred[c * kChunkRed + kSegRed + r]
+__global__ void k_dot_chunk(const double* __restrict__ u, const double* __restrict__ v,
+                            const int64_t* __restrict__ chunkrow, double* __restrict__ chunkred, int64_t n,
+                            int nrhs) {
+    __shared__ double sh[256];
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
+    for (int r = 0; r < nrhs; ++r) {
+        double s = 0.0;
+        for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) s += u[i + r * n] * v[i + r * n];
+        sh[threadIdx.x] = s;
+        __syncthreads();
+        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) chunkred[c * kChunkRed + kSegRed + r] = sh[0];
+        __syncthreads();
+    }
+}
+
+// out[s * 80 + r] = sum over the chunks of segment s (fixed order)
+__global__ void k_dot_seg(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
+                          double* __restrict__ out, int64_t nseg, int nrhs) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nseg * 16) return;
+    const int64_t sg = i / 16;
+    const int r = (int)(i % 16);
+    if (r >= nrhs) return;
+    double v = 0.0;
+    for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v += chunkred[c * kChunkRed + kSegRed + r];
+    out[sg * 80 + r] = v;
 }
 
 // ||A||_inf of every segment into segred[s * kSegRed + 48]
@@ -278,6 +331,42 @@ __global__ void k_cg_p(double* __restrict__ p, const double* __restrict__ z, con
     for (; i < n * nrhs; i += stride) p[i] = z[i] + beta[i / n] * p[i];
 }
 
+// the CG scalars above for every segment: sc[s * 80 + ...]
+__global__ void k_cg_scalars_seg(double* __restrict__ sc, int64_t nseg, int nrhs, int mode) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nseg * 16) return;
+    const int r = (int)(i % 16);
+    if (r >= nrhs) return;
+    double* q = sc + (i / 16) * 80;
+    if (mode == 0) {
+        q[32 + r] = (q[16 + r] != 0.0 && q[r] != 0.0) ? q[r] / q[16 + r] : 0.0;
+    } else {
+        q[64 + r] = q[r] != 0.0 ? q[48 + r] / q[r] : 0.0;
+        q[r] = q[48 + r];
+    }
+}
+
+// x += alpha_s p ; r -= alpha_s q   (alpha of the row's segment)
+__global__ void k_cg_xr_seg(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                            const double* __restrict__ q, const double* __restrict__ sc,
+                            const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) {
+        const double a = sc[(int64_t)rowseg[i % n] * 80 + 32 + i / n];
+        x[i] += a * p[i];
+        r[i] -= a * q[i];
+    }
+}
+
+// p = z + beta_s p
+__global__ void k_cg_p_seg(double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ sc,
+                           const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (; i < n * nrhs; i += stride) p[i] = z[i] + sc[(int64_t)rowseg[i % n] * 80 + 64 + i / n] * p[i];
+}
+
 // c = (float)(s .* r)   and   z = s .* (double)c  (+= when ACC)
 __global__ void k_to32(float* __restrict__ c, const double* __restrict__ r, const double* __restrict__ s, int64_t n,
                        int nrhs) {
@@ -386,14 +475,32 @@ static int dot(mf_handle* h, const double* u, const double* v, double* out, int 
     return 0;
 }
 
+// per-segment dot products into h->d_segsc[s * 80 + off + r]
+static int dot_seg(mf_handle* h, const double* u, const double* v, int off, int nrhs) {
+    if (h->nchunk > 0) {
+        k_dot_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(u, v, h->d_chunkrow, h->d_chunkred, h->n, nrhs);
+        MF_CUDA(cudaGetLastError());
+    }
+    k_dot_seg<<<(unsigned)((h->nseg * 16 + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
+                                                                             h->d_segsc + off, h->nseg, nrhs);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
 // backward error per column into eta[] (host); t receives b - A x when non-null
 static int backward_error(mf_handle* h, const double* x, const double* b, double* t, int nrhs, double* eta,
                           double* maxima = nullptr) {
     Timer tm(h, K_SPMV);
     double* red = h->d_red;  // [0..48) maxima, [48] ||A||_inf
     if (h->nseg > 0) {
-        k_resid_seg<<<(unsigned)h->nseg, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b,
-                                                               t, h->d_segptr, h->d_segred, h->n, nrhs);
+        if (h->nchunk > 0) {
+            k_resid_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc,
+                                                                       h->cur_nz, x, b, t, h->d_chunkrow,
+                                                                       h->d_chunkred, h->n, nrhs);
+            MF_CUDA(cudaGetLastError());
+        }
+        k_seg_max<<<(unsigned)((h->nseg * 48 + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
+                                                                                 h->d_segred, h->nseg);
         MF_CUDA(cudaGetLastError());
         k_seg_eta<<<1, 256, 0, h->stream>>>(h->d_segred, h->nseg, nrhs, red, h->d_segeta);
         MF_CUDA(cudaGetLastError());
@@ -585,14 +692,26 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
         if (eta_out) *eta_out = worst;
         return 0;
     }
-    if (!h->diag && h->nseg == 0) {
-        // preconditioned conjugate gradients (segmented batches use the
-        // refinement below, which keeps every segment independent)
+    if (!h->diag) {
+        // preconditioned conjugate gradients; with row segments (a batch of
+        // independent matrices) every segment has its own CG scalars, so each
+        // matrix follows its own CG recurrence
+        const bool seg = h->nseg > 1;
+        const unsigned sgrid = (unsigned)((std::max<int64_t>(h->nseg, 1) * 16 + 255) / 256);
+        auto dotv = [&](const double* u, const double* v, int off) -> int {
+            return seg ? dot_seg(h, u, v, off, nrhs) : dot(h, u, v, sc + off, nrhs);
+        };
+        auto scalars = [&](int mode) -> int {
+            if (seg) k_cg_scalars_seg<<<sgrid, 256, 0, h->stream>>>(h->d_segsc, h->nseg, nrhs, mode);
+            else k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, mode);
+            MF_CUDA(cudaGetLastError());
+            return 0;
+        };
         MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
         MF_CUDA(cudaMemcpyAsync(R, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
         if ((rc = apply_prec<false>(h, R, Z, nrhs))) return rc;
         MF_CUDA(cudaMemcpyAsync(Pv, Z, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
-        if ((rc = dot(h, R, Z, sc, nrhs))) return rc;  // rz
+        if ((rc = dotv(R, Z, 0))) return rc;  // rz
         for (it = 1; it <= maxit; ++it) {
             {
                 Timer tm(h, K_SPMV);
@@ -600,21 +719,28 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
                                                               n, nrhs);
                 MF_CUDA(cudaGetLastError());
             }
-            if ((rc = dot(h, Pv, Q, sc + 16, nrhs))) return rc;  // pq
-            k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, 0);
-            k_cg_xr<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, sc + 32, n, nrhs);
+            if ((rc = dotv(Pv, Q, 16))) return rc;  // pq
+            if ((rc = scalars(0))) return rc;
+            if (seg)
+                k_cg_xr_seg<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, h->d_segsc, h->d_rowseg, n,
+                                                                        nrhs);
+            else
+                k_cg_xr<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, sc + 32, n, nrhs);
             MF_CUDA(cudaGetLastError());
             if ((rc = backward_error(h, x, b, nullptr, nrhs, eta))) return rc;
             worst = 0.0;
             for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
             if (worst <= tol || it == maxit) break;
             if ((rc = apply_prec<false>(h, R, Z, nrhs))) return rc;
-            if ((rc = dot(h, R, Z, sc + 48, nrhs))) return rc;  // rz_new
-            k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, 1);
-            k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
+            if ((rc = dotv(R, Z, 48))) return rc;  // rz_new
+            if ((rc = scalars(1))) return rc;
+            if (seg)
+                k_cg_p_seg<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, h->d_segsc, h->d_rowseg, n, nrhs);
+            else
+                k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
-    } else if (h->diag && h->nseg == 0) {
+    } else if (h->nseg <= 1) {
         return gmres(h, b, x, nrhs, tol, maxit, iters, eta_out);
     } else {
         // classical iterative refinement
