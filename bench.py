@@ -565,7 +565,7 @@ def run_serving(args, local, world):
 
 
 # served batched form per config: (matrices per device handle, workers, requests)
-SERVED = {1: (32, 4, 1024), 2: (4, 2, 16), 4: (1, 2, 6)}
+SERVED = {1: (32, 4, 1024), 2: (8, 2, 32), 4: (2, 2, 8)}
 
 
 def run_served(args, work, local):

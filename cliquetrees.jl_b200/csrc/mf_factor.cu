@@ -318,6 +318,7 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
     const int w = min(kNB, nn - c0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     T* Pj = P + f.poff;
+#pragma unroll
     for (int e = tid; e < kNB * kNB; e += 256) {
         const int r = e & (kNB - 1), c = e >> 6;
         T v = (r == c) ? T(1) : T(0);
@@ -485,12 +486,14 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
         }
         __syncthreads();
     }
+#pragma unroll
     for (int e = tid; e < kNB * kNB; e += 256) {
         const int r = e & (kNB - 1), c = e >> 6;
         if (r >= c && r < w && c < w) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = A[r + c * LDA];
     }
     if (LDLT && tid < w) d[f.col0 + c0 + tid] = pivs[tid];
     T* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
+#pragma unroll
     for (int e = tid; e < kNB * kNB; e += 256) {
         const int r = e & (kNB - 1), c = e >> 6;
         dst[e] = (r < w && c < w) ? X[r + c * LDA] : T(0);
