@@ -15,8 +15,8 @@
 //               matrices): conjugate gradients with CG scalars per segment
 //               and column (segment dot products over row chunks, summed in
 //               a fixed order), so every matrix follows its own recurrence;
-//   an LDLt handle split into segments: classical iterative refinement
-//               x += M^-1 (b - A x), which keeps the segments independent.
+//   an LDLt handle split into segments: GMRES with one Krylov space per
+//               (segment, column), inner products per segment.
 // With segments the backward error is measured per segment and the loop
 // runs until the worst segment meets the tolerance.
 // Every iteration measures the normwise backward error
@@ -201,26 +201,6 @@ __global__ void k_dot_seg(const double* __restrict__ chunkred, const int64_t* __
     double v = 0.0;
     for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v += chunkred[c * kChunkRed + kSegRed + r];
     out[sg * 80 + r] = v;
-}
-
-// ||A||_inf of every segment into segred[s * kSegRed + 48]
-__global__ void k_anorm_seg(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
-                            const double* __restrict__ nz, const int64_t* __restrict__ segptr,
-                            double* __restrict__ segred) {
-    const int64_t s = blockIdx.x;
-    double v = 0.0;
-    for (int64_t i = segptr[s] + threadIdx.x; i < segptr[s + 1]; i += blockDim.x) {
-        double rs = 0.0;
-        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) rs += fabs(nz[src[p]]);
-        v = fmax(v, rs);
-    }
-    __shared__ double mx;
-    if (threadIdx.x == 0) mx = 0.0;
-    __syncthreads();
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&mx, v);
-    __syncthreads();
-    if (threadIdx.x == 0) segred[s * kSegRed + 48] = mx;
 }
 
 // eta of every (segment, column); segeta[s] = worst column of segment s,
@@ -445,6 +425,89 @@ __global__ void k_colscale(double* __restrict__ dst, const double* __restrict__ 
         dst[k] = src[k] * c[k / n];
 }
 
+// Segmented forms of the GMRES kernels: a right-hand side of every segment
+// has its own Krylov space, so coefficients are indexed (i, segment, column)
+// as c[(i * G + s) * 16 + r] with G segments.
+__global__ void k_mdot_chunk(const double* __restrict__ V, int64_t vs, int J, const double* __restrict__ w,
+                             const int64_t* __restrict__ chunkrow, double* __restrict__ part, int64_t n, int nrhs) {
+    __shared__ double sh[256];
+    const int64_t c = blockIdx.x;
+    const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
+    for (int i = 0; i < J; ++i)
+        for (int r = 0; r < nrhs; ++r) {
+            const double* v = V + i * vs + (int64_t)r * n;
+            const double* ww = w + (int64_t)r * n;
+            double sum = 0.0;
+            for (int64_t k = r0 + threadIdx.x; k < r1; k += blockDim.x) sum += v[k] * ww[k];
+            sh[threadIdx.x] = sum;
+            __syncthreads();
+            for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+                if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) part[(c * J + i) * 16 + r] = sh[0];
+            __syncthreads();
+        }
+}
+__global__ void k_mdot_seg(const double* __restrict__ part, const int64_t* __restrict__ segchunk,
+                           double* __restrict__ out, int64_t G, int J, int nrhs) {
+    const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= (int64_t)J * G * 16) return;
+    const int r = (int)(o % 16);
+    const int64_t sg = (o / 16) % G;
+    const int i = (int)(o / (16 * G));
+    double v = 0.0;
+    if (r < nrhs)
+        for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v += part[(c * J + i) * 16 + r];
+    out[o] = v;
+}
+__global__ void k_mupd_seg(double* __restrict__ w, const double* __restrict__ V, int64_t vs, int J,
+                           const double* __restrict__ c, const int32_t* __restrict__ rowseg, int64_t G, int64_t n,
+                           int nrhs) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = (int64_t)rowseg[k % n] * 16 + k / n;
+        double sum = 0.0;
+        for (int i = 0; i < J; ++i) sum += c[i * G * 16 + q] * V[i * vs + k];
+        w[k] -= sum;
+    }
+}
+__global__ void k_colscale_seg(double* __restrict__ dst, const double* __restrict__ src, const double* __restrict__ c,
+                               const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
+         k += (int64_t)gridDim.x * blockDim.x)
+        dst[k] = src[k] * c[(int64_t)rowseg[k % n] * 16 + k / n];
+}
+
+// ||A||_inf of every chunk into chunkred[c * kChunkRed + 48]; k_seg_anorm
+// takes the maximum over a segment's chunks into segred[s * kSegRed + 48]
+__global__ void k_anorm_chunk(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
+                              const double* __restrict__ nz, const int64_t* __restrict__ chunkrow,
+                              double* __restrict__ chunkred) {
+    const int64_t c = blockIdx.x;
+    double v = 0.0;
+    for (int64_t i = chunkrow[c] + threadIdx.x; i < chunkrow[c + 1]; i += blockDim.x) {
+        double rs = 0.0;
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) rs += fabs(nz[src[p]]);
+        v = fmax(v, rs);
+    }
+    __shared__ double mx;
+    if (threadIdx.x == 0) mx = 0.0;
+    __syncthreads();
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&mx, v);
+    __syncthreads();
+    if (threadIdx.x == 0) chunkred[c * kChunkRed + 48] = mx;
+}
+__global__ void k_seg_anorm(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
+                            double* __restrict__ segred, int64_t nseg) {
+    const int64_t sg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (sg >= nseg) return;
+    double v = 0.0;
+    for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v = fmax(v, chunkred[c * kChunkRed + 48]);
+    segred[sg * kSegRed + 48] = v;
+}
+
 static unsigned gs_blocks(int64_t work) {
     int64_t b = (work + 255) / 256;
     if (b > 148 * 8) b = 148 * 8;
@@ -525,15 +588,22 @@ static int backward_error(mf_handle* h, const double* x, const double* b, double
 }
 
 // Right-preconditioned restarted GMRES, M^-1 = the FP32 factor solve; one
-// Krylov space per right-hand side, all columns advanced together.  Returns
-// the total number of preconditioner applications in *iters.
+// Krylov space per right-hand side, all columns advanced together.  With G
+// row segments (a batch of independent matrices) every (segment, column)
+// pair q = s * 16 + r has its own Krylov space: the inner products are
+// taken per segment and the coefficients applied per row's segment.
+// Returns the total number of preconditioner applications in *iters.
 static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol, int maxit, int* iters,
                  double* eta_out) {
     const int64_t n = h->n;
     const int M = kGmresM;
     const int64_t vs = n * nrhs;
+    const bool seg = h->nseg > 1;
+    const int64_t G = seg ? h->nseg : 1;
+    const int64_t Q = G * 16;  // (segment, column) slots
     const int nblk = (int)std::min<int64_t>(148 * 4, std::max<int64_t>(1, (n + 255) / 256));
-    const int64_t need = (int64_t)(2 * M + 1) * n * h->nrhs_cap + (int64_t)148 * 4 * (M + 1) * 16 + 64 * 16;
+    const int64_t npart = (int64_t)std::max<int64_t>(148 * 4, seg ? h->nchunk : 0) * (M + 1) * 16;
+    const int64_t need = (int64_t)(2 * M + 1) * n * h->nrhs_cap + npart + (M + 1) * Q + 64 * 16;
     if (h->kry_doubles < need) {
         if (h->d_kry) cudaFree(h->d_kry);
         h->d_kry = nullptr;
@@ -544,41 +614,80 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
     }
     double* V = h->d_kry;                                    // M + 1 blocks
     double* Z = V + (int64_t)(M + 1) * n * h->nrhs_cap;      // M blocks
-    double* part = Z + (int64_t)M * n * h->nrhs_cap;         // nblk * (M + 1) * 16
-    double* coef = part + (int64_t)148 * 4 * (M + 1) * 16;   // (M + 1) * 16 coefficients
+    double* part = Z + (int64_t)M * n * h->nrhs_cap;         // partial sums
+    double* coef = part + npart;                             // (M + 1) * Q coefficients
     double* R = h->d_iv + 2 * (int64_t)n * h->nrhs_cap;      // residual
     double eta[16], mx[49];
-    std::vector<double> H((size_t)(M + 1) * M * 16), g((size_t)(M + 1) * 16), cs((size_t)M * 16), sn((size_t)M * 16);
-    std::vector<double> hc((size_t)(M + 1) * 16), beta(16), tgt(16);
+    std::vector<double> H((size_t)(M + 1) * M * Q), g((size_t)(M + 1) * Q), cs((size_t)M * Q), sn((size_t)M * Q);
+    std::vector<double> hc((size_t)(M + 1) * Q), beta(Q), tgt(Q), inv(Q), segred;
     int rc, used = 0;
     double worst = INFINITY;
     MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
+    auto live = [&](int64_t q) { return (int)(q % 16) < nrhs; };
+    // out_host[(i * G + s) * 16 + r] = <V_i, w> over the rows of segment s
     auto mdot = [&](const double* Vb, int J, const double* w, double* out_host) -> int {
-        k_mdot_part<<<nblk, 256, 0, h->stream>>>(Vb, vs, J, w, part, n, nrhs);
+        if (seg) {
+            if (h->nchunk > 0) {
+                k_mdot_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(Vb, vs, J, w, h->d_chunkrow, part, n, nrhs);
+                MF_CUDA(cudaGetLastError());
+            }
+            k_mdot_seg<<<(unsigned)((J * Q + 255) / 256), 256, 0, h->stream>>>(part, h->d_segchunk, coef, G, J,
+                                                                                nrhs);
+        } else {
+            k_mdot_part<<<nblk, 256, 0, h->stream>>>(Vb, vs, J, w, part, n, nrhs);
+            MF_CUDA(cudaGetLastError());
+            k_mdot_final<<<1, 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
+        }
         MF_CUDA(cudaGetLastError());
-        k_mdot_final<<<1, 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
-        MF_CUDA(cudaGetLastError());
-        MF_CUDA(cudaMemcpyAsync(out_host, coef, sizeof(double) * J * 16, cudaMemcpyDeviceToHost, h->stream));
+        MF_CUDA(cudaMemcpyAsync(out_host, coef, sizeof(double) * J * Q, cudaMemcpyDeviceToHost, h->stream));
         MF_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     };
+    auto colscale = [&](double* dst, const double* src, const double* c_host) -> int {
+        MF_CUDA(cudaMemcpyAsync(coef, c_host, sizeof(double) * Q, cudaMemcpyHostToDevice, h->stream));
+        if (seg) k_colscale_seg<<<gs_blocks(vs), 256, 0, h->stream>>>(dst, src, coef, h->d_rowseg, n, nrhs);
+        else k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(dst, src, coef, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+        return 0;
+    };
+    auto mupd = [&](double* w, const double* Vb, int J, const double* c_host) -> int {
+        MF_CUDA(cudaMemcpyAsync(coef, c_host, sizeof(double) * J * Q, cudaMemcpyHostToDevice, h->stream));
+        if (seg) k_mupd_seg<<<gs_blocks(vs), 256, 0, h->stream>>>(w, Vb, vs, J, coef, h->d_rowseg, G, n, nrhs);
+        else k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(w, Vb, vs, J, coef, n, nrhs);
+        MF_CUDA(cudaGetLastError());
+        return 0;
+    };
     while (true) {
-        // true residual and backward error of the current x
+        // true residual and backward error of the current x, and the inner
+        // target of every slot: half the tolerance at the current scale,
+        // on ||r||_2 (>= ||r||_inf)
         if ((rc = backward_error(h, x, b, R, nrhs, eta, mx))) return rc;
         worst = 0.0;
         for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
         if (worst <= tol || used >= maxit) break;
-        // target on ||r||_2 (>= ||r||_inf): half the tolerance at the current scale
-        for (int r = 0; r < nrhs; ++r) tgt[r] = 0.5 * tol * (mx[48] * mx[16 + r] + mx[32 + r]);
+        if (h->nseg > 0) {
+            // per-segment maxima (d_segred) of the residual, x, b and ||A||_inf
+            segred.resize((size_t)h->nseg * kSegRed);
+            MF_CUDA(cudaMemcpyAsync(segred.data(), h->d_segred, sizeof(double) * segred.size(),
+                                    cudaMemcpyDeviceToHost, h->stream));
+            MF_CUDA(cudaStreamSynchronize(h->stream));
+            for (int64_t q = 0; q < Q; ++q) {
+                const double* sr = segred.data() + (q / 16) * kSegRed;  // one segment when !seg
+                const int r = (int)(q % 16);
+                tgt[q] = 0.5 * tol * (sr[48] * sr[16 + r] + sr[32 + r]);
+            }
+        } else {
+            for (int r = 0; r < 16; ++r) tgt[r] = 0.5 * tol * (mx[48] * mx[16 + r] + mx[32 + r]);
+        }
         if ((rc = mdot(R, 1, R, hc.data()))) return rc;
-        for (int r = 0; r < nrhs; ++r) beta[r] = std::sqrt(std::max(hc[r], 0.0));
-        for (int r = 0; r < 16; ++r) hc[r] = (r < nrhs && beta[r] > 0.0) ? 1.0 / beta[r] : 0.0;
-        MF_CUDA(cudaMemcpyAsync(coef, hc.data(), sizeof(double) * 16, cudaMemcpyHostToDevice, h->stream));
-        k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(V, R, coef, n, nrhs);
-        MF_CUDA(cudaGetLastError());
+        for (int64_t q = 0; q < Q; ++q) {
+            beta[q] = live(q) ? std::sqrt(std::max(hc[q], 0.0)) : 0.0;
+            inv[q] = beta[q] > 0.0 ? 1.0 / beta[q] : 0.0;
+        }
+        if ((rc = colscale(V, R, inv.data()))) return rc;
         std::fill(H.begin(), H.end(), 0.0);
         std::fill(g.begin(), g.end(), 0.0);
-        for (int r = 0; r < nrhs; ++r) g[r] = beta[r];
+        for (int64_t q = 0; q < Q; ++q) g[q] = beta[q];
         int j = 0;
         bool stop = false;
         for (; j < M && !stop && used < maxit; ++j) {
@@ -596,58 +705,52 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
             // classical Gram-Schmidt, twice
             for (int pass = 0; pass < 2; ++pass) {
                 if ((rc = mdot(V, j + 1, w, hc.data()))) return rc;
-                MF_CUDA(cudaMemcpyAsync(coef, hc.data(), sizeof(double) * (j + 1) * 16, cudaMemcpyHostToDevice,
-                                        h->stream));
-                k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(w, V, vs, j + 1, coef, n, nrhs);
-                MF_CUDA(cudaGetLastError());
+                if ((rc = mupd(w, V, j + 1, hc.data()))) return rc;
                 for (int i = 0; i <= j; ++i)
-                    for (int r = 0; r < nrhs; ++r) H[((size_t)i * M + j) * 16 + r] += hc[i * 16 + r];
+                    for (int64_t q = 0; q < Q; ++q) H[((size_t)i * M + j) * Q + q] += hc[i * Q + q];
             }
             if ((rc = mdot(w, 1, w, hc.data()))) return rc;
-            std::vector<double> inv(16, 0.0);
             stop = true;
-            for (int r = 0; r < nrhs; ++r) {
-                const double hn = std::sqrt(std::max(hc[r], 0.0));
-                H[((size_t)(j + 1) * M + j) * 16 + r] = hn;
-                inv[r] = hn > 0.0 ? 1.0 / hn : 0.0;
+            for (int64_t q = 0; q < Q; ++q) {
+                if (!live(q)) { inv[q] = 0.0; continue; }
+                const double hn = std::sqrt(std::max(hc[q], 0.0));
+                H[((size_t)(j + 1) * M + j) * Q + q] = hn;
+                inv[q] = hn > 0.0 ? 1.0 / hn : 0.0;
                 // apply the earlier rotations to column j, then a new one
                 for (int i = 0; i < j; ++i) {
-                    double& a = H[((size_t)i * M + j) * 16 + r];
-                    double& c2 = H[((size_t)(i + 1) * M + j) * 16 + r];
-                    const double t0 = cs[i * 16 + r] * a + sn[i * 16 + r] * c2;
-                    c2 = -sn[i * 16 + r] * a + cs[i * 16 + r] * c2;
+                    double& a = H[((size_t)i * M + j) * Q + q];
+                    double& c2 = H[((size_t)(i + 1) * M + j) * Q + q];
+                    const double t0 = cs[i * Q + q] * a + sn[i * Q + q] * c2;
+                    c2 = -sn[i * Q + q] * a + cs[i * Q + q] * c2;
                     a = t0;
                 }
-                double& a = H[((size_t)j * M + j) * 16 + r];
-                double& c2 = H[((size_t)(j + 1) * M + j) * 16 + r];
+                double& a = H[((size_t)j * M + j) * Q + q];
+                double& c2 = H[((size_t)(j + 1) * M + j) * Q + q];
                 const double den = std::hypot(a, c2);
-                const double c = den > 0.0 ? a / den : 1.0, s = den > 0.0 ? c2 / den : 0.0;
-                cs[j * 16 + r] = c;
-                sn[j * 16 + r] = s;
+                const double c = den > 0.0 ? a / den : 1.0, sgn = den > 0.0 ? c2 / den : 0.0;
+                cs[j * Q + q] = c;
+                sn[j * Q + q] = sgn;
                 a = den;
                 c2 = 0.0;
-                g[(j + 1) * 16 + r] = -s * g[j * 16 + r];
-                g[j * 16 + r] = c * g[j * 16 + r];
-                if (std::fabs(g[(j + 1) * 16 + r]) > tgt[r] && hn > 0.0) stop = false;
+                g[(j + 1) * Q + q] = -sgn * g[j * Q + q];
+                g[j * Q + q] = c * g[j * Q + q];
+                if (std::fabs(g[(j + 1) * Q + q]) > tgt[q] && hn > 0.0) stop = false;
             }
-            MF_CUDA(cudaMemcpyAsync(coef, inv.data(), sizeof(double) * 16, cudaMemcpyHostToDevice, h->stream));
-            k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(w, w, coef, n, nrhs);
-            MF_CUDA(cudaGetLastError());
+            if ((rc = colscale(w, w, inv.data()))) return rc;
         }
         // y = H^-1 g (upper triangular, j x j), x += Z y
-        std::vector<double> y((size_t)j * 16, 0.0);
-        for (int r = 0; r < nrhs; ++r)
+        std::vector<double> y((size_t)j * Q, 0.0);
+        for (int64_t q = 0; q < Q; ++q) {
+            if (!live(q)) continue;
             for (int i = j - 1; i >= 0; --i) {
-                double v = g[i * 16 + r];
-                for (int k = i + 1; k < j; ++k) v -= H[((size_t)i * M + k) * 16 + r] * y[k * 16 + r];
-                const double d = H[((size_t)i * M + i) * 16 + r];
-                y[i * 16 + r] = d != 0.0 ? v / d : 0.0;
+                double v = g[i * Q + q];
+                for (int k = i + 1; k < j; ++k) v -= H[((size_t)i * M + k) * Q + q] * y[k * Q + q];
+                const double d = H[((size_t)i * M + i) * Q + q];
+                y[i * Q + q] = d != 0.0 ? v / d : 0.0;
             }
-        for (int i = 0; i < j; ++i)
-            for (int r = 0; r < 16; ++r) y[i * 16 + r] = -y[i * 16 + r];  // k_mupd subtracts
-        MF_CUDA(cudaMemcpyAsync(coef, y.data(), sizeof(double) * j * 16, cudaMemcpyHostToDevice, h->stream));
-        k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(x, Z, vs, j, coef, n, nrhs);
-        MF_CUDA(cudaGetLastError());
+        }
+        for (auto& v : y) v = -v;  // mupd subtracts
+        if ((rc = mupd(x, Z, j, y.data()))) return rc;
     }
     if (iters) *iters = used;
     if (eta_out) *eta_out = worst;
@@ -660,8 +763,13 @@ int launch_anorm(mf_handle* h) {
     k_anorm<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, out, h->n);
     MF_CUDA(cudaGetLastError());
     if (h->nseg > 0) {
-        k_anorm_seg<<<(unsigned)h->nseg, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, h->d_segptr,
-                                                               h->d_segred);
+        if (h->nchunk > 0) {
+            k_anorm_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz,
+                                                                       h->d_chunkrow, h->d_chunkred);
+            MF_CUDA(cudaGetLastError());
+        }
+        k_seg_anorm<<<(unsigned)((h->nseg + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
+                                                                               h->d_segred, h->nseg);
         MF_CUDA(cudaGetLastError());
     }
     return 0;
@@ -740,20 +848,8 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
                 k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
-    } else if (h->nseg <= 1) {
-        return gmres(h, b, x, nrhs, tol, maxit, iters, eta_out);
     } else {
-        // classical iterative refinement
-        MF_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n * nrhs, h->stream));
-        MF_CUDA(cudaMemcpyAsync(R, b, sizeof(double) * n * nrhs, cudaMemcpyDeviceToDevice, h->stream));
-        for (it = 1; it <= maxit; ++it) {
-            if ((rc = apply_prec<true>(h, R, x, nrhs))) return rc;
-            if ((rc = backward_error(h, x, b, R, nrhs, eta))) return rc;
-            worst = 0.0;
-            for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
-            if (worst <= tol) break;
-        }
-        if (it > maxit) it = maxit;
+        return gmres(h, b, x, nrhs, tol, maxit, iters, eta_out);
     }
     if (iters) *iters = it;
     if (eta_out) *eta_out = worst;

@@ -134,10 +134,10 @@ int mf_kernel_choice(const mf_handle* h, int32_t* tc_steps, int32_t* tc_syrk);
 int mf_set_kernel_choice(mf_handle* h, const int32_t* tc_steps, const int32_t* tc_syrk);
 
 /* x = A^-1 b to normwise backward error <= tol in FP64 with the FP32 factor
- * as preconditioner: conjugate gradients (Cholesky), GMRES (LDLt), or
- * classical iterative refinement when segments are set (every segment is
- * refined to its own backward error); B (n x nrhs, ORIGINAL order) is
- * overwritten with x.  *iters and *eta report the worst right-hand side. */
+ * as preconditioner: conjugate gradients (Cholesky) or GMRES (LDLt); when
+ * segments are set (mf_set_segments) every segment runs its own recurrence
+ * and is refined to its own backward error.  B (n x nrhs, ORIGINAL order)
+ * is overwritten with x.  *iters and *eta report the worst right-hand side. */
 int mf_solve_refined(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* perm, double tol, int maxit,
                      int* iters, double* eta);
 int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev,
