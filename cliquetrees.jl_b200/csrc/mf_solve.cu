@@ -574,59 +574,91 @@ __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ front
 
 // backward: W[res tile] = C[res tile] - L21^T x[sep].  Items are (front,
 // 64-column tile, chunk of kBwdRows rows of L21); each writes its partial
-// sums to part[item.pad], staging L rows and the gathered x[sep] through
-// shared memory 64 rows at a time (L read once, coalesced).  k_s_bwd_red
-// then adds the chunks of a tile in a fixed order.
-template <typename T>
-constexpr int bwd_smem() { return (kNB * SLD + kNB * kMaxRhs) * (int)sizeof(T); }
+// sums to part[item.pad] and k_s_bwd_red adds the chunks of a tile in a
+// fixed order.  The chunk's x[sep] rows are gathered into shared memory
+// once; thread (q, c) then owns column c over a quarter of the chunk's rows
+// and streams them from the panel 16 bytes at a time (the rows are taken
+// from the 4-aligned row at or before the chunk start; rows outside the
+// chunk are dropped by a select), with x as a shared-memory broadcast.  The
+// four quarters are added in order.
+constexpr int kBwdAlignRows = kBwdRows + 16;  // staged rows: the chunk, its alignment lead-in, quarters of 4k rows
 
-template <typename T>
+template <typename T, int NR>
+constexpr int bwd_smem() { return (kBwdAlignRows * NR + 4 * NR * kNB) * (int)sizeof(T); }
+
+template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  const int32_t* __restrict__ septgt, const T* __restrict__ P,
                                                  const T* __restrict__ C, T* __restrict__ part, int64_t n,
                                                  int nrhs) {
+    using VT = Vec16<T>;
+    using V = typename VT::type;
+    constexpr int VW = VT::W;
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    T* Lt = reinterpret_cast<T*>(sm_raw);  // [c][a] : Lt[a + c*SLD], 64 rows x 64 columns
-    T* xs = Lt + kNB * SLD;                // [r][a] : xs[a + r*kNB]
+    T* xs = reinterpret_cast<T*>(sm_raw);  // xs[i * NR + r], i = panel row - row0
+    T* red = xs + kBwdAlignRows * NR;      // red[(q * NR + r) * kNB + c]
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, ld = f.ldp;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const T* Pj = P + f.poff;
+    const int tid = threadIdx.x;
     const int32_t* sep = septgt + f.sep0;
     const int c0 = it.a * kNB, wc = min(kNB, nn - c0);
     const int a_beg = it.b * kBwdRows, a_end = min(na, a_beg + kBwdRows);
-    // outputs: (column c, rhs r), at most 64 x 16 = 1024, 4 per thread
-    T acc[4] = {T(0), T(0), T(0), T(0)};
-    for (int a0 = a_beg; a0 < a_end; a0 += kNB) {
-        const int wa = min(kNB, a_end - a0);
-        __syncthreads();
-        for (int i = tid; i < wa * wc; i += nt) {
-            int a = i % wa, c = i / wa;
-            Lt[a + c * SLD] = Pj[(nn + a0 + a) + (int64_t)(c0 + c) * ld];
-        }
-        for (int i = tid; i < wa * nrhs; i += nt) {
-            int a = i % wa, r = i / wa;
-            xs[a + r * kNB] = C[sep[a0 + a] + (int64_t)r * n];
-        }
-        __syncthreads();
+    const int rlo = nn + a_beg, rhi = nn + a_end;  // panel rows of the chunk
+    const int row0 = rlo & ~3;                     // 4-aligned start of the staged rows
+    const int nrow = rhi - row0;                   // <= kBwdAlignRows
+    for (int i = tid; i < kBwdAlignRows * NR; i += 256) {
+        const int a = i % kBwdAlignRows, r = i / kBwdAlignRows;
+        const int row = row0 + a;
+        xs[a * NR + r] = (row >= rlo && row < rhi && r < nrhs) ? C[sep[row - nn] + (int64_t)r * n] : T(0);
+    }
+    __syncthreads();
+    const int c = tid & (kNB - 1), q = tid >> 6;
+    constexpr int QR = kBwdAlignRows / 4;      // rows per quarter (a multiple of 4)
+    const int i0 = q * QR, ni = min(QR, nrow - i0);
+    T acc[NR];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            int o = tid + u * nt;
-            int c = o % kNB, r = o / kNB;
-            if (c < wc && r < nrhs) {
-                T s = T(0);
-                for (int a = 0; a < wa; ++a) s += Lt[a + c * SLD] * xs[a + r * kNB];
-                acc[u] += s;
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    if (c < wc && ni > 0) {
+        // row0 + i0 + i is a multiple of 4 below rhi <= nj, so each 16-byte
+        // load ends inside the column's ldp rows
+        const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + row0 + i0;
+        for (int i = 0; i < QR; i += 8 * VW) {
+            V l[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int ib = i + u * VW;
+                if (ib < ni) {
+                    const T* xr = xs + (i0 + ib) * NR;
+#pragma unroll
+                    for (int e = 0; e < VW; ++e) {
+                        // rows before the chunk hold finite factor entries and meet
+                        // x = 0; rows past it (up to ldp) are dropped here
+                        const T lv = ib + e < ni ? VT::at(l[u], e) : T(0);
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) acc[r] += lv * xr[e * NR + r];
+                    }
+                }
             }
         }
     }
-    T* dst = part + (int64_t)it.pad * (kNB * kMaxRhs);
 #pragma unroll
-    for (int u = 0; u < 4; ++u) dst[tid + u * nt] = acc[u];
+    for (int r = 0; r < NR; ++r) red[(q * NR + r) * kNB + c] = acc[r];
+    __syncthreads();
+    T* dst = part + (int64_t)it.pad * (kNB * kMaxRhs);
+    for (int o = tid; o < kNB * kMaxRhs; o += 256) {
+        const int cc = o % kNB, r = o / kNB;
+        T v = T(0);
+        if (r < NR)
+            v = red[(0 * NR + r) * kNB + cc] + red[(1 * NR + r) * kNB + cc] + red[(2 * NR + r) * kNB + cc] +
+                red[(3 * NR + r) * kNB + cc];
+        dst[o] = v;
+    }
 }
 
-// W[res tile] = C[res tile] - sum over the tile's chunks (in order)
 template <typename T>
 __global__ void __launch_bounds__(256) k_s_bwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                    const T* __restrict__ part, const T* __restrict__ C,
@@ -699,7 +731,9 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
-    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 8>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small_solve_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_bwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -772,8 +806,15 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         const Level& lv = h->levels[L];
         if (lv.s_bwd_l.cnt) {
             Timer t(h, K_S_BWD_L);
-            k_s_bwd_l<T><<<(unsigned)lv.s_bwd_l.cnt, 256, bwd_smem<T>(), h->stream>>>(
-                h->d_fronts, items + lv.s_bwd_l.off, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs);
+            const unsigned gl = (unsigned)lv.s_bwd_l.cnt;
+            const Item* itl = items + lv.s_bwd_l.off;
+            switch (nrb) {
+                case 1: k_s_bwd_l<T, 1><<<gl, 256, bwd_smem<T, 1>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 2: k_s_bwd_l<T, 2><<<gl, 256, bwd_smem<T, 2>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 4: k_s_bwd_l<T, 4><<<gl, 256, bwd_smem<T, 4>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 8: k_s_bwd_l<T, 8><<<gl, 256, bwd_smem<T, 8>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                default: k_s_bwd_l<T, 16><<<gl, 256, bwd_smem<T, 16>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+            }
             MF_CUDA(cudaGetLastError());
             k_s_bwd_red<T><<<(unsigned)lv.s_bwd_red.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_bwd_red.off,
                                                                               sb.part, sb.C, sb.W, n, nrhs);
