@@ -673,7 +673,7 @@ enum GemmRole { G_LEFT = 0, G_TRAIL = 1, G_SYRK = 2, G_TRSM = 3 };
 
 template <typename T, int ROLE, int LDLT>
 __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                              int ob, int c0, T* __restrict__ P, T* __restrict__ M,
+                                              int obs, int obw, int c0, T* __restrict__ P, T* __restrict__ M,
                                               const T* __restrict__ d, const T* __restrict__ inv) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
@@ -687,12 +687,12 @@ __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, 
     if (ROLE == G_LEFT) {
         const int w = min(kNB, nn - c0);
         const int rs = c0 + it.a * kTile;
-        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, ob * kOB, c0, dj);
+        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, obs, c0, dj);
         acc_store<false>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_TRAIL) {
-        const int e = min(nn, (ob + 1) * kOB);
+        const int e = min(nn, obs + obw);
         const int cs = e + it.b * kTile, rs = cs + it.a * kTile;
-        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, ob * kOB, e, dj);
+        gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, obs, e, dj);
         acc_store<false>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_SYRK) {
         const int rs = it.a * kTile, cs = it.b * kTile;
@@ -948,14 +948,15 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         }
         if (h->tuning) MF_CUDA(cudaEventRecord(tev[0], h->stream));
         for (const PanelStep& st : lv.steps) {
-            const int c0 = st.b * kOB + st.s * kNB;
+            const int obs = st.b * lv.kob, obw = lv.kob;
+            const int c0 = obs + st.s * kNB;
             if (std::is_same<T, float>::value && h->use_tc && lv.tc_steps) {
                 // single precision: the GEMM roles run on the tcgen05 tensor cores
                 const FactorBufs<float>& f32b = reinterpret_cast<const FactorBufs<float>&>(fb);
                 int rc;
                 if (st.left_tc.cnt) {
                     Timer t(h, K_LEFT);
-                    if ((rc = tc_launch(h, 0, st.left_tc, st.b, c0, f32b))) return rc;
+                    if ((rc = tc_launch(h, 0, st.left_tc, obs, obw, c0, f32b))) return rc;
                 }
                 if (st.diag.cnt) {
                     Timer t(h, K_DIAG);
@@ -965,18 +966,18 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 }
                 if (st.panel_tc.cnt) {
                     Timer t(h, K_PANEL);
-                    if ((rc = tc_launch(h, 3, st.panel_tc, st.b, c0, f32b))) return rc;
+                    if ((rc = tc_launch(h, 3, st.panel_tc, obs, obw, c0, f32b))) return rc;
                 }
                 if (st.trail_tc.cnt) {
                     Timer t(h, K_UPDATE);
-                    if ((rc = tc_launch(h, 1, st.trail_tc, st.b, c0, f32b))) return rc;
+                    if ((rc = tc_launch(h, 1, st.trail_tc, obs, obw, c0, f32b))) return rc;
                 }
                 continue;
             }
             if (st.left.cnt) {
                 Timer t(h, K_LEFT);
                 k_gemm<T, G_LEFT, LDLT><<<grid_for(st.left.cnt), 256, gs, h->stream>>>(
-                    h->d_fronts, items + st.left.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
+                    h->d_fronts, items + st.left.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.diag.cnt) {
@@ -988,13 +989,13 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             if (st.panel.cnt) {
                 Timer t(h, K_PANEL);
                 k_gemm<T, G_TRSM, LDLT><<<grid_for(st.panel.cnt), 256, gs, h->stream>>>(
-                    h->d_fronts, items + st.panel.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
+                    h->d_fronts, items + st.panel.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.trail.cnt) {
                 Timer t(h, K_UPDATE);
                 k_gemm<T, G_TRAIL, LDLT><<<grid_for(st.trail.cnt), 256, gs, h->stream>>>(
-                    h->d_fronts, items + st.trail.off, st.b, c0, fb.P, fb.M, fb.d, fb.inv);
+                    h->d_fronts, items + st.trail.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
         }
@@ -1002,13 +1003,13 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         if (std::is_same<T, float>::value && h->use_tc && lv.tc_syrk) {
             if (lv.syrk_tc.cnt) {
                 Timer t(h, K_SYRK);
-                int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
+                int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
                 if (rc) return rc;
             }
         } else if (lv.syrk.cnt) {
             Timer t(h, K_SYRK);
             k_gemm<T, G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, gs, h->stream>>>(
-                h->d_fronts, items + lv.syrk.off, 0, 0, fb.P, fb.M, fb.d, fb.inv);
+                h->d_fronts, items + lv.syrk.off, 0, 0, 0, fb.P, fb.M, fb.d, fb.inv);
             MF_CUDA(cudaGetLastError());
         }
         if (h->tuning) {

@@ -71,6 +71,8 @@ constexpr int kNB = 64;         // sub-panel width of the blocked path
 #define MF_KOB 256
 #endif
 constexpr int kOB = MF_KOB;     // outer block: trailing updates run with K = kOB
+constexpr int kOBWide = 2 * kOB;  // outer block of levels whose largest front has >= kWideFrontNN columns
+constexpr int kWideFrontNN = 12288;
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns stay kTile
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
@@ -81,13 +83,13 @@ constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
 
-// One 64-wide sub-panel s of outer block b (columns b*kOB + s*kNB ...).
+// One 64-wide sub-panel s of outer block b (columns b*kob + s*kNB ..., kob the level's outer-block width).
 struct PanelStep {
     int b = 0, s = 0;
     ItemList left;    // (front, row tile)  : left-looking update from the outer block's earlier sub-panels
     ItemList diag;    // (front)            : diagonal block factor + inverse
     ItemList panel;   // (front, row tile)  : panel TRSM below the diagonal block (GEMM with the inverse)
-    ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kOB
+    ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kob
     // the same work in 128-row tiles for the tensor-core (tcgen05) kernels
     ItemList left_tc, panel_tc, trail_tc;
 };
@@ -112,6 +114,7 @@ struct Level {
     ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
     ItemList s_bwd_red;      // (front, col tile, first partial slot)
     int max_nn_blocked = 0;
+    int kob = kOB;           // outer-block width of this level's panel steps (kOB or kOBWide)
     // FP32 kernel choice of this level, set by mf_autotune: 1 = tcgen05
     // tensor-core tiles (128 x 64 / 128 x 128), 0 = FFMA tiles (64 x 64)
     int tc_steps = 1;        // left-looking, TRSM and trailing roles of the panel steps
@@ -317,7 +320,7 @@ int ensure_fp64(mf_handle* h);
 int have_fp64(const mf_handle* h);
 int launch_factor_mixed(mf_handle* h);
 int tc_prepare(mf_handle* h);
-int tc_launch(mf_handle* h, int role, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb);
+int tc_launch(mf_handle* h, int role, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb);
 int launch_assemble_mixed(mf_handle* h, const double* dnz);
 int launch_dl_to_panel(mf_handle* h, const double* dDval, const double* dLval);
 int launch_panel_to_dl(mf_handle* h, double* dDval, double* dLval);

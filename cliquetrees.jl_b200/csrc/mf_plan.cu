@@ -352,10 +352,18 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             lv.max_nn_blocked = std::max(lv.max_nn_blocked, f.nn);
         }
         end(lv.ea);
-        // two-level blocking: outer blocks of kOB columns, sub-panels of kNB
-        for (int ob = 0; ob * kOB < lv.max_nn_blocked; ++ob) {
-            for (int sp = 0; sp < kOB / kNB; ++sp) {
-                const int c0 = ob * kOB + sp * kNB;
+        // two-level blocking: outer blocks of kob columns, sub-panels of kNB;
+        // levels with a very large front take wider outer blocks (trailing
+        // updates with a longer K amortise the tile overheads)
+        {
+            const char* wenv = getenv("MF_WIDE_FRONT_NN");
+            const int wide_nn = wenv ? atoi(wenv) : kWideFrontNN;
+            lv.kob = (wide_nn > 0 && lv.max_nn_blocked >= wide_nn) ? kOBWide : kOB;
+        }
+        const int kob = lv.kob;
+        for (int ob = 0; ob * kob < lv.max_nn_blocked; ++ob) {
+            for (int sp = 0; sp < kob / kNB; ++sp) {
+                const int c0 = ob * kob + sp * kNB;
                 if (c0 >= lv.max_nn_blocked) break;
                 PanelStep st;
                 st.b = ob; st.s = sp;
@@ -383,12 +391,12 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 }
                 end(st.panel);
                 begin(st.trail);
-                const bool last_sub = (sp == kOB / kNB - 1) || (c0 + kNB >= lv.max_nn_blocked);
+                const bool last_sub = (sp == kob / kNB - 1) || (c0 + kNB >= lv.max_nn_blocked);
                 if (last_sub)
                     for (int32_t j : fr) {
                         const Front& f = h->h_fronts[j];
-                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kOB) continue;
-                        const int e = std::min(f.nn, (ob + 1) * kOB);
+                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kob) continue;
+                        const int e = std::min(f.nn, (ob + 1) * kob);
                         if (e >= f.nn) continue;  // no panel columns after this outer block
                         const int nj = f.nn + f.na;
                         for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
@@ -419,8 +427,8 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 if (last_sub)
                     for (int32_t j : fr) {
                         const Front& f = h->h_fronts[j];
-                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kOB) continue;
-                        const int e = std::min(f.nn, (ob + 1) * kOB);
+                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kob) continue;
+                        const int e = std::min(f.nn, (ob + 1) * kob);
                         if (e >= f.nn) continue;
                         const int nj = f.nn + f.na;
                         for (int tj = 0; tj < (int)cdiv(f.nn - e, kTcTrailN); ++tj) {

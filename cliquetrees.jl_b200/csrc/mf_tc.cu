@@ -256,7 +256,7 @@ struct TileGeom {
 };
 
 template <int ROLE>
-__device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, const Item& it, int ob, int c0,
+__device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, const Item& it, int obs, int obw, int c0,
                                               float* P, float* M) {
     constexpr int TN = TcTileN<ROLE>::value;
     const Front f = fronts[it.front];
@@ -266,14 +266,14 @@ __device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, 
     if (ROLE == TC_LEFT) {
         const int w = min(kNB, nn - c0);
         g.xa = c0 + it.a * tc::TM; g.xb = c0;
-        g.kbeg = ob * kOB; g.kend = c0; g.ka0 = g.kb0 = 0;
+        g.kbeg = obs; g.kend = c0; g.ka0 = g.kb0 = 0;
         g.orow = g.xa; g.ocol = c0; g.rlo = c0; g.rhi = nj; g.clo = c0; g.chi = c0 + w; g.tri = true;
         g.C = P + f.poff; g.ldc = f.ldp;
     } else if (ROLE == TC_TRAIL) {
-        const int e = min(nn, (ob + 1) * kOB);
+        const int e = min(nn, obs + obw);
         const int cs = e + it.b * TN;
         g.xa = cs + it.a * tc::TM; g.xb = cs;
-        g.kbeg = ob * kOB; g.kend = e; g.ka0 = g.kb0 = 0;
+        g.kbeg = obs; g.kend = e; g.ka0 = g.kb0 = 0;
         g.orow = g.xa; g.ocol = cs; g.rlo = cs; g.rhi = nj; g.clo = cs; g.chi = nn; g.tri = true;
         g.C = P + f.poff; g.ldc = f.ldp;
     } else if (ROLE == TC_SYRK) {
@@ -300,7 +300,7 @@ __device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, 
 
 template <int ROLE, int LDLT>
 __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__ fronts,
-                                                       const Item* __restrict__ items, int64_t ntiles, int ob, int c0,
+                                                       const Item* __restrict__ items, int64_t ntiles, int obs, int obw, int c0,
                                                        float* __restrict__ P, float* __restrict__ M,
                                                        const float* __restrict__ d,
                                                        const CUtensorMap* __restrict__ maps,
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
             bool ok = true;
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
                 const Item it = items[t];
-                const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+                const TileGeom tg = tile_geom<ROLE>(fronts, it, obs, obw, c0, P, M);
                 if (tg.nchunk == 0) { fail(2); ok = false; break; }
                 const CUtensorMap* amap = maps + it.front;
                 const CUtensorMap* bmap = ROLE == TC_TRSM ? inv_map : amap;
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
         int64_t g = 0;
         for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
             const Item it = items[t];
-            const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+            const TileGeom tg = tile_geom<ROLE>(fronts, it, obs, obw, c0, P, M);
             const float* dvec = (LDLT && ROLE != TC_TRSM) ? d + fronts[it.front].col0 : nullptr;
             bool ok = true;
             for (int c = 0; c < tg.nchunk; ++c, ++g) {
@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
             bool ok = true;
             for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
                 const Item it = items[t];
-                const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+                const TileGeom tg = tile_geom<ROLE>(fronts, it, obs, obw, c0, P, M);
                 const int a = (int)(i & 1);
                 if (i >= 2 && !mbar_wait(&acc_empty[a], (uint32_t)(((i / 2) - 1) & 1), abort)) {
                     fail(1);
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
         int64_t i = 0;
         for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
             const Item it = items[t];
-            const TileGeom tg = tile_geom<ROLE>(fronts, it, ob, c0, P, M);
+            const TileGeom tg = tile_geom<ROLE>(fronts, it, obs, obw, c0, P, M);
             const int a = (int)(i & 1);
             const int row = tg.orow + quarter * 32 + lane;
             const int cbase = tg.ocol + half * HC;
@@ -513,12 +513,12 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
 }
 
 template <int ROLE, int LDLT>
-static int launch_one(mf_handle* h, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb) {
+static int launch_one(mf_handle* h, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb) {
     if (!l.cnt) return 0;
     constexpr int smem = tc::Cfg<TcTileN<ROLE>::value>::SMEM_BYTES;
     const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
     k_gemm_tc<ROLE, LDLT><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
-        h->d_fronts, h->d_items + l.off, l.cnt, ob, c0, fb.P, fb.M, fb.d,
+        h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
         h->d_err);
     MF_CUDA(cudaGetLastError());
@@ -609,20 +609,20 @@ int tc_prepare(mf_handle* h) {
     return h->diag ? set_attrs<1>() : set_attrs<0>();
 }
 
-int tc_launch(mf_handle* h, int role, const ItemList& l, int ob, int c0, const FactorBufs<float>& fb) {
+int tc_launch(mf_handle* h, int role, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb) {
     if (h->diag) {
         switch (role) {
-            case TC_LEFT: return launch_one<TC_LEFT, 1>(h, l, ob, c0, fb);
-            case TC_TRAIL: return launch_one<TC_TRAIL, 1>(h, l, ob, c0, fb);
-            case TC_SYRK: return launch_one<TC_SYRK, 1>(h, l, ob, c0, fb);
-            default: return launch_one<TC_TRSM, 1>(h, l, ob, c0, fb);
+            case TC_LEFT: return launch_one<TC_LEFT, 1>(h, l, obs, obw, c0, fb);
+            case TC_TRAIL: return launch_one<TC_TRAIL, 1>(h, l, obs, obw, c0, fb);
+            case TC_SYRK: return launch_one<TC_SYRK, 1>(h, l, obs, obw, c0, fb);
+            default: return launch_one<TC_TRSM, 1>(h, l, obs, obw, c0, fb);
         }
     }
     switch (role) {
-        case TC_LEFT: return launch_one<TC_LEFT, 0>(h, l, ob, c0, fb);
-        case TC_TRAIL: return launch_one<TC_TRAIL, 0>(h, l, ob, c0, fb);
-        case TC_SYRK: return launch_one<TC_SYRK, 0>(h, l, ob, c0, fb);
-        default: return launch_one<TC_TRSM, 0>(h, l, ob, c0, fb);
+        case TC_LEFT: return launch_one<TC_LEFT, 0>(h, l, obs, obw, c0, fb);
+        case TC_TRAIL: return launch_one<TC_TRAIL, 0>(h, l, obs, obw, c0, fb);
+        case TC_SYRK: return launch_one<TC_SYRK, 0>(h, l, obs, obw, c0, fb);
+        default: return launch_one<TC_TRSM, 0>(h, l, obs, obw, c0, fb);
     }
 }
 
