@@ -802,6 +802,7 @@ int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
     h->d_chunkred = nullptr; h->d_segsc = nullptr;
     h->nseg = 0;
     h->nchunk = 0;
+    h->h_segptr.clear();
     if (nseg == 0) return 0;
     // chunks of at most kChunkRows rows, never across a segment boundary
     std::vector<int64_t> chunkrow{0}, segchunk{0};
@@ -835,6 +836,7 @@ int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
     h->bytes += tot;
     h->nseg = nseg;
     h->nchunk = nch;
+    h->h_segptr.assign(segptr, segptr + nseg + 1);
     return 0;
 }
 

@@ -274,6 +274,7 @@ struct mf_handle {
     double* d_segeta = nullptr;    // per segment: worst backward error of the last refinement step
     // row chunks of at most kChunkRows rows inside one segment, so that the
     // per-segment reductions spread over many CTAs even for large segments
+    std::vector<int64_t> h_segptr; // host copy of the segment boundaries
     int64_t nchunk = 0;
     int64_t* d_chunkrow = nullptr; // nchunk + 1 row boundaries
     int32_t* d_chunkseg = nullptr; // segment of every chunk

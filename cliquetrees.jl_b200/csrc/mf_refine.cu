@@ -659,8 +659,10 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
     };
     while (true) {
         // true residual and backward error of the current x, and the inner
-        // target of every slot: half the tolerance at the current scale,
-        // on ||r||_2 (>= ||r||_inf)
+        // target of every slot on GMRES's ||r||_2: half the tolerance at the
+        // current scale, widened by sqrt(rows) / 8 -- a residual spread over
+        // m rows has ||r||_inf near a few times ||r||_2 / sqrt(m); the outer
+        // loop checks the true backward error and restarts if it is missed
         if ((rc = backward_error(h, x, b, R, nrhs, eta, mx))) return rc;
         worst = 0.0;
         for (int r = 0; r < nrhs; ++r) worst = std::max(worst, eta[r]);
@@ -674,10 +676,13 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
             for (int64_t q = 0; q < Q; ++q) {
                 const double* sr = segred.data() + (q / 16) * kSegRed;  // one segment when !seg
                 const int r = (int)(q % 16);
-                tgt[q] = 0.5 * tol * (sr[48] * sr[16 + r] + sr[32 + r]);
+                const int64_t rows = seg ? h->h_segptr[q / 16 + 1] - h->h_segptr[q / 16] : n;
+                tgt[q] = 0.5 * tol * (sr[48] * sr[16 + r] + sr[32 + r]) *
+                         std::max(1.0, std::sqrt((double)rows) / 8.0);
             }
         } else {
-            for (int r = 0; r < 16; ++r) tgt[r] = 0.5 * tol * (mx[48] * mx[16 + r] + mx[32 + r]);
+            for (int r = 0; r < 16; ++r)
+                tgt[r] = 0.5 * tol * (mx[48] * mx[16 + r] + mx[32 + r]) * std::max(1.0, std::sqrt((double)n) / 8.0);
         }
         if ((rc = mdot(R, 1, R, hc.data()))) return rc;
         for (int64_t q = 0; q < Q; ++q) {
