@@ -79,3 +79,53 @@ def test_realtime_arrivals_are_respected(monkeypatch):
     srv = _server(monkeypatch, workers=2)
     done = srv.serve(_requests(srv, 10, seed=5, spacing=0.01), realtime=True, timeout=30)
     assert all(r.done >= r.arrival for r in done)
+
+
+class FakeFactor:
+    """Stands in for a mixed factorization: records the kernel choice it is given."""
+
+    def __init__(self):
+        self.choice = None
+        self.tuned = 0
+
+    def autotune(self, reps):
+        self.tuned += 1
+        return {"tc_steps": np.array([1, 0, 1], np.int32), "tc_syrk": np.array([1, 1, 0], np.int32)}
+
+    def set_kernel_choice(self, tc_steps, tc_syrk):
+        self.choice = (np.asarray(tc_steps).copy(), np.asarray(tc_syrk).copy())
+
+
+class FakeMixedBatch(FakeBatch):
+    def __init__(self, pat, mixed, device, tol, maxit):
+        super().__init__(pat, mixed, device, tol, maxit)
+        self.F = FakeFactor()
+        if mixed and pat.choice is not None:
+            self.F.set_kernel_choice(*pat.choice)
+
+
+def test_warm_autotunes_once_and_shares_the_choice(monkeypatch):
+    """Mixed serving: warming two handles of a pattern autotunes the first
+    one only; the pattern keeps the choice and the second handle gets it."""
+    monkeypatch.setattr(serve, "_DeviceBatch", FakeMixedBatch)
+    srv = serve.Server(mixed=True, workers=2)
+    gen, order, batch = PATS["g2d12"]
+    srv.add_pattern("g2d12", gen(0), order=order, batch=batch)
+    srv.warm(["g2d12"], per_pattern=2)
+    pat = srv.patterns["g2d12"]
+    assert len(pat.handles) == 2 and not any(h.busy for h in pat.handles)
+    assert sum(h.F.tuned for h in pat.handles) == 1
+    assert pat.choice is not None
+    tuned = [h for h in pat.handles if h.F.tuned][0]
+    other = [h for h in pat.handles if h is not tuned][0]
+    np.testing.assert_array_equal(other.F.choice[0], pat.choice[0])
+    np.testing.assert_array_equal(other.F.choice[1], pat.choice[1])
+
+
+def test_add_pattern_accepts_a_symbolic_result(monkeypatch):
+    monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
+    srv = serve.Server(mixed=False, workers=1)
+    A = tm.grid_laplacian(10, 10, seed=1)
+    P, S = mf.symbolic(A, alg="mindeg")
+    pat = srv.add_pattern("p", A, symbolic_result=(P, S))
+    assert pat.S is S and pat.P is P
