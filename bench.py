@@ -526,7 +526,7 @@ def run_serving(args, local, world):
 
     rates = [float(x) for x in args.rates.split(",") if x]
     srv = make_server(True, True, 4)
-    srv.warm()
+    srv.warm(per_pattern=2)  # both handles of every pattern exist before the timed streams
     sweep = []
     for rate in rates:
         reqs = stream(args.requests, rate, seed=int(rate))

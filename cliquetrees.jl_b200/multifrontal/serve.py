@@ -56,6 +56,7 @@ class Pattern:
     lo_src: np.ndarray = None  # one entry per stored lower-triangle value
     handles: list = field(default_factory=list)
     est_bytes: int = 0         # device bytes of one handle, once known
+    creating: int = 0          # handles of this pattern being built outside the lock
     choice: tuple = None       # mixed form: per-level tcgen05/FFMA choice found by autotuning
 
 
@@ -70,6 +71,11 @@ class Request:
     X: np.ndarray = None
     eta: float = -1.0
     batch_size: int = 0
+
+
+@dataclass
+class _Ticket:
+    est: int  # bytes reserved for a handle being built
 
 
 class _DeviceBatch:
@@ -154,6 +160,7 @@ class Server:
         self.lock = threading.Lock()
         self.cv = threading.Condition(self.lock)
         self.bytes = 0
+        self.reserved = 0  # bytes of handles being built
 
     # -- patterns ----------------------------------------------------------
     def add_pattern(self, key, A0, order="mindeg", batch=1, ldlt=False, symbolic_result=None):
@@ -177,33 +184,76 @@ class Server:
 
     # -- device handles ----------------------------------------------------
     def _acquire(self, pat: Pattern):
-        """A free handle of `pat`, created under the memory cap; None if none can be had now."""
+        """With the lock held: a free handle of `pat` (marked busy); or, when a
+        new handle may be built under the memory cap, a _Ticket that reserves
+        its slot and bytes (the caller builds it with _create, outside the
+        lock, so that building -- seconds for a large pattern -- never stalls
+        the other workers); or None if neither is possible now."""
         for hd in pat.handles:
             if not hd.busy:
                 hd.busy = True
                 return hd
-        if len(pat.handles) >= 2:  # two handles per pattern: one runs while the next batch fills
+        if len(pat.handles) + pat.creating >= 2:  # two per pattern: one runs while the next batch fills
             return None
         # evict idle handles of other patterns while over the cap (least recently used first)
         est = max([hd.bytes for hd in pat.handles] + [pat.est_bytes])
-        while self.bytes + est > self.mem_cap and self.bytes > 0:
+        if not self._make_room(pat, est):
+            return None
+        pat.creating += 1
+        self.reserved += est
+        return _Ticket(est)
+
+    def _make_room(self, pat, need):
+        """With the lock held: evict idle handles of other patterns until `need`
+        more bytes fit under the cap (or nothing else is resident)."""
+        while self.bytes + self.reserved + need > self.mem_cap and self.bytes + self.reserved > 0:
             idle = [(hd.last_used, p, hd) for p in self.patterns.values() for hd in p.handles
                     if not hd.busy and p is not pat]
             if not idle:
-                return None
+                return False
             _, p, hd = min(idle, key=lambda x: x[0])
             p.handles.remove(hd)
             self.bytes -= hd.bytes
             hd.close()
-        hd = _DeviceBatch(pat, self.mixed, self.device, self.tol, self.maxit)
-        pat.est_bytes = hd.bytes
-        if self.bytes + hd.bytes > self.mem_cap and self.bytes > 0:
+        return True
+
+    def _create(self, pat: Pattern, ticket):
+        """Without the lock: build the handle a ticket reserved and admit it
+        (marked busy); None if the cap turns it away once its true size is
+        known (the caller retries later)."""
+        try:
+            hd = _DeviceBatch(pat, self.mixed, self.device, self.tol, self.maxit)
+        except BaseException:
+            with self.cv:
+                pat.creating -= 1
+                self.reserved -= ticket.est
+                self.cv.notify_all()
+            raise
+        with self.cv:
+            pat.creating -= 1
+            self.reserved -= ticket.est
+            pat.est_bytes = hd.bytes
+            if not self._make_room(pat, hd.bytes):
+                self.cv.notify_all()
+                admit = False
+            else:
+                hd.busy = True
+                pat.handles.append(hd)
+                self.bytes += hd.bytes
+                self.cv.notify_all()
+                admit = True
+        if not admit:
             hd.close()  # the next attempt evicts idle handles first
             return None
-        hd.busy = True
-        pat.handles.append(hd)
-        self.bytes += hd.bytes
         return hd
+
+    def _get(self, pat: Pattern):
+        """A handle of `pat` for single-threaded use (warm-up): free or built now."""
+        with self.cv:
+            got = self._acquire(pat)
+        if isinstance(got, _Ticket):
+            return self._create(pat, got)
+        return got
 
     def warm(self, keys=None, per_pattern=1):
         """Create up to ``per_pattern`` handles per pattern (at most 2) and run
@@ -215,7 +265,7 @@ class Server:
             pat = self.patterns[key]
             got = []
             for _ in range(max(1, min(2, per_pattern))):
-                hd = self._acquire(pat)
+                hd = self._get(pat)
                 if hd is None:
                     break
                 got.append(hd)
@@ -268,11 +318,11 @@ class Server:
                         cands = sorted((q[0].arrival, k) for k, q in waiting.items() if q)
                         job = None
                         for _, k in cands:
-                            hd = self._acquire(self.patterns[k])
-                            if hd is not None:
+                            got = self._acquire(self.patterns[k])
+                            if got is not None:
                                 q = waiting[k]
                                 batch = [q.popleft() for _ in range(min(len(q), self.patterns[k].batch))]
-                                job = (hd, batch)
+                                job = (got, k, batch)
                                 break
                         if job is not None:
                             break
@@ -282,7 +332,19 @@ class Server:
                         if pending and not any(waiting.values()) and realtime:
                             timeout = max(0.0, min(0.01, pending[0].arrival - now()))
                         self.cv.wait(timeout)
-                hd, batch = job
+                got, k, batch = job
+                try:
+                    hd = self._create(self.patterns[k], got) if isinstance(got, _Ticket) else got
+                except Exception as e:  # noqa: BLE001
+                    with self.cv:
+                        errors.append(e)
+                        self.cv.notify_all()
+                    return
+                if hd is None:  # turned away by the cap: back to the front of the queue
+                    with self.cv:
+                        waiting[k].extendleft(reversed(batch))
+                        self.cv.notify_all()
+                    continue
                 try:
                     hd.run(batch)
                 except Exception as e:  # noqa: BLE001

@@ -129,3 +129,47 @@ def test_add_pattern_accepts_a_symbolic_result(monkeypatch):
     P, S = mf.symbolic(A, alg="mindeg")
     pat = srv.add_pattern("p", A, symbolic_result=(P, S))
     assert pat.S is S and pat.P is P
+
+
+class SlowBuildBatch(FakeBatch):
+    """Building a handle of pattern g3d6 takes half a second."""
+
+    def __init__(self, pat, mixed, device, tol, maxit):
+        if pat.key == "g3d6":
+            time.sleep(0.5)
+        super().__init__(pat, mixed, device, tol, maxit)
+
+
+def test_building_a_handle_does_not_stall_other_patterns(monkeypatch):
+    """A new handle is built outside the scheduler lock: while one worker
+    builds the slow pattern's handle, the other worker keeps serving the
+    pattern whose handle already exists."""
+    monkeypatch.setattr(serve, "_DeviceBatch", SlowBuildBatch)
+    srv = serve.Server(mixed=False, workers=2)
+    for k, (gen, order, batch) in PATS.items():
+        srv.add_pattern(k, gen(0), order=order, batch=batch)
+    srv.warm(["g2d12"])
+    A3 = PATS["g3d6"][0](5)
+    reqs = [serve.Request(0, "g3d6", srv.lower_values("g3d6", A3), np.ones((A3.shape[0], 1)), arrival=0.0)]
+    for i in range(1, 13):
+        A = PATS["g2d12"][0](100 + i)
+        reqs.append(serve.Request(i, "g2d12", srv.lower_values("g2d12", A), np.ones((A.shape[0], 1)),
+                                  arrival=1e-6 * i))
+    done = srv.serve(reqs, realtime=False, timeout=30)
+    assert len(done) == 13
+    slow = [r for r in done if r.key == "g3d6"][0]
+    fast_done = max(r.done for r in done if r.key == "g2d12")
+    assert fast_done < slow.done - 0.2, (fast_done, slow.done)
+    assert srv.reserved == 0 and all(p.creating == 0 for p in srv.patterns.values())
+
+
+def test_cap_turns_a_new_handle_away_and_the_batch_is_served_later(monkeypatch):
+    """A handle whose true size does not fit is closed and its requests go back
+    to the queue; they are served once the cap allows."""
+    monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
+    srv = _server(monkeypatch, workers=2)
+    srv.warm(["g2d12"])
+    srv.mem_cap = srv.bytes * 1.2
+    done = srv.serve(_requests(srv, 20, seed=9), realtime=False, timeout=30)
+    assert sorted(r.rid for r in done) == list(range(20))
+    assert srv.reserved == 0 and all(p.creating == 0 for p in srv.patterns.values())
