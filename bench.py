@@ -111,9 +111,9 @@ def workload(args, seed=2):
     if c == 1:
         nrhs = args.nrhs or 1
         A = tm.config1(seed=1)
-        P, S = mf.symbolic(A, alg="mindeg")
+        P, S = mf.symbolic(A, alg="amf")
         B = tm.rhs(A.shape[0], nrhs, seed=5)
-        return Work(A, P, S, B, name=f"2d5pt_100^2_chol_factor+solve_{nrhs}rhs", ordering="minimum degree",
+        return Work(A, P, S, B, name=f"2d5pt_100^2_chol_factor+solve_{nrhs}rhs", ordering="AMF",
                     sample=(A, P, S, B, 1.0, "the full problem"))
     if c == 3:
         import scipy.sparse as sp
@@ -122,7 +122,7 @@ def workload(args, seed=2):
         rng = np.random.default_rng(seed)
         sides = rng.integers(8, 49, size=args.batch)
         mats = [tm.config3_matrix(int(s), seed=1000 + i) for i, s in enumerate(sides)]
-        parts = [mf.symbolic(Ai, alg="mindeg") for Ai in mats]
+        parts = [mf.symbolic(Ai, alg="amf") for Ai in mats]
         P, S, off = batch.block_symbolic(parts)
         A = sp.block_diag(mats, format="csc")
         B = tm.rhs(S.n, nrhs, seed=7)
@@ -130,7 +130,7 @@ def workload(args, seed=2):
         Ps, Ss, offs = batch.block_symbolic(parts[:m])
         As = sp.block_diag(mats[:m], format="csc")
         w = Work(A, P, S, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
-                 segments=off, units=args.batch, ordering="minimum degree",
+                 segments=off, units=args.batch, ordering="AMF",
                  sample=(As, Ps, Ss, tm.rhs(Ss.n, nrhs, seed=7), args.batch / m,
                          f"the first {m} matrices of the batch, scaled by count"))
         w.members = (mats, parts)
@@ -140,14 +140,14 @@ def workload(args, seed=2):
         nrhs = args.nrhs or 8
         m = 16000 * side ** 3 // 64000
         A = tm.config4(side=side, m=m, seed=4)
-        P, S = mf.symbolic(A, alg="mindeg")
+        P, S = mf.symbolic(A, alg="amf")
         B = tm.rhs(A.shape[0], nrhs, seed=9)
         ss = min(side, 20)
         ms = 16000 * ss ** 3 // 64000
         As = tm.config4(side=ss, m=ms, seed=4)
-        Ps, Ss = mf.symbolic(As, alg="mindeg")
+        Ps, Ss = mf.symbolic(As, alg="amf")
         return Work(A, P, S, B, name=f"kkt_{side}^3+{m}_ldlt_factor+solve_{nrhs}rhs", diag=1,
-                    ordering="minimum degree",
+                    ordering="AMF",
                     sample=(As, Ps, Ss, tm.rhs(As.shape[0], nrhs, seed=9), S.factor_flops() / Ss.factor_flops(),
                             f"the same construction with a {ss}^3 grid, scaled by factor flops"))
     raise ValueError("config 5 has its own driver")
@@ -481,8 +481,8 @@ def run_serving(args, local, world):
     from multifrontal import testmatrices as tm
 
     specs = {  # key: (grid, batch per handle, ordering)
-        "2d5pt_64": ((64, 64, 1), 16, "mindeg"), "2d5pt_128": ((128, 128, 1), 8, "mindeg"),
-        "2d5pt_256": ((256, 256, 1), 2, "mindeg"), "2d5pt_512": ((512, 512, 1), 1, "mindeg"),
+        "2d5pt_64": ((64, 64, 1), 16, "amf"), "2d5pt_128": ((128, 128, 1), 8, "amf"),
+        "2d5pt_256": ((256, 256, 1), 2, "amf"), "2d5pt_512": ((512, 512, 1), 1, "amf"),
         "3d7pt_16": ((16, 16, 16), 16, "nd"), "3d7pt_48": ((48, 48, 48), 1, "nd"),
     }
     pools = {}   # per pattern: 4 seeded coefficient sets (log-uniform [0.1, 10], diag + 1e-2)
@@ -499,7 +499,7 @@ def run_serving(args, local, world):
     def make_server(mixed, batched, workers):
         srv = serve.Server(mixed=mixed, device=local, workers=workers)
         for k, ((nx, ny, nz), b, o) in specs.items():
-            order = mf.grid_nd_order(nx, ny, nz) if o == "nd" else "mindeg"
+            order = mf.grid_nd_order(nx, ny, nz) if o == "nd" else "amf"
             srv.add_pattern(k, mats[k][0], order=order, batch=b if batched else 1)
             if k not in pools:
                 pools[k] = [srv.lower_values(k, A) for A in mats[k]]

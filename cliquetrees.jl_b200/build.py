@@ -35,11 +35,14 @@ def _stale(target, sources):
 
 
 def build_sym(verbose=False, force=False):
-    src = [os.path.join(CSRC, "symbolic.cpp"), os.path.join(CSRC, "mindeg.cpp")]
+    src = [os.path.join(CSRC, "symbolic.cpp"), os.path.join(CSRC, "mindeg.cpp"), os.path.join(CSRC, "amf.cpp")]
     hdr = [os.path.join(HERE, "..", "include", "cliquetrees_symbolic.h")]
     target = os.path.join(OUT, "libctsym.so")
     if force or _stale(target, src + hdr):
-        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-o", target] + src, verbose)
+        # -ffp-contract=off: the AMF fill score must round exactly as the reference's
+        # separate multiply and subtract do
+        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-Wall", "-o", target] + src,
+             verbose)
     return target
 
 

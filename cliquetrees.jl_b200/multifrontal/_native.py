@@ -52,6 +52,8 @@ def symlib() -> ctypes.CDLL:
         lib.ct_grid_nd_order.restype = ctypes.c_int
         lib.ct_mindeg_order.argtypes = [_i64, _p64, _p64, _p64]
         lib.ct_mindeg_order.restype = ctypes.c_int
+        lib.ct_amf_order.argtypes = [_i64, _p64, _p64, _p64]
+        lib.ct_amf_order.restype = ctypes.c_int
         lib.ct_last_error.argtypes = []
         lib.ct_last_error.restype = ctypes.c_char_p
         _sym = lib

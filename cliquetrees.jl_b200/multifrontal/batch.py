@@ -83,7 +83,7 @@ class BatchedFactorization:
     ``mixed=True``: FP32 fronts + FP64 refinement to per-matrix backward
     error ``tol``."""
 
-    def __init__(self, mats, orders="mindeg", *, ldlt=False, mixed=False, tol=1e-12, maxit=100, device=0,
+    def __init__(self, mats, orders="amf", *, ldlt=False, mixed=False, tol=1e-12, maxit=100, device=0,
                  nrhs_cap=16, symbolics=None):
         self.m = len(mats)
         if symbolics is None:

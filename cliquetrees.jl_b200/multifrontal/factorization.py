@@ -76,7 +76,7 @@ class ChordalFactorization:
 
     DIAG = 0
 
-    def __init__(self, A, P: Permutation | None = None, S: ChordalSymbolic | None = None, *, alg="mindeg",
+    def __init__(self, A, P: Permutation | None = None, S: ChordalSymbolic | None = None, *, alg="amf",
                  device: int = 0, nrhs_cap: int = 16, mixed: bool = False, tol: float = 1e-12, maxit: int = 100):
         """``mixed=True`` selects the mixed-precision form: FP32 fronts on the
         GPU, FP64 refinement in ``ldiv`` to backward error ``tol`` (the

@@ -163,7 +163,7 @@ class Server:
         self.reserved = 0  # bytes of handles being built
 
     # -- patterns ----------------------------------------------------------
-    def add_pattern(self, key, A0, order="mindeg", batch=1, ldlt=False, symbolic_result=None):
+    def add_pattern(self, key, A0, order="amf", batch=1, ldlt=False, symbolic_result=None):
         """Symbolic analysis of a pattern, once (cached by key); an analysis
         already at hand is passed as ``symbolic_result=(P, S)``."""
         if key in self.patterns:

@@ -160,27 +160,35 @@ def mindeg_order(pattern) -> np.ndarray:
 
 
 def amf_order(pattern) -> np.ndarray:
-    """The reference's default ordering is AMF (AMFLib.amf,
-    src/AMFLib.jl:56-91, approximate minimum fill); it is not restated in
-    this package, so this raises.  ``mindeg_order`` is the general-purpose
-    substitute."""
-    raise NotImplementedError("AMF is not restated in this package; use alg='mindeg' (minimum degree)")
+    """Approximate-minimum-fill order: the reference's default ``AMF()``
+    (``AMFLib.amf`` on the simple graph of A, src/elimination_algorithms.jl:1556-1559,
+    src/AMFLib.jl/src/AMFLib.jl:56-155 and hamf_impl! :703-1525), computed by
+    ``libctsym``.  The adjacency lists are the columns of the symmetric
+    pattern with rows ascending, as the reference reads a SparseMatrixCSC."""
+    pattern = as_pattern(pattern)
+    lib = _native.symlib()
+    order = np.empty(pattern.n, np.int64)
+    rc = lib.ct_amf_order(pattern.n, _native.ptr64(pattern.colptr), _native.ptr64(pattern.rowval),
+                          _native.ptr64(order))
+    if rc != 0:
+        raise RuntimeError(lib.ct_last_error().decode())
+    return order
 
 
-def symbolic(A, alg="mindeg"):
+def symbolic(A, alg="amf"):
     """``symbolic(A; alg)`` (chordal_symbolic.jl:68-91) -> (Permutation, ChordalSymbolic).
 
-    ``alg`` is "mindeg" (minimum degree; stands in for the reference default
-    AMF, elimination_algorithms.jl:2380), "natural", or an explicit order
-    vector (0-based; order[i] = vertex eliminated i-th), as
+    ``alg`` is "amf" (the reference default ``AMF()``, elimination_algorithms.jl:2380),
+    "mindeg" (minimum degree, an extra option), "natural", or an explicit
+    order vector (0-based; order[i] = vertex eliminated i-th), as
     `permutation(weights, graph, order)` accepts (elimination_algorithms.jl:776-779)."""
     pat = as_pattern(A)
     n = pat.n
     if isinstance(alg, str):
-        if alg == "mindeg":
-            order = mindeg_order(pat)
-        elif alg == "amf":
+        if alg == "amf":
             order = amf_order(pat)
+        elif alg == "mindeg":
+            order = mindeg_order(pat)
         elif alg == "natural":
             order = np.arange(n, dtype=np.int64)
         else:

@@ -54,12 +54,20 @@ int ct_symbolic_arrays(const ct_symbolic* S, int64_t* order, int64_t* invp, int6
  * explicit permutation (src/elimination_algorithms.jl:776-779). */
 int ct_grid_nd_order(int64_t nx, int64_t ny, int64_t nz, int64_t leaf, int64_t* order);
 
+/* Approximate-minimum-fill elimination order of the symmetric pattern
+ * (colptr, rowval) (both triangles, rows of each column in stored order;
+ * self loops ignored): the reference's default ordering AMF(), i.e.
+ * AMFLib.amf(weights, graph) (src/elimination_algorithms.jl:1556-1559 ->
+ * src/AMFLib.jl/src/AMFLib.jl:56-155, hamf_impl! :703-1525) with unit
+ * weights, restated step by step so that the order is identical.
+ * order[k] = vertex eliminated k-th (0-based). */
+int ct_amf_order(int64_t n, const int64_t* colptr, const int64_t* rowval, int64_t* order);
+
 /* Minimum-degree elimination order of the symmetric pattern (colptr,
  * rowval) (either or both triangles; self loops ignored): quotient graph
  * with approximate external degrees and element absorption (Amestoy, Davis
- * & Duff 1996).  The general-purpose ordering of this package; it stands in
- * for the reference's default AMF (src/AMFLib.jl:56-91), which minimises
- * approximate fill instead of degree and is not restated here. */
+ * & Duff 1996).  An optional ordering; the reference's default is AMF
+ * (ct_amf_order). */
 int ct_mindeg_order(int64_t n, const int64_t* colptr, const int64_t* rowval, int64_t* order);
 
 const char* ct_last_error(void);

@@ -8,6 +8,10 @@ Sources (paths relative to the reference root):
                                   LDLt example (A, unit L, D, F \\ b, signs=)
   src/AMFLib.jl/README.md         AMF order of the 8-vertex graph
   README.md                       clique tree of the 8-vertex graph (alg=MF())
+  test/core.jl                    the 17-vertex graph of Vandenberghe & Andersen
+                                  (Figure 4.3) and its clique tree under the order
+                                  1:17 with Maximal supernodes (Figure 4.7 left):
+                                  parent indices, residuals and separators
 
 The factor displays are in elimination order (P A P^T = L L^T).
 """
@@ -18,7 +22,6 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
 
 
@@ -45,7 +48,42 @@ def _matrix_literal(lines, i):
     return rows, j + 1
 
 
+def _core_maximal(core):
+    """The 17-vertex graph and its Maximal clique tree from test/core.jl."""
+    i = next(k for k, l in enumerate(core) if l.strip().startswith("_graph = BipartiteGraph("))
+    j = next(k for k in range(i, len(core)) if core[k].strip() == "[")
+    G = []
+    j += 1
+    while core[j].strip() != "],":
+        G.append([int(t) for t in core[j].split()])
+        j += 1
+    i = next(k for k in range(j, len(core)) if "cliquetree(graph; alg = 1:17, snd = Maximal())" in core[k])
+    i = next(k for k in range(i, len(core)) if "map(i -> parentindex(tree, i), 1:8)" in core[k])
+    par = re.search(r"\[(.*)\]", core[i + 1]).group(1)
+    parent = [None if t.strip() == "nothing" else int(t) for t in par.split(",")]
+
+    def label_lists(start_marker):
+        k = next(q for q in range(i, len(core)) if start_marker in core[q])
+        lists = []
+        k += 1
+        while len(lists) < 8:
+            m = re.search(r"\[([\d, ]*)\]", core[k])
+            if m:
+                body = m.group(1).strip()
+                lists.append([int(t) for t in body.split(",")] if body else [])
+            k += 1
+        return lists
+
+    res = label_lists("map(i -> view(label, residual(tree, i)), 1:8)")
+    sep = label_lists("map(i -> view(label, separator(tree, i)), 1:8)")
+    return {"graph": G, "order": list(range(1, 18)), "parent": parent, "residual_labels": res,
+            "separator_labels": sep}
+
+
 def main():
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_known_answers.py <path of a CliqueTrees.jl checkout>")
+    REF = sys.argv[1]
     mf = open(os.path.join(REF, "src/Multifrontal.jl/README.md")).read().splitlines()
     out = {"source": "AlgebraicJulia/CliqueTrees.jl READMEs (see make_known_answers.py)"}
     # --- Cholesky example
@@ -110,6 +148,9 @@ def main():
         nodes.append({"bag": bag, "parent": parent})
         stack.append(bag)
     out["cliquetree_mf"] = nodes
+    # --- the 17-vertex graph and its Maximal clique tree (order 1:17)
+    core = open(os.path.join(REF, "test/core.jl")).read().splitlines()
+    out["maximal17"] = _core_maximal(core)
     json.dump(out, open(OUT, "w"), indent=1)
     print("wrote", OUT)
 

@@ -82,7 +82,7 @@ def test_batched_mixed_ldlt_segments_meet_tolerance():
     refinement runs one GMRES per (matrix, column), so every matrix reaches
     the 1e-12 bar on its own and agrees with its solution alone."""
     mats = [tm.config4(side=s, m=max(8, s ** 3 // 4), seed=20 + i) for i, s in enumerate((5, 6, 7, 6, 5))]
-    orders = ["mindeg"] * len(mats)
+    orders = ["amf"] * len(mats)
     B = batch.BatchedFactorization(mats, orders, ldlt=True, mixed=True)
     B.factorize()
     rhs = [tm.rhs(A.shape[0], 2, seed=70 + i) for i, A in enumerate(mats)]
@@ -93,7 +93,7 @@ def test_batched_mixed_ldlt_segments_meet_tolerance():
         assert eta <= 1e-12, (i, eta)
         assert abs(seg[i] - eta) <= 1e-3 * eta + 1e-16
     for i in (0, 3):
-        P, S = mf.symbolic(mats[i], alg="mindeg")
+        P, S = mf.symbolic(mats[i], alg="amf")
         F = mf.ldlt_(mf.ChordalLDLt(mats[i], P, S, mixed=True))
         Xa = mf.ldiv(F, rhs[i])
         assert tm.backward_error(mats[i], Xa, rhs[i]).max() <= 1e-12

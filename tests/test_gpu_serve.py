@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 
 def _patterns():
     return {
-        "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "mindeg", 4),
-        "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "mindeg", 4),
+        "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "amf", 4),
+        "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "amf", 4),
         "g3d6": (lambda s: tm.grid_laplacian(6, 6, 6, seed=s), mf.grid_nd_order(6, 6, 6), 2),
     }
 

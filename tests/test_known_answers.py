@@ -12,9 +12,9 @@ from oracle import oracle
 
 KA = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
 
-# elimination orders (0-based) under which the symbolic restatement yields
-# the reference's displayed factor / tree; the displays fix the final order
-CHOL_ORDER = np.array([3, 1, 4, 2, 5]) - 1
+# elimination order (0-based) under which the symbolic restatement yields
+# the README's clique tree for alg=MF() (MF is not restated; the display
+# fixes the final order)
 TREE_ORDER = np.array([1, 4, 2, 5, 8, 3, 6, 7]) - 1
 
 
@@ -31,10 +31,41 @@ def dense_factor(S, Dval, Lval):
     return L
 
 
+def test_amf_known_order():
+    """AMFLib README: amf(8, graph.colptr, graph.rowval) -> perm (src/AMFLib.jl/README.md)."""
+    G = np.array(KA["amf"]["graph"], float)
+    assert list(mf.amf_order(G) + 1) == KA["amf"]["perm"]
+
+
+def test_default_ordering_is_amf():
+    """symbolic(A) orders with AMF() by default (elimination_algorithms.jl:2380);
+    supernode relabelling keeps this order for the 8-vertex graph."""
+    G = np.array(KA["amf"]["graph"], float)
+    P, S = mf.symbolic(G)
+    assert list(P.perm + 1) == KA["amf"]["perm"]
+    # every bag of the clique tree is a clique of the filled graph in
+    # elimination order: residual columns contiguous, separators after them
+    for j in range(S.nfr):
+        assert np.all(S.sep(j) >= S.resptr[j + 1])
+
+
+def test_maximal_clique_tree_of_the_17_vertex_graph():
+    """test/core.jl "vandenberghe and andersen", snd = Maximal() (Figure 4.7
+    left): parent indices, residuals and separators under the order 1:17."""
+    K = KA["maximal17"]
+    G = np.array(K["graph"], float)
+    P, S = mf.symbolic(G, alg=np.array(K["order"]) - 1)
+    assert S.nfr == len(K["parent"])
+    assert [None if p < 0 else int(p) + 1 for p in S.pnt] == K["parent"]
+    assert [list(map(int, P.perm[S.res(j)] + 1)) for j in range(S.nfr)] == K["residual_labels"]
+    assert [list(map(int, P.perm[S.sep(j)] + 1)) for j in range(S.nfr)] == K["separator_labels"]
+
+
 def test_cholesky_known_factor_and_solve():
+    """README: cholesky!(ChordalCholesky(A)) with the default ordering (AMF)."""
     ka = KA["cholesky"]
     A = np.array(ka["A"])
-    P, S = mf.symbolic(A, alg=CHOL_ORDER)
+    P, S = mf.symbolic(A)
     assert list(P.perm + 1) == [3, 1, 2, 4, 5]
     Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
     info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0)
@@ -49,7 +80,7 @@ def test_cholesky_known_factor_and_solve():
 def test_ldlt_known_factor_and_solve(use_signs):
     ka = KA["ldlt"]
     A = np.array(ka["A"])
-    P, S = mf.symbolic(A, alg=CHOL_ORDER)
+    P, S = mf.symbolic(A)
     Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
     signs = np.array(ka["signs"])[P.perm] if use_signs else None
     info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 1, signs=signs)
@@ -80,7 +111,7 @@ def test_failure_info_is_first_bad_pivot_in_original_order():
     # make the 5x5 example indefinite at original vertex 4
     A = np.array(KA["cholesky"]["A"])
     A[3, 3] = -1.0
-    P, S = mf.symbolic(A, alg=CHOL_ORDER)
+    P, S = mf.symbolic(A)
     Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
     info, *_ = oracle.chol_impl(S, Dval, Lval, 0)
     assert info > 0

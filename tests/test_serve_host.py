@@ -30,8 +30,8 @@ class FakeBatch:
 
 
 PATS = {
-    "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "mindeg", 4),
-    "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "mindeg", 4),
+    "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "amf", 4),
+    "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "amf", 4),
     "g3d6": (lambda s: tm.grid_laplacian(6, 6, 6, seed=s), "natural", 2),
 }
 
@@ -126,7 +126,7 @@ def test_add_pattern_accepts_a_symbolic_result(monkeypatch):
     monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
     srv = serve.Server(mixed=False, workers=1)
     A = tm.grid_laplacian(10, 10, seed=1)
-    P, S = mf.symbolic(A, alg="mindeg")
+    P, S = mf.symbolic(A, alg="amf")
     pat = srv.add_pattern("p", A, symbolic_result=(P, S))
     assert pat.S is S and pat.P is P
 
