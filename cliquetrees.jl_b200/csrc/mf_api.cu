@@ -605,6 +605,7 @@ int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* us
     double* keep = h->d_signs;
     h->d_signs = const_cast<double*>(ds);
     int64_t inf = 0;
+    h->fp64_current = false;  // whatever the FP64 storage holds is an older matrix
     rc = launch_assemble_mixed(h, h->cur_nz);
     if (!rc) rc = init_info(h);
     if (!rc) rc = launch_factor_mixed(h);
@@ -791,7 +792,8 @@ int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
             if (segptr[s + 1] < segptr[s]) { set_error("mf_set_segments: boundaries must not decrease"); return -1; }
     }
     DeviceGuard g(h->device);
-    MF_CUDA(cudaDeviceSynchronize());
+    // only this handle's work can use the buffers replaced below
+    MF_CUDA(cudaStreamSynchronize(h->stream));
     release_graphs(h);
     for (void* p : {(void*)h->d_segptr, (void*)h->d_segred, (void*)h->d_segeta, (void*)h->d_chunkrow,
                     (void*)h->d_chunkseg, (void*)h->d_segchunk, (void*)h->d_rowseg, (void*)h->d_chunkred,

@@ -891,6 +891,11 @@ int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
         set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
         return -1;
     }
+    if (h->mixed && !h->fp64_current) {
+        set_error("the FP64 factor storage does not hold the current matrix: the last mixed factorization "
+                  "stayed in FP32");
+        return -1;
+    }
     Timer t(h, K_OTHER);
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
@@ -1075,9 +1080,11 @@ int launch_factor(mf_handle* h) {
         return -1;
     }
     FactorBufs<double> fb{h->d_P, h->d_M, h->d_inv, h->d_d, h->d_inv2};
-    return run_captured(h, 1, (int64_t)(uintptr_t)h->d_signs, 0, 0, [&]() {
+    int rc = run_captured(h, 1, (int64_t)(uintptr_t)h->d_signs, 0, 0, [&]() {
         return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
     });
+    h->fp64_current = rc == 0;
+    return rc;
 }
 
 int launch_factor_mixed(mf_handle* h) {

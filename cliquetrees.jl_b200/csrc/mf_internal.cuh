@@ -266,6 +266,10 @@ struct mf_handle {
     double* d_red = nullptr;       // reductions and scalars (see mf_refine.cu)
     const double* cur_nz = nullptr; // values of the current matrix (device)
     bool mixed_fallback = false;   // FP32 factorization failed; the FP64 factor is used
+    // the FP64 factor storage holds the factor of the current values: set by
+    // every completed FP64 factorization, cleared when a mixed factorization
+    // stays in FP32 (its FP64 storage then still holds an older matrix)
+    bool fp64_current = false;
     // independent row segments (a batch of matrices factored as one forest):
     // the refinement measures the backward error of every segment separately
     int64_t nseg = 0;

@@ -877,6 +877,11 @@ int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* 
         set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
         return -1;
     }
+    if (h->mixed && !h->fp64_current) {
+        set_error("the FP64 factor storage does not hold the current matrix: the last mixed factorization "
+                  "stayed in FP32; use the refined solve");
+        return -1;
+    }
     if (nrhs > kMaxRhs) { set_error("launch_solve_with: nrhs chunk above 16"); return -1; }
     SolveBufs<double> sb{h->d_P, h->d_inv, h->d_d, R, W, C, part, h->d_inv2};
     return h->diag ? solve_impl<double, 1>(h, sb, (int)nrhs) : solve_impl<double, 0>(h, sb, (int)nrhs);
@@ -885,6 +890,11 @@ int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
     if (!have_fp64(h)) {
         set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
+        return -1;
+    }
+    if (h->mixed && !h->fp64_current) {
+        set_error("the FP64 factor storage does not hold the current matrix: the last mixed factorization "
+                  "stayed in FP32; use the refined solve");
         return -1;
     }
     if (nrhs > kMaxRhs) { set_error("launch_solve: nrhs chunk above 16"); return -1; }

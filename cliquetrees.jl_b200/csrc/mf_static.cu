@@ -16,36 +16,27 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
-#include <mutex>
 
 #include "mf_internal.cuh"
 
 namespace mf {
 
 constexpr int64_t kStaticSolveDoubles = int64_t(1) << 22;  // 32 MiB
-constexpr int kStaticMaxDevices = 64;
 constexpr int64_t kChunkRhs = 16;  // right-hand sides per solve pass (the solve kernels' limit)
 
 static __device__ __align__(256) double g_solve_region[kStaticSolveDoubles];
 
-static std::mutex g_region_mu;
-static double* g_region_addr[kStaticMaxDevices] = {};
-
-// Address of the region on `device`, which the caller has made current.  The
-// first query on a device loads the module and is the setup step.
-static int region_address(int device, double** out) {
-    if (device < 0 || device >= kStaticMaxDevices) {
-        set_error("mf_solve_device_static: device index out of range");
-        return -1;
-    }
-    std::lock_guard<std::mutex> lk(g_region_mu);
-    if (!g_region_addr[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_solve_region);
-        if (e != cudaSuccess) return cuda_fail(e, "mf_solve_device_static: cudaGetSymbolAddress");
-        g_region_addr[device] = static_cast<double*>(p);
-    }
-    *out = g_region_addr[device];
+// Address of the region on the current device (the caller has made the
+// handle's device current).  The lookup runs on every call rather than being
+// cached, so a module reloaded after a device reset or in a new primary
+// context is found at its new address; the first lookup on a device loads the
+// module holding the region, which is why the first call should not run
+// under stream capture.
+static int region_address(double** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_solve_region);
+    if (e != cudaSuccess) return cuda_fail(e, "mf_solve_device_static: cudaGetSymbolAddress");
+    *out = static_cast<double*>(p);
     return 0;
 }
 
@@ -92,7 +83,7 @@ extern "C" int mf_solve_device_static(mf_handle* h, double* B_dev, int64_t nrhs,
     }
     CurrentDevice g(h->device);
     double* base = nullptr;
-    int rc = region_address(h->device, &base);
+    int rc = region_address(&base);
     if (rc) return rc;
     double* C = base;
     double* W = C + szC;

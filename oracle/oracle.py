@@ -2,8 +2,10 @@
 
 Python driver around ``mf_oracle.c`` (a C restatement of CliqueTrees.jl's
 chol_impl!/div_impl!, see the header of that file for the line-by-line
-citations).  Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline
-leg of ``bench.py`` may import this module; the product never does.
+citations) and ``sym_oracle.c`` (the reference's symbolic analysis: AMF and
+the chain to a ChordalSymbolic).  Only tests, ``__graft_entry__.smoke()``
+and the CPU legs of ``bench.py`` may import this module; the product never
+does, and this module imports nothing from the product.
 
 Parity status: the reference is Julia and cannot run in this environment,
 so the restatement is pinned by the in-repository known answers (the 5x5
@@ -23,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libmforacle.so")
 SRC = os.path.join(HERE, "mf_oracle.c")
+SYM_SRC = os.path.join(HERE, "sym_oracle.c")
 
 _i64 = ctypes.c_int64
 _p64 = ctypes.POINTER(ctypes.c_int64)
@@ -30,9 +33,11 @@ _pd = ctypes.POINTER(ctypes.c_double)
 
 
 def build(force: bool = False) -> str:
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(SRC):
-        subprocess.run(["gcc", "-O3", "-march=x86-64-v3", "-fPIC", "-shared", "-o", LIB, SRC, "-ldl", "-lm"],
-                       check=True)
+    stale = not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(SRC), os.path.getmtime(SYM_SRC))
+    if force or stale:
+        # -ffp-contract=off: the AMF fill score rounds as separate multiply and subtract
+        subprocess.run(["gcc", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared", "-o", LIB, SRC,
+                        SYM_SRC, "-ldl", "-lm"], check=True)
     return LIB
 
 
@@ -60,6 +65,13 @@ def lib(nthreads: int = 1):
         L.mfo_div_impl.argtypes = [_i64, _i64] + [_p64] * 7 + [_i64, _i64, _i64, ctypes.c_int, _pd, _pd, _pd, _pd,
                                                                _i64, _i64, ctypes.c_int]
         L.mfo_div_impl.restype = ctypes.c_int
+        L.mfo_amf_order.argtypes = [_i64, _p64, _p64, _p64]
+        L.mfo_amf_order.restype = ctypes.c_int
+        L.mfo_symbolic_create.argtypes = [_i64, _p64, _p64, _p64]
+        L.mfo_symbolic_create.restype = ctypes.c_void_p
+        L.mfo_symbolic_free.argtypes = [ctypes.c_void_p]
+        L.mfo_symbolic_sizes.argtypes = [ctypes.c_void_p, _p64]
+        L.mfo_symbolic_arrays.argtypes = [ctypes.c_void_p] + [_p64] * 11
         rc = L.mfo_init(openblas_path().encode(), nthreads)
         if rc != 0:
             raise RuntimeError(f"mfo_init failed ({rc})")
@@ -115,13 +127,133 @@ def div_impl(S, Dval, Lval, d, diag: int, C, vec: bool = False):
     return C
 
 
+class OracleSymbolic:
+    """The fields of a ChordalSymbolic (chordal_symbolic.jl:15-28), 0-based,
+    as the oracle's own symbolic analysis computes them."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def ndz(self):
+        return int(self.Dptr[-1])
+
+    @property
+    def nlz(self):
+        return int(self.Lptr[-1])
+
+    def res(self, j):
+        return np.arange(self.resptr[j], self.resptr[j + 1], dtype=np.int64)
+
+    def sep(self, j):
+        return self.septgt[self.sepptr[j]:self.sepptr[j + 1]]
+
+    def factor_flops(self):
+        nn = np.diff(self.resptr).astype(np.float64)
+        na = np.diff(self.sepptr).astype(np.float64)
+        return float(np.sum(nn ** 3 / 3.0 + nn * nn * na + nn * na * na))
+
+
+class OraclePermutation:
+    def __init__(self, perm):
+        self.perm = np.ascontiguousarray(perm, dtype=np.int64)
+        self.invp = np.empty_like(self.perm)
+        self.invp[self.perm] = np.arange(self.perm.size, dtype=np.int64)
+
+
+def _csc(A):
+    import scipy.sparse as sp
+    C = sp.csc_matrix(A if sp.issparse(A) else np.asarray(A, dtype=np.float64))
+    C.sum_duplicates()
+    C.sort_indices()
+    return C
+
+
+def pattern(A):
+    """(colptr, rowval) of the symmetric pattern of A, rows ascending (the
+    adjacency lists the reference reads from a SparseMatrixCSC)."""
+    C = _csc(A)
+    C.data = np.ones_like(C.data)
+    P = (C + C.T).tocsc()
+    P.sort_indices()
+    return P.indptr.astype(np.int64), P.indices.astype(np.int64)
+
+
+def amf_order(A):
+    """The reference's default AMF() order (order[k] = vertex eliminated k-th)."""
+    colptr, rowval = pattern(A)
+    n = colptr.size - 1
+    order = np.empty(n, np.int64)
+    rc = lib().mfo_amf_order(n, _p(colptr), _p(rowval), _p(order))
+    if rc != 0:
+        raise RuntimeError(f"mfo_amf_order failed ({rc})")
+    return order
+
+
+def symbolic(A, alg="amf"):
+    """(permutation, symbolic factorization) of A under AMF ("amf") or an
+    explicit order vector, with Maximal supernodes (symbolic(A; alg),
+    chordal_symbolic.jl:68-91)."""
+    colptr, rowval = pattern(A)
+    n = colptr.size - 1
+    order = amf_order(A) if isinstance(alg, str) and alg == "amf" else np.ascontiguousarray(alg, dtype=np.int64)
+    L = lib()
+    h = L.mfo_symbolic_create(n, _p(colptr), _p(rowval), _p(order))
+    if not h:
+        raise RuntimeError("mfo_symbolic_create failed")
+    try:
+        sz = np.zeros(7, np.int64)
+        L.mfo_symbolic_sizes(h, _p(sz))
+        nfr, nsep = int(sz[1]), int(sz[2])
+        a = {k: np.empty(m, np.int64) for k, m in
+             [("perm", n), ("resptr", nfr + 1), ("sepptr", nfr + 1), ("septgt", nsep), ("reltgt", nsep),
+              ("pnt", nfr), ("chdptr", nfr + 2), ("chdtgt", nfr), ("idx", n), ("Dptr", nfr + 1), ("Lptr", nfr + 1)]}
+        L.mfo_symbolic_arrays(h, *[_p(a[k]) for k in ["perm", "resptr", "sepptr", "septgt", "reltgt", "pnt",
+                                                       "chdptr", "chdtgt", "idx", "Dptr", "Lptr"]])
+    finally:
+        L.mfo_symbolic_free(h)
+    perm = a.pop("perm")
+    S = OracleSymbolic(n=n, nfr=nfr, nMptr=int(sz[3]), nMval=int(sz[4]), nNval=int(sz[5]), nFval=int(sz[6]), **a)
+    return OraclePermutation(perm), S
+
+
+def lower_values(A):
+    """Stored entries of the lower triangle of symmetric A, column by column,
+    rows ascending (the values Hermitian(A, :L) holds)."""
+    import scipy.sparse as sp
+    return sp.tril(_csc(A), format="csc")
+
+
 def assemble(S, invp, A):
-    """Dval/Lval holding the permuted lower triangle of A (copyto!,
-    chordal_triangular.jl:852-893) plus the flat slot map."""
-    import sys
-    sys.path.insert(0, os.path.join(HERE, "..", "cliquetrees.jl_b200"))
-    from multifrontal.sparse import assembly_map
-    Lo, slot = assembly_map(S, invp, A)
+    """Dval/Lval holding the permuted lower triangle of A: copyto!(F, A) =
+    sympermute (utils.jl:147-219) + copyto!(::ChordalTriangular, ...)
+    (chordal_triangular.jl:852-893).  Returns (Dval, Lval, lower triangle of
+    A, slot) with slot[k] the flat [Dval; Lval] index of its k-th entry."""
+    Lo = lower_values(A)
+    Lo.sort_indices()
+    n = Lo.shape[0]
+    cols = np.repeat(np.arange(n, dtype=np.int64), np.diff(Lo.indptr))
+    rows = Lo.indices.astype(np.int64)
+    pi, pj = invp[rows], invp[cols]
+    r = np.maximum(pi, pj)
+    c = np.minimum(pi, pj)
+    f = S.idx[c]
+    r0 = S.resptr[f]
+    r1 = S.resptr[f + 1]
+    nn = r1 - r0
+    na = S.sepptr[f + 1] - S.sepptr[f]
+    slot = np.empty(r.size, np.int64)
+    inD = r < r1
+    slot[inD] = S.Dptr[f[inD]] + (r[inD] - r0[inD]) + (c[inD] - r0[inD]) * nn[inD]
+    off = ~inD
+    if np.any(off):
+        big = np.int64(n + 1)
+        keys = np.repeat(np.arange(S.nfr, dtype=np.int64), np.diff(S.sepptr)) * big + S.septgt
+        want = f[off] * big + r[off]
+        loc = np.searchsorted(keys, want)
+        if np.any(loc >= keys.size) or np.any(keys[np.minimum(loc, keys.size - 1)] != want):
+            raise ValueError("matrix entry outside the symbolic pattern")
+        slot[off] = S.ndz + S.Lptr[f[off]] + (loc - S.sepptr[f[off]]) + (c[off] - r0[off]) * na[off]
     flat = np.zeros(S.ndz + S.nlz, np.float64)
     flat[slot] = Lo.data
     return flat[:S.ndz].copy(), flat[S.ndz:].copy(), Lo, slot

@@ -137,3 +137,47 @@ def test_autotune_keeps_refined_accuracy():
     with pytest.raises(ValueError):
         F.set_kernel_choice(np.zeros(nl + 1, np.int32))
     F.close()
+
+
+def _fp32_breakdown_matrix():
+    """A 12x12 grid matrix, SPD in FP64, whose FP32 factorization meets a zero
+    pivot: unit diagonal, off-diagonals 1e-12 except one edge at 1 - 1e-10,
+    which rounds to 1 in single precision (the Schur complement 2e-10 of
+    that pair vanishes)."""
+    A = tm.grid_laplacian(12, 12, seed=1).tocoo()
+    vals = np.where(A.row == A.col, 1.0, -1e-12)
+    u, v = 40, 41  # neighbours on the grid
+    vals[((A.row == u) & (A.col == v)) | ((A.row == v) & (A.col == u))] = -(1.0 - 1e-10)
+    return sp.csc_matrix((vals, (A.row, A.col)), shape=A.shape)
+
+
+def test_fp64_solves_refuse_a_stale_fp64_factor():
+    """After an FP64 fallback the FP64 factor storage stays allocated; a later
+    mixed factorization that stays in FP32 leaves it holding the old matrix,
+    so the FP64 solves and the FP64 factor download must refuse it."""
+    import ctypes
+    A1 = _fp32_breakdown_matrix()
+    A2 = tm.grid_laplacian(12, 12, seed=2)
+    P, S = mf.symbolic(A1)
+    F = mf.ChordalCholesky(A1, P, S, mixed=True)
+    mf.cholesky_(F)
+    assert F.used_fp64 and F.info == 0
+    B = tm.rhs(S.n, 2, seed=3)
+    X1 = mf.ldiv(F, B)
+    assert tm.backward_error(A1, X1, B).max() <= 1e-12
+    lib, h = F._handle.lib, F._handle.h
+    Xp = np.asfortranarray(B.copy())
+    assert lib.mf_solve(h, Xp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2, S.n,
+                        P.perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))) == 0  # FP64 factor is A1's
+    F.copyto(A2)
+    mf.cholesky_(F)
+    assert not F.used_fp64
+    X2 = mf.ldiv(F, B)
+    assert tm.backward_error(A2, X2, B).max() <= 1e-12
+    Xp = np.asfortranarray(B.copy())
+    rc = lib.mf_solve(h, Xp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2, S.n,
+                      P.perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    assert rc == -1 and b"does not hold the current matrix" in lib.mf_last_error()
+    with pytest.raises(RuntimeError):
+        F.factor_arrays()
+    F.close()

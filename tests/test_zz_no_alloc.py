@@ -53,8 +53,13 @@ def test_static_region_solve_matches_device_solve(k, pad):
     assert lib.mf_synchronize(h) == 0
     want = ref[:, :n].cpu().numpy().T
 
-    # two calls in a row through the one region
+    # two calls in a row through the one region, each after a solve of other
+    # right-hand sides (16 columns) has left different data everywhere in it
+    other = _device_block(torch, tm.rhs(n, 16, seed=77), n)
     for _ in range(2):
+        torch.cuda.synchronize()
+        assert lib.mf_solve_device_static(h, other.data_ptr(), 16, n, perm.data_ptr()) == 0, lib.mf_last_error()
+        assert lib.mf_synchronize(h) == 0
         X = _device_block(torch, B, ldb)
         torch.cuda.synchronize()
         rc = lib.mf_solve_device_static(h, X.data_ptr(), k, ldb, perm.data_ptr())
