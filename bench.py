@@ -55,7 +55,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "cliquetrees.jl_b200"))
 
 KERNEL_NAMES = ["assemble", "small", "extend_add", "panel", "update", "syrk", "solve_small", "solve_gather",
-                "solve_fwd", "solve_bwd_l", "solve_bwd", "permute", "other", "diag", "left", "residual"]
+                "solve_fwd", "solve_bwd_l", "solve_bwd", "permute", "other", "diag", "left", "residual",
+                "solve_passes", "solve_rhs"]
 NK = len(KERNEL_NAMES)
 
 
@@ -72,6 +73,10 @@ def parse():
     ap.add_argument("--requests", type=int, default=600, help="config 5: requests per arrival rate")
     ap.add_argument("--rates", default="50,200,1000", help="config 5: Poisson arrival rates (requests/s)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=400.0,
+                    help="reference arm: seconds of CPU oracle runs (warm-up included)")
+    ap.add_argument("--cpu-budget", type=float, default=240.0,
+                    help="GPU arm: seconds of CPU oracle runs for cpu_baseline")
     ap.add_argument("--profile-only", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="mixed form: tcgen05 tiles on every level")
     ap.add_argument("--no-served", action="store_true", help="configs 1, 2, 4: skip the served batched form")
@@ -81,75 +86,77 @@ def parse():
 
 class Work:
     """One configuration's synthetic input: the matrix (block-diagonal for a
-    batch), its symbolic analysis, the right-hand sides, and how to name it."""
+    batch), its elimination order, the right-hand sides, and how to name it.
+    The symbolic analysis is computed by whoever runs the work: the GPU arm
+    with the package's host library, the reference arm with the oracle's own
+    restatement (the two are integer-identical, tests/test_symbolic_vs_oracle.py)."""
 
-    def __init__(self, A, P, S, B, *, name, diag=0, segments=None, units=1, ordering="", sample=None):
-        self.members = None  # batch: (matrices, symbolics) of the members
-        self.A, self.P, self.S, self.B = A, P, S, B
+    def __init__(self, A, order, B, *, name, diag=0, segments=None, units=1, ordering="", members=None):
+        self.A, self.order, self.B = A, order, B
         self.name, self.diag, self.segments, self.units = name, diag, segments, units
         self.ordering = ordering
-        self.sample = sample  # (A, P, S, B, scale) for the bounded CPU sample
+        self.members = members  # batch: (matrices, orders) of the members
+        self.P = self.S = None
+
+    def symbolic_product(self):
+        """(P, S) from the package's host symbolic library."""
+        import multifrontal as mf
+        from multifrontal import batch
+        if self.P is None:
+            if self.members is not None:
+                parts = [mf.symbolic(Ai, alg=oi) for Ai, oi in zip(*self.members)]
+                self.P, self.S, off = batch.block_symbolic(parts)
+                self.parts = parts
+            else:
+                self.P, self.S = mf.symbolic(self.A, alg=self.order)
+        return self.P, self.S
 
 
-def workload(args, seed=2):
-    import multifrontal as mf
+def workload(args, seed=2, oracle_orders=False):
+    """The configuration's matrix, order and right-hand sides.  Orders are
+    the explicit nested-dissection permutation of the config-2 grid and AMF
+    (the reference default) elsewhere; with oracle_orders the oracle computes
+    them (the reference arm loads nothing of the package but its seeded
+    matrix generators, which are plain numpy)."""
     from multifrontal import testmatrices as tm
+    if oracle_orders:
+        from oracle import oracle as om
+        nd_order, amf = om.grid_nd_order, (lambda A: om.amf_order(A))
+    else:
+        import multifrontal as mf
+        nd_order, amf = mf.grid_nd_order, (lambda A: "amf")
     c = args.config
     if c == 2:
         side = args.side or 80
         nrhs = args.nrhs or 4
         A = tm.config2(side, seed=seed)
-        P, S = mf.symbolic(A, alg=mf.grid_nd_order(side, side, side, 8))
         B = tm.rhs(A.shape[0], nrhs, seed=seed + 1)
-        # CPU sample: the same problem on a 48^3 grid, scaled by factor flops
-        ss = min(side, 48)
-        As = tm.config2(ss, seed=seed)
-        Ps, Ss = mf.symbolic(As, alg=mf.grid_nd_order(ss, ss, ss, 8))
-        return Work(A, P, S, B, name=f"3d7pt_{side}^3_chol_factor+solve_{nrhs}rhs", ordering="geometric ND",
-                    sample=(As, Ps, Ss, tm.rhs(As.shape[0], nrhs, seed=seed + 1),
-                            S.factor_flops() / Ss.factor_flops(), f"the same problem on a {ss}^3 grid"))
+        return Work(A, nd_order(side, side, side, 8), B, name=f"3d7pt_{side}^3_chol_factor+solve_{nrhs}rhs",
+                    ordering="geometric ND")
     if c == 1:
         nrhs = args.nrhs or 1
         A = tm.config1(seed=1)
-        P, S = mf.symbolic(A, alg="amf")
         B = tm.rhs(A.shape[0], nrhs, seed=5)
-        return Work(A, P, S, B, name=f"2d5pt_100^2_chol_factor+solve_{nrhs}rhs", ordering="AMF",
-                    sample=(A, P, S, B, 1.0, "the full problem"))
+        return Work(A, amf(A), B, name=f"2d5pt_100^2_chol_factor+solve_{nrhs}rhs", ordering="AMF")
     if c == 3:
         import scipy.sparse as sp
-        from multifrontal import batch
         nrhs = args.nrhs or 4
         rng = np.random.default_rng(seed)
         sides = rng.integers(8, 49, size=args.batch)
         mats = [tm.config3_matrix(int(s), seed=1000 + i) for i, s in enumerate(sides)]
-        parts = [mf.symbolic(Ai, alg="amf") for Ai in mats]
-        P, S, off = batch.block_symbolic(parts)
         A = sp.block_diag(mats, format="csc")
-        B = tm.rhs(S.n, nrhs, seed=7)
-        m = min(64, args.batch)
-        Ps, Ss, offs = batch.block_symbolic(parts[:m])
-        As = sp.block_diag(mats[:m], format="csc")
-        w = Work(A, P, S, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
-                 segments=off, units=args.batch, ordering="AMF",
-                 sample=(As, Ps, Ss, tm.rhs(Ss.n, nrhs, seed=7), args.batch / m,
-                         f"the first {m} matrices of the batch, scaled by count"))
-        w.members = (mats, parts)
-        return w
+        off = np.concatenate([[0], np.cumsum([M.shape[0] for M in mats])]).astype(np.int64)
+        B = tm.rhs(A.shape[0], nrhs, seed=7)
+        return Work(A, None, B, name=f"batch{args.batch}_2d9pt_side8-48_chol_factor+solve_{nrhs}rhs",
+                    segments=off, units=args.batch, ordering="AMF",
+                    members=(mats, [amf(M) for M in mats]))
     if c == 4:
         side = args.side or 40
         nrhs = args.nrhs or 8
         m = 16000 * side ** 3 // 64000
         A = tm.config4(side=side, m=m, seed=4)
-        P, S = mf.symbolic(A, alg="amf")
         B = tm.rhs(A.shape[0], nrhs, seed=9)
-        ss = min(side, 20)
-        ms = 16000 * ss ** 3 // 64000
-        As = tm.config4(side=ss, m=ms, seed=4)
-        Ps, Ss = mf.symbolic(As, alg="amf")
-        return Work(A, P, S, B, name=f"kkt_{side}^3+{m}_ldlt_factor+solve_{nrhs}rhs", diag=1,
-                    ordering="AMF",
-                    sample=(As, Ps, Ss, tm.rhs(As.shape[0], nrhs, seed=9), S.factor_flops() / Ss.factor_flops(),
-                            f"the same construction with a {ss}^3 grid, scaled by factor flops"))
+        return Work(A, amf(A), B, name=f"kkt_{side}^3+{m}_ldlt_factor+solve_{nrhs}rhs", diag=1, ordering="AMF")
     raise ValueError("config 5 has its own driver")
 
 
@@ -233,47 +240,136 @@ def dgemm_peak_tflops(torch, dev):
 
 
 def exec_sizes(lib, h):
+    """(nn, na, parent) of the execution fronts the device runs (after
+    amalgamation)."""
     info = np.zeros(9, np.int64)
     lib.mf_info(h, info.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
     nex = int(info[8])
     nn = np.zeros(nex, np.int64)
     na = np.zeros(nex, np.int64)
+    par = np.zeros(nex, np.int64)
     p64 = ctypes.POINTER(ctypes.c_int64)
     lib.mf_exec_sizes(h, nn.ctypes.data_as(p64), na.ctypes.data_as(p64))
-    return nn, na
+    lib.mf_exec_parents(h, par.ctypes.data_as(p64))
+    return nn, na, par
 
 
-def kernel_flops(nn, na):
-    """Flops per kernel class for one factorization, counted on the fronts
-    the device executes (after amalgamation): fronts with nj <= 96 run in
-    the fused small kernel; for the others the panel kernels (diagonal
-    blocks, TRSM, left and trailing updates) do nn^3/3 + nn^2*na and the
-    SYRK kernel nn*na^2."""
-    nn = nn.astype(np.float64)
-    na = na.astype(np.float64)
+# kernel families of the profiled classes (csrc/)
+CLASS_KERNELS = {
+    "syrk": "k_gemm_tc<2> (FP32: tcgen05 TF32) / k_gemm<double,2> (FP64: DMMA)",
+    "update": "k_gemm_tc<1> / k_gemm<T,1> trailing update",
+    "left": "k_gemm_tc<0> / k_gemm<T,0> left-looking update",
+    "panel": "k_gemm_tc<3> / k_gemm<T,3> panel TRSM (product with the block inverse)",
+    "diag": "k_diag 64x64 diagonal factor + inverse",
+    "small": "k_small fused small fronts",
+    "extend_add": "k_ea extend-add",
+    "solve_small": "k_s_small_fwd / k_s_small_bwd",
+    "solve_fwd": "k_s_sdiag + k_s_ftile forward steps",
+    "solve_bwd": "k_s_sdiag + k_s_btile backward steps",
+    "solve_bwd_l": "k_s_bwd_l + k_s_bwd_red backward L21^T x[sep]",
+    "solve_gather": "k_s_gather",
+    "assemble": "k_scatter",
+    "residual": "FP64 residual / SpMV",
+}
+
+
+def work_model(nn, na, par, w):
+    """Algorithmic work of one factorization and one solve pass per kernel
+    class, counted from the execution fronts (never from measurements):
+    flops nn^3/3 + nn^2 na (panel roles) and nn na^2 (SYRK) for blocked
+    fronts (nj > 96), all three for the fused small fronts; extend-add bytes
+    2 w na_c (na_c + 1) / 2 per child c of a blocked front (read the child's
+    triangle, write the parent slot once); solve bytes w x factor entries
+    read per sweep (forward and backward), split by the kernels that read
+    them."""
+    nnf = nn.astype(np.float64)
+    naf = na.astype(np.float64)
     big = (nn + na) > 96
+    ssmall = ((nn + na) <= 96) | ((nn <= 64) & (na <= 1024))
+    blk_par = np.zeros(nn.size, bool)
+    has = par >= 0
+    blk_par[has] = big[par[has]]
+    diag_e = nnf * (nnf + 1) / 2
+    off_e = nnf * naf
     return {
-        "small": float(np.sum((nn ** 3 / 3 + nn * nn * na + nn * na * na)[~big])),
-        "panel+update": float(np.sum((nn ** 3 / 3 + nn * nn * na)[big])),
-        "syrk": float(np.sum((nn * na * na)[big])),
+        "small": {"flops": float(np.sum((nnf ** 3 / 3 + nnf * nnf * naf + nnf * naf * naf)[~big]))},
+        "panel+update": {"flops": float(np.sum((nnf ** 3 / 3 + nnf * nnf * naf)[big]))},
+        "syrk": {"flops": float(np.sum((nnf * naf * naf)[big]))},
+        "extend_add": {"bytes": float(2 * w * np.sum((naf * (naf + 1) / 2)[blk_par]))},
+        # per solve pass
+        "solve_small": {"bytes": float(2 * w * np.sum((diag_e + off_e)[ssmall]))},
+        "solve_fwd": {"bytes": float(w * np.sum((diag_e + off_e)[~ssmall]))},
+        "solve_bwd": {"bytes": float(w * np.sum(diag_e[~ssmall]))},
+        "solve_bwd_l": {"bytes": float(w * np.sum(off_e[~ssmall]))},
     }
 
 
-def cpu_sample(work):
-    """Time the CPU oracle on the bounded sample of the workload; returns
-    (seconds per full workload estimated from the sample, sample seconds,
-    description)."""
+def oracle_run(A, P, S, B, diag):
+    """One full factor+solve of the workload by the CPU oracle (the C
+    restatement of chol_impl!/div_impl! over the reference's serial front
+    loop, scipy's OpenBLAS); returns seconds."""
     from oracle import oracle
-    A, P, S, B, scale, what = work.sample
     t0 = time.perf_counter()
-    info, X, _ = oracle.factor_and_solve(A, P, S, B, work.diag)
+    info, X, _ = oracle.factor_and_solve(A, P, S, B, diag)
     dt = time.perf_counter() - t0
     if info != 0:
         raise SystemExit(f"bench: CPU oracle failed (info={info})")
-    return dt * scale, dt, what
+    return dt, X
+
+
+def oracle_workload(work):
+    """(units, [(A, P, S, B)]) the oracle runs for one step of the workload:
+    the whole matrix, or for a batch every member on its own (the reference
+    factors one matrix per object)."""
+    from oracle import oracle
+    if work.members is not None:
+        mats, orders = work.members
+        out = []
+        off = work.segments
+        for i, (M, o) in enumerate(zip(mats, orders)):
+            P, S = oracle.symbolic(M, alg=o)
+            out.append((M, P, S, np.asfortranarray(work.B[off[i]:off[i + 1]])))
+        return out
+    P, S = oracle.symbolic(work.A, alg=work.order)
+    return [(work.A, P, S, work.B)]
+
+
+def cpu_baseline_line(work, budget_s):
+    """The CPU oracle on the GPU box's host cores: full factor+solve runs of
+    the workload (no scaling) while they fit in budget_s, at least one; a
+    batch is sampled by its first members, scaled by count."""
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    jobs = oracle_workload(work)
+    if work.members is not None:
+        t_all, done = 0.0, 0
+        for (A, P, S, B) in jobs:
+            dt, _ = oracle_run(A, P, S, B, work.diag)
+            t_all += dt
+            done += 1
+            if t_all > budget_s:
+                break
+        return {"value": done / t_all, "unit": "solves/s", "cores": threads, "kind": "port",
+                "sample": f"the first {done} of the {len(jobs)} matrices of the batch, one full FP64 factor+solve "
+                          f"each ({t_all:.1f} s), as matrices solved per second"}
+    A, P, S, B = jobs[0]
+    times = []
+    while not times or (sum(times) + times[-1] <= budget_s):
+        dt, _ = oracle_run(A, P, S, B, work.diag)
+        times.append(dt)
+    return {"value": len(times) / sum(times), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} full FP64 factor+solve run(s) of the workload itself, "
+                      f"{np.mean(times):.1f} s each (no scaling)"}
 
 
 def run_reference(args, rank):
+    """The reference arm: the CPU oracle (oracle/, a C restatement of the
+    reference's serial multifrontal loop over scipy's OpenBLAS with every
+    host thread) on the same configuration.  A step is one full factor+solve
+    of the workload (every member of a batch).  Steps that do not fit the
+    time budget (--ref-budget seconds, warm-up included) are not run; the
+    line reports the steps actually timed."""
     if rank != 0:
         return
     from oracle import oracle
@@ -284,54 +380,96 @@ def run_reference(args, rank):
                           "unavailable": "the serving configuration has no CPU counterpart in the reference; "
                                          "its CPU leg is reported inside the GPU arm's line"}), flush=True)
         return
-    work = workload(args)
-    for _ in range(args.warmup):
-        cpu_sample(work)
+    work = workload(args, oracle_orders=True)
+    jobs = oracle_workload(work)
+
+    def step():
+        t = 0.0
+        for (A, P, S, B) in jobs:
+            t += oracle_run(A, P, S, B, work.diag)[0]
+        return t
+
+    t_first = step()  # also the first warm-up step
+    warm = 1
+    budget = args.ref_budget
+    spent = t_first
+    while warm < args.warmup and spent + 2 * t_first <= budget:
+        spent += step()
+        warm += 1
     times = []
-    sample_s = 0.0
-    what = ""
-    for _ in range(args.steps):
-        est, dt, what = cpu_sample(work)
-        times.append(est)
-        sample_s += dt
+    while len(times) < args.steps and (not times or spent + t_first <= budget):
+        dt = step()
+        times.append(dt)
+        spent += dt
     tot = sum(times)
-    value = work.units * args.steps / tot
+    value = work.units * len(times) / tot
+    S0 = jobs[0][2]
     line = {
         "impl": "reference", "metric": "solves_per_s", "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+        "steps": len(times), "warmup": warm, "ms_per_step": 1e3 * tot / len(times),
+        "steps_requested": args.steps, "warmup_requested": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": work.name, "n": int(work.S.n), "factor_gflop": work.S.factor_flops() / 1e9,
-                   "ordering": work.ordering},
+        "config": {"workload": work.name, "n": int(work.A.shape[0]),
+                   "factor_gflop": sum(j[2].factor_flops() for j in jobs) / 1e9, "ordering": work.ordering},
         "p50_ms": float(np.percentile(times, 50) * 1e3), "p99_ms": float(np.percentile(times, 99) * 1e3),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"each step times {what} ({sample_s / args.steps:.2f} s) and scales it to "
-                                   f"the workload"},
+                         "sample": f"every step is one full FP64 factor+solve of the workload ({work.units} "
+                                   f"matrices); {len(times)} timed + {warm} warm-up steps fit the "
+                                   f"{budget:.0f} s budget, no scaling"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if len(times) < args.steps or warm < args.warmup:
+        line["note"] = (f"{args.steps} + {args.warmup} full runs would take about "
+                        f"{(args.steps + args.warmup) * t_first:.0f} s; only the runs that fit the "
+                        f"{budget:.0f} s budget were made")
+    del S0
     print(json.dumps(line), flush=True)
 
 
-def roofline(form, peak, peak_src, fl, passes=1):
-    kt = form["kernels"]
+def rooflines(form, peaks, fp64_peak):
+    """Achieved rate and roofline fraction of every profiled kernel class of
+    one form, and the dominant one (largest device time in the profiled
+    step).  Tensor-bound classes are held against the measured dense bf16
+    rate (MEASURED_PEAKS.json, sustained: the kernels run inside a long
+    step) for the mixed form and against cuBLAS DGEMM measured in the run for
+    the FP64 form (no FP64 figure is in MEASURED_PEAKS.json); HBM-bound
+    classes against the measured copy bandwidth."""
+    kt, wm, mixed = form["kernels"], form["work"], form["mixed"]
+    passes = max(kt["solve_passes"]["launches"], 1)
+    hbm = peaks.get("hbm_gbs") or 6650.0
+    tpk = (peaks.get("bf16_tflops_sustained") or 1400.0) if mixed else fp64_peak
+    tsrc = ("bf16_tflops_sustained of MEASURED_PEAKS.json (the TF32 kind issues at half the bf16 rate; the "
+            "kernels run 3 TF32 passes per product)" if mixed else "cuBLAS DGEMM 8192^3 measured in this run")
     classes = {
-        "syrk": (fl["syrk"], ["syrk"]),
-        "panel+update": (fl["panel+update"], ["panel", "update", "diag", "left"]),
-        "small": (fl["small"], ["small"]),
+        "syrk": ("tensor", wm["syrk"]["flops"], ["syrk"]),
+        "panel+update": ("tensor", wm["panel+update"]["flops"], ["panel", "update", "diag", "left"]),
+        "small": ("tensor", wm["small"]["flops"], ["small"]),
+        "extend_add": ("hbm", wm["extend_add"]["bytes"], ["extend_add"]),
+        "solve_small": ("hbm", wm["solve_small"]["bytes"] * passes, ["solve_small"]),
+        "solve_fwd": ("hbm", wm["solve_fwd"]["bytes"] * passes, ["solve_fwd"]),
+        "solve_bwd": ("hbm", wm["solve_bwd"]["bytes"] * passes, ["solve_bwd"]),
+        "solve_bwd_l": ("hbm", wm["solve_bwd_l"]["bytes"] * passes, ["solve_bwd_l"]),
     }
-    cls_ms = {k: sum(kt[x]["ms"] for x in v[1]) for k, v in classes.items()}
-    dom = max(cls_ms, key=cls_ms.get)
-    launches = sum(kt[x]["launches"] for x in classes[dom][1])
-    kms = cls_ms[dom]
-    achieved = classes[dom][0] / (kms / 1e3) / 1e12 if kms > 0 else 0.0
-    per_class = {k: {"tflops": classes[k][0] / (cls_ms[k] / 1e3) / 1e12 if cls_ms[k] > 0 else None,
-                     "ms": cls_ms[k], "gflop": classes[k][0] / 1e9} for k in classes}
-    out = {"kernel": dom, "bound": "tensor" if dom != "small" else "latency", "achieved": achieved,
-           "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
-           "peak_source": peak_src, "flops_per_launch": classes[dom][0] / max(launches, 1),
-           "avg_launch_ms": kms / max(launches, 1), "classes": per_class}
-    if passes > 1:
-        out["mma_passes_per_product"] = passes
-    return out
+    out = {}
+    for name, (bound, work, ks) in classes.items():
+        ms = sum(kt[k]["ms"] for k in ks)
+        launches = sum(kt[k]["launches"] for k in ks)
+        if ms <= 0 or launches == 0:
+            continue
+        if bound == "tensor":
+            ach, unit, peak, src = work / (ms / 1e3) / 1e12, "TFLOP/s", tpk, tsrc
+        else:
+            ach, unit, peak, src = work / (ms / 1e3) / 1e9, "GB/s", hbm, "hbm_gbs of MEASURED_PEAKS.json"
+        out[name] = {"kernel": " + ".join(CLASS_KERNELS.get(k, k) for k in ks), "bound": bound, "achieved": ach,
+                     "peak": peak, "unit": unit, "frac": ach / peak, "ms_per_step": ms, "launches": launches,
+                     "per_launch": work / launches, "avg_launch_ms": ms / launches, "peak_source": src,
+                     "traffic": None}
+    dom = max(out, key=lambda k: out[k]["ms_per_step"])
+    head = dict(out[dom])
+    head["class"] = dom
+    head["classes"] = out
+    head["solve_passes_per_step"] = passes
+    return head
 
 
 def main():
@@ -363,6 +501,7 @@ def main():
             dist.destroy_process_group()
         return
     work = workload(args)
+    P, S = work.symbolic_product()
 
     if args.profile_only:
         r = run_form(args, work, mixed=args.mixed_profile, local=local, world=world, profile_only=True)
@@ -374,34 +513,27 @@ def main():
     unbatched = time_unbatched(work, local) if work.members is not None else None
     served = run_served(args, work, local) if args.config in SERVED and not args.no_served else None
 
-    # roofline: the dominant kernel class of each form against cuBLAS peaks
-    # of the same arithmetic measured in this run
+    # rooflines of every kernel class; the headline is the class with the
+    # largest device time in the step
+    peaks = measured_peaks()
     dgemm = dgemm_peak_tflops(torch, dev)
-    tf32 = gemm_peak_tflops(torch, dev, torch.float32, allow_tf32=True)
-    roof_mixed = roofline(mixed, tf32, "cuBLAS TF32 GEMM 8192^3 measured in this run (the kernels run 3 TF32 "
-                                       "MMA passes per product: hi*hi + hi*lo + lo*hi)", mixed["flops"], passes=3)
-    roof_plain = roofline(plain, dgemm, "cuBLAS DGEMM 8192^3 measured in this run (no FP64 figure in "
-                                        "MEASURED_PEAKS.json)", plain["flops"])
+    roof_mixed = rooflines(mixed, peaks, dgemm)
+    roof_plain = rooflines(plain, peaks, dgemm)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        from oracle import oracle
-        threads = os.cpu_count() or 1
-        oracle.set_threads(threads)
-        est, dt, what = cpu_sample(work)
-        cpu = {"value": work.units / est, "unit": "solves/s", "cores": threads, "kind": "port",
-               "sample": f"{what}: {dt:.2f} s for FP64 factor+solve, scaled to {est:.1f} s for the workload"}
+        cpu = cpu_baseline_line(work, args.cpu_budget)
 
     if rank == 0:
         line = {
             "metric": "solves_per_s", "value": mixed["value"], "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": work.name, "n": int(work.S.n), "fronts": int(work.S.nfr),
-                       "factor_gflop": work.S.factor_flops() / 1e9, "nnz_L": int(work.S.nnz()),
+            "config": {"workload": work.name, "n": int(S.n), "fronts": int(S.nfr),
+                       "factor_gflop": S.factor_flops() / 1e9, "nnz_L": int(S.nnz()),
                        "ordering": work.ordering, "matrices_per_step": work.units,
                        "mode": "mixed: FP32 fronts (3xTF32 tcgen05) + FP64 refinement to backward error 1e-12",
-                       "l2": "inputs larger than L2" if work.S.nnz() * 4 > 126e6 else
+                       "l2": "inputs larger than L2" if S.nnz() * 4 > 126e6 else
                              "working set fits L2 (no flush: a step rewrites every factor entry)",
                        "parallelism": f"replicas x{world}"},
             "p50_ms": mixed["p50_ms"], "p99_ms": mixed["p99_ms"], "backward_error": mixed["backward_error"],
@@ -628,7 +760,8 @@ def time_unbatched(work, local, count=64):
     import multifrontal as mf
     from multifrontal import _native
     from multifrontal.sparse import assembly_map
-    mats, parts = work.members
+    mats = work.members[0]
+    parts = work.parts
     nrhs = work.B.shape[1]
     lib = _native.gpulib()
     jobs = []
@@ -765,9 +898,10 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
     lib.mf_kernel_times(h, ms, ln)
     lib.mf_profile(h, 0)
     ktimes = {KERNEL_NAMES[i]: {"ms": ms[i], "launches": int(ln[i])} for i in range(NK)}
-    launches_per_step = int(sum(ln[i] for i in range(NK)))
-    enn, ena = exec_sizes(lib, h)
-    fl = kernel_flops(enn, ena)
+    launches_per_step = int(sum(ln[i] for i in range(NK) if not KERNEL_NAMES[i].startswith("solve_pass")
+                                and KERNEL_NAMES[i] != "solve_rhs"))
+    enn, ena, epar = exec_sizes(lib, h)
+    wm = work_model(enn, ena, epar, 4 if mixed else 8)
 
     # timed device-resident pass
     for _ in range(args.warmup):
@@ -829,8 +963,8 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(nz_host.numel() * 8 + n * nrhs * 8),
                 "d2h_bytes_per_step": int(n * nrhs * 8 + 8), "backward_error": eta_e2e,
                 "p50_ms": float(np.percentile(e2e_ms, 50)), "p99_ms": float(np.percentile(e2e_ms, 99))},
-        "gpu_launches": launches_per_step * args.steps, "kernels": ktimes, "clocks": ck, "flops": fl,
-        "autotune": tune,
+        "gpu_launches": launches_per_step * args.steps, "kernels": ktimes, "clocks": ck, "work": wm,
+        "mixed": mixed, "autotune": tune,
     }
 
 

@@ -51,7 +51,7 @@ void free_all(mf_handle* h) {
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
                     h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
-                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc};
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet};
     release_graphs(h);
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -918,6 +918,18 @@ int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na) {
         if (nn) nn[e] = h->h_fronts[e].nn;
         if (na) na[e] = h->h_fronts[e].na;
     }
+    return 0;
+}
+
+int mf_logdet(mf_handle* h, double* logabsdet, double* sign) {
+    if (!h || !logabsdet || !sign) { set_error("mf_logdet: bad arguments"); return -1; }
+    DeviceGuard g(h->device);
+    return launch_logdet(h, logabsdet, sign);
+}
+
+int mf_exec_parents(const mf_handle* h, int64_t* parent) {
+    if (!h || (h->nexec && !parent)) { set_error("mf_exec_parents: bad arguments"); return -1; }
+    for (int64_t e = 0; e < h->nexec; ++e) parent[e] = h->h_fronts[e].parent;
     return 0;
 }
 

@@ -203,20 +203,38 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
 // ---------------------------------------------------------------------------
 // extend-add for blocked fronts
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int lower_bound_i32(const int32_t* a, int n, int v) {
+
+// First index a in [0, n) with rel[a] >= v (n if none) for a sorted array,
+// found by the whole warp: each round samples 32 evenly spaced entries with
+// one load per lane and narrows the range by the ballot of the comparisons,
+// so a search over n entries takes about log_32(n) dependent loads instead of
+// log_2(n).  Every lane returns the same index.
+__device__ __forceinline__ int warp_lower_bound(const int32_t* __restrict__ rel, int n, int v, int lane) {
     int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < v) lo = mid + 1; else hi = mid;
+    while (hi - lo > 32) {
+        const int step = (hi - lo + 31) >> 5;
+        const int idx = lo + lane * step;
+        const int x = idx < hi ? __ldg(rel + idx) : INT_MAX;
+        const int k = __popc(__ballot_sync(0xffffffffu, x < v));
+        if (k == 0) return lo;
+        const int nlo = lo + (k - 1) * step + 1;
+        hi = min(lo + k * step, hi);
+        lo = nlo;
     }
-    return lo;
+    const int x = lo + lane < hi ? __ldg(rel + lo + lane) : INT_MAX;
+    return lo + __popc(__ballot_sync(0xffffffffu, x < v));
 }
 
 // One CTA per 16 parent columns; warp w owns parent columns c0 + w and
 // c0 + w + 8 and adds, child after child in a fixed order, the child
 // columns that map onto them.  A column is only ever touched by its warp, so
-// no block barrier and no atomics are needed and the sums are deterministic;
-// the eight warps stream independently.
+// no block barrier and no atomics are needed and the sums are deterministic
+// (the children are added in the reference's order, cholesky.jl:506-514).
+// Each warp finds the child columns that land in its CTA's 16 columns with
+// two warp-cooperative searches of the child's relative indices, then
+// streams each child column in chunks of 4 x 32 rows: the relative indices
+// and child values of the chunk are loaded first, then the 4 parent entries
+// they address, so four independent gather chains are in flight per lane.
 template <typename T>
 __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                             const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
@@ -236,17 +254,30 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
         const Front fc = fronts[chdtgt[p]];
         const int ma = fc.na, lmc = fc.ldm;
-        const int32_t* rel = reltgt + fc.sep0;
+        const int32_t* __restrict__ rel = reltgt + fc.sep0;
         const T* Mc = M + fc.moff;
-        const int b0 = lower_bound_i32(rel, ma, c0);
-        const int b1 = lower_bound_i32(rel, ma, c1);
+        const int b0 = warp_lower_bound(rel, ma, c0, lane);
+        const int b1 = warp_lower_bound(rel, ma, c1, lane);
         for (int b = b0; b < b1; ++b) {
-            const int col = rel[b];
+            const int col = __ldg(rel + b);
             if (((col - c0) & 7) != warp) continue;  // the owner warp of this parent column
             const T* mc = Mc + (int64_t)b * lmc;
             T* dst = col < nn ? Pj + (int64_t)col * ld : Mj + (int64_t)(col - nn) * lm - nn;
-#pragma unroll 4
-            for (int a = b + lane; a < ma; a += 32) dst[rel[a]] += mc[a];
+            int a = b + lane;
+            for (; a + 96 < ma; a += 128) {
+                int r[4];
+                T v[4], o[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    r[u] = __ldg(rel + a + 32 * u);
+                    v[u] = mc[a + 32 * u];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) o[u] = dst[r[u]];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) dst[r[u]] = o[u] + v[u];
+            }
+            for (; a < ma; a += 32) dst[__ldg(rel + a)] += mc[a];
         }
         __syncwarp();
     }
@@ -1096,6 +1127,117 @@ int launch_factor_mixed(mf_handle* h) {
     return run_captured(h, 2, (int64_t)(uintptr_t)h->d_signs, h->use_tc ? 1 : 0, 0, [&]() {
         return h->diag ? factor_impl<float, 1>(h, fb) : factor_impl<float, 0>(h, fb);
     });
+}
+
+}  // namespace mf
+
+// ---------------------------------------------------------------------------
+// log|det| of the factored matrix, reduced on the device
+// (LinearAlgebra.logabsdet / logdet / det of a ChordalFactorization,
+// src/Multifrontal.jl/src/abstract_factorization.jl:156-179).  Cholesky: the
+// terms are log of the squared diagonal of L; LDLt: log|d_j| and the sign of
+// d_j.  A mixed handle without an FP64 factor uses its single-precision factor
+// of S A S and adds -2 log s_j.  Each block reduces a contiguous range of
+// columns in a fixed tree order and writes (sum, negatives, zeros); the host
+// adds the block results in block order, so the result is bitwise repeatable.
+// ---------------------------------------------------------------------------
+namespace mf {
+
+constexpr int kLogdetThreads = 256;
+constexpr int kLogdetBlocks = 296;  // 2 x 148 SMs
+
+template <typename T, int UNIT>
+__global__ void __launch_bounds__(kLogdetThreads)
+k_logdet(const Front* __restrict__ fronts, const RefFront* __restrict__ ref, const int32_t* __restrict__ colref,
+         const T* __restrict__ P, const T* __restrict__ d, const double* __restrict__ scale, int64_t n,
+         double* __restrict__ out) {
+    __shared__ double s_sum[kLogdetThreads];
+    __shared__ int s_neg[kLogdetThreads], s_zero[kLogdetThreads];
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t c0 = blockIdx.x * per;
+    const int64_t c1 = c0 + per < n ? c0 + per : n;
+    double acc = 0.0;
+    int neg = 0, zero = 0;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += kLogdetThreads) {
+        double v;
+        if (UNIT) {
+            v = (double)d[c];
+        } else {
+            const RefFront rf = ref[colref[c]];
+            const Front f = fronts[rf.exec];
+            const int64_t k = c - f.col0;
+            const double l = (double)P[f.poff + k + k * f.ldp];
+            v = l * l;
+        }
+        if (scale) v /= scale[c] * scale[c];
+        if (v == 0.0) zero += 1;
+        if (v < 0.0) neg += 1;
+        acc += log(fabs(v));
+    }
+    s_sum[threadIdx.x] = acc;
+    s_neg[threadIdx.x] = neg;
+    s_zero[threadIdx.x] = zero;
+    __syncthreads();
+    for (int w = kLogdetThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            s_sum[threadIdx.x] += s_sum[threadIdx.x + w];
+            s_neg[threadIdx.x] += s_neg[threadIdx.x + w];
+            s_zero[threadIdx.x] += s_zero[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[3 * blockIdx.x] = s_sum[0];
+        out[3 * blockIdx.x + 1] = (double)s_neg[0];
+        out[3 * blockIdx.x + 2] = (double)s_zero[0];
+    }
+}
+
+int launch_logdet(mf_handle* h, double* logabsdet, double* sign) {
+    const bool fp64 = have_fp64(h) && (!h->mixed || h->fp64_current);
+    if (!fp64 && !h->mixed) {
+        set_error("mf_logdet: no factor on the device");
+        return -1;
+    }
+    if (!h->d_logdet) {
+        MF_CUDA(cudaMalloc((void**)&h->d_logdet, sizeof(double) * 3 * kLogdetBlocks));
+        h->bytes += (int64_t)sizeof(double) * 3 * kLogdetBlocks;
+    }
+    double* part = h->d_logdet;
+    const int64_t n = h->n;
+    if (n > 0) {
+        if (fp64) {
+            if (h->diag)
+                k_logdet<double, 1><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                    h->d_fronts, h->d_ref, h->d_colfront, h->d_P, h->d_d, nullptr, n, part);
+            else
+                k_logdet<double, 0><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                    h->d_fronts, h->d_ref, h->d_colfront, h->d_P, h->d_d, nullptr, n, part);
+        } else {
+            if (h->diag)
+                k_logdet<float, 1><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                    h->d_fronts, h->d_ref, h->d_colfront, h->f32.P, h->f32.d, h->d_scale, n, part);
+            else
+                k_logdet<float, 0><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                    h->d_fronts, h->d_ref, h->d_colfront, h->f32.P, h->f32.d, h->d_scale, n, part);
+        }
+        MF_CUDA(cudaGetLastError());
+    }
+    std::vector<double> hp(3 * kLogdetBlocks, 0.0);
+    cudaError_t e = cudaSuccess;
+    if (n > 0)
+        e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * 3 * kLogdetBlocks, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "mf_logdet");
+    double sum = 0.0, neg = 0.0, zero = 0.0;
+    for (int b = 0; b < kLogdetBlocks; ++b) {
+        sum += hp[3 * b];
+        neg += hp[3 * b + 1];
+        zero += hp[3 * b + 2];
+    }
+    *logabsdet = zero > 0 ? -INFINITY : sum;
+    *sign = zero > 0 ? 0.0 : (fmod(neg, 2.0) == 0.0 ? 1.0 : -1.0);
+    return 0;
 }
 
 }  // namespace mf

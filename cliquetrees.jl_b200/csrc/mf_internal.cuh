@@ -129,7 +129,10 @@ struct KernelTimes {
 enum KernelId {
     K_ASSEMBLE = 0, K_SMALL, K_EA, K_PANEL, K_UPDATE, K_SYRK,
     K_S_SMALL, K_S_GATHER, K_S_FWD, K_S_BWD_L, K_S_BWD, K_PERM, K_OTHER,
-    K_DIAG, K_LEFT, K_SPMV, K_COUNT
+    K_DIAG, K_LEFT, K_SPMV,
+    K_SOLVE_PASS,  // not a kernel: solve passes (launches) made while profiling
+    K_SOLVE_RHS,   // not a kernel: right-hand-side columns those passes solved
+    K_COUNT
 };
 
 // The solves handle a front with one warp when the factorization kept it
@@ -287,6 +290,7 @@ struct mf_handle {
     double* d_chunkred = nullptr;  // per chunk: residual maxima (kSegRed) and dot partials (16)
     double* d_segsc = nullptr;     // per segment: CG scalars (80)
 
+    double* d_logdet = nullptr;    // per-block partial results of mf_logdet (allocated on first use)
     int64_t bytes = 0;             // device bytes allocated
     // optional per-kernel timing
     bool profile = false;
@@ -339,6 +343,8 @@ int launch_solve_mixed(mf_handle* h, int64_t nrhs);
 int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst);
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);
 int launch_anorm(mf_handle* h);
+// log|det A| and sign(det A) from the factor on the device (mf_logdet)
+int launch_logdet(mf_handle* h, double* logabsdet, double* sign);
 constexpr int kSegRed = 49;  // doubles per segment in d_segred
 constexpr int kChunkRows = 16384;  // rows per reduction chunk of a segment
 constexpr int kChunkRed = kSegRed + 16;  // doubles per chunk in d_chunkred

@@ -720,6 +720,10 @@ int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* per
 
 template <typename T, int UNIT>
 static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
+    if (h->profile) {
+        h->times.launches[K_SOLVE_PASS] += 1;
+        h->times.launches[K_SOLVE_RHS] += nrhs;
+    }
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 16>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_ftile<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ftile_smem<T, 4>()));

@@ -97,6 +97,10 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_profile.argtypes = [_vp, ctypes.c_int]
         lib.mf_profile.restype = ctypes.c_int
         lib.mf_kernel_times.argtypes = [_vp, _pd, _p64]
+        lib.mf_logdet.argtypes = [_vp, _pd, _pd]
+        lib.mf_logdet.restype = ctypes.c_int
+        lib.mf_exec_parents.argtypes = [_vp, _p64]
+        lib.mf_exec_parents.restype = ctypes.c_int
         lib.mf_kernel_times.restype = ctypes.c_int
         pint = ctypes.POINTER(ctypes.c_int)
         lib.mf_enable_mixed.argtypes = [_vp]

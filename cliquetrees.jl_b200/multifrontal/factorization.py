@@ -236,31 +236,32 @@ class ChordalFactorization:
     def solve(self, B):
         return ldiv(self, B)
 
+    def logabsdet(self):
+        """(log|det A|, sign det A), reduced on the GPU from the factor's
+        diagonal (logabsdet, abstract_factorization.jl:175-181)."""
+        if not self._factored:
+            raise RuntimeError("factorize first (cholesky_ / ldlt_)")
+        la = ctypes.c_double(0.0)
+        sg = ctypes.c_double(0.0)
+        check(self._handle.lib.mf_logdet(self._handle.h, ctypes.byref(la), ctypes.byref(sg)), "mf_logdet")
+        return float(la.value), float(sg.value)
+
     def logdet(self) -> float:
-        Dval, _, d = self.factor_arrays()
-        diag = _diag_entries(self.S, Dval)
-        if self.DIAG == 0:
-            return float(2.0 * np.sum(np.log(diag)))
-        return float(np.sum(np.log(np.abs(d)).astype(np.float64)))
+        """logdet(F) (abstract_factorization.jl:167-173): 2 logdet(L) for
+        Cholesky; log|det| + log(sign) for LDLt, which, as Julia's log of a
+        negative number, raises for a negative determinant."""
+        la, sg = self.logabsdet()
+        if sg < 0:
+            raise ValueError("logdet of a matrix with negative determinant (DomainError in the reference)")
+        return la if sg > 0 else -np.inf
 
     def det(self) -> float:
-        Dval, _, d = self.factor_arrays()
-        if self.DIAG == 0:
-            diag = _diag_entries(self.S, Dval)
-            return float(np.prod(diag) ** 2)
-        return float(np.prod(d))
+        """det(F) (abstract_factorization.jl:159-165)."""
+        la, sg = self.logabsdet()
+        return float(sg * np.exp(la))
 
     def close(self):
         self._handle.close()
-
-
-def _diag_entries(S: ChordalSymbolic, Dval):
-    out = np.empty(S.n, np.float64)
-    for j in range(S.nfr):
-        nn = S.nn(j)
-        blk = Dval[S.Dptr[j]:S.Dptr[j] + nn * nn].reshape(nn, nn, order="F")
-        out[S.resptr[j]:S.resptr[j + 1]] = np.diag(blk)
-    return out
 
 
 class ChordalCholesky(ChordalFactorization):
@@ -321,6 +322,10 @@ def issuccess(F: ChordalFactorization) -> bool:
 
 def logdet(F: ChordalFactorization) -> float:
     return F.logdet()
+
+
+def logabsdet(F: ChordalFactorization):
+    return F.logabsdet()
 
 
 def det(F: ChordalFactorization) -> float:

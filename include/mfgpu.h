@@ -150,6 +150,16 @@ int mf_get_factor_mixed(mf_handle* h, double* Dval, double* Lval, double* d, dou
 /* Copy the device factor out in the reference layout (any pointer may be NULL). */
 int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d);
 
+/* log|det A| and sign(det A) of the matrix last factored on this handle,
+ * reduced on the device from the factor's diagonal: Cholesky 2 sum log L_jj
+ * with sign +1, LDLt sum log|d_j| with the sign of prod d_j; a zero pivot
+ * gives -inf and sign 0.  A mixed handle whose factor is single precision
+ * uses it and the scaling (log|det A| = log|det S A S| - 2 sum log s_j), to
+ * single-precision accuracy.  Replaces logabsdet / logdet / det of a
+ * factorization, src/Multifrontal.jl/src/abstract_factorization.jl:156-179.
+ * Synchronises the handle's stream. */
+int mf_logdet(mf_handle* h, double* logabsdet, double* sign);
+
 /* Wait for the handle's stream. */
 int mf_synchronize(mf_handle* h);
 
@@ -161,6 +171,10 @@ int mf_info(const mf_handle* h, int64_t* out);
  * entries each), for flop accounting. */
 int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na);
 
+/* Parent of every execution front (mf_info out[8] entries; -1 for roots),
+ * for counting the algorithmic bytes of the extend-add. */
+int mf_exec_parents(const mf_handle* h, int64_t* parent);
+
 /* Host-only inspection of the execution plan a handle would use (no CUDA
  * call): out[0..6] = execution fronts after amalgamation, tree levels,
  * panel values, update-matrix pool values, solve-update pool rows, work
@@ -171,10 +185,11 @@ int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* s
 
 /* Optional per-kernel timing (CUDA events around every launch, stream
  * synchronised after each: for profiling passes only).  mf_kernel_times
- * fills ms[16] and launches[16] in the order: assemble, small, extend-add,
+ * fills ms[18] and launches[18] in the order: assemble, small, extend-add,
  * panel TRSM, trailing update, syrk, solve-small, solve-gather, solve-fwd,
  * solve-bwd-l, solve-bwd, permute, other, diagonal blocks, left update,
- * residual. */
+ * residual; then two counters that are not kernels (ms 0): solve passes
+ * and the right-hand-side columns they solved. */
 int mf_profile(mf_handle* h, int enable);
 int mf_kernel_times(const mf_handle* h, double* ms, int64_t* launches);
 

@@ -142,6 +142,14 @@ class OracleSymbolic:
     def nlz(self):
         return int(self.Lptr[-1])
 
+    def nn(self, j=None):
+        d = np.diff(self.resptr)
+        return d if j is None else int(d[j])
+
+    def na(self, j=None):
+        d = np.diff(self.sepptr)
+        return d if j is None else int(d[j])
+
     def res(self, j):
         return np.arange(self.resptr[j], self.resptr[j + 1], dtype=np.int64)
 
@@ -177,6 +185,42 @@ def pattern(A):
     P = (C + C.T).tocsc()
     P.sort_indices()
     return P.indptr.astype(np.int64), P.indices.astype(np.int64)
+
+
+def grid_nd_order(nx, ny, nz=1, leaf=8):
+    """Nested-dissection order of an nx x ny x nz grid by recursive coordinate
+    bisection (vertex id x + nx*(y + ny*z)): the explicit permutation the
+    3D benchmark workloads pass to symbolic (the reference accepts an order
+    vector, elimination_algorithms.jl:776-779).  Boxes of at most `leaf`
+    vertices (or at most 2 along every axis) are numbered x fastest; a larger
+    box is split at the middle plane of its longest axis (x, then y, then z on
+    ties), and numbered first half, second half, then the separator plane x
+    fastest."""
+    out = []
+
+    def plain(x0, x1, y0, y1, z0, z1):
+        z, y, x = np.meshgrid(np.arange(z0, z1), np.arange(y0, y1), np.arange(x0, x1), indexing="ij")
+        out.append((x + nx * (y + ny * z)).ravel())
+
+    def box(x0, x1, y0, y1, z0, z1):
+        sx, sy, sz = x1 - x0, y1 - y0, z1 - z0
+        if sx <= 0 or sy <= 0 or sz <= 0:
+            return
+        if sx * sy * sz <= leaf or (sx <= 2 and sy <= 2 and sz <= 2):
+            plain(x0, x1, y0, y1, z0, z1)
+            return
+        if sx >= sy and sx >= sz:
+            m = x0 + sx // 2
+            box(x0, m, y0, y1, z0, z1); box(m + 1, x1, y0, y1, z0, z1); plain(m, m + 1, y0, y1, z0, z1)
+        elif sy >= sz:
+            m = y0 + sy // 2
+            box(x0, x1, y0, m, z0, z1); box(x0, x1, m + 1, y1, z0, z1); plain(x0, x1, m, m + 1, z0, z1)
+        else:
+            m = z0 + sz // 2
+            box(x0, x1, y0, y1, z0, m); box(x0, x1, y0, y1, m + 1, z1); plain(x0, x1, y0, y1, m, m + 1)
+
+    box(0, nx, 0, ny, 0, nz)
+    return np.concatenate(out).astype(np.int64)
 
 
 def amf_order(A):

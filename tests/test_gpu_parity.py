@@ -40,10 +40,28 @@ def diag_mask(S):
     return m
 
 
+def ldlt_pivot_scale(S, Dval, Lval, d, adiag):
+    """|a_kk| + sum_j L_kj^2 |d_j|: the scale of the rounding error of the
+    pivot d_k = a_kk - sum_j L_kj^2 d_j (the standard LDLt error bound
+    |L D L^T - A| <= gamma (|A| + |L| |D| |L^T|)); on quasidefinite matrices
+    with tiny static pivots the terms can exceed |d_k| + |a_kk| by 1e6."""
+    sc = np.abs(np.asarray(adiag, float)).copy()
+    for j in range(S.nfr):
+        r0, r1 = S.resptr[j], S.resptr[j + 1]
+        nn, na = r1 - r0, S.sepptr[j + 1] - S.sepptr[j]
+        D = Dval[S.Dptr[j]:S.Dptr[j] + nn * nn].reshape(nn, nn, order="F")
+        L = Lval[S.Lptr[j]:S.Lptr[j] + nn * na].reshape(na, nn, order="F")
+        dj = np.abs(d[r0:r1])
+        sc[r0:r1] += (np.tril(D, -1) ** 2) @ dj
+        sc[S.sep(j)] += (L ** 2) @ dj
+    return sc
+
+
 def assert_factor_close(S, got, want, diag, rtol=1e-10, adiag=None):
     """Factor entries within rtol of each factor's largest entry; LDLt pivots
-    within rtol of |d| + |a_kk| (a pivot is a_kk minus a sum of terms of
-    that size, so cancellation leaves an absolute error on that scale)."""
+    within rtol of |d| + |a_kk| + sum_j L_kj^2 |d_j| (a pivot is a_kk minus
+    a sum of terms of that size, so cancellation leaves an absolute error on
+    that scale; see ldlt_pivot_scale)."""
     Dg, Lg, dg = got
     Dw, Lw, dw = want
     m = lower_mask(S)
@@ -53,7 +71,7 @@ def assert_factor_close(S, got, want, diag, rtol=1e-10, adiag=None):
     np.testing.assert_allclose(Dg[m], Dw[m], rtol=0, atol=rtol * scale)
     np.testing.assert_allclose(Lg, Lw, rtol=0, atol=rtol * scale)
     if diag:
-        scale = np.abs(dw[:S.n]) + (0 if adiag is None else np.abs(adiag))
+        scale = np.abs(dw[:S.n]) + ldlt_pivot_scale(S, Dw, Lw, dw, np.zeros(S.n) if adiag is None else adiag)
         assert np.all(np.abs(dg - dw[:S.n]) <= rtol * scale), np.max(np.abs(dg - dw[:S.n]) / scale)
 
 
