@@ -8,9 +8,11 @@
 //               chol_loop_snd!/chol_loop_nod! (cholesky.jl:434-692) for the
 //               many tiny fronts of a maximal-supernode tree.
 //   k_ea      : extend-add for larger fronts, one CTA per (front, 16 parent
-//               columns); each CTA owns its target columns, so the children
-//               are added in a fixed order without atomics (addscattertri!,
-//               utils.jl:555-579 via chol_send!, cholesky.jl:950-983).
+//               columns, 1024 parent rows); each CTA owns its target entries,
+//               so the children are added in a fixed order without atomics
+//               (addscattertri!, utils.jl:555-579 via chol_send!,
+//               cholesky.jl:950-983).  The panel columns are done before the
+//               front is factored, the update-matrix columns after the SYRK.
 //   k_diag    : per 64-column sub-panel, one CTA per front factors the
 //               diagonal block in shared memory, writes it back and stores
 //               the inverse of the factored block (potrf! of chol_factor!,
@@ -20,8 +22,9 @@
 //               update of a sub-panel from its outer block, trailing update
 //               of the panel after an outer block (K = 256), the TRSM of a
 //               sub-panel as a product with the inverse of its diagonal
-//               block, and M = F22 - L21 D L21^T with K = nn (syrk!,
-//               blas/syrk.jl:137-159).
+//               block, and M = -L21 D L21^T with K = nn (syrk!,
+//               blas/syrk.jl:137-159; the children's F22 is added to M
+//               after it, which reorders the reference's sum F22 - L21 L21^T).
 #include <climits>
 #include <cstdio>
 #include <type_traits>
@@ -204,67 +207,45 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
 // extend-add for blocked fronts
 // ---------------------------------------------------------------------------
 
-// First index a in [0, n) with rel[a] >= v (n if none) for a sorted array,
-// found by the whole warp: each round samples 32 evenly spaced entries with
-// one load per lane and narrows the range by the ballot of the comparisons,
-// so a search over n entries takes about log_32(n) dependent loads instead of
-// log_2(n).  Every lane returns the same index.
-__device__ __forceinline__ int warp_lower_bound(const int32_t* __restrict__ rel, int n, int v, int lane) {
-    int lo = 0, hi = n;
-    while (hi - lo > 32) {
-        const int step = (hi - lo + 31) >> 5;
-        const int idx = lo + lane * step;
-        const int x = idx < hi ? __ldg(rel + idx) : INT_MAX;
-        const int k = __popc(__ballot_sync(0xffffffffu, x < v));
-        if (k == 0) return lo;
-        const int nlo = lo + (k - 1) * step + 1;
-        hi = min(lo + k * step, hi);
-        lo = nlo;
-    }
-    const int x = lo + lane < hi ? __ldg(rel + lo + lane) : INT_MAX;
-    return lo + __popc(__ballot_sync(0xffffffffu, x < v));
-}
-
-// One CTA per 16 parent columns; warp w owns parent columns c0 + w and
-// c0 + w + 8 and adds, child after child in a fixed order, the child
-// columns that map onto them.  A column is only ever touched by its warp, so
-// no block barrier and no atomics are needed and the sums are deterministic
-// (the children are added in the reference's order, cholesky.jl:506-514).
-// Each warp finds the child columns that land in its CTA's 16 columns with
-// two warp-cooperative searches of the child's relative indices, then
-// streams each child column in chunks of 4 x 32 rows: the relative indices
-// and child values of the chunk are loaded first, then the 4 parent entries
-// they address, so four independent gather chains are in flight per lane.
-template <typename T>
+// One CTA per (front, 16 parent columns, kEArows parent rows); warp w owns
+// parent columns c0 + w and c0 + w + 8.  The plan lists, per child in the
+// reference's order (reverse, cholesky.jl:506-514), the child columns b0..b1
+// and rows a0..a1 whose relative indices fall in the item's columns and rows,
+// so the kernel does no searching.  Every parent entry belongs to one CTA and
+// one warp, and the children are added in a fixed order: no atomics, no block
+// barrier, deterministic sums.  PART 0 adds into the panel columns (before
+// the front is factored), PART 1 into the update matrix, which the SYRK has
+// already set to -L21 L21^T (so it is never zeroed or read twice).  A child
+// column streams in chunks of 4 x 32 rows: the relative indices and child
+// values of the chunk are loaded first, then the 4 parent entries they
+// address, so four independent gather chains are in flight per lane.
+template <typename T, int PART>
 __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                            const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
+                                            const Item* __restrict__ all_items, const int32_t* __restrict__ reltgt,
                                             T* __restrict__ P, T* __restrict__ M) {
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp, lm = f.ldm;
-    const int c0 = it.a * kEAcols, c1 = min(c0 + kEAcols, nj);
+    const int nn = f.nn, ld = f.ldp, lm = f.ldm;
+    const int c0 = it.a * kEAcols;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T* Pj = P + f.poff;
     T* Mj = M + f.moff;
-    // zero the update-matrix columns this warp owns
-    for (int col = c0 + warp; col < c1; col += 8)
-        if (col >= nn)
-            for (int r = lane; r < na; r += 32) Mj[r + (int64_t)(col - nn) * lm] = T(0);
-    __syncwarp();
-    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
-        const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na, lmc = fc.ldm;
+    const Item* seg = all_items + it.pad;  // segment offsets index the whole item buffer
+    const int nch = f.chd1 - f.chd0;
+    for (int s = 0; s < nch; ++s) {
+        const Item s1 = seg[2 * s], s2 = seg[2 * s + 1];
+        const int b0 = s1.a, b1 = s1.b, a0 = s2.front, a1 = s2.a;
+        if (b0 >= b1 || a1 <= a0) continue;
+        const Front fc = fronts[s1.front];
         const int32_t* __restrict__ rel = reltgt + fc.sep0;
         const T* Mc = M + fc.moff;
-        const int b0 = warp_lower_bound(rel, ma, c0, lane);
-        const int b1 = warp_lower_bound(rel, ma, c1, lane);
         for (int b = b0; b < b1; ++b) {
             const int col = __ldg(rel + b);
             if (((col - c0) & 7) != warp) continue;  // the owner warp of this parent column
-            const T* mc = Mc + (int64_t)b * lmc;
-            T* dst = col < nn ? Pj + (int64_t)col * ld : Mj + (int64_t)(col - nn) * lm - nn;
-            int a = b + lane;
-            for (; a + 96 < ma; a += 128) {
+            const T* mc = Mc + (int64_t)b * fc.ldm;
+            T* dst = PART == 0 ? Pj + (int64_t)col * ld : Mj + (int64_t)(col - nn) * lm - nn;
+            int a = max(a0, b) + lane;
+            for (; a + 96 < a1; a += 128) {
                 int r[4];
                 T v[4], o[4];
 #pragma unroll
@@ -277,7 +258,7 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 #pragma unroll
                 for (int u = 0; u < 4; ++u) dst[r[u]] = o[u] + v[u];
             }
-            for (; a < ma; a += 32) dst[__ldg(rel + a)] += mc[a];
+            for (; a < a1; a += 32) dst[__ldg(rel + a)] += mc[a];
         }
         __syncwarp();
     }
@@ -688,13 +669,17 @@ __device__ __forceinline__ void acc_for_each(const Acc<float>& acc, F&& fn) {
 
 // C(rbase+r, cbase+c) -= acc (or = acc * colscale when OVERWRITE), for
 // r < rmax, c < cmax; on a diagonal tile only row >= col is written.
-template <bool OVERWRITE, typename T>
+// Store an accumulator tile: MODE 0 C -= acc, MODE 1 C = acc (times the
+// column scale if given), MODE 2 C = -acc (the SYRK writes M = -L21 L21^T;
+// the children's extend-add follows it).
+template <int MODE, typename T>
 __device__ __forceinline__ void acc_store(const Acc<T>& acc, T* C, int64_t ldc, int rbase, int cbase, int rmax,
                                           int cmax, bool diag_tile, const T* colscale) {
     acc_for_each(acc, [&](int r, int c, T v) {
         if (r < rmax && c < cmax && (!diag_tile || rbase + r >= cbase + c)) {
             T* p = C + (rbase + r) + (int64_t)(cbase + c) * ldc;
-            if (OVERWRITE) *p = colscale ? v * colscale[c] : v;
+            if (MODE == 1) *p = colscale ? v * colscale[c] : v;
+            else if (MODE == 2) *p = -v;
             else *p -= v;
         }
     });
@@ -719,16 +704,16 @@ __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, 
         const int w = min(kNB, nn - c0);
         const int rs = c0 + it.a * kTile;
         gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, c0, c0 + w, obs, c0, dj);
-        acc_store<false>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, (const T*)nullptr);
+        acc_store<0>(acc, Pj, ld, rs, c0, nj - rs, w, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_TRAIL) {
         const int e = min(nn, obs + obw);
         const int cs = e + it.b * kTile, rs = cs + it.a * kTile;
         gemm_k_loop<T>(acc, smem, Pj, ld, rs, nj, Pj, ld, cs, nn, obs, e, dj);
-        acc_store<false>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, (const T*)nullptr);
+        acc_store<0>(acc, Pj, ld, rs, cs, nj - rs, nn - cs, it.a == 0, (const T*)nullptr);
     } else if (ROLE == G_SYRK) {
         const int rs = it.a * kTile, cs = it.b * kTile;
         gemm_k_loop<T>(acc, smem, Pj + nn, ld, rs, na, Pj + nn, ld, cs, na, 0, nn, dj);
-        acc_store<false>(acc, M + f.moff, f.ldm, rs, cs, na - rs, na - cs, it.a == it.b, (const T*)nullptr);
+        acc_store<2>(acc, M + f.moff, f.ldm, rs, cs, na - rs, na - cs, it.a == it.b, (const T*)nullptr);
     } else {
         // X (rows below the diagonal block, cols [c0, c0+w)) = X * Linv^T (* D^-1)
         const int w = min(kNB, nn - c0);
@@ -741,7 +726,7 @@ __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, 
             for (int i = threadIdx.x; i < w; i += blockDim.x) sc[i] = T(1) / dj[c0 + i];
             __syncthreads();
         }
-        acc_store<true>(acc, Pj + (int64_t)c0 * ld, ld, rs, 0, nj - rs, w, false, LDLT ? (const T*)sc : nullptr);
+        acc_store<1>(acc, Pj + (int64_t)c0 * ld, ld, rs, 0, nj - rs, w, false, LDLT ? (const T*)sc : nullptr);
     }
 }
 
@@ -978,8 +963,8 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         }
         if (lv.ea.cnt) {
             Timer t(h, K_EA);
-            k_ea<T><<<grid_for(lv.ea.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea.off, h->d_reltgt,
-                                                                h->d_chdtgt, fb.P, fb.M);
+            k_ea<T, 0><<<grid_for(lv.ea.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea.off, items,
+                                                                   h->d_reltgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
         if (h->tuning) MF_CUDA(cudaEventRecord(tev[0], h->stream));
@@ -1046,6 +1031,12 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             Timer t(h, K_SYRK);
             k_gemm<T, G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, gs, h->stream>>>(
                 h->d_fronts, items + lv.syrk.off, 0, 0, 0, fb.P, fb.M, fb.d, fb.inv);
+            MF_CUDA(cudaGetLastError());
+        }
+        if (lv.ea_upd.cnt) {
+            Timer t(h, K_EA);
+            k_ea<T, 1><<<grid_for(lv.ea_upd.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea_upd.off, items,
+                                                                       h->d_reltgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
         if (h->tuning) {

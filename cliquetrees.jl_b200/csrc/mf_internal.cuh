@@ -76,6 +76,7 @@ constexpr int kWideFrontNN = 12288;
 constexpr int kTile = 64;       // tile edge of the grouped update kernels
 constexpr int kTM = 128;        // rows of a tensor-core (tcgen05) tile; columns stay kTile
 constexpr int kEAcols = 16;     // parent columns per extend-add work item
+constexpr int kEArows = 1024;   // parent rows per extend-add work item
 constexpr int kSolveRows = 256; // rows per gather work item
 constexpr int kTcSyrkN = 128;   // tile columns of the tensor-core SYRK
 constexpr int kTcTrailN = 128;  // tile columns of the tensor-core trailing update
@@ -103,7 +104,15 @@ struct SolveStep {
 
 struct Level {
     ItemList small;          // (front)           fused small-front kernel
-    ItemList ea;             // (front, col tile) extend-add for blocked fronts
+    // extend-add for blocked fronts, item (front, col tile, row chunk, first
+    // segment): ea adds the children into the panel columns before the
+    // panel is factored; ea_upd adds them into the update matrix after the
+    // SYRK has written M = -L21 L21^T.  Each item's segments (two Items per
+    // child, children in reverse order) are {child, b0, b1}, {a0, a1}: the
+    // child columns b0..b1 and rows a0..a1 whose relative indices land in the
+    // item's columns and rows.
+    ItemList ea;
+    ItemList ea_upd;
     std::vector<PanelStep> steps;
     ItemList syrk;           // (front, ti, tj)   M -= L L^T
     ItemList syrk_tc;        // 128 x 64 tiles for the tcgen05 kernel

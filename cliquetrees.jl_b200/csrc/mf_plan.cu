@@ -330,6 +330,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     auto end = [&](ItemList& l) { l.cnt = (int64_t)items.size() - l.off; };
     auto push = [&](int32_t f, int32_t a, int32_t b) { items.push_back(Item{f, a, b, 0}); };
     std::vector<Item> gseg;  // forward-gather segments, appended after the levels
+    std::vector<Item> easeg; // extend-add segments, appended after them
 
     for (int L = 0; L <= max_level; ++L) {
         Level& lv = h->levels[L];
@@ -341,17 +342,50 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (f.nn + f.na <= kSmallMax) push(j, 0, 0);
         }
         end(lv.small);
-        begin(lv.ea);
         int max_steps = 0;
-        for (int32_t j : fr) {
-            const Front& f = h->h_fronts[j];
-            int nj = f.nn + f.na;
-            if (nj <= kSmallMax) continue;
-            for (int t = 0; t < cdiv(nj, kEAcols); ++t) push(j, t, 0);
-            max_steps = std::max<int>(max_steps, (int)cdiv(f.nn, kNB));
-            lv.max_nn_blocked = std::max(lv.max_nn_blocked, f.nn);
+        for (int part = 0; part < 2; ++part) {
+            ItemList& el = part ? lv.ea_upd : lv.ea;
+            begin(el);
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                const int nj = f.nn + f.na;
+                if (nj <= kSmallMax) continue;
+                if (!part) {
+                    max_steps = std::max<int>(max_steps, (int)cdiv(f.nn, kNB));
+                    lv.max_nn_blocked = std::max(lv.max_nn_blocked, f.nn);
+                }
+                const int nch = f.chd1 - f.chd0;
+                if (nch == 0) continue;
+                for (int t = 0; t < cdiv(nj, kEAcols); ++t) {
+                    const int c0 = t * kEAcols, c1 = std::min(c0 + kEAcols, nj);
+                    const int pc0 = part ? std::max(c0, f.nn) : c0, pc1 = part ? c1 : std::min(c1, f.nn);
+                    if (pc0 >= pc1) continue;
+                    for (int q = 0; pc0 + q * kEArows < nj; ++q) {
+                        const int r0 = pc0 + q * kEArows, r1 = std::min(r0 + kEArows, nj);
+                        std::vector<Item> segs;
+                        bool any = false;
+                        for (int32_t pp = f.chd1 - 1; pp >= f.chd0; --pp) {
+                            const int32_t c = h->h_exec_chd[(size_t)pp];
+                            const Front& fc = h->h_fronts[(size_t)c];
+                            const int32_t* rel = h->h_exec_rel.data() + fc.sep0;
+                            const int32_t* rend = rel + fc.na;
+                            const int b0 = (int)(std::lower_bound(rel, rend, pc0) - rel);
+                            const int b1 = (int)(std::lower_bound(rel, rend, pc1) - rel);
+                            const int a0 = (int)(std::lower_bound(rel, rend, r0) - rel);
+                            const int a1 = (int)(std::lower_bound(rel, rend, r1) - rel);
+                            // rows a >= b of a child column b (lower triangle)
+                            if (b0 < b1 && a1 > std::max(a0, b0)) any = true;
+                            segs.push_back(Item{c, b0, b1, 0});
+                            segs.push_back(Item{a0, a1, 0, 0});
+                        }
+                        if (!any) continue;
+                        items.push_back(Item{j, t, q, (int32_t)easeg.size()});
+                        easeg.insert(easeg.end(), segs.begin(), segs.end());
+                    }
+                }
+            }
+            end(el);
         }
-        end(lv.ea);
         // two-level blocking: outer blocks of kob columns, sub-panels of kNB;
         // levels with a very large front take wider outer blocks (trailing
         // updates with a longer K amortise the tile overheads)
@@ -553,14 +587,19 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     }
     {
         const int64_t base = (int64_t)items.size();
-        if (base + (int64_t)gseg.size() > INT32_MAX) {
+        const int64_t ebase = base + (int64_t)gseg.size();
+        if (ebase + (int64_t)easeg.size() > INT32_MAX) {
             set_error("plan: too many work items");
             return -3;
         }
-        for (const Level& lv : h->levels)
+        for (const Level& lv : h->levels) {
             for (int64_t i = lv.s_gather.off; i < lv.s_gather.off + lv.s_gather.cnt; ++i)
                 items[(size_t)i].b += (int32_t)base;
+            for (const ItemList* el : {&lv.ea, &lv.ea_upd})
+                for (int64_t i = el->off; i < el->off + el->cnt; ++i) items[(size_t)i].pad += (int32_t)ebase;
+        }
         items.insert(items.end(), gseg.begin(), gseg.end());
+        items.insert(items.end(), easeg.begin(), easeg.end());
     }
     begin(h->inv2_items);
     for (int64_t e = 0; e < (int64_t)h->h_fronts.size(); ++e) {

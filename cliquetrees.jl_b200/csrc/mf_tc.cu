@@ -468,7 +468,9 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
             const int ldc = (int)tg.ldc;
             float* cblk = tg.C + row + (int64_t)cbase * ldc;
             float cv[HC];
-            if (ROLE != TC_TRSM) {
+            // the SYRK writes M = -L21 L21^T without reading it (the extend-add
+            // of the children into M follows it); the panel roles update C
+            if (ROLE != TC_TRSM && ROLE != TC_SYRK) {
 #pragma unroll
                 for (int q = 0; q < HC; ++q) {
                     const int col = cbase + q;
@@ -494,6 +496,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
                     if (row_ok && col >= tg.clo && col < tg.chi && (!tg.tri || row >= col)) {
                         float* p = cblk + (cb + q) * ldc;
                         if (ROLE == TC_TRSM) *p = LDLT ? v[q] / dj[col] : v[q];
+                        else if (ROLE == TC_SYRK) *p = -v[q];
                         else *p = cv[cb + q] - v[q];
                     }
                 }
