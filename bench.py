@@ -274,14 +274,20 @@ CLASS_KERNELS = {
 
 
 def work_model(nn, na, par, w):
-    """Algorithmic work of one factorization and one solve pass per kernel
-    class, counted from the execution fronts (never from measurements):
-    flops nn^3/3 + nn^2 na (panel roles) and nn na^2 (SYRK) for blocked
-    fronts (nj > 96), all three for the fused small fronts; extend-add bytes
-    2 w na_c (na_c + 1) / 2 per child c of a blocked front (read the child's
-    triangle, write the parent slot once); solve bytes w x factor entries
-    read per sweep (forward and backward), split by the kernels that read
-    them."""
+    """Algorithmic work of one factorization and one solve pass per kernel,
+    counted from the execution fronts (never from measurements).
+
+    Blocked fronts (nj > 96) are walked through the device schedule: 64-column
+    sub-panels inside outer blocks of 256 columns (512 for fronts of at least
+    12,288 columns).  Per sub-panel k0 of width w: diag w^3/3 (factor of the
+    diagonal block), panel (nj - k0 - w) w^2 (the triangular solve below it),
+    left 2 K w (nj - k0 - w/2) with K the outer block's earlier columns; per
+    outer block the trailing update 2 K sum_c (nj - c) over the columns after
+    it; the SYRK nn na^2.  These add up to nn^3/3 + nn^2 na + nn na^2 (plus
+    lower-order terms).  Fused small fronts: all three terms.  Extend-add
+    bytes: 2 w na_c (na_c + 1) / 2 per child c of a blocked front (read the
+    child's triangle, write the parent slot once).  Solve bytes: w x factor
+    entries per sweep, split by the kernels that read them."""
     nnf = nn.astype(np.float64)
     naf = na.astype(np.float64)
     big = (nn + na) > 96
@@ -291,9 +297,26 @@ def work_model(nn, na, par, w):
     blk_par[has] = big[par[has]]
     diag_e = nnf * (nnf + 1) / 2
     off_e = nnf * naf
+    fl = {"diag": 0.0, "panel": 0.0, "left": 0.0, "update": 0.0}
+    for a, b in zip(nn[big].tolist(), na[big].tolist()):
+        nj = a + b
+        kob = 512 if a >= 12288 else 256
+        for obs in range(0, a, kob):
+            obe = min(a, obs + kob)
+            for k0 in range(obs, obe, 64):
+                wd = min(64, a - k0)
+                fl["diag"] += wd ** 3 / 3.0
+                fl["panel"] += (nj - k0 - wd) * wd * wd
+                fl["left"] += 2.0 * (k0 - obs) * wd * (nj - k0 - wd / 2.0)
+            if obe < a:
+                m = a - obe  # columns obe .. a-1, column c has nj - c rows
+                fl["update"] += 2.0 * (obe - obs) * (m * nj - (obe * m + m * (m - 1) / 2.0))
     return {
         "small": {"flops": float(np.sum((nnf ** 3 / 3 + nnf * nnf * naf + nnf * naf * naf)[~big]))},
-        "panel+update": {"flops": float(np.sum((nnf ** 3 / 3 + nnf * nnf * naf)[big]))},
+        "diag": {"flops": fl["diag"]},
+        "panel": {"flops": fl["panel"]},
+        "left": {"flops": fl["left"]},
+        "update": {"flops": fl["update"]},
         "syrk": {"flops": float(np.sum((nnf * naf * naf)[big]))},
         "extend_add": {"bytes": float(2 * w * np.sum((naf * (naf + 1) / 2)[blk_par]))},
         # per solve pass
@@ -442,8 +465,11 @@ def rooflines(form, peaks, fp64_peak):
             "kernels run 3 TF32 passes per product)" if mixed else "cuBLAS DGEMM 8192^3 measured in this run")
     classes = {
         "syrk": ("tensor", wm["syrk"]["flops"], ["syrk"]),
-        "panel+update": ("tensor", wm["panel+update"]["flops"], ["panel", "update", "diag", "left"]),
-        "small": ("tensor", wm["small"]["flops"], ["small"]),
+        "update": ("tensor", wm["update"]["flops"], ["update"]),
+        "left": ("tensor", wm["left"]["flops"], ["left"]),
+        "panel": ("tensor", wm["panel"]["flops"], ["panel"]),
+        "diag": ("latency", wm["diag"]["flops"], ["diag"]),
+        "small": ("latency", wm["small"]["flops"], ["small"]),
         "extend_add": ("hbm", wm["extend_add"]["bytes"], ["extend_add"]),
         "solve_small": ("hbm", wm["solve_small"]["bytes"] * passes, ["solve_small"]),
         "solve_fwd": ("hbm", wm["solve_fwd"]["bytes"] * passes, ["solve_fwd"]),
@@ -456,7 +482,10 @@ def rooflines(form, peaks, fp64_peak):
         launches = sum(kt[k]["launches"] for k in ks)
         if ms <= 0 or launches == 0:
             continue
-        if bound == "tensor":
+        if bound in ("tensor", "latency"):
+            # latency-bound kernels (one CTA per front: the 64x64 diagonal
+            # blocks, the fused small fronts) are still held against the
+            # tensor rate their flops would need
             ach, unit, peak, src = work / (ms / 1e3) / 1e12, "TFLOP/s", tpk, tsrc
         else:
             ach, unit, peak, src = work / (ms / 1e3) / 1e9, "GB/s", hbm, "hbm_gbs of MEASURED_PEAKS.json"
@@ -884,9 +913,12 @@ def run_form(args, work, *, mixed, local, world, profile_only=False):
     if mixed:
         _native.check(lib.mf_solve_refined(h, _native.ptrd(Xtmp), 0, n, _native.ptr64(perm_np), tol, maxit,
                                            ctypes.byref(iters), ctypes.byref(eta_dev)), "perm upload")
-    # the mixed form must reach 1e-12; the plain FP64 form is the reference's
-    # arithmetic (static pivots for LDLt), so it only has to be a solution
-    if info.value != 0 or not eta <= (1e-12 if mixed else 1e-8):
+    # bars: mixed form 1e-12; plain FP64 form 1e-13, except the KKT LDLt of
+    # config 4, where the reference's own static-pivot arithmetic reaches only
+    # about 2e-11 to 5e-11 (the CPU oracle at grid sides 16 to 24), so its bar
+    # is 1e-10
+    bar = 1e-12 if mixed else (1e-10 if work.diag else 1e-13)
+    if info.value != 0 or not eta <= bar:
         raise SystemExit(f"bench: check failed (mixed={mixed}, info={info.value}, backward error={eta})")
 
     # profiling pass (per-kernel events; not the timed pass)
