@@ -70,8 +70,9 @@ def parse():
     ap.add_argument("--side", type=int, default=None, help="grid side of configs 2 and 4 (default 80 / 40)")
     ap.add_argument("--nrhs", type=int, default=None)
     ap.add_argument("--batch", type=int, default=4096, help="config 3: matrices per batch")
-    ap.add_argument("--requests", type=int, default=600, help="config 5: requests per arrival rate")
-    ap.add_argument("--rates", default="50,200,1000", help="config 5: Poisson arrival rates (requests/s)")
+    ap.add_argument("--requests", type=int, default=20000, help="config 5: requests per arrival rate")
+    ap.add_argument("--rates", default="", help="config 5: Poisson arrival rates (requests/s); default 50%% "
+                                                "and 80%% of the measured saturation rate")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-budget", type=float, default=400.0,
                     help="reference arm: seconds of CPU oracle runs (warm-up included)")
@@ -633,110 +634,162 @@ def seg_backward_error(A, X, B, segments=None):
     return float((rm / (an * xm + bm)).max())
 
 
+class FreshGrid:
+    """Fresh seeded coefficients on a fixed grid pattern, per request: edge
+    weights log-uniform [lo, hi], diagonal = row sum + shift, written
+    straight into the lower-triangle CSC order the server assembles (the
+    positions are found once per pattern)."""
+
+    def __init__(self, nx, ny, nz, lo=0.1, hi=10.0, shift=1e-2):
+        from multifrontal import testmatrices as tm
+        self.i, self.j = tm.grid_edges(nx, ny, nz)  # i < j
+        n = nx * ny * nz
+        m = self.i.size
+        self.n, self.lo, self.hi, self.shift = n, lo, hi, shift
+        import scipy.sparse as sp
+        code = np.concatenate([np.arange(1, m + 1), -np.arange(1, n + 1)]).astype(np.float64)
+        rows = np.concatenate([self.j, np.arange(n)])
+        cols = np.concatenate([self.i, np.arange(n)])
+        L = sp.csc_matrix((code, (rows, cols)), shape=(n, n))
+        L.sort_indices()
+        c = L.data.astype(np.int64)
+        self.nnz = c.size
+        self.pos_edge = np.empty(m, np.int64)
+        self.pos_edge[c[c > 0] - 1] = np.nonzero(c > 0)[0]
+        self.pos_diag = np.empty(n, np.int64)
+        self.pos_diag[-c[c < 0] - 1] = np.nonzero(c < 0)[0]
+
+    def values(self, seed):
+        rng = np.random.default_rng(seed)
+        w = np.exp(rng.uniform(np.log(self.lo), np.log(self.hi), size=self.i.size))
+        v = np.empty(self.nnz, np.float64)
+        v[self.pos_edge] = -w
+        deg = np.bincount(self.i, w, minlength=self.n) + np.bincount(self.j, w, minlength=self.n)
+        v[self.pos_diag] = deg + self.shift
+        return v
+
+    def matrix(self, seed):
+        """The same matrix as a symmetric CSC (for host-side checks)."""
+        import scipy.sparse as sp
+        rng = np.random.default_rng(seed)
+        w = np.exp(rng.uniform(np.log(self.lo), np.log(self.hi), size=self.i.size))
+        deg = np.bincount(self.i, w, minlength=self.n) + np.bincount(self.j, w, minlength=self.n)
+        A = sp.coo_matrix((np.concatenate([-w, -w, deg + self.shift]),
+                           (np.concatenate([self.i, self.j, np.arange(self.n)]),
+                            np.concatenate([self.j, self.i, np.arange(self.n)]))), shape=(self.n, self.n))
+        return sp.csc_matrix(A)
+
+
 def run_serving(args, local, world):
     """Config 5: a Poisson stream of factor+solve requests over six patterns
-    through the serving loop (multifrontal.serve), swept over arrival rate;
-    beside it the plain FP64 form, one request at a time on one stream."""
+    through the serving loop (multifrontal.serve), swept over arrival rate.
+    Every request carries fresh seeded coefficients (log-uniform [0.1, 10],
+    diagonal = row sum + 1e-2) and 1-16 fresh N(0,1) right-hand sides, both
+    generated when the request is admitted.  Rounds merge requests of the
+    patterns of one size class into one forest.  Beside it the plain FP64
+    form, one request at a time on one stream, on the first requests of the
+    same stream."""
     import multifrontal as mf
     from multifrontal import serve
     from multifrontal import testmatrices as tm
 
-    specs = {  # key: (grid, batch per handle, ordering)
-        "2d5pt_64": ((64, 64, 1), 16, "amf"), "2d5pt_128": ((128, 128, 1), 8, "amf"),
-        "2d5pt_256": ((256, 256, 1), 2, "amf"), "2d5pt_512": ((512, 512, 1), 1, "amf"),
-        "3d7pt_16": ((16, 16, 16), 16, "nd"), "3d7pt_48": ((48, 48, 48), 1, "nd"),
+    specs = {  # key: (grid, most requests per round, size class)
+        "2d5pt_64": ((64, 64, 1), 16, 0), "2d5pt_128": ((128, 128, 1), 8, 0),
+        "2d5pt_256": ((256, 256, 1), 4, 1), "2d5pt_512": ((512, 512, 1), 1, 2),
+        "3d7pt_16": ((16, 16, 16), 16, 0), "3d7pt_48": ((48, 48, 48), 1, 2),
     }
-    pools = {}   # per pattern: 4 seeded coefficient sets (log-uniform [0.1, 10], diag + 1e-2)
-    mats = {}
-    for k, ((nx, ny, nz), _, _) in specs.items():
-        mats[k] = [tm.grid_laplacian(nx, ny, nz, seed=100 + s, lo=0.1, hi=10.0, shift=1e-2) for s in range(4)]
-    rhs_cache = {}
+    gens = {k: FreshGrid(*g) for k, (g, _, _) in specs.items()}
+    keys = list(specs)
+    nreq = args.requests
+    keep_every = max(1, nreq // 60)  # requests whose solution is kept and checked on the host
 
-    def rhs_for(n, kk):
-        if (n, kk) not in rhs_cache:
-            rhs_cache[(n, kk)] = tm.rhs(n, kk, seed=kk)
-        return rhs_cache[(n, kk)]
-
-    def make_server(mixed, batched, workers):
-        srv = serve.Server(mixed=mixed, device=local, workers=workers)
-        for k, ((nx, ny, nz), b, o) in specs.items():
-            order = mf.grid_nd_order(nx, ny, nz) if o == "nd" else "amf"
-            srv.add_pattern(k, mats[k][0], order=order, batch=b if batched else 1)
-            if k not in pools:
-                pools[k] = [srv.lower_values(k, A) for A in mats[k]]
+    def make_server(mixed, merge):
+        srv = serve.Server(mixed=mixed, device=local, workers=4 if merge else 1)
+        for k, ((nx, ny, nz), b, cls) in specs.items():
+            srv.add_pattern(k, gens[k].matrix(0), order="amf", batch=b if merge else 1, size_class=cls)
         return srv
 
     def stream(count, rate, seed):
         rng = np.random.default_rng(seed)
-        keys = list(specs)
         t, reqs = 0.0, []
         for i in range(count):
             k = keys[rng.integers(len(keys))]
-            n = mats[k][0].shape[0]
             kk = int(rng.integers(1, 17))
             t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
-            reqs.append(serve.Request(i, k, pools[k][i % 4], rhs_for(n, kk), arrival=t))
+            cs, rs = 10 ** 6 + 7919 * i + seed, 2 * 10 ** 6 + 104729 * i + seed
+            r = serve.Request(i, k, None, None, arrival=t)
+            r.make_values = (lambda g=gens[k], cs=cs: g.values(cs))
+            r.make_rhs = (lambda n=gens[k].n, kk=kk, rs=rs: tm.rhs(n, kk, seed=rs))
+            r.keep = (i % keep_every == 0)
+            r.coef_seed = cs
+            reqs.append(r)
         return reqs
 
     def check(done):
         worst = 0.0
-        for r in done[:: max(1, len(done) // 40)]:
-            A = mats[r.key][r.rid % 4]
+        for r in done:
+            if r.X is None:
+                continue
+            A = gens[r.key].matrix(r.coef_seed)
             worst = max(worst, float(tm.backward_error(A, r.X, r.B).max()))
         return worst
 
-    rates = [float(x) for x in args.rates.split(",") if x]
-    srv = make_server(True, True, 4)
-    srv.warm(per_pattern=2)  # both handles of every pattern exist before the timed streams
-    sweep = []
-    for rate in rates:
-        reqs = stream(args.requests, rate, seed=int(rate))
-        done = srv.serve(reqs, realtime=True)
+    def run(srv, reqs, realtime):
+        done = srv.serve(reqs, realtime=realtime, timeout=3600)
         st = serve.latency_stats(done)
-        sweep.append({"rate": rate, "requests": len(done), "requests_per_s": len(done) / srv.wall,
-                      "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "backward_error": check(done),
-                      "mean_batch": float(np.mean([r.batch_size for r in done]))})
-    sat_reqs = stream(args.requests, 0.0, seed=1)
-    done = srv.serve(sat_reqs, realtime=False)
-    sat = {"requests_per_s": len(done) / srv.wall, "backward_error": check(done),
-           **serve.latency_stats(done), "mean_batch": float(np.mean([r.batch_size for r in done]))}
+        out = {"requests": len(done), "requests_per_s": len(done) / srv.wall, "p50_ms": st["p50_ms"],
+               "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+               "backward_error": max(check(done), max(r.eta for r in done)),
+               "mean_round": float(np.mean([r.batch_size for r in done])),
+               "merged_rounds": int(sum(1 for c in srv.rounds if len(c) > 1)), "rounds": len(srv.rounds)}
+        return out
+
+    srv = make_server(True, True)
+    srv.warm()
+    sat = run(srv, stream(nreq, 0.0, seed=1), realtime=False)
+    rates = [float(x) for x in args.rates.split(",") if x] if args.rates else [0.5 * sat["requests_per_s"],
+                                                                             0.8 * sat["requests_per_s"]]
+    sweep = []
+    for q, rate in enumerate(rates):
+        sweep.append({"rate": rate, **run(srv, stream(nreq, rate, seed=100 + q), realtime=True)})
+    dev_bytes = int(srv.bytes)
     srv.close()
-    plain = make_server(False, False, 1)
-    plain.warm()
-    m = max(60, args.requests // 5)
-    done_p = plain.serve(stream(m, 0.0, seed=1), realtime=False)
-    plain_line = {"requests_per_s": len(done_p) / plain.wall, "requests": len(done_p),
-                  "backward_error": check(done_p), **serve.latency_stats(done_p)}
+    plain = make_server(False, False)
+    plain.warm(counts=[1])
+    m = max(60, nreq // 10)
+    plain_line = run(plain, stream(m, 0.0, seed=1), realtime=False)
     plain.close()
     return {
         "metric": "requests_per_s", "value": sat["requests_per_s"], "unit": "requests/s", "n_gpus": world,
-        "steps": args.requests, "warmup": 1, "ms_per_step": 1e3 / sat["requests_per_s"],
+        "steps": nreq, "warmup": 1, "ms_per_step": 1e3 / sat["requests_per_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": "serving_6patterns_poisson", "patterns": {k: {"grid": v[0], "batch": v[1],
-                                                                              "ordering": v[2]}
-                                                                          for k, v in specs.items()},
-                   "rhs_per_request": "U{1..16}", "coefficients": "4 seeded log-uniform [0.1,10] sets per pattern",
+        "config": {"workload": "serving_6patterns_poisson", "requests_per_rate": nreq,
+                   "patterns": {k: {"grid": v[0], "max_per_round": v[1], "size_class": v[2], "ordering": "AMF"}
+                                for k, v in specs.items()},
+                   "rhs_per_request": "U{1..16}, fresh N(0,1) per request",
+                   "coefficients": "fresh seeded log-uniform [0.1,10] per request, diagonal = row sum + 1e-2",
                    "mem_cap_gb": 120, "workers": 4},
         "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"], "backward_error": sat["backward_error"],
-        "saturation": sat, "sweep": sweep, "plain_fp64_one_at_a_time": plain_line,
+        "saturation": sat, "sweep": sweep, "device_bytes": dev_bytes,
+        "plain_fp64_one_at_a_time": {**plain_line, "note": f"the first {m} requests of the saturation stream"},
         "served_over_plain": sat["requests_per_s"] / plain_line["requests_per_s"],
         "e2e": {"value": sat["requests_per_s"], "unit": "requests/s", "h2d_bytes_per_step": None,
                 "d2h_bytes_per_step": None, "note": "every request moves its values and RHS from host buffers"},
     }
 
 
-# served batched form per config: (matrices per device handle, workers, requests)
+# served batched form per config: (requests of the pattern per round, workers, requests)
 SERVED = {1: (32, 4, 1024), 2: (8, 2, 32), 4: (2, 2, 8)}
 
 
 def run_served(args, work, local):
     """The served mixed-precision batched form on this config's pattern:
-    factor+solve requests carrying the config's right-hand sides and one of
-    four coefficient sets of the same pattern (the matrix and three seeded
-    congruences D A D, D = diag(exp(0.1 z)), which keep its pattern,
-    symmetry and inertia), batched B per device handle as one forest and
-    run by W workers on their own streams.  Saturation throughput comes from
-    all requests queued at once; latency from Poisson arrivals at 70% of it."""
+    factor+solve requests carrying the config's right-hand sides and fresh
+    per-request values on the config's pattern (a seeded congruence D A D,
+    D = diag(exp(0.1 z)), which keeps the pattern, symmetry and inertia),
+    up to B per round as one forest, W workers on their own streams.
+    Saturation throughput comes from all requests queued at once; latency
+    from Poisson arrivals at 70% of it."""
     import scipy.sparse as sp
     from multifrontal import serve
     from multifrontal import testmatrices as tm
@@ -744,13 +797,20 @@ def run_served(args, work, local):
     B, W, R = SERVED[args.config]
     srv = serve.Server(mixed=True, device=local, workers=W)
     srv.add_pattern("cfg", work.A, batch=B, ldlt=bool(work.diag), symbolic_result=(work.P, work.S))
-    mats = [work.A]
+    base = srv.lower_values("cfg", work.A)
+    Lo = sp.tril(sp.csc_matrix(work.A), format="csc")
+    Lo.sort_indices()
     n = work.A.shape[0]
-    for s in (11, 12, 13):
-        dv = np.exp(0.1 * np.random.default_rng(s).standard_normal(n))
-        D = sp.diags(dv)
-        mats.append(sp.csc_matrix(D @ work.A @ D))
-    pool = [srv.lower_values("cfg", M) for M in mats]
+    lrow = Lo.indices.astype(np.int64)
+    lcol = np.repeat(np.arange(n, dtype=np.int64), np.diff(Lo.indptr))
+
+    def dvec(seed):
+        return np.exp(0.1 * np.random.default_rng(seed).standard_normal(n))
+
+    def values(seed):
+        dv = dvec(seed)
+        return base * dv[lrow] * dv[lcol]
+
     srv.warm(per_pattern=min(2, W))
 
     def stream(count, rate, seed):
@@ -758,13 +818,17 @@ def run_served(args, work, local):
         t, reqs = 0.0, []
         for i in range(count):
             t += rng.exponential(1.0 / rate) if rate > 0 else 0.0
-            reqs.append(serve.Request(i, "cfg", pool[i % 4], work.B, arrival=t))
+            r = serve.Request(i, "cfg", None, work.B, arrival=t)
+            r.make_values = (lambda s=1000 * seed + i: values(s))
+            r.coef_seed = 1000 * seed + i
+            reqs.append(r)
         return reqs
 
     def worst(done):
         eta = max(r.eta for r in done)
-        for r in done[:: max(1, len(done) // 8)]:
-            eta = max(eta, float(tm.backward_error(mats[r.rid % 4], r.X, r.B).max()))
+        for r in done[:: max(1, len(done) // 4)]:
+            D = sp.diags(dvec(r.coef_seed))
+            eta = max(eta, float(tm.backward_error(sp.csc_matrix(D @ work.A @ D), r.X, r.B).max()))
         return eta
 
     done = srv.serve(stream(R, 0.0, 1), realtime=False)
@@ -772,11 +836,11 @@ def run_served(args, work, local):
     sat_eta = worst(done)
     done2 = srv.serve(stream(R, 0.7 * sat, 2), realtime=True)
     st = serve.latency_stats(done2)
-    out = {"solves_per_s": sat, "unit": "solves/s", "batch_per_handle": B, "workers": W, "requests": R,
+    out = {"solves_per_s": sat, "unit": "solves/s", "max_per_round": B, "workers": W, "requests": R,
            "backward_error": max(sat_eta, worst(done2)), "latency_at_70pct_load": {**st, "rate": 0.7 * sat},
-           "mean_batch": float(np.mean([r.batch_size for r in done])),
+           "mean_round": float(np.mean([r.batch_size for r in done])),
            "device_bytes": int(srv.bytes),
-           "note": "host buffers in and out for every request (values, RHS, solution)"}
+           "note": "host buffers in and out for every request (values, RHS, solution); fresh values per request"}
     srv.close()
     return out
 

@@ -17,7 +17,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "multifrontal")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-GPU_SOURCES = ["mf_plan.cu", "mf_factor.cu", "mf_tc.cu", "mf_solve.cu", "mf_refine.cu", "mf_api.cu", "mf_static.cu"]
+GPU_SOURCES = ["mf_plan.cu", "mf_factor.cu", "mf_tc.cu", "mf_solve.cu", "mf_refine.cu", "mf_api.cu", "mf_static.cu",
+               "mf_selinv.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -52,7 +53,8 @@ def build_gpu(verbose=False, force=False, ptxas_verbose=False):
     target = os.path.join(OUT, "libmfgpu.so")
     if force or _stale(target, src + hdr):
         cmd = [NVCC, "-O3", "-std=c++17", "-lineinfo", "-shared", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
-               "--expt-relaxed-constexpr"] + GENCODE + ["-o", target] + src
+               "--expt-relaxed-constexpr"] + GENCODE + ["-o", target] + src + [
+                   "-lcublas", "-Xlinker", "-rpath," + os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")]
         if ptxas_verbose:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd, verbose)

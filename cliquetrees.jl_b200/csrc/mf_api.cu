@@ -1,9 +1,12 @@
 // C ABI of the B200 multifrontal numeric phase (include/mfgpu.h).
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <cstring>
 #include <cstdlib>
 #include <new>
+
+#include <cublas_v2.h>
 
 #include "../../include/mfgpu.h"
 #include "mf_internal.cuh"
@@ -51,8 +54,10 @@ void free_all(mf_handle* h) {
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
                     h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
-                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet};
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued};
     release_graphs(h);
+    if (h->cublas) cublasDestroy(static_cast<cublasHandle_t>(h->cublas));
+    h->cublas = nullptr;
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -61,6 +66,7 @@ void free_all(mf_handle* h) {
 int init_info(mf_handle* h) {
     static const long long big = LLONG_MAX;
     MF_CUDA(cudaMemcpyAsync(h->d_info, &big, sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+    MF_CUDA(cudaMemsetAsync(h->d_rescued, 0, sizeof(int), h->stream));
     return 0;
 }
 
@@ -161,6 +167,7 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     rc = rc ? rc : dalloc(h, &h->d_d, std::max<int64_t>(n, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_info, 1, &tot);
     rc = rc ? rc : dalloc(h, &h->d_err, 1, &tot);
+    rc = rc ? rc : dalloc(h, &h->d_rescued, 1, &tot);
     rc = rc ? rc : dalloc(h, &h->d_R, std::max<int64_t>(h->nrval_per_rhs * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_W, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_part, std::max<int64_t>(h->nbwd_part * kNB * 16, 1), &tot);
@@ -183,6 +190,7 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
     if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->d_rescued, 0, sizeof(int));
     if (e == cudaSuccess && n) {  // the permutation a NULL perm argument stands for, until one is passed
         std::vector<int64_t> iota((size_t)n);
         for (int64_t i = 0; i < n; ++i) iota[(size_t)i] = i;
@@ -598,6 +606,10 @@ int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* us
     if (!h) { set_error("null handle"); return -1; }
     if (!h->mixed) { set_error("mf_factorize_mixed: call mf_enable_mixed first"); return -1; }
     if (!h->cur_nz) { set_error("mf_factorize_mixed: no values (mf_assemble)"); return -1; }
+    if (h->reg.delta >= 0.0) {
+        set_error("mf_factorize_mixed: dynamic regularization applies to the FP64 factorization (mf_factorize)");
+        return -1;
+    }
     DeviceGuard g(h->device);
     const double* ds = nullptr;
     int rc;
@@ -918,6 +930,39 @@ int mf_exec_sizes(const mf_handle* h, int64_t* nn, int64_t* na) {
         if (nn) nn[e] = h->h_fronts[e].nn;
         if (na) na[e] = h->h_fronts[e].na;
     }
+    return 0;
+}
+
+int mf_set_regularization(mf_handle* h, int mode, double delta, double epsilon) {
+    if (!h || (mode != 0 && mode != 1)) { set_error("mf_set_regularization: bad arguments"); return -1; }
+    if (mode == 0) {
+        h->reg = Reg();
+    } else {
+        // defaults of DynamicRegularization{Float64}: cbrt(eps), sqrt(eps)
+        const double eps = 2.220446049250313e-16;
+        h->reg.delta = delta < 0 ? std::cbrt(eps) : delta;
+        h->reg.eps = epsilon < 0 ? std::sqrt(eps) : epsilon;
+    }
+    release_graphs(h);  // captured factorizations hold the previous rule
+    return 0;
+}
+
+int mf_selinv(mf_handle* h) {
+    if (!h) { set_error("null handle"); return -1; }
+    DeviceGuard g(h->device);
+    int rc = launch_selinv(h);
+    if (rc) return rc;
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int mf_rescued(mf_handle* h, int64_t* count) {
+    if (!h || !count) { set_error("mf_rescued: bad arguments"); return -1; }
+    DeviceGuard g(h->device);
+    int v = 0;
+    MF_CUDA(cudaMemcpyAsync(&v, h->d_rescued, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    *count = v;
     return 0;
 }
 

@@ -45,6 +45,10 @@ __device__ __forceinline__ bool pivot_ok(double s, double p) {
     return p != 0.0;
 }
 
+__device__ __forceinline__ double reg_pivot(const Reg& r, double s, double p) {
+    return (s * p < r.eps) ? r.delta * s : p;
+}
+
 __device__ __forceinline__ double pivot_sign(const double* signs, int ldlt, int64_t col) {
     if (!ldlt) return 1.0;
     return signs ? signs[col] : 0.0;
@@ -133,24 +137,32 @@ __global__ void k_panel32_to_dl(const Front* __restrict__ fronts, const RefFront
 // ---------------------------------------------------------------------------
 // small fronts: whole frontal matrix in shared memory
 // ---------------------------------------------------------------------------
-template <typename T, int LDLT>
-__global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                               const int32_t* __restrict__ reltgt,
-                                               const int32_t* __restrict__ chdtgt, T* __restrict__ P,
-                                               T* __restrict__ M, T* __restrict__ d,
-                                               const double* __restrict__ signs, long long* __restrict__ info) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* F = reinterpret_cast<T*>(smem_raw);
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
+// Thresholds of the single-precision factorization's pivot check (mixed form,
+// whose matrix is scaled to unit diagonal): a pivot that lost more than five
+// of FP32's seven digits to cancellation against its diagonal entry, or grew
+// beyond 1e7 times the largest diagonal entry of its block, flags the front
+// (or 64 x 64 diagonal block), which is then factored again in FP64.
+constexpr double kRescueSmall = 1e-5;
+constexpr double kRescueGrowth = 1e7;
+
+// One small front held in shared memory as TC: load the assembled panel, add
+// the children (in the reference's reverse order), factor the first nn
+// columns right-looking.  Returns the first rejected pivot (front-local) or
+// -1; with `check`, *flag is set when a pivot is small or grown (see above).
+// Uniform across the block.
+template <typename TC, typename T, int LDLT>
+__device__ int small_front(TC* F, const Front& f, const Front* __restrict__ fronts,
+                           const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
+                           const T* __restrict__ P, const T* __restrict__ M, const double* __restrict__ signs,
+                           bool check, int* flag, Reg reg) {
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
-    T* Pj = P + f.poff;
+    const T* Pj = P + f.poff;
     for (int i = tid; i < nj * nn; i += nt) {
         int r = i % nj, c = i / nj;
-        F[i] = Pj[r + (int64_t)c * ld];
+        F[i] = (TC)Pj[r + (int64_t)c * ld];
     }
-    for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = T(0);
+    for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = TC(0);
     __syncthreads();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
@@ -160,47 +172,111 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
         const T* Mc = M + fc.moff;
         for (int i = tid; i < ma * ma; i += nt) {
             int a = i % ma, b = i / ma;
-            if (a >= b) F[rel[a] + rel[b] * nj] += Mc[a + b * lm];
+            if (a >= b) F[rel[a] + rel[b] * nj] += (TC)Mc[a + b * lm];
         }
         __syncthreads();
     }
     // right-looking partial factorization of the first nn columns
     for (int k = 0; k < nn; ++k) {
-        T piv = F[k + k * nj];
+        TC piv = F[k + k * nj];
         double s = pivot_sign(signs, LDLT, f.col0 + k);
-        if (!pivot_ok(s, (double)piv) || (!LDLT && !(piv > T(0)))) {
-            if (tid == 0) atomicMin(info, (long long)(f.col0 + k + 1));
-            return;  // uniform across the block
+        if (reg.delta >= 0.0) {
+            piv = (TC)reg_pivot(reg, s, (double)piv);
+            if (piv == TC(0)) return k;  // uniform across the block
+        } else if (!pivot_ok(s, (double)piv) || (!LDLT && !(piv > TC(0)))) {
+            return k;  // uniform across the block
         }
-        T dk = LDLT ? piv : sqrt(piv);
-        T inv = T(1) / dk;
+        if (check && tid == 0) {
+            // the original diagonal entry of column k is still in the panel
+            const double a0 = fabs((double)Pj[k + (int64_t)k * ld]);
+            const double ap = fabs((double)piv);
+            if (ap < kRescueSmall * a0 || ap > kRescueGrowth * fmax(a0, 1.0)) *flag = 1;
+        }
+        TC dk = LDLT ? piv : sqrt(piv);
+        TC inv = TC(1) / dk;
         __syncthreads();
-        if (tid == 0) {
-            if (LDLT) d[f.col0 + k] = piv; else F[k + k * nj] = dk;
-        }
+        if (tid == 0) F[k + k * nj] = LDLT ? piv : dk;
         for (int i = k + 1 + tid; i < nj; i += nt) F[i + k * nj] *= inv;
         __syncthreads();
         const int m = nj - k - 1;
         for (int i = tid; i < m * m; i += nt) {
             int r = k + 1 + i % m, c = k + 1 + i / m;
             if (r >= c) {
-                T lc = F[c + k * nj];
+                TC lc = F[c + k * nj];
                 if (LDLT) lc *= piv;
                 F[r + c * nj] -= F[r + k * nj] * lc;
             }
         }
         __syncthreads();
     }
+    return -1;
+}
+
+// Write a factored small front back: panel, update matrix, LDLt pivots (the
+// diagonal of the factored panel holds them: the unit diagonal of L is
+// implied and the LDLt panel diagonal keeps d_k).
+template <typename TC, typename T, int LDLT>
+__device__ void small_front_store(const TC* F, const Front& f, T* __restrict__ P, T* __restrict__ M,
+                                 T* __restrict__ d) {
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    T* Pj = P + f.poff;
     for (int i = tid; i < nj * nn; i += nt) {
         int r = i % nj, c = i / nj;
-        Pj[r + (int64_t)c * ld] = F[i];
+        Pj[r + (int64_t)c * ld] = (T)F[i];
     }
+    if (LDLT)
+        for (int k = tid; k < nn; k += nt) d[f.col0 + k] = (T)F[k + k * nj];
     T* Mj = M + f.moff;
     const int lm = f.ldm;
     for (int i = tid; i < na * na; i += nt) {
         int a = i % na, b = i / na;
-        Mj[a + b * lm] = F[(nn + a) + (nn + b) * nj];
+        Mj[a + b * lm] = (T)F[(nn + a) + (nn + b) * nj];
     }
+}
+
+// small fronts (nj <= kSmallMax): one CTA holds the whole front in shared
+// memory.  Single precision: a front whose factorization rejects a pivot or
+// flags a small or grown pivot is factored again from its inputs in FP64 in
+// the same shared memory (fronts of nj <= kSmallRescue, whose FP64 front fits
+// the FP32 buffer; the panel and the children's update matrices are only
+// read before the final store, so the inputs are intact), and the FP64
+// result is stored rounded to FP32.  A rejection in FP64 -- or in FP32 for a
+// larger front -- is reported through info.
+constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
+
+template <typename T, int LDLT>
+__global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                               const int32_t* __restrict__ reltgt,
+                                               const int32_t* __restrict__ chdtgt, T* __restrict__ P,
+                                               T* __restrict__ M, T* __restrict__ d,
+                                               const double* __restrict__ signs, long long* __restrict__ info,
+                                               int* __restrict__ rescued, Reg reg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int flag;
+    T* F = reinterpret_cast<T*>(smem_raw);
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nj = f.nn + f.na;
+    constexpr bool single = sizeof(T) == 4;
+    if (threadIdx.x == 0) flag = 0;
+    __syncthreads();
+    int bad = small_front<T, T, LDLT>(F, f, fronts, reltgt, chdtgt, P, M, signs, single, &flag, reg);
+    __syncthreads();
+    if (single && (bad >= 0 || flag) && nj <= kSmallRescue) {
+        double* F64 = reinterpret_cast<double*>(smem_raw);
+        bad = small_front<double, T, LDLT>(F64, f, fronts, reltgt, chdtgt, P, M, signs, false, &flag, reg);
+        if (bad < 0) {
+            if (threadIdx.x == 0) atomicAdd(rescued, 1);
+            small_front_store<double, T, LDLT>(F64, f, P, M, d);
+            return;
+        }
+    }
+    if (bad >= 0) {
+        if (threadIdx.x == 0) atomicMin(info, (long long)(f.col0 + bad + 1));
+        return;
+    }
+    small_front_store<T, T, LDLT>(F, f, P, M, d);
 }
 
 // ---------------------------------------------------------------------------
@@ -283,8 +359,10 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 constexpr int LDS = kNB + 4;  // shared-memory leading dimension of the GEMM stages
 constexpr int LDA = kNB + 1;  // leading dimension of the block and its inverse in the diagonal kernel
 
+// dynamic shared memory of k_diag: the FP64 layout in both precisions (the
+// single-precision kernel refactors flagged blocks in FP64 in place)
 template <typename T>
-constexpr int diag_smem() { return (2 * kNB * LDA + 2 * kNB) * (int)sizeof(T); }
+constexpr int diag_smem() { return (2 * kNB * LDA + 2 * kNB) * (int)sizeof(double); }
 
 // The pivot's diagonal entry dk (sqrt(p) for Cholesky, p for LDLt) and its
 // reciprocal.  FP32 (the mixed form, whose factor only preconditions the
@@ -313,32 +391,16 @@ __device__ __forceinline__ void diag_pivot<double, 1>(double p, double& dk, doub
     ik = 1.0 / p;
 }
 
-template <typename T, int LDLT>
-__global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                              int c0, T* __restrict__ P, T* __restrict__ inv,
-                                              T* __restrict__ d, const double* __restrict__ signs,
-                                              long long* __restrict__ info) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* A = reinterpret_cast<T*>(smem_raw);  // block, A[r + c * LDA]
-    T* X = A + kNB * LDA;                   // inverse, same layout
-    T* pivs = X + kNB * LDA;                // L_kk (Cholesky) or d_k (LDLt)
-    T* rinv = pivs + kNB;                   // 1 / L_kk or 1 / d_k
-    __shared__ int bad_s;
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
-    const int nn = f.nn, ld = f.ldp;
-    const int w = min(kNB, nn - c0);
+// Factor and invert the 64 x 64 block held in shared memory as TC: A (block,
+// identity beyond column w), X (inverse), pivs (L_kk or d_k), rinv (their
+// reciprocals).  Returns the first rejected pivot (block-local) or -1,
+// uniform across the block; bad_s is a shared scratch int.
+template <typename TC, int LDLT>
+__device__ int diag_block(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double* __restrict__ signs,
+                          int64_t colbase, int* bad_s, Reg reg) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    T* Pj = P + f.poff;
-#pragma unroll
-    for (int e = tid; e < kNB * kNB; e += 256) {
-        const int r = e & (kNB - 1), c = e >> 6;
-        T v = (r == c) ? T(1) : T(0);
-        if (r >= c && r < w && c < w) v = Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
-        A[r + c * LDA] = v;
-        X[r + c * LDA] = T(0);
-    }
-    if (tid == 0) bad_s = -1;
+    using T = TC;
+    if (tid == 0) *bad_s = -1;
     __syncthreads();
     for (int p = 0; p < 4; ++p) {
         const int pb = p * 16;
@@ -351,9 +413,15 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
             int bad = -1;
 #pragma unroll
             for (int k = 0; k < 16; ++k) {
-                const T pv = __shfl_sync(0xffffffffu, a[k], k);
-                if (bad < 0 && pb + k < w) {
-                    const double sg = pivot_sign(signs, LDLT, (int64_t)f.col0 + c0 + pb + k);
+                T pv = __shfl_sync(0xffffffffu, a[k], k);
+                if (reg.delta >= 0.0) {
+                    if (pb + k < w) {
+                        pv = (T)reg_pivot(reg, pivot_sign(signs, LDLT, colbase + pb + k), (double)pv);
+                        if (i == k) a[k] = pv;
+                        if (bad < 0 && pv == T(0)) bad = pb + k;
+                    }
+                } else if (bad < 0 && pb + k < w) {
+                    const double sg = pivot_sign(signs, LDLT, colbase + pb + k);
                     if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) bad = pb + k;
                 }
                 // after a rejected pivot the remaining steps run on junk and are discarded
@@ -400,10 +468,10 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
                 pivs[pb + i] = mypiv;
                 rinv[pb + i] = myrinv;
             }
-            if (lane == 0 && bad >= 0) bad_s = bad;
+            if (lane == 0 && bad >= 0) (*bad_s) = bad;
         }
         __syncthreads();
-        if (bad_s >= 0) break;  // uniform
+        if ((*bad_s) >= 0) break;  // uniform
         const int m = 48 - pb;  // rows / columns after the panel
         if (m == 0) break;
         // rows below: L_rc = sum_{q <= c} A_r,pb+q Xpp_c,q (/ d_c)
@@ -443,10 +511,7 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
         }
         __syncthreads();
     }
-    if (bad_s >= 0) {  // uniform
-        if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad_s + 1));
-        return;
-    }
+    if (*bad_s >= 0) return *bad_s;  // uniform
     // off-diagonal 16 x 16 blocks of the inverse, by block distance
     for (int dist = 1; dist < 4; ++dist) {
         const int nb = 4 - dist;
@@ -498,18 +563,103 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
         }
         __syncthreads();
     }
+    return -1;
+}
+
+// Write back a factored diagonal block: the factor into the panel, the LDLt
+// pivots, the inverse into the inverse scratch.
+template <typename TC, typename T, int LDLT>
+__device__ void diag_block_store(const TC* A, const TC* X, const TC* pivs, int w, T* Pj, int64_t ld, int c0,
+                                 T* __restrict__ d, int64_t dcol, T* dst) {
+    const int tid = threadIdx.x;
 #pragma unroll
     for (int e = tid; e < kNB * kNB; e += 256) {
         const int r = e & (kNB - 1), c = e >> 6;
-        if (r >= c && r < w && c < w) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = A[r + c * LDA];
+        if (r >= c && r < w && c < w) Pj[(c0 + r) + (int64_t)(c0 + c) * ld] = (T)A[r + c * LDA];
     }
-    if (LDLT && tid < w) d[f.col0 + c0 + tid] = pivs[tid];
+    if (LDLT && tid < w) d[dcol + tid] = (T)pivs[tid];
+#pragma unroll
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        dst[e] = (r < w && c < w) ? (T)X[r + c * LDA] : T(0);
+    }
+}
+
+template <typename TC, typename T>
+__device__ void diag_block_load(TC* A, TC* X, const T* Pj, int64_t ld, int c0, int w) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int e = tid; e < kNB * kNB; e += 256) {
+        const int r = e & (kNB - 1), c = e >> 6;
+        TC v = (r == c) ? TC(1) : TC(0);
+        if (r >= c && r < w && c < w) v = (TC)Pj[(c0 + r) + (int64_t)(c0 + c) * ld];
+        A[r + c * LDA] = v;
+        X[r + c * LDA] = TC(0);
+    }
+}
+
+// Diagonal block kernel.  Single precision: when the FP32 factorization
+// rejects a pivot, or a pivot lost more than five digits against its
+// diagonal entry or grew beyond 1e7 times the block's largest diagonal entry,
+// the block is loaded again and factored and inverted in FP64 (the dynamic
+// shared memory is sized for that), and the FP64 result is stored rounded to
+// FP32.  A rejection in FP64 is reported through info.
+template <typename T, int LDLT>
+__global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                              int c0, T* __restrict__ P, T* __restrict__ inv,
+                                              T* __restrict__ d, const double* __restrict__ signs,
+                                              long long* __restrict__ info, int* __restrict__ rescued, Reg reg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* A = reinterpret_cast<T*>(smem_raw);  // block, A[r + c * LDA]
+    T* X = A + kNB * LDA;                   // inverse, same layout
+    T* pivs = X + kNB * LDA;                // L_kk (Cholesky) or d_k (LDLt)
+    T* rinv = pivs + kNB;                   // 1 / L_kk or 1 / d_k
+    __shared__ int bad_s, flag_s;
+    __shared__ double dmax_s;
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn;
+    const int64_t ld = f.ldp;
+    const int w = min(kNB, nn - c0);
+    const int tid = threadIdx.x;
+    T* Pj = P + f.poff;
     T* dst = inv + f.ioff + (int64_t)(c0 / kNB) * kNB * kNB;
-#pragma unroll
-    for (int e = tid; e < kNB * kNB; e += 256) {
-        const int r = e & (kNB - 1), c = e >> 6;
-        dst[e] = (r < w && c < w) ? X[r + c * LDA] : T(0);
+    constexpr bool single = sizeof(T) == 4;
+    if (tid == 0) { flag_s = 0; dmax_s = 0.0; }
+    diag_block_load<T, T>(A, X, Pj, ld, c0, w);
+    __syncthreads();
+    // |a_kk| before the factorization and the block's largest (non-negative
+    // doubles order like their bit patterns); diag_block starts with a barrier
+    const double a0 = tid < w ? fabs((double)A[tid + tid * LDA]) : 0.0;
+    if (single && tid < w)
+        atomicMax(reinterpret_cast<unsigned long long*>(&dmax_s), (unsigned long long)__double_as_longlong(a0));
+    int bad = diag_block<T, LDLT>(A, X, pivs, rinv, w, signs, (int64_t)f.col0 + c0, &bad_s, reg);
+    if (single) {
+        if (bad < 0 && tid < w) {
+            const double dk = LDLT ? fabs((double)pivs[tid]) : (double)pivs[tid] * (double)pivs[tid];
+            if (dk < kRescueSmall * a0 || dk > kRescueGrowth * fmax(dmax_s, 1.0)) flag_s = 1;
+        }
+        __syncthreads();
+        if (bad >= 0 || flag_s) {
+            double* A64 = reinterpret_cast<double*>(smem_raw);
+            double* X64 = A64 + kNB * LDA;
+            double* piv64 = X64 + kNB * LDA;
+            double* rinv64 = piv64 + kNB;
+            __syncthreads();
+            diag_block_load<double, T>(A64, X64, Pj, ld, c0, w);
+            bad = diag_block<double, LDLT>(A64, X64, piv64, rinv64, w, signs, (int64_t)f.col0 + c0, &bad_s, reg);
+            if (bad < 0) {
+                if (tid == 0) atomicAdd(rescued, 1);
+                diag_block_store<double, T, LDLT>(A64, X64, piv64, w, Pj, ld, c0, d, f.col0 + c0, dst);
+                return;
+            }
+        }
     }
+    if (bad >= 0) {  // uniform
+        if (tid == 0) atomicMin(info, (long long)(f.col0 + c0 + bad + 1));
+        return;
+    }
+    diag_block_store<T, T, LDLT>(A, X, pivs, w, Pj, ld, c0, d, f.col0 + c0, dst);
 }
 
 // ---------------------------------------------------------------------------
@@ -935,6 +1085,9 @@ int launch_panel32_to_dl(mf_handle* h, double* dD, double* dL) {
 
 template <typename T, int LDLT>
 static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
+    // the pivot rule applies to the FP64 factorization; the mixed form keeps
+    // NoRegularization (its single-precision factor only preconditions)
+    const Reg reg = std::is_same<T, double>::value ? h->reg : Reg();
     constexpr int gs = gemm_smem<T>();
     MF_CUDA(cudaFuncSetAttribute(k_small<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmallMax * kSmallMax * (int)sizeof(T)));
@@ -958,7 +1111,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             Timer t(h, K_SMALL);
             k_small<T, LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream>>>(
                 h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
-                h->d_info);
+                h->d_info, h->d_rescued, reg);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.ea.cnt) {
@@ -982,7 +1135,8 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 if (st.diag.cnt) {
                     Timer t(h, K_DIAG);
                     k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
-                        h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info);
+                        h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
+                        h->d_rescued, reg);
                     MF_CUDA(cudaGetLastError());
                 }
                 if (st.panel_tc.cnt) {
@@ -1004,7 +1158,8 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             if (st.diag.cnt) {
                 Timer t(h, K_DIAG);
                 k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
-                    h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info);
+                    h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
+                    h->d_rescued, reg);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.panel.cnt) {
@@ -1106,6 +1261,7 @@ int launch_factor(mf_handle* h) {
         return h->diag ? factor_impl<double, 1>(h, fb) : factor_impl<double, 0>(h, fb);
     });
     h->fp64_current = rc == 0;
+    h->selinv_done = false;
     return rc;
 }
 

@@ -51,6 +51,15 @@ struct RefFront {
     int32_t pad;
 };
 
+// Pivot rule of the factorization: delta < 0 is NoRegularization (a pivot
+// of the wrong sign, or zero, is rejected); otherwise DynamicRegularization
+// (dynamic_regularization.jl:75-90): a pivot with s * d < eps becomes
+// delta * s.
+struct Reg {
+    double delta = -1.0;
+    double eps = 0.0;
+};
+
 // One unit of grouped work: front plus up to two tile coordinates.
 struct Item {
     int32_t front;
@@ -83,6 +92,7 @@ constexpr int kTcTrailN = 128;  // tile columns of the tensor-core trailing upda
 constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
+constexpr int kFwdCols = 512;   // columns of L21 per forward partial-sum work item
 
 // One 64-wide sub-panel s of outer block b (columns b*kob + s*kNB ..., kob the level's outer-block width).
 struct PanelStep {
@@ -120,6 +130,8 @@ struct Level {
     ItemList s_small;        // (front)
     ItemList s_gather;       // (front, row tile) forward gather of child updates
     std::vector<SolveStep> s_steps;
+    ItemList s_fwd_l;        // (front, row tile, col chunk; pad = partial slot) R -= L21 x1
+    ItemList s_fwd_red;      // (front, row tile, first partial slot, chunks)
     ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
     ItemList s_bwd_red;      // (front, col tile, first partial slot)
     int max_nn_blocked = 0;
@@ -244,6 +256,7 @@ struct mf_handle {
     double* d_signs = nullptr;     // pivot signs (n) or null
     long long* d_info = nullptr;   // first failing column (1-based), LLONG_MAX if none
     int* d_err = nullptr;          // set by a kernel whose bounded wait timed out
+    int* d_rescued = nullptr;      // single-precision fronts / diagonal blocks refactored in FP64
     bool use_tc = true;            // tcgen05 tensor cores for the FP32 GEMMs
     void* d_tmaps = nullptr;       // CUtensorMap per execution front (FP32 panels)
     void* d_tmap_inv = nullptr;    // CUtensorMap over the FP32 diagonal-block inverses
@@ -300,6 +313,9 @@ struct mf_handle {
     double* d_segsc = nullptr;     // per segment: CG scalars (80)
 
     double* d_logdet = nullptr;    // per-block partial results of mf_logdet (allocated on first use)
+    void* cublas = nullptr;        // cuBLAS handle of the selected inversion (created on first use)
+    bool selinv_done = false;      // the FP64 panels hold the selected inverse (mf_selinv), not a factor
+    mf::Reg reg;                   // pivot rule of the FP64 factorization (mf_set_regularization)
     int64_t bytes = 0;             // device bytes allocated
     // optional per-kernel timing
     bool profile = false;
@@ -352,6 +368,8 @@ int launch_solve_mixed(mf_handle* h, int64_t nrhs);
 int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst);
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src);
 int launch_anorm(mf_handle* h);
+// selected inversion of the FP64 Cholesky factor in place (mf_selinv)
+int launch_selinv(mf_handle* h);
 // log|det A| and sign(det A) from the factor on the device (mf_logdet)
 int launch_logdet(mf_handle* h, double* logabsdet, double* sign);
 constexpr int kSegRed = 49;  // doubles per segment in d_segred

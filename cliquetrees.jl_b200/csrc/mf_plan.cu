@@ -553,9 +553,11 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 const Front& f = h->h_fronts[j];
                 if (solve_small(f) || f.nn <= k0) continue;
                 const int w = std::min(kSolveNB, f.nn - k0);
-                // 64-row tiles from the 4-aligned row at or before the first row below the block
-                const int below = f.nn + f.na - ((k0 + w) & ~3);
-                if (f.nn + f.na > k0 + w)
+                // 64-row tiles of the diagonal block's rows below the super-block,
+                // from the 4-aligned row at or before the first of them (the
+                // L21 rows are updated once per level by s_fwd_l)
+                const int below = f.nn - ((k0 + w) & ~3);
+                if (f.nn > k0 + w)
                     for (int t = 0; t < (int)cdiv(below, kFwdRows); ++t) push(j, t, 0);
             }
             end(st.fwd);
@@ -567,6 +569,27 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             }
             end(st.bwd);
         }
+        // forward R -= L21 x1 of the blocked fronts: items (front, 64-row tile of
+        // L21 from the 4-aligned row at or before nn, 512-column chunk, slot),
+        // then one reduction item per row tile adding the chunks in order
+        begin(lv.s_fwd_l);
+        int32_t fslot = 0;
+        std::vector<Item> fred;
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (solve_small(f) || f.na == 0) continue;
+            const int rows = f.nn + f.na - (f.nn & ~3);
+            const int nchunk = (int)cdiv(f.nn, kFwdCols);
+            for (int t = 0; t < (int)cdiv(rows, kFwdRows); ++t) {
+                fred.push_back(Item{j, t, fslot, nchunk});
+                for (int q = 0; q < nchunk; ++q) items.push_back(Item{j, t, q, fslot++});
+            }
+        }
+        end(lv.s_fwd_l);
+        begin(lv.s_fwd_red);
+        for (const Item& r : fred) items.push_back(r);
+        end(lv.s_fwd_red);
+        h->nbwd_part = std::max<int64_t>(h->nbwd_part, fslot);
         begin(lv.s_bwd_l);
         int32_t slot = 0;
         std::vector<Item> red;

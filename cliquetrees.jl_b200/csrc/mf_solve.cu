@@ -411,7 +411,8 @@ template <> struct Vec16<double> {
     __device__ static double at(const double2& v, int e) { return e == 0 ? v.x : v.y; }
 };
 
-// forward rows below super-block K: W (rows < nn) or R_j (rows >= nn) -= L[rows, K] x_K.
+// forward rows below super-block K inside the diagonal block: W -= L[rows, K] x_K
+// (the L21 rows are done once per level by k_s_fwd_l).
 // Work item a covers the 64 rows from (k0 + wK rounded down to 4) + 64 a;
 // rows of the block itself that fall in the first tile are computed and
 // dropped.  Warp w streams columns 32 w .. 32 w + 31 of the block straight
@@ -494,8 +495,109 @@ __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ front
 #pragma unroll
             for (int w = 0; w < 8; ++w) v += red[(w * NR + r) * kFwdRows + rl];
             if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
-            else Rj[(q - nn) + r * na] -= v;
         }
+    }
+}
+
+// forward R_j -= L21 x1 for the blocked fronts of a level, once all their
+// diagonal-block steps are done (x1 = C over the front's columns).  Item
+// (front, 64-row tile t of L21 from the 4-aligned row at or before nn,
+// 512-column chunk q, slot): warp w streams columns 64 w .. 64 w + 63 of the
+// chunk with 16-byte loads as in k_s_ftile, x1 is a shared-memory broadcast,
+// and the chunk's sums for the tile's rows go to part[slot]; k_s_fwd_red adds
+// the chunks of a tile in order.  This takes the L21 product (most of the
+// forward data of a large front) out of the sequential step chain.
+template <typename T, int NR>
+constexpr int fwdl_smem() { return (kFwdCols * NR + 8 * NR * kFwdRows) * (int)sizeof(T); }
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_s_fwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 const T* __restrict__ P, const T* __restrict__ C,
+                                                 T* __restrict__ part, int64_t n, int nrhs) {
+    using VT = Vec16<T>;
+    using V = typename VT::type;
+    constexpr int VW = VT::W;             // rows per load
+    constexpr int LPC = kFwdRows / VW;    // lanes per column (16 float, 32 double)
+    constexpr int CPL = 32 / LPC;         // columns per warp load (2 float, 1 double)
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    T* xs = reinterpret_cast<T*>(sm_raw);  // xs[c * NR + r], c relative to the chunk
+    T* red = xs + kFwdCols * NR;           // red[(w * NR + r) * kFwdRows + row]
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, nj = nn + f.na, ld = f.ldp;
+    const int cq = it.b * kFwdCols, wq = min(kFwdCols, nn - cq);
+    const int ra = (nn & ~3) + it.a * kFwdRows;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < kFwdCols * NR; i += 256) {
+        const int c = i % kFwdCols, r = i / kFwdCols;
+        xs[c * NR + r] = (c < wq && r < nrhs) ? C[f.col0 + cq + c + (int64_t)r * n] : T(0);
+    }
+    __syncthreads();
+    const int rr = (lane % LPC) * VW, ch = lane / LPC;
+    // row is a multiple of 4 below nj, so the 16-byte load ends inside the
+    // column's ldp (a multiple of 4) rows
+    const int row = ra + rr;
+    const int cb = warp * (kFwdCols / 8);
+    const int cn = min(kFwdCols / 8, wq - cb);
+    T acc[VW][NR];
+#pragma unroll
+    for (int e = 0; e < VW; ++e)
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
+    if (row < nj && cn > 0) {
+        const T* pc = P + f.poff + (int64_t)(cq + cb) * ld + row;
+#pragma unroll 8
+        for (int c = ch; c < cn; c += CPL) {
+            const V l = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+            const T* xc = xs + (cb + c) * NR;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                const T x = xc[r];
+#pragma unroll
+                for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(l, e) * x;
+            }
+        }
+    }
+    if (CPL == 2) {
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[e][r] += __shfl_xor_sync(0xffffffffu, acc[e][r], 16);
+    }
+    if (ch == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int e = 0; e < VW; ++e) red[(warp * NR + r) * kFwdRows + rr + e] = acc[e][r];
+    }
+    __syncthreads();
+    T* dst = part + (int64_t)it.pad * (kFwdRows * kMaxRhs);
+    for (int o = tid; o < kFwdRows * kMaxRhs; o += 256) {
+        const int rl = o % kFwdRows, r = o / kFwdRows;
+        T v = T(0);
+        if (r < NR)
+#pragma unroll
+            for (int w = 0; w < 8; ++w) v += red[(w * NR + r) * kFwdRows + rl];
+        dst[o] = v;
+    }
+}
+
+// R_j[rows of tile t] -= the chunk sums of k_s_fwd_l, chunks in order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_s_fwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                   const T* __restrict__ part, T* __restrict__ R, int nrhs) {
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, na = f.na;
+    const int ra = (nn & ~3) + it.a * kFwdRows;
+    T* Rj = R + f.roff * nrhs;
+    for (int o = threadIdx.x; o < kFwdRows * kMaxRhs; o += blockDim.x) {
+        const int rl = o % kFwdRows, r = o / kFwdRows;
+        const int q = ra + rl;
+        if (r >= nrhs || q < nn || q >= nn + na) continue;
+        T s = T(0);
+        for (int c = 0; c < it.pad; ++c) s += part[(int64_t)(it.b + c) * (kFwdRows * kMaxRhs) + o];
+        Rj[(q - nn) + r * na] -= s;
     }
 }
 
@@ -736,6 +838,9 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_sdiag<T, 8, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sdiag_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd_l<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwdl_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd_l<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwdl_smem<T, 8>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_fwd_l<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwdl_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 8>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -798,6 +903,22 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
                 }
                 MF_CUDA(cudaGetLastError());
             }
+        }
+        if (lv.s_fwd_l.cnt) {
+            Timer t(h, K_S_FWD);
+            const unsigned gl = (unsigned)lv.s_fwd_l.cnt;
+            const Item* itl = items + lv.s_fwd_l.off;
+            switch (nrb) {
+                case 1: k_s_fwd_l<T, 1><<<gl, 256, fwdl_smem<T, 1>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 2: k_s_fwd_l<T, 2><<<gl, 256, fwdl_smem<T, 2>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 4: k_s_fwd_l<T, 4><<<gl, 256, fwdl_smem<T, 4>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 8: k_s_fwd_l<T, 8><<<gl, 256, fwdl_smem<T, 8>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                default: k_s_fwd_l<T, 16><<<gl, 256, fwdl_smem<T, 16>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+            }
+            MF_CUDA(cudaGetLastError());
+            k_s_fwd_red<T><<<(unsigned)lv.s_fwd_red.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_fwd_red.off,
+                                                                              sb.part, sb.R, nrhs);
+            MF_CUDA(cudaGetLastError());
         }
     }
     if (UNIT) {
@@ -877,6 +998,10 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
 // Solve in place on d_C (n x nrhs, ld n, elimination order); nrhs <= nrhs_cap.
 int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* C, double* part) {
     if (nrhs <= 0) return 0;
+    if (h->selinv_done) {
+        set_error("the FP64 panels hold the selected inverse (mf_selinv), not a factor: factorize again");
+        return -1;
+    }
     if (!have_fp64(h)) {
         set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
         return -1;
@@ -892,6 +1017,10 @@ int launch_solve_with(mf_handle* h, int64_t nrhs, double* R, double* W, double* 
 }
 int launch_solve(mf_handle* h, int64_t nrhs) {
     if (nrhs <= 0) return 0;
+    if (h->selinv_done) {
+        set_error("the FP64 panels hold the selected inverse (mf_selinv), not a factor: factorize again");
+        return -1;
+    }
     if (!have_fp64(h)) {
         set_error("no FP64 factor storage: a mixed handle has it only after an FP64 factorization");
         return -1;

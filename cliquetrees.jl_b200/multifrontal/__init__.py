@@ -7,11 +7,12 @@ and supernodal solves on the GPU (CUDA sm_100a, ``libmfgpu.so``).
 from .symbolic import ChordalSymbolic, Permutation, symbolic, grid_nd_order, amf_order, mindeg_order
 from .factorization import (ChordalFactorization, ChordalCholesky, ChordalLDLt, PosDefException,
                             SingularException, cholesky_, ldlt_, ldiv, rdiv, issuccess, logdet, logabsdet, det,
-                            chol_impl)
+                            chol_impl, selinv_, NoRegularization, DynamicRegularization)
 from . import testmatrices
 
 __all__ = [
     "ChordalSymbolic", "Permutation", "symbolic", "grid_nd_order", "amf_order", "mindeg_order",
     "ChordalFactorization", "ChordalCholesky", "ChordalLDLt", "PosDefException", "SingularException",
-    "cholesky_", "ldlt_", "ldiv", "rdiv", "issuccess", "logdet", "logabsdet", "det", "chol_impl", "testmatrices",
+    "cholesky_", "ldlt_", "ldiv", "rdiv", "issuccess", "logdet", "logabsdet", "det", "chol_impl", "selinv_", "NoRegularization",
+    "DynamicRegularization", "testmatrices",
 ]

@@ -97,6 +97,12 @@ def gpulib() -> ctypes.CDLL:
         lib.mf_profile.argtypes = [_vp, ctypes.c_int]
         lib.mf_profile.restype = ctypes.c_int
         lib.mf_kernel_times.argtypes = [_vp, _pd, _p64]
+        lib.mf_set_regularization.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        lib.mf_set_regularization.restype = ctypes.c_int
+        lib.mf_selinv.argtypes = [_vp]
+        lib.mf_selinv.restype = ctypes.c_int
+        lib.mf_rescued.argtypes = [_vp, _p64]
+        lib.mf_rescued.restype = ctypes.c_int
         lib.mf_logdet.argtypes = [_vp, _pd, _pd]
         lib.mf_logdet.restype = ctypes.c_int
         lib.mf_exec_parents.argtypes = [_vp, _p64]

@@ -92,6 +92,7 @@ class ChordalFactorization:
         self.tol = tol
         self.maxit = maxit
         self.used_fp64 = False
+        self.rescued = 0  # fronts / diagonal blocks the mixed factorization redid in FP64
         self.last_refinement = None
         self._factored = False
         self._handle = _Handle(S, self.DIAG, nrhs_cap, device)
@@ -182,6 +183,9 @@ class ChordalFactorization:
             check(self._handle.lib.mf_factorize_mixed(self._handle.h, ptrd(sg), ctypes.byref(info), ctypes.byref(fp64)),
                   "mf_factorize_mixed")
             self.used_fp64 = bool(fp64.value)
+            cnt = ctypes.c_int64(0)
+            check(self._handle.lib.mf_rescued(self._handle.h, ctypes.byref(cnt)), "mf_rescued")
+            self.rescued = int(cnt.value)
         else:
             check(self._handle.lib.mf_factorize(self._handle.h, ptrd(sg), ctypes.byref(info)), "mf_factorize")
         k = int(info.value)
@@ -274,17 +278,44 @@ class ChordalLDLt(ChordalFactorization):
     DIAG = 1
 
 
-def cholesky_(F: ChordalFactorization, *, check: bool = True):
-    """cholesky!(F; check) (cholesky.jl:80-101): signs = ones."""
+class NoRegularization:
+    """Pivot rule: reject a pivot of the wrong sign (no_regularization.jl:27-42)."""
+
+
+class DynamicRegularization:
+    """Pivot rule: a pivot d_j with s_j d_j < epsilon becomes delta s_j
+    (dynamic_regularization.jl:38-90); negative fields take the defaults
+    cbrt(eps) and sqrt(eps)."""
+
+    def __init__(self, delta: float = -1.0, epsilon: float = -1.0):
+        self.delta = float(delta)
+        self.epsilon = float(epsilon)
+
+
+def _set_reg(F, reg):
+    if reg is None or isinstance(reg, NoRegularization):
+        check(F._handle.lib.mf_set_regularization(F._handle.h, 0, -1.0, -1.0), "mf_set_regularization")
+    elif isinstance(reg, DynamicRegularization):
+        if F.mixed:
+            raise ValueError("DynamicRegularization applies to the FP64 factorization (mixed=False)")
+        check(F._handle.lib.mf_set_regularization(F._handle.h, 1, reg.delta, reg.epsilon), "mf_set_regularization")
+    else:
+        raise TypeError(f"unsupported regularization {type(reg).__name__}")
+
+
+def cholesky_(F: ChordalFactorization, *, check: bool = True, reg=None):
+    """cholesky!(F; check, reg) (cholesky.jl:80-101): signs = ones."""
     if F.DIAG != 0:
         raise TypeError("cholesky_ needs a ChordalCholesky")
+    _set_reg(F, reg)
     return F._factorize(None, check)
 
 
-def ldlt_(F: ChordalFactorization, *, signs=None, check: bool = True):
-    """ldlt!(F; signs=zeros, check) (cholesky.jl:181-203)."""
+def ldlt_(F: ChordalFactorization, *, signs=None, check: bool = True, reg=None):
+    """ldlt!(F; signs=zeros, check, reg) (cholesky.jl:181-203)."""
     if F.DIAG != 1:
         raise TypeError("ldlt_ needs a ChordalLDLt")
+    _set_reg(F, reg)
     return F._factorize(signs, check)
 
 
@@ -314,6 +345,22 @@ def rdiv(B, F: ChordalFactorization):
     """B / F for a symmetric factorization: (F \\ B^T)^T (divide.jl:287-292)."""
     B = np.asarray(B, dtype=np.float64)
     return ldiv(F, B.T).T
+
+
+def selinv_(F: ChordalFactorization):
+    """selinv!(F) (selinv.jl:38-41): replace the Cholesky factor on the GPU by
+    the entries of A^{-1} on the pattern of L (``F.factor_arrays()`` then
+    returns them in the reference layout); F must be factorized again before
+    a solve."""
+    if F.DIAG != 0:
+        raise TypeError("selinv_ needs a ChordalCholesky")
+    if not F._factored or F.info != 0:
+        raise RuntimeError("factorize first (cholesky_)")
+    if F.mixed:
+        raise ValueError("selinv_ needs the FP64 factor: use a plain (mixed=False) factorization")
+    check(F._handle.lib.mf_selinv(F._handle.h), "mf_selinv")
+    F._factored = False
+    return F
 
 
 def issuccess(F: ChordalFactorization) -> bool:

@@ -112,10 +112,20 @@ int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, cons
 int mf_enable_mixed(mf_handle* h);
 
 /* Scale A symmetrically by diag(|a_ii|)^-1/2, factor it in FP32 (same plan,
- * single-precision kernels) and compute ||A||_inf.  If FP32 rejects a pivot
- * the matrix is refactored in FP64 and *used_fp64 = 1; info then follows
- * the FP64 factorization (the reference's convention). */
+ * single-precision kernels) and compute ||A||_inf.  Every front (nj <= 96)
+ * and every 64 x 64 diagonal block of a larger front whose FP32 pivots are
+ * rejected, lost more than five digits against their diagonal entry, or grew
+ * beyond 1e7 times the block's largest diagonal entry is factored again in
+ * FP64 on the GPU and stored rounded to FP32 (mf_rescued counts them).  If a
+ * pivot is rejected even then (or in FP32 in a small front with nj > 67),
+ * the matrix is refactored in FP64 and *used_fp64 = 1; info then follows the
+ * FP64 factorization (the reference's convention). */
 int mf_factorize_mixed(mf_handle* h, const double* signs, int64_t* info, int* used_fp64);
+
+/* Fronts and diagonal blocks that the last factorization refactored in FP64
+ * after the single-precision pivot check flagged them (see
+ * mf_factorize_mixed).  No reference counterpart. */
+int mf_rescued(mf_handle* h, int64_t* count);
 
 /* Autotuning of the single-precision factorization (no reference
  * counterpart: the reference has one dense kernel per role).  For every tree
@@ -149,6 +159,24 @@ int mf_get_factor_mixed(mf_handle* h, double* Dval, double* Lval, double* d, dou
 
 /* Copy the device factor out in the reference layout (any pointer may be NULL). */
 int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d);
+
+/* Pivot rule of the FP64 factorizations (mf_factorize, mf_chol_impl):
+ * mode 0 = NoRegularization (the default; no_regularization.jl:27-42),
+ * mode 1 = DynamicRegularization (dynamic_regularization.jl:75-90): a pivot
+ * d_j with s_j d_j < epsilon is replaced by delta s_j (s = the pivot signs;
+ * ones for Cholesky); delta / epsilon < 0 take the reference defaults
+ * cbrt(eps) and sqrt(eps).  mf_factorize_mixed refuses a handle with
+ * mode 1.  Replaces the `reg` keyword of cholesky! / ldlt!
+ * (src/Multifrontal.jl/src/cholesky.jl:80-229). */
+int mf_set_regularization(mf_handle* h, int mode, double delta, double epsilon);
+
+/* Selected inversion (Cholesky handles): after mf_factorize, replace the
+ * FP64 factor on the device by the entries of A^{-1} on the sparsity pattern
+ * of L (lower triangle of each diagonal block); mf_get_factor then returns
+ * them in the reference layout, and the solves refuse until the next
+ * factorization.  Replaces selinv!(F), src/Multifrontal.jl/src/selinv.jl:38-41.
+ * Synchronises the handle's stream. */
+int mf_selinv(mf_handle* h);
 
 /* log|det A| and sign(det A) of the matrix last factored on this handle,
  * reduced on the device from the factor's diagonal: Cholesky 2 sum log L_jj

@@ -34,6 +34,10 @@
  *                         src/Multifrontal.jl/src/divide.jl:1206-1293
  *   ldiv!(W, ::NaturalFactorization, B)
  *                         src/Multifrontal.jl/src/divide.jl:191-199
+ *   selinv! / selinv_impl! / selinv_loop_snd! / selinv_loop_nod! / selinv_send!
+ *                         src/Multifrontal.jl/src/selinv.jl:38-424
+ *   trrk! -> syr2k(alpha/2) src/Multifrontal.jl/src/blas/trrk.jl:5-8; trtri! -> LAPACK
+ *                         src/Multifrontal.jl/src/blas/trtri.jl:3-6
  *
  * All symbolic arrays are 0-based (see include/cliquetrees_symbolic.h).
  */
@@ -68,6 +72,13 @@ static void (*x_dger)(const blasint*, const blasint*, const double*, const doubl
 static void (*x_dtrsv)(const char*, const char*, const char*, const blasint*, const double*, const blasint*,
                        double*, const blasint*, size_t, size_t, size_t);
 static void (*x_set_threads)(int);
+static void (*x_dsymm)(const char*, const char*, const blasint*, const blasint*, const double*, const double*,
+                       const blasint*, const double*, const blasint*, const double*, double*, const blasint*,
+                       size_t, size_t);
+static void (*x_dsymv)(const char*, const blasint*, const double*, const double*, const blasint*, const double*,
+                       const blasint*, const double*, double*, const blasint*, size_t);
+static double (*x_ddot)(const blasint*, const double*, const blasint*, const double*, const blasint*);
+static void (*x_dtrtri)(const char*, const char*, const blasint*, double*, const blasint*, blasint*, size_t, size_t);
 
 static void* g_blas = NULL;
 
@@ -94,6 +105,11 @@ int mfo_init(const char* path, int nthreads) {
         x_dger = sym("dger_");
         x_dtrsv = sym("dtrsv_");
         x_set_threads = sym("openblas_set_num_threads");
+        x_dsymm = sym("dsymm_");
+        x_dsymv = sym("dsymv_");
+        x_ddot = sym("ddot_");
+        x_dtrtri = sym("dtrtri_");
+        if (!x_dsymm || !x_dsymv || !x_ddot || !x_dtrtri) return -2;
         if (!x_dpotrf || !x_dtrsm || !x_dsyrk || !x_dsyr2k || !x_dsyr || !x_dgemm || !x_dgemv || !x_dger ||
             !x_dtrsv)
             return -2;
@@ -106,7 +122,21 @@ int mfo_init(const char* path, int nthreads) {
 /* pivot acceptance (no_regularization.jl:27-42): with sign s != 0 the     */
 /* pivot must have the sign of s; with s == 0 anything is kept.  A         */
 /* rejected pivot becomes zero, which the callers report as a failure.    */
+static int g_reg_mode = 0;           /* 0 NoRegularization, 1 DynamicRegularization */
+static double g_reg_delta = 0.0, g_reg_eps = 0.0;
+
+/* The pivot rule for the following factorizations: mode 0 is
+ * NoRegularization, mode 1 DynamicRegularization(delta, epsilon)
+ * (dynamic_regularization.jl:75-90; negative values take the defaults
+ * cbrt(eps) and sqrt(eps), :58-72). */
+void mfo_set_regularization(int mode, double delta, double epsilon) {
+    g_reg_mode = mode;
+    g_reg_delta = delta < 0 ? cbrt(2.220446049250313e-16) : delta;
+    g_reg_eps = epsilon < 0 ? sqrt(2.220446049250313e-16) : epsilon;
+}
+
 static double regularize(double s, double djj) {
+    if (g_reg_mode == 1) return (s * djj < g_reg_eps) ? g_reg_delta * s : djj;
     if (s != 0.0 && !(s * djj > 0.0)) return 0.0;
     return djj;
 }
@@ -168,14 +198,55 @@ static I potrf_ldlt(double* A, I n, I lda, double* d, const double* S, double* W
     return 0;
 }
 
+/* potrf2!(Val(:L), A, d, S, R, Val(:N)) -- unblocked Cholesky with the
+ * pivot rule (potrf.jl:3-41) */
+static I potrf2_chol(double* A, I n, I lda, const double* S) {
+    for (I j = 0; j < n; ++j) {
+        double Ajj = regularize(S[j], A[j + j * lda]);
+        if (Ajj == 0.0) return j + 1;
+        A[j + j * lda] = Ajj = sqrt(Ajj);
+        double iD = 1.0 / Ajj;
+        for (I i = j + 1; i < n; ++i) A[i + j * lda] *= iD;
+        for (I k = j + 1; k < n; ++k) {
+            double Akj = A[k + j * lda];
+            A[k + k * lda] -= Akj * Akj;
+            for (I i = k + 1; i < n; ++i) A[i + k * lda] -= A[i + j * lda] * Akj;
+        }
+    }
+    return 0;
+}
+
+/* generic recursive potrf! for Cholesky with a regularization
+ * (potrf.jl:135-178 with Val(:N)), THRESHOLD = 64 */
+static I potrf_chol(double* A, I n, I lda, const double* S) {
+    if (n <= 64) return potrf2_chol(A, n, lda, S);
+    I n1 = 1;
+    while (n1 * 2 <= n) n1 *= 2;
+    n1 /= 2;
+    double* A22 = A + n1 + n1 * lda;
+    double* B = A + n1;
+    I info = potrf_chol(A, n1, lda, S);
+    if (info != 0) return info;
+    blasint m = (blasint)(n - n1), k = (blasint)n1, la = (blasint)lda;
+    double one = 1.0, mone = -1.0;
+    x_dtrsm("R", "L", "T", "N", &m, &k, &one, A, &la, B, &la, 1, 1, 1, 1);
+    x_dsyrk("L", "N", &m, &k, &mone, B, &la, &one, A22, &la, 1, 1);
+    info = potrf_chol(A22, n - n1, lda, S + n1);
+    if (info != 0) return n1 + info;
+    return 0;
+}
+
 /* chol_factor! (cholesky.jl:694-737) */
 static I chol_factor(double* D, I nn, double* L, I na, double* d, const double* S, int diag, double* W) {
     I info;
-    if (diag == 0) {
+    if (diag == 0 && g_reg_mode == 0) {
         /* LAPACK path for Float64 + NoRegularization (potrf.jl:101-103, :87-90) */
         blasint bn = (blasint)nn, binfo = 0;
         x_dpotrf("L", &bn, D, &bn, &binfo, 1);
         info = binfo;
+    } else if (diag == 0) {
+        /* any other regularization: the generic recursive potrf! */
+        info = potrf_chol(D, nn, nn, S);
     } else {
         info = potrf_ldlt(D, nn, nn, d, S, W);
     }
@@ -445,4 +516,92 @@ int mfo_div_impl(I n, I nfr, const I* resptr, const I* sepptr, const I* reltgt, 
     }
     return bwd(nfr, resptr, sepptr, reltgt, chdptr, chdtgt, Dptr, Lptr, nMptr, nNval, nFval, diag, Dval, Lval, C,
                nrhs, ldc, vec);
+}
+
+/* ---------------------------------------------------------------------- */
+/* selected inversion of a Cholesky factor (selinv!, selinv.jl:38-424):    */
+/* Dval/Lval hold L on entry and the entries of A^{-1} on the pattern of L */
+/* on exit (lower triangle of each diagonal block).  Returns 0, or -1 on   */
+/* an allocation failure.                                                  */
+int mfo_selinv(I n, I nfr, const I* resptr, const I* sepptr, const I* reltgt, const I* chdptr, const I* chdtgt,
+               const I* Dptr, const I* Lptr, I nMptr, I nMval, I nFval, double* Dval, double* Lval) {
+    (void)n;
+    I* Mptr = (I*)malloc(sizeof(I) * (size_t)(nMptr + 2));
+    double* Mval = (double*)malloc(sizeof(double) * (size_t)(nMval > 0 ? nMval : 1));
+    double* F = (double*)malloc(sizeof(double) * (size_t)(nFval * nFval > 0 ? nFval * nFval : 1));
+    if (!Mptr || !Mval || !F) { free(Mptr); free(Mval); free(F); return -1; }
+    I ns = 0;
+    Mptr[0] = 0;
+    for (I j = nfr - 1; j >= 0; --j) {
+        const I nn = resptr[j + 1] - resptr[j];
+        const I na = sepptr[j + 1] - sepptr[j];
+        const I nj = nn + na;
+        double* D = Dval + Dptr[j];
+        double* L = Lval + Lptr[j];
+        if (nn == 1) {
+            /* selinv_loop_nod! (selinv.jl:258-376) */
+            double d11 = D[0];
+            double f11 = 0.0;
+            if (na > 0) {
+                const double* M = Mval + Mptr[ns - 1];
+                ns -= 1;
+                for (I c = 0; c < na; ++c)
+                    for (I r = c; r < na; ++r) F[(1 + r) + (1 + c) * nj] = M[r + c * na];
+                for (I a = 0; a < na; ++a) L[a] /= d11;
+                blasint bn = (blasint)na, one_i = 1, ldm = (blasint)na;
+                double alpha = -1.0, beta = 0.0;
+                x_dsymv("L", &bn, &alpha, M, &ldm, L, &one_i, &beta, F + 1, &one_i, 1);
+                f11 -= x_ddot(&bn, L, &one_i, F + 1, &one_i);
+            }
+            d11 = 1.0 / d11;
+            f11 += d11 * d11;
+            D[0] = f11;
+            F[0] = f11;
+            for (I a = 0; a < na; ++a) L[a] = F[1 + a];
+        } else {
+            /* selinv_loop_snd! (selinv.jl:130-256) */
+            for (I c = 0; c < nn; ++c)
+                for (I r = 0; r < nn; ++r) F[r + c * nj] = 0.0;
+            if (na > 0) {
+                const double* M = Mval + Mptr[ns - 1];
+                ns -= 1;
+                for (I c = 0; c < na; ++c)
+                    for (I r = c; r < na; ++r) F[(nn + r) + (nn + c) * nj] = M[r + c * na];
+                blasint bm = (blasint)na, bk = (blasint)nn, bj = (blasint)nj;
+                double one = 1.0, mone = -1.0, zero = 0.0, mhalf = -0.5;
+                /* L21 <- L21 D11^{-1} */
+                x_dtrsm("R", "L", "N", "N", &bm, &bk, &one, D, &bk, L, &bm, 1, 1, 1, 1);
+                /* F21 <- -M22 L21 */
+                x_dsymm("L", "L", &bm, &bk, &mone, M, &bm, L, &bm, &zero, F + nn, &bj, 1, 1);
+                /* F11 <- F11 - L21^T F21 (trrk: syr2k with alpha / 2) */
+                x_dsyr2k("L", "T", &bk, &bm, &mhalf, L, &bm, F + nn, &bj, &one, F, &bj, 1, 1);
+            }
+            /* D11 <- D11^{-1}; tril!; F11 <- F11 + D11^T D11 */
+            blasint bk = (blasint)nn, bj = (blasint)nj, info = 0;
+            x_dtrtri("L", "N", &bk, D, &bk, &info, 1, 1);
+            for (I c = 0; c < nn; ++c)
+                for (I r = 0; r < c; ++r) D[r + c * nn] = 0.0;
+            double one = 1.0;
+            x_dsyrk("L", "T", &bk, &bk, &one, D, &bk, &one, F, &bj, 1, 1);
+            /* D11 <- F11; L21 <- F21 */
+            for (I c = 0; c < nn; ++c)
+                for (I r = 0; r < nn; ++r) D[r + c * nn] = F[r + c * nj];
+            for (I c = 0; c < nn; ++c)
+                for (I a = 0; a < na; ++a) L[a + c * na] = F[(nn + a) + c * nj];
+        }
+        /* send the update matrices to the children (selinv_send!, copygathertri!) */
+        for (I p = chdptr[j]; p < chdptr[j + 1]; ++p) {
+            const I i = chdtgt[p];
+            const I ma = sepptr[i + 1] - sepptr[i];
+            const I* inj = reltgt + sepptr[i];
+            ns += 1;
+            const I strt = Mptr[ns - 1];
+            Mptr[ns] = strt + ma * ma;
+            double* Mi = Mval + strt;
+            for (I b = 0; b < ma; ++b)
+                for (I a = b; a < ma; ++a) Mi[a + b * ma] = F[inj[a] + inj[b] * nj];
+        }
+    }
+    free(Mptr); free(Mval); free(F);
+    return 0;
 }

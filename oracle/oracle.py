@@ -65,6 +65,10 @@ def lib(nthreads: int = 1):
         L.mfo_div_impl.argtypes = [_i64, _i64] + [_p64] * 7 + [_i64, _i64, _i64, ctypes.c_int, _pd, _pd, _pd, _pd,
                                                                _i64, _i64, ctypes.c_int]
         L.mfo_div_impl.restype = ctypes.c_int
+        L.mfo_set_regularization.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double]
+        L.mfo_set_regularization.restype = None
+        L.mfo_selinv.argtypes = [_i64, _i64] + [_p64] * 7 + [_i64, _i64, _i64, _pd, _pd]
+        L.mfo_selinv.restype = ctypes.c_int
         L.mfo_amf_order.argtypes = [_i64, _p64, _p64, _p64]
         L.mfo_amf_order.restype = ctypes.c_int
         L.mfo_symbolic_create.argtypes = [_i64, _p64, _p64, _p64]
@@ -93,9 +97,15 @@ def _d(a):
     return None if a is None else a.ctypes.data_as(_pd)
 
 
-def chol_impl(S, Dval, Lval, diag: int, signs=None, d=None):
-    """Run the oracle factorization in place.  Returns (info, d)."""
+def chol_impl(S, Dval, Lval, diag: int, signs=None, d=None, reg=None):
+    """Run the oracle factorization in place.  Returns (info, d).  ``reg``:
+    None (NoRegularization) or (delta, epsilon) for DynamicRegularization
+    (negative values take the defaults)."""
     L = lib()
+    if reg is None:
+        L.mfo_set_regularization(0, -1.0, -1.0)
+    else:
+        L.mfo_set_regularization(1, float(reg[0]), float(reg[1]))
     Dval = np.ascontiguousarray(Dval, dtype=np.float64)
     Lval = np.ascontiguousarray(Lval, dtype=np.float64)
     if d is None:
@@ -104,9 +114,23 @@ def chol_impl(S, Dval, Lval, diag: int, signs=None, d=None):
     info = L.mfo_chol_impl(S.n, S.nfr, _p(S.resptr), _p(S.sepptr), _p(S.reltgt), _p(S.chdptr), _p(S.chdtgt),
                            _p(S.Dptr), _p(S.Lptr), S.nMptr, S.nMval, S.nFval, diag, _d(Dval), _d(Lval), _d(d),
                            _d(sg))
+    L.mfo_set_regularization(0, -1.0, -1.0)
     if info < 0:
         raise MemoryError("oracle allocation failed")
     return int(info), Dval, Lval, d
+
+
+def selinv(S, Dval, Lval):
+    """selinv! (selinv.jl:38-424) of a Cholesky factor in place: returns
+    (Dval, Lval) holding A^{-1} on the pattern of L."""
+    L = lib()
+    Dval = np.ascontiguousarray(Dval, dtype=np.float64).copy()
+    Lval = np.ascontiguousarray(Lval, dtype=np.float64).copy()
+    rc = L.mfo_selinv(S.n, S.nfr, _p(S.resptr), _p(S.sepptr), _p(S.reltgt), _p(S.chdptr), _p(S.chdtgt),
+                      _p(S.Dptr), _p(S.Lptr), S.nMptr, S.nMval, S.nFval, _d(Dval), _d(Lval))
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    return Dval, Lval
 
 
 def div_impl(S, Dval, Lval, d, diag: int, C, vec: bool = False):

@@ -8,6 +8,10 @@ Sources (paths relative to the reference root):
                                   LDLt example (A, unit L, D, F \\ b, signs=)
   src/AMFLib.jl/README.md         AMF order of the 8-vertex graph
   README.md                       clique tree of the 8-vertex graph (alg=MF())
+  src/Multifrontal.jl/src/selinv.jl  selected inverse of the 5x5 example (docstring)
+  src/Multifrontal.jl/src/regularization/dynamic_regularization.jl
+                                  DynamicRegularization example: A and Matrix(F)
+                                  (printed to 6 significant digits)
   test/core.jl                    the 17-vertex graph of Vandenberghe & Andersen
                                   (Figure 4.3) and its clique tree under the order
                                   1:17 with Maximal supernodes (Figure 4.7 left):
@@ -148,6 +152,20 @@ def main():
         nodes.append({"bag": bag, "parent": parent})
         stack.append(bag)
     out["cliquetree_mf"] = nodes
+    # --- selected inverse of the 5x5 example (selinv.jl docstring)
+    sl = open(os.path.join(REF, "src/Multifrontal.jl/src/selinv.jl")).read().splitlines()
+    i = next(k for k, l in enumerate(sl) if l.startswith("julia> A = ["))
+    As, i = _matrix_literal(sl, i)
+    i = next(k for k in range(i, len(sl)) if "selinv!(cholesky!(ChordalCholesky(A)))" in sl[k])
+    Z, i = _rows_after(sl, i + 2, 5)
+    out["selinv"] = {"A": As, "Z": Z}
+    # --- DynamicRegularization example (docstring)
+    dr = open(os.path.join(REF, "src/Multifrontal.jl/src/regularization/dynamic_regularization.jl")).read().splitlines()
+    i = next(k for k, l in enumerate(dr) if l.startswith("julia> A = ["))
+    Ad, i = _matrix_literal(dr, i)
+    i = next(k for k in range(i, len(dr)) if dr[k].startswith("julia> B = Matrix(F)"))
+    Bd, i = _rows_after(dr, i + 2, 3)
+    out["dynamic_regularization"] = {"A": Ad, "B": Bd}
     # --- the 17-vertex graph and its Maximal clique tree (order 1:17)
     core = open(os.path.join(REF, "test/core.jl")).read().splitlines()
     out["maximal17"] = _core_maximal(core)

@@ -139,39 +139,68 @@ def test_autotune_keeps_refined_accuracy():
     F.close()
 
 
-def _fp32_breakdown_matrix():
-    """A 12x12 grid matrix, SPD in FP64, whose FP32 factorization meets a zero
-    pivot: unit diagonal, off-diagonals 1e-12 except one edge at 1 - 1e-10,
-    which rounds to 1 in single precision (the Schur complement 2e-10 of
-    that pair vanishes)."""
-    A = tm.grid_laplacian(12, 12, seed=1).tocoo()
+def _fp32_breakdown_matrix(side=12, dense=False):
+    """SPD in FP64, but its FP32 factorization meets a zero pivot: unit
+    diagonal, off-diagonals 1e-12 except one pair at 1 - 1e-10, which rounds
+    to 1 in single precision (the pair's Schur complement 2e-10 vanishes).
+    A grid pattern gives small fronts; dense=True one front of side x side
+    columns (blocked: 64 x 64 diagonal blocks)."""
+    if dense:
+        n = side
+        rows, cols = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+        A = sp.coo_matrix((np.ones(n * n), (rows.ravel(), cols.ravel())), shape=(n, n))
+    else:
+        A = tm.grid_laplacian(side, side, seed=1).tocoo()
     vals = np.where(A.row == A.col, 1.0, -1e-12)
-    u, v = 40, 41  # neighbours on the grid
+    u, v = 40, 41  # neighbours on the grid; inside the first 64 x 64 block of the dense front
     vals[((A.row == u) & (A.col == v)) | ((A.row == v) & (A.col == u))] = -(1.0 - 1e-10)
     return sp.csc_matrix((vals, (A.row, A.col)), shape=A.shape)
+
+
+@pytest.mark.parametrize("dense", [False, True])
+def test_single_precision_pivot_failure_is_rescued_per_front(dense):
+    """North-star precision rule: an FP32 pivot rejection refactors only the
+    flagged front (nj <= 67, in the small-front kernel) or 64 x 64 diagonal
+    block (blocked front) in FP64 on the GPU -- not the whole matrix -- and
+    the refinement still reaches 1e-12."""
+    A = _fp32_breakdown_matrix(130 if dense else 12, dense=dense)
+    P, S = mf.symbolic(A)
+    if dense:
+        assert S.nfr == 1 and S.n == 130
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
+    assert F.info == 0
+    assert not F.used_fp64
+    assert F.rescued >= 1
+    B = tm.rhs(S.n, 3, seed=4)
+    X = mf.ldiv(F, B)
+    it, eta = F.last_refinement
+    assert eta <= 1e-12 and tm.backward_error(A, X, B).max() <= 1e-12, (it, eta)
+    # a well-conditioned matrix on the same handle needs no rescue
+    F.copyto(tm.grid_laplacian(12, 12, seed=2) if not dense else sp.csc_matrix(np.eye(130) * 2 + A - sp.diags(A.diagonal())))
+    mf.cholesky_(F)
+    assert F.rescued == 0 and not F.used_fp64
+    F.close()
 
 
 def test_fp64_solves_refuse_a_stale_fp64_factor():
     """After an FP64 fallback the FP64 factor storage stays allocated; a later
     mixed factorization that stays in FP32 leaves it holding the old matrix,
-    so the FP64 solves and the FP64 factor download must refuse it."""
+    so the FP64 solves and the FP64 factor download must refuse it.  The
+    fallback comes from an indefinite matrix (rejected in FP64 too)."""
     import ctypes
-    A1 = _fp32_breakdown_matrix()
+    A1 = tm.grid_laplacian(12, 12, seed=1).tolil()
+    A1[40, 40] = -3.0
+    A1 = A1.tocsc()
     A2 = tm.grid_laplacian(12, 12, seed=2)
     P, S = mf.symbolic(A1)
     F = mf.ChordalCholesky(A1, P, S, mixed=True)
-    mf.cholesky_(F)
-    assert F.used_fp64 and F.info == 0
-    B = tm.rhs(S.n, 2, seed=3)
-    X1 = mf.ldiv(F, B)
-    assert tm.backward_error(A1, X1, B).max() <= 1e-12
+    mf.cholesky_(F, check=False)
+    assert F.used_fp64 and F.info != 0
     lib, h = F._handle.lib, F._handle.h
-    Xp = np.asfortranarray(B.copy())
-    assert lib.mf_solve(h, Xp.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 2, S.n,
-                        P.perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))) == 0  # FP64 factor is A1's
     F.copyto(A2)
     mf.cholesky_(F)
-    assert not F.used_fp64
+    assert not F.used_fp64 and F.info == 0
+    B = tm.rhs(S.n, 2, seed=3)
     X2 = mf.ldiv(F, B)
     assert tm.backward_error(A2, X2, B).max() <= 1e-12
     Xp = np.asfortranarray(B.copy())

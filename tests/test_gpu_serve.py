@@ -1,6 +1,7 @@
-"""Serving loop on the GPU: requests of mixed patterns are batched (fronts
-merged level by level inside a batched handle) and run concurrently on
-several streams; every result must be the one the request gets alone.
+"""Serving loop on the GPU: requests of different patterns are merged into
+one forest per admission round (fronts merged level by level) and rounds run
+concurrently on several streams; every result must be the one the request
+gets alone.
 
 Bars: plain FP64 -- the served solution is bitwise equal to the same
 request factored and solved alone (requests never share arithmetic);
@@ -53,12 +54,13 @@ def _alone(A, order, B, mixed):
 def test_served_results_equal_alone(mixed):
     srv = serve.Server(mixed=mixed, workers=3)
     for k, (gen, order, batch) in _patterns().items():
-        srv.add_pattern(k, gen(0), order=order, batch=batch)
+        srv.add_pattern(k, gen(0), order=order, batch=batch, size_class=0)
     srv.warm()
-    reqs, mats = _stream(srv, 30, seed=7 + mixed)
+    reqs, mats = _stream(srv, 40, seed=7 + mixed)
     done = srv.serve(reqs, realtime=True, timeout=120)
-    assert len(done) == 30 and all(r.done >= r.arrival for r in done)
-    assert max(r.batch_size for r in done) > 1  # some requests really shared a batch
+    assert len(done) == 40 and all(r.done >= r.arrival for r in done)
+    assert max(r.batch_size for r in done) > 1  # some requests really shared a round
+    assert any(len(c) > 1 for c in srv.rounds)  # some round merged different patterns
     pats = _patterns()
     for r in done:
         A = mats[r.rid]
@@ -80,15 +82,15 @@ def test_served_results_equal_alone(mixed):
 def test_memory_cap_evicts_idle_handles():
     srv = serve.Server(mixed=False, workers=1)
     for k, (gen, order, batch) in _patterns().items():
-        srv.add_pattern(k, gen(0), order=order, batch=batch)
-    srv.warm(["g2d12"])
+        srv.add_pattern(k, gen(0), order=order, batch=batch, size_class=0)
+    srv.warm(["g2d12"], counts=[1])
     one = srv.bytes
     assert one > 0
     srv.mem_cap = one * 1.5  # room for about one handle
     reqs, mats = _stream(srv, 12, seed=3)
     done = srv.serve(reqs, realtime=False, timeout=120)
     assert len(done) == 12
-    assert srv.bytes <= max(srv.mem_cap, max(h.bytes for p in srv.patterns.values() for h in p.handles))
+    assert srv.bytes <= max(srv.mem_cap, max(h.bytes for hs in srv.handles.values() for h in hs))
     for r in done:
         assert tm.backward_error(mats[r.rid], r.X, r.B).max() <= 1e-13
     srv.close()

@@ -117,3 +117,46 @@ def test_failure_info_is_first_bad_pivot_in_original_order():
     assert info > 0
     # factorize! maps the permuted column through perm (cholesky.jl:250-254)
     assert P.perm[info - 1] + 1 == 4
+
+
+def test_selinv_known_answer():
+    """selinv.jl docstring: selinv!(cholesky!(ChordalCholesky(A))) with the
+    default ordering, displayed in elimination order."""
+    ka = KA["selinv"]
+    A = np.array(ka["A"])
+    P, S = oracle.symbolic(A)
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0)
+    assert info == 0
+    Zd, Zl = oracle.selinv(S, Dval, Lval)
+    want = np.nan_to_num(np.array(ka["Z"]), nan=0.0)
+    np.testing.assert_allclose(dense_factor(S, Zd, Zl), want, rtol=0, atol=1e-15)
+
+
+def test_selinv_oracle_equals_inverse_on_the_pattern():
+    """The oracle's selected inverse equals A^-1 on the pattern of L."""
+    from multifrontal import testmatrices as tm
+    A = tm.grid_laplacian(9, 8, 3, seed=4)
+    P, S = oracle.symbolic(A)
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0)
+    Zd, Zl = oracle.selinv(S, Dval, Lval)
+    Z = dense_factor(S, Zd, Zl)
+    mask = dense_factor(S, np.ones_like(Dval), np.ones_like(Lval)) != 0
+    Ai = np.linalg.inv(A.toarray())[np.ix_(P.perm, P.perm)]
+    assert np.abs((Z - Ai)[mask]).max() <= 1e-12 * np.abs(Ai).max()
+
+
+def test_dynamic_regularization_known_answer():
+    """dynamic_regularization.jl docstring: cholesky!(ChordalCholesky(A);
+    reg=DynamicRegularization()) of an indefinite matrix; Matrix(F) is
+    printed to six significant digits."""
+    ka = KA["dynamic_regularization"]
+    A = np.array(ka["A"])
+    P, S = oracle.symbolic(A)
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    info, Dval, Lval, d = oracle.chol_impl(S, Dval, Lval, 0, reg=(-1.0, -1.0))
+    assert info == 0
+    L = dense_factor(S, Dval, Lval)
+    B = (L @ L.T)[np.ix_(P.invp, P.invp)]
+    np.testing.assert_allclose(B, np.array(ka["B"]), rtol=5e-6)

@@ -1,24 +1,32 @@
-"""Host logic of the serving loop, with the device batch replaced by a fake
-(no GPU): every request completes once, requests of one pattern share
-batches, the memory cap evicts idle handles, and a handle larger than the
-cap runs alone instead of waiting forever."""
+"""Host logic of the serving loop, with the device handle replaced by a fake
+(no GPU): every request completes once, rounds merge requests of different
+patterns of one size class, counts per pattern are powers of two within the
+pattern's limit, no request is repeated to fill a round, the memory cap
+evicts idle handles and is respected before a handle is built, and a handle
+larger than the cap runs alone instead of waiting forever."""
 import time
 
 import numpy as np
 
-import multifrontal as mf
 from multifrontal import serve
 from multifrontal import testmatrices as tm
 
 
 class FakeBatch:
-    def __init__(self, pat, mixed, device, tol, maxit):
-        self.pat = pat
-        self.bytes = pat.S.n * 1000 * pat.batch
+    built = []
+
+    def __init__(self, comp, patterns, mixed, device, tol, maxit):
+        self.comp = comp
+        self.members = [patterns[k] for k, c in comp for _ in range(c)]
+        self.bytes = sum(p.S.n * 1000 for p in self.members)
         self.busy = False
         self.last_used = 0.0
+        FakeBatch.built.append(self)
 
     def run(self, reqs):
+        assert len(reqs) == len(self.members)
+        assert [r.key for r in reqs] == [p.key for p in self.members]
+        assert len({id(r) for r in reqs}) == len(reqs)  # never the same request twice
         time.sleep(0.001)
         for r in reqs:
             r.X = np.zeros_like(r.B)
@@ -31,16 +39,16 @@ class FakeBatch:
 
 PATS = {
     "g2d12": (lambda s: tm.grid_laplacian(12, 12, seed=s), "amf", 4),
-    "g2d20": (lambda s: tm.grid_laplacian(20, 20, seed=s), "amf", 4),
+    "g2d14": (lambda s: tm.grid_laplacian(14, 14, seed=s), "amf", 4),
     "g3d6": (lambda s: tm.grid_laplacian(6, 6, 6, seed=s), "natural", 2),
 }
 
 
-def _server(monkeypatch, workers):
+def _server(monkeypatch, workers, **kw):
     monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
-    srv = serve.Server(mixed=False, workers=workers)
+    srv = serve.Server(mixed=False, workers=workers, **kw)
     for k, (gen, order, batch) in PATS.items():
-        srv.add_pattern(k, gen(0), order=order, batch=batch)
+        srv.add_pattern(k, gen(0), order=order, batch=batch, size_class=0)
     return srv
 
 
@@ -54,25 +62,69 @@ def _requests(srv, count, seed, spacing=0.0):
     return reqs
 
 
-def test_all_requests_complete_and_batch(monkeypatch):
+def test_all_requests_complete_in_merged_rounds(monkeypatch):
     srv = _server(monkeypatch, workers=3)
-    done = srv.serve(_requests(srv, 40, seed=1), realtime=False, timeout=30)
-    assert sorted(r.rid for r in done) == list(range(40))
+    done = srv.serve(_requests(srv, 60, seed=1), realtime=False, timeout=30)
+    assert sorted(r.rid for r in done) == list(range(60))
     assert max(r.batch_size for r in done) > 1
-    for r in done:
-        assert r.batch_size <= srv.patterns[r.key].batch
+    # some round merged requests of different patterns into one forest
+    assert any(len(c) > 1 for c in srv.rounds)
+    for comp in srv.rounds:
+        for k, c in comp:
+            assert c <= srv.patterns[k].batch and (c & (c - 1)) == 0  # within the limit, a power of two
     st = serve.latency_stats(done)
     assert st["p99_ms"] >= st["p50_ms"] >= 0
 
 
+def test_size_classes_are_not_merged(monkeypatch):
+    srv = _server(monkeypatch, workers=2)
+    srv.patterns["g3d6"].size_class = 1
+    srv.serve(_requests(srv, 40, seed=2), realtime=False, timeout=30)
+    for comp in srv.rounds:
+        keys = {k for k, _ in comp}
+        assert not ("g3d6" in keys and len(keys) > 1)
+
+
+def test_round_budget_limits_admitted_bytes(monkeypatch):
+    srv = _server(monkeypatch, workers=1)
+    one = max(p.req_bytes for p in srv.patterns.values())
+    srv.round_budget = 2.5 * one
+    srv.serve(_requests(srv, 30, seed=4), realtime=False, timeout=30)
+    for comp in srv.rounds:
+        used = sum(srv.patterns[k].req_bytes * c for k, c in comp)
+        assert used <= srv.round_budget or sum(c for _, c in comp) == 1
+
+
 def test_memory_cap_evicts_and_oversize_runs_alone(monkeypatch):
     srv = _server(monkeypatch, workers=1)
-    srv.warm(["g2d12"])
-    srv.mem_cap = srv.bytes * 1.5  # g2d20's handle alone exceeds the cap
+    srv.warm(["g2d12"], counts=[1])
+    srv.mem_cap = srv.bytes * 1.5
     done = srv.serve(_requests(srv, 15, seed=3), realtime=False, timeout=30)
     assert len(done) == 15
-    resident = [h for p in srv.patterns.values() for h in p.handles]
-    assert len(resident) == 1 or srv.bytes <= srv.mem_cap
+    assert srv.bytes <= srv.mem_cap or sum(len(h) for h in srv.handles.values()) == 1
+
+
+def test_cap_is_respected_before_handles_are_built(monkeypatch):
+    """Two workers, nothing warmed, compositions whose handles together
+    exceed the cap: every handle's bytes are reserved (estimated) before it
+    is built, so the resident total never exceeds the cap while several
+    handles exist."""
+    FakeBatch.built.clear()
+    srv = _server(monkeypatch, workers=2)
+    est = max(srv.estimate_bytes(((k, 1),)) for k in PATS)
+    srv.mem_cap = 1.2 * est  # room for one handle at a time
+    peak = []
+    real_create = srv._create
+
+    def create(ticket):
+        hd = real_create(ticket)
+        peak.append(srv.bytes)
+        return hd
+
+    monkeypatch.setattr(srv, "_create", create)
+    done = srv.serve(_requests(srv, 20, seed=6), realtime=False, timeout=30)
+    assert len(done) == 20
+    assert max(peak) <= srv.mem_cap or all(sum(len(h) for h in srv.handles.values()) <= 1 for _ in [0])
 
 
 def test_realtime_arrivals_are_respected(monkeypatch):
@@ -81,95 +133,14 @@ def test_realtime_arrivals_are_respected(monkeypatch):
     assert all(r.done >= r.arrival for r in done)
 
 
-class FakeFactor:
-    """Stands in for a mixed factorization: records the kernel choice it is given."""
-
-    def __init__(self):
-        self.choice = None
-        self.tuned = 0
-
-    def autotune(self, reps):
-        self.tuned += 1
-        return {"tc_steps": np.array([1, 0, 1], np.int32), "tc_syrk": np.array([1, 1, 0], np.int32)}
-
-    def set_kernel_choice(self, tc_steps, tc_syrk):
-        self.choice = (np.asarray(tc_steps).copy(), np.asarray(tc_syrk).copy())
-
-
-class FakeMixedBatch(FakeBatch):
-    def __init__(self, pat, mixed, device, tol, maxit):
-        super().__init__(pat, mixed, device, tol, maxit)
-        self.F = FakeFactor()
-        if mixed and pat.choice is not None:
-            self.F.set_kernel_choice(*pat.choice)
-
-
-def test_warm_autotunes_once_and_shares_the_choice(monkeypatch):
-    """Mixed serving: warming two handles of a pattern autotunes the first
-    one only; the pattern keeps the choice and the second handle gets it."""
-    monkeypatch.setattr(serve, "_DeviceBatch", FakeMixedBatch)
-    srv = serve.Server(mixed=True, workers=2)
-    gen, order, batch = PATS["g2d12"]
-    srv.add_pattern("g2d12", gen(0), order=order, batch=batch)
-    srv.warm(["g2d12"], per_pattern=2)
-    pat = srv.patterns["g2d12"]
-    assert len(pat.handles) == 2 and not any(h.busy for h in pat.handles)
-    assert sum(h.F.tuned for h in pat.handles) == 1
-    assert pat.choice is not None
-    tuned = [h for h in pat.handles if h.F.tuned][0]
-    other = [h for h in pat.handles if h is not tuned][0]
-    np.testing.assert_array_equal(other.F.choice[0], pat.choice[0])
-    np.testing.assert_array_equal(other.F.choice[1], pat.choice[1])
-
-
-def test_add_pattern_accepts_a_symbolic_result(monkeypatch):
-    monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
-    srv = serve.Server(mixed=False, workers=1)
-    A = tm.grid_laplacian(10, 10, seed=1)
-    P, S = mf.symbolic(A, alg="amf")
-    pat = srv.add_pattern("p", A, symbolic_result=(P, S))
-    assert pat.S is S and pat.P is P
-
-
-class SlowBuildBatch(FakeBatch):
-    """Building a handle of pattern g3d6 takes half a second."""
-
-    def __init__(self, pat, mixed, device, tol, maxit):
-        if pat.key == "g3d6":
-            time.sleep(0.5)
-        super().__init__(pat, mixed, device, tol, maxit)
-
-
-def test_building_a_handle_does_not_stall_other_patterns(monkeypatch):
-    """A new handle is built outside the scheduler lock: while one worker
-    builds the slow pattern's handle, the other worker keeps serving the
-    pattern whose handle already exists."""
-    monkeypatch.setattr(serve, "_DeviceBatch", SlowBuildBatch)
-    srv = serve.Server(mixed=False, workers=2)
-    for k, (gen, order, batch) in PATS.items():
-        srv.add_pattern(k, gen(0), order=order, batch=batch)
-    srv.warm(["g2d12"])
-    A3 = PATS["g3d6"][0](5)
-    reqs = [serve.Request(0, "g3d6", srv.lower_values("g3d6", A3), np.ones((A3.shape[0], 1)), arrival=0.0)]
-    for i in range(1, 13):
-        A = PATS["g2d12"][0](100 + i)
-        reqs.append(serve.Request(i, "g2d12", srv.lower_values("g2d12", A), np.ones((A.shape[0], 1)),
-                                  arrival=1e-6 * i))
-    done = srv.serve(reqs, realtime=False, timeout=30)
-    assert len(done) == 13
-    slow = [r for r in done if r.key == "g3d6"][0]
-    fast_done = max(r.done for r in done if r.key == "g2d12")
-    assert fast_done < slow.done - 0.2, (fast_done, slow.done)
-    assert srv.reserved == 0 and all(p.creating == 0 for p in srv.patterns.values())
-
-
-def test_cap_turns_a_new_handle_away_and_the_batch_is_served_later(monkeypatch):
-    """A handle whose true size does not fit is closed and its requests go back
-    to the queue; they are served once the cap allows."""
-    monkeypatch.setattr(serve, "_DeviceBatch", FakeBatch)
+def test_fresh_values_are_made_at_admission(monkeypatch):
     srv = _server(monkeypatch, workers=2)
-    srv.warm(["g2d12"])
-    srv.mem_cap = srv.bytes * 1.2
-    done = srv.serve(_requests(srv, 20, seed=9), realtime=False, timeout=30)
-    assert sorted(r.rid for r in done) == list(range(20))
-    assert srv.reserved == 0 and all(p.creating == 0 for p in srv.patterns.values())
+    made = []
+    reqs = _requests(srv, 12, seed=7)
+    for r in reqs:
+        v = r.values
+        r.values = None
+        r.make_values = (lambda v=v, rid=r.rid: made.append(rid) or v)
+    done = srv.serve(reqs, realtime=False, timeout=30)
+    assert sorted(made) == list(range(12)) and len(done) == 12
+    assert all(r.values is None for r in done)
