@@ -54,7 +54,7 @@ void free_all(mf_handle* h) {
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
                     h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
-                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued};
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued, h->d_chain};
     release_graphs(h);
     if (h->cublas) cublasDestroy(static_cast<cublasHandle_t>(h->cublas));
     h->cublas = nullptr;
@@ -171,6 +171,7 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     rc = rc ? rc : dalloc(h, &h->d_R, std::max<int64_t>(h->nrval_per_rhs * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_W, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_part, std::max<int64_t>(h->nbwd_part * kNB * 16, 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_chain, std::max<int64_t>(h->nchain, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_C, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_B, std::max<int64_t>(n * nrhs_cap, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_perm, std::max<int64_t>(n, 1), &tot);
@@ -195,6 +196,10 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         std::vector<int64_t> iota((size_t)n);
         for (int64_t i = 0; i < n; ++i) iota[(size_t)i] = i;
         e = up(h->d_perm, iota.data(), sizeof(int64_t) * (size_t)n);
+    }
+    {
+        const char* cenv = getenv("MF_SOLVE_CHAIN");
+        h->solve_chain = !(cenv && cenv[0] == '0');
     }
     {
         const char* tcenv = getenv("MF_TENSOR_CORES");
@@ -348,13 +353,24 @@ static int solve_chunks(mf_handle* h, const int64_t* dperm, double* hostB, doubl
     return 0;
 }
 
+// A bounded device wait that ran out (the tensor-core pipeline's mbarriers,
+// err 1; the solve chain's progress counters, err 2) leaves *d_err set and
+// the result incomplete: report it after the call's last synchronization.
+static int wait_error(mf_handle* h, const char* where) {
+    int err = 0;
+    MF_CUDA(cudaMemcpyAsync(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    MF_CUDA(cudaStreamSynchronize(h->stream));
+    if (!err) return 0;
+    set_error(std::string(where) + (err == 2 ? ": a solve-chain wait timed out" : ": a tensor-core wait timed out"));
+    return -3;
+}
+
 int mf_div_impl(mf_handle* h, double* B, int64_t nrhs, int64_t ldb) {
     if (!h || nrhs < 0 || (nrhs > 0 && (!B || ldb < h->n))) { set_error("mf_div_impl: bad arguments"); return -1; }
     DeviceGuard g(h->device);
     int rc = solve_chunks(h, nullptr, B, nullptr, nrhs, ldb);
     if (rc) return rc;
-    MF_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return wait_error(h, "mf_div_impl");
 }
 
 int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot) {
@@ -520,8 +536,7 @@ int mf_solve(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const int64_t* 
     }
     int rc = solve_chunks(h, h->d_perm, B, nullptr, nrhs, ldb);
     if (rc) return rc;
-    MF_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return wait_error(h, "mf_solve");
 }
 
 int mf_solve_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev) {
@@ -778,8 +793,7 @@ int mf_solve_refined(mf_handle* h, double* B, int64_t nrhs, int64_t ldb, const i
     }
     int rc = refined_chunks(h, B, nullptr, nrhs, ldb, h->d_perm, tol, maxit, iters, eta);
     if (rc) return rc;
-    MF_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return wait_error(h, "mf_solve_refined");
 }
 
 int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t ldb, const int64_t* perm_dev,
@@ -790,7 +804,8 @@ int mf_solve_refined_device(mf_handle* h, double* B_dev, int64_t nrhs, int64_t l
     }
     if (!h->mixed) { set_error("mf_solve_refined_device: call mf_enable_mixed first"); return -1; }
     DeviceGuard g(h->device);
-    return refined_chunks(h, nullptr, B_dev, nrhs, ldb, perm_dev ? perm_dev : h->d_perm, tol, maxit, iters, eta);
+    const int rc = refined_chunks(h, nullptr, B_dev, nrhs, ldb, perm_dev ? perm_dev : h->d_perm, tol, maxit, iters, eta);
+    return rc ? rc : wait_error(h, "mf_solve_refined_device");
 }
 
 int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
@@ -912,8 +927,7 @@ int mf_get_factor(mf_handle* h, double* Dval, double* Lval, double* d) {
 int mf_synchronize(mf_handle* h) {
     if (!h) { set_error("null handle"); return -1; }
     DeviceGuard g(h->device);
-    MF_CUDA(cudaStreamSynchronize(h->stream));
-    return 0;
+    return wait_error(h, "mf_synchronize");
 }
 
 int mf_info(const mf_handle* h, int64_t* out) {

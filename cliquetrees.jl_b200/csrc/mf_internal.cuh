@@ -134,6 +134,13 @@ struct Level {
     ItemList s_fwd_red;      // (front, row tile, first partial slot, chunks)
     ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
     ItemList s_bwd_red;      // (front, col tile, first partial slot)
+    // the super-block chain of the blocked fronts as one launch per
+    // direction (k_s_chain): items (front, a, step K, counter base), a = -1 - q
+    // for diagonal part q, else the tile; d_chain[chain_tk] / [chain_tk + 1]
+    // are the forward / backward ticket counters
+    ItemList s_chain_f;
+    ItemList s_chain_b;
+    int64_t chain_tk = -1;
     int max_nn_blocked = 0;
     int kob = kOB;           // outer-block width of this level's panel steps (kOB or kOBWide)
     // FP32 kernel choice of this level, set by mf_autotune: 1 = tcgen05
@@ -264,6 +271,9 @@ struct mf_handle {
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
     double* d_part = nullptr;      // backward partial sums
     int64_t nbwd_part = 0;         // partial slots (max over levels)
+    int* d_chain = nullptr;        // k_s_chain ticket and progress counters, zeroed per solve
+    int64_t nchain = 0;
+    bool solve_chain = true;       // one k_s_chain launch per level and direction (MF_SOLVE_CHAIN=0: per-step launches)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
     double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
     int64_t* d_perm = nullptr;     // permutation (n)

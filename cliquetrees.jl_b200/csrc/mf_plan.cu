@@ -569,6 +569,65 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             }
             end(st.bwd);
         }
+        // the same chain as k_s_chain items: per step K, kDiagSplit diagonal
+        // parts of every front, then the tiles, the ones the next diagonal
+        // step waits for first (forward: the rows just below the super-block;
+        // backward: the columns just left of it).  Each front gets a
+        // counter block per direction: [finished diagonal parts, steps applied
+        // to each 64-row / 64-column tile of its diagonal block].
+        if (max_sblocks > 0) {
+            lv.chain_tk = h->nchain;
+            h->nchain += 2;
+            std::vector<int32_t> bf;
+            for (int32_t j : fr)
+                if (!solve_small(h->h_fronts[j])) bf.push_back(j);
+            std::vector<int32_t> cbf(bf.size()), cbb(bf.size());
+            for (size_t i = 0; i < bf.size(); ++i) {
+                cbf[i] = (int32_t)h->nchain;
+                h->nchain += 1 + cdiv(h->h_fronts[bf[i]].nn, kNB);
+            }
+            for (size_t i = 0; i < bf.size(); ++i) {
+                cbb[i] = (int32_t)h->nchain;
+                h->nchain += 1 + cdiv(h->h_fronts[bf[i]].nn, kNB);
+            }
+            const int nsplit = kSolveNB / 16;
+            auto fwd_tiles = [&](const Front& f, int k0) {
+                const int w = std::min(kSolveNB, f.nn - k0);
+                return f.nn > k0 + w ? (int)cdiv(f.nn - ((k0 + w) & ~3), kFwdRows) : 0;
+            };
+            begin(lv.s_chain_f);
+            for (int k = 0; k < max_sblocks; ++k) {
+                const int k0 = k * kSolveNB;
+                int maxt = 0;
+                for (size_t i = 0; i < bf.size(); ++i) {
+                    const Front& f = h->h_fronts[bf[i]];
+                    if (f.nn <= k0) continue;
+                    for (int q = 0; q < nsplit; ++q) items.push_back(Item{bf[i], -1 - q, k, cbf[i]});
+                    maxt = std::max(maxt, fwd_tiles(f, k0));
+                }
+                for (int t = 0; t < maxt; ++t)
+                    for (size_t i = 0; i < bf.size(); ++i) {
+                        const Front& f = h->h_fronts[bf[i]];
+                        if (f.nn > k0 && t < fwd_tiles(f, k0)) items.push_back(Item{bf[i], t, k, cbf[i]});
+                    }
+            }
+            end(lv.s_chain_f);
+            begin(lv.s_chain_b);
+            for (int k = max_sblocks - 1; k >= 0; --k) {
+                const int k0 = k * kSolveNB;
+                for (size_t i = 0; i < bf.size(); ++i)
+                    if (h->h_fronts[bf[i]].nn > k0)
+                        for (int q = 0; q < nsplit; ++q) items.push_back(Item{bf[i], -1 - q, k, cbb[i]});
+                for (int t = (int)cdiv(k0, kNB) - 1; t >= 0; --t)
+                    for (size_t i = 0; i < bf.size(); ++i)
+                        if (h->h_fronts[bf[i]].nn > k0) items.push_back(Item{bf[i], t, k, cbb[i]});
+            }
+            end(lv.s_chain_b);
+            if (h->nchain > INT32_MAX) {
+                set_error("plan: too many solve-chain counters");
+                return -3;
+            }
+        }
         // forward R -= L21 x1 of the blocked fronts: items (front, 64-row tile of
         // L21 from the 4-aligned row at or before nn, 512-column chunk, slot),
         // then one reduction item per row tile adding the chunks in order

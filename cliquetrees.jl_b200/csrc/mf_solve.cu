@@ -18,7 +18,6 @@
 namespace mf {
 
 constexpr int kMaxRhs = 16;   // right-hand sides per pass (larger counts are chunked)
-constexpr int SLD = kNB + 1;  // smem leading dimension of the diagonal block
 
 // ---------------------------------------------------------------------------
 // permutation (mul!(C, P, B), multiply.jl:277-280): C[i] = B[perm[i]]
@@ -54,6 +53,29 @@ constexpr int kSmallRows = (kSmallMax + 31) / 32;  // rows per lane (3)
 
 template <typename T, int NR>
 constexpr int small_solve_smem() { return kSmallWarps * kSmallMax * NR * (int)sizeof(T); }
+
+constexpr int kSmallChunk = 8;  // triangular-solve steps whose panel loads are issued together
+
+// Loads for steps k0 .. k0 + kSmallChunk - 1 of a small front's triangular
+// solve: lane i gets, for rows a = i + 32 s, the strictly lower entry L_ak of
+// column k (forward, TRANS = 0) or the entry L_ka of row k left of the
+// diagonal (backward, TRANS = 1), zero elsewhere, and the diagonal L_kk.
+template <typename T, int UNIT, int TRANS = 0>
+__device__ __forceinline__ void small_cols(T (&l)[kSmallChunk][kSmallRows], T (&dg)[kSmallChunk],
+                                           const T* __restrict__ Pj, int ld, int nn, int k0, int lane) {
+#pragma unroll
+    for (int q = 0; q < kSmallChunk; ++q) {
+        const int k = TRANS ? k0 - q : k0 + q;
+        const bool kv = k >= 0 && k < nn;
+#pragma unroll
+        for (int s = 0; s < kSmallRows; ++s) {
+            const int a = lane + 32 * s;
+            const bool v = kv && (TRANS ? a < k : (a > k && a < nn));
+            l[q][s] = v ? (TRANS ? Pj[k + (int64_t)a * ld] : Pj[a + (int64_t)k * ld]) : T(0);
+        }
+        dg[q] = (!UNIT && kv) ? Pj[k + (int64_t)k * ld] : T(1);
+    }
+}
 
 template <typename T, int UNIT, int NR>
 __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* __restrict__ fronts,
@@ -118,23 +140,35 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* _
             const int a = lane + 32 * s;
             x[s][r] = (a < nn && r < nrhs) ? C1[a + r * kSmallMax] : T(0);
         }
-    for (int k = 0; k < nn; ++k) {
-        const int ko = k & 31, ks = k >> 5;
-        T lk[kSmallRows];
+    // The columns come in chunks of kSmallChunk: the next chunk's loads are
+    // issued before the current chunk's steps, so the step chain waits on
+    // shuffles and FMAs rather than on one load per column.
+    T ln[kSmallChunk][kSmallRows], dn[kSmallChunk];
+    small_cols<T, UNIT>(ln, dn, Pj, ld, nn, 0, lane);
+    for (int k0 = 0; k0 < nn; k0 += kSmallChunk) {
+        T lc[kSmallChunk][kSmallRows], dc[kSmallChunk];
 #pragma unroll
-        for (int s = 0; s < kSmallRows; ++s) {
-            const int a = lane + 32 * s;
-            lk[s] = (a > k && a < nn) ? Pj[a + (int64_t)k * ld] : T(0);
+        for (int q = 0; q < kSmallChunk; ++q) {
+            dc[q] = dn[q];
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) lc[q][s] = ln[q][s];
         }
-        const T dinv = UNIT ? T(1) : T(1) / Pj[k + (int64_t)k * ld];
+        small_cols<T, UNIT>(ln, dn, Pj, ld, nn, k0 + kSmallChunk, lane);
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            T own = ks == 0 ? x[0][r] : (ks == 1 ? x[1][r] : x[2][r]);
-            const T xk = __shfl_sync(0xffffffffu, own, ko) * dinv;
+        for (int q = 0; q < kSmallChunk; ++q) {
+            const int k = k0 + q;
+            if (k >= nn) break;  // uniform across the warp
+            const int ko = k & 31, ks = k >> 5;
+            const T dinv = UNIT ? T(1) : T(1) / dc[q];
 #pragma unroll
-            for (int s = 0; s < kSmallRows; ++s) x[s][r] -= lk[s] * xk;
-            if (lane == ko) {
-                if (ks == 0) x[0][r] = xk; else if (ks == 1) x[1][r] = xk; else x[2][r] = xk;
+            for (int r = 0; r < NR; ++r) {
+                T own = ks == 0 ? x[0][r] : (ks == 1 ? x[1][r] : x[2][r]);
+                const T xk = __shfl_sync(0xffffffffu, own, ko) * dinv;
+#pragma unroll
+                for (int s = 0; s < kSmallRows; ++s) x[s][r] -= lc[q][s] * xk;
+                if (lane == ko) {
+                    if (ks == 0) x[0][r] = xk; else if (ks == 1) x[1][r] = xk; else x[2][r] = xk;
+                }
             }
         }
     }
@@ -156,6 +190,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* _
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[r] = T(0);
         const T* lr = Pj + nn + a;
+#pragma unroll 8
         for (int k = 0; k < nn; ++k) {
             const T l = lr[(int64_t)k * ld];
 #pragma unroll
@@ -173,16 +208,14 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
                                                                   const int32_t* __restrict__ septgt,
                                                                   const T* __restrict__ P, T* __restrict__ C,
                                                                   int64_t n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
     if (w >= cnt) return;
-    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;
     const Front f = fronts[items[w].front];
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
-    // C1 = C[res] - L21^T x[sep]: lanes own columns k and walk the rows a in
+    // C[res] - L21^T x[sep]: lanes own columns k and walk the rows a in
     // order, 32 rows at a time: lane i gathers x[sep[a0 + i]] for the chunk
     // (the next chunk's gather is issued before this chunk's products) and
     // the rows' x values reach the other lanes by shuffles
@@ -209,7 +242,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
         }
         const int m = min(32, na - a0);
         const T* pa = Pj + nn + a0;
-#pragma unroll 4
+#pragma unroll 8
         for (int j = 0; j < m; ++j) {
             T xb[NR];
 #pragma unroll
@@ -227,42 +260,54 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
 #pragma unroll
         for (int r = 0; r < NR; ++r) xv[r] = xn[r];
     }
+    // C1 in registers: lane i holds rows k = i + 32 s
+    T c[kSmallRows][NR];
+#pragma unroll
+    for (int s = 0; s < kSmallRows; ++s) {
+        const int k = lane + 32 * s;
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            c[s][r] = (k < nn && r < nrhs) ? C[f.col0 + k + (int64_t)r * n] - acc[s][r] : T(0);
+    }
+    // back substitution, column oriented on L^T: x_k = c_k / L_kk, k
+    // descending, then rows j < k lose L_kj x_k; the rows of L for the next
+    // kSmallChunk steps are loaded while the current ones are applied
+    T ln[kSmallChunk][kSmallRows], dn[kSmallChunk];
+    small_cols<T, UNIT, 1>(ln, dn, Pj, ld, nn, nn - 1, lane);
+    for (int k0 = nn - 1; k0 >= 0; k0 -= kSmallChunk) {
+        T lc[kSmallChunk][kSmallRows], dc[kSmallChunk];
+#pragma unroll
+        for (int q = 0; q < kSmallChunk; ++q) {
+            dc[q] = dn[q];
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) lc[q][s] = ln[q][s];
+        }
+        small_cols<T, UNIT, 1>(ln, dn, Pj, ld, nn, k0 - kSmallChunk, lane);
+#pragma unroll
+        for (int q = 0; q < kSmallChunk; ++q) {
+            const int k = k0 - q;
+            if (k < 0) break;  // uniform across the warp
+            const int ko = k & 31, ks = k >> 5;
+            const T dinv = UNIT ? T(1) : T(1) / dc[q];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+                T own = ks == 0 ? c[0][r] : (ks == 1 ? c[1][r] : c[2][r]);
+                const T xk = __shfl_sync(0xffffffffu, own, ko) * dinv;
+#pragma unroll
+                for (int s = 0; s < kSmallRows; ++s) c[s][r] -= lc[q][s] * xk;
+                if (lane == ko) {
+                    if (ks == 0) c[0][r] = xk; else if (ks == 1) c[1][r] = xk; else c[2][r] = xk;
+                }
+            }
+        }
+    }
 #pragma unroll
     for (int s = 0; s < kSmallRows; ++s) {
         const int k = lane + 32 * s;
         if (k < nn)
 #pragma unroll
             for (int r = 0; r < NR; ++r)
-                if (r < nrhs) C1[k + r * kSmallMax] = C[f.col0 + k + (int64_t)r * n] - acc[s][r];
-    }
-    __syncwarp();
-    // back substitution: x_k = (C1[k] - sum_{a>k} L_ak x_a) / L_kk, k descending
-    for (int k = nn - 1; k >= 0; --k) {
-        T part[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) part[r] = T(0);
-        for (int a = k + 1 + lane; a < nn; a += 32) {
-            const T l = Pj[a + (int64_t)k * ld];
-#pragma unroll
-            for (int r = 0; r < NR; ++r) part[r] += l * C1[a + r * kSmallMax];
-        }
-        const T dinv = UNIT ? T(1) : T(1) / Pj[k + (int64_t)k * ld];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            T v = part[r];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            part[r] = v;
-        }
-        __syncwarp();
-        if (lane == 0)
-#pragma unroll
-            for (int r = 0; r < NR; ++r)
-                if (r < nrhs) C1[k + r * kSmallMax] = (C1[k + r * kSmallMax] - part[r]) * dinv;
-        __syncwarp();
-    }
-    for (int i = lane; i < nn * nrhs; i += 32) {
-        const int a = i % nn, r = i / nn;
-        C[f.col0 + a + (int64_t)r * n] = C1[a + r * kSmallMax];
+                if (r < nrhs) C[f.col0 + k + (int64_t)r * n] = c[s][r];
     }
 }
 
@@ -344,15 +389,13 @@ __device__ __forceinline__ void cpa_wait_all() {
 // input starting at t % 16, and half-warp shuffles add the partial sums.
 constexpr int kDiagSplit = kSolveNB / 16;
 
+// W and C go through L2 only (ld/st .cg): within one k_s_chain launch other
+// CTAs write them, and L1 is not coherent across SMs.
 template <typename T, int NR, int BWD>
-__global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                 int step, const T* __restrict__ inv2, T* __restrict__ C,
-                                                 const T* __restrict__ W, int64_t n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
+__device__ __forceinline__ void sdiag_run(const Front& f, int step, int q, const T* __restrict__ inv2, T* C,
+                                          const T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
     T* b = reinterpret_cast<T*>(sm_raw);  // [r][c] : b[c + r * kSolveNB]
     T* xt = b + kSolveNB * NR;            // forward: xt[c * 16 + a - 16q]; backward: xt[(a - 16q) * 256 + c]
-    const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
-    const int q = blockIdx.x % kDiagSplit;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, f.nn - k0), ld2 = super_ld(wK);
     if (16 * q >= wK) return;  // whole CTA
     const T* X = inv2 + f.i2off + (int64_t)step * kSolveNB * kSolveNB;
@@ -369,7 +412,7 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
     }
     for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
         const int c = i % kSolveNB, r = i / kSolveNB;
-        b[i] = (c < wK && r < nrhs) ? W[f.col0 + k0 + c + (int64_t)r * n] : T(0);
+        b[i] = (c < wK && r < nrhs) ? __ldcg(W + f.col0 + k0 + c + (int64_t)r * n) : T(0);
     }
     cpa_wait_all();
     __syncthreads();
@@ -395,7 +438,16 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
     if (cl == 0 && a < wK)
 #pragma unroll
         for (int r = 0; r < NR; ++r)
-            if (r < nrhs) C[f.col0 + k0 + a + (int64_t)r * n] = acc[r];
+            if (r < nrhs) __stcg(C + f.col0 + k0 + a + (int64_t)r * n, acc[r]);
+}
+
+template <typename T, int NR, int BWD>
+__global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ inv2, T* __restrict__ C,
+                                                 const T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
+    sdiag_run<T, NR, BWD>(f, step, (int)(blockIdx.x % kDiagSplit), inv2, C, W, n, nrhs, sm_raw);
 }
 
 // 16 bytes of consecutive panel entries in one load: 4 floats or 2 doubles
@@ -425,27 +477,23 @@ template <typename T, int NR>
 constexpr int ftile_smem() { return (kSolveNB * NR + 8 * NR * kFwdRows) * (int)sizeof(T); }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
-                                                 T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
+__device__ __forceinline__ void ftile_run(const Front& f, int step, int ta, const T* __restrict__ P, const T* C,
+                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;             // rows per load
     constexpr int LPC = kFwdRows / VW;    // lanes per column (16 float, 32 double)
     constexpr int CPL = 32 / LPC;         // columns per warp load (2 float, 1 double)
-    extern __shared__ __align__(16) unsigned char sm_raw[];
     T* xs = reinterpret_cast<T*>(sm_raw);  // xs[c * NR + r]
     T* red = xs + kSolveNB * NR;           // red[(w * NR + r) * kFwdRows + row]
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
     const int rlo = k0 + wK;
-    const int ra = (rlo & ~3) + it.a * kFwdRows;
+    const int ra = (rlo & ~3) + ta * kFwdRows;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < kSolveNB * NR; i += 256) {
         const int c = i & (kSolveNB - 1), r = i / kSolveNB;
-        xs[c * NR + r] = (c < wK && r < nrhs) ? C[f.col0 + k0 + c + (int64_t)r * n] : T(0);
+        xs[c * NR + r] = (c < wK && r < nrhs) ? __ldcg(C + f.col0 + k0 + c + (int64_t)r * n) : T(0);
     }
     __syncthreads();
     const int rr = (lane % LPC) * VW, ch = lane / LPC;
@@ -486,7 +534,6 @@ __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ front
             for (int e = 0; e < VW; ++e) red[(warp * NR + r) * kFwdRows + rr + e] = acc[e][r];
     }
     __syncthreads();
-    T* Rj = R + f.roff * nrhs;
     for (int o = tid; o < kFwdRows * NR; o += 256) {
         const int rl = o & (kFwdRows - 1), r = o / kFwdRows;
         const int q = ra + rl;
@@ -494,9 +541,22 @@ __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ front
             T v = T(0);
 #pragma unroll
             for (int w = 0; w < 8; ++w) v += red[(w * NR + r) * kFwdRows + rl];
-            if (q < nn) W[f.col0 + q + (int64_t)r * n] -= v;
+            if (q < nn) {
+                T* wp = W + f.col0 + q + (int64_t)r * n;
+                __stcg(wp, __ldcg(wp) - v);
+            }
         }
     }
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
+                                                 T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    ftile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw);
 }
 
 // forward R_j -= L21 x1 for the blocked fronts of a level, once all their
@@ -611,24 +671,20 @@ template <typename T, int NR>
 constexpr int btile_smem() { return (kSolveNB * NR + 4 * NR * kNB) * (int)sizeof(T); }
 
 template <typename T, int NR>
-__global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
-                                                 T* __restrict__ W, int64_t n, int nrhs) {
+__device__ __forceinline__ void btile_run(const Front& f, int step, int ta, const T* __restrict__ P, const T* C,
+                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
     T* xs = reinterpret_cast<T*>(sm_raw);  // xs[i * NR + r]
     T* red = xs + kSolveNB * NR;           // red[(q * NR + r) * kNB + c]
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp;
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
-    const int c0 = it.a * kNB, wc = min(kNB, k0 - c0);
+    const int c0 = ta * kNB, wc = min(kNB, k0 - c0);
     const int tid = threadIdx.x;
     for (int i = tid; i < kSolveNB * NR; i += 256) {
         const int a = i & (kSolveNB - 1), r = i / kSolveNB;
-        xs[a * NR + r] = (a < wK && r < nrhs) ? C[f.col0 + k0 + a + (int64_t)r * n] : T(0);
+        xs[a * NR + r] = (a < wK && r < nrhs) ? __ldcg(C + f.col0 + k0 + a + (int64_t)r * n) : T(0);
     }
     __syncthreads();
     const int c = tid & (kNB - 1), q = tid >> 6;
@@ -669,7 +725,126 @@ __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ front
         if (cc < wc && r < nrhs) {
             const T v = red[(0 * NR + r) * kNB + cc] + red[(1 * NR + r) * kNB + cc] +
                         red[(2 * NR + r) * kNB + cc] + red[(3 * NR + r) * kNB + cc];
-            W[f.col0 + c0 + cc + (int64_t)r * n] -= v;
+            T* wp = W + f.col0 + c0 + cc + (int64_t)r * n;
+            __stcg(wp, __ldcg(wp) - v);
+        }
+    }
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int step, const T* __restrict__ P, const T* __restrict__ C,
+                                                 T* __restrict__ W, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    btile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw);
+}
+
+// ---------------------------------------------------------------------------
+// The super-block chain of a level's blocked fronts in ONE launch per
+// direction (instead of two launches per step).  The plan lists the items
+// in ticket order: per step K (ascending forward, descending backward) the
+// kDiagSplit diagonal parts of every front (it.a = -1 - q), then the tiles
+// (it.a = tile), those the next diagonal step waits for first.  CTAs take
+// items in that order from a ticket counter.  Each front has a counter
+// block in `ctl` at it.pad: [0] finished diagonal parts, [1 + g] steps
+// applied to 64-row (forward) / 64-column (backward) tile g of its diagonal
+// block.  A diagonal part of step K waits until the tiles of super-block K
+// hold every earlier step; a tile item waits for x_K (all diagonal parts of
+// step K) and for its tile's earlier steps.  Every wait is for items with
+// smaller tickets, which running CTAs already hold, so each wait ends.  Each
+// wait is still bounded (kChainWaitNs of %globaltimer): a timeout sets *err,
+// after which every wait gives up at once and the items left do nothing.
+// The arithmetic of each item is k_s_sdiag's / k_s_ftile's / k_s_btile's in
+// the same order, so results equal the per-step launches bit for bit.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kChainWaitNs = 2000000000ull;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned long long chain_clock() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+
+// bounded wait (one thread) until *p >= need; false on timeout or once *err is set
+__device__ bool chain_wait(const int* p, int need, int* err) {
+    if (ld_acquire_gpu(p) >= need) return true;
+    const unsigned long long t0 = chain_clock();
+    unsigned ns = 32;
+    for (;;) {
+        __nanosleep(ns);
+        if (ns < 256) ns <<= 1;
+        if (ld_acquire_gpu(p) >= need) return true;
+        if (*reinterpret_cast<volatile int*>(err)) return false;
+        if (chain_clock() - t0 > kChainWaitNs) {
+            atomicExch(err, 2);
+            return false;
+        }
+    }
+}
+
+template <typename T, int NR, int BWD>
+constexpr int chain_smem() {
+    return sdiag_smem<T, NR>() > (BWD ? btile_smem<T, NR>() : ftile_smem<T, NR>())
+               ? sdiag_smem<T, NR>()
+               : (BWD ? btile_smem<T, NR>() : ftile_smem<T, NR>());
+}
+
+template <typename T, int NR, int BWD>
+__global__ void __launch_bounds__(256) k_s_chain(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 int64_t cnt, int* ticket, int* ctl, const T* __restrict__ inv2,
+                                                 const T* __restrict__ P, T* C, T* W, int64_t n, int nrhs,
+                                                 int* err) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    __shared__ int s_t, s_ok;
+    for (;;) {
+        __syncthreads();  // the previous item is finished by every thread
+        if (threadIdx.x == 0) {
+            s_t = atomicAdd(ticket, 1);
+            s_ok = 1;
+        }
+        __syncthreads();
+        const int64_t t = s_t;
+        if (t >= cnt) return;
+        const Item it = items[t];
+        const Front f = fronts[it.front];
+        const int S = (f.nn + kSolveNB - 1) / kSolveNB, K = it.b;
+        const int done = BWD ? S - 1 - K : K;  // steps applied before step K
+        int* xdone = ctl + it.pad;
+        int* tiles = xdone + 1;
+        if (it.a < 0) {
+            const int g0 = K * (kSolveNB / kNB);
+            const int ng = min(kSolveNB / kNB, (f.nn - K * kSolveNB + kNB - 1) / kNB);
+            if (threadIdx.x < ng) {
+                if (!chain_wait(tiles + g0 + threadIdx.x, done, err)) s_ok = 0;
+                __threadfence();
+            }
+            __syncthreads();
+            if (s_ok) sdiag_run<T, NR, BWD>(f, K, -1 - it.a, inv2, C, W, n, nrhs, sm_raw);
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0 && s_ok) atomicAdd(xdone, 1);
+        } else {
+            const int g = BWD ? it.a : ((K + 1) * kSolveNB) / kNB + it.a;
+            if (threadIdx.x == 0) {
+                if (!chain_wait(xdone, kDiagSplit * (done + 1), err) || !chain_wait(tiles + g, done, err)) s_ok = 0;
+                __threadfence();
+            }
+            __syncthreads();
+            if (s_ok) {
+                if (BWD) btile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw);
+                else ftile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw);
+            }
+            __threadfence();
+            __syncthreads();
+            if (threadIdx.x == 0 && s_ok) atomicAdd(tiles + g, 1);
         }
     }
 }
@@ -820,6 +995,34 @@ int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* per
     return 0;
 }
 
+// one k_s_chain launch: a persistent grid of at most (resident CTAs per SM)
+// x SMs, fewer when the level has fewer items
+template <typename T, int NR, int BWD>
+static int chain_go(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int nrhs) {
+    const ItemList& il = BWD ? lv.s_chain_b : lv.s_chain_f;
+    constexpr int sm = chain_smem<T, NR, BWD>();
+    MF_CUDA(cudaFuncSetAttribute(k_s_chain<T, NR, BWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    int occ = 0;
+    MF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s_chain<T, NR, BWD>, 256, sm));
+    const int64_t grid = std::min<int64_t>(il.cnt, (int64_t)std::max(occ, 1) * std::max(h->num_sms, 1));
+    k_s_chain<T, NR, BWD><<<(unsigned)grid, 256, sm, h->stream>>>(h->d_fronts, h->d_items + il.off, il.cnt,
+                                                                  h->d_chain + lv.chain_tk + BWD, h->d_chain,
+                                                                  sb.inv2, sb.P, sb.C, sb.W, h->n, nrhs, h->d_err);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename T, int BWD>
+static int launch_chain(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int nrb, int nrhs) {
+    switch (nrb) {
+        case 1: return chain_go<T, 1, BWD>(h, lv, sb, nrhs);
+        case 2: return chain_go<T, 2, BWD>(h, lv, sb, nrhs);
+        case 4: return chain_go<T, 4, BWD>(h, lv, sb, nrhs);
+        case 8: return chain_go<T, 8, BWD>(h, lv, sb, nrhs);
+        default: return chain_go<T, 16, BWD>(h, lv, sb, nrhs);
+    }
+}
+
 template <typename T, int UNIT>
 static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     if (h->profile) {
@@ -845,11 +1048,11 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small_solve_smem<T, 16>()));
-    MF_CUDA(cudaFuncSetAttribute(k_s_small_bwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 small_solve_smem<T, 16>()));
     const int nrb = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
     const Item* items = h->d_items;
     const int64_t n = h->n;
+    const bool chain = h->solve_chain && h->nchain > 0;
+    if (chain) MF_CUDA(cudaMemsetAsync(h->d_chain, 0, sizeof(int) * (size_t)h->nchain, h->stream));
     // forward: levels ascending
     for (const Level& lv : h->levels) {
         if (lv.s_small.cnt) {
@@ -877,7 +1080,11 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
                 h->d_fronts, items + lv.s_gather.off, items, h->d_reltgt, sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
-        for (size_t k = 0; k < lv.s_steps.size(); ++k) {
+        if (chain && lv.s_chain_f.cnt) {
+            Timer t(h, K_S_FWD);
+            if (int rc = launch_chain<T, 0>(h, lv, sb, nrb, nrhs)) return rc;
+        }
+        for (size_t k = 0; !chain && k < lv.s_steps.size(); ++k) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.diag.cnt) continue;
             Timer t(h, K_S_FWD);
@@ -895,11 +1102,11 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
                 const unsigned gf = (unsigned)st.fwd.cnt;
                 const Item* itf = items + st.fwd.off;
                 switch (nrb) {
-                    case 1: k_s_ftile<T, 1><<<gf, 256, ftile_smem<T, 1>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
-                    case 2: k_s_ftile<T, 2><<<gf, 256, ftile_smem<T, 2>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
-                    case 4: k_s_ftile<T, 4><<<gf, 256, ftile_smem<T, 4>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
-                    case 8: k_s_ftile<T, 8><<<gf, 256, ftile_smem<T, 8>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
-                    default: k_s_ftile<T, 16><<<gf, 256, ftile_smem<T, 16>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, sb.R, n, nrhs); break;
+                    case 1: k_s_ftile<T, 1><<<gf, 256, ftile_smem<T, 1>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: k_s_ftile<T, 2><<<gf, 256, ftile_smem<T, 2>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: k_s_ftile<T, 4><<<gf, 256, ftile_smem<T, 4>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: k_s_ftile<T, 8><<<gf, 256, ftile_smem<T, 8>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: k_s_ftile<T, 16><<<gf, 256, ftile_smem<T, 16>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
                 }
                 MF_CUDA(cudaGetLastError());
             }
@@ -945,7 +1152,11 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
                                                                               sb.part, sb.C, sb.W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
-        for (size_t k = lv.s_steps.size(); k-- > 0;) {
+        if (chain && lv.s_chain_b.cnt) {
+            Timer t(h, K_S_BWD);
+            if (int rc = launch_chain<T, 1>(h, lv, sb, nrb, nrhs)) return rc;
+        }
+        for (size_t k = lv.s_steps.size(); !chain && k-- > 0;) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.diag.cnt) continue;
             Timer t(h, K_S_BWD);
@@ -978,15 +1189,15 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const Item* it = items + lv.s_small.off;
             const int64_t c = lv.s_small.cnt;
             switch (nrb) {
-                case 1: k_s_small_bwd<T, UNIT, 1><<<g, kSmallWarps * 32, small_solve_smem<T, 1>(), h->stream>>>(
+                case 1: k_s_small_bwd<T, UNIT, 1><<<g, kSmallWarps * 32, 0, h->stream>>>(
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 2: k_s_small_bwd<T, UNIT, 2><<<g, kSmallWarps * 32, small_solve_smem<T, 2>(), h->stream>>>(
+                case 2: k_s_small_bwd<T, UNIT, 2><<<g, kSmallWarps * 32, 0, h->stream>>>(
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 4: k_s_small_bwd<T, UNIT, 4><<<g, kSmallWarps * 32, small_solve_smem<T, 4>(), h->stream>>>(
+                case 4: k_s_small_bwd<T, UNIT, 4><<<g, kSmallWarps * 32, 0, h->stream>>>(
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 8: k_s_small_bwd<T, UNIT, 8><<<g, kSmallWarps * 32, small_solve_smem<T, 8>(), h->stream>>>(
+                case 8: k_s_small_bwd<T, UNIT, 8><<<g, kSmallWarps * 32, 0, h->stream>>>(
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                default: k_s_small_bwd<T, UNIT, 16><<<g, kSmallWarps * 32, small_solve_smem<T, 16>(), h->stream>>>(
+                default: k_s_small_bwd<T, UNIT, 16><<<g, kSmallWarps * 32, 0, h->stream>>>(
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());

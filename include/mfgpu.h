@@ -188,7 +188,11 @@ int mf_selinv(mf_handle* h);
  * Synchronises the handle's stream. */
 int mf_logdet(mf_handle* h, double* logabsdet, double* sign);
 
-/* Wait for the handle's stream. */
+/* Wait for the handle's stream.  Returns -3 if a bounded device wait of
+ * the work it ran timed out (the tensor-core pipeline, or the one-launch
+ * super-block solve chain), so the result of the asynchronous calls
+ * (mf_solve_device, mf_solve_device_static) is incomplete; mf_solve,
+ * mf_div_impl and the refined solves check the same before they return. */
 int mf_synchronize(mf_handle* h);
 
 /* Sizes: out[0..8] = n, nfr, ndz, nlz, panel values, update values,

@@ -139,12 +139,12 @@ def test_autotune_keeps_refined_accuracy():
     F.close()
 
 
-def _fp32_breakdown_matrix(side=12, dense=False):
-    """SPD in FP64, but its FP32 factorization meets a zero pivot: unit
-    diagonal, off-diagonals 1e-12 except one pair at 1 - 1e-10, which rounds
-    to 1 in single precision (the pair's Schur complement 2e-10 vanishes).
-    A grid pattern gives small fronts; dense=True one front of side x side
-    columns (blocked: 64 x 64 diagonal blocks)."""
+def _fp32_rounding_breakdown_matrix(side=12, dense=False):
+    """SPD in FP64, singular once ROUNDED to FP32: unit diagonal,
+    off-diagonals 1e-12 except one pair at 1 - 1e-10, which rounds to 1 in
+    single precision (the pair's Schur complement 2e-10 vanishes).  No
+    per-front redo can help -- the FP32 inputs have lost the information --
+    so the whole factorization falls back to FP64."""
     if dense:
         n = side
         rows, cols = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
@@ -152,19 +152,46 @@ def _fp32_breakdown_matrix(side=12, dense=False):
     else:
         A = tm.grid_laplacian(side, side, seed=1).tocoo()
     vals = np.where(A.row == A.col, 1.0, -1e-12)
-    u, v = 40, 41  # neighbours on the grid; inside the first 64 x 64 block of the dense front
+    u, v = 40, 41  # neighbours on the grid
     vals[((A.row == u) & (A.col == v)) | ((A.row == v) & (A.col == u))] = -(1.0 - 1e-10)
     return sp.csc_matrix((vals, (A.row, A.col)), shape=A.shape)
 
 
+def _fp32_cancellation_matrix(side=12, dense=False):
+    """SPD with every entry exact in FP32, but a pivot that cancels to about
+    1e-7 of its diagonal entry inside one front: the clique {a, b, c} with
+    unit diagonal, a_ca = 0.75 and a_cb = v, the float just below
+    sqrt(0.4375), so the pivot of c is 0.4375 - v^2 > 0 (exact in FP64).
+    The single-precision small-pivot check flags it and the front (small:
+    a separate 3-vertex component) or 64 x 64 diagonal block (dense=True:
+    one 130-column front, natural order, c = column 42 in block 0) is
+    factored again in FP64 from the same FP32 inputs."""
+    v = np.float32(np.sqrt(0.4375))
+    if float(v) ** 2 >= 0.4375:
+        v = np.nextafter(v, np.float32(0))
+    v = float(v)
+    if dense:
+        n = side
+        A = np.full((n, n), -1e-12)
+        np.fill_diagonal(A, 1.0)
+        a, b, c = 40, 41, 42
+        A[c, a] = A[a, c] = 0.75
+        A[c, b] = A[b, c] = v
+        return sp.csc_matrix(A)
+    G = tm.grid_laplacian(side, side, seed=1).tocoo()
+    G = sp.csc_matrix((np.where(G.row == G.col, 1.0, -1e-12), (G.row, G.col)), shape=G.shape)
+    T = np.array([[1.0, -1e-12, 0.75], [-1e-12, 1.0, v], [0.75, v, 1.0]])
+    return sp.block_diag([G, sp.csc_matrix(T)]).tocsc()
+
+
 @pytest.mark.parametrize("dense", [False, True])
-def test_single_precision_pivot_failure_is_rescued_per_front(dense):
-    """North-star precision rule: an FP32 pivot rejection refactors only the
-    flagged front (nj <= 67, in the small-front kernel) or 64 x 64 diagonal
-    block (blocked front) in FP64 on the GPU -- not the whole matrix -- and
-    the refinement still reaches 1e-12."""
-    A = _fp32_breakdown_matrix(130 if dense else 12, dense=dense)
-    P, S = mf.symbolic(A)
+def test_single_precision_small_pivot_is_rescued_per_front(dense):
+    """North-star precision rule: an FP32 pivot flagged by the small-pivot
+    check refactors only the flagged front (nj <= 67, in the small-front
+    kernel) or 64 x 64 diagonal block (blocked front) in FP64 on the GPU --
+    not the whole matrix -- and the refinement still reaches 1e-12."""
+    A = _fp32_cancellation_matrix(130 if dense else 12, dense=dense)
+    P, S = mf.symbolic(A, alg="natural" if dense else "amf")
     if dense:
         assert S.nfr == 1 and S.n == 130
     F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
@@ -175,10 +202,31 @@ def test_single_precision_pivot_failure_is_rescued_per_front(dense):
     X = mf.ldiv(F, B)
     it, eta = F.last_refinement
     assert eta <= 1e-12 and tm.backward_error(A, X, B).max() <= 1e-12, (it, eta)
-    # a well-conditioned matrix on the same handle needs no rescue
-    F.copyto(tm.grid_laplacian(12, 12, seed=2) if not dense else sp.csc_matrix(np.eye(130) * 2 + A - sp.diags(A.diagonal())))
+    # a well-conditioned matrix on the same pattern needs no rescue
+    W = A.copy()
+    W.data = np.where(W.data > 0.5, W.data, -1e-3)
+    W.setdiag(2.0)
+    F.copyto(W)
     mf.cholesky_(F)
     assert F.rescued == 0 and not F.used_fp64
+    F.close()
+
+
+@pytest.mark.parametrize("dense", [False, True])
+def test_single_precision_rounding_breakdown_falls_back_to_fp64(dense):
+    """A matrix that is singular once rounded to FP32 cannot be rescued per
+    front (the FP64 redo reads the same rounded inputs): the FP32
+    factorization reports it and the handle factors the matrix in FP64; the
+    refined solve still meets 1e-12."""
+    A = _fp32_rounding_breakdown_matrix(130 if dense else 12, dense=dense)
+    P, S = mf.symbolic(A)
+    F = mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))
+    assert F.info == 0
+    assert F.used_fp64
+    B = tm.rhs(S.n, 3, seed=4)
+    X = mf.ldiv(F, B)
+    it, eta = F.last_refinement
+    assert eta <= 1e-12 and tm.backward_error(A, X, B).max() <= 1e-12, (it, eta)
     F.close()
 
 

@@ -39,22 +39,45 @@ def test_dynamic_regularization_known_answer():
         mf.cholesky_(F)
 
 
+def _negative_root_pivots(A, P, S):
+    """A with the diagonal of the last column of every elimination-tree root
+    lowered by 1.5 times that column's pivot, so exactly those pivots come out
+    negative and are regularized; no later pivot depends on them (a pivot
+    replaced by delta earlier in the tree would grow every later Schur
+    complement by 1/delta and overflow on a deep tree)."""
+    Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
+    info, Dw, _, _ = oracle.chol_impl(S, Dval, Lval, 0)
+    assert info == 0
+    A = A.tolil()
+    for j in S.roots():
+        nn = S.nn(j)
+        c = S.res(j)[-1]
+        piv = Dw[S.Dptr[j] + (nn - 1) * (nn + 1)] ** 2
+        v = P.perm[c]
+        A[v, v] = A[v, v] - 1.5 * piv
+    return A.tocsc()
+
+
 @pytest.mark.parametrize("big", [False, True])
 def test_dynamic_regularization_matches_oracle(big):
-    """An indefinite grid matrix (diagonal shifted down at every 7th vertex):
-    the rejected pivots are replaced by delta on the GPU exactly as in the
-    oracle; small fronts (k_small) and blocked fronts (k_diag) both."""
-    A = tm.grid_laplacian(26, 25, 24, seed=8) if big else tm.grid_laplacian(30, 29, seed=8)
-    A = A.tolil()
-    for v in range(0, A.shape[0], 7):
-        A[v, v] = -abs(A[v, v])
-    A = A.tocsc()
-    order = mf.grid_nd_order(26, 25, 24) if big else "amf"
+    """Negative pivots at the roots' last columns are replaced by delta on the
+    GPU exactly as in the oracle; small fronts (k_small: nine separate 7 x 6
+    grids, nine roots) and a blocked front (k_diag: the 3D grid's root)."""
+    if big:
+        A = tm.grid_laplacian(26, 25, 24, seed=8)
+        order = mf.grid_nd_order(26, 25, 24)
+    else:
+        A = sp.block_diag([tm.grid_laplacian(7, 6, seed=8 + i) for i in range(9)]).tocsc()
+        order = "amf"
     P, S = mf.symbolic(A, alg=order)
+    A = _negative_root_pivots(A, P, S)
+    with pytest.raises(mf.PosDefException):
+        mf.cholesky_(mf.ChordalCholesky(A, P, S))
     F = mf.cholesky_(mf.ChordalCholesky(A, P, S), reg=mf.DynamicRegularization())
     Dval, Lval, _, _ = oracle.assemble(S, P.invp, A)
     info, Dw, Lw, dw = oracle.chol_impl(S, Dval, Lval, 0, reg=(-1.0, -1.0))
     assert info == 0 and F.info == 0
+    assert np.all(np.isfinite(Dw)) and np.all(np.isfinite(Lw))
     assert_factor_close(S, F.factor_arrays(), (Dw, Lw, dw), 0, rtol=1e-9)
     F.close()
 

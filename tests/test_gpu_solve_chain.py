@@ -1,0 +1,61 @@
+"""The blocked fronts' super-block solve chain as one persistent k_s_chain
+launch per level and direction (MF_SOLVE_CHAIN=1, the default) against the
+per-step launches (MF_SOLVE_CHAIN=0): the items do the same arithmetic in the
+same order, so the solutions must be bitwise equal; both are checked against
+the oracle (normwise backward error <= 1e-13, FP64; <= 1e-12 refined)."""
+import numpy as np
+import pytest
+
+import multifrontal as mf
+from multifrontal import testmatrices as tm
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def grid(nx, ny, nz, seed):
+    A = tm.grid_laplacian(nx, ny, nz, seed=seed, lo=1e-2, hi=1e2)
+    P, S = mf.symbolic(A, alg=mf.grid_nd_order(nx, ny, nz))
+    return A, P, S
+
+
+def both(monkeypatch, make, B):
+    X = {}
+    for v in ("0", "1"):
+        monkeypatch.setenv("MF_SOLVE_CHAIN", v)
+        F = make()
+        X[v] = mf.ldiv(F, B)
+        F.close()
+    return X
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+@pytest.mark.parametrize("nrhs", [1, 3, 16])
+def test_chain_equals_per_step_launches(monkeypatch, ldlt, nrhs):
+    # root separator 32 x 30 = 960 columns (4 super-blocks), two 480-column
+    # fronts on the level below it: several fronts per level with 2-4 steps
+    A, P, S = grid(32, 30, 31, seed=61)
+    B = tm.rhs(S.n, nrhs, seed=nrhs)
+    make = (lambda: mf.ldlt_(mf.ChordalLDLt(A, P, S))) if ldlt else (lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)))
+    X = both(monkeypatch, make, B)
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, int(ldlt))
+    assert np.abs(X["1"] - Xo).max() <= 1e-9 * np.abs(Xo).max()
+
+
+def test_chain_mixed_refined(monkeypatch):
+    A, P, S = grid(30, 29, 28, seed=62)
+    B = tm.rhs(S.n, 4, seed=3)
+    X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True)), B)
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-12
+
+
+def test_chain_partial_last_super_block(monkeypatch):
+    # a root of 21 x 19 = 399 columns: one full super-block and a 143-column one
+    A, P, S = grid(21, 19, 24, seed=63)
+    B = tm.rhs(S.n, 2, seed=4)
+    X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)), B)
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
