@@ -271,9 +271,10 @@ struct mf_handle {
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
     double* d_part = nullptr;      // backward partial sums
     int64_t nbwd_part = 0;         // partial slots (max over levels)
+    mf::ItemList sub_tasks;        // k_s_sub_fwd / _bwd tasks (subtrees of small fronts), one CTA each
     int* d_chain = nullptr;        // k_s_chain ticket and progress counters, zeroed per solve
     int64_t nchain = 0;
-    bool solve_chain = true;       // one k_s_chain launch per level and direction (MF_SOLVE_CHAIN=0: per-step launches)
+    bool solve_chain = false;      // one k_s_chain launch per level and direction (MF_SOLVE_CHAIN=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
     double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
     int64_t* d_perm = nullptr;     // permutation (n)

@@ -294,9 +294,70 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     h->npanel = poff;
     h->ninv = ioff;
     h->ninv2 = ioff2;
+    // ---- subtrees of small fronts solved in one launch per direction
+    // (k_s_sub_fwd / k_s_sub_bwd).  A front heads a task subtree when it
+    // and all its descendants are solve-small, the subtree's cost (one unit
+    // per front plus its panel entries / 256) is at most wmax, and its
+    // parent's subtree is not such a subtree; consecutive heads are packed
+    // into one task up to wmax.  wmax spreads the small part of the forest
+    // over about 16 tasks per SM (148 SMs), at least 48 units.
+    // Opt-in (MF_SUBTREE_SOLVE=1 in the environment): measured slower than
+    // the per-level launches on the 80^3, 100^2 and batched 2D workloads --
+    // a task's narrow levels leave most of its warps idle, while a level
+    // launch keeps every front of the level in flight.
+    std::vector<int32_t> task_of(nex, -1);
+    std::vector<std::vector<int32_t>> task_heads;
+    const char* stenv = getenv("MF_SUBTREE_SOLVE");
+    if (stenv && stenv[0] == '1') {
+        std::vector<char> allsmall(nex, 0);
+        std::vector<double> cost(nex, 0.0);
+        for (int L = 0; L <= max_level; ++L)
+            for (int64_t e = 0; e < nex; ++e) {
+                if (level[e] != L) continue;
+                const Front& f = h->h_fronts[e];
+                bool ok = solve_small(f);
+                double c = 1.0 + (double)(f.nn + f.na) * f.nn / 256.0;
+                for (int32_t p = f.chd0; p < f.chd1; ++p) {
+                    const int32_t ch = h->h_exec_chd[(size_t)p];
+                    ok = ok && allsmall[ch];
+                    c += cost[ch];
+                }
+                allsmall[e] = ok;
+                cost[e] = c;
+            }
+        double tot = 0.0;
+        for (int64_t e = 0; e < nex; ++e)
+            if (allsmall[e] && (eparent[e] < 0 || !allsmall[eparent[e]])) tot += cost[e];
+        const double wmax = std::max(48.0, tot / (148.0 * 16.0));
+        auto fits = [&](int64_t e) { return allsmall[e] && cost[e] <= wmax; };
+        double acc = 0.0;
+        for (int64_t e = 0; e < nex; ++e) {
+            if (!fits(e) || (eparent[e] >= 0 && fits(eparent[e]))) continue;
+            if (task_heads.empty() || acc + cost[e] > wmax) {
+                task_heads.emplace_back();
+                acc = 0.0;
+            }
+            task_heads.back().push_back((int32_t)e);
+            acc += cost[e];
+        }
+        for (size_t t = 0; t < task_heads.size(); ++t) {
+            std::vector<int32_t> stack(task_heads[t].begin(), task_heads[t].end());
+            while (!stack.empty()) {
+                const int32_t e = stack.back();
+                stack.pop_back();
+                task_of[e] = (int32_t)t;
+                const Front& f = h->h_fronts[e];
+                for (int32_t p = f.chd0; p < f.chd1; ++p) stack.push_back(h->h_exec_chd[(size_t)p]);
+            }
+        }
+    }
     {
         // slot lifetimes: produced at level(e), read while level(parent(e))
-        // is processed, reusable from the next level on
+        // is processed, reusable from the next level on.  The solve's update
+        // blocks of task fronts live in a region of their own per task (its
+        // CTA walks the task's levels at its own pace, concurrently with the
+        // other tasks), reused inside the task by the same rule; a head's
+        // block stays until its parent reads it.
         std::vector<std::vector<int32_t>> born(max_level + 1), dies(max_level + 1);
         for (int64_t e = 0; e < nex; ++e) {
             if (h->h_fronts[e].na == 0) continue;
@@ -304,20 +365,32 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             dies[level[eparent[e]]].push_back((int32_t)e);
         }
         PoolAllocator pm, pr;
+        std::vector<PoolAllocator> ptask(task_heads.size());
         for (int L = 0; L <= max_level; ++L) {
             for (int32_t e : born[L]) {
                 Front& f = h->h_fronts[e];
                 f.moff = pm.alloc((int64_t)f.ldm * f.na);
-                f.roff = pr.alloc((int64_t)f.na);  // rows; block is R + roff*nrhs
+                const int32_t t = task_of[e];
+                f.roff = t < 0 ? pr.alloc((int64_t)f.na) : ptask[(size_t)t].alloc((int64_t)f.na);
             }
             for (int32_t e : dies[L]) {
                 Front& f = h->h_fronts[e];
                 pm.release(f.moff, (int64_t)f.ldm * f.na);
-                pr.release(f.roff, (int64_t)f.na);
+                const int32_t t = task_of[e];
+                if (t < 0) pr.release(f.roff, (int64_t)f.na);
+                else if (task_of[eparent[e]] == t) ptask[(size_t)t].release(f.roff, (int64_t)f.na);
             }
         }
         h->nmval = pm.high_water();
-        h->nrval_per_rhs = pr.high_water();
+        int64_t rbase = pr.high_water();
+        std::vector<int64_t> tbase(task_heads.size());
+        for (size_t t = 0; t < task_heads.size(); ++t) {
+            tbase[t] = rbase;
+            rbase += ptask[t].high_water();
+        }
+        for (int64_t e = 0; e < nex; ++e)
+            if (task_of[e] >= 0 && h->h_fronts[e].na > 0) h->h_fronts[e].roff += tbase[(size_t)task_of[e]];
+        h->nrval_per_rhs = rbase;
     }
 
     // ---- work lists
@@ -503,7 +576,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (solve_small(f)) push(j, 0, 0);
+            if (solve_small(f) && task_of[j] < 0) push(j, 0, 0);
         }
         end(lv.s_small);
         // forward gather: item (front, row tile, first segment, segments);
@@ -666,6 +739,44 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_bwd_red);
         for (const Item& r : red) items.push_back(r);
         end(lv.s_bwd_red);
+    }
+    // task lists: task items {first level item, end}, level items {first
+    // front item, end, height}, front items {front}; fronts of a task sorted
+    // by height (a front's height exceeds its children's)
+    {
+        const int64_t ntask = (int64_t)task_heads.size();
+        std::vector<std::vector<int32_t>> members((size_t)ntask);
+        for (int64_t e = 0; e < nex; ++e)
+            if (task_of[e] >= 0) members[(size_t)task_of[e]].push_back((int32_t)e);
+        std::vector<Item> tlev, tfr;
+        std::vector<Item> tasks((size_t)ntask);
+        for (int64_t t = 0; t < ntask; ++t) {
+            std::vector<int32_t>& m = members[(size_t)t];
+            std::stable_sort(m.begin(), m.end(), [&](int32_t a, int32_t b) { return level[a] < level[b]; });
+            tasks[(size_t)t].front = (int32_t)tlev.size();
+            size_t i = 0;
+            while (i < m.size()) {
+                size_t k = i;
+                while (k < m.size() && level[m[k]] == level[m[i]]) ++k;
+                tlev.push_back(Item{(int32_t)tfr.size(), (int32_t)(tfr.size() + (k - i)), level[m[i]], 0});
+                for (size_t q = i; q < k; ++q) tfr.push_back(Item{m[q], 0, 0, 0});
+                i = k;
+            }
+            tasks[(size_t)t].a = (int32_t)tlev.size();
+        }
+        // absolute item indices: tasks, then levels, then fronts
+        const int64_t tb = (int64_t)items.size(), lb = tb + ntask, fb = lb + (int64_t)tlev.size();
+        if (fb + (int64_t)tfr.size() > INT32_MAX) {
+            set_error("plan: too many work items");
+            return -3;
+        }
+        for (Item& t : tasks) { t.front += (int32_t)lb; t.a += (int32_t)lb; }
+        for (Item& l : tlev) { l.front += (int32_t)fb; l.a += (int32_t)fb; }
+        h->sub_tasks.off = tb;
+        h->sub_tasks.cnt = ntask;
+        items.insert(items.end(), tasks.begin(), tasks.end());
+        items.insert(items.end(), tlev.begin(), tlev.end());
+        items.insert(items.end(), tfr.begin(), tfr.end());
     }
     {
         const int64_t base = (int64_t)items.size();

@@ -236,14 +236,17 @@ __global__ void k_seg_eta(const double* __restrict__ segred, int64_t nseg, int n
     if (threadIdx.x < 16) out[threadIdx.x] = mx[threadIdx.x];
 }
 
-// ||A||_inf (max absolute row sum) into *out
+// ||A||_inf (max absolute row sum) into *out: one row per thread, the
+// warp's maximum by shuffles, one atomic per warp (one per row serialised
+// every thread of the grid on the same address)
 __global__ void k_anorm(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
                         const double* __restrict__ nz, double* __restrict__ out, int64_t n) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double s = 0.0;
-    for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) s += fabs(nz[src[p]]);
-    atomic_max_nonneg(out, s);
+    if (i < n)
+        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) s += fabs(nz[src[p]]);
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, s);
 }
 
 // per-column partial dot products: part[blk * 16 + r]
@@ -266,12 +269,16 @@ __global__ void k_dot_part(const double* __restrict__ u, const double* __restric
 }
 
 // out[r] = sum over blocks (fixed order)
+// one warp per right-hand side: lane l adds blocks l, l + 32, ... in order,
+// then a fixed shuffle tree (deterministic, and the loads of a lane are
+// independent instead of one dependent chain over all blocks)
 __global__ void k_dot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int nrhs) {
-    int r = threadIdx.x;
+    const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (r >= nrhs) return;
     double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += part[b * 16 + r];
-    out[r] = s;
+    for (int b = lane; b < nblocks; b += 32) s += part[b * 16 + r];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[r] = s;
 }
 
 // CG scalars: mode 0: alpha = rz / pq; mode 1: beta = rz_new / rz, rz = rz_new
@@ -394,15 +401,17 @@ __global__ void k_mdot_part(const double* __restrict__ V, int64_t vs, int J, con
 }
 
 // out[i * 16 + r] = sum over blocks (fixed order)
+// one warp per output (i, r), as k_dot_final
 __global__ void k_mdot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int J,
                              int nrhs) {
-    for (int o = threadIdx.x; o < J * 16; o += blockDim.x) {
-        const int i = o / 16, r = o % 16;
-        if (r >= nrhs) continue;
-        double s = 0.0;
-        for (int b = 0; b < nblocks; ++b) s += part[((int64_t)b * J + i) * 16 + r];
-        out[o] = s;
-    }
+    const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (o >= J * 16) return;
+    const int i = o / 16, r = o % 16;
+    if (r >= nrhs) return;
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += part[((int64_t)b * J + i) * 16 + r];
+    for (int q = 16; q > 0; q >>= 1) s += __shfl_xor_sync(0xffffffffu, s, q);
+    if (lane == 0) out[o] = s;
 }
 
 // w(:, r) -= sum_{i < J} c[i * 16 + r] V_i(:, r)
@@ -533,7 +542,7 @@ static int dot(mf_handle* h, const double* u, const double* v, double* out, int 
     double* part = h->d_red + kRedPart;
     k_dot_part<<<kRedBlocks, 256, 0, h->stream>>>(u, v, part, h->n, nrhs);
     MF_CUDA(cudaGetLastError());
-    k_dot_final<<<1, 32, 0, h->stream>>>(part, out, kRedBlocks, nrhs);
+    k_dot_final<<<1, 32 * 16, 0, h->stream>>>(part, out, kRedBlocks, nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
@@ -636,7 +645,7 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
         } else {
             k_mdot_part<<<nblk, 256, 0, h->stream>>>(Vb, vs, J, w, part, n, nrhs);
             MF_CUDA(cudaGetLastError());
-            k_mdot_final<<<1, 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
+            k_mdot_final<<<(unsigned)((J * 16 + 7) / 8), 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
         }
         MF_CUDA(cudaGetLastError());
         MF_CUDA(cudaMemcpyAsync(out_host, coef, sizeof(double) * J * Q, cudaMemcpyDeviceToHost, h->stream));

@@ -54,7 +54,14 @@ constexpr int kSmallRows = (kSmallMax + 31) / 32;  // rows per lane (3)
 template <typename T, int NR>
 constexpr int small_solve_smem() { return kSmallWarps * kSmallMax * NR * (int)sizeof(T); }
 
-constexpr int kSmallChunk = 8;  // triangular-solve steps whose panel loads are issued together
+constexpr int kSmallChunk = 4;  // triangular-solve steps whose panel loads are issued together
+
+// Resident 128-thread CTAs per SM the small-front solves are compiled for
+// (a register budget): the per-front work is a chain of dependent loads, so
+// warps in flight set the throughput; wide right-hand-side blocks need the
+// registers instead.
+template <typename T, int NR>
+constexpr int small_min_blocks() { return sizeof(T) == 4 ? (NR <= 4 ? 6 : 4) : (NR <= 4 ? 4 : 2); }
 
 // Loads for steps k0 .. k0 + kSmallChunk - 1 of a small front's triangular
 // solve: lane i gets, for rows a = i + 32 s, the strictly lower entry L_ak of
@@ -77,19 +84,14 @@ __device__ __forceinline__ void small_cols(T (&l)[kSmallChunk][kSmallRows], T (&
     }
 }
 
+// One small front's forward step, by one warp (C1: the warp's shared slice,
+// C1[a + r * kSmallMax]).  The children's update blocks are read through L2
+// (ld.cg): in k_s_sub_fwd another warp of the CTA wrote them.
 template <typename T, int UNIT, int NR>
-__global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* __restrict__ fronts,
-                                                                  const Item* __restrict__ items, int64_t cnt,
-                                                                  const int32_t* __restrict__ reltgt,
-                                                                  const int32_t* __restrict__ chdtgt,
-                                                                  const T* __restrict__ P, T* __restrict__ C,
-                                                                  T* __restrict__ R, int64_t n, int nrhs) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
-    if (w >= cnt) return;  // whole warps only
-    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;  // [r][a] : C1[a + r * kSmallMax]
-    const Front f = fronts[items[w].front];
+__device__ __forceinline__ void small_fwd_front(const Front& f, const Front* __restrict__ fronts,
+                                                const int32_t* __restrict__ reltgt,
+                                                const int32_t* __restrict__ chdtgt, const T* __restrict__ P,
+                                                T* C, T* R, int64_t n, int nrhs, T* C1, int lane) {
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     T* Rj = R + f.roff * nrhs;
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* _
                 mv[u] = T(0);
                 if (i < ma * nrhs) {
                     qv[u] = rel[i % ma];
-                    mv[u] = Mc[i];
+                    mv[u] = __ldcg(Mc + i);
                 }
             }
 #pragma unroll
@@ -203,15 +205,26 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_fwd(const Front* _
 }
 
 template <typename T, int UNIT, int NR>
-__global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* __restrict__ fronts,
+__global__ void __launch_bounds__(kSmallWarps * 32, small_min_blocks<T, NR>()) k_s_small_fwd(const Front* __restrict__ fronts,
                                                                   const Item* __restrict__ items, int64_t cnt,
-                                                                  const int32_t* __restrict__ septgt,
+                                                                  const int32_t* __restrict__ reltgt,
+                                                                  const int32_t* __restrict__ chdtgt,
                                                                   const T* __restrict__ P, T* __restrict__ C,
-                                                                  int64_t n, int nrhs) {
+                                                                  T* __restrict__ R, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
-    if (w >= cnt) return;
+    if (w >= cnt) return;  // whole warps only
+    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;
     const Front f = fronts[items[w].front];
+    small_fwd_front<T, UNIT, NR>(f, fronts, reltgt, chdtgt, P, C, R, n, nrhs, C1, lane);
+}
+
+// One small front's backward step, by one warp.  x[sep] is read through L2
+// (ld.cg): in k_s_sub_bwd the ancestors' warps of the same CTA wrote it.
+template <typename T, int UNIT, int NR>
+__device__ __forceinline__ void small_bwd_front(const Front& f, const int32_t* __restrict__ septgt,
+                                                const T* __restrict__ P, T* C, int64_t n, int nrhs, int lane) {
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const int32_t* sep = septgt + f.sep0;
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
         const bool v = lane < na;
         const int64_t row = v ? sep[lane] : 0;
 #pragma unroll
-        for (int r = 0; r < NR; ++r) xv[r] = (v && r < nrhs) ? C[row + (int64_t)r * n] : T(0);
+        for (int r = 0; r < NR; ++r) xv[r] = (v && r < nrhs) ? __ldcg(C + row + (int64_t)r * n) : T(0);
     }
     for (int a0 = 0; a0 < na; a0 += 32) {
         T xn[NR];
@@ -238,7 +251,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
             const bool v = a < na;
             const int64_t row = v ? sep[a] : 0;
 #pragma unroll
-            for (int r = 0; r < NR; ++r) xn[r] = (v && r < nrhs) ? C[row + (int64_t)r * n] : T(0);
+            for (int r = 0; r < NR; ++r) xn[r] = (v && r < nrhs) ? __ldcg(C + row + (int64_t)r * n) : T(0);
         }
         const int m = min(32, na - a0);
         const T* pa = Pj + nn + a0;
@@ -308,6 +321,73 @@ __global__ void __launch_bounds__(kSmallWarps * 32) k_s_small_bwd(const Front* _
 #pragma unroll
             for (int r = 0; r < NR; ++r)
                 if (r < nrhs) C[f.col0 + k + (int64_t)r * n] = c[s][r];
+    }
+}
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kSmallWarps * 32, small_min_blocks<T, NR>()) k_s_small_bwd(const Front* __restrict__ fronts,
+                                                                  const Item* __restrict__ items, int64_t cnt,
+                                                                  const int32_t* __restrict__ septgt,
+                                                                  const T* __restrict__ P, T* __restrict__ C,
+                                                                  int64_t n, int nrhs) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
+    if (w >= cnt) return;
+    const Front f = fronts[items[w].front];
+    small_bwd_front<T, UNIT, NR>(f, septgt, P, C, n, nrhs, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Subtrees of small fronts in ONE launch per direction: CTA b takes task
+// items[task0 + b] = {first level item, end}; each level item {first front
+// item, end} lists the task's fronts of one tree height.  The CTA's warps
+// take the fronts of a height one per warp (the per-front code of
+// k_s_small_fwd / _bwd) and a block barrier separates the heights, ascending
+// forward (children before parents) and descending backward.  Tasks are
+// disjoint subtrees, so CTAs never wait on one another; what would be one
+// launch per tree level for these fronts is one launch in all.
+// ---------------------------------------------------------------------------
+constexpr int kSubWarps = 8;
+
+template <typename T, int NR>
+constexpr int sub_solve_smem() { return kSubWarps * kSmallMax * NR * (int)sizeof(T); }
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2) k_s_sub_fwd(const Front* __restrict__ fronts,
+                                                              const Item* __restrict__ items, int64_t task0,
+                                                              const int32_t* __restrict__ reltgt,
+                                                              const int32_t* __restrict__ chdtgt,
+                                                              const T* __restrict__ P, T* __restrict__ C,
+                                                              T* __restrict__ R, int64_t n, int nrhs) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;
+    const Item tk = items[task0 + blockIdx.x];
+    for (int L = tk.front; L < tk.a; ++L) {
+        const Item lv = items[L];
+        for (int i = lv.front + wib; i < lv.a; i += kSubWarps) {
+            const Front f = fronts[items[i].front];
+            small_fwd_front<T, UNIT, NR>(f, fronts, reltgt, chdtgt, P, C, R, n, nrhs, C1, lane);
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2) k_s_sub_bwd(const Front* __restrict__ fronts,
+                                                              const Item* __restrict__ items, int64_t task0,
+                                                              const int32_t* __restrict__ septgt,
+                                                              const T* __restrict__ P, T* __restrict__ C,
+                                                              int64_t n, int nrhs) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const Item tk = items[task0 + blockIdx.x];
+    for (int L = tk.a - 1; L >= tk.front; --L) {
+        const Item lv = items[L];
+        for (int i = lv.front + wib; i < lv.a; i += kSubWarps) {
+            const Front f = fronts[items[i].front];
+            small_bwd_front<T, UNIT, NR>(f, septgt, P, C, n, nrhs, lane);
+        }
+        __syncthreads();
     }
 }
 
@@ -761,9 +841,12 @@ __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ front
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kChainWaitNs = 2000000000ull;
 
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+// the poll is a relaxed load (an acquire load would also drop the SM's L1
+// lines on every poll, slowing the working CTAs beside it); the caller's
+// fence after a successful wait orders the data reads that follow
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
     int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -775,13 +858,13 @@ __device__ __forceinline__ unsigned long long chain_clock() {
 
 // bounded wait (one thread) until *p >= need; false on timeout or once *err is set
 __device__ bool chain_wait(const int* p, int need, int* err) {
-    if (ld_acquire_gpu(p) >= need) return true;
+    if (ld_relaxed_gpu(p) >= need) return true;
     const unsigned long long t0 = chain_clock();
     unsigned ns = 32;
     for (;;) {
         __nanosleep(ns);
         if (ns < 256) ns <<= 1;
-        if (ld_acquire_gpu(p) >= need) return true;
+        if (ld_relaxed_gpu(p) >= need) return true;
         if (*reinterpret_cast<volatile int*>(err)) return false;
         if (chain_clock() - t0 > kChainWaitNs) {
             atomicExch(err, 2);
@@ -1048,11 +1131,34 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     MF_CUDA(cudaFuncSetAttribute(k_s_bwd_l<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_smem<T, 4>()));
     MF_CUDA(cudaFuncSetAttribute(k_s_small_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  small_solve_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sub_fwd<T, UNIT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 sub_solve_smem<T, 16>()));
+    MF_CUDA(cudaFuncSetAttribute(k_s_sub_fwd<T, UNIT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 sub_solve_smem<T, 8>()));
     const int nrb = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
     const Item* items = h->d_items;
     const int64_t n = h->n;
     const bool chain = h->solve_chain && h->nchain > 0;
     if (chain) MF_CUDA(cudaMemsetAsync(h->d_chain, 0, sizeof(int) * (size_t)h->nchain, h->stream));
+    if (h->sub_tasks.cnt) {
+        // the subtrees of small fronts, forward, in one launch
+        Timer t(h, K_S_SMALL);
+        const unsigned g = (unsigned)h->sub_tasks.cnt;
+        const int64_t t0 = h->sub_tasks.off;
+        switch (nrb) {
+            case 1: k_s_sub_fwd<T, UNIT, 1><<<g, kSubWarps * 32, sub_solve_smem<T, 1>(), h->stream>>>(
+                        h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+            case 2: k_s_sub_fwd<T, UNIT, 2><<<g, kSubWarps * 32, sub_solve_smem<T, 2>(), h->stream>>>(
+                        h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+            case 4: k_s_sub_fwd<T, UNIT, 4><<<g, kSubWarps * 32, sub_solve_smem<T, 4>(), h->stream>>>(
+                        h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+            case 8: k_s_sub_fwd<T, UNIT, 8><<<g, kSubWarps * 32, sub_solve_smem<T, 8>(), h->stream>>>(
+                        h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+            default: k_s_sub_fwd<T, UNIT, 16><<<g, kSubWarps * 32, sub_solve_smem<T, 16>(), h->stream>>>(
+                        h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
+        }
+        MF_CUDA(cudaGetLastError());
+    }
     // forward: levels ascending
     for (const Level& lv : h->levels) {
         if (lv.s_small.cnt) {
@@ -1202,6 +1308,25 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             }
             MF_CUDA(cudaGetLastError());
         }
+    }
+    if (h->sub_tasks.cnt) {
+        // the subtrees of small fronts, backward, in one launch
+        Timer t(h, K_S_SMALL);
+        const unsigned g = (unsigned)h->sub_tasks.cnt;
+        const int64_t t0 = h->sub_tasks.off;
+        switch (nrb) {
+            case 1: k_s_sub_bwd<T, UNIT, 1><<<g, kSubWarps * 32, 0, h->stream>>>(
+                        h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+            case 2: k_s_sub_bwd<T, UNIT, 2><<<g, kSubWarps * 32, 0, h->stream>>>(
+                        h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+            case 4: k_s_sub_bwd<T, UNIT, 4><<<g, kSubWarps * 32, 0, h->stream>>>(
+                        h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+            case 8: k_s_sub_bwd<T, UNIT, 8><<<g, kSubWarps * 32, 0, h->stream>>>(
+                        h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+            default: k_s_sub_bwd<T, UNIT, 16><<<g, kSubWarps * 32, 0, h->stream>>>(
+                        h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
+        }
+        MF_CUDA(cudaGetLastError());
     }
     return 0;
 }

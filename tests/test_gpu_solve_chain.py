@@ -1,8 +1,10 @@
 """The blocked fronts' super-block solve chain as one persistent k_s_chain
-launch per level and direction (MF_SOLVE_CHAIN=1, the default) against the
-per-step launches (MF_SOLVE_CHAIN=0): the items do the same arithmetic in the
-same order, so the solutions must be bitwise equal; both are checked against
-the oracle (normwise backward error <= 1e-13, FP64; <= 1e-12 refined)."""
+launch per level and direction (MF_SOLVE_CHAIN=1) against the per-step
+launches (MF_SOLVE_CHAIN=0, the default), and the small-front subtrees in one
+launch per direction (MF_SUBTREE_SOLVE=1) against the per-level launches:
+the items do the same arithmetic in the same order, so the solutions must be
+bitwise equal; both are checked against the oracle (normwise backward error
+<= 1e-13, FP64; <= 1e-12 refined)."""
 import numpy as np
 import pytest
 
@@ -19,10 +21,10 @@ def grid(nx, ny, nz, seed):
     return A, P, S
 
 
-def both(monkeypatch, make, B):
+def both(monkeypatch, make, B, var="MF_SOLVE_CHAIN"):
     X = {}
     for v in ("0", "1"):
-        monkeypatch.setenv("MF_SOLVE_CHAIN", v)
+        monkeypatch.setenv(var, v)
         F = make()
         X[v] = mf.ldiv(F, B)
         F.close()
@@ -57,5 +59,20 @@ def test_chain_partial_last_super_block(monkeypatch):
     A, P, S = grid(21, 19, 24, seed=63)
     B = tm.rhs(S.n, 2, seed=4)
     X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)), B)
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+def test_subtree_solves_equal_per_level_launches(monkeypatch, ldlt):
+    """Small fronts as subtree tasks (own update-block regions, one CTA per
+    task) give the per-level results bit for bit: a 2D grid under AMF (most
+    fronts small) and a batch-like forest of separate grids."""
+    import scipy.sparse as sp
+    A = sp.block_diag([tm.grid_laplacian(40, 38, seed=64)] + [tm.grid_laplacian(9, 8, seed=70 + i) for i in range(12)]).tocsc()
+    P, S = mf.symbolic(A)
+    B = tm.rhs(S.n, 3, seed=5)
+    make = (lambda: mf.ldlt_(mf.ChordalLDLt(A, P, S))) if ldlt else (lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)))
+    X = both(monkeypatch, make, B, var="MF_SUBTREE_SOLVE")
     assert np.array_equal(X["0"], X["1"])
     assert tm.backward_error(A, X["1"], B).max() <= 1e-13
