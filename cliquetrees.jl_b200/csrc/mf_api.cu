@@ -19,6 +19,7 @@ template <typename T>
 int dalloc(mf_handle* h, T** p, int64_t count, int64_t* total) {
     *p = nullptr;
     if (count <= 0) return 0;
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     cudaError_t e = cudaMalloc((void**)p, sizeof(T) * (size_t)count);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -46,6 +47,7 @@ struct DeviceGuard {
 };
 
 void free_all(mf_handle* h) {
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     void* ptrs[] = {h->d_fronts, h->d_septgt, h->d_reltgt, h->d_chdtgt, h->d_colfront, h->d_ref, h->d_sepmap,
                     h->d_items,  h->d_P,      h->d_M,      h->d_d,      h->d_signs,    h->d_info, h->d_R,
                     h->d_W,      h->d_C,      h->d_B,      h->d_perm,   h->d_DL,       h->d_slot, h->d_pslot,
@@ -152,6 +154,9 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     for (int64_t j = 0; j < nfr; ++j)
         for (int64_t c = resptr[j]; c < resptr[j + 1]; ++c) colfront[c] = (int32_t)j;
     rc = 0;
+    // allocations and the synchronous uploads below stay clear of other
+    // threads' stream captures
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     rc = rc ? rc : dalloc(h, &h->d_fronts, nex, &tot);
     rc = rc ? rc : dalloc(h, &h->d_septgt, nsep, &tot);
     rc = rc ? rc : dalloc(h, &h->d_reltgt, (int64_t)h->h_exec_rel.size(), &tot);
@@ -253,7 +258,8 @@ int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* s
     if (rc) return rc;
     int64_t launches = 0;
     for (const Level& lv : h.levels) {
-        launches += (lv.small.cnt > 0) + (lv.ea.cnt > 0) + (lv.ea_upd.cnt > 0) + (lv.syrk.cnt > 0);
+        launches += (lv.small_warp.cnt > 0) + (lv.small.cnt > 0) + (lv.ea.cnt > 0) + (lv.ea_upd.cnt > 0) +
+                    (lv.syrk.cnt > 0);
         for (const PanelStep& st : lv.steps)
             launches += (st.left.cnt > 0) + (st.diag.cnt > 0) + (st.panel.cnt > 0) + (st.trail.cnt > 0);
     }
@@ -459,6 +465,7 @@ int mf_set_assembly(mf_handle* h, int64_t nnz, const int64_t* slot) {
             if (r != c) { ccol[pos[c]] = (int32_t)r; csrc[pos[c]++] = k; }
         }
     }
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     void* olds[] = {h->d_pslot, h->d_nz, h->d_nzrow, h->d_nzcol, h->d_dslot, h->d_csrptr, h->d_csrcol, h->d_csrsrc};
     for (void* o : olds)
         if (o) cudaFree(o);
@@ -561,6 +568,7 @@ static int64_t fp64_bytes(const mf_handle* h) {
 int mf::have_fp64(const mf_handle* h) { return h->d_P != nullptr || h->npanel == 0; }
 
 int mf::ensure_fp64(mf_handle* h) {
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     if (have_fp64(h) && (h->d_M || h->nmval <= 0)) return 0;
     int64_t tot = 0;
     int rc = 0;
@@ -588,9 +596,11 @@ int mf_enable_mixed(mf_handle* h) {
     if (!h->d_csrptr) { set_error("mf_enable_mixed: call mf_set_assembly first"); return -1; }
     if (h->mixed) return 0;
     DeviceGuard g(h->device);
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     // the FP64 factor storage is only needed if a factorization falls back
-    // to FP64: release it first (ensure_fp64 brings it back on demand)
-    MF_CUDA(cudaDeviceSynchronize());
+    // to FP64: release it first (ensure_fp64 brings it back on demand); only
+    // this handle's stream can be using it
+    MF_CUDA(cudaStreamSynchronize(h->stream));
     release_graphs(h);
     if (h->d_P) {
         for (double** p : {&h->d_P, &h->d_inv, &h->d_inv2, &h->d_M}) {
@@ -822,6 +832,7 @@ int mf_set_segments(mf_handle* h, int64_t nseg, const int64_t* segptr) {
             if (segptr[s + 1] < segptr[s]) { set_error("mf_set_segments: boundaries must not decrease"); return -1; }
     }
     DeviceGuard g(h->device);
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     // only this handle's work can use the buffers replaced below
     MF_CUDA(cudaStreamSynchronize(h->stream));
     release_graphs(h);

@@ -280,6 +280,135 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
 }
 
 // ---------------------------------------------------------------------------
+// Tiny fronts (nj <= kWarpFrontMax): one WARP per front, kWarpFronts fronts per
+// CTA, warp-synchronous (no block barriers).  Lane r holds row r of the front
+// in the warp's slice of shared memory (leading dimension kWLD, sized for
+// FP64 so a flagged single-precision front can be redone in place).  The
+// arithmetic is k_small's: the children added in the reference's reverse
+// order, one addition per entry and child, then the right-looking partial
+// factorization with the same update expression.
+// ---------------------------------------------------------------------------
+constexpr int kWarpFrontMax = 32;
+constexpr int kWLD = 33;
+constexpr int kWarpFronts = 8;
+constexpr int kWarpSlice = kWLD * kWarpFrontMax * (int)sizeof(double);  // bytes per warp
+
+template <typename TC, typename T, int LDLT>
+__device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ fronts,
+                          const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
+                          const T* __restrict__ P, const T* __restrict__ M, const double* __restrict__ signs,
+                          bool check, bool* flag, Reg reg, int lane) {
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const T* Pj = P + f.poff;
+    const bool row = lane < nj;
+#pragma unroll 4
+    for (int c = 0; c < nj; ++c)
+        if (row) F[lane + c * kWLD] = c < nn ? (TC)Pj[lane + (int64_t)c * ld] : TC(0);
+    __syncwarp();
+    // extend-add, children popped in reverse (cholesky.jl:506-514)
+    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
+        const Front fc = fronts[chdtgt[p]];
+        const int ma = fc.na, lm = fc.ldm;
+        const int32_t* rel = reltgt + fc.sep0;
+        const T* Mc = M + fc.moff;
+        const int ra = lane < ma ? rel[lane] : 0;
+#pragma unroll 4
+        for (int b = 0; b < ma; ++b) {
+            const int rb = __shfl_sync(0xffffffffu, ra, b);
+            if (lane >= b && lane < ma) F[ra + rb * kWLD] += (TC)Mc[lane + b * lm];
+        }
+        __syncwarp();
+    }
+    // right-looking partial factorization of the first nn columns
+    for (int k = 0; k < nn; ++k) {
+        TC piv = F[k + k * kWLD];
+        const double s = pivot_sign(signs, LDLT, f.col0 + k);
+        if (reg.delta >= 0.0) {
+            piv = (TC)reg_pivot(reg, s, (double)piv);
+            if (piv == TC(0)) return k;  // uniform across the warp
+        } else if (!pivot_ok(s, (double)piv) || (!LDLT && !(piv > TC(0)))) {
+            return k;  // uniform across the warp
+        }
+        if (check) {
+            const double a0 = fabs((double)Pj[k + (int64_t)k * ld]);
+            const double ap = fabs((double)piv);
+            if (ap < kRescueSmall * a0 || ap > kRescueGrowth * fmax(a0, 1.0)) *flag = true;
+        }
+        const TC dk = LDLT ? piv : sqrt(piv);
+        const TC inv = TC(1) / dk;
+        __syncwarp();
+        if (lane == k) F[k + k * kWLD] = LDLT ? piv : dk;
+        if (lane > k && row) F[lane + k * kWLD] *= inv;
+        __syncwarp();
+        if (lane > k && row) {
+            const TC lr = F[lane + k * kWLD];
+            for (int c = k + 1; c <= lane; ++c) {
+                TC lc = F[c + k * kWLD];
+                if (LDLT) lc *= piv;
+                F[lane + c * kWLD] -= lr * lc;
+            }
+        }
+        __syncwarp();
+    }
+    return -1;
+}
+
+template <typename TC, typename T, int LDLT>
+__device__ void warp_front_store(const TC* F, const Front& f, T* __restrict__ P, T* __restrict__ M,
+                                 T* __restrict__ d, int lane) {
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    T* Pj = P + f.poff;
+    if (lane < nj)
+        for (int c = 0; c < nn; ++c) Pj[lane + (int64_t)c * ld] = (T)F[lane + c * kWLD];
+    if (LDLT && lane < nn) d[f.col0 + lane] = (T)F[lane + lane * kWLD];
+    T* Mj = M + f.moff;
+    const int lm = f.ldm;
+    if (lane < na)
+        for (int b = 0; b < na; ++b) Mj[lane + b * lm] = (T)F[(nn + lane) + (nn + b) * kWLD];
+}
+
+template <typename T, int LDLT>
+__global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __restrict__ fronts,
+                                                                const Item* __restrict__ items, int64_t cnt,
+                                                                const int32_t* __restrict__ reltgt,
+                                                                const int32_t* __restrict__ chdtgt,
+                                                                T* __restrict__ P, T* __restrict__ M,
+                                                                T* __restrict__ d, const double* __restrict__ signs,
+                                                                long long* __restrict__ info,
+                                                                int* __restrict__ rescued, Reg reg) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (int64_t)blockIdx.x * kWarpFronts + wib;
+    if (w >= cnt) return;  // whole warps only
+    unsigned char* slice = smem_raw + (size_t)wib * kWarpSlice;
+    const Front f = fronts[items[w].front];
+    constexpr bool single = sizeof(T) == 4;
+    bool flag = false;
+    T* F = reinterpret_cast<T*>(slice);
+    int bad = warp_front<T, T, LDLT>(F, f, fronts, reltgt, chdtgt, P, M, signs, single, &flag, reg, lane);
+    if (single && (bad >= 0 || flag)) {
+        // the panel and the children's update matrices are only read before
+        // the final store: refactor from the same inputs in FP64
+        double* F64 = reinterpret_cast<double*>(slice);
+        __syncwarp();
+        bool unused = false;
+        bad = warp_front<double, T, LDLT>(F64, f, fronts, reltgt, chdtgt, P, M, signs, false, &unused, reg, lane);
+        if (bad < 0) {
+            if (lane == 0) atomicAdd(rescued, 1);
+            __syncwarp();
+            warp_front_store<double, T, LDLT>(F64, f, P, M, d, lane);
+            return;
+        }
+    }
+    if (bad >= 0) {
+        if (lane == 0) atomicMin(info, (long long)(f.col0 + bad + 1));
+        return;
+    }
+    __syncwarp();
+    warp_front_store<T, T, LDLT>(F, f, P, M, d, lane);
+}
+
+// ---------------------------------------------------------------------------
 // extend-add for blocked fronts
 // ---------------------------------------------------------------------------
 
@@ -1091,6 +1220,8 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     constexpr int gs = gemm_smem<T>();
     MF_CUDA(cudaFuncSetAttribute(k_small<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmallMax * kSmallMax * (int)sizeof(T)));
+    MF_CUDA(cudaFuncSetAttribute(k_small_warp<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kWarpFronts * kWarpSlice));
     MF_CUDA(cudaFuncSetAttribute(k_diag<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_inv256<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv256_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
@@ -1107,6 +1238,14 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     }
     for (size_t L = 0; L < h->levels.size(); ++L) {
         const Level& lv = h->levels[L];
+        if (lv.small_warp.cnt) {
+            Timer t(h, K_SMALL);
+            const unsigned g = (unsigned)((lv.small_warp.cnt + kWarpFronts - 1) / kWarpFronts);
+            k_small_warp<T, LDLT><<<g, kWarpFronts * 32, kWarpFronts * kWarpSlice, h->stream>>>(
+                h->d_fronts, items + lv.small_warp.off, lv.small_warp.cnt, h->d_reltgt, h->d_chdtgt, fb.P, fb.M,
+                fb.d, h->d_signs, h->d_info, h->d_rescued, reg);
+            MF_CUDA(cudaGetLastError());
+        }
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
             k_small<T, LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream>>>(
@@ -1225,6 +1364,7 @@ int run_captured(mf_handle* h, int64_t k0, int64_t k1, int64_t k2, int64_t k3, c
             MF_CUDA(cudaGraphLaunch(g.exec, h->stream));
             return 0;
         }
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     MF_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     const int rc = body();
     cudaGraph_t graph = nullptr;
@@ -1347,6 +1487,7 @@ int launch_logdet(mf_handle* h, double* logabsdet, double* sign) {
         return -1;
     }
     if (!h->d_logdet) {
+        std::lock_guard<std::recursive_mutex> lk(device_mutex());
         MF_CUDA(cudaMalloc((void**)&h->d_logdet, sizeof(double) * 3 * kLogdetBlocks));
         h->bytes += (int64_t)sizeof(double) * 3 * kLogdetBlocks;
     }

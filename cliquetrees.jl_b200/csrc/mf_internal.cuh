@@ -6,6 +6,7 @@
 
 #include <functional>
 #include <string>
+#include <mutex>
 #include <vector>
 
 namespace mf {
@@ -113,7 +114,8 @@ struct SolveStep {
 };
 
 struct Level {
-    ItemList small;          // (front)           fused small-front kernel
+    ItemList small_warp;     // (front)           fronts with nj <= 32: one warp each (k_small_warp)
+    ItemList small;          // (front)           other fronts with nj <= kSmallMax: one CTA each (k_small)
     // extend-add for blocked fronts, item (front, col tile, row chunk, first
     // segment): ea adds the children into the panel columns before the
     // panel is factored; ea_upd adds them into the update matrix after the
@@ -343,6 +345,11 @@ struct mf_handle {
 namespace mf {
 
 void set_error(const std::string& msg);
+// Held while a stream is being captured into a CUDA graph and around every
+// device allocation, free or device-wide synchronisation of the library:
+// those calls fail ("operation not permitted when stream is capturing") if
+// another thread's stream is capturing at the same moment.
+std::recursive_mutex& device_mutex();
 int cuda_fail(cudaError_t e, const char* where);
 
 #define MF_CUDA(call)                                                  \

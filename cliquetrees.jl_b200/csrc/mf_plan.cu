@@ -18,6 +18,11 @@ namespace mf {
 static thread_local std::string g_last_error;
 
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+std::recursive_mutex& device_mutex() {
+    static std::recursive_mutex mu;
+    return mu;
+}
 const char* last_error() { return g_last_error.c_str(); }
 
 int cuda_fail(cudaError_t e, const char* where) {
@@ -409,10 +414,16 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         Level& lv = h->levels[L];
         const std::vector<int32_t>& fr = by_level[L];
         // factorization
+        begin(lv.small_warp);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (f.nn + f.na <= 32) push(j, 0, 0);
+        }
+        end(lv.small_warp);
         begin(lv.small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn + f.na <= kSmallMax) push(j, 0, 0);
+            if (f.nn + f.na > 32 && f.nn + f.na <= kSmallMax) push(j, 0, 0);
         }
         end(lv.small);
         int max_steps = 0;

@@ -614,6 +614,7 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
     const int64_t npart = (int64_t)std::max<int64_t>(148 * 4, seg ? h->nchunk : 0) * (M + 1) * 16;
     const int64_t need = (int64_t)(2 * M + 1) * n * h->nrhs_cap + npart + (M + 1) * Q + 64 * 16;
     if (h->kry_doubles < need) {
+        std::lock_guard<std::recursive_mutex> lk(device_mutex());
         if (h->d_kry) cudaFree(h->d_kry);
         h->d_kry = nullptr;
         h->kry_doubles = 0;

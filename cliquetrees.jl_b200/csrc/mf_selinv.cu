@@ -177,6 +177,9 @@ static int cublas_fail(cublasStatus_t s, const char* where) {
     } while (0)
 
 int launch_selinv(mf_handle* h) {
+    // allocations, frees and cuBLAS setup below must not meet another
+    // thread's stream capture
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     if (h->diag) { set_error("mf_selinv: selected inversion is defined for Cholesky factorizations"); return -1; }
     if (!have_fp64(h) || (h->mixed && !h->fp64_current)) {
         set_error("mf_selinv: needs the FP64 factor of the current matrix (mf_factorize)");

@@ -589,6 +589,7 @@ static int build_maps(mf_handle* h) {
     }
     void* dm = nullptr;
     void* di = nullptr;
+    std::lock_guard<std::recursive_mutex> lk(device_mutex());
     MF_CUDA(cudaMalloc(&dm, sizeof(CUtensorMap) * maps.size()));
     cudaError_t e = cudaMalloc(&di, sizeof(CUtensorMap));
     if (e == cudaSuccess) e = cudaMemcpy(dm, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice);

@@ -267,7 +267,7 @@ class Server:
             if not hd.busy:
                 hd.busy = True
                 return hd
-        if len(self.handles.get(comp, [])) + self.creating.get(comp, 0) >= 2:
+        if len(self.handles.get(comp, [])) + self.creating.get(comp, 0) >= self.workers:
             return None
         est = self.estimate_bytes(comp)
         if not self._make_room(comp, est):
@@ -390,9 +390,11 @@ class Server:
                         comp = self._form_round(waiting)
                         if comp is not None:
                             got = self._acquire(comp)
-                            if got is None and len(comp) > 1 or (got is None and comp[0][1] > 1):
-                                # the merged composition has no free handle and none can be
-                                # built now: the oldest request's pattern alone
+                            exists = len(self.handles.get(comp, [])) + self.creating.get(comp, 0) > 0
+                            if got is None and not exists and (len(comp) > 1 or comp[0][1] > 1):
+                                # the composition has no handle and none can be built
+                                # under the cap now: the oldest request's pattern alone
+                                # (while its handles are only busy, the round waits for one)
                                 heads = [(q[0].arrival, k) for k, q in waiting.items() if q]
                                 k0 = min(heads)[1]
                                 comp = ((k0, 1),)
