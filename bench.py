@@ -814,7 +814,7 @@ def run_served(args, work, local):
         dv = dvec(seed)
         return base * dv[lrow] * dv[lcol]
 
-    srv.warm(per_pattern=min(2, W))
+    srv.warm(per_pattern=W)
 
     def stream(count, rate, seed):
         # every request's values are made before the stream is served: the

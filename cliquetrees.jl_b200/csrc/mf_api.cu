@@ -56,7 +56,7 @@ void free_all(mf_handle* h) {
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
                     h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
-                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued, h->d_chain};
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued, h->d_chain, h->f32.split};
     release_graphs(h);
     if (h->cublas) cublasDestroy(static_cast<cublasHandle_t>(h->cublas));
     h->cublas = nullptr;
@@ -206,6 +206,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         // the one-launch chain measured slower than the per-step launches
         // on the 80^3 workload (critical path per step unchanged, waits
         // added), so it is opt-in: MF_SOLVE_CHAIN=1
+        const char* senv = getenv("MF_TC_SPLIT");
+        h->tc_split = !(senv && senv[0] == '0');
         const char* cenv = getenv("MF_SOLVE_CHAIN");
         h->solve_chain = cenv && cenv[0] == '1';
     }
@@ -613,6 +615,8 @@ int mf_enable_mixed(mf_handle* h) {
     int rc = 0;
     const int64_t n = h->n, cap = h->nrhs_cap;
     rc = rc ? rc : dalloc(h, &h->f32.P, std::max<int64_t>(h->npanel, 1), &tot);
+    if (h->tc_split)
+        rc = rc ? rc : dalloc(h, &h->f32.split, std::max<int64_t>(h->nsplit_units * kSplitUnitFloats, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.M, std::max<int64_t>(h->nmval, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.inv, std::max<int64_t>(h->ninv, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->f32.inv2, std::max<int64_t>(h->ninv2, 1), &tot);

@@ -288,8 +288,8 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
 // order, one addition per entry and child, then the right-looking partial
 // factorization with the same update expression.
 // ---------------------------------------------------------------------------
-constexpr int kWarpFrontMax = 32;
-constexpr int kWLD = 33;
+constexpr int kWarpFrontMax = kWarpSmallNJ;  // 16: lanes 16..31 idle, registers and shared memory small
+constexpr int kWLD = kWarpFrontMax + 1;
 constexpr int kWarpFronts = 8;
 constexpr int kWarpSlice = kWLD * kWarpFrontMax * (int)sizeof(double);  // bytes per warp
 
@@ -301,9 +301,15 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const bool row = lane < nj;
-#pragma unroll 4
-    for (int c = 0; c < nj; ++c)
-        if (row) F[lane + c * kWLD] = c < nn ? (TC)Pj[lane + (int64_t)c * ld] : TC(0);
+    {
+        // every panel load of the lane in flight at once, then the stores
+        T v[kWarpFrontMax];
+#pragma unroll
+        for (int c = 0; c < kWarpFrontMax; ++c) v[c] = (row && c < nn) ? Pj[lane + (int64_t)c * ld] : T(0);
+#pragma unroll
+        for (int c = 0; c < kWarpFrontMax; ++c)
+            if (row && c < nj) F[lane + c * kWLD] = (TC)v[c];
+    }
     __syncwarp();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
     for (int p = f.chd1 - 1; p >= f.chd0; --p) {
@@ -312,10 +318,13 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
         const int32_t* rel = reltgt + fc.sep0;
         const T* Mc = M + fc.moff;
         const int ra = lane < ma ? rel[lane] : 0;
-#pragma unroll 4
-        for (int b = 0; b < ma; ++b) {
+        T mv[kWarpFrontMax];
+#pragma unroll
+        for (int b = 0; b < kWarpFrontMax; ++b) mv[b] = (b < ma && lane >= b && lane < ma) ? Mc[lane + b * lm] : T(0);
+#pragma unroll
+        for (int b = 0; b < kWarpFrontMax; ++b) {
             const int rb = __shfl_sync(0xffffffffu, ra, b);
-            if (lane >= b && lane < ma) F[ra + rb * kWLD] += (TC)Mc[lane + b * lm];
+            if (b < ma && lane >= b && lane < ma) F[ra + rb * kWLD] += (TC)mv[b];
         }
         __syncwarp();
     }
@@ -524,8 +533,258 @@ __device__ __forceinline__ void diag_pivot<double, 1>(double p, double& dk, doub
 // identity beyond column w), X (inverse), pivs (L_kk or d_k), rinv (their
 // reciprocals).  Returns the first rejected pivot (block-local) or -1,
 // uniform across the block; bad_s is a shared scratch int.
+//
+// Four 16-column panels with look-ahead.  Panel p: warp 0 factors its 16 x 16
+// diagonal block in registers (the pivot chain, by shuffles) while warps 1..7
+// apply panel p-1's update to every entry below that block (the rows and
+// columns the later panels read); then every thread with a row below solves
+// that row against the panel's triangle (forward substitution in registers),
+// and the next panel's 16 x 16 diagonal block takes panel p's update, so warp
+// 0 can start on it at once.  The chain therefore waits for no bulk update.
+// The 16 x 16 inverses (warps 0..3 at once) and the off-diagonal blocks of X
+// follow the factorization.
 template <typename TC, int LDLT>
-__device__ int diag_block(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double* __restrict__ signs,
+__device__ __forceinline__ void diag_factor16(TC* A, TC* pivs, TC* rinv, int pb, int w,
+                                              const double* __restrict__ signs, int64_t colbase, int* bad_s,
+                                              const Reg& reg, int lane) {
+    using T = TC;
+    const int i = lane & 15;  // lanes 16..31 mirror 0..15
+    T a[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) a[j] = j <= i ? A[(pb + i) + (pb + j) * LDA] : T(0);
+    T mypiv = T(1), myrinv = T(1);
+    int bad = -1;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        T pv = __shfl_sync(0xffffffffu, a[k], k);
+        if (reg.delta >= 0.0) {
+            if (pb + k < w) {
+                pv = (T)reg_pivot(reg, pivot_sign(signs, LDLT, colbase + pb + k), (double)pv);
+                if (i == k) a[k] = pv;
+                if (bad < 0 && pv == T(0)) bad = pb + k;
+            }
+        } else if (bad < 0 && pb + k < w) {
+            const double sg = pivot_sign(signs, LDLT, colbase + pb + k);
+            if (!pivot_ok(sg, (double)pv) || (!LDLT && !(pv > T(0)))) bad = pb + k;
+        }
+        // after a rejected pivot the remaining steps run on junk and are discarded
+        T dk, ik;
+        diag_pivot<T, LDLT>(pv, dk, ik);
+        const T aik = a[k];
+        const T lik = aik * ik;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j > k) {  // resolved at compile time once both loops are unrolled
+                const T u = __shfl_sync(0xffffffffu, LDLT ? aik : lik, j);
+                if (i >= j) a[j] -= lik * u;
+            }
+        }
+        if (i > k) a[k] = lik;
+        else if (i == k) {
+            if (!LDLT) a[k] = dk;
+            mypiv = dk;
+            myrinv = ik;
+        }
+    }
+    if (lane < 16) {
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj)
+            if (jj <= i) A[(pb + i) + (pb + jj) * LDA] = a[jj];
+        pivs[pb + i] = mypiv;
+        rinv[pb + i] = myrinv;
+    }
+    if (lane == 0 && bad >= 0) (*bad_s) = bad;
+}
+
+// the inverse of the factored 16 x 16 diagonal block at pb (one warp): lane
+// j owns column j
+template <typename TC, int LDLT>
+__device__ __forceinline__ void diag_inv16(const TC* A, TC* X, const TC* rinv, int pb, int lane) {
+    using T = TC;
+    const int i = lane & 15, j = i;
+    T a[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = k < i ? A[(pb + i) + (pb + k) * LDA] : T(0);
+    const T myrinv = rinv[pb + i];
+    T x[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        T acc = T(0);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            if (k < r) {  // resolved at compile time once both loops are unrolled
+                const T lrk = __shfl_sync(0xffffffffu, a[k], r);
+                if (k >= j) acc += lrk * x[k];
+            }
+        }
+        const T rr = __shfl_sync(0xffffffffu, myrinv, r);
+        x[r] = r < j ? T(0) : (r == j ? (LDLT ? T(1) : rr) : (LDLT ? -acc : -acc * rr));
+    }
+    if (lane < 16)
+#pragma unroll
+        for (int r = 0; r < 16; ++r) X[(pb + r) + (pb + j) * LDA] = x[r];
+}
+
+// A[i, j] -= sum_q L[i, pb + q] (d_q) L[j, pb + q] over a rectangle of rows
+// [r0, 64) x columns [c0, c1), lower triangle only, threads t0.. of the block
+template <typename TC, int LDLT>
+__device__ __forceinline__ void diag_update(TC* A, const TC* pivs, int pb, int r0, int c0, int c1, int t,
+                                            int nt) {
+    using T = TC;
+    const int nr = kNB - r0, nc = c1 - c0;
+    for (int e = t; e < nr * nc; e += nt) {
+        const int i = r0 + e % nr, j = c0 + e / nr;
+        if (i >= j) {
+            T acc = T(0);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                T lj = A[j + (pb + q) * LDA];
+                if (LDLT) lj *= pivs[pb + q];
+                acc += A[i + (pb + q) * LDA] * lj;
+            }
+            A[i + j * LDA] -= acc;
+        }
+    }
+}
+
+// The off-diagonal 16 x 16 blocks of X = L^-1 from the four diagonal
+// inverses already in X, by block distance (the whole CTA).
+template <typename TC>
+__device__ __forceinline__ void diag_inv_offdiag(const TC* A, TC* X) {
+    const int tid = threadIdx.x;
+    using T = TC;
+    for (int dist = 1; dist < 4; ++dist) {
+        const int nb = 4 - dist;
+        T tmp[3];
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {  // T_ij = sum_{k=j}^{i-1} L_ik X_kj
+            const int o = tid + 256 * s;
+            tmp[s] = T(0);
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                T acc = T(0);
+                for (int bk = bj; bk < bi; ++bk)
+#pragma unroll
+                    for (int q = 0; q < 16; ++q)
+                        acc += A[(16 * bi + r) + (16 * bk + q) * LDA] * X[(16 * bk + q) + (16 * bj + c) * LDA];
+                tmp[s] = acc;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {  // X_ij = -X_ii T_ij
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                T acc = T(0);
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    acc += X[(16 * bi + r) + (16 * bi + q) * LDA] * X[(16 * bi + q) + (16 * bj + c) * LDA];
+                tmp[s] = -acc;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int o = tid + 256 * s;
+            if (o < nb * 256) {
+                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
+                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename TC, int LDLT>
+__device__ int diag_block_la(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double* __restrict__ signs,
+                          int64_t colbase, int* bad_s, Reg reg) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    using T = TC;
+    if (tid == 0) *bad_s = -1;
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int pb = p * 16;
+        if (warp == 0) {
+            diag_factor16<TC, LDLT>(A, pivs, rinv, pb, w, signs, colbase, bad_s, reg, lane);
+        } else if (p > 0) {
+            // panel p-1's update of everything below the diagonal block p
+            // (rows >= pb + 16, columns pb .. row); the block itself took it
+            // at the end of the previous panel
+            diag_update<TC, LDLT>(A, pivs, pb - 16, pb + 16, pb, kNB, tid - 32, 224);
+        }
+        __syncthreads();
+        if ((*bad_s) >= 0) break;  // uniform
+        if (p == 3) break;
+        // rows below: solve each row against the panel's triangle, in four
+        // column groups (finish a group, then subtract it from the later
+        // columns at once), which cuts the dependent chain of the
+        // substitution to about a third
+        const int r = pb + 16 + tid;
+        if (r < kNB) {
+            T y[16];
+#pragma unroll
+            for (int c = 0; c < 16; ++c) y[c] = A[r + (pb + c) * LDA];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+#pragma unroll
+                for (int c = 4 * g; c < 4 * g + 4; ++c) {
+#pragma unroll
+                    for (int q = 4 * g; q < c; ++q) y[c] -= y[q] * A[(pb + c) + (pb + q) * LDA];
+                    if (!LDLT) y[c] *= rinv[pb + c];
+                }
+#pragma unroll
+                for (int c = 4 * g + 4; c < 16; ++c)
+#pragma unroll
+                    for (int q = 4 * g; q < 4 * g + 4; ++q) y[c] -= y[q] * A[(pb + c) + (pb + q) * LDA];
+            }
+#pragma unroll
+            for (int c = 0; c < 16; ++c) A[r + (pb + c) * LDA] = LDLT ? y[c] * rinv[pb + c] : y[c];
+        }
+        __syncthreads();
+        // the next diagonal block takes this panel's update now
+        {
+            const int e = tid;
+            if (e < 256) {
+                const int ii = e & 15, jj = e >> 4;
+                const int gi = pb + 16 + ii, gj = pb + 16 + jj;
+                if (ii >= jj) {
+                    T acc = T(0);
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        T lj = A[gj + (pb + q) * LDA];
+                        if (LDLT) lj *= pivs[pb + q];
+                        acc += A[gi + (pb + q) * LDA] * lj;
+                    }
+                    A[gi + gj * LDA] -= acc;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (*bad_s >= 0) return *bad_s;  // uniform
+    // the four 16 x 16 diagonal inverses at once
+    if (warp < 4) diag_inv16<TC, LDLT>(A, X, rinv, warp * 16, lane);
+    __syncthreads();
+    diag_inv_offdiag<TC>(A, X);
+    return -1;
+}
+
+// The sequential version: per panel, warp 0 factors and inverts the 16 x 16
+// diagonal block, then the CTA forms the rows below from that inverse and
+// applies the panel's trailing update.
+template <typename TC, int LDLT>
+__device__ int diag_block_seq(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double* __restrict__ signs,
                           int64_t colbase, int* bad_s, Reg reg) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     using T = TC;
@@ -641,58 +900,19 @@ __device__ int diag_block(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double*
         __syncthreads();
     }
     if (*bad_s >= 0) return *bad_s;  // uniform
-    // off-diagonal 16 x 16 blocks of the inverse, by block distance
-    for (int dist = 1; dist < 4; ++dist) {
-        const int nb = 4 - dist;
-        T tmp[3];
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {  // T_ij = sum_{k=j}^{i-1} L_ik X_kj
-            const int o = tid + 256 * s;
-            tmp[s] = T(0);
-            if (o < nb * 256) {
-                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
-                T acc = T(0);
-                for (int bk = bj; bk < bi; ++bk)
-#pragma unroll
-                    for (int q = 0; q < 16; ++q)
-                        acc += A[(16 * bi + r) + (16 * bk + q) * LDA] * X[(16 * bk + q) + (16 * bj + c) * LDA];
-                tmp[s] = acc;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            const int o = tid + 256 * s;
-            if (o < nb * 256) {
-                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
-                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {  // X_ij = -X_ii T_ij
-            const int o = tid + 256 * s;
-            if (o < nb * 256) {
-                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
-                T acc = T(0);
-#pragma unroll
-                for (int q = 0; q < 16; ++q)
-                    acc += X[(16 * bi + r) + (16 * bi + q) * LDA] * X[(16 * bi + q) + (16 * bj + c) * LDA];
-                tmp[s] = -acc;
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            const int o = tid + 256 * s;
-            if (o < nb * 256) {
-                const int bj = o >> 8, bi = bj + dist, r = (o >> 4) & 15, c = o & 15;
-                X[(16 * bi + r) + (16 * bj + c) * LDA] = tmp[s];
-            }
-        }
-        __syncthreads();
-    }
+    diag_inv_offdiag<TC>(A, X);
     return -1;
+}
+
+// FP32 (the mixed form) takes the look-ahead version; FP64 the sequential
+// one, measured faster for doubles (the look-ahead's update warps compete
+// with warp 0's pivot chain for the FP64 pipes, and the row substitution is
+// a longer FP64 dependency chain than the product with the inverse).
+template <typename TC, int LDLT>
+__device__ int diag_block(TC* A, TC* X, TC* pivs, TC* rinv, int w, const double* __restrict__ signs,
+                          int64_t colbase, int* bad_s, Reg reg) {
+    if (sizeof(TC) == 4) return diag_block_la<TC, LDLT>(A, X, pivs, rinv, w, signs, colbase, bad_s, reg);
+    return diag_block_seq<TC, LDLT>(A, X, pivs, rinv, w, signs, colbase, bad_s, reg);
 }
 
 // Write back a factored diagonal block: the factor into the panel, the LDLt
@@ -1284,7 +1504,9 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 }
                 if (st.trail_tc.cnt) {
                     Timer t(h, K_UPDATE);
-                    if ((rc = tc_launch(h, 1, st.trail_tc, obs, obw, c0, f32b))) return rc;
+                    rc = h->tc_split ? tc_launch_split(h, 1, st.trail_tc, st.split_tc, obs, obw, c0, f32b)
+                                     : tc_launch(h, 1, st.trail_tc, obs, obw, c0, f32b);
+                    if (rc) return rc;
                 }
                 continue;
             }
@@ -1318,7 +1540,9 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         if (std::is_same<T, float>::value && h->use_tc && lv.tc_syrk) {
             if (lv.syrk_tc.cnt) {
                 Timer t(h, K_SYRK);
-                int rc = tc_launch(h, 2, lv.syrk_tc, 0, 0, 0, reinterpret_cast<const FactorBufs<float>&>(fb));
+                const FactorBufs<float>& f32b = reinterpret_cast<const FactorBufs<float>&>(fb);
+                int rc = h->tc_split ? tc_launch_split(h, 2, lv.syrk_tc, lv.split_syrk, 0, 0, 0, f32b)
+                                     : tc_launch(h, 2, lv.syrk_tc, 0, 0, 0, f32b);
                 if (rc) return rc;
             }
         } else if (lv.syrk.cnt) {

@@ -76,6 +76,7 @@ struct ItemList {
 };
 
 constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
+constexpr int kWarpSmallNJ = 16; // of those, fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
 constexpr int kNB = 64;         // sub-panel width of the blocked path
 #ifndef MF_KOB
 #define MF_KOB 256
@@ -90,6 +91,9 @@ constexpr int kEArows = 1024;   // parent rows per extend-add work item
 constexpr int kSolveRows = 256; // rows per gather work item
 constexpr int kTcSyrkN = 128;   // tile columns of the tensor-core SYRK
 constexpr int kTcTrailN = 128;  // tile columns of the tensor-core trailing update
+constexpr int kSplitRows = 128;  // rows of a pre-split operand unit
+constexpr int kSplitK = 32;      // columns (K) of a pre-split operand unit
+constexpr int kSplitUnitFloats = 2 * kSplitRows * kSplitK;  // hi and lo tiles: 32 KB
 constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
@@ -104,6 +108,10 @@ struct PanelStep {
     ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kob
     // the same work in 128-row tiles for the tensor-core (tcgen05) kernels
     ItemList left_tc, panel_tc, trail_tc;
+    // (front, 128-row block, 32-column chunk, first unit): the trailing
+    // update's operands split into TF32 hi / lo tiles once (k_tc_split);
+    // trail_tc items carry the front's first unit in pad
+    ItemList split_tc;
 };
 
 // One 256-column super-block K of the blocked fronts' diagonal blocks.
@@ -114,7 +122,7 @@ struct SolveStep {
 };
 
 struct Level {
-    ItemList small_warp;     // (front)           fronts with nj <= 32: one warp each (k_small_warp)
+    ItemList small_warp;     // (front)           fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
     ItemList small;          // (front)           other fronts with nj <= kSmallMax: one CTA each (k_small)
     // extend-add for blocked fronts, item (front, col tile, row chunk, first
     // segment): ea adds the children into the panel columns before the
@@ -128,6 +136,7 @@ struct Level {
     std::vector<PanelStep> steps;
     ItemList syrk;           // (front, ti, tj)   M -= L L^T
     ItemList syrk_tc;        // 128 x 64 tiles for the tcgen05 kernel
+    ItemList split_syrk;     // (front, row block, chunk, first unit) of the SYRK's split operands
     // solves
     ItemList s_small;        // (front)
     ItemList s_gather;       // (front, row tile) forward gather of child updates
@@ -208,6 +217,7 @@ struct GraphEntry {
 
 // single-precision copy of the factor and solve workspaces (mixed mode)
 struct Mixed {
+    float* split = nullptr;   // pre-split TF32 operand units of the trailing updates / SYRK (32 KB each)
     float* P = nullptr;
     float* M = nullptr;
     float* inv = nullptr;
@@ -273,6 +283,8 @@ struct mf_handle {
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
     double* d_part = nullptr;      // backward partial sums
     int64_t nbwd_part = 0;         // partial slots (max over levels)
+    int64_t nsplit_units = 0;      // largest number of split operand units one launch needs
+    bool tc_split = true;          // tensor-core updates read pre-split operands (MF_TC_SPLIT=0: convert per tile)
     mf::ItemList sub_tasks;        // k_s_sub_fwd / _bwd tasks (subtrees of small fronts), one CTA each
     int* d_chain = nullptr;        // k_s_chain ticket and progress counters, zeroed per solve
     int64_t nchain = 0;
@@ -373,6 +385,8 @@ int have_fp64(const mf_handle* h);
 int launch_factor_mixed(mf_handle* h);
 int tc_prepare(mf_handle* h);
 int tc_launch(mf_handle* h, int role, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb);
+int tc_launch_split(mf_handle* h, int role, const ItemList& l, const ItemList& units, int obs, int obw, int c0,
+                    const FactorBufs<float>& fb);
 int launch_assemble_mixed(mf_handle* h, const double* dnz);
 int launch_dl_to_panel(mf_handle* h, const double* dDval, const double* dLval);
 int launch_panel_to_dl(mf_handle* h, double* dDval, double* dLval);

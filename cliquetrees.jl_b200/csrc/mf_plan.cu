@@ -417,13 +417,13 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.small_warp);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn + f.na <= 32) push(j, 0, 0);
+            if (f.nn + f.na <= kWarpSmallNJ) push(j, 0, 0);
         }
         end(lv.small_warp);
         begin(lv.small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn + f.na > 32 && f.nn + f.na <= kSmallMax) push(j, 0, 0);
+            if (f.nn + f.na > kWarpSmallNJ && f.nn + f.na <= kSmallMax) push(j, 0, 0);
         }
         end(lv.small);
         int max_steps = 0;
@@ -542,6 +542,8 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 }
                 end(st.panel_tc);
                 begin(st.trail_tc);
+                std::vector<Item> split;
+                int64_t units = 0;
                 if (last_sub)
                     for (int32_t j : fr) {
                         const Front& f = h->h_fronts[j];
@@ -549,13 +551,23 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                         const int e = std::min(f.nn, (ob + 1) * kob);
                         if (e >= f.nn) continue;
                         const int nj = f.nn + f.na;
+                        // split operand units of rows [e, nj) x columns [ob*kob, e)
+                        const int nrb = (int)cdiv(nj - e, kSplitRows), nkc = (int)cdiv(e - ob * kob, kSplitK);
+                        for (int rb = 0; rb < nrb; ++rb)
+                            for (int kc = 0; kc < nkc; ++kc) split.push_back(Item{j, rb, kc, (int32_t)units});
                         for (int tj = 0; tj < (int)cdiv(f.nn - e, kTcTrailN); ++tj) {
                             const int cs = e + tj * kTcTrailN;
                             // rows from the first 128-aligned tile that reaches the diagonal
-                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti) push(j, ti, tj);
+                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti)
+                                items.push_back(Item{j, ti, tj, (int32_t)units});
                         }
+                        units += (int64_t)nrb * nkc * (h->diag ? 2 : 1);
                     }
                 end(st.trail_tc);
+                begin(st.split_tc);
+                items.insert(items.end(), split.begin(), split.end());
+                end(st.split_tc);
+                h->nsplit_units = std::max(h->nsplit_units, units);
                 lv.steps.push_back(st);
             }
         }
@@ -570,6 +582,8 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         }
         end(lv.syrk);
         begin(lv.syrk_tc);
+        std::vector<Item> ssplit;
+        int64_t sunits = 0;
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (f.nn + f.na <= kSmallMax || f.na == 0) continue;
@@ -578,9 +592,19 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             const int tcn = (int)cdiv(f.na + delta, kTcSyrkN);
             for (int tj = 0; tj < tcn; ++tj)
                 // 128-row tiles from the diagonal: L21 rows tj * N - delta + 128 ti
-                for (int ti = 0; ti < (int)cdiv(f.na + delta - tj * kTcSyrkN, kTM); ++ti) push(j, ti, tj);
+                for (int ti = 0; ti < (int)cdiv(f.na + delta - tj * kTcSyrkN, kTM); ++ti)
+                    items.push_back(Item{j, ti, tj, (int32_t)sunits});
+            // split operand units of rows [nn & ~3, nj) x columns [0, nn)
+            const int nrb = (int)cdiv(f.na + delta, kSplitRows), nkc = (int)cdiv(f.nn, kSplitK);
+            for (int rb = 0; rb < nrb; ++rb)
+                for (int kc = 0; kc < nkc; ++kc) ssplit.push_back(Item{j, rb, kc, (int32_t)sunits});
+            sunits += (int64_t)nrb * nkc * (h->diag ? 2 : 1);
         }
         end(lv.syrk_tc);
+        begin(lv.split_syrk);
+        items.insert(items.end(), ssplit.begin(), ssplit.end());
+        end(lv.split_syrk);
+        h->nsplit_units = std::max(h->nsplit_units, sunits);
 
         // solves: small fronts (solve_small) one warp each; blocked fronts in
         // 256-column super-block steps using the super-block inverses

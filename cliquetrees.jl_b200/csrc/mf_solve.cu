@@ -456,6 +456,13 @@ __device__ __forceinline__ void cpa(T* dst, const T* src, bool valid) {
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(src), "r"(nb) : "memory");
 }
+// 16 bytes global -> shared in flight (cp.async.cg); a false `valid` writes
+// zeros and reads nothing; both addresses 16-byte aligned
+__device__ __forceinline__ void cpa16(void* dst, const void* src, bool valid) {
+    const unsigned saddr = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(saddr), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
 __device__ __forceinline__ void cpa_wait_all() {
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -479,15 +486,23 @@ __device__ __forceinline__ void sdiag_run(const Front& f, int step, int q, const
     const int k0 = step * kSolveNB, wK = min(kSolveNB, f.nn - k0), ld2 = super_ld(wK);
     if (16 * q >= wK) return;  // whole CTA
     const T* X = inv2 + f.i2off + (int64_t)step * kSolveNB * kSolveNB;
-    for (int e = threadIdx.x; e < 16 * kSolveNB; e += blockDim.x) {
-        if (!BWD) {
-            const int c = e >> 4, a = 16 * q + (e & 15);
-            const bool v = a < wK && c <= a;
-            cpa(xt + e, v ? X + a + (int64_t)c * ld2 : X, v);
-        } else {
-            const int a = 16 * q + (e >> 8), c = e & 255;
-            const bool v = a < wK && c >= a && c < wK;
-            cpa(xt + e, v ? X + c + (int64_t)a * ld2 : X, v);
+    // 16-byte copies (X's columns and ld2 are multiples of 4 elements, so
+    // every copy is aligned and stays inside the ld2 x wK block); entries
+    // outside the triangle the products read come along and are never used
+    constexpr int VWX = 16 / (int)sizeof(T);
+    if (!BWD) {
+        constexpr int G = 16 / VWX;  // copies per column: the CTA's 16 rows
+        for (int e = threadIdx.x; e < G * kSolveNB; e += blockDim.x) {
+            const int c = e / G, g = e % G, a0 = 16 * q + g * VWX;
+            const bool v = c < wK && a0 < ld2;
+            cpa16(xt + c * 16 + g * VWX, v ? X + a0 + (int64_t)c * ld2 : X, v);
+        }
+    } else {
+        constexpr int G = kSolveNB / VWX;  // copies per staged column of X
+        for (int e = threadIdx.x; e < 16 * G; e += blockDim.x) {
+            const int al = e / G, c0 = (e % G) * VWX, a = 16 * q + al;
+            const bool v = a < wK && c0 < ld2;
+            cpa16(xt + al * kSolveNB + c0, v ? X + c0 + (int64_t)a * ld2 : X, v);
         }
     }
     for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
@@ -529,6 +544,9 @@ __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ front
     const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
     sdiag_run<T, NR, BWD>(f, step, (int)(blockIdx.x % kDiagSplit), inv2, C, W, n, nrhs, sm_raw);
 }
+
+constexpr int kColBatch = 16;  // 16-byte panel loads a lane issues before using them (step tiles: few CTAs)
+constexpr int kColBatchL = 8;  // the same for the L21 products (many CTAs: occupancy hides the latency)
 
 // 16 bytes of consecutive panel entries in one load: 4 floats or 2 doubles
 template <typename T> struct Vec16;
@@ -589,15 +607,27 @@ __device__ __forceinline__ void ftile_run(const Front& f, int step, int ta, cons
         for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
     if (row < nj && cn > 0) {
         const T* pc = P + f.poff + (int64_t)(k0 + cb) * ld + row;
-#pragma unroll 8
-        for (int c = ch; c < cn; c += CPL) {
-            const V l = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
-            const T* xc = xs + (cb + c) * NR;
+        // all of a batch's loads are issued before its products (one
+        // memory round trip per 16 columns of a lane, in column order)
+        for (int cb0 = ch; cb0 < cn; cb0 += kColBatch * CPL) {
+            V lb[kColBatch];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const T x = xc[r];
+            for (int u = 0; u < kColBatch; ++u) {
+                const int c = cb0 + u * CPL;
+                if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+            }
 #pragma unroll
-                for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(l, e) * x;
+            for (int u = 0; u < kColBatch; ++u) {
+                const int c = cb0 + u * CPL;
+                if (c < cn) {
+                    const T* xc = xs + (cb + c) * NR;
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const T x = xc[r];
+#pragma unroll
+                        for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(lb[u], e) * x;
+                    }
+                }
             }
         }
     }
@@ -686,15 +716,27 @@ __global__ void __launch_bounds__(256) k_s_fwd_l(const Front* __restrict__ front
         for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
     if (row < nj && cn > 0) {
         const T* pc = P + f.poff + (int64_t)(cq + cb) * ld + row;
-#pragma unroll 8
-        for (int c = ch; c < cn; c += CPL) {
-            const V l = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
-            const T* xc = xs + (cb + c) * NR;
+        // all of a batch's loads are issued before its products (one
+        // memory round trip per 16 columns of a lane, in column order)
+        for (int cb0 = ch; cb0 < cn; cb0 += kColBatchL * CPL) {
+            V lb[kColBatchL];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const T x = xc[r];
+            for (int u = 0; u < kColBatchL; ++u) {
+                const int c = cb0 + u * CPL;
+                if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+            }
 #pragma unroll
-                for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(l, e) * x;
+            for (int u = 0; u < kColBatchL; ++u) {
+                const int c = cb0 + u * CPL;
+                if (c < cn) {
+                    const T* xc = xs + (cb + c) * NR;
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const T x = xc[r];
+#pragma unroll
+                        for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(lb[u], e) * x;
+                    }
+                }
             }
         }
     }
@@ -777,13 +819,13 @@ __device__ __forceinline__ void btile_run(const Front& f, int step, int ta, cons
         // load ends inside the column's ldp rows; rows past the block are
         // dropped by the select below
         const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + k0 + i0;
-        for (int i = 0; i < 64; i += 8 * VW) {
-            V l[8];
+        for (int i = 0; i < 64; i += kColBatch * VW) {
+            V l[kColBatch];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < kColBatch; ++u)
                 if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < kColBatch; ++u) {
                 const int ib = i + u * VW;
                 if (ib < ni) {
                     const T* xr = xs + (i0 + ib) * NR;
@@ -983,13 +1025,13 @@ __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ front
         // row0 + i0 + i is a multiple of 4 below rhi <= nj, so each 16-byte
         // load ends inside the column's ldp rows
         const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + row0 + i0;
-        for (int i = 0; i < QR; i += 8 * VW) {
-            V l[8];
+        for (int i = 0; i < QR; i += kColBatchL * VW) {
+            V l[kColBatchL];
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
+            for (int u = 0; u < kColBatchL; ++u)
                 if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
+            for (int u = 0; u < kColBatchL; ++u) {
                 const int ib = i + u * VW;
                 if (ib < ni) {
                     const T* xr = xs + (i0 + ib) * NR;

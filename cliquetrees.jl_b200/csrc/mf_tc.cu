@@ -82,6 +82,15 @@ struct Cfg {
     static constexpr uint32_t IDESC =
         (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
 };
+// Pre-split operands (SPLIT): no raw stages, three operand stages filled by
+// bulk copies of the pre-split units
+template <int TN>
+struct SplitCfg {
+    static constexpr int NOP = 3;
+    static constexpr int RING_BYTES = NOP * Cfg<TN>::OP_BYTES;
+    static constexpr int SMEM_BYTES = RING_BYTES + 256 + 128;
+};
+static_assert(SplitCfg<128>::SMEM_BYTES <= 232448, "split tensor-core tile exceeds the shared-memory limit");
 static_assert(Cfg<128>::SMEM_BYTES <= 232448, "tensor-core SYRK tile exceeds the shared-memory limit");
 static_assert(Cfg<64>::SMEM_BYTES <= 232448, "tensor-core tile exceeds the shared-memory limit");
 
@@ -157,6 +166,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
             "r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
+}
+
+// non-tensor bulk copy of `bytes` contiguous bytes global -> shared (both
+// 16-byte aligned, bytes a multiple of 16), completing on an mbarrier
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
 }
 
 // Shared-memory matrix descriptor, K-major without swizzle: LBO = stride
@@ -298,22 +316,32 @@ __device__ __forceinline__ TileGeom tile_geom(const Front* __restrict__ fronts, 
     return g;
 }
 
-template <int ROLE, int LDLT>
+// SPLIT: the operands come pre-split (k_tc_split) in 32 KB units of hi and
+// lo tiles already in the operand layout, so the producer bulk-copies a
+// unit of A and one of B into an operand stage and the converter warps idle
+// (TRAIL and SYRK only: their row blocks line up with the units).
+template <int ROLE, int LDLT, bool SPLIT>
 __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__ fronts,
                                                        const Item* __restrict__ items, int64_t ntiles, int obs, int obw, int c0,
                                                        float* __restrict__ P, float* __restrict__ M,
                                                        const float* __restrict__ d,
                                                        const CUtensorMap* __restrict__ maps,
-                                                       const CUtensorMap* __restrict__ inv_map, int* __restrict__ err) {
+                                                       const CUtensorMap* __restrict__ inv_map,
+                                                       const float* __restrict__ split, int* __restrict__ err) {
     using namespace tc;
     constexpr int TN = TcTileN<ROLE>::value;
     using C_ = Cfg<TN>;
-    constexpr int NRAW = C_::NRAW, NOP = C_::NOP;
+    static_assert(!SPLIT || (TN == kSplitRows && TM == kSplitRows && KC == kSplitK),
+                  "pre-split units are 128 rows x 32 columns");
+    constexpr int NRAW = SPLIT ? 0 : C_::NRAW;
+    constexpr int NRAWD = NRAW > 0 ? NRAW : 1;  // divisor in the raw-stage code, which SPLIT never runs
+    constexpr int NOP = SPLIT ? SplitCfg<TN>::NOP : C_::NOP;
+    constexpr int RING = SPLIT ? SplitCfg<TN>::RING_BYTES : C_::RING_BYTES;
     extern __shared__ unsigned char smem_raw[];
     unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
     unsigned char* raw_base = base;
     unsigned char* op_base = base + NRAW * C_::RAW_BYTES;
-    uint64_t* raw_full = reinterpret_cast<uint64_t*>(base + C_::RING_BYTES);  // TMA landed
+    uint64_t* raw_full = reinterpret_cast<uint64_t*>(base + RING);  // TMA landed
     uint64_t* raw_empty = raw_full + NRAW;    // converters done with a raw stage
     uint64_t* op_full = raw_empty + NRAW;     // converters filled an operand stage
     uint64_t* op_empty = op_full + NOP;       // MMAs done with an operand stage
@@ -331,7 +359,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
     }
     if (tid == 0) {
         for (int s = 0; s < NRAW; ++s) { mbar_init(&raw_full[s], 1); mbar_init(&raw_empty[s], NCONV); }
-        for (int s = 0; s < NOP; ++s) { mbar_init(&op_full[s], NCONV); mbar_init(&op_empty[s], 1); }
+        for (int s = 0; s < NOP; ++s) { mbar_init(&op_full[s], SPLIT ? 1 : NCONV); mbar_init(&op_empty[s], 1); }
         for (int s = 0; s < 2; ++s) { mbar_init(&acc_full[s], 1); mbar_init(&acc_empty[s], NEPI); }
         *abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -345,7 +373,37 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
         atomicExch(err, code);
     };
 
-    if (warp == WTMA) {
+    if (SPLIT && warp == WTMA) {
+        // ---------------- bulk-copy producer of pre-split units ----------------
+        if (lane == 0) {
+            int64_t g = 0;
+            bool ok = true;
+            constexpr int nunit = LDLT ? 2 : 1;
+            for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+                const Item it = items[t];
+                const TileGeom tg = tile_geom<ROLE>(fronts, it, obs, obw, c0, P, M);
+                const int nkc = (tg.kend - tg.kbeg + KC - 1) / KC;
+                const int64_t ua = it.pad + ((int64_t)(it.a + it.b) * nkc) * nunit + (LDLT ? 1 : 0);
+                const int64_t ub = it.pad + ((int64_t)it.b * nkc) * nunit;
+                for (int c = 0; c < nkc; ++c, ++g) {
+                    const int os = (int)(g % NOP);
+                    if (g >= NOP && !mbar_wait(&op_empty[os], (uint32_t)(((g / NOP) - 1) & 1), abort)) {
+                        fail(1);
+                        ok = false;
+                        break;
+                    }
+                    unsigned char* st = op_base + os * C_::OP_BYTES;
+                    mbar_expect_tx(&op_full[os], (uint32_t)C_::OP_BYTES);
+                    bulk_load(st, split + (ua + (int64_t)c * nunit) * kSplitUnitFloats, 2 * C_::A_BYTES, &op_full[os]);
+                    bulk_load(st + 2 * C_::A_BYTES, split + (ub + (int64_t)c * nunit) * kSplitUnitFloats,
+                              2 * C_::B_BYTES, &op_full[os]);
+                }
+            }
+            // drain: the copies of the last stages must land before the CTA exits
+            for (int64_t q = (g > NOP ? g - NOP : 0); q < g; ++q)
+                (void)mbar_drain(&op_full[q % NOP], (uint32_t)((q / NOP) & 1));
+        }
+    } else if (warp == WTMA) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
             int64_t g = 0;  // chunks issued by this CTA
@@ -357,8 +415,8 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
                 const CUtensorMap* amap = maps + it.front;
                 const CUtensorMap* bmap = ROLE == TC_TRSM ? inv_map : amap;
                 for (int c = 0; c < tg.nchunk; ++c, ++g) {
-                    const int s = (int)(g % NRAW);
-                    if (g >= NRAW && !mbar_wait(&raw_empty[s], (uint32_t)(((g / NRAW) - 1) & 1), abort)) {
+                    const int s = (int)(g % NRAWD);
+                    if (g >= NRAWD && !mbar_wait(&raw_empty[s], (uint32_t)(((g / NRAWD) - 1) & 1), abort)) {
                         fail(1);
                         ok = false;
                         break;
@@ -375,11 +433,12 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
                 }
             }
             // drain: the last NRAW stages' loads must land before the CTA exits
-            for (int64_t q = (g > NRAW ? g - NRAW : 0); q < g; ++q)
-                (void)mbar_drain(&raw_full[q % NRAW], (uint32_t)((q / NRAW) & 1));
+            for (int64_t q = (g > NRAWD ? g - NRAWD : 0); q < g; ++q)
+                (void)mbar_drain(&raw_full[q % NRAWD], (uint32_t)((q / NRAWD) & 1));
         }
     } else if (warp >= NEPI && warp < NEPI + NCONV) {
-        // ---------------- converters ----------------
+        // ---------------- converters (idle when the operands come pre-split) ----------------
+        if (!SPLIT) {
         const int ct = tid - NEPI * 32;
         int64_t g = 0;
         for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -388,8 +447,8 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
             const float* dvec = (LDLT && ROLE != TC_TRSM) ? d + fronts[it.front].col0 : nullptr;
             bool ok = true;
             for (int c = 0; c < tg.nchunk; ++c, ++g) {
-                const int rs = (int)(g % NRAW), os = (int)(g % NOP);
-                ok = mbar_wait(&raw_full[rs], (uint32_t)((g / NRAW) & 1), abort);
+                const int rs = (int)(g % NRAWD), os = (int)(g % NOP);
+                ok = mbar_wait(&raw_full[rs], (uint32_t)((g / NRAWD) & 1), abort);
                 if (ok && g >= NOP) ok = mbar_wait(&op_empty[os], (uint32_t)(((g / NOP) - 1) & 1), abort);
                 if (!__all_sync(0xffffffffu, ok)) { ok = false; break; }
                 const float* raw = reinterpret_cast<const float*>(raw_base + rs * C_::RAW_BYTES);
@@ -406,6 +465,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
                 }
             }
             if (!ok) { if (lane == 0) fail(1); break; }
+        }
         }
     } else if (warp == WMMA) {
         // ---------------- MMA issuer ----------------
@@ -520,10 +580,92 @@ static int launch_one(mf_handle* h, const ItemList& l, int obs, int obw, int c0,
     if (!l.cnt) return 0;
     constexpr int smem = tc::Cfg<TcTileN<ROLE>::value>::SMEM_BYTES;
     const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
-    k_gemm_tc<ROLE, LDLT><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
+    k_gemm_tc<ROLE, LDLT, false><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
         h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
-        h->d_err);
+        nullptr, h->d_err);
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// One CTA per unit (front, 128-row block, 32-column chunk): the panel's rows
+// R0 + 128 rb .. and columns K0 + 32 kc .. (zero past the front's rows and
+// the role's K range) split into TF32 hi / lo in the operand layout of the
+// tensor-core kernel (convert<>'s), unit by unit; LDLt writes a second unit
+// with the columns scaled by the pivots (the A operand of L D L^T).
+// TRAIL: rows from the outer block's end e = min(nn, obs + obw), K = [obs, e);
+// SYRK: rows from nn & ~3, K = [0, nn).
+template <int LDLT, int SYRK>
+__global__ void __launch_bounds__(256) k_tc_split(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                  int obs, int obw, const float* __restrict__ P,
+                                                  const float* __restrict__ d, float* __restrict__ split) {
+    const Item it = items[blockIdx.x];
+    const Front f = fronts[it.front];
+    const int nn = f.nn, nj = nn + f.na, ld = f.ldp;
+    int R0, K0, Kend;
+    if (SYRK) {
+        R0 = nn & ~3; K0 = 0; Kend = nn;
+    } else {
+        const int e = min(nn, obs + obw);
+        R0 = e; K0 = obs; Kend = e;
+    }
+    const int nkc = (Kend - K0 + kSplitK - 1) / kSplitK;
+    const int m = threadIdx.x & (kSplitRows - 1), kh = threadIdx.x >> 7;
+    const int r = R0 + it.a * kSplitRows + m;
+    const int kb = K0 + it.b * kSplitK + 16 * kh;
+    const float* Pj = P + f.poff;
+    float x[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+        const int k = kb + u;
+        x[u] = (r < nj && k < Kend) ? Pj[r + (int64_t)k * ld] : 0.f;
+    }
+    constexpr int nunit = LDLT ? 2 : 1;
+#pragma unroll
+    for (int v = 0; v < nunit; ++v) {
+        uint32_t* U = reinterpret_cast<uint32_t*>(split) +
+                      ((int64_t)it.pad + ((int64_t)it.a * nkc + it.b) * nunit + v) * kSplitUnitFloats;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float y[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = kb + 4 * q + e;
+                y[e] = x[4 * q + e];
+                if (v == 1 && k < Kend) y[e] *= d[f.col0 + k];
+            }
+            uint4 vh, vl;
+            vh.x = tc::f2tf32(y[0]);
+            vh.y = tc::f2tf32(y[1]);
+            vh.z = tc::f2tf32(y[2]);
+            vh.w = tc::f2tf32(y[3]);
+            vl.x = tc::f2tf32(y[0] - __uint_as_float(vh.x));
+            vl.y = tc::f2tf32(y[1] - __uint_as_float(vh.y));
+            vl.z = tc::f2tf32(y[2] - __uint_as_float(vh.z));
+            vl.w = tc::f2tf32(y[3] - __uint_as_float(vh.w));
+            const int kq = 4 * kh + q;
+            const int off = (kq * (kSplitRows / 8) + (m >> 3)) * 32 + (m & 7) * 4;  // 32-bit words
+            *reinterpret_cast<uint4*>(U + off) = vh;
+            *reinterpret_cast<uint4*>(U + kSplitRows * kSplitK + off) = vl;
+        }
+    }
+}
+
+template <int ROLE, int LDLT>
+static int launch_split(mf_handle* h, const ItemList& l, const ItemList& units, int obs, int obw, int c0,
+                        const FactorBufs<float>& fb) {
+    if (!l.cnt) return 0;
+    if (units.cnt) {
+        k_tc_split<LDLT, ROLE == TC_SYRK><<<(unsigned)units.cnt, 256, 0, h->stream>>>(
+            h->d_fronts, h->d_items + units.off, obs, obw, fb.P, fb.d, h->f32.split);
+        MF_CUDA(cudaGetLastError());
+    }
+    constexpr int smem = tc::SplitCfg<TcTileN<ROLE>::value>::SMEM_BYTES;
+    const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
+    k_gemm_tc<ROLE, LDLT, true><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
+        h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
+        reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
+        h->f32.split, h->d_err);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
@@ -532,10 +674,13 @@ template <int LDLT>
 static int set_attrs() {
     constexpr int s64 = tc::Cfg<kTile>::SMEM_BYTES, ss = tc::Cfg<kTcSyrkN>::SMEM_BYTES;
     constexpr int st = tc::Cfg<kTcTrailN>::SMEM_BYTES;
-    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRAIL, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, st));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_SYRK, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
-    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRSM, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_LEFT, LDLT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRAIL, LDLT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, st));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_SYRK, LDLT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRSM, LDLT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64));
+    constexpr int sp = tc::SplitCfg<128>::SMEM_BYTES;
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_TRAIL, LDLT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
+    MF_CUDA(cudaFuncSetAttribute(k_gemm_tc<TC_SYRK, LDLT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp));
     return 0;
 }
 
@@ -611,6 +756,17 @@ int tc_prepare(mf_handle* h) {
         if (rc) return rc;
     }
     return h->diag ? set_attrs<1>() : set_attrs<0>();
+}
+
+// the trailing update (role 1) or SYRK (role 2) from pre-split operands:
+// k_tc_split over `units`, then the tile kernel
+int tc_launch_split(mf_handle* h, int role, const ItemList& l, const ItemList& units, int obs, int obw, int c0,
+                    const FactorBufs<float>& fb) {
+    if (h->diag)
+        return role == TC_TRAIL ? launch_split<TC_TRAIL, 1>(h, l, units, obs, obw, c0, fb)
+                                : launch_split<TC_SYRK, 1>(h, l, units, obs, obw, c0, fb);
+    return role == TC_TRAIL ? launch_split<TC_TRAIL, 0>(h, l, units, obs, obw, c0, fb)
+                            : launch_split<TC_SYRK, 0>(h, l, units, obs, obw, c0, fb);
 }
 
 int tc_launch(mf_handle* h, int role, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb) {

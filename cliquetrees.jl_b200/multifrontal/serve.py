@@ -333,14 +333,14 @@ class Server:
         pattern whose rounds can hold more, its largest power of two) and run
         a throw-away round through each, so plans, graphs and tensor maps
         exist before timing.  ``per_pattern`` handles per composition (at
-        most 2)."""
+        most one per worker, the most the loop keeps)."""
         for key in keys or list(self.patterns):
             pat = self.patterns[key]
             cs = counts or sorted({1, _pow2_floor(pat.batch)})
             for c in cs:
                 comp = ((key, c),)
                 got = []
-                for _ in range(max(1, min(2, per_pattern))):
+                for _ in range(max(1, min(self.workers, per_pattern))):
                     hd = self._get(comp)
                     if hd is None:
                         break

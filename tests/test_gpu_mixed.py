@@ -258,3 +258,29 @@ def test_fp64_solves_refuse_a_stale_fp64_factor():
     with pytest.raises(RuntimeError):
         F.factor_arrays()
     F.close()
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+def test_pre_split_operands_equal_per_tile_conversion(monkeypatch, ldlt):
+    """The tensor-core trailing updates and SYRK reading operands split into
+    TF32 hi / lo once (k_tc_split, MF_TC_SPLIT=1, the default) compute the
+    same products in the same order as the kernels converting per tile
+    (MF_TC_SPLIT=0): the single-precision factors are bitwise equal."""
+    if ldlt:
+        A = tm.config4(side=12, m=432, per_row=6, seed=9)  # a 633-column front: trailing updates
+        P, S = mf.symbolic(A)
+    else:
+        A = tm.grid_laplacian(30, 29, 28, seed=17, lo=1e-2, hi=1e2)
+        P, S = mf.symbolic(A, alg=mf.grid_nd_order(30, 29, 28))
+    out = {}
+    for v in ("0", "1"):
+        monkeypatch.setenv("MF_TC_SPLIT", v)
+        F = (mf.ldlt_ if ldlt else mf.cholesky_)((mf.ChordalLDLt if ldlt else mf.ChordalCholesky)(A, P, S, mixed=True))
+        assert F.info == 0 and not F.used_fp64
+        out[v] = F.factor_arrays_mixed()
+        B = tm.rhs(S.n, 2, seed=3)
+        X = mf.ldiv(F, B)
+        assert tm.backward_error(A, X, B).max() <= 1e-12
+        F.close()
+    for a, b in zip(out["0"], out["1"]):
+        assert np.array_equal(a, b)
