@@ -204,12 +204,20 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     }
     {
         // the one-launch chain measured slower than the per-step launches
-        // on the 80^3 workload (critical path per step unchanged, waits
-        // added), so it is opt-in: MF_SOLVE_CHAIN=1
+        // on the 80^3 workload (38 steps at most: critical path per step
+        // unchanged, waits added) and faster on the KKT workload's 133-step
+        // root, so by default only levels of many steps use it
         const char* senv = getenv("MF_TC_SPLIT");
         h->tc_split = !(senv && senv[0] == '0');
         const char* cenv = getenv("MF_SOLVE_CHAIN");
-        h->solve_chain = cenv && cenv[0] == '1';
+        h->solve_chain = !cenv ? 2 : cenv[0] == '1' ? 1 : cenv[0] == '0' ? 0 : 2;
+        const char* tenv = getenv("MF_TINY_SOLVE");
+        h->tiny_solve = !(tenv && tenv[0] == '0');
+        // the cluster-per-front level kernels measured slower than the
+        // per-kernel launches on the 80^3 workload (a front's cluster holds
+        // eight register-heavy CTAs however small the front), so opt-in
+        const char* menv = getenv("MF_MID_SOLVE");
+        h->mid_solve = menv && menv[0] == '1';
     }
     {
         const char* tcenv = getenv("MF_TENSOR_CORES");

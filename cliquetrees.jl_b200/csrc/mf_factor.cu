@@ -68,6 +68,7 @@ template <typename T>
 __global__ void k_scatter(T* __restrict__ P, const int64_t* __restrict__ slot, const double* __restrict__ v,
                           int64_t nnz, const int32_t* __restrict__ rowi, const int32_t* __restrict__ coli,
                           const double* __restrict__ scale) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < nnz; i += stride) {
@@ -80,6 +81,7 @@ __global__ void k_scatter(T* __restrict__ P, const int64_t* __restrict__ slot, c
 // scale[i] = 1/sqrt(|a_ii|) (1 where a_ii = 0) from the assembled values
 __global__ void k_diag_scale(double* __restrict__ scale, const int64_t* __restrict__ dslot,
                              const double* __restrict__ v, int64_t n) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t k = dslot[i];
@@ -95,6 +97,7 @@ template <bool TO_PANEL>
 __global__ void k_dl_panel(const Front* __restrict__ fronts, const RefFront* __restrict__ ref,
                            const int32_t* __restrict__ colref, const int32_t* __restrict__ sepmap,
                            double* __restrict__ Dv, double* __restrict__ Lv, double* __restrict__ P, int64_t n) {
+    pdl_prologue();
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -119,6 +122,7 @@ __global__ void k_panel32_to_dl(const Front* __restrict__ fronts, const RefFront
                                 const int32_t* __restrict__ colref, const int32_t* __restrict__ sepmap,
                                 double* __restrict__ Dv, double* __restrict__ Lv, const float* __restrict__ P,
                                 int64_t n) {
+    pdl_prologue();
     int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (warp >= n) return;
@@ -252,6 +256,7 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
                                                T* __restrict__ M, T* __restrict__ d,
                                                const double* __restrict__ signs, long long* __restrict__ info,
                                                int* __restrict__ rescued, Reg reg) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int flag;
     T* F = reinterpret_cast<T*>(smem_raw);
@@ -385,6 +390,7 @@ __global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __
                                                                 T* __restrict__ d, const double* __restrict__ signs,
                                                                 long long* __restrict__ info,
                                                                 int* __restrict__ rescued, Reg reg) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kWarpFronts + wib;
@@ -430,13 +436,34 @@ __global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __
 // barrier, deterministic sums.  PART 0 adds into the panel columns (before
 // the front is factored), PART 1 into the update matrix, which the SYRK has
 // already set to -L21 L21^T (so it is never zeroed or read twice).  A child
-// column streams in chunks of 4 x 32 rows: the relative indices and child
-// values of the chunk are loaded first, then the 4 parent entries they
-// address, so four independent gather chains are in flight per lane.
+// column streams in chunks of up to 4 x 32 rows (ea_chunk).
+// a chunk of U x 32 rows of a child column: the relative indices and child
+// values of the chunk first, then the U parent entries they address, so U
+// independent gather chains are in flight per lane; PRED drops rows >= a1
+template <typename T, int U, bool PRED>
+__device__ __forceinline__ void ea_chunk(const int32_t* __restrict__ rel, const T* mc, T* dst, int a, int a1) {
+    int r[U];
+    T v[U], o[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int aa = a + 32 * u;
+        const bool in = !PRED || aa < a1;
+        r[u] = in ? __ldg(rel + aa) : -1;
+        v[u] = in ? mc[aa] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+        if (r[u] >= 0) o[u] = dst[r[u]];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+        if (r[u] >= 0) dst[r[u]] = o[u] + v[u];
+}
+
 template <typename T, int PART>
 __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                             const Item* __restrict__ all_items, const int32_t* __restrict__ reltgt,
                                             T* __restrict__ P, T* __restrict__ M) {
+    pdl_prologue();
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, ld = f.ldp, lm = f.ldm;
@@ -458,21 +485,15 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
             if (((col - c0) & 7) != warp) continue;  // the owner warp of this parent column
             const T* mc = Mc + (int64_t)b * fc.ldm;
             T* dst = PART == 0 ? Pj + (int64_t)col * ld : Mj + (int64_t)(col - nn) * lm - nn;
+            // full chunks of 4 x 32 rows, then one predicated chunk of at
+            // most 4 x 32 rows (a single row per lane when the rest is that
+            // short: many child columns are, and the predicated slots would
+            // cost instructions for nothing).  Eight chains per lane measured
+            // slower on long columns (more lines in flight than L1 keeps).
             int a = max(a0, b) + lane;
-            for (; a + 96 < a1; a += 128) {
-                int r[4];
-                T v[4], o[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    r[u] = __ldg(rel + a + 32 * u);
-                    v[u] = mc[a + 32 * u];
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) o[u] = dst[r[u]];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) dst[r[u]] = o[u] + v[u];
-            }
-            for (; a < a1; a += 32) dst[__ldg(rel + a)] += mc[a];
+            for (; a + 96 < a1; a += 128) ea_chunk<T, 4, false>(rel, mc, dst, a, a1);
+            if (a + 32 < a1) ea_chunk<T, 4, true>(rel, mc, dst, a, a1);
+            else if (a < a1) dst[__ldg(rel + a)] += mc[a];
         }
         __syncwarp();
     }
@@ -493,7 +514,9 @@ __global__ void __launch_bounds__(256) k_ea(const Front* __restrict__ fronts, co
 // rank-16 update to the trailing block; both are fully unrolled 16-term dot
 // products.  Finally the off-diagonal 16 x 16 blocks of X = L^-1 (unit
 // diagonal for LDLt) follow along the block sub-diagonals,
-// X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj.  About 26 barriers in all.
+// X_ij = -X_ii sum_{k=j}^{i-1} L_ik X_kj.  About 26 barriers in all.  This is
+// diag_block_seq (the FP64 kernel); the FP32 kernel runs diag_block_la,
+// which takes the inverses and the bulk updates off warp 0's chain.
 constexpr int LDS = kNB + 4;  // shared-memory leading dimension of the GEMM stages
 constexpr int LDA = kNB + 1;  // leading dimension of the block and its inverse in the diagonal kernel
 
@@ -958,6 +981,7 @@ __global__ void __launch_bounds__(256, 1) k_diag(const Front* __restrict__ front
                                               int c0, T* __restrict__ P, T* __restrict__ inv,
                                               T* __restrict__ d, const double* __restrict__ signs,
                                               long long* __restrict__ info, int* __restrict__ rescued, Reg reg) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* A = reinterpret_cast<T*>(smem_raw);  // block, A[r + c * LDA]
     T* X = A + kNB * LDA;                   // inverse, same layout
@@ -1190,6 +1214,7 @@ template <typename T, int ROLE, int LDLT>
 __global__ void __launch_bounds__(256) k_gemm(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                               int obs, int obw, int c0, T* __restrict__ P, T* __restrict__ M,
                                               const T* __restrict__ d, const T* __restrict__ inv) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* smem = reinterpret_cast<T*>(smem_raw);
     const Item it = items[blockIdx.x];
@@ -1271,6 +1296,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_inv256(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                 const T* __restrict__ P, const T* __restrict__ inv,
                                                 T* __restrict__ inv2) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* As = reinterpret_cast<T*>(smem_raw);
     T* Bs = As + kNB * ILD;
@@ -1362,7 +1388,7 @@ static int assemble_impl(mf_handle* h, const double* dnz, T* P, const double* sc
     if (h->nnz > 0) {
         int64_t blocks = (h->nnz + 255) / 256;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        k_scatter<T><<<(unsigned)blocks, 256, 0, h->stream>>>(P, h->d_pslot, dnz, h->nnz, h->d_nzrow, h->d_nzcol,
+        launch_k(k_scatter<T>, (unsigned)blocks, 256, 0, h->stream, P, h->d_pslot, dnz, h->nnz, h->d_nzrow, h->d_nzcol,
                                                                scale);
         MF_CUDA(cudaGetLastError());
     }
@@ -1379,7 +1405,7 @@ int launch_assemble(mf_handle* h, const double* dnz) {
 
 int launch_assemble_mixed(mf_handle* h, const double* dnz) {
     if (h->n > 0) {
-        k_diag_scale<<<(unsigned)((h->n + 255) / 256), 256, 0, h->stream>>>(h->d_scale, h->d_dslot, dnz, h->n);
+        launch_k(k_diag_scale, (unsigned)((h->n + 255) / 256), 256, 0, h->stream, h->d_scale, h->d_dslot, dnz, h->n);
         MF_CUDA(cudaGetLastError());
     }
     return assemble_impl<float>(h, dnz, h->f32.P, h->d_scale);
@@ -1395,7 +1421,7 @@ int launch_dl_to_panel(mf_handle* h, const double* dD, const double* dL) {
     int64_t threads = h->n * 32;
     unsigned blocks = (unsigned)((threads + 255) / 256);
     MF_CUDA(cudaMemsetAsync(h->d_P, 0, sizeof(double) * h->npanel, h->stream));
-    k_dl_panel<true><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap,
+    launch_k(k_dl_panel<true>, blocks, 256, 0, h->stream, h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap,
                                                      const_cast<double*>(dD), const_cast<double*>(dL), h->d_P, h->n);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1415,7 +1441,7 @@ int launch_panel_to_dl(mf_handle* h, double* dD, double* dL) {
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
     unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_dl_panel<false><<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
+    launch_k(k_dl_panel<false>, blocks, 256, 0, h->stream, h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
                                                       h->d_P, h->n);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1425,7 +1451,7 @@ int launch_panel32_to_dl(mf_handle* h, double* dD, double* dL) {
     if (h->n == 0) return 0;
     int64_t threads = h->n * 32;
     unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_panel32_to_dl<<<blocks, 256, 0, h->stream>>>(h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
+    launch_k(k_panel32_to_dl, blocks, 256, 0, h->stream, h->d_fronts, h->d_ref, h->d_colfront, h->d_sepmap, dD, dL,
                                                    h->f32.P, h->n);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1461,21 +1487,21 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         if (lv.small_warp.cnt) {
             Timer t(h, K_SMALL);
             const unsigned g = (unsigned)((lv.small_warp.cnt + kWarpFronts - 1) / kWarpFronts);
-            k_small_warp<T, LDLT><<<g, kWarpFronts * 32, kWarpFronts * kWarpSlice, h->stream>>>(
+            launch_k(k_small_warp<T, LDLT>, g, kWarpFronts * 32, kWarpFronts * kWarpSlice, h->stream, 
                 h->d_fronts, items + lv.small_warp.off, lv.small_warp.cnt, h->d_reltgt, h->d_chdtgt, fb.P, fb.M,
                 fb.d, h->d_signs, h->d_info, h->d_rescued, reg);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
-            k_small<T, LDLT><<<grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream>>>(
+            launch_k(k_small<T, LDLT>, grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream, 
                 h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
                 h->d_info, h->d_rescued, reg);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.ea.cnt) {
             Timer t(h, K_EA);
-            k_ea<T, 0><<<grid_for(lv.ea.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea.off, items,
+            launch_k(k_ea<T, 0>, grid_for(lv.ea.cnt), 256, 0, h->stream, h->d_fronts, items + lv.ea.off, items,
                                                                    h->d_reltgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
@@ -1493,7 +1519,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 }
                 if (st.diag.cnt) {
                     Timer t(h, K_DIAG);
-                    k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
+                    launch_k(k_diag<T, LDLT>, grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream, 
                         h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
                         h->d_rescued, reg);
                     MF_CUDA(cudaGetLastError());
@@ -1512,26 +1538,26 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             }
             if (st.left.cnt) {
                 Timer t(h, K_LEFT);
-                k_gemm<T, G_LEFT, LDLT><<<grid_for(st.left.cnt), 256, gs, h->stream>>>(
+                launch_k(k_gemm<T, G_LEFT, LDLT>, grid_for(st.left.cnt), 256, gs, h->stream, 
                     h->d_fronts, items + st.left.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.diag.cnt) {
                 Timer t(h, K_DIAG);
-                k_diag<T, LDLT><<<grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream>>>(
+                launch_k(k_diag<T, LDLT>, grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream, 
                     h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
                     h->d_rescued, reg);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.panel.cnt) {
                 Timer t(h, K_PANEL);
-                k_gemm<T, G_TRSM, LDLT><<<grid_for(st.panel.cnt), 256, gs, h->stream>>>(
+                launch_k(k_gemm<T, G_TRSM, LDLT>, grid_for(st.panel.cnt), 256, gs, h->stream, 
                     h->d_fronts, items + st.panel.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.trail.cnt) {
                 Timer t(h, K_UPDATE);
-                k_gemm<T, G_TRAIL, LDLT><<<grid_for(st.trail.cnt), 256, gs, h->stream>>>(
+                launch_k(k_gemm<T, G_TRAIL, LDLT>, grid_for(st.trail.cnt), 256, gs, h->stream, 
                     h->d_fronts, items + st.trail.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
@@ -1547,13 +1573,13 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             }
         } else if (lv.syrk.cnt) {
             Timer t(h, K_SYRK);
-            k_gemm<T, G_SYRK, LDLT><<<grid_for(lv.syrk.cnt), 256, gs, h->stream>>>(
+            launch_k(k_gemm<T, G_SYRK, LDLT>, grid_for(lv.syrk.cnt), 256, gs, h->stream, 
                 h->d_fronts, items + lv.syrk.off, 0, 0, 0, fb.P, fb.M, fb.d, fb.inv);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.ea_upd.cnt) {
             Timer t(h, K_EA);
-            k_ea<T, 1><<<grid_for(lv.ea_upd.cnt), 256, 0, h->stream>>>(h->d_fronts, items + lv.ea_upd.off, items,
+            launch_k(k_ea<T, 1>, grid_for(lv.ea_upd.cnt), 256, 0, h->stream, h->d_fronts, items + lv.ea_upd.off, items,
                                                                        h->d_reltgt, fb.P, fb.M);
             MF_CUDA(cudaGetLastError());
         }
@@ -1571,7 +1597,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         for (auto& e : tev) cudaEventDestroy(e);
     if (h->inv2_items.cnt) {
         Timer t(h, K_OTHER);
-        k_inv256<T><<<grid_for(h->inv2_items.cnt), 256, inv256_smem<T>(), h->stream>>>(
+        launch_k(k_inv256<T>, grid_for(h->inv2_items.cnt), 256, inv256_smem<T>(), h->stream, 
             h->d_fronts, items + h->inv2_items.off, fb.P, fb.inv, fb.inv2);
         MF_CUDA(cudaGetLastError());
     }
@@ -1662,6 +1688,7 @@ __global__ void __launch_bounds__(kLogdetThreads)
 k_logdet(const Front* __restrict__ fronts, const RefFront* __restrict__ ref, const int32_t* __restrict__ colref,
          const T* __restrict__ P, const T* __restrict__ d, const double* __restrict__ scale, int64_t n,
          double* __restrict__ out) {
+    pdl_prologue();
     __shared__ double s_sum[kLogdetThreads];
     __shared__ int s_neg[kLogdetThreads], s_zero[kLogdetThreads];
     const int64_t per = (n + gridDim.x - 1) / gridDim.x;
@@ -1720,17 +1747,17 @@ int launch_logdet(mf_handle* h, double* logabsdet, double* sign) {
     if (n > 0) {
         if (fp64) {
             if (h->diag)
-                k_logdet<double, 1><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                launch_k(k_logdet<double, 1>, kLogdetBlocks, kLogdetThreads, 0, h->stream, 
                     h->d_fronts, h->d_ref, h->d_colfront, h->d_P, h->d_d, nullptr, n, part);
             else
-                k_logdet<double, 0><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                launch_k(k_logdet<double, 0>, kLogdetBlocks, kLogdetThreads, 0, h->stream, 
                     h->d_fronts, h->d_ref, h->d_colfront, h->d_P, h->d_d, nullptr, n, part);
         } else {
             if (h->diag)
-                k_logdet<float, 1><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                launch_k(k_logdet<float, 1>, kLogdetBlocks, kLogdetThreads, 0, h->stream, 
                     h->d_fronts, h->d_ref, h->d_colfront, h->f32.P, h->f32.d, h->d_scale, n, part);
             else
-                k_logdet<float, 0><<<kLogdetBlocks, kLogdetThreads, 0, h->stream>>>(
+                launch_k(k_logdet<float, 0>, kLogdetBlocks, kLogdetThreads, 0, h->stream, 
                     h->d_fronts, h->d_ref, h->d_colfront, h->f32.P, h->f32.d, h->d_scale, n, part);
         }
         MF_CUDA(cudaGetLastError());

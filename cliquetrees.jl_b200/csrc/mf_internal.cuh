@@ -6,7 +6,9 @@
 
 #include <functional>
 #include <string>
+#include <cstdlib>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 namespace mf {
@@ -77,6 +79,7 @@ struct ItemList {
 
 constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
 constexpr int kWarpSmallNJ = 16; // of those, fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
+constexpr int kTinyNJ = 16;      // solves: fronts with nj <= kTinyNJ take 16 lanes each (k_s_tiny_*)
 constexpr int kNB = 64;         // sub-panel width of the blocked path
 #ifndef MF_KOB
 #define MF_KOB 256
@@ -98,6 +101,9 @@ constexpr int kFwdRows = 64;    // rows per forward-update work item
 constexpr int kSolveNB = 256;   // columns of a solve step: a super-block of four 64-column diagonal blocks
 constexpr int kBwdRows = 512;   // rows of L21 per backward partial-sum work item
 constexpr int kFwdCols = 512;   // columns of L21 per forward partial-sum work item
+constexpr int kChainMinSteps = 64;  // super-block steps of a level from which its solve runs as one k_s_chain launch
+constexpr int kMidCluster = 8;   // CTAs of the cluster that solves one front of a single-super-block level
+constexpr int64_t kMidMaxL21 = 1 << 20;  // such levels' largest nn * na (a cluster streams L21 from 8 SMs)
 
 // One 64-wide sub-panel s of outer block b (columns b*kob + s*kNB ..., kob the level's outer-block width).
 struct PanelStep {
@@ -139,12 +145,18 @@ struct Level {
     ItemList split_syrk;     // (front, row block, chunk, first unit) of the SYRK's split operands
     // solves
     ItemList s_small;        // (front)
+    ItemList s_tiny;         // (front)           small fronts with nj <= kTinyNJ: 16 lanes each
     ItemList s_gather;       // (front, row tile) forward gather of child updates
     std::vector<SolveStep> s_steps;
     ItemList s_fwd_l;        // (front, row tile, col chunk; pad = partial slot) R -= L21 x1
     ItemList s_fwd_red;      // (front, row tile, first partial slot, chunks)
     ItemList s_bwd_l;        // (front, col tile, row chunk; pad = partial slot) C1 -= L^T x[sep]
     ItemList s_bwd_red;      // (front, col tile, first partial slot)
+    // levels whose blocked fronts all have nn <= kSolveNB and nn * na <=
+    // kMidMaxL21: one cluster per front does the forward (k_s_mid_fwd) or
+    // backward (k_s_mid_bwd) work of s_gather .. s_bwd_red in one launch;
+    // item (front, first s_gather item, first s_bwd_l slot, gather tiles)
+    ItemList s_mid;
     // the super-block chain of the blocked fronts as one launch per
     // direction (k_s_chain): items (front, a, step K, counter base), a = -1 - q
     // for diagonal part q, else the tile; d_chain[chain_tk] / [chain_tk + 1]
@@ -175,10 +187,12 @@ enum KernelId {
 };
 
 // The solves handle a front with one warp when the factorization kept it
-// whole (nj <= kSmallMax) or it is narrow; otherwise it is blocked in the
+// whole (nj <= kSmallMax) or it is narrow with a short L21 (a warp streams
+// L21 row by row, so a long one serialises); otherwise it is blocked in the
 // factorization too and its diagonal-block inverses exist.
+constexpr int kSmallSolveNA = 256;
 __host__ __device__ inline bool solve_small(const Front& f) {
-    return f.nn + f.na <= kSmallMax || (f.nn <= kNB && f.na <= 1024);
+    return f.nn + f.na <= kSmallMax || (f.nn <= kNB && f.na <= kSmallSolveNA);
 }
 
 // Super-block K of a blocked front: its inverse X_K (wK x wK, lower, unit
@@ -288,7 +302,10 @@ struct mf_handle {
     mf::ItemList sub_tasks;        // k_s_sub_fwd / _bwd tasks (subtrees of small fronts), one CTA each
     int* d_chain = nullptr;        // k_s_chain ticket and progress counters, zeroed per solve
     int64_t nchain = 0;
-    bool solve_chain = false;      // one k_s_chain launch per level and direction (MF_SOLVE_CHAIN=1)
+    int solve_chain = 2;           // k_s_chain launches: 1 every level (MF_SOLVE_CHAIN=1), 0 none (=0),
+                                   // 2 the levels of at least kChainMinSteps steps (default)
+    bool tiny_solve = true;        // k_s_tiny_* for the fronts with nj <= kTinyNJ (MF_TINY_SOLVE=0: k_s_small_*)
+    bool mid_solve = false;        // one cluster launch per single-super-block level and direction (MF_MID_SOLVE=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
     double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
     int64_t* d_perm = nullptr;     // permutation (n)
@@ -363,6 +380,44 @@ void set_error(const std::string& msg);
 // another thread's stream is capturing at the same moment.
 std::recursive_mutex& device_mutex();
 int cuda_fail(cudaError_t e, const char* where);
+
+// Programmatic dependent launch.  Every kernel of the factorization, solve
+// and refinement paths starts with pdl_prologue(): it waits until the grid
+// it depends on has completed and its memory is visible (a no-op for a grid
+// launched without the attribute), then lets the next grid of the stream be
+// launched.  launch_k() launches with the attribute, so consecutive kernels
+// of a captured graph overlap the next launch's setup with the tail of the
+// current one while keeping stream order for every memory access.  Opt-in
+// (MF_PDL=1 in the environment): on the 80^3 workload the graph replays ran
+// about 2 % slower with it (100.9 vs 98.8 ms FP64, 46.9 vs 45.9 ms mixed).
+__device__ __forceinline__ void pdl_prologue() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("MF_PDL");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 #define MF_CUDA(call)                                                  \
     do {                                                               \

@@ -611,19 +611,29 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (solve_small(f) && task_of[j] < 0) push(j, 0, 0);
+            if (solve_small(f) && task_of[j] < 0 && f.nn + f.na > kTinyNJ) push(j, 0, 0);
         }
         end(lv.s_small);
+        begin(lv.s_tiny);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (solve_small(f) && task_of[j] < 0 && f.nn + f.na <= kTinyNJ) push(j, 0, 0);
+        }
+        end(lv.s_tiny);
         // forward gather: item (front, row tile, first segment, segments);
         // a segment (child, a0, a1) is the run rel[a0:a1] of a child's update
         // rows that lands in the tile, children in reverse order
         begin(lv.s_gather);
         int max_sblocks = 0;
+        int64_t max_l21 = 0;
+        std::vector<int32_t> gfirst;  // per blocked front of the level: its first gather item
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (solve_small(f)) continue;
             const int nj = f.nn + f.na;
             const int nt = (int)cdiv(nj, kSolveRows);
+            gfirst.push_back((int32_t)items.size());
+            max_l21 = std::max<int64_t>(max_l21, (int64_t)f.nn * f.na);
             std::vector<std::vector<Item>> per_tile((size_t)nt);
             for (int32_t p = f.chd1 - 1; p >= f.chd0; --p) {
                 const int32_t c = h->h_exec_chd[(size_t)p];
@@ -760,9 +770,11 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_bwd_l);
         int32_t slot = 0;
         std::vector<Item> red;
+        std::vector<int32_t> bfirst;  // per blocked front of the level: its first partial slot
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
             if (solve_small(f)) continue;
+            bfirst.push_back(slot);
             const int nchunk = std::max<int>(1, (int)cdiv(f.na, kBwdRows));
             for (int t = 0; t < cdiv(f.nn, kNB); ++t) {
                 red.push_back(Item{j, t, slot, 0});
@@ -774,6 +786,20 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_bwd_red);
         for (const Item& r : red) items.push_back(r);
         end(lv.s_bwd_red);
+        // single-super-block levels with short L21s: one cluster per blocked
+        // front (the gather items' segment offsets are made absolute below;
+        // the mid items point at the gather items themselves)
+        begin(lv.s_mid);
+        if (max_sblocks == 1 && max_l21 <= kMidMaxL21) {
+            size_t i = 0;
+            for (int32_t j : fr) {
+                const Front& f = h->h_fronts[j];
+                if (solve_small(f)) continue;
+                items.push_back(Item{j, gfirst[i], bfirst[i], (int32_t)cdiv(f.nn + f.na, kSolveRows)});
+                ++i;
+            }
+        }
+        end(lv.s_mid);
     }
     // task lists: task items {first level item, end}, level items {first
     // front item, end, height}, front items {front}; fronts of a task sorted

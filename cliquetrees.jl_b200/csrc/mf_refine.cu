@@ -46,6 +46,7 @@ __device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
 __global__ void k_spmv(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
                        const int64_t* __restrict__ src, const double* __restrict__ nz, const double* __restrict__ x,
                        double* __restrict__ y, int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     double acc[16];
@@ -63,30 +64,47 @@ __global__ void k_spmv(const int64_t* __restrict__ ptr, const int32_t* __restric
         if (r < nrhs) y[i + r * n] = acc[r];
 }
 
-// t = b - A x and the maxima needed by the backward error:
-// red[0..nrhs) = max|t|, red[16..) = max|x|, red[32..) = max|b|
-__global__ void k_resid(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
-                        const int64_t* __restrict__ src, const double* __restrict__ nz, const double* __restrict__ x,
-                        const double* __restrict__ b, double* __restrict__ t, double* __restrict__ red, int64_t n,
-                        int nrhs) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    if (!live) i = n - 1;  // keep the whole block in the reductions; results of this lane are ignored below
-    double acc[16];
+// t = b - A x for row i (all columns) with the stored-value map; the
+// products are added in the row's stored order
+template <int NR>
+__device__ __forceinline__ void resid_row(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                          const int64_t* __restrict__ src, const double* __restrict__ nz,
+                                          const double* __restrict__ x, int64_t i, int64_t n, int nrhs,
+                                          double (&acc)[NR]) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) acc[r] = 0.0;
-    for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    const int64_t p1 = ptr[i + 1];
+#pragma unroll 4
+    for (int64_t p = ptr[i]; p < p1; ++p) {
         const double a = nz[src[p]];
         const int64_t c = col[p];
 #pragma unroll
-        for (int r = 0; r < 16; ++r)
+        for (int r = 0; r < NR; ++r)
             if (r < nrhs) acc[r] += a * x[c + r * n];
     }
+}
+
+// t = b - A x and the maxima needed by the backward error:
+// red[0..nrhs) = max|t|, red[16..) = max|x|, red[32..) = max|b|
+template <int NR>
+__global__ void __launch_bounds__(256) k_resid(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                               const int64_t* __restrict__ src, const double* __restrict__ nz,
+                                               const double* __restrict__ x, const double* __restrict__ b,
+                                               double* __restrict__ t, double* __restrict__ red, int64_t n,
+                                               int nrhs) {
+    pdl_prologue();
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    if (!live) i = n - 1;  // keep the whole block in the reductions; results of this lane are ignored below
+    double acc[NR];
+    resid_row<NR>(ptr, col, src, nz, x, i, n, nrhs, acc);
     // block-level maxima first, then one atomic per block and quantity
     __shared__ double mx[48];
     if (threadIdx.x < 48) mx[threadIdx.x] = 0.0;
     __syncthreads();
-    for (int r = 0; r < nrhs; ++r) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        if (r >= nrhs) break;  // uniform across the block
         const double bi = b[i + r * n];
         const double ti = bi - acc[r];
         if (t && live) t[i + r * n] = ti;
@@ -106,66 +124,55 @@ __global__ void k_resid(const int64_t* __restrict__ ptr, const int32_t* __restri
     if (threadIdx.x < 48 && (threadIdx.x & 15) < nrhs) atomic_max_nonneg(red + threadIdx.x, mx[threadIdx.x]);
 }
 
-// Per-segment version of k_resid over row chunks (one CTA per chunk, a
-// chunk never crosses a segment boundary): the chunk's maxima go to
-// chunkred[c * kChunkRed + (0|16|32) + r]; k_seg_max combines the chunks of
-// every segment.
-__global__ void k_resid_chunk(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
-                              const int64_t* __restrict__ src, const double* __restrict__ nz,
-                              const double* __restrict__ x, const double* __restrict__ b, double* __restrict__ t,
-                              const int64_t* __restrict__ chunkrow, double* __restrict__ chunkred, int64_t n,
-                              int nrhs) {
-    const int64_t c = blockIdx.x;
-    const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
-    double m[48];
+// Per-segment version: one thread per row, and the maxima of every segment
+// go to segred[s * kSegRed + (0|16|32) + r] (zeroed by k_seg_zero) by
+// atomic max, order-independent; a warp whose rows lie in one segment
+// reduces by shuffles first.
+template <int NR>
+__global__ void __launch_bounds__(256) k_resid_seg(const int64_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                                   const int64_t* __restrict__ src, const double* __restrict__ nz,
+                                                   const double* __restrict__ x, const double* __restrict__ b,
+                                                   double* __restrict__ t, const int32_t* __restrict__ rowseg,
+                                                   double* __restrict__ segred, int64_t n, int nrhs) {
+    pdl_prologue();
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    if (!live) i = n - 1;
+    double acc[NR];
+    resid_row<NR>(ptr, col, src, nz, x, i, n, nrhs, acc);
+    const int sg = live ? rowseg[i] : -1;
+    const int sg0 = __shfl_sync(0xffffffffu, sg, 0);
+    const bool one = __all_sync(0xffffffffu, sg == sg0);
+    if (one && sg0 < 0) return;  // a warp past the last row
+    double* q = segred + (int64_t)(one ? sg0 : sg) * kSegRed;
 #pragma unroll
-    for (int q = 0; q < 48; ++q) m[q] = 0.0;
-    for (int64_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-        double acc[16];
-#pragma unroll
-        for (int r = 0; r < 16; ++r) acc[r] = 0.0;
-        for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) {
-            const double a = nz[src[p]];
-            const int64_t cc = col[p];
-#pragma unroll
-            for (int r = 0; r < 16; ++r)
-                if (r < nrhs) acc[r] += a * x[cc + r * n];
-        }
-#pragma unroll
-        for (int r = 0; r < 16; ++r)
-            if (r < nrhs) {
-                const double bi = b[i + r * n];
-                const double ti = bi - acc[r];
-                if (t) t[i + r * n] = ti;
-                m[r] = fmax(m[r], fabs(ti));
-                m[16 + r] = fmax(m[16 + r], fabs(x[i + r * n]));
-                m[32 + r] = fmax(m[32 + r], fabs(bi));
+    for (int r = 0; r < NR; ++r) {
+        if (r >= nrhs) break;  // uniform across the grid
+        const double bi = b[i + r * n];
+        const double ti = bi - acc[r];
+        if (t && live) t[i + r * n] = ti;
+        double v0 = fabs(ti), v1 = fabs(x[i + r * n]), v2 = fabs(bi);
+        if (one) {
+            for (int o = 16; o > 0; o >>= 1) {
+                v0 = fmax(v0, __shfl_xor_sync(0xffffffffu, v0, o));
+                v1 = fmax(v1, __shfl_xor_sync(0xffffffffu, v1, o));
+                v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, o));
             }
+            if ((threadIdx.x & 31) != 0) continue;
+        } else if (!live) {
+            continue;
+        }
+        atomic_max_nonneg(q + r, v0);
+        atomic_max_nonneg(q + 16 + r, v1);
+        atomic_max_nonneg(q + 32 + r, v2);
     }
-    __shared__ double mx[48];
-    if (threadIdx.x < 48) mx[threadIdx.x] = 0.0;
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < 48; ++q) {
-        if ((q & 15) >= nrhs) continue;  // uniform across the block
-        double v = m[q];
-        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(mx + q, v);
-    }
-    __syncthreads();
-    if (threadIdx.x < 48) chunkred[c * kChunkRed + threadIdx.x] = mx[threadIdx.x];
 }
 
-// segred[s * kSegRed + q] = max over the chunks of segment s (q < 48)
-__global__ void k_seg_max(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
-                          double* __restrict__ segred, int64_t nseg) {
+// segred[s * kSegRed + q] = 0 for q < 48 (entry 48, the segment's ||A||_inf, stays)
+__global__ void k_seg_zero(double* __restrict__ segred, int64_t nseg) {
+    pdl_prologue();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= nseg * 48) return;
-    const int64_t sg = i / 48;
-    const int q = (int)(i % 48);
-    double v = 0.0;
-    for (int64_t c = segchunk[sg]; c < segchunk[sg + 1]; ++c) v = fmax(v, chunkred[c * kChunkRed + q]);
-    segred[sg * kSegRed + q] = v;
+    if (i < nseg * 48) segred[(i / 48) * kSegRed + i % 48] = 0.0;
 }
 
 // per chunk and column: sum of u .* v over the chunk's rows into
@@ -173,6 +180,7 @@ __global__ void k_seg_max(const double* __restrict__ chunkred, const int64_t* __
 __global__ void k_dot_chunk(const double* __restrict__ u, const double* __restrict__ v,
                             const int64_t* __restrict__ chunkrow, double* __restrict__ chunkred, int64_t n,
                             int nrhs) {
+    pdl_prologue();
     __shared__ double sh[256];
     const int64_t c = blockIdx.x;
     const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
@@ -193,6 +201,7 @@ __global__ void k_dot_chunk(const double* __restrict__ u, const double* __restri
 // out[s * 80 + r] = sum over the chunks of segment s (fixed order)
 __global__ void k_dot_seg(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
                           double* __restrict__ out, int64_t nseg, int nrhs) {
+    pdl_prologue();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= nseg * 16) return;
     const int64_t sg = i / 16;
@@ -207,6 +216,7 @@ __global__ void k_dot_seg(const double* __restrict__ chunkred, const int64_t* __
 // out[r] = worst segment of column r
 __global__ void k_seg_eta(const double* __restrict__ segred, int64_t nseg, int nrhs, double* __restrict__ out,
                           double* __restrict__ segeta) {
+    pdl_prologue();
     __shared__ double mx[16];
     if (threadIdx.x < 16) mx[threadIdx.x] = 0.0;
     __syncthreads();
@@ -241,6 +251,7 @@ __global__ void k_seg_eta(const double* __restrict__ segred, int64_t nseg, int n
 // every thread of the grid on the same address)
 __global__ void k_anorm(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
                         const double* __restrict__ nz, double* __restrict__ out, int64_t n) {
+    pdl_prologue();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     double s = 0.0;
     if (i < n)
@@ -252,6 +263,7 @@ __global__ void k_anorm(const int64_t* __restrict__ ptr, const int64_t* __restri
 // per-column partial dot products: part[blk * 16 + r]
 __global__ void k_dot_part(const double* __restrict__ u, const double* __restrict__ v, double* __restrict__ part,
                            int64_t n, int nrhs) {
+    pdl_prologue();
     __shared__ double sh[256];
     for (int r = 0; r < nrhs; ++r) {
         double s = 0.0;
@@ -273,6 +285,7 @@ __global__ void k_dot_part(const double* __restrict__ u, const double* __restric
 // then a fixed shuffle tree (deterministic, and the loads of a lane are
 // independent instead of one dependent chain over all blocks)
 __global__ void k_dot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int nrhs) {
+    pdl_prologue();
     const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (r >= nrhs) return;
     double s = 0.0;
@@ -283,6 +296,7 @@ __global__ void k_dot_final(const double* __restrict__ part, double* __restrict_
 
 // CG scalars: mode 0: alpha = rz / pq; mode 1: beta = rz_new / rz, rz = rz_new
 __global__ void k_cg_scalars(double* __restrict__ sc, int nrhs, int mode) {
+    pdl_prologue();
     int r = threadIdx.x;
     if (r >= nrhs) return;
     double* rz = sc;           // [0..16)
@@ -301,6 +315,7 @@ __global__ void k_cg_scalars(double* __restrict__ sc, int nrhs, int mode) {
 // x += alpha p ; r -= alpha q
 __global__ void k_cg_xr(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                         const double* __restrict__ q, const double* __restrict__ alpha, int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) {
@@ -313,6 +328,7 @@ __global__ void k_cg_xr(double* __restrict__ x, double* __restrict__ r, const do
 // p = z + beta p
 __global__ void k_cg_p(double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ beta,
                        int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) p[i] = z[i] + beta[i / n] * p[i];
@@ -320,6 +336,7 @@ __global__ void k_cg_p(double* __restrict__ p, const double* __restrict__ z, con
 
 // the CG scalars above for every segment: sc[s * 80 + ...]
 __global__ void k_cg_scalars_seg(double* __restrict__ sc, int64_t nseg, int nrhs, int mode) {
+    pdl_prologue();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= nseg * 16) return;
     const int r = (int)(i % 16);
@@ -337,6 +354,7 @@ __global__ void k_cg_scalars_seg(double* __restrict__ sc, int64_t nseg, int nrhs
 __global__ void k_cg_xr_seg(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
                             const double* __restrict__ q, const double* __restrict__ sc,
                             const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) {
@@ -349,6 +367,7 @@ __global__ void k_cg_xr_seg(double* __restrict__ x, double* __restrict__ r, cons
 // p = z + beta_s p
 __global__ void k_cg_p_seg(double* __restrict__ p, const double* __restrict__ z, const double* __restrict__ sc,
                            const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) p[i] = z[i] + sc[(int64_t)rowseg[i % n] * 80 + 64 + i / n] * p[i];
@@ -357,6 +376,7 @@ __global__ void k_cg_p_seg(double* __restrict__ p, const double* __restrict__ z,
 // c = (float)(s .* r)   and   z = s .* (double)c  (+= when ACC)
 __global__ void k_to32(float* __restrict__ c, const double* __restrict__ r, const double* __restrict__ s, int64_t n,
                        int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) c[i] = (float)(s[i % n] * r[i]);
@@ -364,6 +384,7 @@ __global__ void k_to32(float* __restrict__ c, const double* __restrict__ r, cons
 template <bool ACC>
 __global__ void k_from32(double* __restrict__ z, const float* __restrict__ c, const double* __restrict__ s, int64_t n,
                          int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) {
@@ -381,6 +402,7 @@ constexpr int kGmresM = 24;  // restart length
 // part[(blk * J + i) * 16 + r] = this block's share of <V_i(:, r), w(:, r)>
 __global__ void k_mdot_part(const double* __restrict__ V, int64_t vs, int J, const double* __restrict__ w,
                             double* __restrict__ part, int64_t n, int nrhs) {
+    pdl_prologue();
     __shared__ double sh[256];
     for (int i = 0; i < J; ++i)
         for (int r = 0; r < nrhs; ++r) {
@@ -404,6 +426,7 @@ __global__ void k_mdot_part(const double* __restrict__ V, int64_t vs, int J, con
 // one warp per output (i, r), as k_dot_final
 __global__ void k_mdot_final(const double* __restrict__ part, double* __restrict__ out, int nblocks, int J,
                              int nrhs) {
+    pdl_prologue();
     const int o = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (o >= J * 16) return;
     const int i = o / 16, r = o % 16;
@@ -417,6 +440,7 @@ __global__ void k_mdot_final(const double* __restrict__ part, double* __restrict
 // w(:, r) -= sum_{i < J} c[i * 16 + r] V_i(:, r)
 __global__ void k_mupd(double* __restrict__ w, const double* __restrict__ V, int64_t vs, int J,
                        const double* __restrict__ c, int64_t n, int nrhs) {
+    pdl_prologue();
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)(k / n);
@@ -429,6 +453,7 @@ __global__ void k_mupd(double* __restrict__ w, const double* __restrict__ V, int
 // dst(:, r) = src(:, r) * c[r]
 __global__ void k_colscale(double* __restrict__ dst, const double* __restrict__ src, const double* __restrict__ c,
                            int64_t n, int nrhs) {
+    pdl_prologue();
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
          k += (int64_t)gridDim.x * blockDim.x)
         dst[k] = src[k] * c[k / n];
@@ -439,6 +464,7 @@ __global__ void k_colscale(double* __restrict__ dst, const double* __restrict__ 
 // as c[(i * G + s) * 16 + r] with G segments.
 __global__ void k_mdot_chunk(const double* __restrict__ V, int64_t vs, int J, const double* __restrict__ w,
                              const int64_t* __restrict__ chunkrow, double* __restrict__ part, int64_t n, int nrhs) {
+    pdl_prologue();
     __shared__ double sh[256];
     const int64_t c = blockIdx.x;
     const int64_t r0 = chunkrow[c], r1 = chunkrow[c + 1];
@@ -460,6 +486,7 @@ __global__ void k_mdot_chunk(const double* __restrict__ V, int64_t vs, int J, co
 }
 __global__ void k_mdot_seg(const double* __restrict__ part, const int64_t* __restrict__ segchunk,
                            double* __restrict__ out, int64_t G, int J, int nrhs) {
+    pdl_prologue();
     const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (o >= (int64_t)J * G * 16) return;
     const int r = (int)(o % 16);
@@ -473,6 +500,7 @@ __global__ void k_mdot_seg(const double* __restrict__ part, const int64_t* __res
 __global__ void k_mupd_seg(double* __restrict__ w, const double* __restrict__ V, int64_t vs, int J,
                            const double* __restrict__ c, const int32_t* __restrict__ rowseg, int64_t G, int64_t n,
                            int nrhs) {
+    pdl_prologue();
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
          k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t q = (int64_t)rowseg[k % n] * 16 + k / n;
@@ -483,6 +511,7 @@ __global__ void k_mupd_seg(double* __restrict__ w, const double* __restrict__ V,
 }
 __global__ void k_colscale_seg(double* __restrict__ dst, const double* __restrict__ src, const double* __restrict__ c,
                                const int32_t* __restrict__ rowseg, int64_t n, int nrhs) {
+    pdl_prologue();
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n * nrhs;
          k += (int64_t)gridDim.x * blockDim.x)
         dst[k] = src[k] * c[(int64_t)rowseg[k % n] * 16 + k / n];
@@ -493,6 +522,7 @@ __global__ void k_colscale_seg(double* __restrict__ dst, const double* __restric
 __global__ void k_anorm_chunk(const int64_t* __restrict__ ptr, const int64_t* __restrict__ src,
                               const double* __restrict__ nz, const int64_t* __restrict__ chunkrow,
                               double* __restrict__ chunkred) {
+    pdl_prologue();
     const int64_t c = blockIdx.x;
     double v = 0.0;
     for (int64_t i = chunkrow[c] + threadIdx.x; i < chunkrow[c + 1]; i += blockDim.x) {
@@ -510,6 +540,7 @@ __global__ void k_anorm_chunk(const int64_t* __restrict__ ptr, const int64_t* __
 }
 __global__ void k_seg_anorm(const double* __restrict__ chunkred, const int64_t* __restrict__ segchunk,
                             double* __restrict__ segred, int64_t nseg) {
+    pdl_prologue();
     const int64_t sg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (sg >= nseg) return;
     double v = 0.0;
@@ -529,20 +560,20 @@ static inline unsigned row_blocks(int64_t n) { return (unsigned)std::max<int64_t
 // z = M^-1 r (ACC: z += M^-1 r) through the FP32 factor
 template <bool ACC>
 static int apply_prec(mf_handle* h, const double* r, double* z, int nrhs) {
-    k_to32<<<gs_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->f32.C, r, h->d_scale, h->n, nrhs);
+    launch_k(k_to32, gs_blocks(h->n * nrhs), 256, 0, h->stream, h->f32.C, r, h->d_scale, h->n, nrhs);
     MF_CUDA(cudaGetLastError());
     int rc = launch_solve_mixed(h, nrhs);
     if (rc) return rc;
-    k_from32<ACC><<<gs_blocks(h->n * nrhs), 256, 0, h->stream>>>(z, h->f32.C, h->d_scale, h->n, nrhs);
+    launch_k(k_from32<ACC>, gs_blocks(h->n * nrhs), 256, 0, h->stream, z, h->f32.C, h->d_scale, h->n, nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
 
 static int dot(mf_handle* h, const double* u, const double* v, double* out, int nrhs) {
     double* part = h->d_red + kRedPart;
-    k_dot_part<<<kRedBlocks, 256, 0, h->stream>>>(u, v, part, h->n, nrhs);
+    launch_k(k_dot_part, kRedBlocks, 256, 0, h->stream, u, v, part, h->n, nrhs);
     MF_CUDA(cudaGetLastError());
-    k_dot_final<<<1, 32 * 16, 0, h->stream>>>(part, out, kRedBlocks, nrhs);
+    launch_k(k_dot_final, 1, 32 * 16, 0, h->stream, part, out, kRedBlocks, nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
@@ -550,10 +581,10 @@ static int dot(mf_handle* h, const double* u, const double* v, double* out, int 
 // per-segment dot products into h->d_segsc[s * 80 + off + r]
 static int dot_seg(mf_handle* h, const double* u, const double* v, int off, int nrhs) {
     if (h->nchunk > 0) {
-        k_dot_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(u, v, h->d_chunkrow, h->d_chunkred, h->n, nrhs);
+        launch_k(k_dot_chunk, (unsigned)h->nchunk, 256, 0, h->stream, u, v, h->d_chunkrow, h->d_chunkred, h->n, nrhs);
         MF_CUDA(cudaGetLastError());
     }
-    k_dot_seg<<<(unsigned)((h->nseg * 16 + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
+    launch_k(k_dot_seg, (unsigned)((h->nseg * 16 + 255) / 256), 256, 0, h->stream, h->d_chunkred, h->d_segchunk,
                                                                              h->d_segsc + off, h->nseg, nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -565,24 +596,39 @@ static int backward_error(mf_handle* h, const double* x, const double* b, double
     Timer tm(h, K_SPMV);
     double* red = h->d_red;  // [0..48) maxima, [48] ||A||_inf
     if (h->nseg > 0) {
-        if (h->nchunk > 0) {
-            k_resid_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc,
-                                                                       h->cur_nz, x, b, t, h->d_chunkrow,
-                                                                       h->d_chunkred, h->n, nrhs);
+        launch_k(k_seg_zero, (unsigned)((h->nseg * 48 + 255) / 256), 256, 0, h->stream, h->d_segred, h->nseg);
+        MF_CUDA(cudaGetLastError());
+        if (h->n > 0) {
+            const unsigned g = row_blocks(h->n);
+#define MF_RESID_SEG(NRV)                                                                                        \
+    launch_k(k_resid_seg<NRV>, g, 256, 0, h->stream, h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b, t, \
+             h->d_rowseg, h->d_segred, h->n, nrhs)
+            if (nrhs <= 1) MF_RESID_SEG(1);
+            else if (nrhs <= 2) MF_RESID_SEG(2);
+            else if (nrhs <= 4) MF_RESID_SEG(4);
+            else if (nrhs <= 8) MF_RESID_SEG(8);
+            else MF_RESID_SEG(16);
+#undef MF_RESID_SEG
             MF_CUDA(cudaGetLastError());
         }
-        k_seg_max<<<(unsigned)((h->nseg * 48 + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
-                                                                                 h->d_segred, h->nseg);
-        MF_CUDA(cudaGetLastError());
-        k_seg_eta<<<1, 256, 0, h->stream>>>(h->d_segred, h->nseg, nrhs, red, h->d_segeta);
+        launch_k(k_seg_eta, 1, 256, 0, h->stream, h->d_segred, h->nseg, nrhs, red, h->d_segeta);
         MF_CUDA(cudaGetLastError());
         MF_CUDA(cudaMemcpyAsync(eta, red, 16 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         MF_CUDA(cudaStreamSynchronize(h->stream));
         return 0;
     }
     MF_CUDA(cudaMemsetAsync(red, 0, 48 * sizeof(double), h->stream));
-    k_resid<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b, t, red,
-                                                      h->n, nrhs);
+    {
+        const unsigned g = row_blocks(h->n);
+#define MF_RESID(NRV) \
+    launch_k(k_resid<NRV>, g, 256, 0, h->stream, h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, x, b, t, red, h->n, nrhs)
+        if (nrhs <= 1) MF_RESID(1);
+        else if (nrhs <= 2) MF_RESID(2);
+        else if (nrhs <= 4) MF_RESID(4);
+        else if (nrhs <= 8) MF_RESID(8);
+        else MF_RESID(16);
+#undef MF_RESID
+    }
     MF_CUDA(cudaGetLastError());
     double hred[49];
     MF_CUDA(cudaMemcpyAsync(hred, red, 49 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -638,15 +684,15 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
     auto mdot = [&](const double* Vb, int J, const double* w, double* out_host) -> int {
         if (seg) {
             if (h->nchunk > 0) {
-                k_mdot_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(Vb, vs, J, w, h->d_chunkrow, part, n, nrhs);
+                launch_k(k_mdot_chunk, (unsigned)h->nchunk, 256, 0, h->stream, Vb, vs, J, w, h->d_chunkrow, part, n, nrhs);
                 MF_CUDA(cudaGetLastError());
             }
-            k_mdot_seg<<<(unsigned)((J * Q + 255) / 256), 256, 0, h->stream>>>(part, h->d_segchunk, coef, G, J,
+            launch_k(k_mdot_seg, (unsigned)((J * Q + 255) / 256), 256, 0, h->stream, part, h->d_segchunk, coef, G, J,
                                                                                 nrhs);
         } else {
-            k_mdot_part<<<nblk, 256, 0, h->stream>>>(Vb, vs, J, w, part, n, nrhs);
+            launch_k(k_mdot_part, nblk, 256, 0, h->stream, Vb, vs, J, w, part, n, nrhs);
             MF_CUDA(cudaGetLastError());
-            k_mdot_final<<<(unsigned)((J * 16 + 7) / 8), 256, 0, h->stream>>>(part, coef, nblk, J, nrhs);
+            launch_k(k_mdot_final, (unsigned)((J * 16 + 7) / 8), 256, 0, h->stream, part, coef, nblk, J, nrhs);
         }
         MF_CUDA(cudaGetLastError());
         MF_CUDA(cudaMemcpyAsync(out_host, coef, sizeof(double) * J * Q, cudaMemcpyDeviceToHost, h->stream));
@@ -655,15 +701,15 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
     };
     auto colscale = [&](double* dst, const double* src, const double* c_host) -> int {
         MF_CUDA(cudaMemcpyAsync(coef, c_host, sizeof(double) * Q, cudaMemcpyHostToDevice, h->stream));
-        if (seg) k_colscale_seg<<<gs_blocks(vs), 256, 0, h->stream>>>(dst, src, coef, h->d_rowseg, n, nrhs);
-        else k_colscale<<<gs_blocks(vs), 256, 0, h->stream>>>(dst, src, coef, n, nrhs);
+        if (seg) launch_k(k_colscale_seg, gs_blocks(vs), 256, 0, h->stream, dst, src, coef, h->d_rowseg, n, nrhs);
+        else launch_k(k_colscale, gs_blocks(vs), 256, 0, h->stream, dst, src, coef, n, nrhs);
         MF_CUDA(cudaGetLastError());
         return 0;
     };
     auto mupd = [&](double* w, const double* Vb, int J, const double* c_host) -> int {
         MF_CUDA(cudaMemcpyAsync(coef, c_host, sizeof(double) * J * Q, cudaMemcpyHostToDevice, h->stream));
-        if (seg) k_mupd_seg<<<gs_blocks(vs), 256, 0, h->stream>>>(w, Vb, vs, J, coef, h->d_rowseg, G, n, nrhs);
-        else k_mupd<<<gs_blocks(vs), 256, 0, h->stream>>>(w, Vb, vs, J, coef, n, nrhs);
+        if (seg) launch_k(k_mupd_seg, gs_blocks(vs), 256, 0, h->stream, w, Vb, vs, J, coef, h->d_rowseg, G, n, nrhs);
+        else launch_k(k_mupd, gs_blocks(vs), 256, 0, h->stream, w, Vb, vs, J, coef, n, nrhs);
         MF_CUDA(cudaGetLastError());
         return 0;
     };
@@ -713,7 +759,7 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
             ++used;
             {
                 Timer tm(h, K_SPMV);
-                k_spmv<<<row_blocks(n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Zj, w,
+                launch_k(k_spmv, row_blocks(n), 256, 0, h->stream, h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Zj, w,
                                                               n, nrhs);
                 MF_CUDA(cudaGetLastError());
             }
@@ -775,15 +821,15 @@ static int gmres(mf_handle* h, const double* b, double* x, int nrhs, double tol,
 int launch_anorm(mf_handle* h) {
     double* out = h->d_red + 48;
     MF_CUDA(cudaMemsetAsync(out, 0, sizeof(double), h->stream));
-    k_anorm<<<row_blocks(h->n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz, out, h->n);
+    launch_k(k_anorm, row_blocks(h->n), 256, 0, h->stream, h->d_csrptr, h->d_csrsrc, h->cur_nz, out, h->n);
     MF_CUDA(cudaGetLastError());
     if (h->nseg > 0) {
         if (h->nchunk > 0) {
-            k_anorm_chunk<<<(unsigned)h->nchunk, 256, 0, h->stream>>>(h->d_csrptr, h->d_csrsrc, h->cur_nz,
+            launch_k(k_anorm_chunk, (unsigned)h->nchunk, 256, 0, h->stream, h->d_csrptr, h->d_csrsrc, h->cur_nz,
                                                                        h->d_chunkrow, h->d_chunkred);
             MF_CUDA(cudaGetLastError());
         }
-        k_seg_anorm<<<(unsigned)((h->nseg + 255) / 256), 256, 0, h->stream>>>(h->d_chunkred, h->d_segchunk,
+        launch_k(k_seg_anorm, (unsigned)((h->nseg + 255) / 256), 256, 0, h->stream, h->d_chunkred, h->d_segchunk,
                                                                                h->d_segred, h->nseg);
         MF_CUDA(cudaGetLastError());
     }
@@ -825,8 +871,8 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
             return seg ? dot_seg(h, u, v, off, nrhs) : dot(h, u, v, sc + off, nrhs);
         };
         auto scalars = [&](int mode) -> int {
-            if (seg) k_cg_scalars_seg<<<sgrid, 256, 0, h->stream>>>(h->d_segsc, h->nseg, nrhs, mode);
-            else k_cg_scalars<<<1, 32, 0, h->stream>>>(sc, nrhs, mode);
+            if (seg) launch_k(k_cg_scalars_seg, sgrid, 256, 0, h->stream, h->d_segsc, h->nseg, nrhs, mode);
+            else launch_k(k_cg_scalars, 1, 32, 0, h->stream, sc, nrhs, mode);
             MF_CUDA(cudaGetLastError());
             return 0;
         };
@@ -838,17 +884,17 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
         for (it = 1; it <= maxit; ++it) {
             {
                 Timer tm(h, K_SPMV);
-                k_spmv<<<row_blocks(n), 256, 0, h->stream>>>(h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Pv, Q,
+                launch_k(k_spmv, row_blocks(n), 256, 0, h->stream, h->d_csrptr, h->d_csrcol, h->d_csrsrc, h->cur_nz, Pv, Q,
                                                               n, nrhs);
                 MF_CUDA(cudaGetLastError());
             }
             if ((rc = dotv(Pv, Q, 16))) return rc;  // pq
             if ((rc = scalars(0))) return rc;
             if (seg)
-                k_cg_xr_seg<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, h->d_segsc, h->d_rowseg, n,
+                launch_k(k_cg_xr_seg, gs_blocks(n * nrhs), 256, 0, h->stream, x, R, Pv, Q, h->d_segsc, h->d_rowseg, n,
                                                                         nrhs);
             else
-                k_cg_xr<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(x, R, Pv, Q, sc + 32, n, nrhs);
+                launch_k(k_cg_xr, gs_blocks(n * nrhs), 256, 0, h->stream, x, R, Pv, Q, sc + 32, n, nrhs);
             MF_CUDA(cudaGetLastError());
             if ((rc = backward_error(h, x, b, nullptr, nrhs, eta))) return rc;
             worst = 0.0;
@@ -858,9 +904,9 @@ int refine(mf_handle* h, const double* b, double* x, int nrhs, double tol, int m
             if ((rc = dotv(R, Z, 48))) return rc;  // rz_new
             if ((rc = scalars(1))) return rc;
             if (seg)
-                k_cg_p_seg<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, h->d_segsc, h->d_rowseg, n, nrhs);
+                launch_k(k_cg_p_seg, gs_blocks(n * nrhs), 256, 0, h->stream, Pv, Z, h->d_segsc, h->d_rowseg, n, nrhs);
             else
-                k_cg_p<<<gs_blocks(n * nrhs), 256, 0, h->stream>>>(Pv, Z, sc + 64, n, nrhs);
+                launch_k(k_cg_p, gs_blocks(n * nrhs), 256, 0, h->stream, Pv, Z, sc + 64, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
     } else {

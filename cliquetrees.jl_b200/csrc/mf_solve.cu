@@ -25,6 +25,7 @@ constexpr int kMaxRhs = 16;   // right-hand sides per pass (larger counts are ch
 template <bool IN>
 __global__ void k_perm(double* __restrict__ C, double* B, const int64_t* __restrict__ perm, int64_t n,
                        int64_t ldb, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) {
@@ -36,13 +37,14 @@ __global__ void k_perm(double* __restrict__ C, double* B, const int64_t* __restr
 
 template <typename T>
 __global__ void k_diag_div(T* __restrict__ C, const T* __restrict__ d, int64_t n, int nrhs) {
+    pdl_prologue();
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (; i < n * nrhs; i += stride) C[i] /= d[i % n];
 }
 
 // ---------------------------------------------------------------------------
-// small fronts (nj <= 96, or nn <= 64 and na <= 1024): one warp per front,
+// small fronts (nj <= 96, or nn <= 64 and na <= 256): one warp per front,
 // kSmallWarps fronts per CTA, warp-synchronous (no block barriers).  The
 // front's right-hand-side block C1 (nn x nrhs) lives in the warp's slice of
 // shared memory; lane i holds rows i, i + 32, i + 64 in registers during the
@@ -211,6 +213,7 @@ __global__ void __launch_bounds__(kSmallWarps * 32, small_min_blocks<T, NR>()) k
                                                                   const int32_t* __restrict__ chdtgt,
                                                                   const T* __restrict__ P, T* __restrict__ C,
                                                                   T* __restrict__ R, int64_t n, int nrhs) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
@@ -330,11 +333,179 @@ __global__ void __launch_bounds__(kSmallWarps * 32, small_min_blocks<T, NR>()) k
                                                                   const int32_t* __restrict__ septgt,
                                                                   const T* __restrict__ P, T* __restrict__ C,
                                                                   int64_t n, int nrhs) {
+    pdl_prologue();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kSmallWarps + wib;
     if (w >= cnt) return;
     const Front f = fronts[items[w].front];
     small_bwd_front<T, UNIT, NR>(f, septgt, P, C, n, nrhs, lane);
+}
+
+// ---------------------------------------------------------------------------
+// Tiny fronts (nj <= kTinyNJ): 16 lanes per front, two fronts per warp, lane
+// g owning row g of its front (forward) or column g (backward).  Each lane
+// issues all its panel loads at the start (row g of the panel forward,
+// column g backward), so a front costs a few dependent memory trips and
+// twice as many fronts are in flight per warp as with k_s_small_*.  Loops
+// over columns run to the warp's largest front (shuffles take the whole
+// warp) with the other front's steps predicated off.  Each entry gets the
+// operations of k_s_small_fwd / _bwd in the same order, so the results are
+// bitwise equal to them.
+// ---------------------------------------------------------------------------
+constexpr int kTinyWarps = 4;
+constexpr int kTinyFronts = kTinyWarps * 32 / kTinyNJ;  // fronts per CTA
+
+template <typename T, int NR>
+constexpr int tiny_min_blocks() {
+    return sizeof(T) == 4 ? (NR <= 4 ? 10 : NR <= 8 ? 8 : 4) : (NR <= 2 ? 8 : NR <= 4 ? 6 : NR <= 8 ? 4 : 3);
+}
+
+__device__ __forceinline__ Front tiny_front(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                            int64_t w, int64_t cnt) {
+    Front f{};
+    if (w < cnt) f = fronts[items[w].front];
+    else f.chd0 = f.chd1 = 0;  // nn = na = 0: every step predicated off
+    return f;
+}
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s_tiny_fwd(
+    const Front* __restrict__ fronts, const Item* __restrict__ items, int64_t cnt, const int32_t* __restrict__ reltgt,
+    const int32_t* __restrict__ chdtgt, const T* __restrict__ P, T* __restrict__ C, T* __restrict__ R, int64_t n,
+    int nrhs) {
+    pdl_prologue();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    constexpr unsigned kAll = 0xffffffffu;
+    const int g = threadIdx.x & (kTinyNJ - 1), slot = threadIdx.x / kTinyNJ;
+    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * kTinyFronts + slot, cnt);
+    T* Wv = reinterpret_cast<T*>(sm_raw) + slot * kTinyNJ * NR;  // Wv[row * NR + r]
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const T* Pj = P + f.poff;
+    T lr[kTinyNJ];  // row g of the panel
+#pragma unroll
+    for (int k = 0; k < kTinyNJ; ++k) lr[k] = (g < nj && k < nn) ? Pj[g + (int64_t)k * ld] : T(0);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) Wv[g * NR + r] = (g < nn && r < nrhs) ? C[f.col0 + g + (int64_t)r * n] : T(0);
+    __syncwarp();
+    // child updates, children in reverse order (one addition per entry and child)
+    const int nch = f.chd1 - f.chd0;
+    const int nchw = max(nch, __shfl_xor_sync(kAll, nch, kTinyNJ));
+    for (int i = 0; i < nchw; ++i) {
+        if (i < nch) {
+            const Front fc = fronts[chdtgt[f.chd1 - 1 - i]];
+            const int ma = fc.na;
+            if (g < ma) {
+                const int q = reltgt[fc.sep0 + g];
+                const T* Mc = R + fc.roff * nrhs + g;
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if (r < nrhs) Wv[q * NR + r] += Mc[r * ma];
+            }
+        }
+        __syncwarp();
+    }
+    T x[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) x[r] = Wv[g * NR + r];
+    const int nnw = max(nn, __shfl_xor_sync(kAll, nn, kTinyNJ));
+    // forward substitution: x_k = w_k / L_kk, rows k < a < nn lose L_ak x_k
+#pragma unroll
+    for (int k = 0; k < kTinyNJ; ++k) {
+        if (k >= nnw) break;  // uniform across the warp
+        const T dk = __shfl_sync(kAll, lr[k], k, kTinyNJ);
+        const T dinv = UNIT ? T(1) : T(1) / dk;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const T xk = __shfl_sync(kAll, x[r], k, kTinyNJ) * dinv;
+            if (k < nn) {
+                if (g > k && g < nn) x[r] -= lr[k] * xk;
+                if (g == k) x[r] = xk;
+            }
+        }
+    }
+    if (g < nn)
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) C[f.col0 + g + (int64_t)r * n] = x[r];
+    // R_j = (child sums) - L21 x
+    T acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+#pragma unroll
+    for (int k = 0; k < kTinyNJ; ++k) {
+        if (k >= nnw) break;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const T xk = __shfl_sync(kAll, x[r], k, kTinyNJ);
+            if (k < nn) acc[r] += lr[k] * xk;
+        }
+    }
+    if (g >= nn && g < nj) {
+        T* Rj = R + f.roff * nrhs + (g - nn);
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) Rj[(int64_t)r * na] = x[r] - acc[r];
+    }
+}
+
+template <typename T, int UNIT, int NR>
+__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s_tiny_bwd(
+    const Front* __restrict__ fronts, const Item* __restrict__ items, int64_t cnt, const int32_t* __restrict__ septgt,
+    const T* __restrict__ P, T* __restrict__ C, int64_t n, int nrhs) {
+    pdl_prologue();
+    constexpr unsigned kAll = 0xffffffffu;
+    const int g = threadIdx.x & (kTinyNJ - 1), slot = threadIdx.x / kTinyNJ;
+    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * kTinyFronts + slot, cnt);
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const T* Pj = P + f.poff;
+    T cv[kTinyNJ];  // column g of the panel
+#pragma unroll
+    for (int i = 0; i < kTinyNJ; ++i) cv[i] = (g < nn && i < nj) ? Pj[i + (int64_t)g * ld] : T(0);
+    T xs[NR];  // lanes nn .. nj - 1: x of the separator rows
+    {
+        const bool v = g >= nn && g < nj;
+        const int64_t row = v ? septgt[f.sep0 + g - nn] : 0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) xs[r] = (v && r < nrhs) ? __ldcg(C + row + (int64_t)r * n) : T(0);
+    }
+    // C1 - L21^T x[sep], separator rows in order
+    T acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = T(0);
+    const int njw = max(nj, __shfl_xor_sync(kAll, nj, kTinyNJ));
+#pragma unroll
+    for (int i = 0; i < kTinyNJ; ++i) {
+        if (i >= njw) break;  // uniform across the warp
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const T xb = __shfl_sync(kAll, xs[r], i, kTinyNJ);
+            if (i >= nn && i < nj) acc[r] += cv[i] * xb;
+        }
+    }
+    T c[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) c[r] = (g < nn && r < nrhs) ? C[f.col0 + g + (int64_t)r * n] - acc[r] : T(0);
+    // back substitution on L^T: x_k = c_k / L_kk, k descending; columns
+    // j < k lose L_kj x_k
+    const int nnw = max(nn, __shfl_xor_sync(kAll, nn, kTinyNJ));
+#pragma unroll
+    for (int k = kTinyNJ - 1; k >= 0; --k) {
+        if (k >= nnw) continue;  // uniform across the warp
+        const T dk = __shfl_sync(kAll, cv[k], k, kTinyNJ);
+        const T dinv = UNIT ? T(1) : T(1) / dk;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const T xk = __shfl_sync(kAll, c[r], k, kTinyNJ) * dinv;
+            if (k < nn) {
+                if (g < k) c[r] -= cv[k] * xk;
+                if (g == k) c[r] = xk;
+            }
+        }
+    }
+    if (g < nn)
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+            if (r < nrhs) C[f.col0 + g + (int64_t)r * n] = c[r];
 }
 
 // ---------------------------------------------------------------------------
@@ -359,6 +530,7 @@ __global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2)
                                                               const int32_t* __restrict__ chdtgt,
                                                               const T* __restrict__ P, T* __restrict__ C,
                                                               T* __restrict__ R, int64_t n, int nrhs) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     T* C1 = reinterpret_cast<T*>(sm_raw) + wib * kSmallMax * NR;
@@ -379,6 +551,7 @@ __global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2)
                                                               const int32_t* __restrict__ septgt,
                                                               const T* __restrict__ P, T* __restrict__ C,
                                                               int64_t n, int nrhs) {
+    pdl_prologue();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const Item tk = items[task0 + blockIdx.x];
     for (int L = tk.a - 1; L >= tk.front; --L) {
@@ -396,11 +569,9 @@ __global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2)
 // ---------------------------------------------------------------------------
 // forward gather: W[res] = C[res] + child updates, R_j = child updates
 template <typename T>
-__global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                  const Item* __restrict__ all_items,
-                                                  const int32_t* __restrict__ reltgt, const T* __restrict__ C,
-                                                  T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
-    const Item it = items[blockIdx.x];
+__device__ __forceinline__ void gather_run(const Item& it, const Front* __restrict__ fronts,
+                                           const Item* __restrict__ all_items, const int32_t* __restrict__ reltgt,
+                                           const T* __restrict__ C, T* W, T* R, int64_t n, int nrhs) {
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na;
     const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
@@ -431,6 +602,15 @@ __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fron
         }
         __syncthreads();
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                  const Item* __restrict__ all_items,
+                                                  const int32_t* __restrict__ reltgt, const T* __restrict__ C,
+                                                  T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
+    pdl_prologue();
+    gather_run<T>(items[blockIdx.x], fronts, all_items, reltgt, C, W, R, n, nrhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -540,6 +720,7 @@ template <typename T, int NR, int BWD>
 __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ inv2, T* __restrict__ C,
                                                  const T* __restrict__ W, int64_t n, int nrhs) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
     sdiag_run<T, NR, BWD>(f, step, (int)(blockIdx.x % kDiagSplit), inv2, C, W, n, nrhs, sm_raw);
@@ -663,6 +844,7 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
@@ -684,6 +866,7 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_fwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ part, int64_t n, int nrhs) {
+    pdl_prologue();
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;             // rows per load
@@ -768,6 +951,7 @@ __global__ void __launch_bounds__(256) k_s_fwd_l(const Front* __restrict__ front
 template <typename T>
 __global__ void __launch_bounds__(256) k_s_fwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                    const T* __restrict__ part, T* __restrict__ R, int nrhs) {
+    pdl_prologue();
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na;
@@ -857,6 +1041,7 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
@@ -927,6 +1112,7 @@ __global__ void __launch_bounds__(256) k_s_chain(const Front* __restrict__ front
                                                  int64_t cnt, int* ticket, int* ctl, const T* __restrict__ inv2,
                                                  const T* __restrict__ P, T* C, T* W, int64_t n, int nrhs,
                                                  int* err) {
+    pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     __shared__ int s_t, s_ok;
     for (;;) {
@@ -988,19 +1174,18 @@ constexpr int kBwdAlignRows = kBwdRows + 16;  // staged rows: the chunk, its ali
 template <typename T, int NR>
 constexpr int bwd_smem() { return (kBwdAlignRows * NR + 4 * NR * kNB) * (int)sizeof(T); }
 
-template <typename T, int NR>
-__global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                 const int32_t* __restrict__ septgt, const T* __restrict__ P,
-                                                 const T* __restrict__ C, T* __restrict__ part, int64_t n,
-                                                 int nrhs) {
+// one work item (front f, 64-column tile it.a, row chunk it.b, slot it.pad);
+// BATCH 16-byte loads of a thread are in flight at once (the order of the
+// products does not depend on it)
+template <typename T, int NR, int BATCH>
+__device__ __forceinline__ void bwdl_run(const Front& f, const Item& it, const int32_t* __restrict__ septgt,
+                                         const T* __restrict__ P, const T* __restrict__ C, T* part, int64_t n,
+                                         int nrhs, unsigned char* sm_raw) {
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
     T* xs = reinterpret_cast<T*>(sm_raw);  // xs[i * NR + r], i = panel row - row0
     T* red = xs + kBwdAlignRows * NR;      // red[(q * NR + r) * kNB + c]
-    const Item it = items[blockIdx.x];
-    const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, ld = f.ldp;
     const int tid = threadIdx.x;
     const int32_t* sep = septgt + f.sep0;
@@ -1025,13 +1210,13 @@ __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ front
         // row0 + i0 + i is a multiple of 4 below rhi <= nj, so each 16-byte
         // load ends inside the column's ldp rows
         const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + row0 + i0;
-        for (int i = 0; i < QR; i += kColBatchL * VW) {
-            V l[kColBatchL];
+        for (int i = 0; i < QR; i += BATCH * VW) {
+            V l[BATCH];
 #pragma unroll
-            for (int u = 0; u < kColBatchL; ++u)
+            for (int u = 0; u < BATCH; ++u)
                 if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
 #pragma unroll
-            for (int u = 0; u < kColBatchL; ++u) {
+            for (int u = 0; u < BATCH; ++u) {
                 const int ib = i + u * VW;
                 if (ib < ni) {
                     const T* xr = xs + (i0 + ib) * NR;
@@ -1061,21 +1246,210 @@ __global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ front
     }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) k_s_bwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                   const T* __restrict__ part, const T* __restrict__ C,
-                                                   T* __restrict__ W, int64_t n, int nrhs) {
+template <typename T, int NR>
+__global__ void __launch_bounds__(256) k_s_bwd_l(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                 const int32_t* __restrict__ septgt, const T* __restrict__ P,
+                                                 const T* __restrict__ C, T* __restrict__ part, int64_t n,
+                                                 int nrhs) {
+    pdl_prologue();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
+    bwdl_run<T, NR, kColBatchL>(f, it, septgt, P, C, part, n, nrhs, sm_raw);
+}
+
+// W[tile it.a of the front's columns] = C - (the chunk sums at part[it.b ...],
+// chunks in order); part is read through L2 (in k_s_mid_bwd other CTAs of
+// the cluster wrote it)
+template <typename T>
+__device__ __forceinline__ void bwdred_run(const Front& f, const Item& it, const T* part, const T* __restrict__ C,
+                                           T* W, int64_t n, int nrhs) {
     const int c0 = it.a * kNB, wc = min(kNB, f.nn - c0);
     const int nchunk = (f.na + kBwdRows - 1) / kBwdRows;
     for (int o = threadIdx.x; o < kNB * kMaxRhs; o += blockDim.x) {
         const int c = o % kNB, r = o / kNB;
         if (c >= wc || r >= nrhs) continue;
         T s = T(0);
-        for (int q = 0; q < nchunk; ++q) s += part[(int64_t)(it.b + q) * (kNB * kMaxRhs) + o];
+        for (int q = 0; q < nchunk; ++q) s += __ldcg(part + (int64_t)(it.b + q) * (kNB * kMaxRhs) + o);
         const int64_t idx = f.col0 + c0 + c + (int64_t)r * n;
         W[idx] = C[idx] - s;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_s_bwd_red(const Front* __restrict__ fronts, const Item* __restrict__ items,
+                                                   const T* __restrict__ part, const T* __restrict__ C,
+                                                   T* __restrict__ W, int64_t n, int nrhs) {
+    pdl_prologue();
+    const Item it = items[blockIdx.x];
+    bwdred_run<T>(fronts[it.front], it, part, C, W, n, nrhs);
+}
+
+// ---------------------------------------------------------------------------
+// Levels whose blocked fronts are single super-blocks (nn <= kSolveNB) with
+// a short L21: one thread-block cluster of kMidCluster CTAs per front does
+// the level's whole forward (or backward) work in one launch, instead of
+// the four (three) dependent launches above.  Phases are separated by the
+// cluster's hardware barrier (every CTA of a cluster is resident at once, so
+// the barrier needs no bounded wait); data crossing CTAs goes through L2
+// (stores, a gpu-scope fence before the barrier, .cg loads after it).
+//   forward : gather tiles -> x = X W[res] (the 16 parts of k_s_sdiag) ->
+//             R_j -= L21 x, one warp per 64-row tile of L21;
+//   backward: L21^T x[sep] partial sums (k_s_bwd_l items) -> W = C - sums
+//             (k_s_bwd_red) -> x = X^T W (the 16 parts of k_s_sdiag).
+// Every entry gets the same operations in the same order as in the
+// per-kernel launches, so the results are bitwise equal to them.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mid_cluster_sync() {
+    __threadfence();
+    asm volatile("barrier.cluster.arrive.release.aligned;\n"
+                 "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+
+template <typename T, int NR>
+constexpr int midf_smem() {
+    return sdiag_smem<T, NR>() > (kSolveNB * NR + 8 * NR * kFwdRows) * (int)sizeof(T)
+               ? sdiag_smem<T, NR>()
+               : (kSolveNB * NR + 8 * NR * kFwdRows) * (int)sizeof(T);
+}
+template <typename T, int NR>
+constexpr int midb_smem() { return sdiag_smem<T, NR>() > bwd_smem<T, NR>() ? sdiag_smem<T, NR>() : bwd_smem<T, NR>(); }
+
+// R_j[rows of 64-row L21 tile t] -= L21 x1 with one warp (nn <= kSolveNB):
+// for each 64-column group g the warp does what warp g of k_s_fwd_l does for
+// the tile (same lanes, same column order), and the group sums are added in
+// group order in the warp's slice of shared memory, as k_s_fwd_l adds its
+// warps' sums; the single chunk's sum is then taken from R as k_s_fwd_red does
+template <typename T, int NR>
+__device__ __forceinline__ void midf_tile(const Front& f, int t, const T* __restrict__ P, const T* xs, T* tot,
+                                          T* R, int nrhs) {
+    using VT = Vec16<T>;
+    using V = typename VT::type;
+    constexpr int VW = VT::W;
+    constexpr int LPC = kFwdRows / VW;
+    constexpr int CPL = 32 / LPC;
+    constexpr int GC = kFwdCols / 8;  // columns per group: one warp's share in k_s_fwd_l
+    const int lane = threadIdx.x & 31;
+    const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
+    const int ra = (nn & ~3) + t * kFwdRows;
+    const int rr = (lane % LPC) * VW, ch = lane / LPC;
+    const int row = ra + rr;
+    const int ng = (nn + GC - 1) / GC;
+    for (int g = 0; g < ng; ++g) {
+        const int cb = g * GC, cn = min(GC, nn - cb);
+        T acc[VW][NR];
+#pragma unroll
+        for (int e = 0; e < VW; ++e)
+#pragma unroll
+            for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
+        if (row < nj) {
+            const T* pc = P + f.poff + (int64_t)cb * ld + row;
+            for (int cb0 = ch; cb0 < cn; cb0 += kColBatch * CPL) {
+                V lb[kColBatch];
+#pragma unroll
+                for (int u = 0; u < kColBatch; ++u) {
+                    const int c = cb0 + u * CPL;
+                    if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+                }
+#pragma unroll
+                for (int u = 0; u < kColBatch; ++u) {
+                    const int c = cb0 + u * CPL;
+                    if (c < cn) {
+                        const T* xc = xs + (cb + c) * NR;
+#pragma unroll
+                        for (int r = 0; r < NR; ++r) {
+                            const T x = xc[r];
+#pragma unroll
+                            for (int e = 0; e < VW; ++e) acc[e][r] += VT::at(lb[u], e) * x;
+                        }
+                    }
+                }
+            }
+        }
+        if (CPL == 2) {
+#pragma unroll
+            for (int e = 0; e < VW; ++e)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) acc[e][r] += __shfl_xor_sync(0xffffffffu, acc[e][r], 16);
+        }
+        if (ch == 0) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+#pragma unroll
+                for (int e = 0; e < VW; ++e) {
+                    T* tp = tot + r * kFwdRows + rr + e;
+                    *tp = (g == 0 ? T(0) : *tp) + acc[e][r];
+                }
+        }
+    }
+    __syncwarp();
+    T* Rj = R + f.roff * nrhs;
+    for (int o = lane; o < kFwdRows * NR; o += 32) {
+        const int rl = o % kFwdRows, r = o / kFwdRows;
+        const int q = ra + rl;
+        if (r < nrhs && q >= nn && q < nj) {
+            T* rp = Rj + (q - nn) + (int64_t)r * na;
+            *rp = __ldcg(rp) - (T(0) + tot[r * kFwdRows + rl]);
+        }
+    }
+    __syncwarp();
+}
+
+// item (front, first gather item, first backward partial slot, gather tiles)
+template <typename T, int NR>
+__global__ void __cluster_dims__(kMidCluster, 1, 1) __launch_bounds__(256)
+    k_s_mid_fwd(const Front* __restrict__ fronts, const Item* __restrict__ mid, const Item* __restrict__ all_items,
+                const int32_t* __restrict__ reltgt, const T* __restrict__ inv2, const T* __restrict__ P, T* C, T* W,
+                T* R, int64_t n, int nrhs) {
+    pdl_prologue();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const Item m = mid[blockIdx.x / kMidCluster];
+    const int rank = (int)(blockIdx.x % kMidCluster);
+    const Front f = fronts[m.front];
+    for (int t = rank; t < m.pad; t += kMidCluster) gather_run<T>(all_items[m.a + t], fronts, all_items, reltgt, C, W, R, n, nrhs);
+    mid_cluster_sync();
+    for (int q = rank; q < kDiagSplit; q += kMidCluster) {
+        sdiag_run<T, NR, 0>(f, 0, q, inv2, C, W, n, nrhs, sm_raw);
+        __syncthreads();
+    }
+    mid_cluster_sync();
+    if (f.na > 0) {
+        T* xs = reinterpret_cast<T*>(sm_raw);  // xs[c * NR + r]
+        T* tot = xs + kSolveNB * NR;           // per warp: tot[r * kFwdRows + row]
+        for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
+            const int c = i % kSolveNB, r = i / kSolveNB;
+            xs[c * NR + r] = (c < f.nn && r < nrhs) ? __ldcg(C + f.col0 + c + (int64_t)r * n) : T(0);
+        }
+        __syncthreads();
+        const int warp = threadIdx.x >> 5;
+        const int ntile = (f.nn + f.na - (f.nn & ~3) + kFwdRows - 1) / kFwdRows;
+        for (int t = rank * 8 + warp; t < ntile; t += kMidCluster * 8)
+            midf_tile<T, NR>(f, t, P, xs, tot + warp * NR * kFwdRows, R, nrhs);
+    }
+}
+
+template <typename T, int NR>
+__global__ void __cluster_dims__(kMidCluster, 1, 1) __launch_bounds__(256)
+    k_s_mid_bwd(const Front* __restrict__ fronts, const Item* __restrict__ mid, const int32_t* __restrict__ septgt,
+                const T* __restrict__ inv2, const T* __restrict__ P, T* C, T* W, T* part, int64_t n, int nrhs) {
+    pdl_prologue();
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    const Item m = mid[blockIdx.x / kMidCluster];
+    const int rank = (int)(blockIdx.x % kMidCluster);
+    const Front f = fronts[m.front];
+    const int nct = (f.nn + kNB - 1) / kNB;
+    const int nchunk = max(1, (f.na + kBwdRows - 1) / kBwdRows);
+    for (int u = rank; u < nct * nchunk; u += kMidCluster) {
+        bwdl_run<T, NR, kColBatch>(f, Item{m.front, u / nchunk, u % nchunk, m.b + u}, septgt, P, C, part, n, nrhs,
+                                   sm_raw);
+        __syncthreads();
+    }
+    mid_cluster_sync();
+    for (int t = rank; t < nct; t += kMidCluster) bwdred_run<T>(f, Item{m.front, t, m.b + t * nchunk, 0}, part, C, W, n, nrhs);
+    mid_cluster_sync();
+    for (int q = rank; q < kDiagSplit; q += kMidCluster) {
+        sdiag_run<T, NR, 1>(f, 0, q, inv2, C, W, n, nrhs, sm_raw);
+        __syncthreads();
     }
 }
 
@@ -1091,7 +1465,7 @@ static unsigned grid_stride_blocks(int64_t work) {
 
 int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs) {
     Timer t(h, K_PERM);
-    k_perm<true><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->d_C, const_cast<double*>(B), perm, h->n,
+    launch_k(k_perm<true>, grid_stride_blocks(h->n * nrhs), 256, 0, h->stream, h->d_C, const_cast<double*>(B), perm, h->n,
                                                                          ldb, (int)nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1099,14 +1473,14 @@ int launch_permute_in(mf_handle* h, const double* B, int64_t ldb, const int64_t*
 
 int launch_permute_out(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs) {
     Timer t(h, K_PERM);
-    k_perm<false><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(h->d_C, B, perm, h->n, ldb, (int)nrhs);
+    launch_k(k_perm<false>, grid_stride_blocks(h->n * nrhs), 256, 0, h->stream, h->d_C, B, perm, h->n, ldb, (int)nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
 }
 
 int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, double* dst) {
     Timer t(h, K_PERM);
-    k_perm<true><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(dst, const_cast<double*>(B), perm, h->n, ldb,
+    launch_k(k_perm<true>, grid_stride_blocks(h->n * nrhs), 256, 0, h->stream, dst, const_cast<double*>(B), perm, h->n, ldb,
                                                                          (int)nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1114,7 +1488,7 @@ int launch_permute_to(mf_handle* h, const double* B, int64_t ldb, const int64_t*
 
 int launch_permute_from(mf_handle* h, double* B, int64_t ldb, const int64_t* perm, int64_t nrhs, const double* src) {
     Timer t(h, K_PERM);
-    k_perm<false><<<grid_stride_blocks(h->n * nrhs), 256, 0, h->stream>>>(const_cast<double*>(src), B, perm, h->n,
+    launch_k(k_perm<false>, grid_stride_blocks(h->n * nrhs), 256, 0, h->stream, const_cast<double*>(src), B, perm, h->n,
                                                                           ldb, (int)nrhs);
     MF_CUDA(cudaGetLastError());
     return 0;
@@ -1130,7 +1504,7 @@ static int chain_go(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int n
     int occ = 0;
     MF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_s_chain<T, NR, BWD>, 256, sm));
     const int64_t grid = std::min<int64_t>(il.cnt, (int64_t)std::max(occ, 1) * std::max(h->num_sms, 1));
-    k_s_chain<T, NR, BWD><<<(unsigned)grid, 256, sm, h->stream>>>(h->d_fronts, h->d_items + il.off, il.cnt,
+    launch_k(k_s_chain<T, NR, BWD>, (unsigned)grid, 256, sm, h->stream, h->d_fronts, h->d_items + il.off, il.cnt,
                                                                   h->d_chain + lv.chain_tk + BWD, h->d_chain,
                                                                   sb.inv2, sb.P, sb.C, sb.W, h->n, nrhs, h->d_err);
     MF_CUDA(cudaGetLastError());
@@ -1145,6 +1519,75 @@ static int launch_chain(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, i
         case 4: return chain_go<T, 4, BWD>(h, lv, sb, nrhs);
         case 8: return chain_go<T, 8, BWD>(h, lv, sb, nrhs);
         default: return chain_go<T, 16, BWD>(h, lv, sb, nrhs);
+    }
+}
+
+// one cluster launch for the blocked fronts of a single-super-block level
+template <typename T, int NR, int BWD>
+static int mid_go(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int nrhs) {
+    const unsigned g = (unsigned)(lv.s_mid.cnt * kMidCluster);
+    const Item* it = h->d_items + lv.s_mid.off;
+    if (!BWD) {
+        MF_CUDA(cudaFuncSetAttribute(k_s_mid_fwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, midf_smem<T, NR>()));
+        launch_k(k_s_mid_fwd<T, NR>, g, 256, midf_smem<T, NR>(), h->stream, h->d_fronts, it, h->d_items, h->d_reltgt,
+                 sb.inv2, sb.P, sb.C, sb.W, sb.R, h->n, nrhs);
+    } else {
+        MF_CUDA(cudaFuncSetAttribute(k_s_mid_bwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, midb_smem<T, NR>()));
+        launch_k(k_s_mid_bwd<T, NR>, g, 256, midb_smem<T, NR>(), h->stream, h->d_fronts, it, h->d_septgt, sb.inv2,
+                 sb.P, sb.C, sb.W, sb.part, h->n, nrhs);
+    }
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename T, int BWD>
+static int launch_mid(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int nrb, int nrhs) {
+    switch (nrb) {
+        case 1: return mid_go<T, 1, BWD>(h, lv, sb, nrhs);
+        case 2: return mid_go<T, 2, BWD>(h, lv, sb, nrhs);
+        case 4: return mid_go<T, 4, BWD>(h, lv, sb, nrhs);
+        case 8: return mid_go<T, 8, BWD>(h, lv, sb, nrhs);
+        default: return mid_go<T, 16, BWD>(h, lv, sb, nrhs);
+    }
+}
+
+// the tiny fronts of a level: k_s_tiny_* (16 lanes per front), or the
+// warp-per-front k_s_small_* when switched off
+template <typename T, int UNIT, int NR, int BWD>
+static int tiny_go(mf_handle* h, const ItemList& il, const SolveBufs<T>& sb, int nrhs) {
+    const Item* it = h->d_items + il.off;
+    const int64_t c = il.cnt;
+    if (h->tiny_solve) {
+        const unsigned g = (unsigned)((c + kTinyFronts - 1) / kTinyFronts);
+        constexpr int sm = kTinyFronts * kTinyNJ * NR * (int)sizeof(T);
+        if (!BWD)
+            launch_k(k_s_tiny_fwd<T, UNIT, NR>, g, kTinyWarps * 32, sm, h->stream, h->d_fronts, it, c, h->d_reltgt,
+                     h->d_chdtgt, sb.P, sb.C, sb.R, h->n, nrhs);
+        else
+            launch_k(k_s_tiny_bwd<T, UNIT, NR>, g, kTinyWarps * 32, 0, h->stream, h->d_fronts, it, c, h->d_septgt,
+                     sb.P, sb.C, h->n, nrhs);
+    } else {
+        const unsigned g = (unsigned)((c + kSmallWarps - 1) / kSmallWarps);
+        if (!BWD)
+            launch_k(k_s_small_fwd<T, UNIT, NR>, g, kSmallWarps * 32, small_solve_smem<T, NR>(), h->stream,
+                     h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, h->n, nrhs);
+        else
+            launch_k(k_s_small_bwd<T, UNIT, NR>, g, kSmallWarps * 32, 0, h->stream, h->d_fronts, it, c, h->d_septgt,
+                     sb.P, sb.C, h->n, nrhs);
+    }
+    MF_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename T, int UNIT, int BWD>
+static int launch_tiny(mf_handle* h, const ItemList& il, const SolveBufs<T>& sb, int nrb, int nrhs) {
+    Timer t(h, K_S_SMALL);
+    switch (nrb) {
+        case 1: return tiny_go<T, UNIT, 1, BWD>(h, il, sb, nrhs);
+        case 2: return tiny_go<T, UNIT, 2, BWD>(h, il, sb, nrhs);
+        case 4: return tiny_go<T, UNIT, 4, BWD>(h, il, sb, nrhs);
+        case 8: return tiny_go<T, UNIT, 8, BWD>(h, il, sb, nrhs);
+        default: return tiny_go<T, UNIT, 16, BWD>(h, il, sb, nrhs);
     }
 }
 
@@ -1180,54 +1623,71 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     const int nrb = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : nrhs <= 8 ? 8 : 16;
     const Item* items = h->d_items;
     const int64_t n = h->n;
-    const bool chain = h->solve_chain && h->nchain > 0;
-    if (chain) MF_CUDA(cudaMemsetAsync(h->d_chain, 0, sizeof(int) * (size_t)h->nchain, h->stream));
+    // the chain kernel for a level: every level (MF_SOLVE_CHAIN=1), none
+    // (=0), or by default the levels of at least kChainMinSteps super-block
+    // steps, where overlapping the steps' tiles outweighs the waits
+    auto use_chain = [&](const Level& lv) {
+        if (h->nchain <= 0 || h->solve_chain == 0) return false;
+        return h->solve_chain == 1 || (int)lv.s_steps.size() >= kChainMinSteps;
+    };
+    bool any_chain = false;
+    for (const Level& lv : h->levels) any_chain = any_chain || use_chain(lv);
+    if (any_chain) MF_CUDA(cudaMemsetAsync(h->d_chain, 0, sizeof(int) * (size_t)h->nchain, h->stream));
     if (h->sub_tasks.cnt) {
         // the subtrees of small fronts, forward, in one launch
         Timer t(h, K_S_SMALL);
         const unsigned g = (unsigned)h->sub_tasks.cnt;
         const int64_t t0 = h->sub_tasks.off;
         switch (nrb) {
-            case 1: k_s_sub_fwd<T, UNIT, 1><<<g, kSubWarps * 32, sub_solve_smem<T, 1>(), h->stream>>>(
+            case 1: launch_k(k_s_sub_fwd<T, UNIT, 1>, g, kSubWarps * 32, sub_solve_smem<T, 1>(), h->stream, 
                         h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-            case 2: k_s_sub_fwd<T, UNIT, 2><<<g, kSubWarps * 32, sub_solve_smem<T, 2>(), h->stream>>>(
+            case 2: launch_k(k_s_sub_fwd<T, UNIT, 2>, g, kSubWarps * 32, sub_solve_smem<T, 2>(), h->stream, 
                         h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-            case 4: k_s_sub_fwd<T, UNIT, 4><<<g, kSubWarps * 32, sub_solve_smem<T, 4>(), h->stream>>>(
+            case 4: launch_k(k_s_sub_fwd<T, UNIT, 4>, g, kSubWarps * 32, sub_solve_smem<T, 4>(), h->stream, 
                         h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-            case 8: k_s_sub_fwd<T, UNIT, 8><<<g, kSubWarps * 32, sub_solve_smem<T, 8>(), h->stream>>>(
+            case 8: launch_k(k_s_sub_fwd<T, UNIT, 8>, g, kSubWarps * 32, sub_solve_smem<T, 8>(), h->stream, 
                         h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-            default: k_s_sub_fwd<T, UNIT, 16><<<g, kSubWarps * 32, sub_solve_smem<T, 16>(), h->stream>>>(
+            default: launch_k(k_s_sub_fwd<T, UNIT, 16>, g, kSubWarps * 32, sub_solve_smem<T, 16>(), h->stream, 
                         h->d_fronts, items, t0, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
         }
         MF_CUDA(cudaGetLastError());
     }
     // forward: levels ascending
     for (const Level& lv : h->levels) {
+        if (lv.s_tiny.cnt)
+            if (int rc = launch_tiny<T, UNIT, 0>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
             const unsigned g = (unsigned)((lv.s_small.cnt + kSmallWarps - 1) / kSmallWarps);
             const Item* it = items + lv.s_small.off;
             const int64_t c = lv.s_small.cnt;
             switch (nrb) {
-                case 1: k_s_small_fwd<T, UNIT, 1><<<g, kSmallWarps * 32, small_solve_smem<T, 1>(), h->stream>>>(
+                case 1: launch_k(k_s_small_fwd<T, UNIT, 1>, g, kSmallWarps * 32, small_solve_smem<T, 1>(), h->stream, 
                             h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-                case 2: k_s_small_fwd<T, UNIT, 2><<<g, kSmallWarps * 32, small_solve_smem<T, 2>(), h->stream>>>(
+                case 2: launch_k(k_s_small_fwd<T, UNIT, 2>, g, kSmallWarps * 32, small_solve_smem<T, 2>(), h->stream, 
                             h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-                case 4: k_s_small_fwd<T, UNIT, 4><<<g, kSmallWarps * 32, small_solve_smem<T, 4>(), h->stream>>>(
+                case 4: launch_k(k_s_small_fwd<T, UNIT, 4>, g, kSmallWarps * 32, small_solve_smem<T, 4>(), h->stream, 
                             h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-                case 8: k_s_small_fwd<T, UNIT, 8><<<g, kSmallWarps * 32, small_solve_smem<T, 8>(), h->stream>>>(
+                case 8: launch_k(k_s_small_fwd<T, UNIT, 8>, g, kSmallWarps * 32, small_solve_smem<T, 8>(), h->stream, 
                             h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
-                default: k_s_small_fwd<T, UNIT, 16><<<g, kSmallWarps * 32, small_solve_smem<T, 16>(), h->stream>>>(
+                default: launch_k(k_s_small_fwd<T, UNIT, 16>, g, kSmallWarps * 32, small_solve_smem<T, 16>(), h->stream, 
                             h->d_fronts, it, c, h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
         }
+        const bool mid = h->mid_solve && lv.s_mid.cnt;
+        if (mid) {
+            Timer t(h, K_S_FWD);
+            if (int rc = launch_mid<T, 0>(h, lv, sb, nrb, nrhs)) return rc;
+            continue;
+        }
         if (lv.s_gather.cnt) {
             Timer t(h, K_S_GATHER);
-            k_s_gather<T><<<(unsigned)lv.s_gather.cnt, 256, 0, h->stream>>>(
+            launch_k(k_s_gather<T>, (unsigned)lv.s_gather.cnt, 256, 0, h->stream, 
                 h->d_fronts, items + lv.s_gather.off, items, h->d_reltgt, sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
+        const bool chain = use_chain(lv);
         if (chain && lv.s_chain_f.cnt) {
             Timer t(h, K_S_FWD);
             if (int rc = launch_chain<T, 0>(h, lv, sb, nrb, nrhs)) return rc;
@@ -1239,22 +1699,22 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const unsigned gd = (unsigned)st.diag.cnt;
             const Item* itd = items + st.diag.off;
             switch (nrb) {
-                case 1: k_s_sdiag<T, 1, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 2: k_s_sdiag<T, 2, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 4: k_s_sdiag<T, 4, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 8: k_s_sdiag<T, 8, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                default: k_s_sdiag<T, 16, 0><<<gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 1: launch_k(k_s_sdiag<T, 1, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: launch_k(k_s_sdiag<T, 2, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: launch_k(k_s_sdiag<T, 4, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: launch_k(k_s_sdiag<T, 8, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: launch_k(k_s_sdiag<T, 16, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
             if (st.fwd.cnt) {
                 const unsigned gf = (unsigned)st.fwd.cnt;
                 const Item* itf = items + st.fwd.off;
                 switch (nrb) {
-                    case 1: k_s_ftile<T, 1><<<gf, 256, ftile_smem<T, 1>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 2: k_s_ftile<T, 2><<<gf, 256, ftile_smem<T, 2>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 4: k_s_ftile<T, 4><<<gf, 256, ftile_smem<T, 4>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 8: k_s_ftile<T, 8><<<gf, 256, ftile_smem<T, 8>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    default: k_s_ftile<T, 16><<<gf, 256, ftile_smem<T, 16>(), h->stream>>>(h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 1: launch_k(k_s_ftile<T, 1>, gf, 256, ftile_smem<T, 1>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: launch_k(k_s_ftile<T, 2>, gf, 256, ftile_smem<T, 2>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: launch_k(k_s_ftile<T, 4>, gf, 256, ftile_smem<T, 4>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: launch_k(k_s_ftile<T, 8>, gf, 256, ftile_smem<T, 8>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: launch_k(k_s_ftile<T, 16>, gf, 256, ftile_smem<T, 16>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
                 }
                 MF_CUDA(cudaGetLastError());
             }
@@ -1264,69 +1724,75 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const unsigned gl = (unsigned)lv.s_fwd_l.cnt;
             const Item* itl = items + lv.s_fwd_l.off;
             switch (nrb) {
-                case 1: k_s_fwd_l<T, 1><<<gl, 256, fwdl_smem<T, 1>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 2: k_s_fwd_l<T, 2><<<gl, 256, fwdl_smem<T, 2>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 4: k_s_fwd_l<T, 4><<<gl, 256, fwdl_smem<T, 4>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 8: k_s_fwd_l<T, 8><<<gl, 256, fwdl_smem<T, 8>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
-                default: k_s_fwd_l<T, 16><<<gl, 256, fwdl_smem<T, 16>(), h->stream>>>(h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 1: launch_k(k_s_fwd_l<T, 1>, gl, 256, fwdl_smem<T, 1>(), h->stream, h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 2: launch_k(k_s_fwd_l<T, 2>, gl, 256, fwdl_smem<T, 2>(), h->stream, h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 4: launch_k(k_s_fwd_l<T, 4>, gl, 256, fwdl_smem<T, 4>(), h->stream, h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 8: launch_k(k_s_fwd_l<T, 8>, gl, 256, fwdl_smem<T, 8>(), h->stream, h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
+                default: launch_k(k_s_fwd_l<T, 16>, gl, 256, fwdl_smem<T, 16>(), h->stream, h->d_fronts, itl, sb.P, sb.C, sb.part, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
-            k_s_fwd_red<T><<<(unsigned)lv.s_fwd_red.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_fwd_red.off,
+            launch_k(k_s_fwd_red<T>, (unsigned)lv.s_fwd_red.cnt, 256, 0, h->stream, h->d_fronts, items + lv.s_fwd_red.off,
                                                                               sb.part, sb.R, nrhs);
             MF_CUDA(cudaGetLastError());
         }
     }
     if (UNIT) {
         Timer t(h, K_OTHER);
-        k_diag_div<T><<<grid_stride_blocks(n * nrhs), 256, 0, h->stream>>>(sb.C, sb.d, n, nrhs);
+        launch_k(k_diag_div<T>, grid_stride_blocks(n * nrhs), 256, 0, h->stream, sb.C, sb.d, n, nrhs);
         MF_CUDA(cudaGetLastError());
     }
     // backward: levels descending
     for (size_t L = h->levels.size(); L-- > 0;) {
         const Level& lv = h->levels[L];
-        if (lv.s_bwd_l.cnt) {
+        const bool mid = h->mid_solve && lv.s_mid.cnt;
+        if (mid) {
+            Timer t(h, K_S_BWD);
+            if (int rc = launch_mid<T, 1>(h, lv, sb, nrb, nrhs)) return rc;
+        }
+        if (!mid && lv.s_bwd_l.cnt) {
             Timer t(h, K_S_BWD_L);
             const unsigned gl = (unsigned)lv.s_bwd_l.cnt;
             const Item* itl = items + lv.s_bwd_l.off;
             switch (nrb) {
-                case 1: k_s_bwd_l<T, 1><<<gl, 256, bwd_smem<T, 1>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 2: k_s_bwd_l<T, 2><<<gl, 256, bwd_smem<T, 2>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 4: k_s_bwd_l<T, 4><<<gl, 256, bwd_smem<T, 4>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
-                case 8: k_s_bwd_l<T, 8><<<gl, 256, bwd_smem<T, 8>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
-                default: k_s_bwd_l<T, 16><<<gl, 256, bwd_smem<T, 16>(), h->stream>>>(h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 1: launch_k(k_s_bwd_l<T, 1>, gl, 256, bwd_smem<T, 1>(), h->stream, h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 2: launch_k(k_s_bwd_l<T, 2>, gl, 256, bwd_smem<T, 2>(), h->stream, h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 4: launch_k(k_s_bwd_l<T, 4>, gl, 256, bwd_smem<T, 4>(), h->stream, h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                case 8: launch_k(k_s_bwd_l<T, 8>, gl, 256, bwd_smem<T, 8>(), h->stream, h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
+                default: launch_k(k_s_bwd_l<T, 16>, gl, 256, bwd_smem<T, 16>(), h->stream, h->d_fronts, itl, h->d_septgt, sb.P, sb.C, sb.part, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
-            k_s_bwd_red<T><<<(unsigned)lv.s_bwd_red.cnt, 256, 0, h->stream>>>(h->d_fronts, items + lv.s_bwd_red.off,
+            launch_k(k_s_bwd_red<T>, (unsigned)lv.s_bwd_red.cnt, 256, 0, h->stream, h->d_fronts, items + lv.s_bwd_red.off,
                                                                               sb.part, sb.C, sb.W, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
-        if (chain && lv.s_chain_b.cnt) {
+        const bool chain = use_chain(lv);
+        if (!mid && chain && lv.s_chain_b.cnt) {
             Timer t(h, K_S_BWD);
             if (int rc = launch_chain<T, 1>(h, lv, sb, nrb, nrhs)) return rc;
         }
-        for (size_t k = lv.s_steps.size(); !chain && k-- > 0;) {
+        for (size_t k = lv.s_steps.size(); !mid && !chain && k-- > 0;) {
             const SolveStep& st = lv.s_steps[k];
             if (!st.diag.cnt) continue;
             Timer t(h, K_S_BWD);
             const unsigned gd = (unsigned)st.diag.cnt;
             const Item* itd = items + st.diag.off;
             switch (nrb) {
-                case 1: k_s_sdiag<T, 1, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 2: k_s_sdiag<T, 2, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 4: k_s_sdiag<T, 4, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 8: k_s_sdiag<T, 8, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                default: k_s_sdiag<T, 16, 1><<<gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream>>>(h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 1: launch_k(k_s_sdiag<T, 1, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: launch_k(k_s_sdiag<T, 2, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: launch_k(k_s_sdiag<T, 4, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: launch_k(k_s_sdiag<T, 8, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: launch_k(k_s_sdiag<T, 16, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
             if (st.bwd.cnt) {
                 const unsigned gb = (unsigned)st.bwd.cnt;
                 const Item* itb = items + st.bwd.off;
                 switch (nrb) {
-                    case 1: k_s_btile<T, 1><<<gb, 256, btile_smem<T, 1>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 2: k_s_btile<T, 2><<<gb, 256, btile_smem<T, 2>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 4: k_s_btile<T, 4><<<gb, 256, btile_smem<T, 4>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 8: k_s_btile<T, 8><<<gb, 256, btile_smem<T, 8>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    default: k_s_btile<T, 16><<<gb, 256, btile_smem<T, 16>(), h->stream>>>(h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 1: launch_k(k_s_btile<T, 1>, gb, 256, btile_smem<T, 1>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: launch_k(k_s_btile<T, 2>, gb, 256, btile_smem<T, 2>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: launch_k(k_s_btile<T, 4>, gb, 256, btile_smem<T, 4>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: launch_k(k_s_btile<T, 8>, gb, 256, btile_smem<T, 8>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: launch_k(k_s_btile<T, 16>, gb, 256, btile_smem<T, 16>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
                 }
                 MF_CUDA(cudaGetLastError());
             }
@@ -1337,19 +1803,21 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const Item* it = items + lv.s_small.off;
             const int64_t c = lv.s_small.cnt;
             switch (nrb) {
-                case 1: k_s_small_bwd<T, UNIT, 1><<<g, kSmallWarps * 32, 0, h->stream>>>(
+                case 1: launch_k(k_s_small_bwd<T, UNIT, 1>, g, kSmallWarps * 32, 0, h->stream, 
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 2: k_s_small_bwd<T, UNIT, 2><<<g, kSmallWarps * 32, 0, h->stream>>>(
+                case 2: launch_k(k_s_small_bwd<T, UNIT, 2>, g, kSmallWarps * 32, 0, h->stream, 
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 4: k_s_small_bwd<T, UNIT, 4><<<g, kSmallWarps * 32, 0, h->stream>>>(
+                case 4: launch_k(k_s_small_bwd<T, UNIT, 4>, g, kSmallWarps * 32, 0, h->stream, 
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                case 8: k_s_small_bwd<T, UNIT, 8><<<g, kSmallWarps * 32, 0, h->stream>>>(
+                case 8: launch_k(k_s_small_bwd<T, UNIT, 8>, g, kSmallWarps * 32, 0, h->stream, 
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-                default: k_s_small_bwd<T, UNIT, 16><<<g, kSmallWarps * 32, 0, h->stream>>>(
+                default: launch_k(k_s_small_bwd<T, UNIT, 16>, g, kSmallWarps * 32, 0, h->stream, 
                             h->d_fronts, it, c, h->d_septgt, sb.P, sb.C, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
         }
+        if (lv.s_tiny.cnt)
+            if (int rc = launch_tiny<T, UNIT, 1>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
     }
     if (h->sub_tasks.cnt) {
         // the subtrees of small fronts, backward, in one launch
@@ -1357,15 +1825,15 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         const unsigned g = (unsigned)h->sub_tasks.cnt;
         const int64_t t0 = h->sub_tasks.off;
         switch (nrb) {
-            case 1: k_s_sub_bwd<T, UNIT, 1><<<g, kSubWarps * 32, 0, h->stream>>>(
+            case 1: launch_k(k_s_sub_bwd<T, UNIT, 1>, g, kSubWarps * 32, 0, h->stream, 
                         h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-            case 2: k_s_sub_bwd<T, UNIT, 2><<<g, kSubWarps * 32, 0, h->stream>>>(
+            case 2: launch_k(k_s_sub_bwd<T, UNIT, 2>, g, kSubWarps * 32, 0, h->stream, 
                         h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-            case 4: k_s_sub_bwd<T, UNIT, 4><<<g, kSubWarps * 32, 0, h->stream>>>(
+            case 4: launch_k(k_s_sub_bwd<T, UNIT, 4>, g, kSubWarps * 32, 0, h->stream, 
                         h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-            case 8: k_s_sub_bwd<T, UNIT, 8><<<g, kSubWarps * 32, 0, h->stream>>>(
+            case 8: launch_k(k_s_sub_bwd<T, UNIT, 8>, g, kSubWarps * 32, 0, h->stream, 
                         h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
-            default: k_s_sub_bwd<T, UNIT, 16><<<g, kSubWarps * 32, 0, h->stream>>>(
+            default: launch_k(k_s_sub_bwd<T, UNIT, 16>, g, kSubWarps * 32, 0, h->stream, 
                         h->d_fronts, items, t0, h->d_septgt, sb.P, sb.C, n, nrhs); break;
         }
         MF_CUDA(cudaGetLastError());

@@ -328,6 +328,7 @@ __global__ void __launch_bounds__(tc::NT, 1) k_gemm_tc(const Front* __restrict__
                                                        const CUtensorMap* __restrict__ maps,
                                                        const CUtensorMap* __restrict__ inv_map,
                                                        const float* __restrict__ split, int* __restrict__ err) {
+    pdl_prologue();
     using namespace tc;
     constexpr int TN = TcTileN<ROLE>::value;
     using C_ = Cfg<TN>;
@@ -580,7 +581,7 @@ static int launch_one(mf_handle* h, const ItemList& l, int obs, int obw, int c0,
     if (!l.cnt) return 0;
     constexpr int smem = tc::Cfg<TcTileN<ROLE>::value>::SMEM_BYTES;
     const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
-    k_gemm_tc<ROLE, LDLT, false><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
+    launch_k(k_gemm_tc<ROLE, LDLT, false>, (unsigned)grid, tc::NT, smem, h->stream, 
         h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
         nullptr, h->d_err);
@@ -599,6 +600,7 @@ template <int LDLT, int SYRK>
 __global__ void __launch_bounds__(256) k_tc_split(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                   int obs, int obw, const float* __restrict__ P,
                                                   const float* __restrict__ d, float* __restrict__ split) {
+    pdl_prologue();
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
     const int nn = f.nn, nj = nn + f.na, ld = f.ldp;
@@ -656,13 +658,13 @@ static int launch_split(mf_handle* h, const ItemList& l, const ItemList& units, 
                         const FactorBufs<float>& fb) {
     if (!l.cnt) return 0;
     if (units.cnt) {
-        k_tc_split<LDLT, ROLE == TC_SYRK><<<(unsigned)units.cnt, 256, 0, h->stream>>>(
+        launch_k(k_tc_split<LDLT, ROLE == TC_SYRK>, (unsigned)units.cnt, 256, 0, h->stream, 
             h->d_fronts, h->d_items + units.off, obs, obw, fb.P, fb.d, h->f32.split);
         MF_CUDA(cudaGetLastError());
     }
     constexpr int smem = tc::SplitCfg<TcTileN<ROLE>::value>::SMEM_BYTES;
     const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
-    k_gemm_tc<ROLE, LDLT, true><<<(unsigned)grid, tc::NT, smem, h->stream>>>(
+    launch_k(k_gemm_tc<ROLE, LDLT, true>, (unsigned)grid, tc::NT, smem, h->stream, 
         h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
         h->f32.split, h->d_err);

@@ -1,10 +1,14 @@
 """The blocked fronts' super-block solve chain as one persistent k_s_chain
-launch per level and direction (MF_SOLVE_CHAIN=1) against the per-step
-launches (MF_SOLVE_CHAIN=0, the default), and the small-front subtrees in one
-launch per direction (MF_SUBTREE_SOLVE=1) against the per-level launches:
-the items do the same arithmetic in the same order, so the solutions must be
-bitwise equal; both are checked against the oracle (normwise backward error
-<= 1e-13, FP64; <= 1e-12 refined)."""
+launch per level and direction (MF_SOLVE_CHAIN=1; by default only levels
+of 64 or more steps) against the per-step launches (MF_SOLVE_CHAIN=0), the
+small-front subtrees in one launch per direction (MF_SUBTREE_SOLVE=1)
+against the per-level launches, the single-super-block levels as one
+cluster launch per level and direction (MF_MID_SOLVE=1) against the
+per-kernel launches, and fronts of at most 16 rows solved 16 lanes each
+(MF_TINY_SOLVE=1, the default) against one warp each: the items do the same
+arithmetic in the same order, so the solutions must be bitwise equal; all
+are checked against the oracle (normwise backward error <= 1e-13, FP64;
+<= 1e-12 refined)."""
 import numpy as np
 import pytest
 
@@ -76,3 +80,71 @@ def test_subtree_solves_equal_per_level_launches(monkeypatch, ldlt):
     X = both(monkeypatch, make, B, var="MF_SUBTREE_SOLVE")
     assert np.array_equal(X["0"], X["1"])
     assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+@pytest.mark.parametrize("nrhs", [1, 3, 16])
+def test_mid_levels_equal_per_kernel_launches(monkeypatch, ldlt, nrhs):
+    """A 3D grid under geometric nested dissection: most levels hold only
+    single-super-block fronts (one cluster launch per level and direction),
+    the top levels keep the stepped kernels."""
+    A, P, S = grid(20, 19, 18, seed=65)
+    B = tm.rhs(S.n, nrhs, seed=6 + nrhs)
+    make = (lambda: mf.ldlt_(mf.ChordalLDLt(A, P, S))) if ldlt else (lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)))
+    X = both(monkeypatch, make, B, var="MF_MID_SOLVE")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, int(ldlt))
+    assert np.abs(X["1"] - Xo).max() <= 1e-9 * np.abs(Xo).max()
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+def test_mid_levels_mixed_refined(monkeypatch, ldlt):
+    A, P, S = grid(24, 23, 22, seed=66)
+    B = tm.rhs(S.n, 4, seed=8)
+    make = ((lambda: mf.ldlt_(mf.ChordalLDLt(A, P, S, mixed=True))) if ldlt
+            else (lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True))))
+    X = both(monkeypatch, make, B, var="MF_MID_SOLVE")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-12
+
+
+def test_mid_level_root_without_l21(monkeypatch):
+    """An 8 x 8 x 8 grid: the root front (a 64-column separator, no L21) is
+    itself a single-super-block level, and the 2D 60 x 50 grid under AMF
+    adds levels that mix warp-per-front fronts with cluster fronts."""
+    import scipy.sparse as sp
+    A = sp.block_diag([tm.grid_laplacian(8, 8, 8, seed=67), tm.grid_laplacian(60, 50, seed=68)]).tocsc()
+    P, S = mf.symbolic(A)
+    B = tm.rhs(S.n, 2, seed=9)
+    X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)), B, var="MF_MID_SOLVE")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+
+
+@pytest.mark.parametrize("ldlt", [False, True])
+@pytest.mark.parametrize("nrhs", [1, 4, 16])
+def test_tiny_fronts_equal_warp_per_front(monkeypatch, ldlt, nrhs):
+    """Fronts with at most 16 rows solved 16 lanes each (MF_TINY_SOLVE=1,
+    the default) against one warp each (MF_TINY_SOLVE=0): a forest of 2D
+    9-point grids under AMF, whose lowest levels are all such fronts."""
+    import scipy.sparse as sp
+    mats = [tm.config3_matrix(int(s), seed=300 + i) for i, s in enumerate([8, 13, 21, 30, 17, 9, 25, 11])]
+    A = sp.block_diag(mats).tocsc()
+    P, S = mf.symbolic(A)
+    B = tm.rhs(S.n, nrhs, seed=10 + nrhs)
+    make = (lambda: mf.ldlt_(mf.ChordalLDLt(A, P, S))) if ldlt else (lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S)))
+    X = both(monkeypatch, make, B, var="MF_TINY_SOLVE")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-13
+    info, Xo, _ = oracle.factor_and_solve(A, P, S, B, int(ldlt))
+    assert np.abs(X["1"] - Xo).max() <= 1e-9 * np.abs(Xo).max()
+
+
+def test_tiny_fronts_mixed_refined(monkeypatch):
+    A = tm.grid_laplacian(70, 65, stencil=9, seed=69)
+    P, S = mf.symbolic(A)
+    B = tm.rhs(S.n, 3, seed=11)
+    X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True)), B, var="MF_TINY_SOLVE")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= 1e-12
