@@ -248,6 +248,7 @@ __device__ void small_front_store(const TC* F, const Front& f, T* __restrict__ P
 // result is stored rounded to FP32.  A rejection in FP64 -- or in FP32 for a
 // larger front -- is reported through info.
 constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
+constexpr int kSmallNarrowNJ = 48;  // levels whose small fronts all have nj <= this run 128-thread CTAs
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -1494,7 +1495,14 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         }
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
-            launch_k(k_small<T, LDLT>, grid_for(lv.small.cnt), 256, kSmallMax * kSmallMax * sizeof(T), h->stream, 
+            // shared memory for the level's largest front (as FP64 up to
+            // kSmallRescue rows, for the in-place rescue of an FP32 front) and
+            // 128 threads for levels of narrow fronts: more fronts in flight
+            const int mj = lv.small_maxnj;
+            const int rj = std::min(mj, kSmallRescue);
+            const size_t sm = std::max<size_t>((size_t)mj * mj * sizeof(T), sizeof(T) == 4 ? (size_t)rj * rj * 8 : 0);
+            const unsigned nt = mj <= kSmallNarrowNJ ? 128 : 256;
+            launch_k(k_small<T, LDLT>, grid_for(lv.small.cnt), nt, sm, h->stream, 
                 h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
                 h->d_info, h->d_rescued, reg);
             MF_CUDA(cudaGetLastError());

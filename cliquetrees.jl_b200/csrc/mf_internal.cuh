@@ -130,6 +130,7 @@ struct SolveStep {
 struct Level {
     ItemList small_warp;     // (front)           fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
     ItemList small;          // (front)           other fronts with nj <= kSmallMax: one CTA each (k_small)
+    int small_maxnj = 0;     // largest nj of those (sizes k_small's shared memory and CTA)
     // extend-add for blocked fronts, item (front, col tile, row chunk, first
     // segment): ea adds the children into the panel columns before the
     // panel is factored; ea_upd adds them into the update matrix after the

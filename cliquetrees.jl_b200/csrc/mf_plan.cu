@@ -423,7 +423,10 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn + f.na > kWarpSmallNJ && f.nn + f.na <= kSmallMax) push(j, 0, 0);
+            if (f.nn + f.na > kWarpSmallNJ && f.nn + f.na <= kSmallMax) {
+                push(j, 0, 0);
+                lv.small_maxnj = std::max(lv.small_maxnj, f.nn + f.na);
+            }
         }
         end(lv.small);
         int max_steps = 0;
