@@ -268,7 +268,7 @@ int mf_plan_info(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* s
     if (rc) return rc;
     int64_t launches = 0;
     for (const Level& lv : h.levels) {
-        launches += (lv.small_warp.cnt > 0) + (lv.small.cnt > 0) + (lv.ea.cnt > 0) + (lv.ea_upd.cnt > 0) +
+        launches += (lv.small_warp.cnt > 0) + (lv.small_warp2.cnt > 0) + (lv.small.cnt > 0) + (lv.ea.cnt > 0) + (lv.ea_upd.cnt > 0) +
                     (lv.syrk.cnt > 0);
         for (const PanelStep& st : lv.steps)
             launches += (st.left.cnt > 0) + (st.diag.cnt > 0) + (st.panel.cnt > 0) + (st.trail.cnt > 0);

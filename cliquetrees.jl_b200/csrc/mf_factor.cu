@@ -248,7 +248,8 @@ __device__ void small_front_store(const TC* F, const Front& f, T* __restrict__ P
 // result is stored rounded to FP32.  A rejection in FP64 -- or in FP32 for a
 // larger front -- is reported through info.
 constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
-constexpr int kSmallNarrowNJ = 48;  // levels whose small fronts all have nj <= this run 128-thread CTAs
+constexpr int kSmallNarrowNJ = 48;     // levels whose small fronts all have nj <= this ...
+constexpr int kSmallWideLevel = 4 * 148;  // ... and that hold at least this many run 128-thread CTAs
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -286,20 +287,21 @@ __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts,
 }
 
 // ---------------------------------------------------------------------------
-// Tiny fronts (nj <= kWarpFrontMax): one WARP per front, kWarpFronts fronts per
-// CTA, warp-synchronous (no block barriers).  Lane r holds row r of the front
-// in the warp's slice of shared memory (leading dimension kWLD, sized for
-// FP64 so a flagged single-precision front can be redone in place).  The
+// Tiny fronts (nj <= ROWS, ROWS = 16 or 32): one WARP per front, kWarpFronts
+// fronts per CTA, warp-synchronous (no block barriers).  Lane r holds row r of
+// the front in the warp's slice of shared memory (leading dimension ROWS + 1,
+// sized for FP64 so a flagged single-precision front can be redone in place).  The
 // arithmetic is k_small's: the children added in the reference's reverse
 // order, one addition per entry and child, then the right-looking partial
 // factorization with the same update expression.
 // ---------------------------------------------------------------------------
-constexpr int kWarpFrontMax = kWarpSmallNJ;  // 16: lanes 16..31 idle, registers and shared memory small
-constexpr int kWLD = kWarpFrontMax + 1;
+// ROWS = 16 (nj <= kWarpSmallNJ: lanes 16..31 idle, registers and shared
+// memory small) or 32 (kWarpSmallNJ < nj <= kWarpSmallNJ2)
 constexpr int kWarpFronts = 8;
-constexpr int kWarpSlice = kWLD * kWarpFrontMax * (int)sizeof(double);  // bytes per warp
+template <int ROWS>
+constexpr int warp_slice() { return (ROWS + 1) * ROWS * (int)sizeof(double); }  // bytes per warp
 
-template <typename TC, typename T, int LDLT>
+template <typename TC, typename T, int LDLT, int ROWS>
 __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ fronts,
                           const int32_t* __restrict__ reltgt, const int32_t* __restrict__ chdtgt,
                           const T* __restrict__ P, const T* __restrict__ M, const double* __restrict__ signs,
@@ -309,12 +311,12 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
     const bool row = lane < nj;
     {
         // every panel load of the lane in flight at once, then the stores
-        T v[kWarpFrontMax];
+        T v[ROWS];
 #pragma unroll
-        for (int c = 0; c < kWarpFrontMax; ++c) v[c] = (row && c < nn) ? Pj[lane + (int64_t)c * ld] : T(0);
+        for (int c = 0; c < ROWS; ++c) v[c] = (row && c < nn) ? Pj[lane + (int64_t)c * ld] : T(0);
 #pragma unroll
-        for (int c = 0; c < kWarpFrontMax; ++c)
-            if (row && c < nj) F[lane + c * kWLD] = (TC)v[c];
+        for (int c = 0; c < ROWS; ++c)
+            if (row && c < nj) F[lane + c * (ROWS + 1)] = (TC)v[c];
     }
     __syncwarp();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
@@ -324,19 +326,19 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
         const int32_t* rel = reltgt + fc.sep0;
         const T* Mc = M + fc.moff;
         const int ra = lane < ma ? rel[lane] : 0;
-        T mv[kWarpFrontMax];
+        T mv[ROWS];
 #pragma unroll
-        for (int b = 0; b < kWarpFrontMax; ++b) mv[b] = (b < ma && lane >= b && lane < ma) ? Mc[lane + b * lm] : T(0);
+        for (int b = 0; b < ROWS; ++b) mv[b] = (b < ma && lane >= b && lane < ma) ? Mc[lane + b * lm] : T(0);
 #pragma unroll
-        for (int b = 0; b < kWarpFrontMax; ++b) {
+        for (int b = 0; b < ROWS; ++b) {
             const int rb = __shfl_sync(0xffffffffu, ra, b);
-            if (b < ma && lane >= b && lane < ma) F[ra + rb * kWLD] += (TC)mv[b];
+            if (b < ma && lane >= b && lane < ma) F[ra + rb * (ROWS + 1)] += (TC)mv[b];
         }
         __syncwarp();
     }
     // right-looking partial factorization of the first nn columns
     for (int k = 0; k < nn; ++k) {
-        TC piv = F[k + k * kWLD];
+        TC piv = F[k + k * (ROWS + 1)];
         const double s = pivot_sign(signs, LDLT, f.col0 + k);
         if (reg.delta >= 0.0) {
             piv = (TC)reg_pivot(reg, s, (double)piv);
@@ -352,15 +354,15 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
         const TC dk = LDLT ? piv : sqrt(piv);
         const TC inv = TC(1) / dk;
         __syncwarp();
-        if (lane == k) F[k + k * kWLD] = LDLT ? piv : dk;
-        if (lane > k && row) F[lane + k * kWLD] *= inv;
+        if (lane == k) F[k + k * (ROWS + 1)] = LDLT ? piv : dk;
+        if (lane > k && row) F[lane + k * (ROWS + 1)] *= inv;
         __syncwarp();
         if (lane > k && row) {
-            const TC lr = F[lane + k * kWLD];
+            const TC lr = F[lane + k * (ROWS + 1)];
             for (int c = k + 1; c <= lane; ++c) {
-                TC lc = F[c + k * kWLD];
+                TC lc = F[c + k * (ROWS + 1)];
                 if (LDLT) lc *= piv;
-                F[lane + c * kWLD] -= lr * lc;
+                F[lane + c * (ROWS + 1)] -= lr * lc;
             }
         }
         __syncwarp();
@@ -368,21 +370,21 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
     return -1;
 }
 
-template <typename TC, typename T, int LDLT>
+template <typename TC, typename T, int LDLT, int ROWS>
 __device__ void warp_front_store(const TC* F, const Front& f, T* __restrict__ P, T* __restrict__ M,
                                  T* __restrict__ d, int lane) {
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     T* Pj = P + f.poff;
     if (lane < nj)
-        for (int c = 0; c < nn; ++c) Pj[lane + (int64_t)c * ld] = (T)F[lane + c * kWLD];
-    if (LDLT && lane < nn) d[f.col0 + lane] = (T)F[lane + lane * kWLD];
+        for (int c = 0; c < nn; ++c) Pj[lane + (int64_t)c * ld] = (T)F[lane + c * (ROWS + 1)];
+    if (LDLT && lane < nn) d[f.col0 + lane] = (T)F[lane + lane * (ROWS + 1)];
     T* Mj = M + f.moff;
     const int lm = f.ldm;
     if (lane < na)
-        for (int b = 0; b < na; ++b) Mj[lane + b * lm] = (T)F[(nn + lane) + (nn + b) * kWLD];
+        for (int b = 0; b < na; ++b) Mj[lane + b * lm] = (T)F[(nn + lane) + (nn + b) * (ROWS + 1)];
 }
 
-template <typename T, int LDLT>
+template <typename T, int LDLT, int ROWS>
 __global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __restrict__ fronts,
                                                                 const Item* __restrict__ items, int64_t cnt,
                                                                 const int32_t* __restrict__ reltgt,
@@ -396,23 +398,23 @@ __global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int64_t w = (int64_t)blockIdx.x * kWarpFronts + wib;
     if (w >= cnt) return;  // whole warps only
-    unsigned char* slice = smem_raw + (size_t)wib * kWarpSlice;
+    unsigned char* slice = smem_raw + (size_t)wib * warp_slice<ROWS>();
     const Front f = fronts[items[w].front];
     constexpr bool single = sizeof(T) == 4;
     bool flag = false;
     T* F = reinterpret_cast<T*>(slice);
-    int bad = warp_front<T, T, LDLT>(F, f, fronts, reltgt, chdtgt, P, M, signs, single, &flag, reg, lane);
+    int bad = warp_front<T, T, LDLT, ROWS>(F, f, fronts, reltgt, chdtgt, P, M, signs, single, &flag, reg, lane);
     if (single && (bad >= 0 || flag)) {
         // the panel and the children's update matrices are only read before
         // the final store: refactor from the same inputs in FP64
         double* F64 = reinterpret_cast<double*>(slice);
         __syncwarp();
         bool unused = false;
-        bad = warp_front<double, T, LDLT>(F64, f, fronts, reltgt, chdtgt, P, M, signs, false, &unused, reg, lane);
+        bad = warp_front<double, T, LDLT, ROWS>(F64, f, fronts, reltgt, chdtgt, P, M, signs, false, &unused, reg, lane);
         if (bad < 0) {
             if (lane == 0) atomicAdd(rescued, 1);
             __syncwarp();
-            warp_front_store<double, T, LDLT>(F64, f, P, M, d, lane);
+            warp_front_store<double, T, LDLT, ROWS>(F64, f, P, M, d, lane);
             return;
         }
     }
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(kWarpFronts * 32) k_small_warp(const Front* __
         return;
     }
     __syncwarp();
-    warp_front_store<T, T, LDLT>(F, f, P, M, d, lane);
+    warp_front_store<T, T, LDLT, ROWS>(F, f, P, M, d, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -1467,8 +1469,10 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
     constexpr int gs = gemm_smem<T>();
     MF_CUDA(cudaFuncSetAttribute(k_small<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  kSmallMax * kSmallMax * (int)sizeof(T)));
-    MF_CUDA(cudaFuncSetAttribute(k_small_warp<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kWarpFronts * kWarpSlice));
+    MF_CUDA(cudaFuncSetAttribute(k_small_warp<T, LDLT, kWarpSmallNJ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kWarpFronts * warp_slice<kWarpSmallNJ>()));
+    MF_CUDA(cudaFuncSetAttribute(k_small_warp<T, LDLT, kWarpSmallNJ2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kWarpFronts * warp_slice<kWarpSmallNJ2>()));
     MF_CUDA(cudaFuncSetAttribute(k_diag<T, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_inv256<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv256_smem<T>()));
     MF_CUDA(cudaFuncSetAttribute(k_gemm<T, G_LEFT, LDLT>, cudaFuncAttributeMaxDynamicSharedMemorySize, gs));
@@ -1488,20 +1492,30 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         if (lv.small_warp.cnt) {
             Timer t(h, K_SMALL);
             const unsigned g = (unsigned)((lv.small_warp.cnt + kWarpFronts - 1) / kWarpFronts);
-            launch_k(k_small_warp<T, LDLT>, g, kWarpFronts * 32, kWarpFronts * kWarpSlice, h->stream, 
-                h->d_fronts, items + lv.small_warp.off, lv.small_warp.cnt, h->d_reltgt, h->d_chdtgt, fb.P, fb.M,
-                fb.d, h->d_signs, h->d_info, h->d_rescued, reg);
+            launch_k(k_small_warp<T, LDLT, kWarpSmallNJ>, g, kWarpFronts * 32, kWarpFronts * warp_slice<kWarpSmallNJ>(),
+                h->stream, h->d_fronts, items + lv.small_warp.off, lv.small_warp.cnt, h->d_reltgt, h->d_chdtgt, fb.P,
+                fb.M, fb.d, h->d_signs, h->d_info, h->d_rescued, reg);
+            MF_CUDA(cudaGetLastError());
+        }
+        if (lv.small_warp2.cnt) {
+            Timer t(h, K_SMALL);
+            const unsigned g = (unsigned)((lv.small_warp2.cnt + kWarpFronts - 1) / kWarpFronts);
+            launch_k(k_small_warp<T, LDLT, kWarpSmallNJ2>, g, kWarpFronts * 32,
+                kWarpFronts * warp_slice<kWarpSmallNJ2>(), h->stream, h->d_fronts, items + lv.small_warp2.off,
+                lv.small_warp2.cnt, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs, h->d_info, h->d_rescued,
+                reg);
             MF_CUDA(cudaGetLastError());
         }
         if (lv.small.cnt) {
             Timer t(h, K_SMALL);
             // shared memory for the level's largest front (as FP64 up to
             // kSmallRescue rows, for the in-place rescue of an FP32 front) and
-            // 128 threads for levels of narrow fronts: more fronts in flight
+            // 128 threads for levels of many narrow fronts: more fronts in
+            // flight (a level of few fronts keeps 256 threads, for latency)
             const int mj = lv.small_maxnj;
             const int rj = std::min(mj, kSmallRescue);
             const size_t sm = std::max<size_t>((size_t)mj * mj * sizeof(T), sizeof(T) == 4 ? (size_t)rj * rj * 8 : 0);
-            const unsigned nt = mj <= kSmallNarrowNJ ? 128 : 256;
+            const unsigned nt = (mj <= kSmallNarrowNJ && lv.small.cnt >= kSmallWideLevel) ? 128 : 256;
             launch_k(k_small<T, LDLT>, grid_for(lv.small.cnt), nt, sm, h->stream, 
                 h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
                 h->d_info, h->d_rescued, reg);

@@ -79,6 +79,7 @@ struct ItemList {
 
 constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
 constexpr int kWarpSmallNJ = 16; // of those, fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
+constexpr int kWarpSmallNJ2 = 32; // and kWarpSmallNJ < nj <= kWarpSmallNJ2: one warp each, 32-row variant
 constexpr int kTinyNJ = 16;      // solves: fronts with nj <= kTinyNJ take 16 lanes each (k_s_tiny_*)
 constexpr int kNB = 64;         // sub-panel width of the blocked path
 #ifndef MF_KOB
@@ -129,6 +130,7 @@ struct SolveStep {
 
 struct Level {
     ItemList small_warp;     // (front)           fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
+    ItemList small_warp2;    // (front)           kWarpSmallNJ < nj <= kWarpSmallNJ2: one warp each (MF_WARP_FRONT32=0: k_small)
     ItemList small;          // (front)           other fronts with nj <= kSmallMax: one CTA each (k_small)
     int small_maxnj = 0;     // largest nj of those (sizes k_small's shared memory and CTA)
     // extend-add for blocked fronts, item (front, col tile, row chunk, first

@@ -410,6 +410,10 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     std::vector<Item> gseg;  // forward-gather segments, appended after the levels
     std::vector<Item> easeg; // extend-add segments, appended after them
 
+    // the 32-row warp-per-front factor measured slower than k_small with its
+    // per-level sizing (2D batch and 100^2 grid), so it is opt-in
+    const char* w32env = getenv("MF_WARP_FRONT32");
+    const bool warp32 = w32env && w32env[0] == '1';
     for (int L = 0; L <= max_level; ++L) {
         Level& lv = h->levels[L];
         const std::vector<int32_t>& fr = by_level[L];
@@ -420,10 +424,16 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (f.nn + f.na <= kWarpSmallNJ) push(j, 0, 0);
         }
         end(lv.small_warp);
+        begin(lv.small_warp2);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            if (warp32 && f.nn + f.na > kWarpSmallNJ && f.nn + f.na <= kWarpSmallNJ2) push(j, 0, 0);
+        }
+        end(lv.small_warp2);
         begin(lv.small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (f.nn + f.na > kWarpSmallNJ && f.nn + f.na <= kSmallMax) {
+            if (f.nn + f.na > (warp32 ? kWarpSmallNJ2 : kWarpSmallNJ) && f.nn + f.na <= kSmallMax) {
                 push(j, 0, 0);
                 lv.small_maxnj = std::max(lv.small_maxnj, f.nn + f.na);
             }
