@@ -81,6 +81,7 @@ constexpr int kSmallMax = 96;   // fronts with nj <= kSmallMax: one fused CTA
 constexpr int kWarpSmallNJ = 16; // of those, fronts with nj <= kWarpSmallNJ: one warp each (k_small_warp)
 constexpr int kWarpSmallNJ2 = 32; // and kWarpSmallNJ < nj <= kWarpSmallNJ2: one warp each, 32-row variant
 constexpr int kTinyNJ = 16;      // solves: fronts with nj <= kTinyNJ take 16 lanes each (k_s_tiny_*)
+constexpr int kTinyNJ2 = 32;     // and kTinyNJ < nj <= kTinyNJ2 a warp each, with k_s_tiny_*'s design
 constexpr int kNB = 64;         // sub-panel width of the blocked path
 #ifndef MF_KOB
 #define MF_KOB 256
@@ -149,6 +150,7 @@ struct Level {
     // solves
     ItemList s_small;        // (front)
     ItemList s_tiny;         // (front)           small fronts with nj <= kTinyNJ: 16 lanes each
+    ItemList s_tiny2;        // (front)           small fronts with kTinyNJ < nj <= kTinyNJ2: a warp each
     ItemList s_gather;       // (front, row tile) forward gather of child updates
     std::vector<SolveStep> s_steps;
     ItemList s_fwd_l;        // (front, row tile, col chunk; pad = partial slot) R -= L21 x1

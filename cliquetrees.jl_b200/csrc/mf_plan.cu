@@ -624,7 +624,7 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         begin(lv.s_small);
         for (int32_t j : fr) {
             const Front& f = h->h_fronts[j];
-            if (solve_small(f) && task_of[j] < 0 && f.nn + f.na > kTinyNJ) push(j, 0, 0);
+            if (solve_small(f) && task_of[j] < 0 && f.nn + f.na > kTinyNJ2) push(j, 0, 0);
         }
         end(lv.s_small);
         begin(lv.s_tiny);
@@ -633,6 +633,13 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (solve_small(f) && task_of[j] < 0 && f.nn + f.na <= kTinyNJ) push(j, 0, 0);
         }
         end(lv.s_tiny);
+        begin(lv.s_tiny2);
+        for (int32_t j : fr) {
+            const Front& f = h->h_fronts[j];
+            const int nj = f.nn + f.na;
+            if (solve_small(f) && task_of[j] < 0 && nj > kTinyNJ && nj <= kTinyNJ2) push(j, 0, 0);
+        }
+        end(lv.s_tiny2);
         // forward gather: item (front, row tile, first segment, segments);
         // a segment (child, a0, a1) is the run rel[a0:a1] of a child's update
         // rows that lands in the tile, children in reverse order

@@ -342,22 +342,32 @@ __global__ void __launch_bounds__(kSmallWarps * 32, small_min_blocks<T, NR>()) k
 }
 
 // ---------------------------------------------------------------------------
-// Tiny fronts (nj <= kTinyNJ): 16 lanes per front, two fronts per warp, lane
-// g owning row g of its front (forward) or column g (backward).  Each lane
+// Tiny fronts (nj <= G, G = 16 or 32): G lanes per front (two fronts per warp
+// for G = 16), lane g owning row g of its front (forward) or column g
+// (backward).  Each lane
 // issues all its panel loads at the start (row g of the panel forward,
-// column g backward), so a front costs a few dependent memory trips and
-// twice as many fronts are in flight per warp as with k_s_small_*.  Loops
-// over columns run to the warp's largest front (shuffles take the whole
-// warp) with the other front's steps predicated off.  Each entry gets the
+// column g backward), so a front costs a few dependent memory trips instead
+// of k_s_small_*'s chain of column steps, and for G = 16 twice as many
+// fronts are in flight per warp.  Loops over columns run to the warp's
+// largest front (shuffles take the whole warp) with the other front's steps
+// predicated off.  Each entry gets the
 // operations of k_s_small_fwd / _bwd in the same order, so the results are
 // bitwise equal to them.
 // ---------------------------------------------------------------------------
 constexpr int kTinyWarps = 4;
-constexpr int kTinyFronts = kTinyWarps * 32 / kTinyNJ;  // fronts per CTA
+template <int G>
+constexpr int tiny_fronts() { return kTinyWarps * 32 / G; }  // fronts per CTA
 
-template <typename T, int NR>
+// the larger of v and the other front's v in the warp (G = 16)
+template <int G>
+__device__ __forceinline__ int tiny_warp_max(int v) {
+    return G == 32 ? v : max(v, __shfl_xor_sync(0xffffffffu, v, 16));
+}
+
+template <typename T, int NR, int G>
 constexpr int tiny_min_blocks() {
-    return sizeof(T) == 4 ? (NR <= 4 ? 10 : NR <= 8 ? 8 : 4) : (NR <= 2 ? 8 : NR <= 4 ? 6 : NR <= 8 ? 4 : 3);
+    return G == 16 ? (sizeof(T) == 4 ? (NR <= 4 ? 10 : NR <= 8 ? 8 : 4) : (NR <= 2 ? 8 : NR <= 4 ? 6 : NR <= 8 ? 4 : 3))
+                   : (sizeof(T) == 4 ? (NR <= 4 ? 8 : NR <= 8 ? 6 : 3) : (NR <= 4 ? 4 : NR <= 8 ? 3 : 2));
 }
 
 __device__ __forceinline__ Front tiny_front(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -368,28 +378,28 @@ __device__ __forceinline__ Front tiny_front(const Front* __restrict__ fronts, co
     return f;
 }
 
-template <typename T, int UNIT, int NR>
-__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s_tiny_fwd(
+template <typename T, int UNIT, int NR, int G>
+__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR, G>()) k_s_tiny_fwd(
     const Front* __restrict__ fronts, const Item* __restrict__ items, int64_t cnt, const int32_t* __restrict__ reltgt,
     const int32_t* __restrict__ chdtgt, const T* __restrict__ P, T* __restrict__ C, T* __restrict__ R, int64_t n,
     int nrhs) {
     pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     constexpr unsigned kAll = 0xffffffffu;
-    const int g = threadIdx.x & (kTinyNJ - 1), slot = threadIdx.x / kTinyNJ;
-    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * kTinyFronts + slot, cnt);
-    T* Wv = reinterpret_cast<T*>(sm_raw) + slot * kTinyNJ * NR;  // Wv[row * NR + r]
+    const int g = threadIdx.x & (G - 1), slot = threadIdx.x / G;
+    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * tiny_fronts<G>() + slot, cnt);
+    T* Wv = reinterpret_cast<T*>(sm_raw) + slot * G * NR;  // Wv[row * NR + r]
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const T* Pj = P + f.poff;
-    T lr[kTinyNJ];  // row g of the panel
+    T lr[G];  // row g of the panel
 #pragma unroll
-    for (int k = 0; k < kTinyNJ; ++k) lr[k] = (g < nj && k < nn) ? Pj[g + (int64_t)k * ld] : T(0);
+    for (int k = 0; k < G; ++k) lr[k] = (g < nj && k < nn) ? Pj[g + (int64_t)k * ld] : T(0);
 #pragma unroll
     for (int r = 0; r < NR; ++r) Wv[g * NR + r] = (g < nn && r < nrhs) ? C[f.col0 + g + (int64_t)r * n] : T(0);
     __syncwarp();
     // child updates, children in reverse order (one addition per entry and child)
     const int nch = f.chd1 - f.chd0;
-    const int nchw = max(nch, __shfl_xor_sync(kAll, nch, kTinyNJ));
+    const int nchw = tiny_warp_max<G>(nch);
     for (int i = 0; i < nchw; ++i) {
         if (i < nch) {
             const Front fc = fronts[chdtgt[f.chd1 - 1 - i]];
@@ -407,16 +417,16 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s
     T x[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) x[r] = Wv[g * NR + r];
-    const int nnw = max(nn, __shfl_xor_sync(kAll, nn, kTinyNJ));
+    const int nnw = tiny_warp_max<G>(nn);
     // forward substitution: x_k = w_k / L_kk, rows k < a < nn lose L_ak x_k
 #pragma unroll
-    for (int k = 0; k < kTinyNJ; ++k) {
+    for (int k = 0; k < G; ++k) {
         if (k >= nnw) break;  // uniform across the warp
-        const T dk = __shfl_sync(kAll, lr[k], k, kTinyNJ);
+        const T dk = __shfl_sync(kAll, lr[k], k, G);
         const T dinv = UNIT ? T(1) : T(1) / dk;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const T xk = __shfl_sync(kAll, x[r], k, kTinyNJ) * dinv;
+            const T xk = __shfl_sync(kAll, x[r], k, G) * dinv;
             if (k < nn) {
                 if (g > k && g < nn) x[r] -= lr[k] * xk;
                 if (g == k) x[r] = xk;
@@ -432,11 +442,11 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
 #pragma unroll
-    for (int k = 0; k < kTinyNJ; ++k) {
+    for (int k = 0; k < G; ++k) {
         if (k >= nnw) break;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const T xk = __shfl_sync(kAll, x[r], k, kTinyNJ);
+            const T xk = __shfl_sync(kAll, x[r], k, G);
             if (k < nn) acc[r] += lr[k] * xk;
         }
     }
@@ -448,19 +458,19 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s
     }
 }
 
-template <typename T, int UNIT, int NR>
-__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s_tiny_bwd(
+template <typename T, int UNIT, int NR, int G>
+__global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR, G>()) k_s_tiny_bwd(
     const Front* __restrict__ fronts, const Item* __restrict__ items, int64_t cnt, const int32_t* __restrict__ septgt,
     const T* __restrict__ P, T* __restrict__ C, int64_t n, int nrhs) {
     pdl_prologue();
     constexpr unsigned kAll = 0xffffffffu;
-    const int g = threadIdx.x & (kTinyNJ - 1), slot = threadIdx.x / kTinyNJ;
-    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * kTinyFronts + slot, cnt);
+    const int g = threadIdx.x & (G - 1), slot = threadIdx.x / G;
+    const Front f = tiny_front(fronts, items, (int64_t)blockIdx.x * tiny_fronts<G>() + slot, cnt);
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const T* Pj = P + f.poff;
-    T cv[kTinyNJ];  // column g of the panel
+    T cv[G];  // column g of the panel
 #pragma unroll
-    for (int i = 0; i < kTinyNJ; ++i) cv[i] = (g < nn && i < nj) ? Pj[i + (int64_t)g * ld] : T(0);
+    for (int i = 0; i < G; ++i) cv[i] = (g < nn && i < nj) ? Pj[i + (int64_t)g * ld] : T(0);
     T xs[NR];  // lanes nn .. nj - 1: x of the separator rows
     {
         const bool v = g >= nn && g < nj;
@@ -472,13 +482,13 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s
     T acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
-    const int njw = max(nj, __shfl_xor_sync(kAll, nj, kTinyNJ));
+    const int njw = tiny_warp_max<G>(nj);
 #pragma unroll
-    for (int i = 0; i < kTinyNJ; ++i) {
+    for (int i = 0; i < G; ++i) {
         if (i >= njw) break;  // uniform across the warp
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const T xb = __shfl_sync(kAll, xs[r], i, kTinyNJ);
+            const T xb = __shfl_sync(kAll, xs[r], i, G);
             if (i >= nn && i < nj) acc[r] += cv[i] * xb;
         }
     }
@@ -487,15 +497,15 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR>()) k_s
     for (int r = 0; r < NR; ++r) c[r] = (g < nn && r < nrhs) ? C[f.col0 + g + (int64_t)r * n] - acc[r] : T(0);
     // back substitution on L^T: x_k = c_k / L_kk, k descending; columns
     // j < k lose L_kj x_k
-    const int nnw = max(nn, __shfl_xor_sync(kAll, nn, kTinyNJ));
+    const int nnw = tiny_warp_max<G>(nn);
 #pragma unroll
-    for (int k = kTinyNJ - 1; k >= 0; --k) {
+    for (int k = G - 1; k >= 0; --k) {
         if (k >= nnw) continue;  // uniform across the warp
-        const T dk = __shfl_sync(kAll, cv[k], k, kTinyNJ);
+        const T dk = __shfl_sync(kAll, cv[k], k, G);
         const T dinv = UNIT ? T(1) : T(1) / dk;
 #pragma unroll
         for (int r = 0; r < NR; ++r) {
-            const T xk = __shfl_sync(kAll, c[r], k, kTinyNJ) * dinv;
+            const T xk = __shfl_sync(kAll, c[r], k, G) * dinv;
             if (k < nn) {
                 if (g < k) c[r] -= cv[k] * xk;
                 if (g == k) c[r] = xk;
@@ -658,13 +668,25 @@ constexpr int kDiagSplit = kSolveNB / 16;
 
 // W and C go through L2 only (ld/st .cg): within one k_s_chain launch other
 // CTAs write them, and L1 is not coherent across SMs.
-template <typename T, int NR, int BWD>
+// Each step function issues the loads that depend on nothing computed in
+// this solve (the panel, the inverse) first, then calls wait() -- a no-op in
+// the per-step kernels, the chain's bounded waits in k_s_chain; a false
+// return (a timed-out wait, uniform across the CTA) skips the rest.
+struct NoWait {
+    __device__ bool operator()() const { return true; }
+};
+
+template <typename T, int NR, int BWD, typename Wait = NoWait>
 __device__ __forceinline__ void sdiag_run(const Front& f, int step, int q, const T* __restrict__ inv2, T* C,
-                                          const T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
+                                          const T* W, int64_t n, int nrhs, unsigned char* sm_raw,
+                                          Wait wait = Wait()) {
     T* b = reinterpret_cast<T*>(sm_raw);  // [r][c] : b[c + r * kSolveNB]
     T* xt = b + kSolveNB * NR;            // forward: xt[c * 16 + a - 16q]; backward: xt[(a - 16q) * 256 + c]
     const int k0 = step * kSolveNB, wK = min(kSolveNB, f.nn - k0), ld2 = super_ld(wK);
-    if (16 * q >= wK) return;  // whole CTA
+    if (16 * q >= wK) {  // whole CTA: nothing to compute, the wait still taken
+        wait();
+        return;
+    }
     const T* X = inv2 + f.i2off + (int64_t)step * kSolveNB * kSolveNB;
     // 16-byte copies (X's columns and ld2 are multiples of 4 elements, so
     // every copy is aligned and stays inside the ld2 x wK block); entries
@@ -684,6 +706,10 @@ __device__ __forceinline__ void sdiag_run(const Front& f, int step, int q, const
             const bool v = a < wK && c0 < ld2;
             cpa16(xt + al * kSolveNB + c0, v ? X + c0 + (int64_t)a * ld2 : X, v);
         }
+    }
+    if (!wait()) {
+        cpa_wait_all();
+        return;
     }
     for (int i = threadIdx.x; i < kSolveNB * NR; i += blockDim.x) {
         const int c = i % kSolveNB, r = i / kSolveNB;
@@ -755,9 +781,9 @@ template <> struct Vec16<double> {
 template <typename T, int NR>
 constexpr int ftile_smem() { return (kSolveNB * NR + 8 * NR * kFwdRows) * (int)sizeof(T); }
 
-template <typename T, int NR>
+template <typename T, int NR, typename Wait = NoWait>
 __device__ __forceinline__ void ftile_run(const Front& f, int step, int ta, const T* __restrict__ P, const T* C,
-                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
+                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw, Wait wait = Wait()) {
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;             // rows per load
@@ -770,33 +796,43 @@ __device__ __forceinline__ void ftile_run(const Front& f, int step, int ta, cons
     const int rlo = k0 + wK;
     const int ra = (rlo & ~3) + ta * kFwdRows;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < kSolveNB * NR; i += 256) {
-        const int c = i & (kSolveNB - 1), r = i / kSolveNB;
-        xs[c * NR + r] = (c < wK && r < nrhs) ? __ldcg(C + f.col0 + k0 + c + (int64_t)r * n) : T(0);
-    }
-    __syncthreads();
     const int rr = (lane % LPC) * VW, ch = lane / LPC;
     // row is a multiple of 4 below nj, so the 16-byte load ends inside the
     // column's ldp (a multiple of 4) rows
     const int row = ra + rr;
     const int cb = warp * 32;
     const int cn = min(32, wK - cb);
+    const bool act = row < nj && cn > 0;
+    const T* pc = P + f.poff + (int64_t)(k0 + cb) * ld + row;
+    // the first batch of panel loads (all of a lane's for FP32) before x_K
+    V lb[kColBatch];
+    if (act)
+#pragma unroll
+        for (int u = 0; u < kColBatch; ++u) {
+            const int c = ch + u * CPL;
+            if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+        }
+    if (!wait()) return;
+    for (int i = tid; i < kSolveNB * NR; i += 256) {
+        const int c = i & (kSolveNB - 1), r = i / kSolveNB;
+        xs[c * NR + r] = (c < wK && r < nrhs) ? __ldcg(C + f.col0 + k0 + c + (int64_t)r * n) : T(0);
+    }
+    __syncthreads();
     T acc[VW][NR];
 #pragma unroll
     for (int e = 0; e < VW; ++e)
 #pragma unroll
         for (int r = 0; r < NR; ++r) acc[e][r] = T(0);
-    if (row < nj && cn > 0) {
-        const T* pc = P + f.poff + (int64_t)(k0 + cb) * ld + row;
+    if (act) {
         // all of a batch's loads are issued before its products (one
         // memory round trip per 16 columns of a lane, in column order)
         for (int cb0 = ch; cb0 < cn; cb0 += kColBatch * CPL) {
-            V lb[kColBatch];
+            if (cb0 != ch)
 #pragma unroll
-            for (int u = 0; u < kColBatch; ++u) {
-                const int c = cb0 + u * CPL;
-                if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
-            }
+                for (int u = 0; u < kColBatch; ++u) {
+                    const int c = cb0 + u * CPL;
+                    if (c < cn) lb[u] = *reinterpret_cast<const V*>(pc + (int64_t)c * ld);
+                }
 #pragma unroll
             for (int u = 0; u < kColBatch; ++u) {
                 const int c = cb0 + u * CPL;
@@ -976,9 +1012,9 @@ __global__ void __launch_bounds__(256) k_s_fwd_red(const Front* __restrict__ fro
 template <typename T, int NR>
 constexpr int btile_smem() { return (kSolveNB * NR + 4 * NR * kNB) * (int)sizeof(T); }
 
-template <typename T, int NR>
+template <typename T, int NR, typename Wait = NoWait>
 __device__ __forceinline__ void btile_run(const Front& f, int step, int ta, const T* __restrict__ P, const T* C,
-                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw) {
+                                          T* W, int64_t n, int nrhs, unsigned char* sm_raw, Wait wait = Wait()) {
     using VT = Vec16<T>;
     using V = typename VT::type;
     constexpr int VW = VT::W;
@@ -988,26 +1024,34 @@ __device__ __forceinline__ void btile_run(const Front& f, int step, int ta, cons
     const int k0 = step * kSolveNB, wK = min(kSolveNB, nn - k0);
     const int c0 = ta * kNB, wc = min(kNB, k0 - c0);
     const int tid = threadIdx.x;
+    const int c = tid & (kNB - 1), q = tid >> 6;
+    const int i0 = q * 64, ni = min(64, wK - i0);  // rows of this quarter inside the block
+    const bool act = c < wc && ni > 0;
+    // k0 + i0 + i is a multiple of 4 below nn <= nj, so each 16-byte load
+    // ends inside the column's ldp rows; rows past the block are dropped by
+    // the select below.  The first batch (all of a thread's for FP32) is
+    // issued before x_K.
+    const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + k0 + i0;
+    V l[kColBatch];
+    if (act)
+#pragma unroll
+        for (int u = 0; u < kColBatch; ++u)
+            if (u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + u * VW);
+    if (!wait()) return;
     for (int i = tid; i < kSolveNB * NR; i += 256) {
         const int a = i & (kSolveNB - 1), r = i / kSolveNB;
         xs[a * NR + r] = (a < wK && r < nrhs) ? __ldcg(C + f.col0 + k0 + a + (int64_t)r * n) : T(0);
     }
     __syncthreads();
-    const int c = tid & (kNB - 1), q = tid >> 6;
-    const int i0 = q * 64, ni = min(64, wK - i0);  // rows of this quarter inside the block
     T acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = T(0);
-    if (c < wc && ni > 0) {
-        // k0 + i0 + i is a multiple of 4 below nn <= nj, so each 16-byte
-        // load ends inside the column's ldp rows; rows past the block are
-        // dropped by the select below
-        const T* pc = P + f.poff + (int64_t)(c0 + c) * ld + k0 + i0;
+    if (act) {
         for (int i = 0; i < 64; i += kColBatch * VW) {
-            V l[kColBatch];
+            if (i != 0)
 #pragma unroll
-            for (int u = 0; u < kColBatch; ++u)
-                if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
+                for (int u = 0; u < kColBatch; ++u)
+                    if (i + u * VW < ni) l[u] = *reinterpret_cast<const V*>(pc + i + u * VW);
 #pragma unroll
             for (int u = 0; u < kColBatch; ++u) {
                 const int ib = i + u * VW;
@@ -1130,29 +1174,36 @@ __global__ void __launch_bounds__(256) k_s_chain(const Front* __restrict__ front
         const int done = BWD ? S - 1 - K : K;  // steps applied before step K
         int* xdone = ctl + it.pad;
         int* tiles = xdone + 1;
+        // the waits run inside the step functions, after the loads of the
+        // panel or the inverse (which depend on nothing in this solve)
         if (it.a < 0) {
             const int g0 = K * (kSolveNB / kNB);
             const int ng = min(kSolveNB / kNB, (f.nn - K * kSolveNB + kNB - 1) / kNB);
-            if (threadIdx.x < ng) {
-                if (!chain_wait(tiles + g0 + threadIdx.x, done, err)) s_ok = 0;
-                __threadfence();
-            }
-            __syncthreads();
-            if (s_ok) sdiag_run<T, NR, BWD>(f, K, -1 - it.a, inv2, C, W, n, nrhs, sm_raw);
+            auto wait = [&]() -> bool {
+                if (threadIdx.x < ng) {
+                    if (!chain_wait(tiles + g0 + threadIdx.x, done, err)) s_ok = 0;
+                    __threadfence();
+                }
+                __syncthreads();
+                return s_ok != 0;
+            };
+            sdiag_run<T, NR, BWD>(f, K, -1 - it.a, inv2, C, W, n, nrhs, sm_raw, wait);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0 && s_ok) atomicAdd(xdone, 1);
         } else {
             const int g = BWD ? it.a : ((K + 1) * kSolveNB) / kNB + it.a;
-            if (threadIdx.x == 0) {
-                if (!chain_wait(xdone, kDiagSplit * (done + 1), err) || !chain_wait(tiles + g, done, err)) s_ok = 0;
-                __threadfence();
-            }
-            __syncthreads();
-            if (s_ok) {
-                if (BWD) btile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw);
-                else ftile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw);
-            }
+            auto wait = [&]() -> bool {
+                if (threadIdx.x == 0) {
+                    if (!chain_wait(xdone, kDiagSplit * (done + 1), err) || !chain_wait(tiles + g, done, err))
+                        s_ok = 0;
+                    __threadfence();
+                }
+                __syncthreads();
+                return s_ok != 0;
+            };
+            if (BWD) btile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw, wait);
+            else ftile_run<T, NR>(f, K, it.a, P, C, W, n, nrhs, sm_raw, wait);
             __threadfence();
             __syncthreads();
             if (threadIdx.x == 0 && s_ok) atomicAdd(tiles + g, 1);
@@ -1553,19 +1604,19 @@ static int launch_mid(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int
 
 // the tiny fronts of a level: k_s_tiny_* (16 lanes per front), or the
 // warp-per-front k_s_small_* when switched off
-template <typename T, int UNIT, int NR, int BWD>
+template <typename T, int UNIT, int NR, int BWD, int G>
 static int tiny_go(mf_handle* h, const ItemList& il, const SolveBufs<T>& sb, int nrhs) {
     const Item* it = h->d_items + il.off;
     const int64_t c = il.cnt;
     if (h->tiny_solve) {
-        const unsigned g = (unsigned)((c + kTinyFronts - 1) / kTinyFronts);
-        constexpr int sm = kTinyFronts * kTinyNJ * NR * (int)sizeof(T);
+        const unsigned g = (unsigned)((c + tiny_fronts<G>() - 1) / tiny_fronts<G>());
+        constexpr int sm = tiny_fronts<G>() * G * NR * (int)sizeof(T);
         if (!BWD)
-            launch_k(k_s_tiny_fwd<T, UNIT, NR>, g, kTinyWarps * 32, sm, h->stream, h->d_fronts, it, c, h->d_reltgt,
-                     h->d_chdtgt, sb.P, sb.C, sb.R, h->n, nrhs);
+            launch_k(k_s_tiny_fwd<T, UNIT, NR, G>, g, kTinyWarps * 32, sm, h->stream, h->d_fronts, it, c,
+                     h->d_reltgt, h->d_chdtgt, sb.P, sb.C, sb.R, h->n, nrhs);
         else
-            launch_k(k_s_tiny_bwd<T, UNIT, NR>, g, kTinyWarps * 32, 0, h->stream, h->d_fronts, it, c, h->d_septgt,
-                     sb.P, sb.C, h->n, nrhs);
+            launch_k(k_s_tiny_bwd<T, UNIT, NR, G>, g, kTinyWarps * 32, 0, h->stream, h->d_fronts, it, c,
+                     h->d_septgt, sb.P, sb.C, h->n, nrhs);
     } else {
         const unsigned g = (unsigned)((c + kSmallWarps - 1) / kSmallWarps);
         if (!BWD)
@@ -1579,15 +1630,15 @@ static int tiny_go(mf_handle* h, const ItemList& il, const SolveBufs<T>& sb, int
     return 0;
 }
 
-template <typename T, int UNIT, int BWD>
+template <typename T, int UNIT, int BWD, int G>
 static int launch_tiny(mf_handle* h, const ItemList& il, const SolveBufs<T>& sb, int nrb, int nrhs) {
     Timer t(h, K_S_SMALL);
     switch (nrb) {
-        case 1: return tiny_go<T, UNIT, 1, BWD>(h, il, sb, nrhs);
-        case 2: return tiny_go<T, UNIT, 2, BWD>(h, il, sb, nrhs);
-        case 4: return tiny_go<T, UNIT, 4, BWD>(h, il, sb, nrhs);
-        case 8: return tiny_go<T, UNIT, 8, BWD>(h, il, sb, nrhs);
-        default: return tiny_go<T, UNIT, 16, BWD>(h, il, sb, nrhs);
+        case 1: return tiny_go<T, UNIT, 1, BWD, G>(h, il, sb, nrhs);
+        case 2: return tiny_go<T, UNIT, 2, BWD, G>(h, il, sb, nrhs);
+        case 4: return tiny_go<T, UNIT, 4, BWD, G>(h, il, sb, nrhs);
+        case 8: return tiny_go<T, UNIT, 8, BWD, G>(h, il, sb, nrhs);
+        default: return tiny_go<T, UNIT, 16, BWD, G>(h, il, sb, nrhs);
     }
 }
 
@@ -1655,7 +1706,9 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
     // forward: levels ascending
     for (const Level& lv : h->levels) {
         if (lv.s_tiny.cnt)
-            if (int rc = launch_tiny<T, UNIT, 0>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
+            if (int rc = launch_tiny<T, UNIT, 0, kTinyNJ>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
+        if (lv.s_tiny2.cnt)
+            if (int rc = launch_tiny<T, UNIT, 0, kTinyNJ2>(h, lv.s_tiny2, sb, nrb, nrhs)) return rc;
         if (lv.s_small.cnt) {
             Timer t(h, K_S_SMALL);
             const unsigned g = (unsigned)((lv.s_small.cnt + kSmallWarps - 1) / kSmallWarps);
@@ -1817,7 +1870,9 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             MF_CUDA(cudaGetLastError());
         }
         if (lv.s_tiny.cnt)
-            if (int rc = launch_tiny<T, UNIT, 1>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
+            if (int rc = launch_tiny<T, UNIT, 1, kTinyNJ>(h, lv.s_tiny, sb, nrb, nrhs)) return rc;
+        if (lv.s_tiny2.cnt)
+            if (int rc = launch_tiny<T, UNIT, 1, kTinyNJ2>(h, lv.s_tiny2, sb, nrb, nrhs)) return rc;
     }
     if (h->sub_tasks.cnt) {
         // the subtrees of small fronts, backward, in one launch
