@@ -249,7 +249,8 @@ __device__ void small_front_store(const TC* F, const Front& f, T* __restrict__ P
 // larger front -- is reported through info.
 constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
 constexpr int kSmallNarrowNJ = 48;     // levels whose small fronts all have nj <= this ...
-constexpr int kSmallWideLevel = 4 * 148;  // ... and that hold at least this many run 128-thread CTAs
+constexpr int kSmallWideLevel = 4 * 148;  // ... and that hold at least this many run 128-thread CTAs,
+constexpr int kSmallTinyNJ = 32;       // 64-thread CTAs when nj <= this
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -679,6 +680,7 @@ template <typename TC>
 __device__ __forceinline__ void diag_inv_offdiag(const TC* A, TC* X) {
     const int tid = threadIdx.x;
     using T = TC;
+#pragma unroll 1
     for (int dist = 1; dist < 4; ++dist) {
         const int nb = 4 - dist;
         T tmp[3];
@@ -738,7 +740,9 @@ __device__ int diag_block_la(TC* A, TC* X, TC* pivs, TC* rinv, int w, const doub
     using T = TC;
     if (tid == 0) *bad_s = -1;
     __syncthreads();
-#pragma unroll
+    // the panel loop stays rolled: its body runs once per panel and block,
+    // and four unrolled copies made the kernel wait on instruction fetches
+#pragma unroll 1
     for (int p = 0; p < 4; ++p) {
         const int pb = p * 16;
         if (warp == 0) {
@@ -816,6 +820,7 @@ __device__ int diag_block_seq(TC* A, TC* X, TC* pivs, TC* rinv, int w, const dou
     using T = TC;
     if (tid == 0) *bad_s = -1;
     __syncthreads();
+#pragma unroll 1
     for (int p = 0; p < 4; ++p) {
         const int pb = p * 16;
         if (warp == 0) {
@@ -1515,7 +1520,8 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             const int mj = lv.small_maxnj;
             const int rj = std::min(mj, kSmallRescue);
             const size_t sm = std::max<size_t>((size_t)mj * mj * sizeof(T), sizeof(T) == 4 ? (size_t)rj * rj * 8 : 0);
-            const unsigned nt = (mj <= kSmallNarrowNJ && lv.small.cnt >= kSmallWideLevel) ? 128 : 256;
+            const bool wide = lv.small.cnt >= kSmallWideLevel;
+            const unsigned nt = !wide || mj > kSmallNarrowNJ ? 256 : mj <= kSmallTinyNJ ? 64 : 128;
             launch_k(k_small<T, LDLT>, grid_for(lv.small.cnt), nt, sm, h->stream, 
                 h->d_fronts, items + lv.small.off, h->d_reltgt, h->d_chdtgt, fb.P, fb.M, fb.d, h->d_signs,
                 h->d_info, h->d_rescued, reg);
