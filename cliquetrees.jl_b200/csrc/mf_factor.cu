@@ -148,6 +148,7 @@ __global__ void k_panel32_to_dl(const Front* __restrict__ fronts, const RefFront
 // (or 64 x 64 diagonal block), which is then factored again in FP64.
 constexpr double kRescueSmall = 1e-5;
 constexpr double kRescueGrowth = 1e7;
+constexpr int kSmallKids = 32;  // children whose records k_small fetches up front
 
 // One small front held in shared memory as TC: load the assembled panel, add
 // the children (in the reference's reverse order), factor the first nn
@@ -162,6 +163,19 @@ __device__ int small_front(TC* F, const Front& f, const Front* __restrict__ fron
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const int tid = threadIdx.x, nt = blockDim.x;
     const T* Pj = P + f.poff;
+    // the children's records (first kSmallKids, in the order they are added),
+    // fetched at once beside the panel load instead of one dependent pair of
+    // loads per child
+    __shared__ int kid_na[kSmallKids], kid_lm[kSmallKids], kid_sep0[kSmallKids];
+    __shared__ int64_t kid_moff[kSmallKids];
+    const int nch = f.chd1 - f.chd0;
+    for (int q = tid; q < min(nch, kSmallKids); q += nt) {
+        const Front fc = fronts[chdtgt[f.chd1 - 1 - q]];
+        kid_na[q] = fc.na;
+        kid_lm[q] = fc.ldm;
+        kid_sep0[q] = fc.sep0;
+        kid_moff[q] = fc.moff;
+    }
     for (int i = tid; i < nj * nn; i += nt) {
         int r = i % nj, c = i / nj;
         F[i] = (TC)Pj[r + (int64_t)c * ld];
@@ -169,19 +183,34 @@ __device__ int small_front(TC* F, const Front& f, const Front* __restrict__ fron
     for (int i = tid; i < nj * na; i += nt) F[nj * nn + i] = TC(0);
     __syncthreads();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
-    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
-        const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na, lm = fc.ldm;
-        const int32_t* rel = reltgt + fc.sep0;
-        const T* Mc = M + fc.moff;
+    for (int q = 0; q < nch; ++q) {
+        int ma, lm, sep0;
+        int64_t moff;
+        if (q < kSmallKids) {
+            ma = kid_na[q], lm = kid_lm[q], sep0 = kid_sep0[q], moff = kid_moff[q];
+        } else {
+            const Front fc = fronts[chdtgt[f.chd1 - 1 - q]];
+            ma = fc.na, lm = fc.ldm, sep0 = fc.sep0, moff = fc.moff;
+        }
+        const int32_t* rel = reltgt + sep0;
+        const T* Mc = M + moff;
         for (int i = tid; i < ma * ma; i += nt) {
             int a = i % ma, b = i / ma;
             if (a >= b) F[rel[a] + rel[b] * nj] += (TC)Mc[a + b * lm];
         }
         __syncthreads();
     }
-    // right-looking partial factorization of the first nn columns
+    // right-looking partial factorization of the first nn columns, one
+    // block barrier per column: step k reads column k unscaled and scales
+    // its entries on the fly (the same rounded products the stored scaled
+    // column holds), and column k is written back scaled -- with its
+    // diagonal entry -- during step k + 1, which touches only columns > k
+    TC pk = TC(0), ik = TC(0);  // the previous column's stored diagonal and reciprocal
     for (int k = 0; k < nn; ++k) {
+        if (k > 0) {
+            if (tid == 0) F[(k - 1) + (k - 1) * nj] = pk;
+            for (int i = k + tid; i < nj; i += nt) F[i + (k - 1) * nj] *= ik;
+        }
         TC piv = F[k + k * nj];
         double s = pivot_sign(signs, LDLT, f.col0 + k);
         if (reg.delta >= 0.0) {
@@ -198,19 +227,23 @@ __device__ int small_front(TC* F, const Front& f, const Front* __restrict__ fron
         }
         TC dk = LDLT ? piv : sqrt(piv);
         TC inv = TC(1) / dk;
-        __syncthreads();
-        if (tid == 0) F[k + k * nj] = LDLT ? piv : dk;
-        for (int i = k + 1 + tid; i < nj; i += nt) F[i + k * nj] *= inv;
-        __syncthreads();
         const int m = nj - k - 1;
         for (int i = tid; i < m * m; i += nt) {
             int r = k + 1 + i % m, c = k + 1 + i / m;
             if (r >= c) {
-                TC lc = F[c + k * nj];
+                TC lc = F[c + k * nj] * inv;
                 if (LDLT) lc *= piv;
-                F[r + c * nj] -= F[r + k * nj] * lc;
+                const TC lr = F[r + k * nj] * inv;
+                F[r + c * nj] -= lr * lc;
             }
         }
+        pk = LDLT ? piv : dk;
+        ik = inv;
+        __syncthreads();
+    }
+    if (nn > 0) {
+        if (tid == 0) F[(nn - 1) + (nn - 1) * nj] = pk;
+        for (int i = nn + tid; i < nj; i += nt) F[i + (nn - 1) * nj] *= ik;
         __syncthreads();
     }
     return -1;
@@ -310,6 +343,15 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
     const int nn = f.nn, na = f.na, nj = nn + na, ld = f.ldp;
     const T* Pj = P + f.poff;
     const bool row = lane < nj;
+    // lane q fetches the record of the q-th child to add (children past 32
+    // are read in the loop), beside the panel loads
+    const int nch = f.chd1 - f.chd0;
+    int kna = 0, klm = 0, ksep = 0;
+    int64_t kmoff = 0;
+    if (lane < nch) {
+        const Front fc = fronts[chdtgt[f.chd1 - 1 - lane]];
+        kna = fc.na, klm = fc.ldm, ksep = fc.sep0, kmoff = fc.moff;
+    }
     {
         // every panel load of the lane in flight at once, then the stores
         T v[ROWS];
@@ -321,11 +363,16 @@ __device__ int warp_front(TC* F, const Front& f, const Front* __restrict__ front
     }
     __syncwarp();
     // extend-add, children popped in reverse (cholesky.jl:506-514)
-    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
-        const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na, lm = fc.ldm;
-        const int32_t* rel = reltgt + fc.sep0;
-        const T* Mc = M + fc.moff;
+    for (int q = 0; q < nch; ++q) {
+        int ma = __shfl_sync(0xffffffffu, kna, q & 31), lm = __shfl_sync(0xffffffffu, klm, q & 31);
+        int sep0 = __shfl_sync(0xffffffffu, ksep, q & 31);
+        int64_t moff = __shfl_sync(0xffffffffu, kmoff, q & 31);
+        if (q >= 32) {
+            const Front fc = fronts[chdtgt[f.chd1 - 1 - q]];
+            ma = fc.na, lm = fc.ldm, sep0 = fc.sep0, moff = fc.moff;
+        }
+        const int32_t* rel = reltgt + sep0;
+        const T* Mc = M + moff;
         const int ra = lane < ma ? rel[lane] : 0;
         T mv[ROWS];
 #pragma unroll

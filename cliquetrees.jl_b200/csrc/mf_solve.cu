@@ -102,13 +102,26 @@ __device__ __forceinline__ void small_fwd_front(const Front& f, const Front* __r
         C1[a + r * kSmallMax] = C[f.col0 + a + (int64_t)r * n];
     }
     for (int i = lane; i < na * nrhs; i += 32) Rj[i] = T(0);
+    // lane q fetches the record of the q-th child to add (children past 32
+    // are read in the loop)
+    const int nch = f.chd1 - f.chd0;
+    int kna = 0, ksep = 0;
+    int64_t kroff = 0;
+    if (lane < nch) {
+        const Front fc = fronts[chdtgt[f.chd1 - 1 - lane]];
+        kna = fc.na, ksep = fc.sep0, kroff = fc.roff;
+    }
     __syncwarp();
     // child updates, children in reverse order (the reference pops its stack)
-    for (int p = f.chd1 - 1; p >= f.chd0; --p) {
-        const Front fc = fronts[chdtgt[p]];
-        const int ma = fc.na;
-        const int32_t* rel = reltgt + fc.sep0;
-        const T* Mc = R + fc.roff * nrhs;
+    for (int q = 0; q < nch; ++q) {
+        int ma = __shfl_sync(0xffffffffu, kna, q & 31), sep0 = __shfl_sync(0xffffffffu, ksep, q & 31);
+        int64_t roff = __shfl_sync(0xffffffffu, kroff, q & 31);
+        if (q >= 32) {
+            const Front fc = fronts[chdtgt[f.chd1 - 1 - q]];
+            ma = fc.na, sep0 = fc.sep0, roff = fc.roff;
+        }
+        const int32_t* rel = reltgt + sep0;
+        const T* Mc = R + roff * nrhs;
         // four loads per lane in flight before the adds (the child's rows
         // are distinct, so one child's adds never collide)
         for (int i0 = 0; i0 < ma * nrhs; i0 += 128) {
@@ -397,16 +410,30 @@ __global__ void __launch_bounds__(kTinyWarps * 32, tiny_min_blocks<T, NR, G>()) 
 #pragma unroll
     for (int r = 0; r < NR; ++r) Wv[g * NR + r] = (g < nn && r < nrhs) ? C[f.col0 + g + (int64_t)r * n] : T(0);
     __syncwarp();
-    // child updates, children in reverse order (one addition per entry and child)
+    // child updates, children in reverse order (one addition per entry and
+    // child); lane g fetches child g's record up front (children past G
+    // are read in the loop)
     const int nch = f.chd1 - f.chd0;
     const int nchw = tiny_warp_max<G>(nch);
+    int kna = 0, ksep = 0;
+    int64_t kroff = 0;
+    if (g < nch) {
+        const Front fc = fronts[chdtgt[f.chd1 - 1 - g]];
+        kna = fc.na, ksep = fc.sep0, kroff = fc.roff;
+    }
     for (int i = 0; i < nchw; ++i) {
+        const int src = (threadIdx.x & ~(G - 1) & 31) + (i & (G - 1));
+        int ma = __shfl_sync(kAll, kna, src);
+        int sep0 = __shfl_sync(kAll, ksep, src);
+        int64_t roff = __shfl_sync(kAll, kroff, src);
         if (i < nch) {
-            const Front fc = fronts[chdtgt[f.chd1 - 1 - i]];
-            const int ma = fc.na;
+            if (i >= G) {
+                const Front fc = fronts[chdtgt[f.chd1 - 1 - i]];
+                ma = fc.na, sep0 = fc.sep0, roff = fc.roff;
+            }
             if (g < ma) {
-                const int q = reltgt[fc.sep0 + g];
-                const T* Mc = R + fc.roff * nrhs + g;
+                const int q = reltgt[sep0 + g];
+                const T* Mc = R + roff * nrhs + g;
 #pragma unroll
                 for (int r = 0; r < NR; ++r)
                     if (r < nrhs) Wv[q * NR + r] += Mc[r * ma];
