@@ -211,6 +211,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         h->tc_split = !(senv && senv[0] == '0');
         const char* cenv = getenv("MF_SOLVE_CHAIN");
         h->solve_chain = !cenv ? 2 : cenv[0] == '1' ? 1 : cenv[0] == '0' ? 0 : 2;
+        const char* penv = getenv("MF_STEP_PDL");
+        h->step_pdl = !(penv && penv[0] == '0');
         const char* tenv = getenv("MF_TINY_SOLVE");
         h->tiny_solve = !(tenv && tenv[0] == '0');
         // the cluster-per-front level kernels measured slower than the

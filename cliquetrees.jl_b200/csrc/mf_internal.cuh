@@ -310,6 +310,7 @@ struct mf_handle {
     int solve_chain = 2;           // k_s_chain launches: 1 every level (MF_SOLVE_CHAIN=1), 0 none (=0),
                                    // 2 the levels of at least kChainMinSteps steps (default)
     bool tiny_solve = true;        // k_s_tiny_* for the fronts with nj <= kTinyNJ (MF_TINY_SOLVE=0: k_s_small_*)
+    bool step_pdl = true;          // solve-step kernels launched for programmatic dependence (MF_STEP_PDL=0: off)
     bool mid_solve = false;        // one cluster launch per single-super-block level and direction (MF_MID_SOLVE=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
     double* d_B = nullptr;         // rhs in original order (n * nrhs_cap)
@@ -408,9 +409,10 @@ inline bool pdl_enabled() {
     return on;
 }
 
+// the launch itself: with the attribute when `pdl`
 template <typename... KArgs, typename... Args>
-inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                            Args&&... args) {
+inline cudaError_t launch_kx(bool pdl, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                             cudaStream_t st, Args&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
@@ -420,9 +422,24 @@ inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cfg.numAttrs = pdl ? 1 : 0;
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                            Args&&... args) {
+    return launch_kx(pdl_enabled(), kern, grid, block, smem, st, std::forward<Args>(args)...);
+}
+
+// The blocked solve-step kernels (k_s_sdiag, k_s_ftile, k_s_btile) let the
+// next grid launch at once and wait for the previous one only after they
+// have issued their loads of the panel or the inverse, which no kernel of
+// the solve writes; they are launched with the attribute unless
+// MF_STEP_PDL=0, so each step's launch and those loads overlap the step
+// before it.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 
 #define MF_CUDA(call)                                                  \
     do {                                                               \

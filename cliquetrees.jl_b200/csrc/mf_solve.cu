@@ -702,6 +702,14 @@ constexpr int kDiagSplit = kSolveNB / 16;
 struct NoWait {
     __device__ bool operator()() const { return true; }
 };
+// the per-step kernels: wait for the previous grid of the stream (launched
+// for programmatic dependence; a no-op otherwise)
+struct PdlWait {
+    __device__ bool operator()() const {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        return true;
+    }
+};
 
 template <typename T, int NR, int BWD, typename Wait = NoWait>
 __device__ __forceinline__ void sdiag_run(const Front& f, int step, int q, const T* __restrict__ inv2, T* C,
@@ -773,10 +781,10 @@ template <typename T, int NR, int BWD>
 __global__ void __launch_bounds__(256) k_s_sdiag(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ inv2, T* __restrict__ C,
                                                  const T* __restrict__ W, int64_t n, int nrhs) {
-    pdl_prologue();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Front f = fronts[items[blockIdx.x / kDiagSplit].front];
-    sdiag_run<T, NR, BWD>(f, step, (int)(blockIdx.x % kDiagSplit), inv2, C, W, n, nrhs, sm_raw);
+    sdiag_run<T, NR, BWD>(f, step, (int)(blockIdx.x % kDiagSplit), inv2, C, W, n, nrhs, sm_raw, PdlWait());
 }
 
 constexpr int kColBatch = 16;  // 16-byte panel loads a lane issues before using them (step tiles: few CTAs)
@@ -907,11 +915,11 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_ftile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
-    pdl_prologue();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    ftile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw);
+    ftile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw, PdlWait());
 }
 
 // forward R_j -= L21 x1 for the blocked fronts of a level, once all their
@@ -1112,11 +1120,11 @@ template <typename T, int NR>
 __global__ void __launch_bounds__(256) k_s_btile(const Front* __restrict__ fronts, const Item* __restrict__ items,
                                                  int step, const T* __restrict__ P, const T* __restrict__ C,
                                                  T* __restrict__ W, int64_t n, int nrhs) {
-    pdl_prologue();
+    pdl_trigger();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item it = items[blockIdx.x];
     const Front f = fronts[it.front];
-    btile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw);
+    btile_run<T, NR>(f, step, it.a, P, C, W, n, nrhs, sm_raw, PdlWait());
 }
 
 // ---------------------------------------------------------------------------
@@ -1779,22 +1787,22 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const unsigned gd = (unsigned)st.diag.cnt;
             const Item* itd = items + st.diag.off;
             switch (nrb) {
-                case 1: launch_k(k_s_sdiag<T, 1, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 2: launch_k(k_s_sdiag<T, 2, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 4: launch_k(k_s_sdiag<T, 4, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 8: launch_k(k_s_sdiag<T, 8, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                default: launch_k(k_s_sdiag<T, 16, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 1: launch_kx(h->step_pdl, k_s_sdiag<T, 1, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: launch_kx(h->step_pdl, k_s_sdiag<T, 2, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: launch_kx(h->step_pdl, k_s_sdiag<T, 4, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: launch_kx(h->step_pdl, k_s_sdiag<T, 8, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: launch_kx(h->step_pdl, k_s_sdiag<T, 16, 0>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
             if (st.fwd.cnt) {
                 const unsigned gf = (unsigned)st.fwd.cnt;
                 const Item* itf = items + st.fwd.off;
                 switch (nrb) {
-                    case 1: launch_k(k_s_ftile<T, 1>, gf, 256, ftile_smem<T, 1>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 2: launch_k(k_s_ftile<T, 2>, gf, 256, ftile_smem<T, 2>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 4: launch_k(k_s_ftile<T, 4>, gf, 256, ftile_smem<T, 4>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 8: launch_k(k_s_ftile<T, 8>, gf, 256, ftile_smem<T, 8>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    default: launch_k(k_s_ftile<T, 16>, gf, 256, ftile_smem<T, 16>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 1: launch_kx(h->step_pdl, k_s_ftile<T, 1>, gf, 256, ftile_smem<T, 1>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: launch_kx(h->step_pdl, k_s_ftile<T, 2>, gf, 256, ftile_smem<T, 2>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: launch_kx(h->step_pdl, k_s_ftile<T, 4>, gf, 256, ftile_smem<T, 4>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: launch_kx(h->step_pdl, k_s_ftile<T, 8>, gf, 256, ftile_smem<T, 8>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: launch_kx(h->step_pdl, k_s_ftile<T, 16>, gf, 256, ftile_smem<T, 16>(), h->stream, h->d_fronts, itf, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
                 }
                 MF_CUDA(cudaGetLastError());
             }
@@ -1857,22 +1865,22 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
             const unsigned gd = (unsigned)st.diag.cnt;
             const Item* itd = items + st.diag.off;
             switch (nrb) {
-                case 1: launch_k(k_s_sdiag<T, 1, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 2: launch_k(k_s_sdiag<T, 2, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 4: launch_k(k_s_sdiag<T, 4, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                case 8: launch_k(k_s_sdiag<T, 8, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
-                default: launch_k(k_s_sdiag<T, 16, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 1: launch_kx(h->step_pdl, k_s_sdiag<T, 1, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 1>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 2: launch_kx(h->step_pdl, k_s_sdiag<T, 2, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 2>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 4: launch_kx(h->step_pdl, k_s_sdiag<T, 4, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 4>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                case 8: launch_kx(h->step_pdl, k_s_sdiag<T, 8, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 8>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
+                default: launch_kx(h->step_pdl, k_s_sdiag<T, 16, 1>, gd * kDiagSplit, 256, sdiag_smem<T, 16>(), h->stream, h->d_fronts, itd, (int)k, sb.inv2, sb.C, sb.W, n, nrhs); break;
             }
             MF_CUDA(cudaGetLastError());
             if (st.bwd.cnt) {
                 const unsigned gb = (unsigned)st.bwd.cnt;
                 const Item* itb = items + st.bwd.off;
                 switch (nrb) {
-                    case 1: launch_k(k_s_btile<T, 1>, gb, 256, btile_smem<T, 1>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 2: launch_k(k_s_btile<T, 2>, gb, 256, btile_smem<T, 2>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 4: launch_k(k_s_btile<T, 4>, gb, 256, btile_smem<T, 4>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    case 8: launch_k(k_s_btile<T, 8>, gb, 256, btile_smem<T, 8>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
-                    default: launch_k(k_s_btile<T, 16>, gb, 256, btile_smem<T, 16>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 1: launch_kx(h->step_pdl, k_s_btile<T, 1>, gb, 256, btile_smem<T, 1>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 2: launch_kx(h->step_pdl, k_s_btile<T, 2>, gb, 256, btile_smem<T, 2>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 4: launch_kx(h->step_pdl, k_s_btile<T, 4>, gb, 256, btile_smem<T, 4>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    case 8: launch_kx(h->step_pdl, k_s_btile<T, 8>, gb, 256, btile_smem<T, 8>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
+                    default: launch_kx(h->step_pdl, k_s_btile<T, 16>, gb, 256, btile_smem<T, 16>(), h->stream, h->d_fronts, itb, (int)k, sb.P, sb.C, sb.W, n, nrhs); break;
                 }
                 MF_CUDA(cudaGetLastError());
             }

@@ -106,7 +106,6 @@ class _DeviceBatch:
     or several patterns, as one forest on the handle's own stream."""
 
     def __init__(self, comp, patterns, mixed: bool, device: int, tol: float, maxit: int):
-        import torch
         self.comp = comp
         members = [patterns[k] for k, c in comp for _ in range(c)]
         self.members = members
@@ -119,8 +118,10 @@ class _DeviceBatch:
         self.lib = _native.gpulib()
         self.h = self.F._handle.h
         check(self.lib.mf_set_segments(self.h, len(members), ptr64(np.ascontiguousarray(off))), "mf_set_segments")
-        self.stream = torch.cuda.Stream(device=device)
-        check(self.lib.mf_set_stream(self.h, ctypes.c_void_p(self.stream.cuda_stream)), "mf_set_stream")
+        # the handle keeps the non-blocking stream the library created for it:
+        # torch.cuda.Stream() hands out streams from a fixed per-device pool,
+        # so past its size two handles would share a stream and two workers
+        # could capture graphs on it at once
         info = np.zeros(9, np.int64)
         self.lib.mf_info(self.h, info.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
         self.bytes = int(info[6])

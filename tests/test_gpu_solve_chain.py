@@ -148,3 +148,17 @@ def test_tiny_fronts_mixed_refined(monkeypatch):
     X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=True)), B, var="MF_TINY_SOLVE")
     assert np.array_equal(X["0"], X["1"])
     assert tm.backward_error(A, X["1"], B).max() <= 1e-12
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_step_kernels_with_programmatic_launch_equal_plain_launches(monkeypatch, mixed):
+    """The per-step kernels launched for programmatic dependence (they issue
+    their panel / inverse loads, then wait for the previous grid;
+    MF_STEP_PDL=1, the default) against plain stream-ordered launches
+    (MF_STEP_PDL=0), with the chain kernel off so every level runs the steps."""
+    monkeypatch.setenv("MF_SOLVE_CHAIN", "0")
+    A, P, S = grid(32, 30, 31, seed=71)
+    B = tm.rhs(S.n, 4, seed=14)
+    X = both(monkeypatch, lambda: mf.cholesky_(mf.ChordalCholesky(A, P, S, mixed=mixed)), B, var="MF_STEP_PDL")
+    assert np.array_equal(X["0"], X["1"])
+    assert tm.backward_error(A, X["1"], B).max() <= (1e-12 if mixed else 1e-13)
