@@ -201,21 +201,42 @@ __device__ __forceinline__ void small_fwd_front(const Front& f, const Front* __r
                 }
     }
     __syncwarp();
-    // R_j -= L21 x: lanes own rows of L21 (coalesced along the panel columns)
-    for (int a = lane; a < na; a += 32) {
-        T acc[NR];
+    // R_j -= L21 x: lanes own rows of L21 (coalesced along the panel
+    // columns), two rows (a, a + 32) at a time with eight columns of both
+    // loaded before their products: sixteen loads in flight per lane
+    for (int a = lane; a < na; a += 64) {
+        const bool two = a + 32 < na;
+        T acc0[NR], acc1[NR];
 #pragma unroll
-        for (int r = 0; r < NR; ++r) acc[r] = T(0);
-        const T* lr = Pj + nn + a;
-#pragma unroll 8
-        for (int k = 0; k < nn; ++k) {
-            const T l = lr[(int64_t)k * ld];
+        for (int r = 0; r < NR; ++r) acc0[r] = acc1[r] = T(0);
+        const T* lr0 = Pj + nn + a;
+        const T* lr1 = lr0 + 32;
+        for (int k0 = 0; k0 < nn; k0 += 8) {
+            T l0[8], l1[8];
 #pragma unroll
-            for (int r = 0; r < NR; ++r) acc[r] += l * C1[k + r * kSmallMax];
+            for (int u = 0; u < 8; ++u) {
+                const int k = k0 + u;
+                l0[u] = k < nn ? lr0[(int64_t)k * ld] : T(0);
+                l1[u] = (two && k < nn) ? lr1[(int64_t)k * ld] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int k = k0 + u;
+                if (k < nn)
+#pragma unroll
+                    for (int r = 0; r < NR; ++r) {
+                        const T c = C1[k + r * kSmallMax];
+                        acc0[r] += l0[u] * c;
+                        acc1[r] += l1[u] * c;
+                    }
+            }
         }
 #pragma unroll
         for (int r = 0; r < NR; ++r)
-            if (r < nrhs) Rj[a + r * na] -= acc[r];
+            if (r < nrhs) {
+                Rj[a + r * na] -= acc0[r];
+                if (two) Rj[a + 32 + r * na] -= acc1[r];
+            }
     }
 }
 
