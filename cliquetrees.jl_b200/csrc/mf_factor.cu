@@ -1594,9 +1594,9 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 }
                 if (st.diag.cnt) {
                     Timer t(h, K_DIAG);
-                    launch_k(k_diag<T, LDLT>, grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream, 
-                        h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
-                        h->d_rescued, reg);
+                    launch_kx(h->panel_pdl || pdl_enabled(), k_diag<T, LDLT>, grid_for(st.diag.cnt), 256,
+                        diag_smem<T>(), h->stream, h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d,
+                        h->d_signs, h->d_info, h->d_rescued, reg);
                     MF_CUDA(cudaGetLastError());
                 }
                 if (st.panel_tc.cnt) {
@@ -1613,21 +1613,21 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             }
             if (st.left.cnt) {
                 Timer t(h, K_LEFT);
-                launch_k(k_gemm<T, G_LEFT, LDLT>, grid_for(st.left.cnt), 256, gs, h->stream, 
-                    h->d_fronts, items + st.left.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
+                launch_kx(h->panel_pdl || pdl_enabled(), k_gemm<T, G_LEFT, LDLT>, grid_for(st.left.cnt), 256, gs,
+                    h->stream, h->d_fronts, items + st.left.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.diag.cnt) {
                 Timer t(h, K_DIAG);
-                launch_k(k_diag<T, LDLT>, grid_for(st.diag.cnt), 256, diag_smem<T>(), h->stream, 
-                    h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d, h->d_signs, h->d_info,
-                    h->d_rescued, reg);
+                launch_kx(h->panel_pdl || pdl_enabled(), k_diag<T, LDLT>, grid_for(st.diag.cnt), 256,
+                    diag_smem<T>(), h->stream, h->d_fronts, items + st.diag.off, c0, fb.P, fb.inv, fb.d,
+                    h->d_signs, h->d_info, h->d_rescued, reg);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.panel.cnt) {
                 Timer t(h, K_PANEL);
-                launch_k(k_gemm<T, G_TRSM, LDLT>, grid_for(st.panel.cnt), 256, gs, h->stream, 
-                    h->d_fronts, items + st.panel.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
+                launch_kx(h->panel_pdl || pdl_enabled(), k_gemm<T, G_TRSM, LDLT>, grid_for(st.panel.cnt), 256, gs,
+                    h->stream, h->d_fronts, items + st.panel.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
             }
             if (st.trail.cnt) {

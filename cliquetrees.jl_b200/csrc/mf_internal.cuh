@@ -310,6 +310,8 @@ struct mf_handle {
     int solve_chain = 2;           // k_s_chain launches: 1 every level (MF_SOLVE_CHAIN=1), 0 none (=0),
                                    // 2 the levels of at least kChainMinSteps steps (default)
     bool tiny_solve = true;        // k_s_tiny_* for the fronts with nj <= kTinyNJ (MF_TINY_SOLVE=0: k_s_small_*)
+    bool panel_pdl = false;        // the factorization's sub-panel chain (left-looking, diagonal block, TRSM)
+                                   // launched for programmatic dependence (MF_PANEL_PDL=1)
     bool step_pdl = true;          // solve-step kernels launched for programmatic dependence (MF_STEP_PDL=0: off)
     bool mid_solve = false;        // one cluster launch per single-super-block level and direction (MF_MID_SOLVE=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
