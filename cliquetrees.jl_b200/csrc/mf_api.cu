@@ -56,7 +56,8 @@ void free_all(mf_handle* h) {
                     h->f32.inv,  h->f32.d,    h->f32.R,    h->f32.W,    h->f32.C,      h->d_err,
                     h->d_part,   h->f32.part, h->d_tmaps,  h->d_tmap_inv, h->d_segptr, h->d_segred,
                     h->d_segeta, h->d_kry,    h->d_inv2,   h->f32.inv2,   h->d_chunkrow, h->d_chunkseg,
-                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued, h->d_chain, h->f32.split};
+                    h->d_segchunk, h->d_rowseg, h->d_chunkred, h->d_segsc, h->d_logdet, h->d_rescued, h->d_chain, h->f32.split,
+                    h->d_grow, h->d_gcon};
     release_graphs(h);
     if (h->cublas) cublasDestroy(static_cast<cublasHandle_t>(h->cublas));
     h->cublas = nullptr;
@@ -165,6 +166,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     rc = rc ? rc : dalloc(h, &h->d_ref, nfr, &tot);
     rc = rc ? rc : dalloc(h, &h->d_sepmap, (int64_t)h->h_sepmap.size(), &tot);
     rc = rc ? rc : dalloc(h, &h->d_items, (int64_t)h->h_items.size(), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_grow, std::max<int64_t>((int64_t)h->h_grow.size(), 1), &tot);
+    rc = rc ? rc : dalloc(h, &h->d_gcon, std::max<int64_t>((int64_t)h->h_gcon.size(), 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_P, h->npanel, &tot);
     rc = rc ? rc : dalloc(h, &h->d_inv, std::max<int64_t>(h->ninv, 1), &tot);
     rc = rc ? rc : dalloc(h, &h->d_inv2, std::max<int64_t>(h->ninv2, 1), &tot);
@@ -194,6 +197,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
     if (e == cudaSuccess) e = up(h->d_ref, h->h_ref.data(), sizeof(RefFront) * nfr);
     if (e == cudaSuccess) e = up(h->d_sepmap, h->h_sepmap.data(), sizeof(int32_t) * h->h_sepmap.size());
     if (e == cudaSuccess) e = up(h->d_items, h->h_items.data(), sizeof(Item) * h->h_items.size());
+    if (e == cudaSuccess) e = up(h->d_grow, h->h_grow.data(), sizeof(int64_t) * h->h_grow.size());
+    if (e == cudaSuccess) e = up(h->d_gcon, h->h_gcon.data(), sizeof(GCon) * h->h_gcon.size());
     if (e == cudaSuccess) e = cudaMemset(h->d_P, 0, sizeof(double) * std::max<int64_t>(h->npanel, 0));
     if (e == cudaSuccess) e = cudaMemset(h->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->d_rescued, 0, sizeof(int));

@@ -72,6 +72,15 @@ struct Item {
 };
 
 // A contiguous list of items inside the uploaded item buffer.
+// one child update row that lands on a row of a blocked front, for the
+// forward gather: the child's R block (at R + roff * nrhs, leading dimension
+// ma) row a
+struct GCon {
+    int64_t roff;
+    int32_t a;
+    int32_t ma;
+};
+
 struct ItemList {
     int64_t off = 0;
     int64_t cnt = 0;
@@ -301,6 +310,10 @@ struct mf_handle {
     double* d_R = nullptr;         // solve updates (sum na * nrhs_cap)
     double* d_W = nullptr;         // solve work (n * nrhs_cap)
     double* d_part = nullptr;      // backward partial sums
+    std::vector<int64_t> h_grow;   // forward gather: per row of every blocked front, its first GCon
+    std::vector<mf::GCon> h_gcon;  // forward gather contributions, row by row
+    int64_t* d_grow = nullptr;
+    mf::GCon* d_gcon = nullptr;
     int64_t nbwd_part = 0;         // partial slots (max over levels)
     int64_t nsplit_units = 0;      // largest number of split operand units one launch needs
     bool tc_split = true;          // tensor-core updates read pre-split operands (MF_TC_SPLIT=0: convert per tile)

@@ -407,7 +407,6 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
     auto begin = [&](ItemList& l) { l.off = (int64_t)items.size(); };
     auto end = [&](ItemList& l) { l.cnt = (int64_t)items.size() - l.off; };
     auto push = [&](int32_t f, int32_t a, int32_t b) { items.push_back(Item{f, a, b, 0}); };
-    std::vector<Item> gseg;  // forward-gather segments, appended after the levels
     std::vector<Item> easeg; // extend-add segments, appended after them
 
     // the 32-row warp-per-front factor measured slower than k_small with its
@@ -640,9 +639,11 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             if (solve_small(f) && task_of[j] < 0 && nj > kTinyNJ && nj <= kTinyNJ2) push(j, 0, 0);
         }
         end(lv.s_tiny2);
-        // forward gather: item (front, row tile, first segment, segments);
-        // a segment (child, a0, a1) is the run rel[a0:a1] of a child's update
-        // rows that lands in the tile, children in reverse order
+        // forward gather: item (front, row tile, first row pointer of the
+        // front, 0).  Row q of a blocked front owns the list of the children's
+        // update rows that land on it, children in reverse order (the order
+        // the reference adds them): h_grow[base + q] .. h_grow[base + q + 1]
+        // index h_gcon, one record (child roff, child row, child na) each
         begin(lv.s_gather);
         int max_sblocks = 0;
         int64_t max_l21 = 0;
@@ -654,24 +655,32 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
             const int nt = (int)cdiv(nj, kSolveRows);
             gfirst.push_back((int32_t)items.size());
             max_l21 = std::max<int64_t>(max_l21, (int64_t)f.nn * f.na);
-            std::vector<std::vector<Item>> per_tile((size_t)nt);
+            std::vector<int32_t> cnt((size_t)nj + 1, 0);
             for (int32_t p = f.chd1 - 1; p >= f.chd0; --p) {
-                const int32_t c = h->h_exec_chd[(size_t)p];
-                const Front& fc = h->h_fronts[(size_t)c];
+                const Front& fc = h->h_fronts[(size_t)h->h_exec_chd[(size_t)p]];
                 const int32_t* rel = h->h_exec_rel.data() + fc.sep0;
-                int a = 0;
-                while (a < fc.na) {
-                    const int t = rel[a] / kSolveRows;
-                    int b = a + 1;
-                    while (b < fc.na && rel[b] / kSolveRows == t) ++b;
-                    per_tile[(size_t)t].push_back(Item{c, a, b, 0});
-                    a = b;
-                }
+                for (int a = 0; a < fc.na; ++a) cnt[(size_t)rel[a] + 1] += 1;
             }
-            for (int t = 0; t < nt; ++t) {
-                items.push_back(Item{j, t, (int32_t)gseg.size(), (int32_t)per_tile[(size_t)t].size()});
-                gseg.insert(gseg.end(), per_tile[(size_t)t].begin(), per_tile[(size_t)t].end());
+            const int64_t base = (int64_t)h->h_grow.size(), c0 = (int64_t)h->h_gcon.size();
+            if (base + nj + 1 > INT32_MAX) {
+                set_error("plan: too many gather rows");
+                return -3;
             }
+            std::vector<int64_t> at((size_t)nj);
+            int64_t run = c0;
+            for (int q = 0; q <= nj; ++q) {
+                run += cnt[(size_t)q];
+                h->h_grow.push_back(run);
+                if (q < nj) at[(size_t)q] = run;
+            }
+            h->h_gcon.resize((size_t)run);
+            for (int32_t p = f.chd1 - 1; p >= f.chd0; --p) {
+                const Front& fc = h->h_fronts[(size_t)h->h_exec_chd[(size_t)p]];
+                const int32_t* rel = h->h_exec_rel.data() + fc.sep0;
+                for (int a = 0; a < fc.na; ++a)
+                    h->h_gcon[(size_t)at[(size_t)rel[a]]++] = GCon{fc.roff, a, fc.na};
+            }
+            for (int t = 0; t < nt; ++t) items.push_back(Item{j, t, (int32_t)base, 0});
             max_sblocks = std::max<int>(max_sblocks, (int)cdiv(f.nn, kSolveNB));
         }
         end(lv.s_gather);
@@ -860,19 +869,14 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
         items.insert(items.end(), tfr.begin(), tfr.end());
     }
     {
-        const int64_t base = (int64_t)items.size();
-        const int64_t ebase = base + (int64_t)gseg.size();
+        const int64_t ebase = (int64_t)items.size();
         if (ebase + (int64_t)easeg.size() > INT32_MAX) {
             set_error("plan: too many work items");
             return -3;
         }
-        for (const Level& lv : h->levels) {
-            for (int64_t i = lv.s_gather.off; i < lv.s_gather.off + lv.s_gather.cnt; ++i)
-                items[(size_t)i].b += (int32_t)base;
+        for (const Level& lv : h->levels)
             for (const ItemList* el : {&lv.ea, &lv.ea_upd})
                 for (int64_t i = el->off; i < el->off + el->cnt; ++i) items[(size_t)i].pad += (int32_t)ebase;
-        }
-        items.insert(items.end(), gseg.begin(), gseg.end());
         items.insert(items.end(), easeg.begin(), easeg.end());
     }
     begin(h->inv2_items);

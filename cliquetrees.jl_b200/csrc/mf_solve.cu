@@ -625,50 +625,41 @@ __global__ void __launch_bounds__(kSubWarps * 32, small_min_blocks<T, NR>() / 2)
 // ---------------------------------------------------------------------------
 // blocked fronts
 // ---------------------------------------------------------------------------
-// forward gather: W[res] = C[res] + child updates, R_j = child updates
+// forward gather: W[res] = C[res] + child updates, R_j = child updates.
+// One thread per (row, right-hand side) of the item's 256-row tile adds the
+// row's own list of child contributions (h_grow / h_gcon, children in the
+// reference's order), so no two threads touch one entry and the tile needs
+// no barrier
 template <typename T>
 __device__ __forceinline__ void gather_run(const Item& it, const Front* __restrict__ fronts,
-                                           const Item* __restrict__ all_items, const int32_t* __restrict__ reltgt,
+                                           const int64_t* __restrict__ grow, const GCon* __restrict__ gcon,
                                            const T* __restrict__ C, T* W, T* R, int64_t n, int nrhs) {
     const Front f = fronts[it.front];
     const int nn = f.nn, na = f.na, nj = nn + na;
     const int p0 = it.a * kSolveRows, p1 = min(p0 + kSolveRows, nj);
-    const int tid = threadIdx.x, nt = blockDim.x;
-    T* Rj = R + f.roff * nrhs;
     const int w = p1 - p0;
-    for (int i = tid; i < w * nrhs; i += nt) {
-        int q = p0 + i % w, r = i / w;
-        if (q < nn) W[f.col0 + q + (int64_t)r * n] = C[f.col0 + q + (int64_t)r * n];
-        else Rj[(q - nn) + r * na] = T(0);
-    }
-    __syncthreads();
-    // the plan's segments of this tile: (child, a0, a1), children in reverse
-    // order, at all_items[it.b ...] (indices into the whole item array)
-    for (int s = 0; s < it.pad; ++s) {
-        const Item sg = all_items[it.b + s];
-        const Front fc = fronts[sg.front];
-        const int ma = fc.na;
-        const int32_t* rel = reltgt + fc.sep0;
-        const T* Mc = R + fc.roff * nrhs;
-        const int cnt = sg.b - sg.a;
-        for (int i = tid; i < cnt * nrhs; i += nt) {
-            const int a = sg.a + i % cnt, r = i / cnt;
-            const int q = rel[a];
-            const T v = Mc[a + r * ma];
-            if (q < nn) W[f.col0 + q + (int64_t)r * n] += v;
-            else Rj[(q - nn) + r * na] += v;
+    const int64_t* rp = grow + it.b;
+    T* Rj = R + f.roff * nrhs;
+    for (int i = threadIdx.x; i < w * nrhs; i += blockDim.x) {
+        const int q = p0 + i % w, r = i / w;
+        T v = q < nn ? C[f.col0 + q + (int64_t)r * n] : T(0);
+        const int64_t e1 = rp[q + 1];
+        for (int64_t e = rp[q]; e < e1; ++e) {
+            const GCon g = gcon[e];
+            v += R[g.roff * nrhs + g.a + (int64_t)r * g.ma];
         }
-        __syncthreads();
+        if (q < nn) W[f.col0 + q + (int64_t)r * n] = v;
+        else Rj[(q - nn) + (int64_t)r * na] = v;
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_s_gather(const Front* __restrict__ fronts, const Item* __restrict__ items,
-                                                  const Item* __restrict__ all_items,
-                                                  const int32_t* __restrict__ reltgt, const T* __restrict__ C,
+                                                  const int64_t* __restrict__ grow,
+                                                  const GCon* __restrict__ gcon, const T* __restrict__ C,
                                                   T* __restrict__ W, T* __restrict__ R, int64_t n, int nrhs) {
     pdl_prologue();
-    gather_run<T>(items[blockIdx.x], fronts, all_items, reltgt, C, W, R, n, nrhs);
+    gather_run<T>(items[blockIdx.x], fronts, grow, gcon, C, W, R, n, nrhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1506,14 +1497,14 @@ __device__ __forceinline__ void midf_tile(const Front& f, int t, const T* __rest
 template <typename T, int NR>
 __global__ void __cluster_dims__(kMidCluster, 1, 1) __launch_bounds__(256)
     k_s_mid_fwd(const Front* __restrict__ fronts, const Item* __restrict__ mid, const Item* __restrict__ all_items,
-                const int32_t* __restrict__ reltgt, const T* __restrict__ inv2, const T* __restrict__ P, T* C, T* W,
-                T* R, int64_t n, int nrhs) {
+                const int64_t* __restrict__ grow, const GCon* __restrict__ gcon, const T* __restrict__ inv2,
+                const T* __restrict__ P, T* C, T* W, T* R, int64_t n, int nrhs) {
     pdl_prologue();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Item m = mid[blockIdx.x / kMidCluster];
     const int rank = (int)(blockIdx.x % kMidCluster);
     const Front f = fronts[m.front];
-    for (int t = rank; t < m.pad; t += kMidCluster) gather_run<T>(all_items[m.a + t], fronts, all_items, reltgt, C, W, R, n, nrhs);
+    for (int t = rank; t < m.pad; t += kMidCluster) gather_run<T>(all_items[m.a + t], fronts, grow, gcon, C, W, R, n, nrhs);
     mid_cluster_sync();
     for (int q = rank; q < kDiagSplit; q += kMidCluster) {
         sdiag_run<T, NR, 0>(f, 0, q, inv2, C, W, n, nrhs, sm_raw);
@@ -1636,8 +1627,8 @@ static int mid_go(mf_handle* h, const Level& lv, const SolveBufs<T>& sb, int nrh
     const Item* it = h->d_items + lv.s_mid.off;
     if (!BWD) {
         MF_CUDA(cudaFuncSetAttribute(k_s_mid_fwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, midf_smem<T, NR>()));
-        launch_k(k_s_mid_fwd<T, NR>, g, 256, midf_smem<T, NR>(), h->stream, h->d_fronts, it, h->d_items, h->d_reltgt,
-                 sb.inv2, sb.P, sb.C, sb.W, sb.R, h->n, nrhs);
+        launch_k(k_s_mid_fwd<T, NR>, g, 256, midf_smem<T, NR>(), h->stream, h->d_fronts, it, h->d_items, h->d_grow,
+                 h->d_gcon, sb.inv2, sb.P, sb.C, sb.W, sb.R, h->n, nrhs);
     } else {
         MF_CUDA(cudaFuncSetAttribute(k_s_mid_bwd<T, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, midb_smem<T, NR>()));
         launch_k(k_s_mid_bwd<T, NR>, g, 256, midb_smem<T, NR>(), h->stream, h->d_fronts, it, h->d_septgt, sb.inv2,
@@ -1793,7 +1784,7 @@ static int solve_impl(mf_handle* h, const SolveBufs<T>& sb, int nrhs) {
         if (lv.s_gather.cnt) {
             Timer t(h, K_S_GATHER);
             launch_k(k_s_gather<T>, (unsigned)lv.s_gather.cnt, 256, 0, h->stream, 
-                h->d_fronts, items + lv.s_gather.off, items, h->d_reltgt, sb.C, sb.W, sb.R, n, nrhs);
+                h->d_fronts, items + lv.s_gather.off, h->d_grow, h->d_gcon, sb.C, sb.W, sb.R, n, nrhs);
             MF_CUDA(cudaGetLastError());
         }
         const bool chain = use_chain(lv);
