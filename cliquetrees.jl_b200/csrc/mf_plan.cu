@@ -742,32 +742,55 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 const int w = std::min(kSolveNB, f.nn - k0);
                 return f.nn > k0 + w ? (int)cdiv(f.nn - ((k0 + w) & ~3), kFwdRows) : 0;
             };
-            begin(lv.s_chain_f);
-            for (int k = 0; k < max_sblocks; ++k) {
+            // Ticket order D(0) C(0) D(1) B(0) C(1) D(2) B(1) ...: D(k) the
+            // diagonal parts of step k, C(k) its four tiles of the next
+            // super-block (what D(k + 1) waits for), B(k) its other tiles.  The
+            // next step's diagonal parts come right after the tiles they wait
+            // for instead of behind the step's bulk, and every item still
+            // waits only on smaller tickets (C(k + 1) on B(k) and D(k + 1)).
+            auto diag_parts = [&](int k) {
+                for (size_t i = 0; i < bf.size(); ++i)
+                    if (h->h_fronts[bf[i]].nn > k * kSolveNB)
+                        for (int q = 0; q < nsplit; ++q) items.push_back(Item{bf[i], -1 - q, k, cbf[i]});
+            };
+            auto fwd_range = [&](int k, int t0, int t1) {
                 const int k0 = k * kSolveNB;
                 int maxt = 0;
-                for (size_t i = 0; i < bf.size(); ++i) {
-                    const Front& f = h->h_fronts[bf[i]];
-                    if (f.nn <= k0) continue;
-                    for (int q = 0; q < nsplit; ++q) items.push_back(Item{bf[i], -1 - q, k, cbf[i]});
-                    maxt = std::max(maxt, fwd_tiles(f, k0));
-                }
-                for (int t = 0; t < maxt; ++t)
+                for (size_t i = 0; i < bf.size(); ++i)
+                    if (h->h_fronts[bf[i]].nn > k0) maxt = std::max(maxt, fwd_tiles(h->h_fronts[bf[i]], k0));
+                for (int t = t0; t < std::min(t1, maxt); ++t)
                     for (size_t i = 0; i < bf.size(); ++i) {
                         const Front& f = h->h_fronts[bf[i]];
                         if (f.nn > k0 && t < fwd_tiles(f, k0)) items.push_back(Item{bf[i], t, k, cbf[i]});
                     }
+            };
+            begin(lv.s_chain_f);
+            diag_parts(0);
+            for (int k = 0; k < max_sblocks; ++k) {
+                fwd_range(k, 0, 4);                                   // C(k)
+                if (k + 1 < max_sblocks) diag_parts(k + 1);           // D(k + 1)
+                fwd_range(k, 4, INT32_MAX);                           // B(k)
             }
             end(lv.s_chain_f);
-            begin(lv.s_chain_b);
-            for (int k = max_sblocks - 1; k >= 0; --k) {
-                const int k0 = k * kSolveNB;
+            auto bdiag_parts = [&](int k) {
                 for (size_t i = 0; i < bf.size(); ++i)
-                    if (h->h_fronts[bf[i]].nn > k0)
+                    if (h->h_fronts[bf[i]].nn > k * kSolveNB)
                         for (int q = 0; q < nsplit; ++q) items.push_back(Item{bf[i], -1 - q, k, cbb[i]});
-                for (int t = (int)cdiv(k0, kNB) - 1; t >= 0; --t)
+            };
+            // tiles t1 - 1 down to t0 of step k (columns left of super-block k)
+            auto bwd_range = [&](int k, int t0, int t1) {
+                const int k0 = k * kSolveNB;
+                for (int t = t1 - 1; t >= std::max(t0, 0); --t)
                     for (size_t i = 0; i < bf.size(); ++i)
                         if (h->h_fronts[bf[i]].nn > k0) items.push_back(Item{bf[i], t, k, cbb[i]});
+            };
+            begin(lv.s_chain_b);
+            bdiag_parts(max_sblocks - 1);
+            for (int k = max_sblocks - 1; k >= 0; --k) {
+                const int nt = (int)cdiv(k * kSolveNB, kNB);
+                bwd_range(k, nt - 4, nt);                             // C(k)
+                if (k > 0) bdiag_parts(k - 1);                        // D(k - 1)
+                bwd_range(k, 0, nt - 4);                              // B(k)
             }
             end(lv.s_chain_b);
             if (h->nchain > INT32_MAX) {
