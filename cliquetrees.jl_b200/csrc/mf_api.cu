@@ -64,6 +64,11 @@ void free_all(mf_handle* h) {
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    h->side = nullptr;
+    h->ev_fork = h->ev_join = nullptr;
 }
 
 int init_info(mf_handle* h) {
@@ -139,9 +144,15 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         rc = -4;
     }
     if (rc) { delete h; return rc; }
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
-        set_error("cudaStreamCreate failed");
+        set_error("cudaStreamCreate / cudaEventCreate failed");
+        if (h->stream) cudaStreamDestroy(h->stream);
+        if (h->side) cudaStreamDestroy(h->side);
+        if (h->ev_fork) cudaEventDestroy(h->ev_fork);
         delete h;
         return -3;
     }
@@ -220,6 +231,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         // no faster (80^3: 42.5 vs 42.2 ms; KKT: 232.6 vs 228.9 ms): opt-in
         const char* ppenv = getenv("MF_PANEL_PDL");
         h->panel_pdl = ppenv && ppenv[0] == '1';
+        const char* lenv = getenv("MF_LOOKAHEAD");
+        h->lookahead = !(lenv && lenv[0] == '0');
         const char* penv = getenv("MF_STEP_PDL");
         h->step_pdl = !(penv && penv[0] == '0');
         const char* tenv = getenv("MF_TINY_SOLVE");

@@ -284,6 +284,7 @@ constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
 constexpr int kSmallNarrowNJ = 48;     // levels whose small fronts all have nj <= this ...
 constexpr int kSmallWideLevel = 4 * 148;  // ... and that hold at least this many run 128-thread CTAs,
 constexpr int kSmallTinyNJ = 32;       // 64-thread CTAs when nj <= this
+constexpr int kSideFreeSMs = 24;       // SMs the look-ahead trailing update leaves to the sub-panel kernels
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -1581,6 +1582,36 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             MF_CUDA(cudaGetLastError());
         }
         if (h->tuning) MF_CUDA(cudaEventRecord(tev[0], h->stream));
+        // Look-ahead: an outer block's trailing update runs its tiles of the
+        // next outer block's columns on `stream` and the rest on `side`,
+        // beside the next block's sub-panels (which touch only their own
+        // columns); `stream` waits for `side` before the next trailing update
+        // (its columns overlap, and it reuses the split operands) and before
+        // the SYRK.  The persistent tensor-core kernel on `side` leaves
+        // kSideFreeSMs SMs to the sub-panel kernels.  Profile and tuning runs
+        // stay on one stream.
+        const bool la_on = h->lookahead && h->side && !h->profile && !h->tuning;
+        bool pending = false;
+        auto join = [&]() -> int {
+            if (pending) MF_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+            pending = false;
+            return 0;
+        };
+        // launch `body` on `side` after the work queued on `stream` so far
+        auto on_side = [&](const std::function<int()>& body) -> int {
+            MF_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+            MF_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+            cudaStream_t main = h->stream;
+            h->stream = h->side;
+            h->grid_cap = std::max(1, (h->num_sms > 0 ? h->num_sms : 148) - kSideFreeSMs);
+            const int rc = body();
+            h->grid_cap = 0;
+            h->stream = main;
+            if (rc) return rc;
+            MF_CUDA(cudaEventRecord(h->ev_join, h->side));
+            pending = true;
+            return 0;
+        };
         for (const PanelStep& st : lv.steps) {
             const int obs = st.b * lv.kob, obw = lv.kob;
             const int c0 = obs + st.s * kNB;
@@ -1605,9 +1636,20 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
                 }
                 if (st.trail_tc.cnt) {
                     Timer t(h, K_UPDATE);
-                    rc = h->tc_split ? tc_launch_split(h, 1, st.trail_tc, st.split_tc, obs, obw, c0, f32b)
-                                     : tc_launch(h, 1, st.trail_tc, obs, obw, c0, f32b);
+                    if ((rc = join())) return rc;
+                    const bool la = la_on && st.trail_tc_ncrit > 0 && st.trail_tc_ncrit < st.trail_tc.cnt;
+                    const ItemList crit{st.trail_tc.off, la ? st.trail_tc_ncrit : st.trail_tc.cnt};
+                    rc = h->tc_split ? tc_launch_split(h, 1, crit, st.split_tc, obs, obw, c0, f32b)
+                                     : tc_launch(h, 1, crit, obs, obw, c0, f32b);
                     if (rc) return rc;
+                    if (la) {
+                        const ItemList bulk{st.trail_tc.off + st.trail_tc_ncrit, st.trail_tc.cnt - st.trail_tc_ncrit};
+                        rc = on_side([&]() {
+                            return h->tc_split ? tc_launch_split(h, 1, bulk, ItemList{}, obs, obw, c0, f32b)
+                                               : tc_launch(h, 1, bulk, obs, obw, c0, f32b);
+                        });
+                        if (rc) return rc;
+                    }
                 }
                 continue;
             }
@@ -1632,11 +1674,24 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             }
             if (st.trail.cnt) {
                 Timer t(h, K_UPDATE);
-                launch_k(k_gemm<T, G_TRAIL, LDLT>, grid_for(st.trail.cnt), 256, gs, h->stream, 
+                if (int rc = join()) return rc;
+                const bool la = la_on && st.trail_ncrit > 0 && st.trail_ncrit < st.trail.cnt;
+                const int64_t ncrit = la ? st.trail_ncrit : st.trail.cnt;
+                launch_k(k_gemm<T, G_TRAIL, LDLT>, grid_for(ncrit), 256, gs, h->stream,
                     h->d_fronts, items + st.trail.off, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
                 MF_CUDA(cudaGetLastError());
+                if (la) {
+                    const int rc = on_side([&]() -> int {
+                        launch_k(k_gemm<T, G_TRAIL, LDLT>, grid_for(st.trail.cnt - ncrit), 256, gs, h->stream,
+                            h->d_fronts, items + st.trail.off + ncrit, obs, obw, c0, fb.P, fb.M, fb.d, fb.inv);
+                        MF_CUDA(cudaGetLastError());
+                        return 0;
+                    });
+                    if (rc) return rc;
+                }
             }
         }
+        if (int rc = join()) return rc;
         if (h->tuning) MF_CUDA(cudaEventRecord(tev[1], h->stream));
         if (std::is_same<T, float>::value && h->use_tc && lv.tc_syrk) {
             if (lv.syrk_tc.cnt) {

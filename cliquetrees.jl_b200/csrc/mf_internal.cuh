@@ -123,6 +123,9 @@ struct PanelStep {
     ItemList diag;    // (front)            : diagonal block factor + inverse
     ItemList panel;   // (front, row tile)  : panel TRSM below the diagonal block (GEMM with the inverse)
     ItemList trail;   // (front, ti, tj)    : after the last sub-panel of an outer block: trailing update, K = kob
+    // the first trail_ncrit (trail_tc_ncrit) items update the next outer
+    // block's columns; the rest may run beside that block's sub-panels
+    int64_t trail_ncrit = 0, trail_tc_ncrit = 0;
     // the same work in 128-row tiles for the tensor-core (tcgen05) kernels
     ItemList left_tc, panel_tc, trail_tc;
     // (front, 128-row block, 32-column chunk, first unit): the trailing
@@ -325,6 +328,11 @@ struct mf_handle {
     bool tiny_solve = true;        // k_s_tiny_* for the fronts with nj <= kTinyNJ (MF_TINY_SOLVE=0: k_s_small_*)
     bool panel_pdl = false;        // the factorization's sub-panel chain (left-looking, diagonal block, TRSM)
                                    // launched for programmatic dependence (MF_PANEL_PDL=1)
+    cudaStream_t side = nullptr;   // the factorization's look-ahead stream (trailing updates beside the next
+                                   // outer block's sub-panels), forked from and joined into `stream`
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool lookahead = true;         // MF_LOOKAHEAD=0: every trailing update on `stream`
+    int grid_cap = 0;              // while > 0: the persistent tensor-core kernels' CTA count limit
     bool step_pdl = true;          // solve-step kernels launched for programmatic dependence (MF_STEP_PDL=0: off)
     bool mid_solve = false;        // one cluster launch per single-super-block level and direction (MF_MID_SOLVE=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order

@@ -520,20 +520,26 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                     for (int t = 0; t < (int)cdiv(f.nn + f.na - c0 - w, kTile); ++t) push(j, t, 0);
                 }
                 end(st.panel);
+                // trailing update: first the tiles of the next outer block's
+                // columns (what its sub-panels wait for), then the rest
+                // (st.trail_ncrit / trail_tc_ncrit count the first part)
                 begin(st.trail);
                 const bool last_sub = (sp == kob / kNB - 1) || (c0 + kNB >= lv.max_nn_blocked);
                 if (last_sub)
-                    for (int32_t j : fr) {
-                        const Front& f = h->h_fronts[j];
-                        if (f.nn + f.na <= kSmallMax || f.nn <= ob * kob) continue;
-                        const int e = std::min(f.nn, (ob + 1) * kob);
-                        if (e >= f.nn) continue;  // no panel columns after this outer block
-                        const int nj = f.nn + f.na;
-                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
-                            const int cs = e + tj * kTile;
-                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTile); ++ti) push(j, ti, tj);
+                    for (int part = 0; part < 2; ++part)
+                        for (int32_t j : fr) {
+                            const Front& f = h->h_fronts[j];
+                            if (f.nn + f.na <= kSmallMax || f.nn <= ob * kob) continue;
+                            const int e = std::min(f.nn, (ob + 1) * kob);
+                            if (e >= f.nn) continue;  // no panel columns after this outer block
+                            const int nj = f.nn + f.na;
+                            for (int tj = 0; tj < (int)cdiv(f.nn - e, kTile); ++tj) {
+                                if ((tj < kob / kTile) != (part == 0)) continue;
+                                const int cs = e + tj * kTile;
+                                for (int ti = 0; ti < (int)cdiv(nj - cs, kTile); ++ti) push(j, ti, tj);
+                            }
+                            if (part == 0) st.trail_ncrit = (int64_t)items.size() - st.trail.off;
                         }
-                    }
                 end(st.trail);
                 // 128-row tiles for the tcgen05 kernels
                 begin(st.left_tc);
@@ -556,8 +562,10 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                 begin(st.trail_tc);
                 std::vector<Item> split;
                 int64_t units = 0;
-                if (last_sub)
-                    for (int32_t j : fr) {
+                if (last_sub) {
+                    std::vector<int64_t> ubase(fr.size(), -1);
+                    for (size_t i = 0; i < fr.size(); ++i) {
+                        const int32_t j = fr[i];
                         const Front& f = h->h_fronts[j];
                         if (f.nn + f.na <= kSmallMax || f.nn <= ob * kob) continue;
                         const int e = std::min(f.nn, (ob + 1) * kob);
@@ -567,14 +575,27 @@ int build_plan(mf_handle* h, const int64_t* resptr, const int64_t* sepptr, const
                         const int nrb = (int)cdiv(nj - e, kSplitRows), nkc = (int)cdiv(e - ob * kob, kSplitK);
                         for (int rb = 0; rb < nrb; ++rb)
                             for (int kc = 0; kc < nkc; ++kc) split.push_back(Item{j, rb, kc, (int32_t)units});
-                        for (int tj = 0; tj < (int)cdiv(f.nn - e, kTcTrailN); ++tj) {
-                            const int cs = e + tj * kTcTrailN;
-                            // rows from the first 128-aligned tile that reaches the diagonal
-                            for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti)
-                                items.push_back(Item{j, ti, tj, (int32_t)units});
-                        }
+                        ubase[i] = units;
                         units += (int64_t)nrb * nkc * (h->diag ? 2 : 1);
                     }
+                    for (int part = 0; part < 2; ++part) {
+                        for (size_t i = 0; i < fr.size(); ++i) {
+                            if (ubase[i] < 0) continue;
+                            const int32_t j = fr[i];
+                            const Front& f = h->h_fronts[j];
+                            const int e = std::min(f.nn, (ob + 1) * kob);
+                            const int nj = f.nn + f.na;
+                            for (int tj = 0; tj < (int)cdiv(f.nn - e, kTcTrailN); ++tj) {
+                                if ((tj < kob / kTcTrailN) != (part == 0)) continue;
+                                const int cs = e + tj * kTcTrailN;
+                                // rows from the first 128-aligned tile that reaches the diagonal
+                                for (int ti = 0; ti < (int)cdiv(nj - cs, kTM); ++ti)
+                                    items.push_back(Item{j, ti, tj, (int32_t)ubase[i]});
+                            }
+                        }
+                        if (part == 0) st.trail_tc_ncrit = (int64_t)items.size() - st.trail_tc.off;
+                    }
+                }
                 end(st.trail_tc);
                 begin(st.split_tc);
                 items.insert(items.end(), split.begin(), split.end());

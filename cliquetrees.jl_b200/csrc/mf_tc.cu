@@ -580,7 +580,7 @@ template <int ROLE, int LDLT>
 static int launch_one(mf_handle* h, const ItemList& l, int obs, int obw, int c0, const FactorBufs<float>& fb) {
     if (!l.cnt) return 0;
     constexpr int smem = tc::Cfg<TcTileN<ROLE>::value>::SMEM_BYTES;
-    const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
+    const int64_t grid = std::min<int64_t>(l.cnt, h->grid_cap > 0 ? h->grid_cap : h->num_sms > 0 ? h->num_sms : 148);
     launch_kx(pdl_enabled() || (h->panel_pdl && (ROLE == 0 || ROLE == 3)), k_gemm_tc<ROLE, LDLT, false>,
               (unsigned)grid, tc::NT, smem, h->stream, 
         h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
@@ -664,7 +664,7 @@ static int launch_split(mf_handle* h, const ItemList& l, const ItemList& units, 
         MF_CUDA(cudaGetLastError());
     }
     constexpr int smem = tc::SplitCfg<TcTileN<ROLE>::value>::SMEM_BYTES;
-    const int64_t grid = std::min<int64_t>(l.cnt, h->num_sms > 0 ? h->num_sms : 148);
+    const int64_t grid = std::min<int64_t>(l.cnt, h->grid_cap > 0 ? h->grid_cap : h->num_sms > 0 ? h->num_sms : 148);
     launch_k(k_gemm_tc<ROLE, LDLT, true>, (unsigned)grid, tc::NT, smem, h->stream, 
         h->d_fronts, h->d_items + l.off, l.cnt, obs, obw, c0, fb.P, fb.M, fb.d,
         reinterpret_cast<const CUtensorMap*>(h->d_tmaps), reinterpret_cast<const CUtensorMap*>(h->d_tmap_inv),
