@@ -231,6 +231,8 @@ int mf_create(int64_t n, int64_t nfr, const int64_t* resptr, const int64_t* sepp
         // no faster (80^3: 42.5 vs 42.2 ms; KKT: 232.6 vs 228.9 ms): opt-in
         const char* ppenv = getenv("MF_PANEL_PDL");
         h->panel_pdl = ppenv && ppenv[0] == '1';
+        const char* fenv = getenv("MF_SIDE_FREE_SMS");
+        if (fenv && atoi(fenv) >= 0) h->side_free_sms = atoi(fenv);
         const char* lenv = getenv("MF_LOOKAHEAD");
         h->lookahead = !(lenv && lenv[0] == '0');
         const char* penv = getenv("MF_STEP_PDL");

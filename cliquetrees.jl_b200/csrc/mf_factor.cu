@@ -284,7 +284,6 @@ constexpr int kSmallRescue = 67;  // 67^2 doubles <= kSmallMax^2 floats
 constexpr int kSmallNarrowNJ = 48;     // levels whose small fronts all have nj <= this ...
 constexpr int kSmallWideLevel = 4 * 148;  // ... and that hold at least this many run 128-thread CTAs,
 constexpr int kSmallTinyNJ = 32;       // 64-thread CTAs when nj <= this
-constexpr int kSideFreeSMs = 24;       // SMs the look-ahead trailing update leaves to the sub-panel kernels
 
 template <typename T, int LDLT>
 __global__ void __launch_bounds__(256) k_small(const Front* __restrict__ fronts, const Item* __restrict__ items,
@@ -1588,7 +1587,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
         // columns); `stream` waits for `side` before the next trailing update
         // (its columns overlap, and it reuses the split operands) and before
         // the SYRK.  The persistent tensor-core kernel on `side` leaves
-        // kSideFreeSMs SMs to the sub-panel kernels.  Profile and tuning runs
+        // side_free_sms SMs to the sub-panel kernels.  Profile and tuning runs
         // stay on one stream.
         const bool la_on = h->lookahead && h->side && !h->profile && !h->tuning;
         bool pending = false;
@@ -1603,7 +1602,7 @@ static int factor_impl(mf_handle* h, const FactorBufs<T>& fb) {
             MF_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
             cudaStream_t main = h->stream;
             h->stream = h->side;
-            h->grid_cap = std::max(1, (h->num_sms > 0 ? h->num_sms : 148) - kSideFreeSMs);
+            h->grid_cap = std::max(1, (h->num_sms > 0 ? h->num_sms : 148) - h->side_free_sms);
             const int rc = body();
             h->grid_cap = 0;
             h->stream = main;

@@ -333,6 +333,7 @@ struct mf_handle {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool lookahead = true;         // MF_LOOKAHEAD=0: every trailing update on `stream`
     int grid_cap = 0;              // while > 0: the persistent tensor-core kernels' CTA count limit
+    int side_free_sms = 24;        // SMs the look-ahead trailing update leaves to the sub-panel kernels (MF_SIDE_FREE_SMS)
     bool step_pdl = true;          // solve-step kernels launched for programmatic dependence (MF_STEP_PDL=0: off)
     bool mid_solve = false;        // one cluster launch per single-super-block level and direction (MF_MID_SOLVE=1)
     double* d_C = nullptr;         // solve rhs / solution (n * nrhs_cap), permuted order
