@@ -1,7 +1,7 @@
 """Mixed-precision form on the GPU: FP32 fronts (same plan, single-precision
 kernels) with FP64 refinement, checked against the FP64 oracle.
 
-Bar: normwise backward error <= 1e-12 (the north star's mixed target) and
+Bar: normwise backward error <= 1e-12 (the refinement's default tolerance) and
 the solution within 1e-9 relative of the oracle's or 4 kappa_1 eps."""
 import numpy as np
 import pytest
